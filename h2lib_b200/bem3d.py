@@ -1,0 +1,305 @@
+"""Python mirror of H2Lib's bem3d / h2matrix / krylovsolvers interface for the B200 path.
+
+Function names, argument order and meaning follow H2Lib (file:line of the reference given per
+function); every compute call goes through the C ABI of libh2b200.so (include/h2b200.h).
+Arrays may be numpy arrays (host) or CUDA tensors exposing data_ptr() (device).
+"""
+import ctypes as C
+
+import numpy as np
+
+from ._lib import (BASIS_CONSTANT, BASIS_LINEAR, DLP, HELMHOLTZ, LAPLACE, MESH_CUBE,
+                   MESH_SPHERE, SLP, H2BError, check, checkp, lib)
+
+__all__ = [
+    "BASIS_CONSTANT_BEM3D", "BASIS_LINEAR_BEM3D", "Surface3d", "new_sphere_surface3d",
+    "new_cube_surface3d", "new_slp_laplace_bem3d", "new_dlp_laplace_bem3d",
+    "new_slp_helmholtz_bem3d", "new_dlp_helmholtz_bem3d", "assemble_bem3d_amatrix",
+    "nearfield", "Tree", "build_tree", "H2Matrix", "addeval_h2matrix_avector",
+    "solve_gmres_h2matrix_avector", "solve_gmres", "quad_export",
+]
+
+BASIS_CONSTANT_BEM3D = BASIS_CONSTANT
+BASIS_LINEAR_BEM3D = BASIS_LINEAR
+
+
+def _ptr(a):
+    """Raw pointer of a numpy array or a CUDA tensor."""
+    if a is None:
+        return None
+    if hasattr(a, "data_ptr"):
+        return C.c_void_p(a.data_ptr())
+    if isinstance(a, np.ndarray):
+        if not a.flags["C_CONTIGUOUS"] and not a.flags["F_CONTIGUOUS"]:
+            raise ValueError("array must be contiguous")
+        return C.c_void_p(a.ctypes.data)
+    raise TypeError(f"unsupported array type {type(a)}")
+
+
+class Surface3d:
+    """Mesh arrays of H2Lib's struct _surface3d (Library/surface3d.h:45) plus the device copy."""
+
+    def __init__(self, x, t):
+        self.x = np.ascontiguousarray(x, dtype=np.float64).reshape(-1, 3)
+        self.t = np.ascontiguousarray(t, dtype=np.uint32).reshape(-1, 3)
+        self.vertices = self.x.shape[0]
+        self.triangles = self.t.shape[0]
+        self.n = np.zeros((self.triangles, 3))
+        self.g = np.zeros(self.triangles)
+        h = np.zeros(2)
+        check(lib.h2b_prepare_surface(self.vertices, self.x, self.triangles, self.t, self.n,
+                                      self.g, h), "prepare_surface3d")
+        self.hmin, self.hmax = h
+        self._dev = None
+
+    @property
+    def handle(self):
+        if self._dev is None:
+            self._dev = checkp(lib.h2b_surface_new(self.vertices, self.x, self.triangles, self.t,
+                                                   self.n, self.g), "h2b_surface_new")
+        return self._dev
+
+    def __del__(self):
+        if getattr(self, "_dev", None):
+            lib.h2b_surface_del(self._dev)
+            self._dev = None
+
+
+def _macro(kind, split):
+    nv, nt = C.c_uint32(), C.c_uint32()
+    check(lib.h2b_macro_mesh_size(kind, split, C.byref(nv), C.byref(nt)), "macro_mesh_size")
+    x = np.zeros((nv.value, 3))
+    t = np.zeros((nt.value, 3), dtype=np.uint32)
+    check(lib.h2b_macro_mesh_build(kind, split, x, t), "macro_mesh_build")
+    return x, t
+
+
+def new_sphere_surface3d(split):
+    """new_sphere_macrosurface3d + build_from_macrosurface3d_surface3d(mg, split)
+    (Library/macrosurface3d.c:81, :707): 8*split^2 triangles on the unit sphere."""
+    return Surface3d(*_macro(MESH_SPHERE, split))
+
+
+def new_cube_surface3d(split):
+    """new_cube_macrosurface3d + build_from_macrosurface3d_surface3d (Library/macrosurface3d.c:390,
+    :707): 12*split^2 triangles on the surface of [-1,1]^3."""
+    return Surface3d(*_macro(MESH_CUBE, split))
+
+
+def new_ellipsoid_surface3d(split, axes):
+    """Sphere refined `split` times, scaled per axis (semi-axes `axes`)."""
+    x, t = _macro(MESH_SPHERE, split)
+    check(lib.h2b_scale_vertices(x.shape[0], x, np.asarray(axes, dtype=np.float64)), "scale")
+    return Surface3d(x, t)
+
+
+class Bem3d:
+    """Operator handle: the counterpart of H2Lib's pbem3d (Library/bem3d.h:290)."""
+
+    def __init__(self, gr, pde, layer, q_regular, q_singular, row_basis, col_basis, k=0.0,
+                 alpha=0.0):
+        self.gr = gr
+        self.pde, self.layer = pde, layer
+        self.row_basis, self.col_basis = row_basis, col_basis
+        self.k = complex(k)
+        self.alpha = complex(alpha)
+        self.q_regular, self.q_singular = q_regular, q_singular
+        self.handle = checkp(lib.h2b_bem_new(gr.handle, pde, layer, row_basis, col_basis,
+                                             q_regular, q_singular, self.k.real, self.k.imag,
+                                             self.alpha.real, self.alpha.imag), "h2b_bem_new")
+        self.rows = gr.vertices if row_basis == BASIS_LINEAR else gr.triangles
+        self.cols = gr.vertices if col_basis == BASIS_LINEAR else gr.triangles
+        self.dtype = np.complex128 if pde == HELMHOLTZ else np.float64
+
+    def __del__(self):
+        if getattr(self, "handle", None):
+            lib.h2b_bem_del(self.handle)
+            self.handle = None
+
+
+def new_slp_laplace_bem3d(gr, q_regular, q_singular, row_basis, col_basis):
+    """Library/laplacebem3d.c:844"""
+    return Bem3d(gr, LAPLACE, SLP, q_regular, q_singular, row_basis, col_basis)
+
+
+def new_dlp_laplace_bem3d(gr, q_regular, q_singular, row_basis, col_basis, alpha):
+    """Library/laplacebem3d.c:1012"""
+    return Bem3d(gr, LAPLACE, DLP, q_regular, q_singular, row_basis, col_basis, alpha=alpha)
+
+
+def new_slp_helmholtz_bem3d(k, gr, q_regular, q_singular, row_basis, col_basis):
+    """Library/helmholtzbem3d.c:1008"""
+    return Bem3d(gr, HELMHOLTZ, SLP, q_regular, q_singular, row_basis, col_basis, k=k)
+
+
+def new_dlp_helmholtz_bem3d(k, gr, q_regular, q_singular, row_basis, col_basis, alpha):
+    """Library/helmholtzbem3d.c:1177"""
+    return Bem3d(gr, HELMHOLTZ, DLP, q_regular, q_singular, row_basis, col_basis, k=k,
+                 alpha=alpha)
+
+
+def nearfield(bem, ridx, cidx, ntrans=False, out=None):
+    """bem->nearfield(ridx, cidx, bem, ntrans, N) (Library/bem3d.h:380).  Returns N as a
+    column-major (Fortran-ordered) numpy array of shape (rows, cols) (transposed if ntrans)."""
+    rows = bem.rows if ridx is None else len(ridx)
+    cols = bem.cols if cidx is None else len(cidx)
+    ri = None if ridx is None else np.ascontiguousarray(ridx, dtype=np.uint32)
+    ci = None if cidx is None else np.ascontiguousarray(cidx, dtype=np.uint32)
+    shape = (cols, rows) if ntrans else (rows, cols)
+    if out is None:
+        out = np.zeros(shape, dtype=bem.dtype, order="F")
+    ld = out.shape[0] if isinstance(out, np.ndarray) else shape[0]
+    check(lib.h2b_bem_nearfield(bem.handle, _ptr(ri), rows, _ptr(ci), cols, int(ntrans),
+                                _ptr(out), ld), "nearfield")
+    return out
+
+
+def assemble_bem3d_amatrix(bem, G=None):
+    """Library/bem3d.c:9988: dense matrix of the operator (square)."""
+    if G is None:
+        G = np.zeros((bem.rows, bem.rows), dtype=bem.dtype, order="F")
+    ld = G.shape[0] if isinstance(G, np.ndarray) else bem.rows
+    check(lib.h2b_bem_assemble_amatrix(bem.handle, _ptr(G), ld), "assemble_bem3d_amatrix")
+    return G
+
+
+class Tree:
+    """Cluster trees + block leaves (build_bem3d_cluster, Library/bem3d.c:932;
+    build_strict_block + admissible_max_cluster, Library/block.c:258/52)."""
+
+    def __init__(self, handle):
+        self.handle = handle
+        info = np.zeros(8, dtype=np.uint64)
+        check(lib.h2b_tree_info(handle, info), "tree_info")
+        self.row_clusters, self.col_clusters = int(info[0]), int(info[1])
+        self.row_n, self.col_n = int(info[2]), int(info[3])
+        self.blocks, self.admissible, self.near_entries = int(info[4]), int(info[5]), int(info[6])
+        self.row_depth, self.col_depth = int(info[7]) & 0xFFFFFFFF, int(info[7]) >> 32
+
+    def clusters(self, which=0):
+        n = self.row_clusters if which == 0 else self.col_clusters
+        m = self.row_n if which == 0 else self.col_n
+        rec = np.zeros((n, 3), dtype=np.uint32)
+        box = np.zeros((n, 6))
+        idx = np.zeros(m, dtype=np.uint32)
+        check(lib.h2b_tree_export_clusters(self.handle, which, _ptr(rec), _ptr(box), _ptr(idx)),
+              "export_clusters")
+        return rec, box, idx
+
+    def block_records(self):
+        rec = np.zeros((self.blocks, 5), dtype=np.uint32)
+        check(lib.h2b_tree_export_blocks(self.handle, rec), "export_blocks")
+        return rec
+
+    def __del__(self):
+        if getattr(self, "handle", None):
+            lib.h2b_tree_del(self.handle)
+            self.handle = None
+
+
+def build_tree(gr, row_basis, col_basis, clf, eta):
+    return Tree(checkp(lib.h2b_tree_new(gr.vertices, gr.x, gr.triangles, gr.t, row_basis,
+                                        col_basis, clf, eta), "h2b_tree_new"))
+
+
+class H2Matrix:
+    """Device H2 matrix with Chebyshev interpolation (setup_h2matrix_aprx_inter_bem3d,
+    Library/bem3d.c:9658)."""
+
+    def __init__(self, bem, tree, m):
+        self.bem, self.tree, self.m = bem, tree, m
+        self.handle = checkp(lib.h2b_h2matrix_new(bem.handle, tree.handle, m), "h2matrix_new")
+        self.rows, self.cols, self.dtype = bem.rows, bem.cols, bem.dtype
+
+    def assemble(self):
+        """assemble_bem3d_h2matrix_row/col_clusterbasis + assemble_bem3d_h2matrix."""
+        check(lib.h2b_h2matrix_assemble_all(self.handle), "h2matrix_assemble_all")
+        return self
+
+    def info(self):
+        info = np.zeros(8, dtype=np.uint64)
+        check(lib.h2b_h2matrix_info(self.handle, info), "h2matrix_info")
+        return dict(near_entries=int(info[0]), coupling_entries=int(info[1]),
+                    leaf_entries=int(info[2]), transfer_entries=int(info[3]),
+                    bytes=int(info[4]), admissible=int(info[5]), near_blocks=int(info[6]),
+                    rank=int(info[7]))
+
+    def export(self, part, count=0xFFFFFFFF):
+        n = C.c_uint64()
+        check(lib.h2b_h2matrix_export(self.handle, part, count, None, C.byref(n)), "export")
+        if self.dtype == np.complex128:
+            out = np.zeros(n.value // 2, dtype=np.complex128)
+        else:
+            out = np.zeros(n.value)
+        check(lib.h2b_h2matrix_export(self.handle, part, count, _ptr(out), C.byref(n)), "export")
+        return out
+
+    def __del__(self):
+        if getattr(self, "handle", None):
+            lib.h2b_h2matrix_del(self.handle)
+            self.handle = None
+
+
+def addeval_h2matrix_avector(alpha, h2, x, y):
+    """y += alpha * A x (Library/h2matrix.c:1269)."""
+    alpha = complex(alpha)
+    check(lib.h2b_h2matrix_addeval(alpha.real, alpha.imag, h2.handle, _ptr(x), _ptr(y)),
+          "addeval_h2matrix_avector")
+    return y
+
+
+def solve_gmres(ops, coefs, b, x, eps, maxiter, kmax):
+    """GMRES on sum_i coefs[i] * ops[i] (solve_gmres_avector, Library/krylovsolvers.c:183)."""
+    arr = (C.c_void_p * len(ops))(*[o.handle for o in ops])
+    cf = np.zeros(2 * len(ops))
+    for i, c in enumerate(coefs):
+        cf[2 * i], cf[2 * i + 1] = complex(c).real, complex(c).imag
+    return check(lib.h2b_solve_gmres(len(ops), C.cast(arr, C.c_void_p), cf, _ptr(b), _ptr(x),
+                                     eps, maxiter, kmax), "solve_gmres")
+
+
+def solve_gmres_h2matrix_avector(A, b, x, eps, maxiter, kmax):
+    """Library/krylovsolvers.c:254"""
+    return solve_gmres([A], [1.0], b, x, eps, maxiter, kmax)
+
+
+def residual_norm(ops, coefs, b, x):
+    arr = (C.c_void_p * len(ops))(*[o.handle for o in ops])
+    cf = np.zeros(2 * len(ops))
+    for i, c in enumerate(coefs):
+        cf[2 * i], cf[2 * i + 1] = complex(c).real, complex(c).imag
+    r = C.c_double()
+    check(lib.h2b_residual_norm(len(ops), C.cast(arr, C.c_void_p), cf, _ptr(b), _ptr(x),
+                                C.byref(r)), "residual_norm")
+    return r.value
+
+
+def project_l2_harmonic(bem, z, w=None):
+    """projectL2_bem3d_l_avector with eval_dirichlet_fundamental_laplacebem3d
+    (Library/bem3d.c:9009, Library/laplacebem3d.c:1391)."""
+    if w is None:
+        w = np.zeros(bem.gr.vertices)
+    check(lib.h2b_project_l2_harmonic(bem.handle, np.asarray(z, dtype=np.float64), _ptr(w)),
+          "project_l2_harmonic")
+    return w
+
+
+def l2_error_harmonic(bem, z, u):
+    """(normL2diff_l_bem3d, normL2_bem3d) against the Neumann trace of 1/|x - z|."""
+    e, n = C.c_double(), C.c_double()
+    check(lib.h2b_l2_error_harmonic(bem.handle, np.asarray(z, dtype=np.float64), _ptr(u),
+                                    C.byref(e), C.byref(n)), "l2_error_harmonic")
+    return e.value, n.value
+
+
+def quad_export(q, q2, row_basis, col_basis, which):
+    """Quadrature rule tables (Library/singquad2d.c:25-320): dict of arrays."""
+    n = C.c_uint32()
+    check(lib.h2b_quad_export(q, q2, row_basis, col_basis, which, C.byref(n), None, None, None,
+                              None, None), "quad_export")
+    n = n.value
+    x0, x1, y0, y1 = (np.zeros(n) for _ in range(4))
+    w = np.zeros((4 if which == 4 else 10) * n)
+    check(lib.h2b_quad_export(q, q2, row_basis, col_basis, which, C.byref(C.c_uint32()),
+                              _ptr(x0), _ptr(x1), _ptr(y0), _ptr(y1), _ptr(w)), "quad_export")
+    return dict(n=n, x0=x0, x1=x1, y0=y0, y1=y1, w=w.reshape(-1, n))

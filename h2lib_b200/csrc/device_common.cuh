@@ -1,0 +1,68 @@
+// Device-side building blocks shared by the h2b200 CUDA sources (sm_100a only).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "h2b200_internal.h"
+
+#define H2B_CUDA_TRY(call)                                                                     \
+  do {                                                                                        \
+    cudaError_t err__ = (call);                                                               \
+    if (err__ != cudaSuccess) {                                                               \
+      h2b_set_error("%s:%d: %s: %s", __FILE__, __LINE__, #call, cudaGetErrorString(err__));  \
+      return H2B_ERR_CUDA;                                                                    \
+    }                                                                                         \
+  } while (0)
+
+// 1/(4 pi): constant of the fundamental solutions of Laplace and Helmholtz
+// (KERNEL_CONST_LAPLACEBEM3D, Library/laplacebem3d.c:33; KERNEL_CONST_HELMHOLTZBEM3D,
+// Library/helmholtzbem3d.c:25).
+#define H2B_KERNEL_CONST 0.0795774715459476679
+
+// One triangle as the quadrature kernels read it: 128 bytes, 16-byte aligned, loaded with eight
+// 16-byte vector loads.  Vertices are in the triangle's own order (H2Lib's gr->t[i]).
+struct __align__(16) TriRec {
+  double a[3], b[3], c[3];  // vertex coordinates
+  double n[3];              // unit normal
+  double g;                 // Gram determinant = 2 * area
+  uint32_t v[3];            // vertex ids
+  uint32_t pad0;
+  double pad1;
+};
+static_assert(sizeof(TriRec) == 128, "TriRec must be 128 bytes");
+
+// A triangle referenced by a nearfield tile: its id and the local output row/column index of each
+// of its three vertices (linear basis) or of the triangle itself in l[0] (constant basis); -1 when
+// the vertex is outside the tile.
+struct TriRef {
+  uint32_t t;
+  int16_t l[3];
+  int16_t pad;
+};
+static_assert(sizeof(TriRef) == 12, "TriRef must be 12 bytes");
+
+// Reciprocal square root in FP64, full precision.
+// Seed: the FP32 hardware approximation (rsqrtf on the value rounded to FP32); two Newton-Raphson
+// steps y <- y + y/2 (1 - x y^2) in FP64 (the classical iteration for x^{-1/2}; each step squares
+// the relative error: 2^-22 -> 2^-44 -> below FP64 rounding).  Inputs are squared distances of
+// quadrature points, positive and well inside the FP32 range.
+__device__ __forceinline__ double rsqrt_nr(double x) {
+  double y = (double) rsqrtf((float) x);
+  double h = x * y;
+  double e = fma(-h, y, 1.0);
+  y = fma(0.5 * y, e, y);
+  h = x * y;
+  e = fma(-h, y, 1.0);
+  return fma(0.5 * y, e, y);
+}
+
+struct dcomplex {
+  double re, im;
+};
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}

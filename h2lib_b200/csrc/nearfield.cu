@@ -1,0 +1,552 @@
+// Nearfield quadrature kernels (sm_100a, FP64).
+//
+// Work is split by Sauter-Schwab case, as the reference's quadrature selection does per pair
+// (select_quadrature_singquad2d, Library/singquad2d.c:549):
+//   * near_dist_kernel — one CTA per output tile (<= 64 x 64 entries); one thread per distant
+//     triangle pair (no shared vertex, q^4 tensor points, fully unrolled with the rule in
+//     constant memory); pair results are accumulated in a shared-memory tile and the tile is
+//     written to HBM once with coalesced column-major stores.  Singular pairs are skipped here.
+//   * near_sing_kernel — one warp per singular pair (vertex: 2 q2^4, edge / identical: 6 q2^4
+//     points), lanes stride over the points, the three Sauter-Schwab rules are staged once per
+//     CTA into shared memory with bulk asynchronous copies (cp.async.bulk, global -> shared,
+//     completion on an mbarrier), partial sums are combined with warp shuffles and the result is
+//     written (constant basis) or added (linear basis) to the entries of its pair.
+// The second kernel runs after the first on the same stream, so its stores/additions land on top
+// of the distant-pair tile values.
+//
+// Per point the kernels evaluate the integrand of assemble_cc_near_bem3d (Library/bem3d.c:1151)
+// and assemble_ll_near_bem3d (:3038) with the kernels of Library/laplacebem3d.c:36/84 and
+// Library/helmholtzbem3d.c:27/140.  The quadrature point difference x - y is formed directly as
+// (A_t - A_s) + t_x (B_t - A_t) + s_x (C_t - B_t) - t_y (B_s - A_s) - s_y (C_s - B_s), which is
+// the reference's A(1-t) + B(t-s) + C s map on both triangles, without forming x and y first.
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "device_common.cuh"
+#include "h2b200_plan.h"
+#include "nearfield.h"
+
+namespace {
+
+constexpr int KK_LSLP = H2B_KK_LSLP;
+constexpr int KK_LDLP = H2B_KK_LDLP;
+constexpr int KK_LBOTH = H2B_KK_LBOTH;
+constexpr int KK_HSLP = H2B_KK_HSLP;
+constexpr int KK_HDLP = H2B_KK_HDLP;
+
+template <int KK> struct KT;
+template <> struct KT<KK_LSLP> { static constexpr int NCH = 1, NOUT = 1; static constexpr bool CPLX = false; };
+template <> struct KT<KK_LDLP> { static constexpr int NCH = 1, NOUT = 1; static constexpr bool CPLX = false; };
+template <> struct KT<KK_LBOTH> { static constexpr int NCH = 2, NOUT = 2; static constexpr bool CPLX = false; };
+template <> struct KT<KK_HSLP> { static constexpr int NCH = 2, NOUT = 1; static constexpr bool CPLX = true; };
+template <> struct KT<KK_HDLP> { static constexpr int NCH = 2, NOUT = 1; static constexpr bool CPLX = true; };
+
+// Distant tensor rules for q = 1..5 (q^4 points each): x0, x1, y0, y1, w.
+constexpr int DIST_TOTAL = 1 + 16 + 81 + 256 + 625;
+__host__ __device__ constexpr int dist_off(int q) {
+  return q == 1 ? 0 : q == 2 ? 1 : q == 3 ? 17 : q == 4 ? 98 : 354;
+}
+__constant__ double c_dist[5][DIST_TOTAL];
+
+// Kernel values at difference d = x - y; ns = unit normal of the column triangle.
+template <int KK>
+__device__ __forceinline__ void eval_kernel(double dx, double dy, double dz, double n0, double n1,
+                                            double n2, double k_re, double k_imn, double kv[2]) {
+  double r2 = fma(dx, dx, fma(dy, dy, dz * dz));
+  double rinv = rsqrt_nr(r2);
+  if constexpr (KK == KK_LSLP) {
+    kv[0] = rinv;
+  } else if constexpr (KK == KK_LDLP) {
+    double dot = fma(dx, n0, fma(dy, n1, dz * n2));
+    kv[0] = dot * (rinv * rinv * rinv);
+  } else if constexpr (KK == KK_LBOTH) {
+    double dot = fma(dx, n0, fma(dy, n1, dz * n2));
+    kv[0] = rinv;
+    kv[1] = dot * (rinv * rinv * rinv);
+  } else if constexpr (KK == KK_HSLP) {
+    double r = r2 * rinv, rn = rinv, s, c;
+    if (k_imn != 0.0) rn *= exp(k_imn * r);
+    sincos(k_re * r, &s, &c);
+    kv[0] = rn * c;
+    kv[1] = rn * s;
+  } else {  // KK_HDLP
+    double dot = fma(dx, n0, fma(dy, n1, dz * n2));
+    double re = (rinv * rinv * rinv) * dot, r = r2 * rinv, s, c;
+    if (k_imn != 0.0) re *= exp(k_imn * r);
+    double kr = k_re * r;
+    sincos(kr, &s, &c);
+    kv[0] = fma(kr, s, c) * re;
+    kv[1] = fma(-c, kr, s) * re;
+  }
+}
+
+__device__ __forceinline__ double vtx(const TriRec &T, int i, int d) {
+  return i == 0 ? T.a[d] : (i == 1 ? T.b[d] : T.c[d]);
+}
+
+// Pair geometry: D0 = A_t - A_s, P1 = B_t - A_t, P2 = C_t - B_t, Q1 = B_s - A_s, Q2 = C_s - B_s.
+struct PairGeo {
+  double d0[3], p1[3], p2[3], q1[3], q2[3];
+};
+
+__device__ __forceinline__ void pair_geo(const TriRec &T, const TriRec &S, const int tp[3],
+                                         const int sp[3], PairGeo &g) {
+#pragma unroll
+  for (int d = 0; d < 3; d++) {
+    double ta = vtx(T, tp[0], d), tb = vtx(T, tp[1], d), tc = vtx(T, tp[2], d);
+    double sa = vtx(S, sp[0], d), sb = vtx(S, sp[1], d), sc = vtx(S, sp[2], d);
+    g.d0[d] = ta - sa;
+    g.p1[d] = tb - ta;
+    g.p2[d] = tc - tb;
+    g.q1[d] = sb - sa;
+    g.q2[d] = sc - sb;
+  }
+}
+
+__device__ __forceinline__ void pair_geo_id(const TriRec &T, const TriRec &S, PairGeo &g) {
+#pragma unroll
+  for (int d = 0; d < 3; d++) {
+    g.d0[d] = T.a[d] - S.a[d];
+    g.p1[d] = T.b[d] - T.a[d];
+    g.p2[d] = T.c[d] - T.b[d];
+    g.q1[d] = S.b[d] - S.a[d];
+    g.q2[d] = S.c[d] - S.b[d];
+  }
+}
+
+// Accumulate one quadrature point into acc[ch][i][j] (i row basis, j column basis).
+template <int KK, bool RL, bool CL>
+__device__ __forceinline__ void quad_point(const PairGeo &g, double tx, double sx, double ty,
+                                           double sy, double w, double n0, double n1, double n2,
+                                           double k_re, double k_imn,
+                                           double (&acc)[KT<KK>::NCH][RL ? 3 : 1][CL ? 3 : 1]) {
+  constexpr int NCH = KT<KK>::NCH;
+  double dx = fma(-sy, g.q2[0], fma(-ty, g.q1[0], fma(sx, g.p2[0], fma(tx, g.p1[0], g.d0[0]))));
+  double dy = fma(-sy, g.q2[1], fma(-ty, g.q1[1], fma(sx, g.p2[1], fma(tx, g.p1[1], g.d0[1]))));
+  double dz = fma(-sy, g.q2[2], fma(-ty, g.q1[2], fma(sx, g.p2[2], fma(tx, g.p1[2], g.d0[2]))));
+  double kv[2];
+  eval_kernel<KK>(dx, dy, dz, n0, n1, n2, k_re, k_imn, kv);
+  if constexpr (!RL && !CL) {
+#pragma unroll
+    for (int c = 0; c < NCH; c++) acc[c][0][0] = fma(w, kv[c], acc[c][0][0]);
+  } else {
+    double pr[3] = {1.0 - tx, tx - sx, sx};
+    double pc[3] = {1.0 - ty, ty - sy, sy};
+#pragma unroll
+    for (int c = 0; c < NCH; c++) {
+      double u[CL ? 3 : 1];
+#pragma unroll
+      for (int j = 0; j < (CL ? 3 : 1); j++) u[j] = (CL ? pc[j] * w : w) * kv[c];
+#pragma unroll
+      for (int i = 0; i < (RL ? 3 : 1); i++)
+#pragma unroll
+        for (int j = 0; j < (CL ? 3 : 1); j++)
+          acc[c][i][j] = RL ? fma(pr[i], u[j], acc[c][i][j]) : acc[c][i][j] + u[j];
+    }
+  }
+}
+
+struct DistArgs {
+  const TriRec *tri;
+  const TriRef *refs;
+  const h2b_tile *tiles;
+  double *out0, *out1;
+  double kconst, k_re, k_imn;
+  int q;  // runtime q for the generic variant
+};
+
+// Shared-memory accumulator tile: [NOUT*(CPLX?2:1)][64*64] doubles.
+template <int Q, int KK, bool RL, bool CL>
+__global__ void __launch_bounds__(256, 2) near_dist_kernel(DistArgs a) {
+  constexpr int NCH = KT<KK>::NCH;
+  constexpr int NR = RL ? 3 : 1, NC = CL ? 3 : 1;
+  constexpr int PLANES = KT<KK>::CPLX ? 2 : KT<KK>::NOUT;
+  constexpr int TS = H2B_TILE_MAX * H2B_TILE_MAX;
+  extern __shared__ double sacc[];
+
+  const h2b_tile tl = a.tiles[blockIdx.x];
+  const int rows = tl.rows, cols = tl.cols;
+  for (int e = threadIdx.x; e < PLANES * TS; e += blockDim.x) sacc[e] = 0.0;
+  __syncthreads();
+
+  const uint32_t ntr = tl.tr_len, nsc = tl.sc_len;
+  const uint32_t npairs = ntr * nsc;
+  const int q = Q > 0 ? Q : a.q;
+  const int nq = q * q * q * q;
+  const double *cx0 = &c_dist[0][dist_off(Q > 0 ? Q : 1)];
+  const double *cx1 = &c_dist[1][dist_off(Q > 0 ? Q : 1)];
+  const double *cy0 = &c_dist[2][dist_off(Q > 0 ? Q : 1)];
+  const double *cy1 = &c_dist[3][dist_off(Q > 0 ? Q : 1)];
+  const double *cw = &c_dist[4][dist_off(Q > 0 ? Q : 1)];
+  if (Q == 0) {
+    cx0 = &c_dist[0][dist_off(q)];
+    cx1 = &c_dist[1][dist_off(q)];
+    cy0 = &c_dist[2][dist_off(q)];
+    cy1 = &c_dist[3][dist_off(q)];
+    cw = &c_dist[4][dist_off(q)];
+  }
+
+  for (uint32_t p = threadIdx.x; p < npairs; p += blockDim.x) {
+    const uint32_t is = p / ntr, it = p - is * ntr;
+    const TriRef rt = a.refs[tl.tr_off + it];
+    const TriRef st = a.refs[tl.sc_off + is];
+    const TriRec &T = a.tri[rt.t];
+    const TriRec &S = a.tri[st.t];
+    const uint32_t tv0 = T.v[0], tv1 = T.v[1], tv2 = T.v[2];
+    const uint32_t sv0 = S.v[0], sv1 = S.v[1], sv2 = S.v[2];
+    const bool singular = tv0 == sv0 || tv0 == sv1 || tv0 == sv2 || tv1 == sv0 || tv1 == sv1 ||
+                          tv1 == sv2 || tv2 == sv0 || tv2 == sv1 || tv2 == sv2;
+    if (singular) continue;
+
+    PairGeo g;
+    pair_geo_id(T, S, g);
+    const double n0 = S.n[0], n1 = S.n[1], n2 = S.n[2];
+    double acc[NCH][NR][NC];
+#pragma unroll
+    for (int c = 0; c < NCH; c++)
+#pragma unroll
+      for (int i = 0; i < NR; i++)
+#pragma unroll
+        for (int j = 0; j < NC; j++) acc[c][i][j] = 0.0;
+
+    if constexpr (Q > 0) {
+#pragma unroll
+      for (int k = 0; k < Q * Q * Q * Q; k++)
+        quad_point<KK, RL, CL>(g, cx0[k], cx1[k], cy0[k], cy1[k], cw[k], n0, n1, n2, a.k_re,
+                               a.k_imn, acc);
+    } else {
+      for (int k = 0; k < nq; k++)
+        quad_point<KK, RL, CL>(g, cx0[k], cx1[k], cy0[k], cy1[k], cw[k], n0, n1, n2, a.k_re,
+                               a.k_imn, acc);
+    }
+
+    const double f2 = (S.g * a.kconst) * T.g;
+#pragma unroll
+    for (int i = 0; i < NR; i++) {
+      const int lr = rt.l[i];
+#pragma unroll
+      for (int j = 0; j < NC; j++) {
+        const int lc = st.l[j];
+        if (lr < 0 || lc < 0) continue;
+        const int e = lr + H2B_TILE_MAX * lc;
+#pragma unroll
+        for (int c = 0; c < NCH; c++) {
+          const double v = acc[c][i][j] * f2;
+          if constexpr (RL || CL)
+            atomicAdd(&sacc[c * TS + e], v);
+          else
+            sacc[c * TS + e] = v;
+        }
+      }
+    }
+  }
+  __syncthreads();
+
+  const bool ntrans = tl.flags & 1u;
+  for (int e = threadIdx.x; e < rows * cols; e += blockDim.x) {
+    const int r = e % rows, c = e / rows;
+    const uint64_t o = ntrans ? tl.out_off + c + (uint64_t) r * tl.ld
+                              : tl.out_off + r + (uint64_t) c * tl.ld;
+    const int se = r + H2B_TILE_MAX * c;
+    if constexpr (KT<KK>::CPLX) {
+      a.out0[2 * o] = sacc[se];
+      a.out0[2 * o + 1] = ntrans ? -sacc[TS + se] : sacc[TS + se];
+    } else {
+      a.out0[o] = sacc[se];
+      if constexpr (KT<KK>::NOUT == 2) a.out1[o] = sacc[TS + se];
+    }
+  }
+}
+
+struct SingArgs {
+  const TriRec *tri;
+  const TriRef *refs;
+  const h2b_tile *tiles;
+  const h2b_sing *sing;
+  uint32_t nsing;
+  double *out0, *out1;
+  double kconst, k_re, k_imn;
+  double alpha_re, alpha_im;  // identity coefficient of the double layer output
+  double mass[9];
+  const double *rule;         // packed singular rules: [case 1..3] x {x0,x1,y0,y1,w} x n_case
+  uint32_t rule_n[4];         // points per case (index 1..3)
+  uint32_t rule_off[4];       // offset (in doubles) of each case's block in `rule`
+  uint32_t rule_total;        // doubles in `rule` (multiple of 2, 16-byte aligned)
+  int staged;                 // 1: copy `rule` into shared memory first
+  int *err;                   // set to 1 if the staging copy did not complete
+};
+
+// One warp per singular pair.  The three rules are copied into shared memory once per CTA.
+template <int KK, bool RL, bool CL>
+__global__ void __launch_bounds__(256) near_sing_kernel(SingArgs a) {
+  constexpr int NCH = KT<KK>::NCH;
+  constexpr int NR = RL ? 3 : 1, NC = CL ? 3 : 1;
+  extern __shared__ __align__(16) double srule[];
+  __shared__ __align__(8) uint64_t bar;
+
+  // Stage the packed rule table: one bulk copy global -> shared, completion on an mbarrier.
+  // Tables too large for shared memory are read from global memory (L2-resident) instead.
+  const double *rules = a.rule;
+  if (a.staged) {
+    const uint32_t bytes = a.rule_total * 8u;
+    const uint32_t sbar = (uint32_t) __cvta_generic_to_shared(&bar);
+    if (threadIdx.x == 0) {
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(sbar));
+      asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      const uint32_t sdst = (uint32_t) __cvta_generic_to_shared(srule);
+      asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(sbar), "r"(bytes)
+                   : "memory");
+      // chunks of at most 64 KiB; every chunk starts and ends on a 16-byte boundary
+      for (uint32_t off = 0; off < bytes; off += 65536u) {
+        const uint32_t n = bytes - off < 65536u ? bytes - off : 65536u;
+        asm volatile(
+            "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                sdst + off),
+            "l"(reinterpret_cast<const char *>(a.rule) + off), "r"(n), "r"(sbar)
+            : "memory");
+      }
+    }
+    // bounded wait on phase 0 of the barrier
+    uint32_t done = 0;
+    for (uint32_t spin = 0; spin < (1u << 24) && !done; spin++) {
+      asm volatile(
+          "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0;\n selp.u32 %0, 1, 0, p;\n}"
+          : "=r"(done)
+          : "r"(sbar)
+          : "memory");
+    }
+    if (!done) {
+      if (threadIdx.x == 0) atomicExch(a.err, 1);
+      return;
+    }
+    rules = srule;
+  }
+
+  const int lane = threadIdx.x & 31;
+  const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+
+  for (uint32_t pi = warp; pi < a.nsing; pi += nwarps) {
+    const h2b_sing sp = a.sing[pi];
+    const uint32_t cs = sp.code & 3u;
+    const int tp[3] = {(int) ((sp.code >> 2) & 3u), (int) ((sp.code >> 4) & 3u),
+                       (int) ((sp.code >> 6) & 3u)};
+    const int sq[3] = {(int) ((sp.code >> 8) & 3u), (int) ((sp.code >> 10) & 3u),
+                       (int) ((sp.code >> 12) & 3u)};
+    const TriRef rt = a.refs[sp.tr];
+    const TriRef st = a.refs[sp.sc];
+    const TriRec &T = a.tri[rt.t];
+    const TriRec &S = a.tri[st.t];
+    PairGeo g;
+    pair_geo(T, S, tp, sq, g);
+    const double n0 = S.n[0], n1 = S.n[1], n2 = S.n[2];
+    const uint32_t n = a.rule_n[cs];
+    const double *rx0 = rules + a.rule_off[cs];
+    const double *rx1 = rx0 + n, *ry0 = rx0 + 2 * n, *ry1 = rx0 + 3 * n, *rw = rx0 + 4 * n;
+
+    double acc[NCH][NR][NC];
+#pragma unroll
+    for (int c = 0; c < NCH; c++)
+#pragma unroll
+      for (int i = 0; i < NR; i++)
+#pragma unroll
+        for (int j = 0; j < NC; j++) acc[c][i][j] = 0.0;
+    for (uint32_t k = lane; k < n; k += 32)
+      quad_point<KK, RL, CL>(g, rx0[k], rx1[k], ry0[k], ry1[k], rw[k], n0, n1, n2, a.k_re, a.k_imn,
+                             acc);
+#pragma unroll
+    for (int c = 0; c < NCH; c++)
+#pragma unroll
+      for (int i = 0; i < NR; i++)
+#pragma unroll
+        for (int j = 0; j < NC; j++) acc[c][i][j] = warp_sum(acc[c][i][j]);
+
+    if (lane == 0) {
+      const h2b_tile tl = a.tiles[sp.tile];
+      const bool ntrans = tl.flags & 1u;
+      const double f2 = (S.g * a.kconst) * T.g;
+      const bool ident = (cs == 3u) && (rt.t == st.t);
+#pragma unroll
+      for (int i = 0; i < NR; i++) {
+        const int lr = RL ? rt.l[tp[i]] : rt.l[0];
+#pragma unroll
+        for (int j = 0; j < NC; j++) {
+          const int lc = CL ? st.l[sq[j]] : st.l[0];
+          if (lr < 0 || lc < 0) continue;
+          const uint64_t o = ntrans ? tl.out_off + lc + (uint64_t) lr * tl.ld
+                                    : tl.out_off + lr + (uint64_t) lc * tl.ld;
+          if constexpr (!RL && !CL) {
+            // constant basis: this pair is the whole entry
+            if constexpr (KT<KK>::CPLX) {
+              double re = acc[0][0][0] * f2, im = acc[1][0][0] * f2;
+              if (ident) {
+                re += 0.5 * a.alpha_re * T.g;
+                im += 0.5 * a.alpha_im * T.g;
+              }
+              a.out0[2 * o] = re;
+              a.out0[2 * o + 1] = ntrans ? -im : im;
+            } else if constexpr (KT<KK>::NOUT == 2) {
+              a.out0[o] = acc[0][0][0] * f2;
+              a.out1[o] = acc[1][0][0] * f2 + (ident ? 0.5 * a.alpha_re * T.g : 0.0);
+            } else {
+              a.out0[o] = acc[0][0][0] * f2 + (ident ? 0.5 * a.alpha_re * T.g : 0.0);
+            }
+          } else {
+            if constexpr (KT<KK>::CPLX) {
+              atomicAdd(&a.out0[2 * o], acc[0][i][j] * f2);
+              atomicAdd(&a.out0[2 * o + 1], (ntrans ? -1.0 : 1.0) * acc[1][i][j] * f2);
+            } else {
+              atomicAdd(&a.out0[o], acc[0][i][j] * f2);
+              if constexpr (KT<KK>::NOUT == 2) atomicAdd(&a.out1[o], acc[1][i][j] * f2);
+            }
+          }
+        }
+      }
+      // identity term of linear bases: alpha * mass_{lk} * g on the vertex pairs of the triangle
+      if constexpr (RL && CL) {
+        if (ident && (a.alpha_re != 0.0 || a.alpha_im != 0.0)) {
+          double *dst = KT<KK>::NOUT == 2 ? a.out1 : a.out0;
+          for (int l = 0; l < 3; l++)
+            for (int k = 0; k < 3; k++) {
+              const int lr = rt.l[l], lc = st.l[k];
+              if (lr < 0 || lc < 0) continue;
+              const uint64_t o = ntrans ? tl.out_off + lc + (uint64_t) lr * tl.ld
+                                        : tl.out_off + lr + (uint64_t) lc * tl.ld;
+              const double m = a.mass[l + 3 * k] * T.g;
+              if constexpr (KT<KK>::CPLX) {
+                atomicAdd(&dst[2 * o], m * a.alpha_re);
+                atomicAdd(&dst[2 * o + 1], (ntrans ? -1.0 : 1.0) * m * a.alpha_im);
+              } else {
+                atomicAdd(&dst[o], m * a.alpha_re);
+              }
+            }
+        }
+      }
+    }
+  }
+}
+
+template <int Q, int KK, bool RL, bool CL>
+int launch_dist(const h2b_near_launch *L, cudaStream_t st) {
+  constexpr int PLANES = KT<KK>::CPLX ? 2 : KT<KK>::NOUT;
+  const size_t smem = sizeof(double) * PLANES * H2B_TILE_MAX * H2B_TILE_MAX;
+  static bool attr_set = false;
+  if (!attr_set) {
+    H2B_CUDA_TRY(cudaFuncSetAttribute(near_dist_kernel<Q, KK, RL, CL>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem));
+    attr_set = true;
+  }
+  DistArgs a;
+  a.tri = (const TriRec *) L->tri;
+  a.refs = (const TriRef *) L->refs;
+  a.tiles = L->tiles;
+  a.out0 = L->out0;
+  a.out1 = L->out1;
+  a.kconst = L->kconst;
+  a.k_re = L->k_re;
+  a.k_imn = L->k_imn;
+  a.q = (int) L->q;
+  if (L->ntiles > 0) near_dist_kernel<Q, KK, RL, CL><<<L->ntiles, 256, smem, st>>>(a);
+  H2B_CUDA_TRY(cudaGetLastError());
+  return H2B_OK;
+}
+
+template <int KK, bool RL, bool CL>
+int launch_sing(const h2b_near_launch *L, cudaStream_t st) {
+  if (L->nsing == 0) return H2B_OK;
+  const int staged = sizeof(double) * L->rule_total <= 200u * 1024u;
+  const size_t smem = staged ? sizeof(double) * L->rule_total : 0;
+  static size_t attr_set = 0;
+  if (smem > attr_set) {
+    H2B_CUDA_TRY(cudaFuncSetAttribute(near_sing_kernel<KK, RL, CL>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem));
+    attr_set = smem;
+  }
+  SingArgs a;
+  a.tri = (const TriRec *) L->tri;
+  a.refs = (const TriRef *) L->refs;
+  a.tiles = L->tiles;
+  a.sing = L->sing;
+  a.nsing = L->nsing;
+  a.out0 = L->out0;
+  a.out1 = L->out1;
+  a.kconst = L->kconst;
+  a.k_re = L->k_re;
+  a.k_imn = L->k_imn;
+  a.alpha_re = L->alpha_re;
+  a.alpha_im = L->alpha_im;
+  for (int i = 0; i < 9; i++) a.mass[i] = L->mass[i];
+  a.rule = L->rule;
+  for (int i = 0; i < 4; i++) {
+    a.rule_n[i] = L->rule_n[i];
+    a.rule_off[i] = L->rule_off[i];
+  }
+  a.rule_total = L->rule_total;
+  a.staged = staged;
+  a.err = L->err;
+  int sms = L->num_sms > 0 ? L->num_sms : 148;
+  uint32_t want = (L->nsing + 7) / 8;  // 8 warps per CTA
+  uint32_t grid = want < (uint32_t) sms ? want : (uint32_t) sms;
+  near_sing_kernel<KK, RL, CL><<<grid, 256, smem, st>>>(a);
+  H2B_CUDA_TRY(cudaGetLastError());
+  return H2B_OK;
+}
+
+template <int KK, bool RL, bool CL>
+int launch_kk_basis(const h2b_near_launch *L, cudaStream_t st) {
+  int rc;
+  if (L->q == 2)
+    rc = launch_dist<2, KK, RL, CL>(L, st);
+  else
+    rc = launch_dist<0, KK, RL, CL>(L, st);
+  if (rc != H2B_OK) return rc;
+  return launch_sing<KK, RL, CL>(L, st);
+}
+
+template <int KK>
+int launch_kk(const h2b_near_launch *L, cudaStream_t st) {
+  if (L->row_linear && L->col_linear) return launch_kk_basis<KK, true, true>(L, st);
+  if (L->row_linear) return launch_kk_basis<KK, true, false>(L, st);
+  if (L->col_linear) return launch_kk_basis<KK, false, true>(L, st);
+  return launch_kk_basis<KK, false, false>(L, st);
+}
+
+}  // namespace
+
+extern "C" int h2b_near_upload_dist_rules(void) {
+  static double host[5][DIST_TOTAL];
+  for (int q = 1; q <= 5; q++) {
+    h2b_quad qd;
+    int rc = h2b_quad_build((uint32_t) q, 1, H2B_BASIS_CONSTANT, H2B_BASIS_CONSTANT, &qd);
+    if (rc != H2B_OK) return rc;
+    const h2b_rule *r = &qd.rule[H2B_RULE_DIST];
+    for (uint32_t k = 0; k < r->n; k++) {
+      host[0][dist_off(q) + k] = r->x0[k];
+      host[1][dist_off(q) + k] = r->x1[k];
+      host[2][dist_off(q) + k] = r->y0[k];
+      host[3][dist_off(q) + k] = r->y1[k];
+      host[4][dist_off(q) + k] = r->w[9 * (size_t) r->n + k];
+    }
+    h2b_quad_free(&qd);
+  }
+  H2B_CUDA_TRY(cudaMemcpyToSymbol(c_dist, host, sizeof(host)));
+  return H2B_OK;
+}
+
+extern "C" int h2b_near_launch_kernels(const h2b_near_launch *L, cudaStream_t st) {
+  if (L->q < 1 || L->q > 5) {
+    h2b_set_error("regular quadrature order %u not supported (1..5)", L->q);
+    return H2B_ERR_ARG;
+  }
+  switch (L->kk) {
+    case KK_LSLP: return launch_kk<KK_LSLP>(L, st);
+    case KK_LDLP: return launch_kk<KK_LDLP>(L, st);
+    case KK_LBOTH: return launch_kk<KK_LBOTH>(L, st);
+    case KK_HSLP: return launch_kk<KK_HSLP>(L, st);
+    case KK_HDLP: return launch_kk<KK_HDLP>(L, st);
+    default: h2b_set_error("unknown kernel kind %d", L->kk); return H2B_ERR_ARG;
+  }
+}

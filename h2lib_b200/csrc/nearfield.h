@@ -1,0 +1,48 @@
+/* Launch description of the nearfield quadrature kernels (nearfield.cu). */
+#ifndef H2B200_NEARFIELD_H
+#define H2B200_NEARFIELD_H
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "h2b200_plan.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* kernel kinds */
+#define H2B_KK_LSLP 0   /* Laplace single layer, real */
+#define H2B_KK_LDLP 1   /* Laplace double layer, real */
+#define H2B_KK_LBOTH 2  /* Laplace single and double layer together (two real outputs) */
+#define H2B_KK_HSLP 3   /* Helmholtz single layer, complex */
+#define H2B_KK_HDLP 4   /* Helmholtz double layer, complex */
+
+typedef struct {
+  int kk;
+  int row_linear, col_linear;
+  uint32_t q;                    /* regular order: distant pairs use q^4 points */
+  const void *tri;               /* TriRec[triangles] */
+  const void *refs;              /* TriRef pool */
+  const h2b_tile *tiles;
+  uint32_t ntiles;
+  const h2b_sing *sing;          /* sorted by case */
+  uint32_t nsing;
+  double *out0, *out1;           /* out1: double-layer output of H2B_KK_LBOTH */
+  double kconst, k_re, k_imn;    /* 1/(4 pi); Re k; -Im k */
+  double alpha_re, alpha_im;     /* identity coefficient of the double layer output */
+  double mass[9];                /* linear-basis mass matrix on the reference triangle */
+  const double *rule;            /* packed singular rules (device) */
+  uint32_t rule_n[4], rule_off[4], rule_total;
+  int num_sms;
+  int *err;                      /* device flag */
+} h2b_near_launch;
+
+int h2b_near_upload_dist_rules(void);
+int h2b_near_launch_kernels(const h2b_near_launch *L, cudaStream_t st);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

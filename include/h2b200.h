@@ -1,0 +1,273 @@
+/* h2b200 — B200-native boundary-element quadrature, H2 matrix-vector product and GMRES.
+ *
+ * The C ABI below is the drop-in boundary for H2Lib's 3D BEM hot path.  Every entry point takes
+ * plain pointers and sizes; no CUDA, torch or H2Lib types appear in a signature, so H2Lib (C), a
+ * ctypes binding or any FFI can call it.  Each function names the H2Lib interface it replaces
+ * (file:line in the H2Lib source tree).
+ *
+ * Conventions shared with H2Lib:
+ *   - matrices are column-major, entry (i,j) at a[i + j*ld], ld >= rows  (Library/amatrix.h:43);
+ *   - "field" arrays of complex operators (Helmholtz) are interleaved (re, im) doubles, i.e. the
+ *     memory layout of C99 `double _Complex` used by H2Lib's USE_COMPLEX build;
+ *   - index lists (ridx/cidx) may be NULL meaning the identity 0..n-1  (Library/bem3d.h:380);
+ *   - basis identifiers equal H2Lib's basisfunctionbem3d values: 'c' constant, 'l' linear
+ *     (Library/bem3d.h:167-175).
+ * Pointers to matrix/vector data may be host or device pointers; the library detects which and
+ * copies as needed (host buffers are staged through pinned memory).
+ *
+ * Errors: every function returning int returns H2B_OK (0) or a negative H2B_ERR_* code and leaves
+ * a message for h2b_last_error().  H2Lib itself aborts on errors (Library/basic.c:106-117); the
+ * replacement reports them instead, and never falls back to a CPU computation: without a usable
+ * CUDA device every compute entry point fails with H2B_ERR_CUDA.
+ *
+ * Threading: handles may be used from several host threads if each thread uses its own handle; a
+ * single handle serialises its work on its own CUDA stream.
+ */
+#ifndef H2B200_H
+#define H2B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define H2B_OK 0
+#define H2B_ERR_ARG (-1)
+#define H2B_ERR_NOMEM (-2)
+#define H2B_ERR_CUDA (-3)
+#define H2B_ERR_INTERNAL (-4)
+#define H2B_ERR_STATE (-5)
+#define H2B_ERR_TIMEOUT (-6)
+
+#define H2B_BASIS_CONSTANT 'c'
+#define H2B_BASIS_LINEAR 'l'
+
+#define H2B_LAPLACE 0
+#define H2B_HELMHOLTZ 1
+
+#define H2B_SLP 0
+#define H2B_DLP 1
+
+#define H2B_MESH_SPHERE 0
+#define H2B_MESH_CUBE 1
+
+/* Precision of an assembled operator / matvec. */
+#define H2B_FP64 0
+#define H2B_FP32 1
+
+typedef struct h2b_surface h2b_surface;
+typedef struct h2b_bem h2b_bem;
+typedef struct h2b_tree h2b_tree;
+typedef struct h2b_h2matrix h2b_h2matrix;
+
+/* ------------------------------------------------------------------------------------------
+ * Status
+ * ------------------------------------------------------------------------------------------ */
+
+/* Message of the last failed call on this host thread ("" if none). */
+const char *h2b_last_error(void);
+
+/* Library version string. */
+const char *h2b_version(void);
+
+/* Select and initialise the CUDA device used by handles created afterwards on this thread.
+ * Returns H2B_ERR_CUDA if no sm_100 device is usable. */
+int h2b_device_init(int device);
+
+/* ------------------------------------------------------------------------------------------
+ * Host-side geometry (no GPU needed)
+ * ------------------------------------------------------------------------------------------ */
+
+/* Sizes of a refined macro surface.  Replaces new_sphere_macrosurface3d (Library/
+ * macrosurface3d.c:81) / new_cube_macrosurface3d (:390) + build_from_macrosurface3d_surface3d
+ * (:707): kind H2B_MESH_SPHERE or H2B_MESH_CUBE, split >= 1. */
+int h2b_macro_mesh_size(int kind, uint32_t split, uint32_t *vertices, uint32_t *triangles);
+
+/* Vertex coordinates x[3*vertices] and triangles t[3*triangles] of the refined macro surface, with
+ * H2Lib's vertex and triangle numbering. */
+int h2b_macro_mesh_build(int kind, uint32_t split, double *x, uint32_t *t);
+
+/* Unit normals n[3*triangles], Gram determinants g[triangles] (= 2*area) and (hmin, hmax).
+ * Replaces prepare_surface3d (Library/surface3d.c:51). hminmax may be NULL. */
+int h2b_prepare_surface(uint32_t vertices, const double *x, uint32_t triangles,
+                        const uint32_t *t, double *n, double *g, double *hminmax);
+
+/* Scale vertex coordinates per axis (used to make ellipsoids from the sphere). */
+int h2b_scale_vertices(uint32_t vertices, double *x, const double scale[3]);
+
+/* Quadrature tables, for inspection and tests.  which: 0 distant, 1 vertex, 2 edge, 3 identical
+ * Sauter-Schwab rule (Library/singquad2d.c:50/80/129/206), 4 single-triangle rule (:25).  Any
+ * output pointer may be NULL; w10 receives 10*n weights (rows 0..8 basis-weighted, row 9 raw;
+ * 4*n for the single-triangle rule).  Call once with all NULL to get n. */
+int h2b_quad_export(uint32_t q, uint32_t q2, int row_basis, int col_basis, int which,
+                    uint32_t *n, double *x0, double *x1, double *y0, double *y1, double *w10);
+
+/* ------------------------------------------------------------------------------------------
+ * Cluster tree and block tree (host)
+ * ------------------------------------------------------------------------------------------ */
+
+/* Build the row and column cluster trees (build_bem3d_cluster, Library/bem3d.c:932 ->
+ * build_adaptive_cluster, Library/cluster.c:80) and the strict block tree with the max-norm
+ * admissibility (build_strict_block, Library/block.c:258 + admissible_max_cluster, :52).
+ * row_basis/col_basis choose triangles ('c') or vertices ('l') as indices. */
+h2b_tree *h2b_tree_new(uint32_t vertices, const double *x, uint32_t triangles,
+                       const uint32_t *t, int row_basis, int col_basis, uint32_t clf,
+                       double eta);
+
+/* Build from explicit flattened trees (what an H2Lib integration passes after walking its own
+ * pcluster / pblock): per cluster in pre-order off, size, sons (0 or 2) and the bounding box
+ * (bmin[3], bmax[3]); idx the root index array; per leaf block (block-tree pre-order, sons
+ * column-major) the pre-order ids of its row and column clusters and its admissibility flag. */
+h2b_tree *h2b_tree_new_flat(uint32_t row_clusters, const uint32_t *row_off,
+                            const uint32_t *row_size, const uint32_t *row_sons,
+                            const double *row_box, uint32_t row_n, const uint32_t *row_idx,
+                            uint32_t col_clusters, const uint32_t *col_off,
+                            const uint32_t *col_size, const uint32_t *col_sons,
+                            const double *col_box, uint32_t col_n, const uint32_t *col_idx,
+                            uint32_t blocks, const uint32_t *block_rc,
+                            const uint32_t *block_cc, const uint8_t *block_adm);
+
+void h2b_tree_del(h2b_tree *tree);
+
+/* Counts: clusters of the row/column tree, index-set sizes, leaf blocks, admissible blocks,
+ * nearfield entries (sum over inadmissible blocks of rows*cols), depth of the row/column tree. */
+int h2b_tree_info(const h2b_tree *tree, uint64_t info[8]);
+
+/* Export one tree (which = 0 row, 1 column): rec[3*clusters] = (off, size, sons), box[6*clusters]
+ * = (bmin, bmax), idx[n].  Any pointer may be NULL. */
+int h2b_tree_export_clusters(const h2b_tree *tree, int which, uint32_t *rec, double *box,
+                             uint32_t *idx);
+
+/* Export the leaf blocks: rec[5*blocks] = (row off, row size, col off, col size, admissible). */
+int h2b_tree_export_blocks(const h2b_tree *tree, uint32_t *rec);
+
+/* ------------------------------------------------------------------------------------------
+ * Device-resident surface and operators
+ * ------------------------------------------------------------------------------------------ */
+
+/* Upload a surface mesh (vertices x[3*nv], triangles t[3*nt], normals n[3*nt], Gram determinants
+ * g[nt] — the fields of H2Lib's struct _surface3d, Library/surface3d.h:45). */
+h2b_surface *h2b_surface_new(uint32_t vertices, const double *x, uint32_t triangles,
+                             const uint32_t *t, const double *n, const double *g);
+void h2b_surface_del(h2b_surface *s);
+
+/* Boundary integral operator.  Replaces
+ *   new_slp_laplace_bem3d(gr, q_regular, q_singular, row, col)        Library/laplacebem3d.c:844
+ *   new_dlp_laplace_bem3d(gr, q_regular, q_singular, row, col, alpha) Library/laplacebem3d.c:1012
+ *   new_slp_helmholtz_bem3d(k, gr, q_regular, q_singular, row, col)   Library/helmholtzbem3d.c:1008
+ *   new_dlp_helmholtz_bem3d(k, gr, ..., alpha)                        Library/helmholtzbem3d.c:1177
+ * pde H2B_LAPLACE / H2B_HELMHOLTZ, layer H2B_SLP / H2B_DLP; (k_re, k_im) the wave number
+ * (Helmholtz only; H2Lib's convention e^{i k r} with damping for Im k > 0); (alpha_re, alpha_im)
+ * the coefficient of the identity added to the DLP (H2Lib's bem->alpha: 0.5*alpha*g on the cc
+ * diagonal, alpha*mass*g for linear bases). */
+h2b_bem *h2b_bem_new(const h2b_surface *s, int pde, int layer, int row_basis, int col_basis,
+                     uint32_t q_regular, uint32_t q_singular, double k_re, double k_im,
+                     double alpha_re, double alpha_im);
+void h2b_bem_del(h2b_bem *bem);
+
+/* Nearfield block fill — the bem->nearfield callback (Library/bem3d.h:380; implementations
+ * assemble_cc_near_bem3d, Library/bem3d.c:1151, and assemble_ll_near_bem3d, :3038):
+ * N[i + j*ld] = entry (ridx[i], cidx[j]) for i < rows, j < cols; with ntrans the conjugate
+ * transpose is written, N[j + i*ld].  ridx/cidx: triangle (c) or vertex (l) indices; NULL =
+ * identity.  N may be a host or device pointer; complex operators write interleaved pairs. */
+int h2b_bem_nearfield(const h2b_bem *bem, const uint32_t *ridx, uint32_t rows,
+                      const uint32_t *cidx, uint32_t cols, int ntrans, double *N, uint64_t ld);
+
+/* Dense matrix of the whole operator.  Replaces assemble_bem3d_amatrix (Library/bem3d.c:9988).
+ * G has n rows and n columns (n = triangles or vertices by basis), column-major with ld. */
+int h2b_bem_assemble_amatrix(const h2b_bem *bem, double *G, uint64_t ld);
+
+/* ------------------------------------------------------------------------------------------
+ * H2 matrices
+ * ------------------------------------------------------------------------------------------ */
+
+/* Device H2 matrix with Chebyshev interpolation of order m in each direction (rank m^3) on the
+ * given trees.  Replaces build_from_cluster_clusterbasis (Library/clusterbasis.c:251) +
+ * build_from_block_h2matrix (Library/h2matrix.c:438) + setup_h2matrix_aprx_inter_bem3d
+ * (Library/bem3d.c:9658).  All storage is FP64. */
+h2b_h2matrix *h2b_h2matrix_new(const h2b_bem *bem, const h2b_tree *tree, uint32_t m);
+void h2b_h2matrix_del(h2b_h2matrix *h2);
+
+/* Assembly.  Replace assemble_bem3d_h2matrix_row_clusterbasis (Library/bem3d.c:10407),
+ * _col_clusterbasis (:10436), assemble_bem3d_nearfield_h2matrix (:10325),
+ * assemble_bem3d_farfield_h2matrix (:10337) and assemble_bem3d_h2matrix (:10313; nearfield +
+ * farfield).  h2b_h2matrix_assemble_all does all five in one pass. */
+int h2b_h2matrix_assemble_row_clusterbasis(h2b_h2matrix *h2);
+int h2b_h2matrix_assemble_col_clusterbasis(h2b_h2matrix *h2);
+int h2b_h2matrix_assemble_nearfield(h2b_h2matrix *h2);
+int h2b_h2matrix_assemble_farfield(h2b_h2matrix *h2);
+int h2b_h2matrix_assemble(h2b_h2matrix *h2);
+int h2b_h2matrix_assemble_all(h2b_h2matrix *h2);
+
+/* Assemble the nearfield blocks of two operators on the same tree in one pass (e.g. V and K
+ * of a Laplace Dirichlet problem share every triangle pair and quadrature point). */
+int h2b_h2matrix_assemble_nearfield_pair(h2b_h2matrix *a, h2b_h2matrix *b);
+
+/* Storage and counts: info[0] nearfield entries, [1] coupling entries, [2] leaf-basis entries,
+ * [3] transfer entries, [4] bytes of device storage, [5] admissible blocks, [6] nearfield blocks,
+ * [7] rank k. */
+int h2b_h2matrix_info(const h2b_h2matrix *h2, uint64_t info[8]);
+
+/* Copy parts back for inspection, in H2Lib's layouts and orders (pre-order, column-major):
+ * part 0: leaf bases of the row basis, 1: transfer matrices of the row basis (all non-root
+ * clusters), 2/3 the same for the column basis, 4: coupling matrices of the admissible blocks,
+ * 5: nearfield blocks.  'count' limits the number of matrices (block-tree order); out may be NULL
+ * to query the number of doubles. */
+int h2b_h2matrix_export(const h2b_h2matrix *h2, int part, uint32_t count, double *out,
+                        uint64_t *ndoubles);
+
+/* y += alpha * A x.  Replaces addeval_h2matrix_avector (Library/h2matrix.c:1269): forward
+ * transform (Library/clusterbasis.c:524), coupling and nearfield (fastaddeval, Library/h2matrix.c:
+ * 1211), backward transform (Library/clusterbasis.c:749).  x has columns, y rows entries of the
+ * operator (complex operators: interleaved).  Host or device pointers. */
+int h2b_h2matrix_addeval(double alpha_re, double alpha_im, const h2b_h2matrix *h2,
+                         const double *x, double *y);
+
+/* Same with nrhs right-hand sides stored as columns of X (ldx) and Y (ldy). */
+int h2b_h2matrix_addeval_multi(double alpha_re, double alpha_im, const h2b_h2matrix *h2,
+                               uint32_t nrhs, const double *X, uint64_t ldx, double *Y,
+                               uint64_t ldy);
+
+/* ------------------------------------------------------------------------------------------
+ * GMRES
+ * ------------------------------------------------------------------------------------------ */
+
+/* Restarted GMRES with Householder QR on the operator  A = sum_i coef_i * H_i  (nterms H2
+ * matrices of the same size; nterms = 1, coef = 1 for a single matrix).  Replaces
+ * solve_gmres_avector (Library/krylovsolvers.c:183) with addeval_h2matrix_avector as operator,
+ * i.e. solve_gmres_h2matrix_avector (:254), and Brakhage-Werner style combinations.  Same
+ * algorithm as init_gmres / step_gmres / finish_gmres (Library/krylov.c:612/659/725): stops when
+ * the estimated residual |rhat_k| <= eps * ||b||, restarts every kmax-1 steps, at most
+ * maxiter-1 steps.  x holds the start vector and receives the solution.  Returns the number of
+ * iterations (>= 0) or a negative H2B_ERR_* code.  coef is interleaved complex (2*nterms). */
+int h2b_solve_gmres(uint32_t nterms, const h2b_h2matrix *const *ops, const double *coef,
+                    const double *b, double *x, double eps, uint32_t maxiter, uint32_t kmax);
+
+/* Relative residual ||b - A x|| / ||b|| computed in FP64 on the device (diagnostic). */
+int h2b_residual_norm(uint32_t nterms, const h2b_h2matrix *const *ops, const double *coef,
+                      const double *b, const double *x, double *relres);
+
+/* ------------------------------------------------------------------------------------------
+ * Right-hand sides and errors (Laplace test data)
+ * ------------------------------------------------------------------------------------------ */
+
+/* L2 projection of the harmonic function g(x) = 1/|x - z| onto the linear basis.  Replaces
+ * projectL2_bem3d_l_avector (Library/bem3d.c:9009) with f = eval_dirichlet_fundamental_
+ * laplacebem3d (Library/laplacebem3d.c:1391; z = (1.2, 1.2, 1.2) there).  Result in w[vertices]
+ * (host or device). */
+int h2b_project_l2_harmonic(const h2b_bem *bem, const double z[3], double *w);
+
+/* L2 norm of the difference between the linear-basis function u and the Neumann trace
+ * d/dn 1/|x - z| (normL2diff_l_bem3d, Library/bem3d.c:8954 with
+ * eval_neumann_fundamental_laplacebem3d, Library/laplacebem3d.c:1412), and the norm of the trace
+ * itself (normL2_bem3d, :8704). */
+int h2b_l2_error_harmonic(const h2b_bem *bem, const double z[3], const double *u, double *err,
+                          double *norm);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

@@ -1,0 +1,777 @@
+/* Golden-vector generator: runs the unmodified H2Lib reference (compiled from its own sources into
+ * oracle/_ref/libh2ref_{real,complex}.so by oracle/Makefile) on the synthetic inputs the tests use,
+ * and writes raw arrays plus a manifest into an output directory.  make_golden.py drives it and
+ * packs the arrays into the committed .npz fixtures.
+ *
+ * Built twice: without USE_COMPLEX (Laplace, real field) and with it (Helmholtz, complex field).
+ *
+ * Usage: gen_golden <outdir> <section> [...]
+ * Sections (real build):    quad sphere8 sphere4 h2small config2 cube
+ * Sections (complex build): helm_sphere4 helm_h2small
+ */
+#include <math.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include "basic.h"
+#include "bem3d.h"
+#include "block.h"
+#include "cluster.h"
+#include "clusterbasis.h"
+#include "gaussquad.h"
+#include "h2matrix.h"
+#include "krylovsolvers.h"
+#include "laplacebem3d.h"
+#include "macrosurface3d.h"
+#include "singquad2d.h"
+#include "surface3d.h"
+#ifdef USE_COMPLEX
+#include "helmholtzbem3d.h"
+#endif
+
+static const char *outdir;
+static FILE *manifest;
+
+/* ---------- raw array writer ---------- */
+
+static void
+dump(const char *name, const char *dtype, size_t esize, const void *data, int ndim,
+     size_t d0, size_t d1)
+{
+  char path[4096];
+  size_t n = (ndim == 1 ? d0 : d0 * d1);
+  FILE *f;
+
+  snprintf(path, sizeof(path), "%s/%s.bin", outdir, name);
+  f = fopen(path, "wb");
+  if (!f) {
+    perror(path);
+    exit(1);
+  }
+  if (n > 0 && fwrite(data, esize, n, f) != n) {
+    perror(path);
+    exit(1);
+  }
+  fclose(f);
+  if (ndim == 1)
+    fprintf(manifest, "%s %s %zu\n", name, dtype, d0);
+  else
+    fprintf(manifest, "%s %s %zu %zu\n", name, dtype, d0, d1);
+  fflush(manifest);
+}
+
+static void
+dump_real(const char *name, const real *v, int ndim, size_t d0, size_t d1)
+{
+  dump(name, "f8", sizeof(real), v, ndim, d0, d1);
+}
+
+static void
+dump_uint(const char *name, const uint *v, int ndim, size_t d0, size_t d1)
+{
+  dump(name, "u4", sizeof(uint), v, ndim, d0, d1);
+}
+
+static void
+dump_scalar(const char *name, double v)
+{
+  dump(name, "f8", sizeof(double), &v, 1, 1, 0);
+}
+
+/* Matrix stored column-major with ld: written as (cols, rows) C-order == column-major contiguous. */
+static void
+dump_amatrix(const char *name, pcamatrix A)
+{
+  size_t rows = A->rows, cols = A->cols, j;
+  field *buf = (field *) malloc(sizeof(field) * (rows * cols + 1));
+
+  for (j = 0; j < cols; j++)
+    memcpy(buf + j * rows, A->a + j * A->ld, sizeof(field) * rows);
+#ifdef USE_COMPLEX
+  dump(name, "c16", sizeof(field), buf, 2, cols, rows);
+#else
+  dump(name, "f8", sizeof(field), buf, 2, cols, rows);
+#endif
+  free(buf);
+}
+
+static void
+dump_avector(const char *name, pcavector v)
+{
+#ifdef USE_COMPLEX
+  dump(name, "c16", sizeof(field), v->v, 1, v->dim, 0);
+#else
+  dump(name, "f8", sizeof(field), v->v, 1, v->dim, 0);
+#endif
+}
+
+static void
+dump_mesh(const char *prefix, pcsurface3d gr)
+{
+  char name[256];
+
+  snprintf(name, sizeof(name), "%s_x", prefix);
+  dump_real(name, &gr->x[0][0], 2, gr->vertices, 3);
+  snprintf(name, sizeof(name), "%s_t", prefix);
+  dump_uint(name, &gr->t[0][0], 2, gr->triangles, 3);
+  snprintf(name, sizeof(name), "%s_n", prefix);
+  dump_real(name, &gr->n[0][0], 2, gr->triangles, 3);
+  snprintf(name, sizeof(name), "%s_g", prefix);
+  dump_real(name, gr->g, 1, gr->triangles, 0);
+  snprintf(name, sizeof(name), "%s_h", prefix);
+  {
+    real h[2] = { gr->hmin, gr->hmax };
+    dump_real(name, h, 1, 2, 0);
+  }
+}
+
+/* Deterministic test vector (stored in the fixture, so no bitwise libm agreement is needed). */
+static void
+seeded_avector(pavector x, uint salt)
+{
+  uint i;
+  for (i = 0; i < x->dim; i++) {
+    real re = sin(0.37 * i + 0.1 * salt) + 0.5 * cos(1.3 * i + 0.7);
+#ifdef USE_COMPLEX
+    real im = cos(0.21 * i + 0.3 * salt) - 0.25 * sin(2.1 * i);
+    x->v[i] = re + im * I;
+#else
+    x->v[i] = re;
+#endif
+  }
+}
+
+/* ---------- cluster / block tree flattening ---------- */
+
+typedef struct {
+  uint n, cap;
+  uint *rec;   /* per cluster: offset, size, sons */
+  real *box;   /* per cluster: bmin[3], bmax[3] */
+} ctree_t;
+
+static void
+flatten_cluster(pccluster t, const uint *root_idx, ctree_t *ct)
+{
+  uint i;
+  if (ct->n == ct->cap) {
+    ct->cap = ct->cap ? 2 * ct->cap : 256;
+    ct->rec = realloc(ct->rec, sizeof(uint) * 3 * ct->cap);
+    ct->box = realloc(ct->box, sizeof(real) * 6 * ct->cap);
+  }
+  ct->rec[3 * ct->n + 0] = (uint) (t->idx - root_idx);
+  ct->rec[3 * ct->n + 1] = t->size;
+  ct->rec[3 * ct->n + 2] = t->sons;
+  for (i = 0; i < 3; i++) {
+    ct->box[6 * ct->n + i] = t->bmin[i];
+    ct->box[6 * ct->n + 3 + i] = t->bmax[i];
+  }
+  ct->n++;
+  for (i = 0; i < t->sons; i++)
+    flatten_cluster(t->son[i], root_idx, ct);
+}
+
+static void
+dump_cluster(const char *prefix, pccluster root)
+{
+  ctree_t ct = { 0, 0, NULL, NULL };
+  char name[256];
+
+  flatten_cluster(root, root->idx, &ct);
+  snprintf(name, sizeof(name), "%s_ctree", prefix);
+  dump_uint(name, ct.rec, 2, ct.n, 3);
+  snprintf(name, sizeof(name), "%s_cbox", prefix);
+  dump_real(name, ct.box, 2, ct.n, 6);
+  snprintf(name, sizeof(name), "%s_idx", prefix);
+  dump_uint(name, root->idx, 1, root->size, 0);
+  free(ct.rec);
+  free(ct.box);
+}
+
+typedef struct {
+  uint n, cap;
+  uint *rec;   /* per leaf block: rc offset, rc size, cc offset, cc size, admissible */
+} btree_t;
+
+static void
+flatten_block(pcblock b, const uint *ridx0, const uint *cidx0, btree_t *bt)
+{
+  uint i, j;
+  if (b->son == NULL) {
+    if (bt->n == bt->cap) {
+      bt->cap = bt->cap ? 2 * bt->cap : 1024;
+      bt->rec = realloc(bt->rec, sizeof(uint) * 5 * bt->cap);
+    }
+    bt->rec[5 * bt->n + 0] = (uint) (b->rc->idx - ridx0);
+    bt->rec[5 * bt->n + 1] = b->rc->size;
+    bt->rec[5 * bt->n + 2] = (uint) (b->cc->idx - cidx0);
+    bt->rec[5 * bt->n + 3] = b->cc->size;
+    bt->rec[5 * bt->n + 4] = b->a ? 1 : 0;
+    bt->n++;
+    return;
+  }
+  for (j = 0; j < b->csons; j++)
+    for (i = 0; i < b->rsons; i++)
+      flatten_block(b->son[i + j * b->rsons], ridx0, cidx0, bt);
+}
+
+static void
+dump_block(const char *prefix, pcblock b, pccluster rroot, pccluster croot)
+{
+  btree_t bt = { 0, 0, NULL };
+  char name[256];
+
+  flatten_block(b, rroot->idx, croot->idx, &bt);
+  snprintf(name, sizeof(name), "%s_blocks", prefix);
+  dump_uint(name, bt.rec, 2, bt.n, 5);
+  free(bt.rec);
+}
+
+/* Leaf bases V and transfer matrices E of a cluster basis, pre-order, concatenated. */
+typedef struct {
+  size_t n, cap;
+  field *v;
+} fbuf_t;
+
+static void
+fbuf_push(fbuf_t *b, pcamatrix A)
+{
+  size_t need = (size_t) A->rows * A->cols, j;
+  if (b->n + need > b->cap) {
+    b->cap = (b->n + need) * 2 + 1024;
+    b->v = realloc(b->v, sizeof(field) * b->cap);
+  }
+  for (j = 0; j < A->cols; j++)
+    memcpy(b->v + b->n + j * A->rows, A->a + j * A->ld, sizeof(field) * A->rows);
+  b->n += need;
+}
+
+static void
+collect_basis(pcclusterbasis cb, fbuf_t *V, fbuf_t *E, int is_root)
+{
+  uint i;
+  if (!is_root)
+    fbuf_push(E, &cb->E);
+  if (cb->sons == 0)
+    fbuf_push(V, &cb->V);
+  for (i = 0; i < cb->sons; i++)
+    collect_basis(cb->son[i], V, E, 0);
+}
+
+static void
+dump_basis(const char *prefix, pcclusterbasis cb)
+{
+  fbuf_t V = { 0, 0, NULL }, E = { 0, 0, NULL };
+  char name[256];
+  collect_basis(cb, &V, &E, 1);
+#ifdef USE_COMPLEX
+  const char *dt = "c16";
+#else
+  const char *dt = "f8";
+#endif
+  snprintf(name, sizeof(name), "%s_V", prefix);
+  dump(name, dt, sizeof(field), V.v, 1, V.n, 0);
+  snprintf(name, sizeof(name), "%s_E", prefix);
+  dump(name, dt, sizeof(field), E.v, 1, E.n, 0);
+  free(V.v);
+  free(E.v);
+}
+
+/* Coupling matrices of the first `limit` admissible leaves (block-tree pre-order). */
+static void
+collect_coupling(pch2matrix G, fbuf_t *S, uint *count, uint limit)
+{
+  uint i, j;
+  if (*count >= limit)
+    return;
+  if (G->u) {
+    fbuf_push(S, &G->u->S);
+    (*count)++;
+    return;
+  }
+  if (G->son)
+    for (j = 0; j < G->csons; j++)
+      for (i = 0; i < G->rsons; i++)
+        collect_coupling(G->son[i + j * G->rsons], S, count, limit);
+}
+
+/* Nearfield matrices of the first `limit` inadmissible leaves (block-tree pre-order). */
+static void
+collect_near(pch2matrix G, fbuf_t *N, uint *count, uint limit)
+{
+  uint i, j;
+  if (*count >= limit)
+    return;
+  if (G->f) {
+    fbuf_push(N, G->f);
+    (*count)++;
+    return;
+  }
+  if (G->son)
+    for (j = 0; j < G->csons; j++)
+      for (i = 0; i < G->rsons; i++)
+        collect_near(G->son[i + j * G->rsons], N, count, limit);
+}
+
+static void
+dump_h2parts(const char *prefix, pch2matrix G, uint limit)
+{
+  fbuf_t S = { 0, 0, NULL }, N = { 0, 0, NULL };
+  uint cnt = 0;
+  char name[256];
+#ifdef USE_COMPLEX
+  const char *dt = "c16";
+#else
+  const char *dt = "f8";
+#endif
+  collect_coupling(G, &S, &cnt, limit);
+  snprintf(name, sizeof(name), "%s_S", prefix);
+  dump(name, dt, sizeof(field), S.v, 1, S.n, 0);
+  cnt = 0;
+  collect_near(G, &N, &cnt, limit);
+  snprintf(name, sizeof(name), "%s_N", prefix);
+  dump(name, dt, sizeof(field), N.v, 1, N.n, 0);
+  free(S.v);
+  free(N.v);
+}
+
+/* ---------- sections ---------- */
+
+#ifndef USE_COMPLEX
+
+static void
+section_quad(void)
+{
+  uint qs[4] = { 2, 3, 4, 5 }, i, j;
+  char name[64];
+  psingquad2d sq;
+  pmacrosurface3d mg;
+  psurface3d gr;
+
+  for (i = 0; i < 4; i++) {
+    real x[8], w[8];
+    assemble_gauss(qs[i], x, w);
+    for (j = 0; j < qs[i]; j++) {
+      x[j] = 0.5 + 0.5 * x[j];
+      w[j] = 0.5 * w[j];
+    }
+    snprintf(name, sizeof(name), "gauss%u_x", qs[i]);
+    dump_real(name, x, 1, qs[i], 0);
+    snprintf(name, sizeof(name), "gauss%u_w", qs[i]);
+    dump_real(name, w, 1, qs[i], 0);
+  }
+
+  mg = new_sphere_macrosurface3d();
+  gr = build_from_macrosurface3d_surface3d(mg, 2);
+  sq = build_singquad2d(gr, 2, 4);
+  /* VREAL == 1 in the scalar build, so vnq == n for every rule. */
+  dump_real("dist_x", sq->x_dist, 2, 2, sq->n_dist);
+  dump_real("dist_y", sq->y_dist, 2, 2, sq->n_dist);
+  dump_real("dist_w", sq->w_dist + 9 * sq->n_dist, 1, sq->n_dist, 0);
+  dump_real("vert_x", sq->x_vert, 2, 2, sq->n_vert);
+  dump_real("vert_y", sq->y_vert, 2, 2, sq->n_vert);
+  dump_real("vert_w", sq->w_vert + 9 * sq->n_vert, 1, sq->n_vert, 0);
+  dump_real("edge_x", sq->x_edge, 2, 2, sq->n_edge);
+  dump_real("edge_y", sq->y_edge, 2, 2, sq->n_edge);
+  dump_real("edge_w", sq->w_edge + 9 * sq->n_edge, 1, sq->n_edge, 0);
+  dump_real("id_x", sq->x_id, 2, 2, sq->n_id);
+  dump_real("id_y", sq->y_id, 2, 2, sq->n_id);
+  dump_real("id_w", sq->w_id + 9 * sq->n_id, 1, sq->n_id, 0);
+  dump_real("single_x", sq->x_single, 1, sq->n_single, 0);
+  dump_real("single_y", sq->y_single, 1, sq->n_single, 0);
+  dump_real("single_w", sq->w_single + 3 * sq->n_single, 1, sq->n_single, 0);
+  /* basis-weighted (ll) edge rule: all ten weight rows */
+  weight_basisfunc_ll_singquad2d(sq->x_edge, sq->y_edge, sq->w_edge, sq->n_edge);
+  dump_real("edge_w_ll", sq->w_edge, 2, 10, sq->n_edge);
+  weight_basisfunc_l_singquad2d(sq->x_single, sq->y_single, sq->w_single, sq->n_single);
+  dump_real("single_w_l", sq->w_single, 2, 4, sq->n_single);
+  del_singquad2d(sq);
+  del_surface3d(gr);
+  del_macrosurface3d(mg);
+}
+
+static void
+dense_pair(const char *prefix, psurface3d gr, basisfunctionbem3d rb, basisfunctionbem3d cb,
+           int with_block)
+{
+  pbem3d slp, dlp;
+  pamatrix A;
+  uint n = (rb == BASIS_LINEAR_BEM3D) ? gr->vertices : gr->triangles;
+  uint m = (cb == BASIS_LINEAR_BEM3D) ? gr->vertices : gr->triangles;
+  char name[256];
+
+  slp = new_slp_laplace_bem3d(gr, 2, 4, rb, cb);
+  dlp = new_dlp_laplace_bem3d(gr, 2, 4, rb, cb, 0.5);
+
+  A = new_amatrix(n, m);
+  slp->nearfield(NULL, NULL, slp, false, A);
+  snprintf(name, sizeof(name), "%s_slp", prefix);
+  dump_amatrix(name, A);
+  dlp->nearfield(NULL, NULL, dlp, false, A);
+  snprintf(name, sizeof(name), "%s_dlp", prefix);
+  dump_amatrix(name, A);
+  del_amatrix(A);
+
+  if (with_block) {
+    /* a ragged sub-block with non-contiguous, unsorted index lists */
+    uint ridx[7] = { 5, 9, 20, 33, 2, 61, 40 };
+    uint cidx[5] = { 1, 40, 2, 60, 65 };
+    pamatrix B = new_amatrix(7, 5);
+    slp->nearfield(ridx, cidx, slp, false, B);
+    snprintf(name, sizeof(name), "%s_slp_block", prefix);
+    dump_amatrix(name, B);
+    dlp->nearfield(ridx, cidx, dlp, false, B);
+    snprintf(name, sizeof(name), "%s_dlp_block", prefix);
+    dump_amatrix(name, B);
+    /* transposed write */
+    {
+      pamatrix Bt = new_amatrix(5, 7);
+      dlp->nearfield(ridx, cidx, dlp, true, Bt);
+      snprintf(name, sizeof(name), "%s_dlp_block_trans", prefix);
+      dump_amatrix(name, Bt);
+      del_amatrix(Bt);
+    }
+    dump_uint("block_ridx", ridx, 1, 7, 0);
+    dump_uint("block_cidx", cidx, 1, 5, 0);
+    del_amatrix(B);
+  }
+  del_laplace_bem3d(slp);
+  del_laplace_bem3d(dlp);
+}
+
+static void
+section_sphere8(void)
+{
+  pmacrosurface3d mg = new_sphere_macrosurface3d();
+  psurface3d gr = build_from_macrosurface3d_surface3d(mg, 8);
+  pbem3d slp, dlp;
+  pamatrix G;
+
+  dump_mesh("sphere8", gr);
+  /* config 1: assemble_bem3d_amatrix, cc, q=2/4 */
+  slp = new_slp_laplace_bem3d(gr, 2, 4, BASIS_CONSTANT_BEM3D, BASIS_CONSTANT_BEM3D);
+  dlp = new_dlp_laplace_bem3d(gr, 2, 4, BASIS_CONSTANT_BEM3D, BASIS_CONSTANT_BEM3D, 0.5);
+  G = new_amatrix(gr->triangles, gr->triangles);
+  assemble_bem3d_amatrix(slp, G);
+  dump_amatrix("c1_slp", G);
+  assemble_bem3d_amatrix(dlp, G);
+  dump_amatrix("c1_dlp", G);
+  del_amatrix(G);
+  del_laplace_bem3d(slp);
+  del_laplace_bem3d(dlp);
+  del_surface3d(gr);
+  del_macrosurface3d(mg);
+}
+
+static void
+section_sphere4(void)
+{
+  pmacrosurface3d mg = new_sphere_macrosurface3d();
+  psurface3d gr = build_from_macrosurface3d_surface3d(mg, 4);
+
+  dump_mesh("sphere4", gr);
+  dense_pair("s4cc", gr, BASIS_CONSTANT_BEM3D, BASIS_CONSTANT_BEM3D, 0);
+  dense_pair("s4ll", gr, BASIS_LINEAR_BEM3D, BASIS_LINEAR_BEM3D, 1);
+  del_surface3d(gr);
+  del_macrosurface3d(mg);
+}
+
+/* Full H2 pipeline on one mesh: trees, bases, coupling, nearfield, matvec. */
+static void
+h2_case(const char *prefix, psurface3d gr, basisfunctionbem3d basis, uint clf, real eta,
+        uint m, uint parts_limit, int with_solve)
+{
+  pbem3d slp, dlp;
+  pcluster root;
+  pblock broot;
+  pclusterbasis Vrb, Vcb, Krb, Kcb;
+  ph2matrix V, K;
+  pavector x, y;
+  char name[256];
+  double t0;
+  pstopwatch sw = new_stopwatch();
+
+  slp = new_slp_laplace_bem3d(gr, 2, 4, basis, basis);
+  dlp = new_dlp_laplace_bem3d(gr, 2, 4, basis, basis, 0.5);
+  root = build_bem3d_cluster(slp, clf, basis);
+  broot = build_strict_block(root, root, &eta, admissible_max_cluster);
+  snprintf(name, sizeof(name), "%s", prefix);
+  dump_cluster(name, root);
+  dump_block(name, broot, root, root);
+
+  Vrb = build_from_cluster_clusterbasis(root);
+  Vcb = build_from_cluster_clusterbasis(root);
+  Krb = build_from_cluster_clusterbasis(root);
+  Kcb = build_from_cluster_clusterbasis(root);
+  V = build_from_block_h2matrix(broot, Vrb, Vcb);
+  K = build_from_block_h2matrix(broot, Krb, Kcb);
+  setup_h2matrix_aprx_inter_bem3d(slp, Vrb, Vcb, broot, m);
+  setup_h2matrix_aprx_inter_bem3d(dlp, Krb, Kcb, broot, m);
+
+  start_stopwatch(sw);
+  assemble_bem3d_h2matrix_row_clusterbasis(slp, Vrb);
+  assemble_bem3d_h2matrix_col_clusterbasis(slp, Vcb);
+  assemble_bem3d_h2matrix(slp, V);
+  t0 = stop_stopwatch(sw);
+  snprintf(name, sizeof(name), "%s_time_slp_assembly", prefix);
+  dump_scalar(name, t0);
+  start_stopwatch(sw);
+  assemble_bem3d_h2matrix_row_clusterbasis(dlp, Krb);
+  assemble_bem3d_h2matrix_col_clusterbasis(dlp, Kcb);
+  assemble_bem3d_h2matrix(dlp, K);
+  t0 = stop_stopwatch(sw);
+  snprintf(name, sizeof(name), "%s_time_dlp_assembly", prefix);
+  dump_scalar(name, t0);
+
+  if (parts_limit > 0) {
+    snprintf(name, sizeof(name), "%s_Vrow", prefix);
+    dump_basis(name, Vrb);
+    snprintf(name, sizeof(name), "%s_Kcol", prefix);
+    dump_basis(name, Kcb);
+    snprintf(name, sizeof(name), "%s_Vparts", prefix);
+    dump_h2parts(name, V, parts_limit);
+    snprintf(name, sizeof(name), "%s_Kparts", prefix);
+    dump_h2parts(name, K, parts_limit);
+  }
+
+  x = new_avector(V->cb->t->size);
+  y = new_avector(V->rb->t->size);
+  seeded_avector(x, 1);
+  snprintf(name, sizeof(name), "%s_x", prefix);
+  dump_avector(name, x);
+  clear_avector(y);
+  start_stopwatch(sw);
+  addeval_h2matrix_avector(1.0, V, x, y);
+  t0 = stop_stopwatch(sw);
+  snprintf(name, sizeof(name), "%s_time_matvec", prefix);
+  dump_scalar(name, t0);
+  snprintf(name, sizeof(name), "%s_ySLP", prefix);
+  dump_avector(name, y);
+  clear_avector(y);
+  addeval_h2matrix_avector(1.0, K, x, y);
+  snprintf(name, sizeof(name), "%s_yDLP", prefix);
+  dump_avector(name, y);
+
+  if (with_solve) {
+    /* Interior Dirichlet problem: V u = (K + 1/2 M) g_D, GMRES(50) to 1e-8, start from zero. */
+    pavector f = new_avector(x->dim), b = new_avector(x->dim), u = new_avector(x->dim);
+    uint iter;
+    real err, nrm;
+    projectL2_bem3d_l_avector(dlp, eval_dirichlet_fundamental_laplacebem3d, f, NULL);
+    snprintf(name, sizeof(name), "%s_gD", prefix);
+    dump_avector(name, f);
+    clear_avector(b);
+    addeval_h2matrix_avector(1.0, K, f, b);
+    snprintf(name, sizeof(name), "%s_b", prefix);
+    dump_avector(name, b);
+    clear_avector(u);
+    start_stopwatch(sw);
+    iter = solve_gmres_h2matrix_avector(V, b, u, 1.0e-8, 1000, 50);
+    t0 = stop_stopwatch(sw);
+    snprintf(name, sizeof(name), "%s_time_gmres", prefix);
+    dump_scalar(name, t0);
+    snprintf(name, sizeof(name), "%s_gmres_iter", prefix);
+    dump_scalar(name, (double) iter);
+    snprintf(name, sizeof(name), "%s_u", prefix);
+    dump_avector(name, u);
+    err = normL2diff_l_bem3d(slp, u, eval_neumann_fundamental_laplacebem3d, NULL);
+    nrm = normL2_bem3d(slp, eval_neumann_fundamental_laplacebem3d, NULL);
+    snprintf(name, sizeof(name), "%s_l2err", prefix);
+    dump_scalar(name, err);
+    snprintf(name, sizeof(name), "%s_l2norm", prefix);
+    dump_scalar(name, nrm);
+    del_avector(f);
+    del_avector(b);
+    del_avector(u);
+  }
+
+  del_avector(x);
+  del_avector(y);
+  del_h2matrix(V);
+  del_h2matrix(K);
+  del_block(broot);
+  freemem(root->idx);
+  del_cluster(root);
+  del_laplace_bem3d(slp);
+  del_laplace_bem3d(dlp);
+  del_stopwatch(sw);
+}
+
+static void
+section_h2small(void)
+{
+  pmacrosurface3d mg = new_sphere_macrosurface3d();
+  psurface3d gr = build_from_macrosurface3d_surface3d(mg, 8);
+  h2_case("h2ll", gr, BASIS_LINEAR_BEM3D, 16, 1.4, 3, 24, 1);
+  h2_case("h2cc", gr, BASIS_CONSTANT_BEM3D, 16, 1.4, 3, 24, 0);
+  del_surface3d(gr);
+  del_macrosurface3d(mg);
+}
+
+static void
+section_config2(void)
+{
+  pmacrosurface3d mg = new_sphere_macrosurface3d();
+  psurface3d gr = build_from_macrosurface3d_surface3d(mg, 64);
+  dump_real("c2mesh_x", &gr->x[0][0], 2, gr->vertices, 3);
+  dump_uint("c2mesh_t", &gr->t[0][0], 2, gr->triangles, 3);
+  h2_case("c2", gr, BASIS_LINEAR_BEM3D, 64, 1.4, 4, 0, 1);
+  del_surface3d(gr);
+  del_macrosurface3d(mg);
+}
+
+static void
+section_cube(void)
+{
+  pmacrosurface3d mg = new_cube_macrosurface3d();
+  psurface3d gr = build_from_macrosurface3d_surface3d(mg, 4);
+  dump_mesh("cube4", gr);
+  del_surface3d(gr);
+  gr = build_from_macrosurface3d_surface3d(mg, 64);
+  dump_real("cube64_x", &gr->x[0][0], 2, gr->vertices, 3);
+  dump_uint("cube64_t", &gr->t[0][0], 2, gr->triangles, 3);
+  del_surface3d(gr);
+  del_macrosurface3d(mg);
+}
+
+#else /* USE_COMPLEX */
+
+static void
+section_helm_sphere4(void)
+{
+  pmacrosurface3d mg = new_sphere_macrosurface3d();
+  psurface3d gr = build_from_macrosurface3d_surface3d(mg, 4);
+  field k = 2.0;
+  pbem3d slp, dlp;
+  pamatrix A = new_amatrix(gr->triangles, gr->triangles);
+
+  slp = new_slp_helmholtz_bem3d(k, gr, 2, 4, BASIS_CONSTANT_BEM3D, BASIS_CONSTANT_BEM3D);
+  dlp = new_dlp_helmholtz_bem3d(k, gr, 2, 4, BASIS_CONSTANT_BEM3D, BASIS_CONSTANT_BEM3D, 0.5);
+  slp->nearfield(NULL, NULL, slp, false, A);
+  dump_amatrix("hs4cc_slp", A);
+  dlp->nearfield(NULL, NULL, dlp, false, A);
+  dump_amatrix("hs4cc_dlp", A);
+  del_helmholtz_bem3d(slp);
+  del_helmholtz_bem3d(dlp);
+  /* complex wavenumber (damped) */
+  k = 2.0 + 0.5 * I;
+  slp = new_slp_helmholtz_bem3d(k, gr, 2, 4, BASIS_CONSTANT_BEM3D, BASIS_CONSTANT_BEM3D);
+  slp->nearfield(NULL, NULL, slp, false, A);
+  dump_amatrix("hs4cc_slp_damped", A);
+  del_helmholtz_bem3d(slp);
+  del_amatrix(A);
+  del_surface3d(gr);
+  del_macrosurface3d(mg);
+}
+
+static void
+section_helm_h2small(void)
+{
+  pmacrosurface3d mg = new_sphere_macrosurface3d();
+  psurface3d gr = build_from_macrosurface3d_surface3d(mg, 8);
+  field k = 2.0;
+  real eta = 1.4;
+  pbem3d slp, dlp;
+  pcluster root;
+  pblock broot;
+  pclusterbasis Vrb, Vcb, Krb, Kcb;
+  ph2matrix V, K;
+  pavector x, y;
+
+  slp = new_slp_helmholtz_bem3d(k, gr, 2, 4, BASIS_CONSTANT_BEM3D, BASIS_CONSTANT_BEM3D);
+  dlp = new_dlp_helmholtz_bem3d(k, gr, 2, 4, BASIS_CONSTANT_BEM3D, BASIS_CONSTANT_BEM3D, 0.5);
+  root = build_bem3d_cluster(slp, 16, BASIS_CONSTANT_BEM3D);
+  broot = build_strict_block(root, root, &eta, admissible_max_cluster);
+  dump_cluster("hh2", root);
+  dump_block("hh2", broot, root, root);
+  Vrb = build_from_cluster_clusterbasis(root);
+  Vcb = build_from_cluster_clusterbasis(root);
+  Krb = build_from_cluster_clusterbasis(root);
+  Kcb = build_from_cluster_clusterbasis(root);
+  V = build_from_block_h2matrix(broot, Vrb, Vcb);
+  K = build_from_block_h2matrix(broot, Krb, Kcb);
+  setup_h2matrix_aprx_inter_bem3d(slp, Vrb, Vcb, broot, 3);
+  setup_h2matrix_aprx_inter_bem3d(dlp, Krb, Kcb, broot, 3);
+  assemble_bem3d_h2matrix_row_clusterbasis(slp, Vrb);
+  assemble_bem3d_h2matrix_col_clusterbasis(slp, Vcb);
+  assemble_bem3d_h2matrix(slp, V);
+  assemble_bem3d_h2matrix_row_clusterbasis(dlp, Krb);
+  assemble_bem3d_h2matrix_col_clusterbasis(dlp, Kcb);
+  assemble_bem3d_h2matrix(dlp, K);
+  dump_basis("hh2_Vrow", Vrb);
+  dump_basis("hh2_Kcol", Kcb);
+  dump_h2parts("hh2_Vparts", V, 24);
+
+  x = new_avector(gr->triangles);
+  y = new_avector(gr->triangles);
+  seeded_avector(x, 2);
+  dump_avector("hh2_x", x);
+  clear_avector(y);
+  addeval_h2matrix_avector(1.0, V, x, y);
+  dump_avector("hh2_ySLP", y);
+  clear_avector(y);
+  addeval_h2matrix_avector(1.0, K, x, y);
+  dump_avector("hh2_yDLP", y);
+
+  del_avector(x);
+  del_avector(y);
+  del_h2matrix(V);
+  del_h2matrix(K);
+  del_block(broot);
+  freemem(root->idx);
+  del_cluster(root);
+  del_helmholtz_bem3d(slp);
+  del_helmholtz_bem3d(dlp);
+  del_surface3d(gr);
+  del_macrosurface3d(mg);
+}
+
+#endif
+
+int
+main(int argc, char **argv)
+{
+  char path[4096];
+  int i;
+
+  init_h2lib(&argc, &argv);
+  if (argc < 3) {
+    fprintf(stderr, "usage: %s outdir section...\n", argv[0]);
+    return 2;
+  }
+  outdir = argv[1];
+  snprintf(path, sizeof(path), "%s/manifest.txt", outdir);
+  manifest = fopen(path, "a");
+  if (!manifest) {
+    perror(path);
+    return 1;
+  }
+  for (i = 2; i < argc; i++) {
+#ifndef USE_COMPLEX
+    if (!strcmp(argv[i], "quad"))
+      section_quad();
+    else if (!strcmp(argv[i], "sphere8"))
+      section_sphere8();
+    else if (!strcmp(argv[i], "sphere4"))
+      section_sphere4();
+    else if (!strcmp(argv[i], "h2small"))
+      section_h2small();
+    else if (!strcmp(argv[i], "config2"))
+      section_config2();
+    else if (!strcmp(argv[i], "cube"))
+      section_cube();
+#else
+    if (!strcmp(argv[i], "helm_sphere4"))
+      section_helm_sphere4();
+    else if (!strcmp(argv[i], "helm_h2small"))
+      section_helm_h2small();
+#endif
+    else {
+      fprintf(stderr, "unknown section %s\n", argv[i]);
+      return 2;
+    }
+  }
+  fclose(manifest);
+  uninit_h2lib();
+  return 0;
+}

@@ -1,0 +1,72 @@
+"""Regenerate the golden fixtures in this directory from the unmodified H2Lib reference.
+
+Builds oracle/_ref/libh2ref_{real,complex}.so from the reference sources (oracle/Makefile), compiles
+gen_golden.c against them, runs the requested sections and packs each section's raw arrays into
+``<section>.npz``.  Needs the reference tree (REF, default /root/reference); the tests themselves only
+read the committed .npz files.
+
+    python tests/golden/make_golden.py [section ...]
+
+Sections: quad sphere8 sphere4 h2small config2 cube helm_sphere4 helm_h2small
+"""
+import os
+import subprocess
+import sys
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+REF = os.environ.get("REF", "/root/reference")
+REFOUT = os.path.join(ROOT, "oracle", "_ref")
+
+REAL_SECTIONS = ["quad", "sphere8", "sphere4", "h2small", "config2", "cube"]
+COMPLEX_SECTIONS = ["helm_sphere4", "helm_h2small"]
+DTYPES = {"f8": np.float64, "u4": np.uint32, "c16": np.complex128}
+# Arrays stored only in part, to keep the fixtures small: name -> number of leading columns kept
+# (matrices are written column-major, i.e. shape (cols, rows)).
+CROP = {"c1_dlp": 128}
+
+
+def build():
+    subprocess.check_call(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "ref",
+                           f"REF={REF}", f"-j{os.cpu_count()}"])
+    exes = {}
+    for variant, flags in (("real", []), ("complex", ["-DUSE_COMPLEX"])):
+        exe = os.path.join(REFOUT, f"gen_golden_{variant}")
+        subprocess.check_call(["gcc", "-O2", "-w", *flags, f"-I{REF}/Library",
+                               os.path.join(HERE, "gen_golden.c"), "-o", exe,
+                               f"-L{REFOUT}", f"-lh2ref_{variant}",
+                               f"-Wl,-rpath,{REFOUT}", "-lm"])
+        exes[variant] = exe
+    return exes
+
+
+def run_section(exe, section):
+    with tempfile.TemporaryDirectory() as tmp:
+        subprocess.check_call([exe, tmp, section])
+        arrays = {}
+        with open(os.path.join(tmp, "manifest.txt")) as fh:
+            for line in fh:
+                parts = line.split()
+                name, dt, shape = parts[0], DTYPES[parts[1]], tuple(int(s) for s in parts[2:])
+                data = np.fromfile(os.path.join(tmp, name + ".bin"), dtype=dt)
+                data = data.reshape(shape)
+                if name in CROP:
+                    data = data[:CROP[name]].copy()
+                arrays[name] = data
+    out = os.path.join(HERE, f"{section}.npz")
+    np.savez_compressed(out, **arrays)
+    print(f"{section}: {len(arrays)} arrays -> {os.path.relpath(out, ROOT)}")
+
+
+def main(argv):
+    sections = argv or REAL_SECTIONS + COMPLEX_SECTIONS
+    exes = build()
+    for s in sections:
+        run_section(exes["complex" if s in COMPLEX_SECTIONS else "real"], s)
+
+
+if __name__ == "__main__":
+    main(sys.argv[1:])

@@ -1,0 +1,158 @@
+"""Pin the CPU oracle against golden vectors produced by the unmodified H2Lib reference.
+
+Everything here runs on the CPU.  Tolerances: rules and meshes to 1e-14 (rounding of the
+Gauss nodes), nearfield entries to 1e-12 with the row-scaled entrywise rule (the parity bound of
+the FP64 path), H2 parts / matvecs to 1e-12 relative.
+"""
+import numpy as np
+import pytest
+
+from conftest import fortran, rel_entry_err
+from oracle import oracle as orc
+
+L, C = ord("l"), ord("c")
+
+
+def mesh_from(g, prefix):
+    return orc.Mesh(g[f"{prefix}_x"], g[f"{prefix}_t"], g[f"{prefix}_n"], g[f"{prefix}_g"])
+
+
+def test_gauss_rules(gold):
+    g = gold("quad")
+    for q in (2, 3, 4, 5):
+        x, w = orc.gauss01(q)
+        np.testing.assert_allclose(x, g[f"gauss{q}_x"], rtol=0, atol=2e-15)
+        np.testing.assert_allclose(w, g[f"gauss{q}_w"], rtol=0, atol=2e-15)
+
+
+@pytest.mark.parametrize("which,name", [(0, "dist"), (1, "vert"), (2, "edge"), (3, "id")])
+def test_sauter_schwab_rules(gold, which, name):
+    g = gold("quad")
+    r = orc.rule(2, 4, which)
+    np.testing.assert_allclose(r["x0"], g[f"{name}_x"][0], atol=1e-15)
+    np.testing.assert_allclose(r["x1"], g[f"{name}_x"][1], atol=1e-15)
+    np.testing.assert_allclose(r["y0"], g[f"{name}_y"][0], atol=1e-15)
+    np.testing.assert_allclose(r["y1"], g[f"{name}_y"][1], atol=1e-15)
+    np.testing.assert_allclose(r["w"], g[f"{name}_w"], rtol=1e-13, atol=1e-18)
+    # every rule integrates 1 over the product of two reference triangles (area 1/2 each)
+    assert abs(r["w"].sum() - 0.25) < 1e-13
+
+
+@pytest.mark.parametrize("layer", [orc.SLP, orc.DLP])
+@pytest.mark.parametrize("basis", ["cc", "ll"])
+def test_nearfield_sphere4(gold, layer, basis):
+    g = gold("sphere4")
+    mesh = mesh_from(g, "sphere4")
+    b = L if basis == "ll" else C
+    alpha = 0.5 if layer == orc.DLP else 0.0
+    A = orc.nearfield(mesh, orc.LAPLACE, layer, b, b, alpha=alpha)
+    ref = fortran(g[f"s4{basis}_{'slp' if layer == orc.SLP else 'dlp'}"])
+    assert A.shape == ref.shape
+    assert rel_entry_err(A, ref) < 1e-12
+
+
+def test_nearfield_ll_ragged_block_and_transpose(gold):
+    g = gold("sphere4")
+    mesh = mesh_from(g, "sphere4")
+    ridx, cidx = g["block_ridx"], g["block_cidx"]
+    A = orc.nearfield(mesh, orc.LAPLACE, orc.SLP, L, L, ridx, cidx)
+    assert rel_entry_err(A, fortran(g["s4ll_slp_block"])) < 1e-12
+    A = orc.nearfield(mesh, orc.LAPLACE, orc.DLP, L, L, ridx, cidx, alpha=0.5)
+    assert rel_entry_err(A, fortran(g["s4ll_dlp_block"])) < 1e-12
+    At = orc.nearfield(mesh, orc.LAPLACE, orc.DLP, L, L, ridx, cidx, alpha=0.5, ntrans=True)
+    assert rel_entry_err(At, fortran(g["s4ll_dlp_block_trans"])) < 1e-12
+
+
+def test_nearfield_config1_dense(gold):
+    """512 x 512 cc SLP / DLP on the sphere refined x8 (the entrywise parity case)."""
+    g = gold("sphere8")
+    mesh = mesh_from(g, "sphere8")
+    A = orc.nearfield(mesh, orc.LAPLACE, orc.SLP, C, C)
+    assert rel_entry_err(A, fortran(g["c1_slp"])) < 1e-12
+    cols = g["c1_dlp"].shape[0]
+    A = orc.nearfield(mesh, orc.LAPLACE, orc.DLP, C, C, cidx=np.arange(cols), alpha=0.5)
+    assert rel_entry_err(A, fortran(g["c1_dlp"])) < 1e-12
+
+
+@pytest.mark.parametrize("name,layer,k,alpha", [
+    ("hs4cc_slp", orc.SLP, 2.0, 0.0), ("hs4cc_dlp", orc.DLP, 2.0, 0.5),
+    ("hs4cc_slp_damped", orc.SLP, 2.0 + 0.5j, 0.0)])
+def test_nearfield_helmholtz(gold, name, layer, k, alpha):
+    mesh = mesh_from(gold("sphere4"), "sphere4")
+    A = orc.nearfield(mesh, orc.HELMHOLTZ, layer, C, C, k=k, alpha=alpha)
+    assert rel_entry_err(A, fortran(gold("helm_sphere4")[name])) < 1e-12
+
+
+def tree_arrays(g, prefix):
+    rec, box, idx = g[f"{prefix}_ctree"], g[f"{prefix}_cbox"], g[f"{prefix}_idx"]
+    key = {(int(o), int(s)): i for i, (o, s, _) in enumerate(rec)}
+    blk = g[f"{prefix}_blocks"]
+    brc = np.array([key[(int(b[0]), int(b[1]))] for b in blk], dtype=np.uint32)
+    bcc = np.array([key[(int(b[2]), int(b[3]))] for b in blk], dtype=np.uint32)
+    return (rec, box, idx), (brc, bcc, blk[:, 4].astype(np.uint8))
+
+
+def oracle_h2(g, mesh, prefix, basis, layer, m, pde=orc.LAPLACE, k=0.0):
+    tree, blocks = tree_arrays(g, prefix)
+    alpha = 0.5 if layer == orc.DLP else 0.0
+    return orc.H2(mesh, pde, layer, basis, basis, m, tree, tree, blocks, k=k, alpha=alpha)
+
+
+def relerr(a, b):
+    return float(np.linalg.norm(np.ravel(a) - np.ravel(b)) / np.linalg.norm(np.ravel(b)))
+
+
+@pytest.mark.parametrize("prefix,basis", [("h2ll", L), ("h2cc", C)])
+def test_h2_parts_and_matvec(gold, prefix, basis):
+    g = gold("h2small")
+    mesh = mesh_from(gold("sphere8"), "sphere8")
+    V = oracle_h2(g, mesh, prefix, basis, orc.SLP, 3)
+    K = oracle_h2(g, mesh, prefix, basis, orc.DLP, 3)
+    assert relerr(V.export(0), g[f"{prefix}_Vrow_V"]) < 1e-12
+    assert relerr(V.export(1), g[f"{prefix}_Vrow_E"]) < 1e-12
+    assert relerr(K.export(2), g[f"{prefix}_Kcol_V"]) < 1e-12
+    assert relerr(K.export(3), g[f"{prefix}_Kcol_E"]) < 1e-12
+    assert relerr(V.export(4, 24), g[f"{prefix}_Vparts_S"]) < 1e-12
+    assert relerr(V.export(5, 24), g[f"{prefix}_Vparts_N"]) < 1e-12
+    assert relerr(K.export(5, 24), g[f"{prefix}_Kparts_N"]) < 1e-12
+    x = g[f"{prefix}_x"]
+    y = V.addeval(1.0, x, np.zeros(V.rows))
+    assert relerr(y, g[f"{prefix}_ySLP"]) < 1e-12
+    y = K.addeval(1.0, x, np.zeros(K.rows))
+    assert relerr(y, g[f"{prefix}_yDLP"]) < 1e-12
+
+
+def test_dirichlet_solve_small(gold):
+    """Interior Dirichlet problem V u = (K + M/2) g_D on the sphere refined x8, GMRES(50) to
+    1e-8: same iteration count as the reference, same solution and L2 error."""
+    g = gold("h2small")
+    mesh = mesh_from(gold("sphere8"), "sphere8")
+    V = oracle_h2(g, mesh, "h2ll", L, orc.SLP, 3)
+    K = oracle_h2(g, mesh, "h2ll", L, orc.DLP, 3)
+    z = (1.2, 1.2, 1.2)
+    gD = orc.project_l2_harmonic(mesh, z)
+    assert relerr(gD, g["h2ll_gD"]) < 1e-12
+    b = K.addeval(1.0, gD, np.zeros(K.rows))
+    assert relerr(b, g["h2ll_b"]) < 1e-12
+    u = np.zeros(V.rows)
+    it = orc.gmres([V], [1.0], b, u, 1e-8, 1000, 50)
+    assert it == int(g["h2ll_gmres_iter"][0])
+    assert relerr(u, g["h2ll_u"]) < 1e-9
+    err, nrm = orc.l2_error_harmonic(mesh, z, u)
+    assert abs(err - g["h2ll_l2err"][0]) < 1e-9 * g["h2ll_l2norm"][0]
+    assert abs(nrm - g["h2ll_l2norm"][0]) < 1e-12
+
+
+def test_helmholtz_h2_matvec(gold):
+    g = gold("helm_h2small")
+    mesh = mesh_from(gold("sphere8"), "sphere8")
+    V = oracle_h2(g, mesh, "hh2", C, orc.SLP, 3, pde=orc.HELMHOLTZ, k=2.0)
+    K = oracle_h2(g, mesh, "hh2", C, orc.DLP, 3, pde=orc.HELMHOLTZ, k=2.0)
+    assert relerr(V.export(0), g["hh2_Vrow_V"]) < 1e-12
+    assert relerr(K.export(2), g["hh2_Kcol_V"]) < 1e-12
+    assert relerr(V.export(4, 24), g["hh2_Vparts_S"]) < 1e-12
+    x = np.ascontiguousarray(g["hh2_x"])
+    y = V.addeval(1.0, x, np.zeros(2 * V.rows)).view(np.complex128)
+    assert relerr(y, g["hh2_ySLP"]) < 1e-12
+    y = K.addeval(1.0, x, np.zeros(2 * K.rows)).view(np.complex128)
+    assert relerr(y, g["hh2_yDLP"]) < 1e-12
