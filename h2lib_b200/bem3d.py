@@ -61,7 +61,10 @@ class Surface3d:
 
     def __del__(self):
         if getattr(self, "_dev", None):
-            lib.h2b_surface_del(self._dev)
+            try:
+                lib.h2b_surface_del(self._dev)
+            except Exception:  # interpreter shutdown
+                pass
             self._dev = None
 
 
@@ -113,7 +116,10 @@ class Bem3d:
 
     def __del__(self):
         if getattr(self, "handle", None):
-            lib.h2b_bem_del(self.handle)
+            try:
+                lib.h2b_bem_del(self.handle)
+            except Exception:  # interpreter shutdown
+                pass
             self.handle = None
 
 
@@ -193,7 +199,10 @@ class Tree:
 
     def __del__(self):
         if getattr(self, "handle", None):
-            lib.h2b_tree_del(self.handle)
+            try:
+                lib.h2b_tree_del(self.handle)
+            except Exception:  # interpreter shutdown
+                pass
             self.handle = None
 
 
@@ -236,7 +245,10 @@ class H2Matrix:
 
     def __del__(self):
         if getattr(self, "handle", None):
-            lib.h2b_h2matrix_del(self.handle)
+            try:
+                lib.h2b_h2matrix_del(self.handle)
+            except Exception:  # interpreter shutdown
+                pass
             self.handle = None
 
 

@@ -1,0 +1,536 @@
+// C-ABI implementation: H2 matrices (structure upload, assembly, export, matvec).
+#include <cuda_runtime.h>
+#include <math.h>
+#include <string.h>
+
+#include <algorithm>
+#include <vector>
+
+#include "api_h2.h"
+
+// ------------------------------------------------------------------------------------------
+// helpers
+// ------------------------------------------------------------------------------------------
+
+template <typename T>
+static int upload(T **dst, const std::vector<T> &src, cudaStream_t st) {
+  *dst = nullptr;
+  if (src.empty()) return H2B_OK;
+  H2B_CUDA_TRY(cudaMalloc((void **) dst, sizeof(T) * src.size()));
+  H2B_CUDA_TRY(cudaMemcpyAsync(*dst, src.data(), sizeof(T) * src.size(), cudaMemcpyHostToDevice,
+                               st));
+  return H2B_OK;
+}
+
+template <typename T>
+static void dfree(T *&p) {
+  if (p) cudaFree((void *) p);
+  p = nullptr;
+}
+
+// Chebyshev nodes cos(pi (2i+1)/(2m)) (setup_interpolation_bem3d, Library/bem3d.c:4978) mapped to
+// the box [a, b] of each axis, widened by 5e-3 on both sides when narrower than 5e-3
+// (assemble_interpoints3d_realavector, Library/bem3d.c:5236).
+static void box_points(const double *bmin, const double *bmax, uint32_t m, double *out) {
+  const double e = 1.0 / (2.0 * m);
+  for (int d = 0; d < 3; d++) {
+    double a = bmin[d], b = bmax[d];
+    if (b - a < 5.0e-3) {
+      b += 5.0e-3;
+      a -= 5.0e-3;
+    }
+    const double c = (b + a) * 0.5, h = (b - a) * 0.5;
+    for (uint32_t i = 0; i < m; i++) out[d * m + i] = c + h * cos(M_PI * (2.0 * i * e + e));
+  }
+}
+
+static void devtree_free(DevCTree &t) {
+  dfree(t.d_off); dfree(t.d_size); dfree(t.d_father); dfree(t.d_son0); dfree(t.d_son1);
+  dfree(t.d_idx); dfree(t.d_leaves); dfree(t.d_nonroot); dfree(t.d_levels); dfree(t.d_voff);
+  dfree(t.d_pts); dfree(t.d_V); dfree(t.d_E); dfree(t.d_counter); dfree(t.d_refs);
+  dfree(t.d_tr_off); dfree(t.d_tr_len);
+}
+
+static int devtree_build(DevCTree &t, const h2b_ctree &c, int basis, uint32_t m, uint32_t k,
+                         h2b_adjacency *adj, cudaStream_t st) {
+  t.n = c.n;
+  t.nidx = c.nidx;
+  t.depth = c.depth;
+  std::vector<uint32_t> leaves, nonroot;
+  std::vector<uint64_t> voff(c.n, 0);
+  std::vector<double> pts((size_t) c.n * 3 * m);
+  uint64_t vtot = 0;
+  t.max_rows = 0;
+  for (uint32_t i = 0; i < c.n; i++) {
+    if (c.sons[i] == 0) {
+      leaves.push_back(i);
+      voff[i] = vtot;
+      vtot += (uint64_t) c.size[i] * k;
+      t.max_rows = std::max(t.max_rows, c.size[i]);
+    }
+    if (i > 0) nonroot.push_back(i);
+    box_points(c.bmin + 3 * (size_t) i, c.bmax + 3 * (size_t) i, m, pts.data() + (size_t) i * 3 * m);
+  }
+  t.vtotal = vtot;
+  t.nleaves = (uint32_t) leaves.size();
+  t.leaves = leaves;
+  // clusters by level
+  std::vector<std::vector<uint32_t>> bylevel(c.depth);
+  for (uint32_t i = 0; i < c.n; i++) bylevel[c.level[i]].push_back(i);
+  std::vector<uint32_t> levels;
+  t.level_start.assign(c.depth + 1, 0);
+  for (uint32_t l = 0; l < c.depth; l++) {
+    t.level_start[l] = (uint32_t) levels.size();
+    levels.insert(levels.end(), bylevel[l].begin(), bylevel[l].end());
+  }
+  t.level_start[c.depth] = (uint32_t) levels.size();
+  // triangle lists of the leaves (basis assembly)
+  h2b_nearplan tmp;
+  h2b_nearplan_init(&tmp);
+  std::vector<uint32_t> tr_off(leaves.size()), tr_len(leaves.size());
+  for (size_t i = 0; i < leaves.size(); i++) {
+    const uint32_t cl = leaves[i];
+    if (h2b_nearplan_add_reflist(&tmp, adj, basis == H2B_BASIS_LINEAR, c.idx + c.off[cl],
+                                 c.size[cl], &tr_off[i], &tr_len[i]) != H2B_OK) {
+      h2b_nearplan_free(&tmp);
+      h2b_set_error("h2matrix: out of host memory");
+      return H2B_ERR_NOMEM;
+    }
+  }
+  std::vector<TriRef> refs(tmp.nrefs);
+  memcpy(refs.data(), tmp.refs, sizeof(TriRef) * tmp.nrefs);
+  h2b_nearplan_free(&tmp);
+
+  std::vector<uint32_t> off(c.off, c.off + c.n), size(c.size, c.size + c.n),
+      father(c.father, c.father + c.n), son0(c.son0, c.son0 + c.n), son1(c.son1, c.son1 + c.n),
+      idx(c.idx, c.idx + c.nidx);
+  int rc;
+  if ((rc = upload(&t.d_off, off, st)) || (rc = upload(&t.d_size, size, st)) ||
+      (rc = upload(&t.d_father, father, st)) || (rc = upload(&t.d_son0, son0, st)) ||
+      (rc = upload(&t.d_son1, son1, st)) || (rc = upload(&t.d_idx, idx, st)) ||
+      (rc = upload(&t.d_leaves, leaves, st)) || (rc = upload(&t.d_nonroot, nonroot, st)) ||
+      (rc = upload(&t.d_levels, levels, st)) || (rc = upload(&t.d_voff, voff, st)) ||
+      (rc = upload(&t.d_pts, pts, st)) || (rc = upload(&t.d_refs, refs, st)) ||
+      (rc = upload(&t.d_tr_off, tr_off, st)) || (rc = upload(&t.d_tr_len, tr_len, st)))
+    return rc;
+  H2B_CUDA_TRY(cudaMalloc(&t.d_V, sizeof(double) * std::max<uint64_t>(vtot, 1)));
+  H2B_CUDA_TRY(cudaMalloc(&t.d_E, sizeof(double) * std::max<uint64_t>((uint64_t) (c.n - 1) * k * k, 1)));
+  H2B_CUDA_TRY(cudaMalloc(&t.d_counter, sizeof(unsigned) * c.n));
+  H2B_CUDA_TRY(cudaMemsetAsync(t.d_counter, 0, sizeof(unsigned) * c.n, st));
+  return H2B_OK;
+}
+
+// ------------------------------------------------------------------------------------------
+// construction
+// ------------------------------------------------------------------------------------------
+
+extern "C" void h2b_h2matrix_del(h2b_h2matrix *h) {
+  if (!h) return;
+  if (h->st) cudaStreamSynchronize(h->st);
+  devtree_free(h->rt);
+  devtree_free(h->ct);
+  dfree(h->d_adm_rc); dfree(h->d_adm_cc); dfree(h->d_S);
+  dfree(h->d_near_rc); dfree(h->d_near_cc); dfree(h->d_near_off); dfree(h->d_N);
+  dfree(h->d_tiles); dfree(h->d_refs); dfree(h->d_sing);
+  dfree(h->d_xp); dfree(h->d_yp); dfree(h->d_xt); dfree(h->d_yt);
+  dfree(h->d_xs); dfree(h->d_ys); dfree(h->d_ws); dfree(h->d_wsl);
+  dfree(h->d_xio); dfree(h->d_yio);
+  if (h->st) cudaStreamDestroy(h->st);
+  delete h;
+}
+
+extern "C" h2b_h2matrix *h2b_h2matrix_new(const h2b_bem *bem, const h2b_tree *tree, uint32_t m) {
+  if (!bem || !tree) {
+    h2b_set_error("h2b_h2matrix_new: NULL operator or tree");
+    return NULL;
+  }
+  if (m < 1 || m > 5) {
+    h2b_set_error("h2b_h2matrix_new: interpolation order %u outside 1..5", m);
+    return NULL;
+  }
+  const uint32_t nr = h2b_bem_rows(bem), nc = h2b_bem_cols(bem);
+  if (tree->row.nidx != nr || tree->col.nidx != nc) {
+    h2b_set_error("h2b_h2matrix_new: tree index sets (%u, %u) do not match the operator (%u, %u)",
+                  tree->row.nidx, tree->col.nidx, nr, nc);
+    return NULL;
+  }
+  if (h2b_ensure_device() != H2B_OK) return NULL;
+  h2b_h2matrix *h = new h2b_h2matrix();
+  h->bem = bem;
+  h->tree = tree;
+  h->m = m;
+  h->k = m * m * m;
+  h->cx = bem->pde == H2B_HELMHOLTZ;
+  h->num_sms = bem->s->num_sms;
+  int rc = H2B_OK;
+  if (cudaStreamCreateWithFlags(&h->st, cudaStreamNonBlocking) != cudaSuccess) {
+    h2b_set_error("h2b_h2matrix_new: %s", cudaGetErrorString(cudaGetLastError()));
+    delete h;
+    return NULL;
+  }
+  h2b_adjacency *adj = const_cast<h2b_adjacency *>(&bem->s->adj);
+  rc = devtree_build(h->rt, tree->row, bem->row_basis, m, h->k, adj, h->st);
+  if (rc == H2B_OK) rc = devtree_build(h->ct, tree->col, bem->col_basis, m, h->k, adj, h->st);
+
+  // blocks
+  std::vector<uint32_t> arc, acc, nrc, ncc;
+  std::vector<uint64_t> noff;
+  uint64_t ntot = 0;
+  h2b_nearplan plan;
+  h2b_nearplan_init(&plan);
+  for (uint32_t b = 0; rc == H2B_OK && b < tree->blocks.n; b++) {
+    const uint32_t r = tree->blocks.rc[b], c = tree->blocks.cc[b];
+    if (tree->blocks.adm[b]) {
+      arc.push_back(r);
+      acc.push_back(c);
+    } else {
+      nrc.push_back(r);
+      ncc.push_back(c);
+      noff.push_back(ntot);
+      const uint32_t rows = tree->row.size[r], cols = tree->col.size[c];
+      rc = h2b_nearplan_add_block(&plan, adj, bem->row_basis, bem->col_basis,
+                                  tree->row.idx + tree->row.off[r], rows,
+                                  tree->col.idx + tree->col.off[c], cols, ntot, rows, 0, 64);
+      ntot += (uint64_t) rows * cols;
+    }
+  }
+  if (rc == H2B_OK) rc = h2b_nearplan_finalize(&plan);
+  h->nadm = (uint32_t) arc.size();
+  h->nnear = (uint32_t) nrc.size();
+  h->near_total = ntot;
+  h->ntiles = plan.ntiles;
+  h->nsing = plan.nsing;
+  if (rc == H2B_OK) {
+    const size_t W = h->cx ? 2 : 1;
+    std::vector<h2b_tile> tiles(plan.tiles, plan.tiles + plan.ntiles);
+    std::vector<h2b_triref> refs(plan.refs, plan.refs + plan.nrefs);
+    std::vector<h2b_sing> sing(plan.sing, plan.sing + plan.nsing);
+    if ((rc = upload(&h->d_adm_rc, arc, h->st)) || (rc = upload(&h->d_adm_cc, acc, h->st)) ||
+        (rc = upload(&h->d_near_rc, nrc, h->st)) || (rc = upload(&h->d_near_cc, ncc, h->st)) ||
+        (rc = upload(&h->d_near_off, noff, h->st)) || (rc = upload(&h->d_tiles, tiles, h->st)) ||
+        (rc = upload(&h->d_refs, refs, h->st)) || (rc = upload(&h->d_sing, sing, h->st))) {
+    } else if (cudaMalloc(&h->d_S, sizeof(double) * W * std::max<uint64_t>((uint64_t) h->nadm * h->k * h->k, 1)) != cudaSuccess ||
+               cudaMalloc(&h->d_N, sizeof(double) * W * std::max<uint64_t>(ntot, 1)) != cudaSuccess ||
+               cudaMalloc(&h->d_xp, sizeof(double) * W * nc) != cudaSuccess ||
+               cudaMalloc(&h->d_yp, sizeof(double) * W * nr) != cudaSuccess ||
+               cudaMalloc(&h->d_xt, sizeof(double) * W * h->k * tree->col.n) != cudaSuccess ||
+               cudaMalloc(&h->d_yt, sizeof(double) * W * h->k * tree->row.n) != cudaSuccess ||
+               cudaMalloc(&h->d_xio, sizeof(double) * W * nc) != cudaSuccess ||
+               cudaMalloc(&h->d_yio, sizeof(double) * W * nr) != cudaSuccess) {
+      h2b_set_error("h2b_h2matrix_new: device allocation failed: %s",
+                    cudaGetErrorString(cudaGetLastError()));
+      rc = H2B_ERR_NOMEM;
+    }
+  }
+  h2b_nearplan_free(&plan);
+  // single-triangle rule (raw and linear-basis weighted)
+  if (rc == H2B_OK) {
+    const h2b_quad &qd = bem->quad;
+    std::vector<double> xs(qd.xs, qd.xs + qd.ns), ys(qd.ys, qd.ys + qd.ns),
+        ws(qd.ws + 3 * qd.ns, qd.ws + 4 * qd.ns), wsl(qd.ws, qd.ws + 3 * qd.ns);
+    h->ns = qd.ns;
+    if ((rc = upload(&h->d_xs, xs, h->st)) || (rc = upload(&h->d_ys, ys, h->st)) ||
+        (rc = upload(&h->d_ws, ws, h->st)) || (rc = upload(&h->d_wsl, wsl, h->st))) {
+    }
+  }
+  if (rc == H2B_OK && cudaStreamSynchronize(h->st) != cudaSuccess) {
+    h2b_set_error("h2b_h2matrix_new: %s", cudaGetErrorString(cudaGetLastError()));
+    rc = H2B_ERR_CUDA;
+  }
+  if (rc != H2B_OK) {
+    h2b_h2matrix_del(h);
+    return NULL;
+  }
+  h2b_h2_fill_mvm_plan(h);
+  return h;
+}
+
+void h2b_h2_fill_mvm_plan(h2b_h2matrix *h) {
+  MvmPlan &p = h->mvm;
+  memset(&p, 0, sizeof(p));
+  p.cx = h->cx;
+  p.num_sms = h->num_sms;
+  p.k = (int) h->k;
+  p.nrow = h->rt.nidx;
+  p.ncol = h->ct.nidx;
+  p.nrow_clusters = h->rt.n;
+  p.ridx = h->rt.d_idx;
+  p.cidx = h->ct.d_idx;
+  p.xp = h->d_xp;
+  p.yp = h->d_yp;
+  p.xt = h->d_xt;
+  p.yt = h->d_yt;
+  p.fwd = MvmForwardArgs{h->ct.d_leaves, h->ct.d_father, h->ct.d_son0, h->ct.d_son1,
+                         h->ct.d_size, h->ct.d_off, h->ct.d_voff, h->ct.d_V, h->ct.d_E, h->d_xp,
+                         h->d_xt, h->ct.d_counter, h->ct.nleaves, (int) h->k};
+  p.cpl = MvmCoupleArgs{h->d_adm_rc, h->d_adm_cc, h->d_S, h->d_near_rc, h->d_near_cc,
+                        h->d_near_off, h->d_N, h->rt.d_size, h->ct.d_size, h->rt.d_off,
+                        h->ct.d_off, h->d_xt, h->d_xp, h->d_yt, h->d_yp, h->nadm, h->nnear,
+                        (int) h->k};
+  p.down = MvmDownArgs{nullptr, h->rt.d_father, h->rt.d_E, h->d_yt, (int) h->k};
+  p.bwd = MvmBackArgs{h->rt.d_leaves, h->rt.d_size, h->rt.d_off, h->rt.d_voff, h->rt.d_V,
+                      h->d_yt, h->d_yp, h->rt.nleaves, (int) h->k};
+  p.level_list = h->rt.d_levels;
+  p.rdepth = std::min<uint32_t>(h->rt.depth, 64);
+  for (uint32_t l = 0; l <= p.rdepth; l++) p.level_start[l] = h->rt.level_start[l];
+}
+
+// ------------------------------------------------------------------------------------------
+// assembly
+// ------------------------------------------------------------------------------------------
+
+static int assemble_basis(h2b_h2matrix *h, DevCTree &t, int basis, int dn) {
+  FarLeafArgs la;
+  la.tri = h->bem->s->d_tri;
+  la.refs = t.d_refs;
+  la.leaves = t.d_leaves;
+  la.tr_off = t.d_tr_off;
+  la.tr_len = t.d_tr_len;
+  la.size = t.d_size;
+  la.voff = t.d_voff;
+  la.pts = t.d_pts;
+  la.xs = h->d_xs;
+  la.ys = h->d_ys;
+  la.ws = h->d_ws;
+  la.wsl = h->d_wsl;
+  la.V = t.d_V;
+  la.nleaves = t.nleaves;
+  la.max_rows = t.max_rows;
+  la.m = (int) h->m;
+  la.k = (int) h->k;
+  la.ns = (int) h->ns;
+  int rc = h2b_far_leaf_basis(&la, basis == H2B_BASIS_LINEAR, dn, h->st);
+  if (rc != H2B_OK) return rc;
+  FarTransferArgs ta{t.d_nonroot, t.d_father, t.d_pts, t.d_E, t.n - 1, (int) h->m, (int) h->k};
+  return h2b_far_transfer(&ta, h->st);
+}
+
+static int finish(h2b_h2matrix *h, int rc) {
+  if (rc != H2B_OK) return rc;
+  if (cudaStreamSynchronize(h->st) != cudaSuccess) {
+    h2b_set_error("h2matrix: %s", cudaGetErrorString(cudaGetLastError()));
+    return H2B_ERR_CUDA;
+  }
+  return H2B_OK;
+}
+
+extern "C" int h2b_h2matrix_assemble_row_clusterbasis(h2b_h2matrix *h) {
+  if (!h) return H2B_ERR_ARG;
+  // row side: Lagrange polynomials (assemble_bem3d_lagrange_{c,l}_amatrix)
+  return finish(h, assemble_basis(h, h->rt, h->bem->row_basis, 0));
+}
+
+extern "C" int h2b_h2matrix_assemble_col_clusterbasis(h2b_h2matrix *h) {
+  if (!h) return H2B_ERR_ARG;
+  // column side of the double layer: normal derivatives (assemble_bem3d_dn_lagrange_*)
+  return finish(h, assemble_basis(h, h->ct, h->bem->col_basis, h->bem->layer == H2B_DLP));
+}
+
+extern "C" int h2b_h2matrix_assemble_farfield(h2b_h2matrix *h) {
+  if (!h) return H2B_ERR_ARG;
+  FarCouplingArgs ca{h->d_adm_rc, h->d_adm_cc, h->rt.d_pts, h->ct.d_pts, h->d_S, h->nadm,
+                     (int) h->m, (int) h->k, h->bem->kconst, h->bem->k_re, -h->bem->k_im};
+  return finish(h, h2b_far_coupling(&ca, h->cx, h->st));
+}
+
+static int launch_near(h2b_h2matrix *h, h2b_h2matrix *h2) {
+  h2b_near_launch L;
+  h2b_fill_launch(h->bem, &L);
+  L.refs = h->d_refs;
+  L.tiles = h->d_tiles;
+  L.ntiles = h->ntiles;
+  L.sing = h->d_sing;
+  L.nsing = h->nsing;
+  L.out0 = h->d_N;
+  if (h2) {
+    L.kk = H2B_KK_LBOTH;
+    L.out1 = h2->d_N;
+    L.alpha_re = h2->bem->alpha_re;
+    L.alpha_im = h2->bem->alpha_im;
+  }
+  int rc = h2b_near_launch_kernels(&L, h->st);
+  if (rc == H2B_OK) rc = h2b_check_err_flag(h->bem, h->st);
+  return rc;
+}
+
+extern "C" int h2b_h2matrix_assemble_nearfield(h2b_h2matrix *h) {
+  if (!h) return H2B_ERR_ARG;
+  return finish(h, launch_near(h, nullptr));
+}
+
+extern "C" int h2b_h2matrix_assemble_nearfield_pair(h2b_h2matrix *a, h2b_h2matrix *b) {
+  if (!a || !b) return H2B_ERR_ARG;
+  const h2b_bem *A = a->bem, *B = b->bem;
+  if (a->tree != b->tree || A->s != B->s || A->pde != H2B_LAPLACE || B->pde != H2B_LAPLACE ||
+      A->layer != H2B_SLP || B->layer != H2B_DLP || A->row_basis != B->row_basis ||
+      A->col_basis != B->col_basis || A->q != B->q || A->q2 != B->q2) {
+    h2b_set_error("h2b_h2matrix_assemble_nearfield_pair: needs a Laplace SLP and DLP pair on the "
+                  "same tree, surface, bases and quadrature orders");
+    return H2B_ERR_ARG;
+  }
+  cudaEvent_t ev;
+  H2B_CUDA_TRY(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+  // b's storage must be idle before a's stream writes it
+  cudaEventRecord(ev, b->st);
+  cudaStreamWaitEvent(a->st, ev, 0);
+  int rc = finish(a, launch_near(a, b));
+  cudaEventDestroy(ev);
+  return rc;
+}
+
+extern "C" int h2b_h2matrix_assemble(h2b_h2matrix *h) {
+  if (!h) return H2B_ERR_ARG;
+  int rc = h2b_h2matrix_assemble_farfield(h);
+  if (rc == H2B_OK) rc = h2b_h2matrix_assemble_nearfield(h);
+  return rc;
+}
+
+extern "C" int h2b_h2matrix_assemble_all(h2b_h2matrix *h) {
+  if (!h) return H2B_ERR_ARG;
+  int rc = assemble_basis(h, h->rt, h->bem->row_basis, 0);
+  if (rc == H2B_OK) rc = assemble_basis(h, h->ct, h->bem->col_basis, h->bem->layer == H2B_DLP);
+  if (rc == H2B_OK) {
+    FarCouplingArgs ca{h->d_adm_rc, h->d_adm_cc, h->rt.d_pts, h->ct.d_pts, h->d_S, h->nadm,
+                       (int) h->m, (int) h->k, h->bem->kconst, h->bem->k_re, -h->bem->k_im};
+    rc = h2b_far_coupling(&ca, h->cx, h->st);
+  }
+  if (rc == H2B_OK) rc = launch_near(h, nullptr);
+  return finish(h, rc);
+}
+
+// ------------------------------------------------------------------------------------------
+// inspection
+// ------------------------------------------------------------------------------------------
+
+extern "C" int h2b_h2matrix_info(const h2b_h2matrix *h, uint64_t info[8]) {
+  if (!h || !info) return H2B_ERR_ARG;
+  const uint64_t W = h->cx ? 2 : 1;
+  info[0] = h->near_total;
+  info[1] = (uint64_t) h->nadm * h->k * h->k;
+  info[2] = h->rt.vtotal + h->ct.vtotal;
+  info[3] = (uint64_t) (h->rt.n - 1 + h->ct.n - 1) * h->k * h->k;
+  info[4] = 8 * (W * (info[0] + info[1]) + info[2] + info[3]);
+  info[5] = h->nadm;
+  info[6] = h->nnear;
+  info[7] = h->k;
+  return H2B_OK;
+}
+
+extern "C" int h2b_h2matrix_export(const h2b_h2matrix *h, int part, uint32_t count, double *out,
+                                   uint64_t *ndoubles) {
+  if (!h || !ndoubles) return H2B_ERR_ARG;
+  const uint64_t W = h->cx ? 2 : 1, kk = (uint64_t) h->k * h->k;
+  const double *src = nullptr;
+  uint64_t n = 0;
+  switch (part) {
+    case 0:
+    case 2: {
+      const DevCTree &t = part == 0 ? h->rt : h->ct;
+      const h2b_ctree &c = part == 0 ? h->tree->row : h->tree->col;
+      uint32_t got = 0;
+      for (uint32_t i = 0; i < c.n && got < count; i++)
+        if (c.sons[i] == 0) {
+          n += (uint64_t) c.size[i] * h->k;
+          got++;
+        }
+      src = t.d_V;
+      break;
+    }
+    case 1:
+    case 3: {
+      const DevCTree &t = part == 1 ? h->rt : h->ct;
+      n = (uint64_t) std::min<uint32_t>(count, t.n - 1) * kk;
+      src = t.d_E;
+      break;
+    }
+    case 4:
+      n = (uint64_t) std::min<uint32_t>(count, h->nadm) * kk * W;
+      src = h->d_S;
+      break;
+    case 5: {
+      const uint32_t nb = std::min<uint32_t>(count, h->nnear);
+      uint64_t e = 0;
+      for (uint32_t b = 0, j = 0; b < h->tree->blocks.n && j < nb; b++)
+        if (!h->tree->blocks.adm[b]) {
+          e += (uint64_t) h->tree->row.size[h->tree->blocks.rc[b]] *
+               h->tree->col.size[h->tree->blocks.cc[b]];
+          j++;
+        }
+      n = e * W;
+      src = h->d_N;
+      break;
+    }
+    default:
+      h2b_set_error("h2b_h2matrix_export: part %d outside 0..5", part);
+      return H2B_ERR_ARG;
+  }
+  *ndoubles = n;
+  if (out && n) {
+    H2B_CUDA_TRY(cudaMemcpyAsync(out, src, sizeof(double) * n, cudaMemcpyDeviceToHost, h->st));
+    H2B_CUDA_TRY(cudaStreamSynchronize(h->st));
+  }
+  return H2B_OK;
+}
+
+// ------------------------------------------------------------------------------------------
+// matvec
+// ------------------------------------------------------------------------------------------
+
+int h2b_h2_addeval_dev(const h2b_h2matrix *h, double ar, double ai, const double *dx, double *dy,
+                       cudaStream_t st) {
+  return h2b_mvm_launch(&h->mvm, dx, dy, ar, ai, st);
+}
+
+extern "C" int h2b_h2matrix_addeval_multi(double alpha_re, double alpha_im,
+                                          const h2b_h2matrix *h, uint32_t nrhs, const double *X,
+                                          uint64_t ldx, double *Y, uint64_t ldy) {
+  if (!h || !X || !Y) {
+    h2b_set_error("h2b_h2matrix_addeval_multi: NULL argument");
+    return H2B_ERR_ARG;
+  }
+  if (ldx < h->ct.nidx || ldy < h->rt.nidx) {
+    h2b_set_error("h2b_h2matrix_addeval_multi: leading dimensions too small");
+    return H2B_ERR_ARG;
+  }
+  const size_t W = h->cx ? 2 : 1;
+  for (uint32_t r = 0; r < nrhs; r++) {
+    int rc = h2b_h2matrix_addeval(alpha_re, alpha_im, h, X + W * ldx * r, Y + W * ldy * r);
+    if (rc != H2B_OK) return rc;
+  }
+  return H2B_OK;
+}
+
+extern "C" int h2b_h2matrix_addeval(double alpha_re, double alpha_im, const h2b_h2matrix *h,
+                                    const double *x, double *y) {
+  if (!h || !x || !y) {
+    h2b_set_error("h2b_h2matrix_addeval: NULL argument");
+    return H2B_ERR_ARG;
+  }
+  const size_t W = h->cx ? 2 : 1;
+  const bool dx = h2b_is_device_ptr(x), dy = h2b_is_device_ptr(y);
+  const double *xd = x;
+  double *yd = y;
+  if (!dx) {
+    H2B_CUDA_TRY(cudaMemcpyAsync(h->d_xio, x, sizeof(double) * W * h->ct.nidx,
+                                 cudaMemcpyHostToDevice, h->st));
+    xd = h->d_xio;
+  }
+  if (!dy) {
+    H2B_CUDA_TRY(cudaMemcpyAsync(h->d_yio, y, sizeof(double) * W * h->rt.nidx,
+                                 cudaMemcpyHostToDevice, h->st));
+    yd = h->d_yio;
+  }
+  int rc = h2b_h2_addeval_dev(h, alpha_re, alpha_im, xd, yd, h->st);
+  if (rc == H2B_OK && !dy) {
+    if (cudaMemcpyAsync(y, yd, sizeof(double) * W * h->rt.nidx, cudaMemcpyDeviceToHost,
+                        h->st) != cudaSuccess) {
+      h2b_set_error("h2b_h2matrix_addeval: %s", cudaGetErrorString(cudaGetLastError()));
+      rc = H2B_ERR_CUDA;
+    }
+  }
+  if (rc == H2B_OK && cudaStreamSynchronize(h->st) != cudaSuccess) {
+    h2b_set_error("h2b_h2matrix_addeval: %s", cudaGetErrorString(cudaGetLastError()));
+    rc = H2B_ERR_CUDA;
+  }
+  return rc;
+}

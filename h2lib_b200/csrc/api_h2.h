@@ -1,0 +1,53 @@
+// H2 matrix handle layout shared by api_h2.cu and api_solve.cu.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <vector>
+
+#include "api_internal.h"
+#include "farfield.h"
+#include "h2b200_tree.h"
+#include "h2mvm.h"
+
+struct DevCTree {
+  uint32_t n = 0, nidx = 0, depth = 0, nleaves = 0, max_rows = 0;
+  uint64_t vtotal = 0;
+  uint32_t *d_off = nullptr, *d_size = nullptr, *d_father = nullptr, *d_son0 = nullptr,
+           *d_son1 = nullptr, *d_idx = nullptr, *d_leaves = nullptr, *d_nonroot = nullptr,
+           *d_levels = nullptr;
+  uint64_t *d_voff = nullptr;
+  double *d_pts = nullptr, *d_V = nullptr, *d_E = nullptr;
+  unsigned *d_counter = nullptr;
+  TriRef *d_refs = nullptr;
+  uint32_t *d_tr_off = nullptr, *d_tr_len = nullptr;
+  std::vector<uint32_t> leaves, level_start;
+};
+
+struct h2b_h2matrix {
+  const h2b_bem *bem = nullptr;
+  const h2b_tree *tree = nullptr;
+  uint32_t m = 0, k = 0, ns = 0;
+  int cx = 0, num_sms = 148;
+  cudaStream_t st = nullptr;
+  DevCTree rt, ct;
+  uint32_t nadm = 0, nnear = 0, ntiles = 0, nsing = 0;
+  uint64_t near_total = 0;
+  uint32_t *d_adm_rc = nullptr, *d_adm_cc = nullptr;
+  double *d_S = nullptr;
+  uint32_t *d_near_rc = nullptr, *d_near_cc = nullptr;
+  uint64_t *d_near_off = nullptr;
+  double *d_N = nullptr;
+  h2b_tile *d_tiles = nullptr;
+  h2b_triref *d_refs = nullptr;
+  h2b_sing *d_sing = nullptr;
+  double *d_xp = nullptr, *d_yp = nullptr, *d_xt = nullptr, *d_yt = nullptr;
+  double *d_xio = nullptr, *d_yio = nullptr;  // staging of host vectors
+  double *d_xs = nullptr, *d_ys = nullptr, *d_ws = nullptr, *d_wsl = nullptr;
+  MvmPlan mvm;
+};
+
+void h2b_h2_fill_mvm_plan(h2b_h2matrix *h);
+int h2b_h2_addeval_dev(const h2b_h2matrix *h, double ar, double ai, const double *dx, double *dy,
+                       cudaStream_t st);

@@ -1,0 +1,202 @@
+// Farfield fill kernels of the Chebyshev-interpolation H2 matrix (sm_100a, FP64).
+//
+//   leaf bases      V_t[i, nu] = int phi_i L_nu   (or the normal derivative d/dn L_nu for the
+//                   double-layer column basis), q^2-point rule per triangle:
+//                   assemble_bem3d_lagrange_{c,l}_amatrix, Library/bem3d.c:7616/7758 and
+//                   assemble_bem3d_dn_lagrange_{c,l}_amatrix, :8024/8200;
+//   transfers       E_s[i, nu] = L^father_nu(xi^son_i):  assemble_bem3d_lagrange_amatrix, :8497;
+//   coupling        S_b[i, j] = (1/4pi) g(xi^row_i, xi^col_j):  assemble_bem3d_inter_uniform,
+//                   :6079 -> fill_bem3d, :3439.
+// Interpolation points per cluster are the tensor Chebyshev nodes of its bounding box widened to
+// at least 2 * 5e-3 per axis (assemble_interpoints3d_realavector, :5236); the host computes the
+// m one-dimensional nodes per axis and cluster (pts[c][axis][mu]).  The multi-index
+// nu = (jx * m + jy) * m + jz orders the tensor basis as the reference does.
+// The bases are real for both Laplace and (non-directional) Helmholtz; the coupling matrices
+// are complex for Helmholtz.  One CTA per leaf / cluster / admissible block.
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "device_common.cuh"
+#include "farfield.h"
+
+namespace {
+
+constexpr int MMAX = 8;
+
+__device__ __forceinline__ double lagr1(double x, const double *xi, int mu, int m) {
+  double v = 1.0;
+  for (int l = 0; l < m; l++)
+    if (l != mu) v *= (x - xi[l]) / (xi[mu] - xi[l]);
+  return v;
+}
+
+__device__ __forceinline__ double dlagr1(double x, const double *xi, int mu, int m) {
+  double s = 0.0;
+  for (int l = 0; l < m; l++) {
+    if (l == mu) continue;
+    double tmp = 1.0;
+    for (int l2 = 0; l2 < m; l2++)
+      if (l2 != mu && l2 != l) tmp *= (x - xi[l2]) / (xi[mu] - xi[l2]);
+    s += tmp / (xi[mu] - xi[l]);
+  }
+  return s;
+}
+
+// Leaf bases.  Rows of leaf c: its triangles (constant basis) or vertices (linear basis).
+// trl: TriRef list of the triangles touching the cluster (linear basis) with local row indices;
+// for the constant basis the list holds the cluster's own triangles with l[0] = row.
+// Shared memory: the cluster's V block (rows x k doubles) accumulated by atomics, plus the
+// 1D Lagrange values of one triangle batch.
+template <bool LINEAR, bool DN>
+__global__ void __launch_bounds__(256) leaf_basis_kernel(FarLeafArgs a) {
+  extern __shared__ double smem[];
+  const uint32_t leaf = blockIdx.x;
+  const uint32_t c = a.leaves[leaf];
+  const int m = a.m, k = a.k;
+  const uint32_t rows = a.size[c];
+  const uint32_t tr0 = a.tr_off[leaf], ntr = a.tr_len[leaf];
+  const double *px = a.pts + (size_t) c * 3 * m, *py = px + m, *pz = px + 2 * m;
+  double *V = smem;  // rows * k
+  const int ns = a.ns;
+  for (uint32_t e = threadIdx.x; e < rows * (uint32_t) k; e += blockDim.x) V[e] = 0.0;
+  __syncthreads();
+
+  // work item = (triangle, nu)
+  const uint32_t items = ntr * (uint32_t) k;
+  for (uint32_t it = threadIdx.x; it < items; it += blockDim.x) {
+    const uint32_t s = it / (uint32_t) k;
+    const int nu = (int) (it - s * (uint32_t) k);
+    const int jx = nu / (m * m), jy = (nu / m) % m, jz = nu % m;
+    const TriRef r = a.refs[tr0 + s];
+    const TriRec &T = a.tri[r.t];
+    double sum[3] = {0.0, 0.0, 0.0};
+    for (int q = 0; q < ns; q++) {
+      const double tx = a.xs[q], sx = a.ys[q];
+      const double Ax = 1.0 - tx, Bx = tx - sx, Cx = sx;
+      double X[3];
+#pragma unroll
+      for (int d = 0; d < 3; d++) X[d] = T.a[d] * Ax + T.b[d] * Bx + T.c[d] * Cx;
+      double val;
+      if (!DN) {
+        val = lagr1(X[0], px, jx, m) * lagr1(X[1], py, jy, m) * lagr1(X[2], pz, jz, m);
+      } else {
+        const double lx = lagr1(X[0], px, jx, m), ly = lagr1(X[1], py, jy, m),
+                     lz = lagr1(X[2], pz, jz, m);
+        val = T.n[0] * (dlagr1(X[0], px, jx, m) * ly * lz) +
+              T.n[1] * (lx * dlagr1(X[1], py, jy, m) * lz) +
+              T.n[2] * (lx * ly * dlagr1(X[2], pz, jz, m));
+      }
+      if (LINEAR) {
+#pragma unroll
+        for (int l = 0; l < 3; l++) sum[l] += a.wsl[l * ns + q] * val;
+      } else {
+        sum[0] += a.ws[q] * val;
+      }
+    }
+    if (LINEAR) {
+#pragma unroll
+      for (int l = 0; l < 3; l++) {
+        const int row = r.l[l];
+        if (row >= 0) atomicAdd(&V[row + (uint32_t) nu * rows], sum[l] * T.g);
+      }
+    } else {
+      V[r.l[0] + (uint32_t) nu * rows] = T.g * sum[0];
+    }
+  }
+  __syncthreads();
+  double *out = a.V + a.voff[c];
+  for (uint32_t e = threadIdx.x; e < rows * (uint32_t) k; e += blockDim.x) out[e] = V[e];
+}
+
+// Transfer matrix of every non-root cluster: E_c[i, nu] = L^father_nu(xi^c_i), k x k.
+__global__ void __launch_bounds__(256) transfer_kernel(FarTransferArgs a) {
+  const uint32_t c = a.clusters[blockIdx.x];
+  const uint32_t f = a.father[c];
+  const int m = a.m, k = a.k;
+  const double *fp = a.pts + (size_t) f * 3 * m, *sp = a.pts + (size_t) c * 3 * m;
+  __shared__ double L1[3][MMAX][MMAX];  // L1[d][point a][basis mu]
+  for (int e = threadIdx.x; e < 3 * m * m; e += blockDim.x) {
+    const int d = e / (m * m), p = (e / m) % m, mu = e % m;
+    L1[d][p][mu] = lagr1(sp[d * m + p], fp + d * m, mu, m);
+  }
+  __syncthreads();
+  double *E = a.E + (size_t) (c - 1) * k * k;  // clusters 1..n-1 in pre-order
+  for (int e = threadIdx.x; e < k * k; e += blockDim.x) {
+    const int i = e % k, nu = e / k;
+    const int ia = i / (m * m), ib = (i / m) % m, ic = i % m;
+    const int jx = nu / (m * m), jy = (nu / m) % m, jz = nu % m;
+    E[e] = L1[0][ia][jx] * L1[1][ib][jy] * L1[2][ic][jz];
+  }
+}
+
+// Coupling matrices: S_b[i, j] = (1/4pi) g(xi^r_i, xi^c_j).
+template <bool CX>
+__global__ void __launch_bounds__(256) coupling_kernel(FarCouplingArgs a) {
+  const uint32_t b = blockIdx.x;
+  const uint32_t rc = a.rc[b], cc = a.cc[b];
+  const int m = a.m, k = a.k;
+  const double *rp = a.rpts + (size_t) rc * 3 * m, *cp = a.cpts + (size_t) cc * 3 * m;
+  double *S = a.S + (size_t) b * k * k * (CX ? 2 : 1);
+  for (int e = threadIdx.x; e < k * k; e += blockDim.x) {
+    const int i = e % k, j = e / k;
+    const double x0 = rp[i / (m * m)], x1 = rp[m + (i / m) % m], x2 = rp[2 * m + i % m];
+    const double y0 = cp[j / (m * m)], y1 = cp[m + (j / m) % m], y2 = cp[2 * m + j % m];
+    const double d0 = x0 - y0, d1 = x1 - y1, d2 = x2 - y2;
+    const double r2 = d0 * d0 + d1 * d1 + d2 * d2;
+    const double rinv = 1.0 / sqrt(r2);
+    if (!CX) {
+      S[e] = a.kconst * rinv;
+    } else {
+      double r = r2 * rinv, rn = rinv, s, c;
+      if (a.k_imn != 0.0) rn *= exp(a.k_imn * r);
+      sincos(a.k_re * r, &s, &c);
+      S[2 * e] = a.kconst * (rn * c);
+      S[2 * e + 1] = a.kconst * (rn * s);
+    }
+  }
+}
+
+}  // namespace
+
+extern "C" int h2b_far_leaf_basis(const FarLeafArgs *a, int linear, int dn, cudaStream_t st) {
+  if (a->nleaves == 0) return H2B_OK;
+  const size_t smem = sizeof(double) * (size_t) a->max_rows * a->k;
+  if (smem > 200u * 1024u) {
+    h2b_set_error("leaf basis block of %u x %d exceeds shared memory", a->max_rows, a->k);
+    return H2B_ERR_ARG;
+  }
+#define LAUNCH(L, D)                                                                        \
+  do {                                                                                      \
+    H2B_CUDA_TRY(cudaFuncSetAttribute(leaf_basis_kernel<L, D>,                             \
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem)); \
+    leaf_basis_kernel<L, D><<<a->nleaves, 256, smem, st>>>(*a);                             \
+  } while (0)
+  if (linear && dn) LAUNCH(true, true);
+  else if (linear) LAUNCH(true, false);
+  else if (dn) LAUNCH(false, true);
+  else LAUNCH(false, false);
+#undef LAUNCH
+  H2B_CUDA_TRY(cudaGetLastError());
+  return H2B_OK;
+}
+
+extern "C" int h2b_far_transfer(const FarTransferArgs *a, cudaStream_t st) {
+  if (a->n == 0) return H2B_OK;
+  if (a->m > MMAX) {
+    h2b_set_error("interpolation order %d > %d", a->m, MMAX);
+    return H2B_ERR_ARG;
+  }
+  transfer_kernel<<<a->n, 256, 0, st>>>(*a);
+  H2B_CUDA_TRY(cudaGetLastError());
+  return H2B_OK;
+}
+
+extern "C" int h2b_far_coupling(const FarCouplingArgs *a, int cx, cudaStream_t st) {
+  if (a->n == 0) return H2B_OK;
+  if (cx)
+    coupling_kernel<true><<<a->n, 256, 0, st>>>(*a);
+  else
+    coupling_kernel<false><<<a->n, 256, 0, st>>>(*a);
+  H2B_CUDA_TRY(cudaGetLastError());
+  return H2B_OK;
+}

@@ -1,0 +1,45 @@
+// Launch descriptions of the farfield fill kernels (farfield.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "device_common.cuh"
+
+struct FarLeafArgs {
+  const TriRec *tri;
+  const TriRef *refs;       // per leaf: triangles touching it with local rows
+  const uint32_t *leaves;   // leaf cluster ids
+  const uint32_t *tr_off, *tr_len;  // per leaf (index into refs)
+  const uint32_t *size;     // per cluster
+  const uint64_t *voff;     // per cluster: offset of its leaf basis
+  const double *pts;        // per cluster: 3 x m interpolation nodes
+  const double *xs, *ys;    // single-triangle rule (ns points)
+  const double *ws;         // raw weights (ns)
+  const double *wsl;        // linear-basis weighted weights (3 x ns)
+  double *V;
+  uint32_t nleaves, max_rows;
+  int m, k, ns;
+};
+
+struct FarTransferArgs {
+  const uint32_t *clusters;  // non-root cluster ids
+  const uint32_t *father;
+  const double *pts;
+  double *E;                 // (n_clusters - 1) x k x k, cluster c at (c-1)*k*k
+  uint32_t n;
+  int m, k;
+};
+
+struct FarCouplingArgs {
+  const uint32_t *rc, *cc;   // per admissible block
+  const double *rpts, *cpts;
+  double *S;                 // per block k x k (complex: interleaved)
+  uint32_t n;
+  int m, k;
+  double kconst, k_re, k_imn;
+};
+
+extern "C" int h2b_far_leaf_basis(const FarLeafArgs *a, int linear, int dn, cudaStream_t st);
+extern "C" int h2b_far_transfer(const FarTransferArgs *a, cudaStream_t st);
+extern "C" int h2b_far_coupling(const FarCouplingArgs *a, int cx, cudaStream_t st);

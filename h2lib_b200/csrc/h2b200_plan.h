@@ -70,6 +70,10 @@ int h2b_nearplan_add_block(h2b_nearplan *p, h2b_adjacency *adj, int row_basis, i
                            uint32_t cols, uint64_t out_off, uint32_t ld, int ntrans,
                            uint32_t tile);
 int h2b_nearplan_finalize(h2b_nearplan *p);
+/* Triangle list of an index set (linear: triangles touching the vertices, with local rows;
+ * constant: the triangles themselves), appended to p->refs. */
+int h2b_nearplan_add_reflist(h2b_nearplan *p, h2b_adjacency *adj, int linear,
+                             const uint32_t *idx, uint32_t n, uint32_t *off, uint32_t *len);
 uint32_t h2b_pair_code(const uint32_t *tv, const uint32_t *sv);
 
 #ifdef __cplusplus

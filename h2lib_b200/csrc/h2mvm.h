@@ -1,0 +1,68 @@
+// Device layout of an H2 matrix as the matvec kernels read it (h2mvm.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+struct MvmForwardArgs {       // column cluster basis
+  const uint32_t *leaves;     // leaf ids
+  const uint32_t *father, *son0, *son1;
+  const uint32_t *size, *off;
+  const uint64_t *voff;
+  const double *V, *E;
+  const double *xp;
+  double *xt;
+  unsigned *counter;          // per cluster arrival counters (zero between products)
+  uint32_t nleaves;
+  int k;
+};
+
+struct MvmCoupleArgs {
+  const uint32_t *adm_rc, *adm_cc;
+  const double *S;
+  const uint32_t *near_rc, *near_cc;
+  const uint64_t *near_off;
+  const double *N;
+  const uint32_t *rsize, *csize, *roff, *coff;
+  const double *xt, *xp;
+  double *yt, *yp;
+  uint32_t nadm, nnear;
+  int k;
+};
+
+struct MvmDownArgs {          // row cluster basis
+  const uint32_t *clusters;   // clusters of one level
+  const uint32_t *father;
+  const double *E;
+  double *yt;
+  int k;
+};
+
+struct MvmBackArgs {
+  const uint32_t *leaves;
+  const uint32_t *size, *off;
+  const uint64_t *voff;
+  const double *V;
+  const double *yt;
+  double *yp;
+  uint32_t nleaves;
+  int k;
+};
+
+struct MvmPlan {
+  int cx, num_sms;
+  int k;
+  uint32_t nrow, ncol, nrow_clusters;
+  const uint32_t *ridx, *cidx;   // device index arrays of the row / column tree
+  double *xp, *yp, *xt, *yt;     // work vectors
+  MvmForwardArgs fwd;
+  MvmCoupleArgs cpl;
+  MvmDownArgs down;
+  MvmBackArgs bwd;
+  const uint32_t *level_list;    // row-tree clusters sorted by level (device)
+  uint32_t level_start[65];      // host copy of the level offsets
+  uint32_t rdepth;
+};
+
+extern "C" int h2b_mvm_launch(const MvmPlan *p, const double *x, double *y, double ar, double ai,
+                              cudaStream_t st);

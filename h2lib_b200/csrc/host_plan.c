@@ -146,6 +146,13 @@ add_reflist(h2b_nearplan *p, h2b_adjacency *adj, int linear, const uint32_t *idx
   return H2B_OK;
 }
 
+int
+h2b_nearplan_add_reflist(h2b_nearplan *p, h2b_adjacency *adj, int linear, const uint32_t *idx,
+                         uint32_t n, uint32_t *off, uint32_t *len)
+{
+  return add_reflist(p, adj, linear, idx, n, off, len);
+}
+
 /* Vertex permutation of a pair: returns the number of shared vertices and the packed code
  * case | tp0<<2 | tp1<<4 | tp2<<6 | sp0<<8 | sp1<<10 | sp2<<12. */
 uint32_t

@@ -405,17 +405,18 @@ __global__ void __launch_bounds__(256) near_sing_kernel(SingArgs a) {
           }
         }
       }
-      // identity term of linear bases: alpha * mass_{lk} * g on the vertex pairs of the triangle
-      if constexpr (RL && CL) {
+      // identity term of linear bases: alpha * mass * g on the basis functions of the triangle
+      // (ll: 3 x 3 mass matrix; cl / lc: 1/6 per vertex)
+      if constexpr (RL || CL) {
         if (ident && (a.alpha_re != 0.0 || a.alpha_im != 0.0)) {
           double *dst = KT<KK>::NOUT == 2 ? a.out1 : a.out0;
-          for (int l = 0; l < 3; l++)
-            for (int k = 0; k < 3; k++) {
+          for (int l = 0; l < NR; l++)
+            for (int k = 0; k < NC; k++) {
               const int lr = rt.l[l], lc = st.l[k];
               if (lr < 0 || lc < 0) continue;
               const uint64_t o = ntrans ? tl.out_off + lc + (uint64_t) lr * tl.ld
                                         : tl.out_off + lr + (uint64_t) lc * tl.ld;
-              const double m = a.mass[l + 3 * k] * T.g;
+              const double m = (RL && CL ? a.mass[l + 3 * k] : a.mass[RL ? l : k]) * T.g;
               if constexpr (KT<KK>::CPLX) {
                 atomicAdd(&dst[2 * o], m * a.alpha_re);
                 atomicAdd(&dst[2 * o + 1], (ntrans ? -1.0 : 1.0) * m * a.alpha_im);

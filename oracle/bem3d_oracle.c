@@ -457,11 +457,15 @@ op_nearfield(const op_t *o, const uint32_t *ridx, uint32_t rows, const uint32_t 
           else
             put(N, cx, (uint64_t) lr + (uint64_t) lc * ld, v, 1);
         }
-        else if (rl && cl) {
-          for (k = 0; k < 3; k++)
-            for (l = 0; l < 3; l++) {
-              int32_t lr = rloc[o->t[3 * (size_t) tt + l]], lc = cloc[o->t[3 * (size_t) ss + k]];
-              cplx v = o->mass[l + 3 * k] * (o->alpha * o->g[tt]);
+        else {
+          /* mixed bases: mass[i] = 1/6 for the linear side's local function i
+           * (Library/bem3d.c:1936-1963 and the lc counterpart) */
+          for (k = 0; k < (cl ? 3u : 1u); k++)
+            for (l = 0; l < (rl ? 3u : 1u); l++) {
+              int32_t lr = rl ? rloc[o->t[3 * (size_t) tt + l]] : rloc[tt];
+              int32_t lc = cl ? cloc[o->t[3 * (size_t) ss + k]] : cloc[ss];
+              double m = (rl && cl) ? o->mass[l + 3 * k] : o->mass[rl ? l : k];
+              cplx v = m * (o->alpha * o->g[tt]);
               if (lr < 0 || lc < 0) continue;
               if (ntrans)
                 put(N, cx, (uint64_t) lc + (uint64_t) lr * ld, conj(v), 1);

@@ -472,6 +472,8 @@ section_sphere4(void)
   dump_mesh("sphere4", gr);
   dense_pair("s4cc", gr, BASIS_CONSTANT_BEM3D, BASIS_CONSTANT_BEM3D, 0);
   dense_pair("s4ll", gr, BASIS_LINEAR_BEM3D, BASIS_LINEAR_BEM3D, 1);
+  dense_pair("s4cl", gr, BASIS_CONSTANT_BEM3D, BASIS_LINEAR_BEM3D, 0);
+  dense_pair("s4lc", gr, BASIS_LINEAR_BEM3D, BASIS_CONSTANT_BEM3D, 0);
   del_surface3d(gr);
   del_macrosurface3d(mg);
 }

@@ -1,0 +1,128 @@
+"""H2 matrices on the B200 through the C ABI: bases, transfers, coupling and nearfield blocks,
+matrix-vector products and the GMRES Dirichlet solve, against the reference's golden vectors
+(tolerance 1e-12 relative for assembled parts and products; the solve must take the same number
+of GMRES iterations and reproduce the solution to 1e-9 relative)."""
+import numpy as np
+import pytest
+
+from h2lib_b200 import bem3d as hb
+
+pytestmark = pytest.mark.gpu
+L, C = hb.BASIS_LINEAR_BEM3D, hb.BASIS_CONSTANT_BEM3D
+Z = (1.2, 1.2, 1.2)
+
+
+def relerr(a, b):
+    a, b = np.ravel(a), np.ravel(b)
+    return float(np.linalg.norm(a - b) / np.linalg.norm(b))
+
+
+@pytest.fixture(scope="module")
+def s8():
+    return hb.new_sphere_surface3d(8)
+
+
+def build_pair(gr, basis, clf, m, eta=1.4):
+    slp = hb.new_slp_laplace_bem3d(gr, 2, 4, basis, basis)
+    dlp = hb.new_dlp_laplace_bem3d(gr, 2, 4, basis, basis, 0.5)
+    tree = hb.build_tree(gr, basis, basis, clf, eta)
+    return slp, dlp, tree, hb.H2Matrix(slp, tree, m), hb.H2Matrix(dlp, tree, m)
+
+
+@pytest.mark.parametrize("prefix,basis", [("h2ll", L), ("h2cc", C)])
+def test_h2_parts_match_reference(gold, s8, prefix, basis):
+    g = gold("h2small")
+    slp, dlp, tree, V, K = build_pair(s8, basis, 16, 3)
+    V.assemble()
+    K.assemble()
+    assert relerr(V.export(0), g[f"{prefix}_Vrow_V"]) < 1e-12
+    assert relerr(V.export(1), g[f"{prefix}_Vrow_E"]) < 1e-12
+    assert relerr(K.export(2), g[f"{prefix}_Kcol_V"]) < 1e-12
+    assert relerr(K.export(3), g[f"{prefix}_Kcol_E"]) < 1e-12
+    assert relerr(V.export(4, 24), g[f"{prefix}_Vparts_S"]) < 1e-12
+    assert relerr(V.export(5, 24), g[f"{prefix}_Vparts_N"]) < 1e-12
+    assert relerr(K.export(5, 24), g[f"{prefix}_Kparts_N"]) < 1e-12
+    x = g[f"{prefix}_x"]
+    y = hb.addeval_h2matrix_avector(1.0, V, x, np.zeros(V.rows))
+    assert relerr(y, g[f"{prefix}_ySLP"]) < 1e-12
+    y = hb.addeval_h2matrix_avector(1.0, K, x, np.zeros(K.rows))
+    assert relerr(y, g[f"{prefix}_yDLP"]) < 1e-12
+    # y += alpha A x accumulates
+    y2 = hb.addeval_h2matrix_avector(-2.0, K, x, y.copy())
+    assert relerr(y2, -g[f"{prefix}_yDLP"]) < 1e-12
+
+
+def test_fused_nearfield_pair_equals_separate(s8):
+    from h2lib_b200._lib import check, lib
+    slp, dlp, tree, V, K = build_pair(s8, L, 16, 3)
+    V.assemble()
+    K.assemble()
+    nv, nk = V.export(5), K.export(5)
+    V2, K2 = hb.H2Matrix(slp, tree, 3), hb.H2Matrix(dlp, tree, 3)
+    check(lib.h2b_h2matrix_assemble_nearfield_pair(V2.handle, K2.handle), "pair")
+    assert relerr(V2.export(5), nv) < 1e-14
+    assert relerr(K2.export(5), nk) < 1e-14
+
+
+def test_helmholtz_h2(gold, s8):
+    g = gold("helm_h2small")
+    slp = hb.new_slp_helmholtz_bem3d(2.0, s8, 2, 4, C, C)
+    dlp = hb.new_dlp_helmholtz_bem3d(2.0, s8, 2, 4, C, C, 0.5)
+    tree = hb.build_tree(s8, C, C, 16, 1.4)
+    V = hb.H2Matrix(slp, tree, 3).assemble()
+    K = hb.H2Matrix(dlp, tree, 3).assemble()
+    assert relerr(V.export(0), g["hh2_Vrow_V"].real) < 1e-12
+    assert relerr(K.export(2), g["hh2_Kcol_V"].real) < 1e-12
+    assert relerr(V.export(4, 24), g["hh2_Vparts_S"]) < 1e-12
+    x = np.ascontiguousarray(g["hh2_x"])
+    y = hb.addeval_h2matrix_avector(1.0, V, x, np.zeros(V.rows, dtype=np.complex128))
+    assert relerr(y, g["hh2_ySLP"]) < 1e-12
+    y = hb.addeval_h2matrix_avector(1.0, K, x, np.zeros(K.rows, dtype=np.complex128))
+    assert relerr(y, g["hh2_yDLP"]) < 1e-12
+
+
+def test_dirichlet_solve_small(gold, s8):
+    g = gold("h2small")
+    slp, dlp, tree, V, K = build_pair(s8, L, 16, 3)
+    V.assemble()
+    K.assemble()
+    gD = hb.project_l2_harmonic(dlp, Z)
+    assert relerr(gD, g["h2ll_gD"]) < 1e-12
+    b = hb.addeval_h2matrix_avector(1.0, K, gD, np.zeros(K.rows))
+    assert relerr(b, g["h2ll_b"]) < 1e-12
+    u = np.zeros(V.rows)
+    it = hb.solve_gmres_h2matrix_avector(V, b, u, 1e-8, 1000, 50)
+    assert it == int(g["h2ll_gmres_iter"][0])
+    assert relerr(u, g["h2ll_u"]) < 1e-9
+    err, nrm = hb.l2_error_harmonic(slp, Z, u)
+    assert abs(err / nrm - g["h2ll_l2err"][0] / g["h2ll_l2norm"][0]) < 1e-9
+    assert hb.residual_norm([V], [1.0], b, u) < 1.1e-8
+
+
+def test_config2_matvec_and_solve(gold):
+    """Sphere refined x64 (32768 triangles, 16386 vertices), linear basis, leaf size 64,
+    eta 1.4, m = 4: the matvecs, the GMRES(50) iteration count (161 in the reference) and the
+    relative L2 error of the Neumann trace (2.297e-2)."""
+    g = gold("config2")
+    gr = hb.new_sphere_surface3d(64)
+    slp, dlp, tree, V, K = build_pair(gr, L, 64, 4)
+    from h2lib_b200._lib import check, lib
+    check(lib.h2b_h2matrix_assemble_row_clusterbasis(V.handle), "rb")
+    check(lib.h2b_h2matrix_assemble_col_clusterbasis(V.handle), "cb")
+    check(lib.h2b_h2matrix_assemble_farfield(V.handle), "far")
+    check(lib.h2b_h2matrix_assemble_row_clusterbasis(K.handle), "rb")
+    check(lib.h2b_h2matrix_assemble_col_clusterbasis(K.handle), "cb")
+    check(lib.h2b_h2matrix_assemble_farfield(K.handle), "far")
+    check(lib.h2b_h2matrix_assemble_nearfield_pair(V.handle, K.handle), "near pair")
+    x = g["c2_x"]
+    assert relerr(hb.addeval_h2matrix_avector(1.0, V, x, np.zeros(V.rows)), g["c2_ySLP"]) < 1e-12
+    assert relerr(hb.addeval_h2matrix_avector(1.0, K, x, np.zeros(K.rows)), g["c2_yDLP"]) < 1e-12
+    gD = hb.project_l2_harmonic(dlp, Z)
+    assert relerr(gD, g["c2_gD"]) < 1e-12
+    b = hb.addeval_h2matrix_avector(1.0, K, gD, np.zeros(K.rows))
+    u = np.zeros(V.rows)
+    it = hb.solve_gmres_h2matrix_avector(V, b, u, 1e-8, 1000, 50)
+    assert it == int(g["c2_gmres_iter"][0])
+    assert relerr(u, g["c2_u"]) < 1e-8
+    err, nrm = hb.l2_error_harmonic(slp, Z, u)
+    assert abs(err / nrm - g["c2_l2err"][0] / g["c2_l2norm"][0]) < 1e-8

@@ -39,13 +39,13 @@ def test_sauter_schwab_rules(gold, which, name):
 
 
 @pytest.mark.parametrize("layer", [orc.SLP, orc.DLP])
-@pytest.mark.parametrize("basis", ["cc", "ll"])
+@pytest.mark.parametrize("basis", ["cc", "ll", "cl", "lc"])
 def test_nearfield_sphere4(gold, layer, basis):
     g = gold("sphere4")
     mesh = mesh_from(g, "sphere4")
-    b = L if basis == "ll" else C
+    rb, cb = (L if basis[0] == "l" else C), (L if basis[1] == "l" else C)
     alpha = 0.5 if layer == orc.DLP else 0.0
-    A = orc.nearfield(mesh, orc.LAPLACE, layer, b, b, alpha=alpha)
+    A = orc.nearfield(mesh, orc.LAPLACE, layer, rb, cb, alpha=alpha)
     ref = fortran(g[f"s4{basis}_{'slp' if layer == orc.SLP else 'dlp'}"])
     assert A.shape == ref.shape
     assert rel_entry_err(A, ref) < 1e-12
