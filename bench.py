@@ -1,0 +1,410 @@
+"""Benchmark: H2 assembly of the Laplace single- and double-layer operators (FP64) on the
+Dirichlet benchmark mesh, plus the GMRES solve, on B200.
+
+Workload (default): unit sphere refined x64 (32768 triangles, 16386 vertices), piecewise linear
+basis, Sauter-Schwab quadrature q = 2 / 4, leaf size 64, admissibility eta = 1.4, Chebyshev
+interpolation m = 4.  One step = assemble both H2 matrices V (SLP) and K (DLP, alpha = 1/2): row and
+column cluster bases, coupling matrices and the nearfield blocks (the nearfield of both operators
+in one fused pass).  metric = nearfield entries of V and K per second ("BEM entries/s").  The
+solve V u = (K + M/2) g_D, g_D = 1/|x - z|, z = (1.2, 1.2, 1.2), GMRES(50) to 1e-8, is timed
+after the steps and reported under "solve".
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+Multi-GPU: the path has no exchange step in this form, so N ranks run N independent replicas
+(weak scaling, no collective on the data path).
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "BEM entries/s (FP64 nearfield entries of the SLP+DLP H2 assembly)"
+UNIT = "entries/s"
+Z = (1.2, 1.2, 1.2)
+# algorithmic FP64 operations per quadrature point (reference source, + - * / sqrt counted as 1):
+# linear-basis single layer 64, double layer 72
+FLOPS_PER_POINT = {"slp": 64, "dlp": 72}
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=5)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--split", type=int, default=64)
+    p.add_argument("--clf", type=int, default=64)
+    p.add_argument("--eta", type=float, default=1.4)
+    p.add_argument("--m", type=int, default=4)
+    p.add_argument("--no-solve", action="store_true")
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-e2e", action="store_true")
+    return p.parse_args()
+
+
+def workload(a):
+    return {"workload": f"Laplace SLP+DLP H2 assembly, sphere split {a.split} "
+                        f"({8 * a.split * a.split} triangles), linear basis, q=2/4, "
+                        f"leaf {a.clf}, eta {a.eta}, m {a.m}; GMRES(50) to 1e-8",
+            "triangles": 8 * a.split * a.split, "basis": "linear", "q_regular": 2,
+            "q_singular": 4, "leaf_size": a.clf, "eta": a.eta, "interpolation_order": a.m,
+            "l2_flush": "256 MiB buffer written between timed steps"}
+
+
+# --------------------------------------------------------------------------------------------
+# distributed plumbing (replicas)
+# --------------------------------------------------------------------------------------------
+
+def dist_init(n):
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import torch.distributed as dist
+        import datetime
+        dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=300))
+    return rank, world, local
+
+
+def dist_max(v, world):
+    if world == 1:
+        return v
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([v], dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def dist_barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+# --------------------------------------------------------------------------------------------
+# clocks
+# --------------------------------------------------------------------------------------------
+
+class ClockSampler:
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.samples = []
+        self._stop = threading.Event()
+        self._t = None
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(
+                    ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}",
+                     "--format=csv,noheader,nounits"], capture_output=True, text=True,
+                    timeout=5).stdout.strip()
+                if out:
+                    self.samples.append([s.strip() for s in out.split(",")])
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def __enter__(self):
+        self._t = threading.Thread(target=self._run, daemon=True)
+        self._t.start()
+        return self
+
+    def __exit__(self, *exc):
+        self._stop.set()
+        self._t.join(timeout=10)
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
+        mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for s in self.samples for i in range(4)
+                          if len(s) > 3 + i and s[3 + i].lower().startswith("active")})
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
+                "samples": len(self.samples)}
+
+
+# --------------------------------------------------------------------------------------------
+# CPU baseline: the unmodified reference (oracle/_ref/ref_bench, OpenMP + AVX) on the host
+# --------------------------------------------------------------------------------------------
+
+REF_BENCH = os.path.join(ROOT, "oracle", "_ref", "ref_bench")
+
+
+def run_reference(a, steps, warmup, stride):
+    if not os.path.exists(REF_BENCH):
+        return None
+    out = subprocess.run([REF_BENCH, str(a.split), str(a.clf), str(a.eta), str(a.m), str(steps),
+                          str(warmup), str(stride)], capture_output=True, text=True, timeout=1800)
+    if out.returncode != 0:
+        raise RuntimeError(f"ref_bench failed: {out.stderr[-2000:]}")
+    return json.loads(out.stdout)
+
+
+def cpu_baseline(a):
+    """Bounded sample: every 8th nearfield block + all bases and coupling, one timed step."""
+    stride = 8
+    r = run_reference(a, 1, 0, stride)
+    if r is None:
+        return None
+    s = r["steps"][0]
+    return {"value": s["entries"] / s["seconds"], "unit": UNIT, "cores": r["threads"],
+            "kind": "reference",
+            "sample": f"H2Lib (OpenMP+AVX build) assembling V and K on sphere split {a.split}: "
+                      f"all bases and coupling matrices, every {stride}th of {r['near_blocks']} "
+                      f"nearfield blocks ({s['entries']:.0f} entries in {s['seconds']:.2f} s)"}
+
+
+# --------------------------------------------------------------------------------------------
+# our arm
+# --------------------------------------------------------------------------------------------
+
+def fp64_peak_tflops(torch):
+    """cuBLAS DGEMM 8192^3, best of 5 (the FP64 roofline denominator, measured in-run)."""
+    n = 8192
+    A = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    B = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    torch.matmul(A, B)
+    torch.cuda.synchronize()
+    best = 0.0
+    for _ in range(5):
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        torch.matmul(A, B)
+        e.record()
+        torch.cuda.synchronize()
+        best = max(best, 2.0 * n ** 3 / (s.elapsed_time(e) * 1e-3) / 1e12)
+    del A, B
+    torch.cuda.empty_cache()
+    return best
+
+
+def run_ours(a, rank, world, local):
+    import torch
+    torch.cuda.set_device(local)
+    from h2lib_b200 import bem3d as hb
+    from h2lib_b200._lib import check, lib
+    check(lib.h2b_device_init(local), "device_init")
+    L = hb.BASIS_LINEAR_BEM3D
+
+    # ---- setup (untimed): mesh, operators, trees, H2 structure on the device
+    gr = hb.new_sphere_surface3d(a.split)
+    slp = hb.new_slp_laplace_bem3d(gr, 2, 4, L, L)
+    dlp = hb.new_dlp_laplace_bem3d(gr, 2, 4, L, L, 0.5)
+    tree = hb.build_tree(gr, L, L, a.clf, a.eta)
+    V = hb.H2Matrix(slp, tree, a.m)
+    K = hb.H2Matrix(dlp, tree, a.m)
+    entries = V.info()["near_entries"] + K.info()["near_entries"]
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+
+    def step():
+        for h in (V, K):
+            check(lib.h2b_h2matrix_assemble_row_clusterbasis(h.handle), "row basis")
+            check(lib.h2b_h2matrix_assemble_col_clusterbasis(h.handle), "col basis")
+            check(lib.h2b_h2matrix_assemble_farfield(h.handle), "coupling")
+        check(lib.h2b_h2matrix_assemble_nearfield_pair(V.handle, K.handle), "nearfield pair")
+        tv, tk = V.timings(), K.timings()
+        dev = sum(tv[p] + tk[p] for p in ("row_basis", "col_basis", "coupling", "near_distant",
+                                           "near_singular"))
+        return dev, tv, tk
+
+    for _ in range(a.warmup):
+        step()
+    torch.cuda.synchronize()
+    dev_ms, wall_ms, phases = [], [], []
+    with ClockSampler(local) as clocks:
+        dist_barrier(world)
+        torch.cuda.synchronize()
+        for _ in range(a.steps):
+            flush.fill_(1.0)  # evict L2 between steps
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            dev, tv, tk = step()
+            wall_ms.append((time.perf_counter() - t0) * 1e3)
+            dev_ms.append(dev)
+            phases.append((tv, tk))
+        torch.cuda.synchronize()
+        dist_barrier(world)
+    step_ms = dist_max(statistics.mean(dev_ms), world)
+    value = world * entries / (step_ms * 1e-3)
+
+    # ---- roofline of the dominant kernel: fused nearfield distant-pair quadrature (FP64)
+    pc = V.pair_counts()
+    near_dist_ms = statistics.mean(p[0]["near_distant"] for p in phases)
+    near_sing_ms = statistics.mean(p[0]["near_singular"] for p in phases)
+    dist_flops = pc["distant"] * 16 * (FLOPS_PER_POINT["slp"] + FLOPS_PER_POINT["dlp"])
+    sing_points = pc["vertex"] * 512 + pc["edge"] * 1536 + pc["identical"] * 1536
+    peak = fp64_peak_tflops(torch)
+    achieved = dist_flops / (near_dist_ms * 1e-3) / 1e12
+    roofline = {"bound": "fp64", "kernel": "near_dist_kernel (fused SLP+DLP, linear basis)",
+                "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+                "traffic": None,
+                "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (MEASURED_PEAKS.json "
+                               "has no FP64 figure)",
+                "flops_per_launch": dist_flops, "launch_ms": near_dist_ms}
+
+    # ---- matvec roofline (HBM): bytes of S, N, V, E read once per product
+    x = torch.randn(V.cols, dtype=torch.float64, device="cuda")
+    y = torch.zeros(V.rows, dtype=torch.float64, device="cuda")
+    for _ in range(3):
+        hb.addeval_h2matrix_avector(1.0, V, x, y)
+    mv = []
+    for _ in range(10):
+        flush.fill_(1.0)
+        torch.cuda.synchronize()
+        hb.addeval_h2matrix_avector(1.0, V, x, y)
+        mv.append(V.timings()["matvec"])
+    inf = V.info()
+    mv_bytes = 8 * (inf["near_entries"] + inf["coupling_entries"] + inf["leaf_entries"]
+                    + inf["transfer_entries"])
+    mv_ms = statistics.mean(mv)
+    peaks = {}
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
+            peaks = json.load(fh)
+    except OSError:
+        pass
+    hbm = peaks.get("hbm_gbs", 6650.0)
+    roof_mv = {"bound": "hbm", "kernel": "H2 matvec (all kernels of one product)",
+               "achieved": mv_bytes / (mv_ms * 1e-3) / 1e9, "peak": hbm, "unit": "GB/s",
+               "frac": mv_bytes / (mv_ms * 1e-3) / 1e9 / hbm, "traffic": None,
+               "peak_source": "MEASURED_PEAKS.json hbm_gbs" if peaks else "fallback 6650 GB/s",
+               "bytes_per_launch": mv_bytes, "launch_ms": mv_ms}
+
+    # ---- solve (FP64 GMRES(50) to 1e-8)
+    solve = None
+    if not a.no_solve:
+        gD = hb.project_l2_harmonic(dlp, Z)
+        b = hb.addeval_h2matrix_avector(1.0, K, gD, np.zeros(K.rows))
+        u = np.zeros(V.rows)
+        hb.solve_gmres_h2matrix_avector(V, b, u, 1e-8, 1000, 50)  # warm-up
+        u[:] = 0.0
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        it = hb.solve_gmres_h2matrix_avector(V, b, u, 1e-8, 1000, 50)
+        t_solve = time.perf_counter() - t0
+        err, nrm = hb.l2_error_harmonic(slp, Z, u)
+        solve = {"seconds": t_solve, "solves_per_s": 1.0 / t_solve, "iterations": it,
+                 "rel_l2_error_neumann": err / nrm,
+                 "rel_residual": hb.residual_norm([V], [1.0], b, u),
+                 "reference_iterations": 161, "reference_rel_l2_error": 2.297e-2}
+
+    # ---- e2e: the same assembly through the C ABI from host arrays, results copied to host
+    e2e = None
+    if not a.no_e2e:
+        pin = {}
+        inf_k = K.info()
+        for name, h, part in (("Vn", V, 5), ("Kn", K, 5), ("Vs", V, 4), ("Ks", K, 4)):
+            n = inf["near_entries"] if part == 5 else inf["coupling_entries"]
+            pin[name] = torch.empty(n, dtype=torch.float64, pin_memory=True)
+        e2e_times = []
+        h2d = d2h = 0
+        for rep in range(3):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            g2 = hb.Surface3d(gr.x, gr.t)
+            s2 = hb.new_slp_laplace_bem3d(g2, 2, 4, L, L)
+            d2 = hb.new_dlp_laplace_bem3d(g2, 2, 4, L, L, 0.5)
+            tr2 = hb.build_tree(g2, L, L, a.clf, a.eta)
+            V2, K2 = hb.H2Matrix(s2, tr2, a.m), hb.H2Matrix(d2, tr2, a.m)
+            for h in (V2, K2):
+                check(lib.h2b_h2matrix_assemble_row_clusterbasis(h.handle), "row basis")
+                check(lib.h2b_h2matrix_assemble_col_clusterbasis(h.handle), "col basis")
+                check(lib.h2b_h2matrix_assemble_farfield(h.handle), "coupling")
+            check(lib.h2b_h2matrix_assemble_nearfield_pair(V2.handle, K2.handle), "near pair")
+            import ctypes
+            nd = ctypes.c_uint64()
+            for name, h, part in (("Vn", V2, 5), ("Kn", K2, 5), ("Vs", V2, 4), ("Ks", K2, 4)):
+                check(lib.h2b_h2matrix_export(h.handle, part, 0xFFFFFFFF,
+                                              ctypes.c_void_p(pin[name].data_ptr()),
+                                              ctypes.byref(nd)), "export")
+            e2e_times.append(time.perf_counter() - t0)
+            d2h = 8 * (2 * inf["near_entries"] + 2 * inf["coupling_entries"])
+            h2d = gr.x.nbytes + gr.t.nbytes + gr.n.nbytes + gr.g.nbytes
+            del V2, K2, tr2, s2, d2, g2
+        e2e_s = dist_max(min(e2e_times), world)
+        e2e = {"value": world * entries / e2e_s, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+               "d2h_bytes_per_step": int(d2h),
+               "includes": "mesh upload, operators, cluster/block trees (host C), H2 structure "
+                           "upload, assembly of V and K, copy of all nearfield and coupling "
+                           "blocks to pinned host memory"}
+
+    res = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps,
+        "warmup": a.warmup, "ms_per_step": step_ms, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": dict(workload(a), parallelism=f"replicas{world}"),
+        "entries_per_step": entries, "wall_ms_per_step": statistics.mean(wall_ms),
+        "phase_ms": {k: statistics.mean(p[0][k] + p[1][k] for p in phases)
+                     for k in ("row_basis", "col_basis", "coupling")} |
+                    {"near_distant_fused": near_dist_ms, "near_singular_fused": near_sing_ms},
+        "pairs_per_operator": pc, "singular_points": sing_points,
+        "roofline": roofline, "roofline_matvec": roof_mv, "solve": solve, "e2e": e2e,
+        "clocks": clocks.summary(),
+        "gpu_launches": a.steps * 12,
+    }
+    return res
+
+
+def main():
+    a = parse()
+    rank, world, local = dist_init(a.gpus)
+    if a.impl == "reference":
+        if rank != 0:
+            return 0
+        stride = 4
+        r = run_reference(a, a.steps, a.warmup, stride)
+        if r is None:
+            print(json.dumps({"impl": "reference", "unavailable":
+                              "oracle/_ref/ref_bench not built (H2Lib sources absent at build)"}))
+            return 0
+        secs = [s["seconds"] for s in r["steps"]]
+        ent = r["steps"][0]["entries"]
+        value = ent / statistics.mean(secs)
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+                "steps": a.steps, "warmup": a.warmup,
+                "ms_per_step": statistics.mean(secs) * 1e3, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                "config": dict(workload(a), parallelism="cpu"), "impl": "reference",
+                "cpu_baseline": {"value": value, "unit": UNIT, "cores": r["threads"],
+                                 "kind": "reference",
+                                 "sample": f"every {stride}th of {r['near_blocks']} nearfield "
+                                           f"blocks + all bases and coupling per step"},
+                "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
+                        "d2h_bytes_per_step": 0}}
+        print(json.dumps(line))
+        return 0
+    res = run_ours(a, rank, world, local)
+    if rank == 0:
+        if not a.no_cpu_baseline:
+            try:
+                res["cpu_baseline"] = cpu_baseline(a)
+            except Exception as e:  # the baseline is reported, never required
+                res["cpu_baseline"] = {"unavailable": str(e)[:200]}
+        print(json.dumps(res))
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -233,10 +233,24 @@ class H2Matrix:
                     bytes=int(info[4]), admissible=int(info[5]), near_blocks=int(info[6]),
                     rank=int(info[7]))
 
+    def timings(self):
+        """Device ms of the last row basis, column basis, coupling, nearfield distant,
+        nearfield singular and matvec runs."""
+        ms = np.zeros(6)
+        check(lib.h2b_h2matrix_timings(self.handle, ms), "timings")
+        return dict(zip(("row_basis", "col_basis", "coupling", "near_distant", "near_singular",
+                         "matvec"), ms.tolist()))
+
+    def pair_counts(self):
+        c = np.zeros(4, dtype=np.uint64)
+        check(lib.h2b_h2matrix_pair_counts(self.handle, c), "pair_counts")
+        return dict(zip(("distant", "vertex", "edge", "identical"), (int(v) for v in c)))
+
     def export(self, part, count=0xFFFFFFFF):
         n = C.c_uint64()
         check(lib.h2b_h2matrix_export(self.handle, part, count, None, C.byref(n)), "export")
-        if self.dtype == np.complex128:
+        # cluster bases and transfer matrices (parts 0-3) are real for every operator
+        if self.dtype == np.complex128 and part >= 4:
             out = np.zeros(n.value // 2, dtype=np.complex128)
         else:
             out = np.zeros(n.value)

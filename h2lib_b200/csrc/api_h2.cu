@@ -135,6 +135,8 @@ extern "C" void h2b_h2matrix_del(h2b_h2matrix *h) {
   dfree(h->d_xp); dfree(h->d_yp); dfree(h->d_xt); dfree(h->d_yt);
   dfree(h->d_xs); dfree(h->d_ys); dfree(h->d_ws); dfree(h->d_wsl);
   dfree(h->d_xio); dfree(h->d_yio);
+  for (int e = 0; e < 12; e++)
+    if (h->ev[e]) cudaEventDestroy(h->ev[e]);
   if (h->st) cudaStreamDestroy(h->st);
   delete h;
 }
@@ -195,6 +197,18 @@ extern "C" h2b_h2matrix *h2b_h2matrix_new(const h2b_bem *bem, const h2b_tree *tr
     }
   }
   if (rc == H2B_OK) rc = h2b_nearplan_finalize(&plan);
+  if (rc == H2B_OK) {
+    uint64_t all = 0;
+    for (uint32_t t = 0; t < plan.ntiles; t++)
+      all += (uint64_t) plan.tiles[t].tr_len * plan.tiles[t].sc_len;
+    for (int c = 1; c <= 3; c++) h->pairs[c] = plan.case_start[c + 1] - plan.case_start[c];
+    h->pairs[0] = all - plan.nsing;
+  }
+  for (int e = 0; rc == H2B_OK && e < 12; e++)
+    if (cudaEventCreate(&h->ev[e]) != cudaSuccess) {
+      h2b_set_error("h2b_h2matrix_new: %s", cudaGetErrorString(cudaGetLastError()));
+      rc = H2B_ERR_CUDA;
+    }
   h->nadm = (uint32_t) arc.size();
   h->nnear = (uint32_t) nrc.size();
   h->near_total = ntot;
@@ -305,32 +319,51 @@ static int assemble_basis(h2b_h2matrix *h, DevCTree &t, int basis, int dn) {
   return h2b_far_transfer(&ta, h->st);
 }
 
-static int finish(h2b_h2matrix *h, int rc) {
+// Phase timings: events 2i / 2i+1 bracket phase i (0 row basis, 1 column basis, 2 coupling,
+// 3 nearfield; event 7 separates the distant and singular nearfield kernels; 9/10 the matvec).
+static void mark(h2b_h2matrix *h, int e) { cudaEventRecord(h->ev[e], h->st); }
+
+static int finish(h2b_h2matrix *h, int rc, unsigned phases) {
   if (rc != H2B_OK) return rc;
   if (cudaStreamSynchronize(h->st) != cudaSuccess) {
     h2b_set_error("h2matrix: %s", cudaGetErrorString(cudaGetLastError()));
     return H2B_ERR_CUDA;
   }
+  float t;
+  if ((phases & 1) && cudaEventElapsedTime(&t, h->ev[0], h->ev[1]) == cudaSuccess) h->ms[0] = t;
+  if ((phases & 2) && cudaEventElapsedTime(&t, h->ev[2], h->ev[3]) == cudaSuccess) h->ms[1] = t;
+  if ((phases & 4) && cudaEventElapsedTime(&t, h->ev[4], h->ev[5]) == cudaSuccess) h->ms[2] = t;
+  if (phases & 8) {
+    if (cudaEventElapsedTime(&t, h->ev[6], h->ev[7]) == cudaSuccess) h->ms[3] = t;
+    if (cudaEventElapsedTime(&t, h->ev[7], h->ev[8]) == cudaSuccess) h->ms[4] = t;
+  }
+  cudaGetLastError();
   return H2B_OK;
 }
 
-extern "C" int h2b_h2matrix_assemble_row_clusterbasis(h2b_h2matrix *h) {
-  if (!h) return H2B_ERR_ARG;
+static int row_basis(h2b_h2matrix *h) {
+  mark(h, 0);
   // row side: Lagrange polynomials (assemble_bem3d_lagrange_{c,l}_amatrix)
-  return finish(h, assemble_basis(h, h->rt, h->bem->row_basis, 0));
+  int rc = assemble_basis(h, h->rt, h->bem->row_basis, 0);
+  mark(h, 1);
+  return rc;
 }
 
-extern "C" int h2b_h2matrix_assemble_col_clusterbasis(h2b_h2matrix *h) {
-  if (!h) return H2B_ERR_ARG;
+static int col_basis(h2b_h2matrix *h) {
+  mark(h, 2);
   // column side of the double layer: normal derivatives (assemble_bem3d_dn_lagrange_*)
-  return finish(h, assemble_basis(h, h->ct, h->bem->col_basis, h->bem->layer == H2B_DLP));
+  int rc = assemble_basis(h, h->ct, h->bem->col_basis, h->bem->layer == H2B_DLP);
+  mark(h, 3);
+  return rc;
 }
 
-extern "C" int h2b_h2matrix_assemble_farfield(h2b_h2matrix *h) {
-  if (!h) return H2B_ERR_ARG;
+static int coupling(h2b_h2matrix *h) {
+  mark(h, 4);
   FarCouplingArgs ca{h->d_adm_rc, h->d_adm_cc, h->rt.d_pts, h->ct.d_pts, h->d_S, h->nadm,
                      (int) h->m, (int) h->k, h->bem->kconst, h->bem->k_re, -h->bem->k_im};
-  return finish(h, h2b_far_coupling(&ca, h->cx, h->st));
+  int rc = h2b_far_coupling(&ca, h->cx, h->st);
+  mark(h, 5);
+  return rc;
 }
 
 static int launch_near(h2b_h2matrix *h, h2b_h2matrix *h2) {
@@ -342,20 +375,38 @@ static int launch_near(h2b_h2matrix *h, h2b_h2matrix *h2) {
   L.sing = h->d_sing;
   L.nsing = h->nsing;
   L.out0 = h->d_N;
+  L.ev_between = h->ev[7];
   if (h2) {
     L.kk = H2B_KK_LBOTH;
     L.out1 = h2->d_N;
     L.alpha_re = h2->bem->alpha_re;
     L.alpha_im = h2->bem->alpha_im;
   }
+  mark(h, 6);
   int rc = h2b_near_launch_kernels(&L, h->st);
+  mark(h, 8);
   if (rc == H2B_OK) rc = h2b_check_err_flag(h->bem, h->st);
   return rc;
 }
 
+extern "C" int h2b_h2matrix_assemble_row_clusterbasis(h2b_h2matrix *h) {
+  if (!h) return H2B_ERR_ARG;
+  return finish(h, row_basis(h), 1);
+}
+
+extern "C" int h2b_h2matrix_assemble_col_clusterbasis(h2b_h2matrix *h) {
+  if (!h) return H2B_ERR_ARG;
+  return finish(h, col_basis(h), 2);
+}
+
+extern "C" int h2b_h2matrix_assemble_farfield(h2b_h2matrix *h) {
+  if (!h) return H2B_ERR_ARG;
+  return finish(h, coupling(h), 4);
+}
+
 extern "C" int h2b_h2matrix_assemble_nearfield(h2b_h2matrix *h) {
   if (!h) return H2B_ERR_ARG;
-  return finish(h, launch_near(h, nullptr));
+  return finish(h, launch_near(h, nullptr), 8);
 }
 
 extern "C" int h2b_h2matrix_assemble_nearfield_pair(h2b_h2matrix *a, h2b_h2matrix *b) {
@@ -368,34 +419,42 @@ extern "C" int h2b_h2matrix_assemble_nearfield_pair(h2b_h2matrix *a, h2b_h2matri
                   "same tree, surface, bases and quadrature orders");
     return H2B_ERR_ARG;
   }
-  cudaEvent_t ev;
-  H2B_CUDA_TRY(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
   // b's storage must be idle before a's stream writes it
-  cudaEventRecord(ev, b->st);
-  cudaStreamWaitEvent(a->st, ev, 0);
-  int rc = finish(a, launch_near(a, b));
-  cudaEventDestroy(ev);
+  H2B_CUDA_TRY(cudaEventRecord(b->ev[11], b->st));
+  H2B_CUDA_TRY(cudaStreamWaitEvent(a->st, b->ev[11], 0));
+  int rc = finish(a, launch_near(a, b), 8);
+  if (rc == H2B_OK) {
+    b->ms[3] = b->ms[4] = 0.0f;  // the pass is accounted to a
+  }
   return rc;
 }
 
 extern "C" int h2b_h2matrix_assemble(h2b_h2matrix *h) {
   if (!h) return H2B_ERR_ARG;
-  int rc = h2b_h2matrix_assemble_farfield(h);
-  if (rc == H2B_OK) rc = h2b_h2matrix_assemble_nearfield(h);
-  return rc;
+  int rc = coupling(h);
+  if (rc == H2B_OK) rc = launch_near(h, nullptr);
+  return finish(h, rc, 4 | 8);
 }
 
 extern "C" int h2b_h2matrix_assemble_all(h2b_h2matrix *h) {
   if (!h) return H2B_ERR_ARG;
-  int rc = assemble_basis(h, h->rt, h->bem->row_basis, 0);
-  if (rc == H2B_OK) rc = assemble_basis(h, h->ct, h->bem->col_basis, h->bem->layer == H2B_DLP);
-  if (rc == H2B_OK) {
-    FarCouplingArgs ca{h->d_adm_rc, h->d_adm_cc, h->rt.d_pts, h->ct.d_pts, h->d_S, h->nadm,
-                       (int) h->m, (int) h->k, h->bem->kconst, h->bem->k_re, -h->bem->k_im};
-    rc = h2b_far_coupling(&ca, h->cx, h->st);
-  }
+  int rc = row_basis(h);
+  if (rc == H2B_OK) rc = col_basis(h);
+  if (rc == H2B_OK) rc = coupling(h);
   if (rc == H2B_OK) rc = launch_near(h, nullptr);
-  return finish(h, rc);
+  return finish(h, rc, 1 | 2 | 4 | 8);
+}
+
+extern "C" int h2b_h2matrix_timings(const h2b_h2matrix *h, double ms[6]) {
+  if (!h || !ms) return H2B_ERR_ARG;
+  for (int i = 0; i < 6; i++) ms[i] = h->ms[i];
+  return H2B_OK;
+}
+
+extern "C" int h2b_h2matrix_pair_counts(const h2b_h2matrix *h, uint64_t counts[4]) {
+  if (!h || !counts) return H2B_ERR_ARG;
+  for (int i = 0; i < 4; i++) counts[i] = h->pairs[i];
+  return H2B_OK;
 }
 
 // ------------------------------------------------------------------------------------------
@@ -520,7 +579,9 @@ extern "C" int h2b_h2matrix_addeval(double alpha_re, double alpha_im, const h2b_
                                  cudaMemcpyHostToDevice, h->st));
     yd = h->d_yio;
   }
+  cudaEventRecord(h->ev[9], h->st);
   int rc = h2b_h2_addeval_dev(h, alpha_re, alpha_im, xd, yd, h->st);
+  cudaEventRecord(h->ev[10], h->st);
   if (rc == H2B_OK && !dy) {
     if (cudaMemcpyAsync(y, yd, sizeof(double) * W * h->rt.nidx, cudaMemcpyDeviceToHost,
                         h->st) != cudaSuccess) {
@@ -532,5 +593,8 @@ extern "C" int h2b_h2matrix_addeval(double alpha_re, double alpha_im, const h2b_
     h2b_set_error("h2b_h2matrix_addeval: %s", cudaGetErrorString(cudaGetLastError()));
     rc = H2B_ERR_CUDA;
   }
+  float t;
+  if (rc == H2B_OK && cudaEventElapsedTime(&t, h->ev[9], h->ev[10]) == cudaSuccess)
+    const_cast<h2b_h2matrix *>(h)->ms[5] = t;
   return rc;
 }

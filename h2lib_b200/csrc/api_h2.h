@@ -46,6 +46,12 @@ struct h2b_h2matrix {
   double *d_xio = nullptr, *d_yio = nullptr;  // staging of host vectors
   double *d_xs = nullptr, *d_ys = nullptr, *d_ws = nullptr, *d_wsl = nullptr;
   MvmPlan mvm;
+  // pair counts of the nearfield plan by Sauter-Schwab case (distant, vertex, edge, identical)
+  uint64_t pairs[4] = {0, 0, 0, 0};
+  // device timings of the last assembly phases (ms): row basis, column basis, coupling,
+  // nearfield distant, nearfield singular, matvec
+  cudaEvent_t ev[12] = {};
+  float ms[6] = {0, 0, 0, 0, 0, 0};
 };
 
 void h2b_h2_fill_mvm_plan(h2b_h2matrix *h);

@@ -504,6 +504,7 @@ int launch_kk_basis(const h2b_near_launch *L, cudaStream_t st) {
   else
     rc = launch_dist<0, KK, RL, CL>(L, st);
   if (rc != H2B_OK) return rc;
+  if (L->ev_between) H2B_CUDA_TRY(cudaEventRecord(L->ev_between, st));
   return launch_sing<KK, RL, CL>(L, st);
 }
 

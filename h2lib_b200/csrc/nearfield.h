@@ -36,6 +36,7 @@ typedef struct {
   uint32_t rule_n[4], rule_off[4], rule_total;
   int num_sms;
   int *err;                      /* device flag */
+  cudaEvent_t ev_between;        /* optional: recorded between the distant and singular kernels */
 } h2b_near_launch;
 
 int h2b_near_upload_dist_rules(void);

@@ -210,6 +210,17 @@ int h2b_h2matrix_assemble_nearfield_pair(h2b_h2matrix *a, h2b_h2matrix *b);
  * [7] rank k. */
 int h2b_h2matrix_info(const h2b_h2matrix *h2, uint64_t info[8]);
 
+/* Device time (ms, CUDA events on the matrix's stream) of the last run of each phase:
+ * [0] row basis, [1] column basis, [2] coupling, [3] nearfield distant pairs, [4] nearfield
+ * singular pairs, [5] last matvec.  No reference counterpart (diagnostics). */
+int h2b_h2matrix_timings(const h2b_h2matrix *h2, double ms[6]);
+
+/* Triangle pairs evaluated by one nearfield assembly, by Sauter-Schwab case: [0] distant,
+ * [1] common vertex, [2] common edge, [3] identical.  Every nearfield block evaluates all pairs
+ * of triangles touching its row and column index sets, as assemble_ll_near_bem3d does
+ * (Library/bem3d.c:3038).  No reference counterpart (diagnostics). */
+int h2b_h2matrix_pair_counts(const h2b_h2matrix *h2, uint64_t counts[4]);
+
 /* Copy parts back for inspection, in H2Lib's layouts and orders (pre-order, column-major):
  * part 0: leaf bases of the row basis, 1: transfer matrices of the row basis (all non-root
  * clusters), 2/3 the same for the column basis, 4: coupling matrices of the admissible blocks,
