@@ -9,7 +9,9 @@ import os
 import numpy as np
 
 PKG = os.path.dirname(os.path.abspath(__file__))
-LIBPATH = os.path.join(PKG, "libh2b200.so")
+# H2B_LIBRARY selects another build of the same library (e.g. a variant compiled with different
+# kernel options); by default the in-tree libh2b200.so is used.
+LIBPATH = os.environ.get("H2B_LIBRARY") or os.path.join(PKG, "libh2b200.so")
 
 H2B_OK = 0
 BASIS_CONSTANT = ord("c")
@@ -75,6 +77,7 @@ _SIGS = {
     "h2b_project_l2_harmonic": (C.c_int, [vp, _f64p, vp]),
     "h2b_l2_error_harmonic": (C.c_int, [vp, _f64p, vp, C.POINTER(C.c_double),
                                         C.POINTER(C.c_double)]),
+    "h2b_integrate_plane_wave": (C.c_int, [vp, _f64p, _f64p, C.c_double, C.c_double, vp]),
 }
 
 

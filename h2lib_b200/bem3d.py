@@ -318,6 +318,18 @@ def l2_error_harmonic(bem, z, u):
     return e.value, n.value
 
 
+def integrate_plane_wave(bem, kvec, src=(0.0, 0.0, 0.0), coef=1.0, b=None):
+    """b_t = coef * int_t exp(i kvec.(x - src)) (integrate_bem3d_c_avector with
+    rhs_dirichlet_plane_helmholtzbem3d, Library/bem3d.c:8579, Library/helmholtzbem3d.c:1611)."""
+    if b is None:
+        b = np.zeros(bem.gr.triangles, dtype=np.complex128)
+    coef = complex(coef)
+    check(lib.h2b_integrate_plane_wave(bem.handle, np.asarray(kvec, dtype=np.float64),
+                                       np.asarray(src, dtype=np.float64), coef.real, coef.imag,
+                                       _ptr(b)), "integrate_plane_wave")
+    return b
+
+
 def quad_export(q, q2, row_basis, col_basis, which):
     """Quadrature rule tables (Library/singquad2d.c:25-320): dict of arrays."""
     n = C.c_uint32()

@@ -52,32 +52,34 @@ def _compile(cmd):
     return res.stderr
 
 
-def build(force=False, verbose=False):
-    os.makedirs(BUILD, exist_ok=True)
+def build(force=False, verbose=False, defines=(), lib=LIB, build_dir=BUILD):
+    """Compile and link; `defines` (e.g. ["-DH2B_FOO=1"]) build a variant into `lib`,
+    with objects in `build_dir`."""
+    os.makedirs(build_dir, exist_ok=True)
     nvcc = _nvcc()
     newest_header = max((os.path.getmtime(h) for h in _headers()), default=0.0)
     jobs, objs = [], []
     for src in sorted(glob.glob(os.path.join(CSRC, "*.c"))):
-        obj = os.path.join(BUILD, os.path.basename(src) + ".o")
+        obj = os.path.join(build_dir, os.path.basename(src) + ".o")
         objs.append(obj)
         if force or _stale(src, obj, newest_header):
-            jobs.append(["gcc", *CFLAGS, "-c", src, "-o", obj])
+            jobs.append(["gcc", *CFLAGS, *defines, "-c", src, "-o", obj])
     for src in sorted(glob.glob(os.path.join(CSRC, "*.cu"))):
-        obj = os.path.join(BUILD, os.path.basename(src) + ".o")
+        obj = os.path.join(build_dir, os.path.basename(src) + ".o")
         objs.append(obj)
         if force or _stale(src, obj, newest_header):
-            jobs.append([nvcc, *NVFLAGS, "-c", src, "-o", obj])
+            jobs.append([nvcc, *NVFLAGS, *defines, "-c", src, "-o", obj])
     if jobs:
         with concurrent.futures.ThreadPoolExecutor(max_workers=os.cpu_count() or 4) as ex:
             for out in ex.map(_compile, jobs):
                 if verbose and out:
                     print(out, file=sys.stderr)
-    if jobs or force or not os.path.exists(LIB) or \
-            any(os.path.getmtime(o) > os.path.getmtime(LIB) for o in objs):
-        tmp = LIB + ".tmp"
+    if jobs or force or not os.path.exists(lib) or \
+            any(os.path.getmtime(o) > os.path.getmtime(lib) for o in objs):
+        tmp = lib + ".tmp"
         _compile([nvcc, *ARCH, "-shared", "-o", tmp, *objs, "-lcuda", "-lm"])
-        os.replace(tmp, LIB)
-    return LIB
+        os.replace(tmp, lib)
+    return lib
 
 
 if __name__ == "__main__":

@@ -293,8 +293,11 @@ void h2b_h2_fill_mvm_plan(h2b_h2matrix *h) {
 // assembly
 // ------------------------------------------------------------------------------------------
 
+// The column basis is stored transposed (V^T, E^T), the layout the forward transform reads.
 static int assemble_basis(h2b_h2matrix *h, DevCTree &t, int basis, int dn) {
+  const int transposed = (&t == &h->ct);
   FarLeafArgs la;
+  la.transposed = transposed;
   la.tri = h->bem->s->d_tri;
   la.refs = t.d_refs;
   la.leaves = t.d_leaves;
@@ -315,7 +318,8 @@ static int assemble_basis(h2b_h2matrix *h, DevCTree &t, int basis, int dn) {
   la.ns = (int) h->ns;
   int rc = h2b_far_leaf_basis(&la, basis == H2B_BASIS_LINEAR, dn, h->st);
   if (rc != H2B_OK) return rc;
-  FarTransferArgs ta{t.d_nonroot, t.d_father, t.d_pts, t.d_E, t.n - 1, (int) h->m, (int) h->k};
+  FarTransferArgs ta{t.d_nonroot, t.d_father, t.d_pts, t.d_E, t.n - 1, (int) h->m, (int) h->k,
+                     transposed};
   return h2b_far_transfer(&ta, h->st);
 }
 
@@ -527,6 +531,22 @@ extern "C" int h2b_h2matrix_export(const h2b_h2matrix *h, int part, uint32_t cou
   if (out && n) {
     H2B_CUDA_TRY(cudaMemcpyAsync(out, src, sizeof(double) * n, cudaMemcpyDeviceToHost, h->st));
     H2B_CUDA_TRY(cudaStreamSynchronize(h->st));
+    if (part == 2 || part == 3) {
+      // the column basis is stored transposed on the device: return H2Lib's layout
+      const h2b_ctree &c = h->tree->col;
+      std::vector<double> tmp;
+      uint64_t pos = 0;
+      uint32_t got = 0;
+      for (uint32_t i = (part == 2 ? 0 : 1); i < c.n && got < count && pos < n; i++) {
+        if (part == 2 && c.sons[i] != 0) continue;
+        const uint64_t rows = part == 2 ? c.size[i] : h->k, k = h->k;
+        tmp.assign(out + pos, out + pos + rows * k);
+        for (uint64_t r = 0; r < rows; r++)
+          for (uint64_t nu = 0; nu < k; nu++) out[pos + r + nu * rows] = tmp[nu + r * k];
+        pos += rows * k;
+        got++;
+      }
+    }
   }
   return H2B_OK;
 }

@@ -330,6 +330,29 @@ __global__ void l2err_kernel(HarmArgs a, const double *u, double *out) {
   }
 }
 
+// b[t] = coef * g_t * sum_q w_q exp(i kvec . (x_q - src))  (integrate_bem3d_c_avector,
+// Library/bem3d.c:8579, with rhs_dirichlet_plane_helmholtzbem3d, Library/helmholtzbem3d.c:1611)
+__global__ void plane_wave_kernel(HarmArgs a, double k0, double k1, double k2, double cre,
+                                  double cim, double *b) {
+  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= a.nt) return;
+  const TriRec &T = a.tri[t];
+  double sr = 0.0, si = 0.0;
+  for (int q = 0; q < a.ns; q++) {
+    double X[3];
+    tri_point(T, a.xs[q], a.ys[q], X);
+    const double ph = k0 * (X[0] - a.z0) + k1 * (X[1] - a.z1) + k2 * (X[2] - a.z2);
+    double s, c;
+    sincos(ph, &s, &c);
+    sr += a.ws[q] * c;
+    si += a.ws[q] * s;
+  }
+  sr *= T.g;
+  si *= T.g;
+  b[2 * t] = cre * sr - cim * si;
+  b[2 * t + 1] = cre * si + cim * sr;
+}
+
 int harm_args(const h2b_bem *bem, const double z[3], double *scratch, HarmArgs *a,
               cudaStream_t st) {
   const h2b_quad &qd = bem->quad;
@@ -428,5 +451,29 @@ extern "C" int h2b_l2_error_harmonic(const h2b_bem *bem, const double z[3], cons
   H2B_CUDA_TRY(cudaStreamSynchronize(st));
   *err = sqrt(h[0]);
   *norm = sqrt(h[1]);
+  return H2B_OK;
+}
+
+extern "C" int h2b_integrate_plane_wave(const h2b_bem *bem, const double kvec[3],
+                                        const double src[3], double coef_re, double coef_im,
+                                        double *b) {
+  if (!bem || !kvec || !src || !b || bem->row_basis != H2B_BASIS_CONSTANT) {
+    h2b_set_error("h2b_integrate_plane_wave: needs an operator with a constant row basis");
+    return H2B_ERR_ARG;
+  }
+  const h2b_surface *s = bem->s;
+  cudaStream_t st = s->stream;
+  DevBuf buf;
+  buf.st = st;
+  H2B_CUDA_TRY(cudaMallocAsync(&buf.p, sizeof(double) * (2 * (size_t) s->nt + 6 * 64), st));
+  double *db = (double *) buf.p, *rule = db + 2 * (size_t) s->nt;
+  HarmArgs a;
+  int rc = harm_args(bem, src, rule, &a, st);
+  if (rc != H2B_OK) return rc;
+  plane_wave_kernel<<<(s->nt + 127) / 128, 128, 0, st>>>(a, kvec[0], kvec[1], kvec[2], coef_re,
+                                                          coef_im, db);
+  H2B_CUDA_TRY(cudaGetLastError());
+  H2B_CUDA_TRY(cudaMemcpyAsync(b, db, sizeof(double) * 2 * s->nt, cudaMemcpyDefault, st));
+  H2B_CUDA_TRY(cudaStreamSynchronize(st));
   return H2B_OK;
 }

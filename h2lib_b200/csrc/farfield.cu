@@ -43,10 +43,15 @@ __device__ __forceinline__ double dlagr1(double x, const double *xi, int mu, int
 }
 
 // Leaf bases.  Rows of leaf c: its triangles (constant basis) or vertices (linear basis).
-// trl: TriRef list of the triangles touching the cluster (linear basis) with local row indices;
-// for the constant basis the list holds the cluster's own triangles with l[0] = row.
-// Shared memory: the cluster's V block (rows x k doubles) accumulated by atomics, plus the
-// 1D Lagrange values of one triangle batch.
+// The CTA's triangle list (TriRef, local row indices) is processed in batches of BATCH
+// triangles: first the one-dimensional Lagrange values (and derivatives) at every quadrature
+// point of the batch are tabulated in shared memory (3 axes x m), then each (triangle, nu) work
+// item forms the tensor products from the table.  The cluster's V block (rows x k) is
+// accumulated in shared memory (atomics for the linear basis, where a vertex receives the
+// integrals of all triangles around it) and written once.
+constexpr int BATCH = 32;
+constexpr int NSMAX = 64;   // single-triangle rule points (q^2, q <= 8)
+
 template <bool LINEAR, bool DN>
 __global__ void __launch_bounds__(256) leaf_basis_kernel(FarLeafArgs a) {
   extern __shared__ double smem[];
@@ -55,57 +60,76 @@ __global__ void __launch_bounds__(256) leaf_basis_kernel(FarLeafArgs a) {
   const int m = a.m, k = a.k;
   const uint32_t rows = a.size[c];
   const uint32_t tr0 = a.tr_off[leaf], ntr = a.tr_len[leaf];
-  const double *px = a.pts + (size_t) c * 3 * m, *py = px + m, *pz = px + 2 * m;
-  double *V = smem;  // rows * k
+  const double *pts = a.pts + (size_t) c * 3 * m;
   const int ns = a.ns;
+  double *V = smem;                                   // rows * k
+  double *tab = V + (size_t) rows * k;                // BATCH * ns * 3 * m  (values)
+  double *dtab = tab + (size_t) BATCH * ns * 3 * m;   // same size (derivatives, DN only)
   for (uint32_t e = threadIdx.x; e < rows * (uint32_t) k; e += blockDim.x) V[e] = 0.0;
-  __syncthreads();
 
-  // work item = (triangle, nu)
-  const uint32_t items = ntr * (uint32_t) k;
-  for (uint32_t it = threadIdx.x; it < items; it += blockDim.x) {
-    const uint32_t s = it / (uint32_t) k;
-    const int nu = (int) (it - s * (uint32_t) k);
-    const int jx = nu / (m * m), jy = (nu / m) % m, jz = nu % m;
-    const TriRef r = a.refs[tr0 + s];
-    const TriRec &T = a.tri[r.t];
-    double sum[3] = {0.0, 0.0, 0.0};
-    for (int q = 0; q < ns; q++) {
+  for (uint32_t b0 = 0; b0 < ntr; b0 += BATCH) {
+    const uint32_t nb = ntr - b0 < (uint32_t) BATCH ? ntr - b0 : (uint32_t) BATCH;
+    __syncthreads();
+    // table: entry ((s * ns + q) * 3 + d) * m + mu
+    for (uint32_t e = threadIdx.x; e < nb * ns * 3 * m; e += blockDim.x) {
+      const int mu = (int) (e % m), d = (int) ((e / m) % 3);
+      const uint32_t sq = e / (3 * m), s = sq / ns, q = sq % ns;
+      const TriRec &T = a.tri[a.refs[tr0 + b0 + s].t];
       const double tx = a.xs[q], sx = a.ys[q];
-      const double Ax = 1.0 - tx, Bx = tx - sx, Cx = sx;
-      double X[3];
+      const double x = T.a[d] * (1.0 - tx) + T.b[d] * (tx - sx) + T.c[d] * sx;
+      const double *xi = pts + d * m;
+      tab[e] = lagr1(x, xi, mu, m);
+      if (DN) dtab[e] = dlagr1(x, xi, mu, m);
+    }
+    __syncthreads();
+    // work item = (triangle in batch, nu)
+    for (uint32_t it = threadIdx.x; it < nb * (uint32_t) k; it += blockDim.x) {
+      const uint32_t s = it / (uint32_t) k;
+      const int nu = (int) (it - s * (uint32_t) k);
+      const int jx = nu / (m * m), jy = (nu / m) % m, jz = nu % m;
+      const TriRef r = a.refs[tr0 + b0 + s];
+      const TriRec &T = a.tri[r.t];
+      double sum[3] = {0.0, 0.0, 0.0};
+      for (int q = 0; q < ns; q++) {
+        const double *t3 = tab + ((size_t) s * ns + q) * 3 * m;
+        const double lx = t3[jx], ly = t3[m + jy], lz = t3[2 * m + jz];
+        double val;
+        if (!DN) {
+          val = lx * ly * lz;
+        } else {
+          const double *d3 = dtab + ((size_t) s * ns + q) * 3 * m;
+          val = T.n[0] * (d3[jx] * ly * lz) + T.n[1] * (lx * d3[m + jy] * lz) +
+                T.n[2] * (lx * ly * d3[2 * m + jz]);
+        }
+        if (LINEAR) {
 #pragma unroll
-      for (int d = 0; d < 3; d++) X[d] = T.a[d] * Ax + T.b[d] * Bx + T.c[d] * Cx;
-      double val;
-      if (!DN) {
-        val = lagr1(X[0], px, jx, m) * lagr1(X[1], py, jy, m) * lagr1(X[2], pz, jz, m);
-      } else {
-        const double lx = lagr1(X[0], px, jx, m), ly = lagr1(X[1], py, jy, m),
-                     lz = lagr1(X[2], pz, jz, m);
-        val = T.n[0] * (dlagr1(X[0], px, jx, m) * ly * lz) +
-              T.n[1] * (lx * dlagr1(X[1], py, jy, m) * lz) +
-              T.n[2] * (lx * ly * dlagr1(X[2], pz, jz, m));
+          for (int l = 0; l < 3; l++) sum[l] += a.wsl[l * ns + q] * val;
+        } else {
+          sum[0] += a.ws[q] * val;
+        }
       }
       if (LINEAR) {
 #pragma unroll
-        for (int l = 0; l < 3; l++) sum[l] += a.wsl[l * ns + q] * val;
+        for (int l = 0; l < 3; l++) {
+          const int row = r.l[l];
+          if (row >= 0) atomicAdd(&V[row + (uint32_t) nu * rows], sum[l] * T.g);
+        }
       } else {
-        sum[0] += a.ws[q] * val;
+        V[r.l[0] + (uint32_t) nu * rows] = T.g * sum[0];
       }
-    }
-    if (LINEAR) {
-#pragma unroll
-      for (int l = 0; l < 3; l++) {
-        const int row = r.l[l];
-        if (row >= 0) atomicAdd(&V[row + (uint32_t) nu * rows], sum[l] * T.g);
-      }
-    } else {
-      V[r.l[0] + (uint32_t) nu * rows] = T.g * sum[0];
     }
   }
   __syncthreads();
   double *out = a.V + a.voff[c];
-  for (uint32_t e = threadIdx.x; e < rows * (uint32_t) k; e += blockDim.x) out[e] = V[e];
+  if (a.transposed) {
+    // V^T, k x rows column-major: consecutive threads write consecutive nu
+    for (uint32_t e = threadIdx.x; e < rows * (uint32_t) k; e += blockDim.x) {
+      const uint32_t nu = e % (uint32_t) k, i = e / (uint32_t) k;
+      out[e] = V[i + nu * rows];
+    }
+  } else {
+    for (uint32_t e = threadIdx.x; e < rows * (uint32_t) k; e += blockDim.x) out[e] = V[e];
+  }
 }
 
 // Transfer matrix of every non-root cluster: E_c[i, nu] = L^father_nu(xi^c_i), k x k.
@@ -125,7 +149,11 @@ __global__ void __launch_bounds__(256) transfer_kernel(FarTransferArgs a) {
     const int i = e % k, nu = e / k;
     const int ia = i / (m * m), ib = (i / m) % m, ic = i % m;
     const int jx = nu / (m * m), jy = (nu / m) % m, jz = nu % m;
-    E[e] = L1[0][ia][jx] * L1[1][ib][jy] * L1[2][ic][jz];
+    const double v = L1[0][ia][jx] * L1[1][ib][jy] * L1[2][ic][jz];
+    if (a.transposed)
+      E[nu + (size_t) i * k] = v;
+    else
+      E[e] = v;
   }
 }
 
@@ -160,9 +188,11 @@ __global__ void __launch_bounds__(256) coupling_kernel(FarCouplingArgs a) {
 
 extern "C" int h2b_far_leaf_basis(const FarLeafArgs *a, int linear, int dn, cudaStream_t st) {
   if (a->nleaves == 0) return H2B_OK;
-  const size_t smem = sizeof(double) * (size_t) a->max_rows * a->k;
-  if (smem > 200u * 1024u) {
-    h2b_set_error("leaf basis block of %u x %d exceeds shared memory", a->max_rows, a->k);
+  const size_t smem = sizeof(double) * ((size_t) a->max_rows * a->k +
+                                        2 * (size_t) BATCH * a->ns * 3 * a->m);
+  if (smem > 200u * 1024u || a->ns > NSMAX) {
+    h2b_set_error("leaf basis block of %u x %d (rule of %d points) exceeds shared memory",
+                  a->max_rows, a->k, a->ns);
     return H2B_ERR_ARG;
   }
 #define LAUNCH(L, D)                                                                        \

@@ -20,6 +20,7 @@ struct FarLeafArgs {
   double *V;
   uint32_t nleaves, max_rows;
   int m, k, ns;
+  int transposed;           // store V^T (k x rows) instead of V (rows x k)
 };
 
 struct FarTransferArgs {
@@ -29,6 +30,7 @@ struct FarTransferArgs {
   double *E;                 // (n_clusters - 1) x k x k, cluster c at (c-1)*k*k
   uint32_t n;
   int m, k;
+  int transposed;            // store E^T
 };
 
 struct FarCouplingArgs {

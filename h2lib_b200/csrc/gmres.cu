@@ -253,57 +253,80 @@ __device__ void apply_givens(cd rho, cd *a, cd *b) {
   *b = csub(cmul(c, bb), cmul(s, aa));
 }
 
-// Single-thread bookkeeping kernels (tiny O(k^2) work).
+// Bookkeeping kernels: one CTA of SMALL_THREADS threads (>= kmax); O(k) work per thread for the
+// triangular products, sequential only where the algorithm is (Givens, triangular solve).
+constexpr int SMALL_THREADS = GMRES_KMAX;
+
+__device__ double block_sum_small(double v, double *red) {
+  v = warp_sum(v);
+  __syncthreads();
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+  __syncthreads();
+  double s = 0.0;
+  for (int w = 0; w < SMALL_THREADS / 32; w++) s += red[w];
+  return s;  // valid in every thread
+}
+
 template <bool CX>
-__global__ void small_kernel(GmresDev g, int phase) {
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+__global__ void __launch_bounds__(SMALL_THREADS) small_kernel(GmresDev g, int phase) {
+  __shared__ double zr[GMRES_KMAX], zi[GMRES_KMAX], red[SMALL_THREADS / 32];
   GmresState *s = g.state;
   const uint32_t k = s->k;
   const uint32_t nb = g.nblocks;
+  const uint32_t t = threadIdx.x;
+  __syncthreads();  // every thread has read k before anyone may change it
   if (phase == 0) {
-    // after vth(mode 0): w = V^H a; u = T^H w
-    for (uint32_t j = 0; j <= k; j++) {
-      cd w = sum_parts(g, j, nb);
-      g.w[2 * j] = w.re;
-      g.w[2 * j + 1] = w.im;
+    // after vth: w = V^H a; u = T^H w
+    if (t <= k) {
+      cd w = sum_parts(g, t, nb);
+      zr[t] = w.re;
+      zi[t] = w.im;
+      g.w[2 * t] = w.re;
+      g.w[2 * t + 1] = w.im;
     }
-    for (uint32_t j = 0; j <= k; j++) {
+    __syncthreads();
+    if (t <= k) {
       cd u = {0.0, 0.0};
-      for (uint32_t i = 0; i <= j; i++)
-        u = cadd(u, cmul(cconj(Tij(g, i, j)), cd{g.w[2 * i], g.w[2 * i + 1]}));
-      g.u[2 * j] = u.re;
-      g.u[2 * j + 1] = u.im;
+      for (uint32_t i = 0; i <= t; i++) u = cadd(u, cmul(cconj(Tij(g, i, t)), cd{zr[i], zi[i]}));
+      g.u[2 * t] = u.re;
+      g.u[2 * t + 1] = u.im;
     }
   } else if (phase == 1) {
     // after apply_v_norm: Householder scalars of column k+1, rows >= k+1
-    double norm2 = 0.0;
-    for (uint32_t b = 0; b < nb; b++) norm2 += g.part[(size_t) b * g.ldpart * 2];
-    const double *a = g.qr + (size_t) (CX ? 2 : 1) * (k + 1) * g.n;
-    const cd diag = ld<CX>(a, k + 1);
-    householder(diag, norm2, s, k + 1, g);
+    double part = 0.0;
+    for (uint32_t b = t; b < nb; b += SMALL_THREADS) part += g.part[(size_t) b * g.ldpart * 2];
+    const double norm2 = block_sum_small(part, red);
+    if (t == 0) {
+      const double *a = g.qr + (size_t) (CX ? 2 : 1) * (k + 1) * g.n;
+      householder(ld<CX>(a, k + 1), norm2, s, k + 1, g);
+    }
   } else if (phase == 2) {
     // after scale_vth: T column k+1; u for q; Givens; k += 1
     const cd tau = {g.tau[2 * (k + 1)], g.tau[2 * (k + 1) + 1]};
-    cd z[GMRES_KMAX];
-    for (uint32_t j = 0; j <= k; j++) {
-      z[j] = cadd(sum_parts(g, j, nb), cconj(vij<CX>(g, k + 1, j)));  // + conj(v_j[k+1]) * 1
+    if (t <= k) {
+      const cd z = cadd(sum_parts(g, t, nb), cconj(vij<CX>(g, k + 1, t)));  // + conj(v_t[k+1])
+      zr[t] = z.re;
+      zi[t] = z.im;
     }
-    for (uint32_t i = 0; i <= k; i++) {
-      cd t = {0.0, 0.0};
-      for (uint32_t j = i; j <= k; j++) t = cadd(t, cmul(Tij(g, i, j), z[j]));
-      setT(g, i, k + 1, cmul(cd{-tau.re, -tau.im}, t));
+    __syncthreads();
+    if (t <= k) {
+      cd acc = {0.0, 0.0};
+      for (uint32_t j = t; j <= k; j++) acc = cadd(acc, cmul(Tij(g, t, j), cd{zr[j], zi[j]}));
+      setT(g, t, k + 1, cmul(cd{-tau.re, -tau.im}, acc));
     }
-    setT(g, k + 1, k + 1, tau);
+    if (t == 0) setT(g, k + 1, k + 1, tau);
+    __syncthreads();
     // u = T y, y_j = conj(V[k+1, j]) (j <= k), y_{k+1} = 1
-    for (uint32_t i = 0; i <= k + 1; i++) {
-      cd t = {0.0, 0.0};
-      for (uint32_t j = i; j <= k + 1; j++) {
+    if (t <= k + 1) {
+      cd acc = {0.0, 0.0};
+      for (uint32_t j = t; j <= k + 1; j++) {
         const cd y = j == k + 1 ? cd{1.0, 0.0} : cconj(vij<CX>(g, k + 1, j));
-        t = cadd(t, cmul(Tij(g, i, j), y));
+        acc = cadd(acc, cmul(Tij(g, t, j), y));
       }
-      g.u[2 * i] = t.re;
-      g.u[2 * i + 1] = t.im;
+      g.u[2 * t] = acc.re;
+      g.u[2 * t + 1] = acc.im;
     }
+    if (t != 0) return;
     // Givens rotations on the new Hessenberg column (rows 0..k+1 of column k+1)
     double *col = g.qr + (size_t) (CX ? 2 : 1) * (k + 1) * g.n;
     for (uint32_t i = 0; i < k; i++) {
@@ -326,49 +349,68 @@ __global__ void small_kernel(GmresDev g, int phase) {
     s->k = k + 1;
     s->err = sqrt(cabs2(r1));
   } else if (phase == 3) {
-    // finish: rhat_k = R^{-1} rhat_k; z = V_k^H rhat; u = T_k z
-    cd r[GMRES_KMAX];
-    for (uint32_t j = 0; j < k; j++) r[j] = {g.rhat[2 * j], g.rhat[2 * j + 1]};
+    // finish: rhat_k = R^{-1} rhat_k (back substitution, row by row); z = V_k^H rhat;
+    // u = T_k z
+    if (t < k) {
+      zr[t] = g.rhat[2 * t];
+      zi[t] = g.rhat[2 * t + 1];
+    }
+    __syncthreads();
     for (uint32_t jj = k; jj-- > 0;) {
-      cd acc = r[jj];
-      for (uint32_t i = jj + 1; i < k; i++)
-        acc = csub(acc, cmul(ld<CX>(g.qr + (size_t) (CX ? 2 : 1) * (i + 1) * g.n, jj), r[i]));
-      r[jj] = cdiv(acc, ld<CX>(g.qr + (size_t) (CX ? 2 : 1) * (jj + 1) * g.n, jj));
+      if (t == 0) {
+        const cd r = cdiv(cd{zr[jj], zi[jj]}, ld<CX>(g.qr + (size_t) (CX ? 2 : 1) * (jj + 1) * g.n, jj));
+        zr[jj] = r.re;
+        zi[jj] = r.im;
+      }
+      __syncthreads();
+      // eliminate the solved unknown from the rows above (column jj+1 of R)
+      if (t < jj) {
+        const cd v = cmul(ld<CX>(g.qr + (size_t) (CX ? 2 : 1) * (jj + 1) * g.n, t), cd{zr[jj], zi[jj]});
+        zr[t] -= v.re;
+        zi[t] -= v.im;
+      }
+      __syncthreads();
     }
-    for (uint32_t j = 0; j < k; j++) {
-      g.rhat[2 * j] = r[j].re;
-      g.rhat[2 * j + 1] = r[j].im;
+    if (t < k) {
+      g.rhat[2 * t] = zr[t];
+      g.rhat[2 * t + 1] = zi[t];
     }
-    cd z[GMRES_KMAX];
-    for (uint32_t j = 0; j < k; j++) {
-      cd acc = r[j];
-      for (uint32_t i = j + 1; i < k; i++) acc = cadd(acc, cmul(cconj(vij<CX>(g, i, j)), r[i]));
-      z[j] = acc;
+    __shared__ double wr[GMRES_KMAX], wi[GMRES_KMAX];
+    if (t < k) {
+      cd acc = {zr[t], zi[t]};
+      for (uint32_t i = t + 1; i < k; i++) acc = cadd(acc, cmul(cconj(vij<CX>(g, i, t)), cd{zr[i], zi[i]}));
+      wr[t] = acc.re;
+      wi[t] = acc.im;
     }
-    for (uint32_t i = 0; i < k; i++) {
-      cd t = {0.0, 0.0};
-      for (uint32_t j = i; j < k; j++) t = cadd(t, cmul(Tij(g, i, j), z[j]));
-      g.u[2 * i] = t.re;
-      g.u[2 * i + 1] = t.im;
+    __syncthreads();
+    if (t < k) {
+      cd acc = {0.0, 0.0};
+      for (uint32_t j = t; j < k; j++) acc = cadd(acc, cmul(Tij(g, t, j), cd{wr[j], wi[j]}));
+      g.u[2 * t] = acc.re;
+      g.u[2 * t + 1] = acc.im;
     }
-  } else if (phase == 4) {
-    // init: Householder scalars of column 0 from ||r||^2 (in part[b][0])
-    double norm2 = 0.0;
-    for (uint32_t b = 0; b < nb; b++) norm2 += g.part[(size_t) b * g.ldpart * 2];
-    householder(ld<CX>(g.qr, 0), norm2, s, 0, g);
+  } else if (phase == 4 || phase == 6) {
+    // ||r||^2 (init, Householder of column 0) or ||b||^2, from part[b][0]
+    double part = 0.0;
+    for (uint32_t b = t; b < nb; b += SMALL_THREADS) part += g.part[(size_t) b * g.ldpart * 2];
+    const double norm2 = block_sum_small(part, red);
+    if (t == 0) {
+      if (phase == 4)
+        householder(ld<CX>(g.qr, 0), norm2, s, 0, g);
+      else
+        s->bnorm = sqrt(norm2);
+    }
   } else if (phase == 5) {
     // init, after scaling column 0: T, rhat, k, err
-    for (uint32_t i = 0; i < 2 * (g.kmax + 1); i++) g.rhat[i] = 0.0;
-    g.rhat[0] = s->alpha_re;
-    g.rhat[1] = s->alpha_im;
-    setT(g, 0, 0, cd{g.tau[0], g.tau[1]});
-    s->k = 0;
-    s->err = sqrt(s->alpha_re * s->alpha_re + s->alpha_im * s->alpha_im);
-  } else if (phase == 6) {
-    // ||b||: sum of partial squares (part[b][0])
-    double norm2 = 0.0;
-    for (uint32_t b = 0; b < nb; b++) norm2 += g.part[(size_t) b * g.ldpart * 2];
-    s->bnorm = sqrt(norm2);
+    for (uint32_t i = t; i < 2 * (g.kmax + 1); i += SMALL_THREADS) g.rhat[i] = 0.0;
+    __syncthreads();
+    if (t == 0) {
+      g.rhat[0] = s->alpha_re;
+      g.rhat[1] = s->alpha_im;
+      setT(g, 0, 0, cd{g.tau[0], g.tau[1]});
+      s->k = 0;
+      s->err = sqrt(s->alpha_re * s->alpha_re + s->alpha_im * s->alpha_im);
+    }
   }
 }
 
@@ -440,11 +482,11 @@ int step_impl(const GmresDev &g, const GmresOp &op, cudaStream_t st) {
   int rc = op.apply(op.ctx, g.q, g.abuf, 1.0, 0.0, st);
   if (rc != H2B_OK) return rc;
   vth_kernel<CX><<<nb, TPB, 0, st>>>(g);
-  small_kernel<CX><<<1, 32, 0, st>>>(g, 0);
+  small_kernel<CX><<<1, SMALL_THREADS, 0, st>>>(g, 0);
   apply_v_norm_kernel<CX><<<nb, TPB, 0, st>>>(g);
-  small_kernel<CX><<<1, 32, 0, st>>>(g, 1);
+  small_kernel<CX><<<1, SMALL_THREADS, 0, st>>>(g, 1);
   scale_vth_kernel<CX><<<nb, TPB, 0, st>>>(g);
-  small_kernel<CX><<<1, 32, 0, st>>>(g, 2);
+  small_kernel<CX><<<1, SMALL_THREADS, 0, st>>>(g, 2);
   make_q_kernel<CX><<<nb, TPB, 0, st>>>(g);
   H2B_CUDA_TRY(cudaGetLastError());
   return H2B_OK;
@@ -458,9 +500,9 @@ int init_impl(const GmresDev &g, const GmresOp &op, const double *b, double *x, 
   int rc = op.apply(op.ctx, x, g.qr, -1.0, 0.0, st);
   if (rc != H2B_OK) return rc;
   norm0_kernel<CX><<<nb, TPB, 0, st>>>(g);
-  small_kernel<CX><<<1, 32, 0, st>>>(g, 4);
+  small_kernel<CX><<<1, SMALL_THREADS, 0, st>>>(g, 4);
   scale0_kernel<CX><<<nb, TPB, 0, st>>>(g);
-  small_kernel<CX><<<1, 32, 0, st>>>(g, 5);
+  small_kernel<CX><<<1, SMALL_THREADS, 0, st>>>(g, 5);
   H2B_CUDA_TRY(cudaGetLastError());
   return H2B_OK;
 }
@@ -469,7 +511,7 @@ template <bool CX>
 int finish_impl(const GmresDev &g, const GmresOp &op, const double *b, double *x,
                 cudaStream_t st) {
   const uint32_t nb = g.nblocks;
-  small_kernel<CX><<<1, 32, 0, st>>>(g, 3);
+  small_kernel<CX><<<1, SMALL_THREADS, 0, st>>>(g, 3);
   update_x_kernel<CX><<<nb, TPB, 0, st>>>(g, x);
   H2B_CUDA_TRY(cudaGetLastError());
   return init_impl<CX>(g, op, b, x, st);
@@ -478,7 +520,7 @@ int finish_impl(const GmresDev &g, const GmresOp &op, const double *b, double *x
 template <bool CX>
 int bnorm_impl(const GmresDev &g, const double *b, cudaStream_t st) {
   copy_b_kernel<CX><<<g.nblocks, TPB, 0, st>>>(g, b);
-  small_kernel<CX><<<1, 32, 0, st>>>(g, 6);
+  small_kernel<CX><<<1, SMALL_THREADS, 0, st>>>(g, 6);
   H2B_CUDA_TRY(cudaGetLastError());
   return H2B_OK;
 }

@@ -5,12 +5,19 @@
 //   coupling / near     yt_t += S_b xt_s,  y_t += N_b x_s      (fastaddeval, Library/h2matrix.c:1211)
 //   backward transform  yt_s += E_s yt_t,  y_t += V_t yt_t     (Library/clusterbasis.c:749)
 // Vectors are kept in cluster order (xp[i] = x[idx[i]]) so that every cluster's entries are
-// contiguous.  The forward transform is one launch: a CTA per leaf, and the CTA that finishes
-// the last son of a cluster continues with the father (an atomic arrival counter per cluster,
-// reset by that CTA), so no CTA ever waits for another.  Coupling and nearfield blocks share one
-// launch (a CTA per block, results added with FP64 atomics).  The backward transform runs level
-// by level from the root; the leaf level adds V_t yt_t.  All kernels are memory-bound GEMVs:
-// column-major panels are read with consecutive threads on consecutive rows.
+// contiguous.  Three launches do the work:
+//   1. forward + nearfield: CTAs [0, leaves) compute xt of their leaf, and the CTA that finishes
+//      the last son of a cluster continues with the father (an atomic arrival counter per
+//      cluster, reset by that CTA), so no CTA ever waits for another; CTAs [leaves, leaves +
+//      nearfield blocks) add N_b x_s into yp meanwhile (the nearfield does not need xt);
+//   2. coupling: a CTA per admissible block adds S_b xt_s into yt (FP64 atomics);
+//   3. backward: a CTA per leaf walks its root-to-leaf path (upper transfers recomputed per leaf,
+//      read from L2) and adds V_t yt_t.
+// The column cluster basis is stored transposed (V^T: k x rows, E^T: k x k, both column-major)
+// so that the forward GEMVs read consecutive addresses with consecutive threads; the row basis is
+// stored as H2Lib does (V: rows x k, E: k x k).  Every GEMV splits its reduction over G = 256 / k
+// thread groups and combines the partial sums in shared memory, which keeps 256 loads in flight
+// per CTA instead of one dependent chain.
 // CX: complex coefficients (Helmholtz) — S, N, x, y complex (interleaved); V, E real.
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -20,23 +27,10 @@
 
 namespace {
 
-template <bool CX> struct Val;
-template <> struct Val<false> {
-  double v;
-  __device__ static Val zero() { return Val{0.0}; }
-};
-template <> struct Val<true> {
-  double re, im;
-  __device__ static Val zero() { return Val{0.0, 0.0}; }
-};
+constexpr int TPB = 256;
+constexpr int KMAXW = 2 * 128;  // k <= 128 complex coefficients
 
-__device__ __forceinline__ void vadd_atomic(double *p, const Val<false> &v) { atomicAdd(p, v.v); }
-__device__ __forceinline__ void vadd_atomic(double *p, const Val<true> &v) {
-  atomicAdd(p, v.re);
-  atomicAdd(p + 1, v.im);
-}
-
-// xp = x[idx] (cluster order); clears nothing else
+// xp = x[idx] (cluster order)
 template <bool CX>
 __global__ void gather_kernel(const double *__restrict__ x, const uint32_t *__restrict__ idx,
                               double *__restrict__ xp, uint32_t n) {
@@ -67,87 +61,60 @@ __global__ void scatter_kernel(const double *__restrict__ yp, const uint32_t *__
   }
 }
 
-// out[nu] = sum_i P[i + nu*rows] * v[i] for nu < k: warp per column, lanes over rows.
-template <bool CX>
-__device__ __forceinline__ void panel_tmv(const double *__restrict__ P, uint32_t rows, int k,
-                                          const double *__restrict__ v, double *__restrict__ out) {
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  for (int nu = warp; nu < k; nu += nw) {
-    const double *col = P + (size_t) nu * rows;
-    double sr = 0.0, si = 0.0;
-    for (uint32_t i = lane; i < rows; i += 32) {
-      const double p = col[i];
-      // v may have been written by another CTA of this launch: read through L2
-      if (CX) {
-        sr = fma(p, __ldcg(v + 2 * i), sr);
-        si = fma(p, __ldcg(v + 2 * i + 1), si);
-      } else {
-        sr = fma(p, __ldcg(v + i), sr);
-      }
-    }
-    sr = warp_sum(sr);
-    if (CX) si = warp_sum(si);
-    if (lane == 0) {
-      if (CX) {
-        out[2 * nu] = sr;
-        out[2 * nu + 1] = si;
-      } else {
-        out[nu] = sr;
-      }
-    }
-  }
-}
-
-template <bool CX>
-__global__ void __launch_bounds__(256) forward_kernel(MvmForwardArgs a) {
-  const int k = a.k;
+// out[r] = sum_{c < ncols} P[r + c*ld] * v[c] for r < nrows (P column-major, real), v complex if
+// CX.  Threads: r = t % nrows, group g = t / nrows takes the columns c = g mod G.  The result is
+// written to `out` (shared or global) by the group-0 threads; `red` holds G * nrows * W doubles.
+// All threads of the CTA must call it (it synchronises).  With VGLOBAL, `v` is a global array
+// read through L2 (it may have been written by another CTA of the same launch); otherwise `v`
+// is in shared memory.
+template <bool CX, bool VGLOBAL>
+__device__ __forceinline__ void gemv_split(const double *__restrict__ P, uint32_t ld,
+                                           uint32_t nrows, uint32_t ncols,
+                                           const double *__restrict__ v, double *red,
+                                           double *out) {
   constexpr int W = CX ? 2 : 1;
-  __shared__ double tmp[2 * 2 * 128];  // two sons' contributions (k <= 128, complex)
-  __shared__ int last;
-  uint32_t c = a.leaves[blockIdx.x];
-  // leaf: xt_c = V_c^T xp[off .. off + size)
-  panel_tmv<CX>(a.V + a.voff[c], a.size[c], k, a.xp + (size_t) W * a.off[c],
-                a.xt + (size_t) W * k * c);
-  // climb while this CTA completes the last son of the father
-  while (true) {
-    __syncthreads();
-    const uint32_t f = a.father[c];
-    if (f == UINT32_MAX) return;
-    if (threadIdx.x == 0) {
-      __threadfence();
-      const unsigned old = atomicAdd(&a.counter[f], 1u);
-      last = (old == 1u);
-      if (last) a.counter[f] = 0u;  // reset for the next product
-      __threadfence();
+  const uint32_t G = blockDim.x / nrows;
+  const uint32_t t = threadIdx.x, r = t % nrows, g = t / nrows;
+  double sr = 0.0, si = 0.0;
+  if (g < G) {
+#pragma unroll 4
+    for (uint32_t c = g; c < ncols; c += G) {
+      const double p = P[r + (size_t) c * ld];
+      const double vr = VGLOBAL ? __ldcg(v + W * c) : v[W * c];
+      sr = fma(p, vr, sr);
+      if (CX) si = fma(p, VGLOBAL ? __ldcg(v + W * c + 1) : v[W * c + 1], si);
     }
-    __syncthreads();
-    if (!last) return;
-    // xt_f = E_s0^T xt_s0 + E_s1^T xt_s1 (k x k transfers, column-major, rows = son points)
-    const uint32_t s0 = a.son0[f], s1 = a.son1[f];
-    panel_tmv<CX>(a.E + (size_t) (s0 - 1) * k * k, (uint32_t) k, k,
-                  a.xt + (size_t) W * k * s0, tmp);
-    panel_tmv<CX>(a.E + (size_t) (s1 - 1) * k * k, (uint32_t) k, k,
-                  a.xt + (size_t) W * k * s1, tmp + W * k);
-    __syncthreads();
-    for (int e = threadIdx.x; e < W * k; e += blockDim.x)
-      a.xt[(size_t) W * k * f + e] = tmp[e] + tmp[W * k + e];
-    c = f;
+    red[W * (g * nrows + r)] = sr;
+    if (CX) red[W * (g * nrows + r) + 1] = si;
   }
+  __syncthreads();
+  if (t < nrows) {
+    double ar = 0.0, ai = 0.0;
+    for (uint32_t h = 0; h < G; h++) {
+      ar += red[W * (h * nrows + t)];
+      if (CX) ai += red[W * (h * nrows + t) + 1];
+    }
+    out[W * t] = ar;
+    if (CX) out[W * t + 1] = ai;
+  }
+  __syncthreads();
 }
 
-// y_rows += M x_cols for a column-major rows x cols panel M (ld = rows); atomics on the output.
+// y_rows += M x_cols for a column-major rows x cols panel M (ld = rows, complex if CX).  The
+// column groups' partial sums are combined in shared memory (`red`, blockDim * W doubles), so
+// each output row receives one atomic addition per block.  All threads must call it.
 template <bool CX>
 __device__ __forceinline__ void panel_mv_atomic(const double *__restrict__ M, uint32_t rows,
                                                 uint32_t cols, const double *__restrict__ xv,
-                                                double *__restrict__ yv) {
+                                                double *__restrict__ yv, double *red) {
   constexpr int W = CX ? 2 : 1;
-  // threads: row r = t % rows_per, column group g = t / rows_per
-  const uint32_t rb = rows < 64 ? rows : 64;   // rows per pass
+  const uint32_t rb = rows < 64 ? rows : 64;  // rows per pass
   const uint32_t groups = blockDim.x / rb;
   for (uint32_t r0 = 0; r0 < rows; r0 += rb) {
-    const uint32_t r = r0 + threadIdx.x % rb, g = threadIdx.x / rb;
+    const uint32_t rl = threadIdx.x % rb, r = r0 + rl, g = threadIdx.x / rb;
     if (g < groups && r < rows) {
       double sr = 0.0, si = 0.0;
+#pragma unroll 4
       for (uint32_t j = g; j < cols; j += groups) {
         const size_t e = (size_t) r + (size_t) j * rows;
         if (CX) {
@@ -158,72 +125,124 @@ __device__ __forceinline__ void panel_mv_atomic(const double *__restrict__ M, ui
           sr = fma(M[e], xv[j], sr);
         }
       }
-      atomicAdd(&yv[W * r], sr);
-      if (CX) atomicAdd(&yv[W * r + 1], si);
+      red[W * (g * rb + rl)] = sr;
+      if (CX) red[W * (g * rb + rl) + 1] = si;
     }
+    __syncthreads();
+    if (threadIdx.x < rb && r0 + threadIdx.x < rows) {
+      double ar = 0.0, ai = 0.0;
+      for (uint32_t h = 0; h < groups; h++) {
+        ar += red[W * (h * rb + threadIdx.x)];
+        if (CX) ai += red[W * (h * rb + threadIdx.x) + 1];
+      }
+      atomicAdd(&yv[W * (r0 + threadIdx.x)], ar);
+      if (CX) atomicAdd(&yv[W * (r0 + threadIdx.x) + 1], ai);
+    }
+    __syncthreads();
   }
 }
 
+// Launch 1: forward transform (CTAs < nleaves) and nearfield blocks (the other CTAs).
 template <bool CX>
-__global__ void __launch_bounds__(256) couple_near_kernel(MvmCoupleArgs a) {
+__global__ void __launch_bounds__(TPB) forward_near_kernel(MvmForwardArgs a, MvmCoupleArgs c) {
   constexpr int W = CX ? 2 : 1;
+  __shared__ double red[TPB * W];
+  __shared__ double tmp[2 * KMAXW];
+  __shared__ int last;
+  if (blockIdx.x >= a.nleaves) {
+    const uint32_t nb = blockIdx.x - a.nleaves;
+    const uint32_t r = c.near_rc[nb], cc = c.near_cc[nb];
+    panel_mv_atomic<CX>(c.N + (size_t) W * c.near_off[nb], c.rsize[r], c.csize[cc],
+                        c.xp + (size_t) W * c.coff[cc], c.yp + (size_t) W * c.roff[r], red);
+    return;
+  }
+  const uint32_t k = (uint32_t) a.k;
+  uint32_t cl = a.leaves[blockIdx.x];
+  // leaf: xt_c = V_c^T xp[off .. off + size): V^T stored k x size (ld = k)
+  gemv_split<CX, true>(a.V + a.voff[cl], k, k, a.size[cl], a.xp + (size_t) W * a.off[cl], red,
+                       a.xt + (size_t) W * k * cl);
+  // climb while this CTA completes the last son of the father
+  while (true) {
+    const uint32_t f = a.father[cl];
+    if (f == UINT32_MAX) return;
+    __threadfence();  // this CTA's xt writes are visible device-wide before it arrives
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      const unsigned old = atomicAdd(&a.counter[f], 1u);
+      last = (old == 1u);
+      if (last) a.counter[f] = 0u;  // reset for the next product
+    }
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    // xt_f = E_s0^T xt_s0 + E_s1^T xt_s1: both E^T panels are k x k (ld = k)
+    const uint32_t s0 = a.son0[f], s1 = a.son1[f];
+    gemv_split<CX, true>(a.E + (size_t) (s0 - 1) * k * k, k, k, k, a.xt + (size_t) W * k * s0,
+                         red, tmp);
+    gemv_split<CX, true>(a.E + (size_t) (s1 - 1) * k * k, k, k, k, a.xt + (size_t) W * k * s1,
+                         red, tmp + W * k);
+    for (uint32_t e = threadIdx.x; e < W * k; e += blockDim.x)
+      a.xt[(size_t) W * k * f + e] = tmp[e] + tmp[W * k + e];
+    cl = f;
+  }
+}
+
+// Launch 2: coupling blocks yt_r += S_b xt_c.
+template <bool CX>
+__global__ void __launch_bounds__(TPB) coupling_mv_kernel(MvmCoupleArgs a) {
+  constexpr int W = CX ? 2 : 1;
+  __shared__ double red[TPB * W];
   const uint32_t b = blockIdx.x;
   const uint32_t k = (uint32_t) a.k;
-  if (b < a.nadm) {
-    panel_mv_atomic<CX>(a.S + (size_t) W * k * k * b, k, k, a.xt + (size_t) W * k * a.adm_cc[b],
-                        a.yt + (size_t) W * k * a.adm_rc[b]);
-  } else {
-    const uint32_t nb = b - a.nadm;
-    const uint32_t r = a.near_rc[nb], c = a.near_cc[nb];
-    panel_mv_atomic<CX>(a.N + (size_t) W * a.near_off[nb], a.rsize[r], a.csize[c],
-                        a.xp + (size_t) W * a.coff[c], a.yp + (size_t) W * a.roff[r]);
-  }
+  panel_mv_atomic<CX>(a.S + (size_t) W * k * k * b, k, k, a.xt + (size_t) W * k * a.adm_cc[b],
+                      a.yt + (size_t) W * k * a.adm_rc[b], red);
 }
 
-// yt_c += E_c yt_father(c) for the clusters of one level (E_c: k x k, rows = c's points).
+// Launch 3: backward transform, a CTA per row leaf walking root -> leaf:
+// t_root = yt_root, t_c = yt_c + E_c t_father(c) (the recursion of backward_clusterbasis_avector,
+// Library/clusterbasis.c:749), then yp[leaf rows] += V_leaf t_leaf.
 template <bool CX>
-__global__ void __launch_bounds__(256) downsweep_kernel(MvmDownArgs a) {
+__global__ void __launch_bounds__(TPB) backward_chain_kernel(MvmBackArgs a, const uint32_t *father,
+                                                             const double *E) {
   constexpr int W = CX ? 2 : 1;
-  const uint32_t c = a.clusters[blockIdx.x];
-  const uint32_t f = a.father[c];
-  const int k = a.k;
-  __shared__ double yf[2 * 128];
-  for (int e = threadIdx.x; e < W * k; e += blockDim.x) yf[e] = a.yt[(size_t) W * k * f + e];
-  __syncthreads();
-  const double *E = a.E + (size_t) (c - 1) * k * k;
-  for (int i = threadIdx.x; i < k; i += blockDim.x) {
-    double sr = 0.0, si = 0.0;
-    for (int j = 0; j < k; j++) {
-      const double e = E[i + (size_t) j * k];
-      sr = fma(e, yf[W * j], sr);
-      if (CX) si = fma(e, yf[W * j + 1], si);
+  __shared__ double red[TPB * W];
+  __shared__ double tcur[KMAXW], tnew[KMAXW];
+  __shared__ uint32_t path[64];
+  __shared__ int depth;
+  const uint32_t leaf = a.leaves[blockIdx.x];
+  const uint32_t k = (uint32_t) a.k;
+  if (threadIdx.x == 0) {
+    int d = 0;
+    uint32_t c = leaf;
+    while (c != UINT32_MAX && d < 64) {
+      path[d++] = c;
+      c = father[c];
     }
-    a.yt[(size_t) W * k * c + W * i] += sr;
-    if (CX) a.yt[(size_t) W * k * c + W * i + 1] += si;
+    depth = d;  // path[d-1] is the root
   }
-}
-
-// yp[off + i] += sum_nu V_c[i, nu] yt_c[nu] for every row leaf.
-template <bool CX>
-__global__ void __launch_bounds__(256) backward_leaf_kernel(MvmBackArgs a) {
-  constexpr int W = CX ? 2 : 1;
-  const uint32_t c = a.leaves[blockIdx.x];
-  const int k = a.k;
-  const uint32_t rows = a.size[c];
-  __shared__ double yc[2 * 128];
-  for (int e = threadIdx.x; e < W * k; e += blockDim.x) yc[e] = a.yt[(size_t) W * k * c + e];
   __syncthreads();
-  const double *V = a.V + a.voff[c];
-  double *yp = a.yp + (size_t) W * a.off[c];
-  for (uint32_t i = threadIdx.x; i < rows; i += blockDim.x) {
-    double sr = 0.0, si = 0.0;
-    for (int nu = 0; nu < k; nu++) {
-      const double v = V[i + (size_t) nu * rows];
-      sr = fma(v, yc[W * nu], sr);
-      if (CX) si = fma(v, yc[W * nu + 1], si);
+  const int d = depth;
+  for (uint32_t e = threadIdx.x; e < W * k; e += blockDim.x)
+    tcur[e] = a.yt[(size_t) W * k * path[d - 1] + e];
+  __syncthreads();
+  for (int l = d - 2; l >= 0; l--) {
+    const uint32_t c = path[l];
+    gemv_split<CX, false>(E + (size_t) (c - 1) * k * k, k, k, k, tcur, red, tnew);
+    for (uint32_t e = threadIdx.x; e < W * k; e += blockDim.x)
+      tcur[e] = tnew[e] + a.yt[(size_t) W * k * c + e];
+    __syncthreads();
+  }
+  // yp[off + i] += sum_nu V[i, nu] t[nu]  (V: rows x k, ld = rows)
+  const uint32_t rows = a.size[leaf];
+  double *yp = a.yp + (size_t) W * a.off[leaf];
+  for (uint32_t r0 = 0; r0 < rows; r0 += TPB) {
+    const uint32_t nr = rows - r0 < (uint32_t) TPB ? rows - r0 : (uint32_t) TPB;
+    gemv_split<CX, false>(a.V + a.voff[leaf] + r0, rows, nr, k, tcur, red, tnew);
+    for (uint32_t i = threadIdx.x; i < nr; i += blockDim.x) {
+      yp[W * (r0 + i)] += tnew[W * i];
+      if (CX) yp[W * (r0 + i) + 1] += tnew[W * i + 1];
     }
-    yp[W * i] += sr;
-    if (CX) yp[W * i + 1] += si;
+    __syncthreads();
   }
 }
 
@@ -234,36 +253,28 @@ extern "C" int h2b_mvm_launch(const MvmPlan *p, const double *x, double *y, doub
   const int cx = p->cx;
   const size_t W = cx ? 2 : 1;
   const int sms = p->num_sms > 0 ? p->num_sms : 148;
+  if (p->k > 128) {
+    h2b_set_error("matvec: rank %d > 128", p->k);
+    return H2B_ERR_ARG;
+  }
   H2B_CUDA_TRY(cudaMemsetAsync(p->yp, 0, sizeof(double) * W * p->nrow, st));
   H2B_CUDA_TRY(cudaMemsetAsync(p->yt, 0, sizeof(double) * W * p->k * p->nrow_clusters, st));
   const uint32_t gg = (p->ncol + 255) / 256 < (uint32_t) (4 * sms) ? (p->ncol + 255) / 256
                                                                    : (uint32_t) (4 * sms);
-  MvmForwardArgs fa = p->fwd;
-  MvmCoupleArgs ca = p->cpl;
-  MvmBackArgs ba = p->bwd;
+  const MvmForwardArgs &fa = p->fwd;
+  const MvmCoupleArgs &ca = p->cpl;
+  const MvmBackArgs &ba = p->bwd;
   if (cx) {
     gather_kernel<true><<<gg, 256, 0, st>>>(x, p->cidx, p->xp, p->ncol);
-    forward_kernel<true><<<fa.nleaves, 256, 0, st>>>(fa);
-    couple_near_kernel<true><<<ca.nadm + ca.nnear, 256, 0, st>>>(ca);
-    for (uint32_t l = 1; l < p->rdepth; l++) {
-      MvmDownArgs da = p->down;
-      da.clusters = p->level_list + p->level_start[l];
-      const uint32_t n = p->level_start[l + 1] - p->level_start[l];
-      if (n) downsweep_kernel<true><<<n, 128, 0, st>>>(da);
-    }
-    backward_leaf_kernel<true><<<ba.nleaves, 128, 0, st>>>(ba);
+    forward_near_kernel<true><<<fa.nleaves + ca.nnear, TPB, 0, st>>>(fa, ca);
+    if (ca.nadm) coupling_mv_kernel<true><<<ca.nadm, TPB, 0, st>>>(ca);
+    backward_chain_kernel<true><<<ba.nleaves, TPB, 0, st>>>(ba, p->down.father, p->down.E);
     scatter_kernel<true><<<gg, 256, 0, st>>>(p->yp, p->ridx, y, p->nrow, ar, ai);
   } else {
     gather_kernel<false><<<gg, 256, 0, st>>>(x, p->cidx, p->xp, p->ncol);
-    forward_kernel<false><<<fa.nleaves, 256, 0, st>>>(fa);
-    couple_near_kernel<false><<<ca.nadm + ca.nnear, 256, 0, st>>>(ca);
-    for (uint32_t l = 1; l < p->rdepth; l++) {
-      MvmDownArgs da = p->down;
-      da.clusters = p->level_list + p->level_start[l];
-      const uint32_t n = p->level_start[l + 1] - p->level_start[l];
-      if (n) downsweep_kernel<false><<<n, 128, 0, st>>>(da);
-    }
-    backward_leaf_kernel<false><<<ba.nleaves, 128, 0, st>>>(ba);
+    forward_near_kernel<false><<<fa.nleaves + ca.nnear, TPB, 0, st>>>(fa, ca);
+    if (ca.nadm) coupling_mv_kernel<false><<<ca.nadm, TPB, 0, st>>>(ca);
+    backward_chain_kernel<false><<<ba.nleaves, TPB, 0, st>>>(ba, p->down.father, p->down.E);
     scatter_kernel<false><<<gg, 256, 0, st>>>(p->yp, p->ridx, y, p->nrow, ar, ai);
   }
   H2B_CUDA_TRY(cudaGetLastError());

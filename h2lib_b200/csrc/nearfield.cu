@@ -157,7 +157,10 @@ struct DistArgs {
 
 // Shared-memory accumulator tile: [NOUT*(CPLX?2:1)][64*64] doubles.
 template <int Q, int KK, bool RL, bool CL>
-__global__ void __launch_bounds__(256, 2) near_dist_kernel(DistArgs a) {
+#ifndef H2B_DIST_MINBLOCKS
+#define H2B_DIST_MINBLOCKS 2
+#endif
+__global__ void __launch_bounds__(256, H2B_DIST_MINBLOCKS) near_dist_kernel(DistArgs a) {
   constexpr int NCH = KT<KK>::NCH;
   constexpr int NR = RL ? 3 : 1, NC = CL ? 3 : 1;
   constexpr int PLANES = KT<KK>::CPLX ? 2 : KT<KK>::NOUT;
@@ -277,8 +280,10 @@ struct SingArgs {
 };
 
 // One warp per singular pair.  The three rules are copied into shared memory once per CTA.
+// 512 threads: one CTA per SM holds the staged rules, 16 warps hide the FP64 latencies.
+constexpr int SING_THREADS = 512;
 template <int KK, bool RL, bool CL>
-__global__ void __launch_bounds__(256) near_sing_kernel(SingArgs a) {
+__global__ void __launch_bounds__(SING_THREADS, 1) near_sing_kernel(SingArgs a) {
   constexpr int NCH = KT<KK>::NCH;
   constexpr int NR = RL ? 3 : 1, NC = CL ? 3 : 1;
   extern __shared__ __align__(16) double srule[];
@@ -489,9 +494,10 @@ int launch_sing(const h2b_near_launch *L, cudaStream_t st) {
   a.staged = staged;
   a.err = L->err;
   int sms = L->num_sms > 0 ? L->num_sms : 148;
-  uint32_t want = (L->nsing + 7) / 8;  // 8 warps per CTA
+  const uint32_t wpc = SING_THREADS / 32;
+  uint32_t want = (L->nsing + wpc - 1) / wpc;
   uint32_t grid = want < (uint32_t) sms ? want : (uint32_t) sms;
-  near_sing_kernel<KK, RL, CL><<<grid, 256, smem, st>>>(a);
+  near_sing_kernel<KK, RL, CL><<<grid, SING_THREADS, smem, st>>>(a);
   H2B_CUDA_TRY(cudaGetLastError());
   return H2B_OK;
 }

@@ -277,6 +277,13 @@ int h2b_project_l2_harmonic(const h2b_bem *bem, const double z[3], double *w);
 int h2b_l2_error_harmonic(const h2b_bem *bem, const double z[3], const double *u, double *err,
                           double *norm);
 
+/* b[t] = coef * int_{triangle t} exp(i kvec . (x - src)) dx for the constant basis (a plane wave
+ * as Dirichlet datum).  Replaces integrate_bem3d_c_avector (Library/bem3d.c:8579) with
+ * rhs_dirichlet_plane_helmholtzbem3d (Library/helmholtzbem3d.c:1611); coef = -1 gives the
+ * datum -u_inc of a sound-soft scatterer.  b: interleaved complex, host or device. */
+int h2b_integrate_plane_wave(const h2b_bem *bem, const double kvec[3], const double src[3],
+                             double coef_re, double coef_im, double *b);
+
 #ifdef __cplusplus
 }
 #endif

@@ -21,6 +21,7 @@
  * Nothing in the product library links this file.
  */
 #include <complex.h>
+#include <stdio.h>
 #include <math.h>
 #include <stdlib.h>
 #include <string.h>
@@ -1205,6 +1206,8 @@ orc_gmres(uint32_t nterms, orc_h2 *const *ops, const double *coef, const double 
     gm_step(&A, &g);
     err = cabs(g.rhat[g.k]);
     iter++;
+    if (getenv("ORC_GMRES_TRACE"))
+      fprintf(stderr, "gmres %u %.17e\n", iter, err / (eps * norm));
   }
   gm_finish(&A, bv, xv, &g);
   for (i = 0; i < n; i++) {

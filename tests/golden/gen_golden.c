@@ -728,6 +728,108 @@ section_helm_h2small(void)
   del_macrosurface3d(mg);
 }
 
+/* Brakhage-Werner operator (K + M/2) - i eta V of Tests/test_helmholtzbem3d.c:26-65 */
+typedef struct {
+  ph2matrix V, KM;
+  field eta;
+} bw_t;
+
+static void
+addeval_bw(field alpha, void *matrix, pcavector x, pavector y)
+{
+  bw_t *bw = (bw_t *) matrix;
+  addeval_h2matrix_avector(alpha, bw->KM, x, y);
+  addeval_h2matrix_avector(-I * alpha * bw->eta, bw->V, x, y);
+}
+
+/* Config 3: cube refined to 49152 triangles, constant basis, k = 2, m = 5, leaf 64, eta 1.4;
+ * plane wave along (1,1,1)/sqrt(3); Dirichlet data -u_inc; GMRES(80) to 1e-8. */
+static void
+section_config3(void)
+{
+  pmacrosurface3d mg = new_cube_macrosurface3d();
+  psurface3d gr = build_from_macrosurface3d_surface3d(mg, 64);
+  field k = 2.0;
+  real eta = 1.4;
+  pbem3d slp, dlp;
+  pcluster root;
+  pblock broot;
+  pclusterbasis Vrb, Vcb, Krb, Kcb;
+  ph2matrix V, K;
+  pavector x, y, b, u;
+  helmholtz_data hdata;
+  real kvec[3], src[3] = {0.0, 0.0, 0.0};
+  bw_t bw;
+  uint iter, i;
+  pstopwatch sw = new_stopwatch();
+
+  slp = new_slp_helmholtz_bem3d(k, gr, 2, 4, BASIS_CONSTANT_BEM3D, BASIS_CONSTANT_BEM3D);
+  dlp = new_dlp_helmholtz_bem3d(k, gr, 2, 4, BASIS_CONSTANT_BEM3D, BASIS_CONSTANT_BEM3D, 0.5);
+  root = build_bem3d_cluster(slp, 64, BASIS_CONSTANT_BEM3D);
+  broot = build_strict_block(root, root, &eta, admissible_max_cluster);
+  dump_cluster("c3", root);
+  dump_block("c3", broot, root, root);
+  Vrb = build_from_cluster_clusterbasis(root);
+  Vcb = build_from_cluster_clusterbasis(root);
+  Krb = build_from_cluster_clusterbasis(root);
+  Kcb = build_from_cluster_clusterbasis(root);
+  V = build_from_block_h2matrix(broot, Vrb, Vcb);
+  K = build_from_block_h2matrix(broot, Krb, Kcb);
+  setup_h2matrix_aprx_inter_bem3d(slp, Vrb, Vcb, broot, 5);
+  setup_h2matrix_aprx_inter_bem3d(dlp, Krb, Kcb, broot, 5);
+  start_stopwatch(sw);
+  assemble_bem3d_h2matrix_row_clusterbasis(slp, Vrb);
+  assemble_bem3d_h2matrix_col_clusterbasis(slp, Vcb);
+  assemble_bem3d_h2matrix(slp, V);
+  assemble_bem3d_h2matrix_row_clusterbasis(dlp, Krb);
+  assemble_bem3d_h2matrix_col_clusterbasis(dlp, Kcb);
+  assemble_bem3d_h2matrix(dlp, K);
+  dump_scalar("c3_time_assembly", stop_stopwatch(sw));
+
+  x = new_avector(gr->triangles);
+  y = new_avector(gr->triangles);
+  seeded_avector(x, 3);
+  dump_avector("c3_x", x);
+  clear_avector(y);
+  addeval_h2matrix_avector(1.0, V, x, y);
+  dump_avector("c3_ySLP", y);
+  clear_avector(y);
+  addeval_h2matrix_avector(1.0, K, x, y);
+  dump_avector("c3_yDLP", y);
+
+  for (i = 0; i < 3; i++)
+    kvec[i] = REAL(k) / REAL_SQRT(3.0);
+  hdata.kvec = kvec;
+  hdata.source = src;
+  hdata.eta = k;
+  b = new_avector(gr->triangles);
+  u = new_avector(gr->triangles);
+  integrate_bem3d_c_avector(dlp, rhs_dirichlet_plane_helmholtzbem3d, b, (void *) &hdata);
+  scale_avector(-1.0, b);
+  dump_avector("c3_b", b);
+  bw.V = V;
+  bw.KM = K;
+  bw.eta = k;
+  clear_avector(u);
+  start_stopwatch(sw);
+  iter = solve_gmres_avector(&bw, addeval_bw, b, u, 1.0e-8, 1000, 80);
+  dump_scalar("c3_time_gmres", stop_stopwatch(sw));
+  dump_scalar("c3_gmres_iter", (double) iter);
+  dump_avector("c3_u", u);
+
+  del_avector(x); del_avector(y); del_avector(b); del_avector(u);
+  del_h2matrix(V);
+  del_h2matrix(K);
+  del_block(broot);
+  freemem(root->idx);
+  del_cluster(root);
+  del_helmholtz_bem3d(slp);
+  del_helmholtz_bem3d(dlp);
+  del_surface3d(gr);
+  del_macrosurface3d(mg);
+  del_stopwatch(sw);
+}
+
 #endif
 
 int
@@ -767,6 +869,8 @@ main(int argc, char **argv)
       section_helm_sphere4();
     else if (!strcmp(argv[i], "helm_h2small"))
       section_helm_h2small();
+    else if (!strcmp(argv[i], "config3"))
+      section_config3();
 #endif
     else {
       fprintf(stderr, "unknown section %s\n", argv[i]);

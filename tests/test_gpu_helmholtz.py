@@ -1,0 +1,45 @@
+"""Helmholtz Brakhage-Werner solve on the B200 (config 3): unit cube refined to 49152 triangles,
+piecewise constant basis, k = 2, Chebyshev interpolation m = 5, leaf size 64, eta = 1.4, plane
+wave along (1,1,1)/sqrt(3), GMRES(80) to 1e-8 on (K + M/2) - i k V (Tests/test_helmholtzbem3d.c:
+26-65).  Compared with the reference's golden vectors: trees, matvecs (1e-12), right-hand side,
+iteration count and solution."""
+import numpy as np
+import pytest
+
+from h2lib_b200 import bem3d as hb
+
+pytestmark = pytest.mark.gpu
+C = hb.BASIS_CONSTANT_BEM3D
+
+
+def relerr(a, b):
+    a, b = np.ravel(a), np.ravel(b)
+    return float(np.linalg.norm(a - b) / np.linalg.norm(b))
+
+
+def test_config3_brakhage_werner(gold):
+    g = gold("config3")
+    k = 2.0
+    gr = hb.new_cube_surface3d(64)
+    slp = hb.new_slp_helmholtz_bem3d(k, gr, 2, 4, C, C)
+    dlp = hb.new_dlp_helmholtz_bem3d(k, gr, 2, 4, C, C, 0.5)
+    tree = hb.build_tree(gr, C, C, 64, 1.4)
+    rec, box, idx = tree.clusters(0)
+    np.testing.assert_array_equal(rec, g["c3_ctree"])
+    np.testing.assert_array_equal(idx, g["c3_idx"])
+    np.testing.assert_array_equal(tree.block_records(), g["c3_blocks"])
+    V = hb.H2Matrix(slp, tree, 5).assemble()
+    K = hb.H2Matrix(dlp, tree, 5).assemble()
+    x = np.ascontiguousarray(g["c3_x"])
+    y = hb.addeval_h2matrix_avector(1.0, V, x, np.zeros(V.rows, dtype=np.complex128))
+    assert relerr(y, g["c3_ySLP"]) < 1e-12
+    y = hb.addeval_h2matrix_avector(1.0, K, x, np.zeros(K.rows, dtype=np.complex128))
+    assert relerr(y, g["c3_yDLP"]) < 1e-12
+    d = np.ones(3) / np.sqrt(3.0)
+    b = hb.integrate_plane_wave(slp, k * d, coef=-1.0)
+    assert relerr(b, g["c3_b"]) < 1e-12
+    u = np.zeros(V.rows, dtype=np.complex128)
+    it = hb.solve_gmres([K, V], [1.0, -1j * k], b, u, 1e-8, 1000, 80)
+    assert abs(it - int(g["c3_gmres_iter"][0])) <= 1
+    assert relerr(u, g["c3_u"]) < 1e-6
+    assert hb.residual_norm([K, V], [1.0, -1j * k], b, u) < 1.05e-8
