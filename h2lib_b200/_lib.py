@@ -74,6 +74,8 @@ _SIGS = {
     "h2b_solve_gmres": (C.c_int, [C.c_uint32, vp, _f64p, vp, vp, C.c_double, C.c_uint32,
                                   C.c_uint32]),
     "h2b_residual_norm": (C.c_int, [C.c_uint32, vp, _f64p, vp, vp, C.POINTER(C.c_double)]),
+    "h2b_solve_gmres_noalloc": (C.c_int, [C.c_uint32, vp, _f64p, vp, vp, C.c_double,
+                                          C.c_uint32, C.c_uint32]),
     "h2b_project_l2_harmonic": (C.c_int, [vp, _f64p, vp]),
     "h2b_l2_error_harmonic": (C.c_int, [vp, _f64p, vp, C.POINTER(C.c_double),
                                         C.POINTER(C.c_double)]),

@@ -256,6 +256,24 @@ int h2b_h2matrix_addeval_multi(double alpha_re, double alpha_im, const h2b_h2mat
 int h2b_solve_gmres(uint32_t nterms, const h2b_h2matrix *const *ops, const double *coef,
                     const double *b, double *x, double eps, uint32_t maxiter, uint32_t kmax);
 
+/* GMRES that allocates nothing.  No counterpart in the reference (H2Lib allocates its Krylov work
+ * space with new_avector / new_amatrix in solve_gmres_avector).  For callers that cannot allocate
+ * device memory during a solve — a device-memory budget fixed at start-up, an allocator owned by
+ * another framework, or a real-time loop that forbids allocation calls — this variant of
+ * h2b_solve_gmres takes its work space (Householder vectors, compact-WY factor, staging vectors)
+ * from a fixed device array of H2B_NOALLOC_SCRATCH_BYTES bytes compiled into the library, which
+ * every GPU that loads the library holds until the process exits, and launches the step kernels
+ * directly (no CUDA graph).  Problems whose work space, about 8 * (n * kmax + 4 n) bytes (twice
+ * that for complex operators), exceeds the array are rejected with H2B_ERR_ARG.  Same algorithm,
+ * arguments and result as h2b_solve_gmres; b and x may be host or device pointers.
+ * The first call on a device looks up the array's device address (cudaGetSymbolAddress): make it
+ * before any stream capture.  All calls share the array and it keeps the last call's contents;
+ * calls that overlap on the GPU race, so serialise them. */
+#define H2B_NOALLOC_SCRATCH_BYTES (24u << 20)
+int h2b_solve_gmres_noalloc(uint32_t nterms, const h2b_h2matrix *const *ops, const double *coef,
+                            const double *b, double *x, double eps, uint32_t maxiter,
+                            uint32_t kmax);
+
 /* Relative residual ||b - A x|| / ||b|| computed in FP64 on the device (diagnostic). */
 int h2b_residual_norm(uint32_t nterms, const h2b_h2matrix *const *ops, const double *coef,
                       const double *b, const double *x, double *relres);
