@@ -315,28 +315,36 @@ def run_ours(a, rank, world, local):
         for name, h, part in (("Vn", V, 5), ("Kn", K, 5), ("Vs", V, 4), ("Ks", K, 4)):
             n = inf["near_entries"] if part == 5 else inf["coupling_entries"]
             pin[name] = torch.empty(n, dtype=torch.float64, pin_memory=True)
-        e2e_times = []
+        e2e_times, e2e_phases = [], []
         h2d = d2h = 0
+        import ctypes
         for rep in range(3):
             torch.cuda.synchronize()
             t0 = time.perf_counter()
             g2 = hb.Surface3d(gr.x, gr.t)
             s2 = hb.new_slp_laplace_bem3d(g2, 2, 4, L, L)
             d2 = hb.new_dlp_laplace_bem3d(g2, 2, 4, L, L, 0.5)
+            t1 = time.perf_counter()
             tr2 = hb.build_tree(g2, L, L, a.clf, a.eta)
+            t2 = time.perf_counter()
             V2, K2 = hb.H2Matrix(s2, tr2, a.m), hb.H2Matrix(d2, tr2, a.m)
+            t3 = time.perf_counter()
             for h in (V2, K2):
                 check(lib.h2b_h2matrix_assemble_row_clusterbasis(h.handle), "row basis")
                 check(lib.h2b_h2matrix_assemble_col_clusterbasis(h.handle), "col basis")
                 check(lib.h2b_h2matrix_assemble_farfield(h.handle), "coupling")
             check(lib.h2b_h2matrix_assemble_nearfield_pair(V2.handle, K2.handle), "near pair")
-            import ctypes
+            t4 = time.perf_counter()
             nd = ctypes.c_uint64()
             for name, h, part in (("Vn", V2, 5), ("Kn", K2, 5), ("Vs", V2, 4), ("Ks", K2, 4)):
                 check(lib.h2b_h2matrix_export(h.handle, part, 0xFFFFFFFF,
                                               ctypes.c_void_p(pin[name].data_ptr()),
                                               ctypes.byref(nd)), "export")
-            e2e_times.append(time.perf_counter() - t0)
+            t5 = time.perf_counter()
+            e2e_times.append(t5 - t0)
+            e2e_phases.append({"surface_and_operators": t1 - t0, "trees": t2 - t1,
+                               "h2_structure": t3 - t2, "assembly": t4 - t3,
+                               "copy_to_host": t5 - t4})
             d2h = 8 * (2 * inf["near_entries"] + 2 * inf["coupling_entries"])
             h2d = gr.x.nbytes + gr.t.nbytes + gr.n.nbytes + gr.g.nbytes
             del V2, K2, tr2, s2, d2, g2
@@ -345,7 +353,9 @@ def run_ours(a, rank, world, local):
                "d2h_bytes_per_step": int(d2h),
                "includes": "mesh upload, operators, cluster/block trees (host C), H2 structure "
                            "upload, assembly of V and K, copy of all nearfield and coupling "
-                           "blocks to pinned host memory"}
+                           "blocks to pinned host memory",
+               "phase_ms": {k: 1e3 * e2e_phases[e2e_times.index(min(e2e_times))][k]
+                            for k in e2e_phases[0]}}
 
     res = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps,
