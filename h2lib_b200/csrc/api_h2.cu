@@ -1,6 +1,7 @@
 // C-ABI implementation: H2 matrices (structure upload, assembly, export, matvec).
 #include <cuda_runtime.h>
 #include <math.h>
+#include <stdlib.h>
 #include <string.h>
 
 #include <algorithm>
@@ -49,6 +50,72 @@ static void devtree_free(DevCTree &t) {
   dfree(t.d_idx); dfree(t.d_leaves); dfree(t.d_nonroot); dfree(t.d_levels); dfree(t.d_voff);
   dfree(t.d_pts); dfree(t.d_V); dfree(t.d_E); dfree(t.d_counter); dfree(t.d_refs);
   dfree(t.d_tr_off); dfree(t.d_tr_len);
+  dfree(t.d_W); dfree(t.d_woff); dfree(t.d_fitems); dfree(t.d_wleaves); dfree(t.d_mitems);
+}
+
+// Flattened bases: W_t for the clusters of admissible blocks (`adm`, ids of this tree) and all
+// their descendants (which the products W_f = [W_s E_s] pass through).  Flatten items are
+// grouped by father level, deepest first; matvec items cover the admissible clusters in pieces
+// of at most H2B_MVM_FLAT_ROWS rows.
+static int devtree_flat_setup(DevCTree &t, const h2b_ctree &c, const std::vector<uint32_t> &adm,
+                              uint32_t k, cudaStream_t st) {
+  std::vector<char> in_adm(c.n, 0), need(c.n, 0);
+  for (uint32_t a : adm) in_adm[a] = 1;
+  // pre-order: a father precedes its sons
+  for (uint32_t i = 0; i < c.n; i++)
+    need[i] = in_adm[i] || (c.father[i] != UINT32_MAX && need[c.father[i]]);
+  std::vector<uint64_t> woff(c.n, 0);
+  uint64_t tot = 0;
+  for (uint32_t i = 0; i < c.n; i++)
+    if (need[i]) {
+      woff[i] = tot;
+      tot += (uint64_t) c.size[i] * k;
+    }
+  t.wtotal = tot;
+  std::vector<uint32_t> wleaves, fitems, mitems;
+  for (uint32_t i = 0; i < c.n; i++)
+    if (need[i] && c.sons[i] == 0) wleaves.push_back(i);
+  t.fitem_start.assign(c.depth + 1, 0);
+  t.fitem_count.assign(c.depth + 1, 0);
+  uint32_t nitems = 0;
+  for (int l = (int) c.depth - 1; l >= 0; l--) {
+    t.fitem_start[l] = nitems;
+    for (uint32_t f = 0; f < c.n; f++) {
+      if (!need[f] || c.level[f] != (uint32_t) l || c.sons[f] == 0) continue;
+      const uint32_t sons[2] = {c.son0[f], c.son1[f]};
+      for (uint32_t q = 0; q < c.sons[f] && q < 2; q++)
+        for (uint32_t r0 = 0; r0 < c.size[sons[q]]; r0 += H2B_FLAT_ROWS) {
+          const uint32_t nr = std::min<uint32_t>(H2B_FLAT_ROWS, c.size[sons[q]] - r0);
+          fitems.insert(fitems.end(), {f, sons[q], r0, nr});
+          nitems++;
+        }
+    }
+    t.fitem_count[l] = nitems - t.fitem_start[l];
+  }
+  for (uint32_t i = 0; i < c.n; i++)
+    if (in_adm[i])
+      for (uint32_t r0 = 0; r0 < c.size[i]; r0 += H2B_MVM_FLAT_ROWS)
+        mitems.insert(mitems.end(), {i, r0, std::min<uint32_t>(H2B_MVM_FLAT_ROWS, c.size[i] - r0)});
+  t.nwleaves = (uint32_t) wleaves.size();
+  t.nmitems = (uint32_t) (mitems.size() / 3);
+  int rc;
+  if ((rc = upload(&t.d_woff, woff, st)) || (rc = upload(&t.d_wleaves, wleaves, st)) ||
+      (rc = upload(&t.d_fitems, fitems, st)) || (rc = upload(&t.d_mitems, mitems, st)))
+    return rc;
+  H2B_CUDA_TRY(cudaMalloc(&t.d_W, sizeof(double) * std::max<uint64_t>(tot, 1)));
+  return H2B_OK;
+}
+
+// W from V and E: leaves first, then the father levels from the deepest up.
+static int devtree_flatten(DevCTree &t, uint32_t k, int transposed, cudaStream_t st) {
+  FlatLeafArgs la{t.d_wleaves, t.d_size, t.d_voff, t.d_woff, t.d_V, t.d_W, t.nwleaves, (int) k};
+  int rc = h2b_flat_leaves(&la, st);
+  for (int l = (int) t.depth - 1; rc == H2B_OK && l >= 0; l--) {
+    FlatArgs fa{t.d_fitems + 4 * (size_t) t.fitem_start[l], t.d_off, t.d_size, t.d_woff, t.d_E,
+                t.d_W, t.fitem_count[l], (int) k, transposed};
+    rc = h2b_flat_level(&fa, st);
+  }
+  return rc;
 }
 
 static int devtree_build(DevCTree &t, const h2b_ctree &c, int basis, uint32_t m, uint32_t k,
@@ -141,6 +208,49 @@ extern "C" void h2b_h2matrix_del(h2b_h2matrix *h) {
   delete h;
 }
 
+// Singular pairs of the uploaded tiles, found on the device in two passes (count, then write
+// grouped by Sauter-Schwab case: vertex, edge, identical), and the pair counts per case.
+static int classify_singular(h2b_h2matrix *h, uint64_t all_pairs) {
+  uint32_t *d_cur = nullptr;
+  H2B_CUDA_TRY(cudaMalloc(&d_cur, sizeof(uint32_t) * 8));
+  int rc = H2B_OK;
+  uint32_t cnt[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  if (cudaMemsetAsync(d_cur, 0, sizeof(uint32_t) * 8, h->st) != cudaSuccess) rc = H2B_ERR_CUDA;
+  if (rc == H2B_OK)
+    rc = h2b_near_classify(h->bem->s->d_tri, h->d_refs, h->d_tiles, h->ntiles, d_cur, nullptr,
+                           nullptr, h->st);
+  if (rc == H2B_OK &&
+      (cudaMemcpyAsync(cnt, d_cur, sizeof(uint32_t) * 4, cudaMemcpyDeviceToHost, h->st) !=
+           cudaSuccess ||
+       cudaStreamSynchronize(h->st) != cudaSuccess))
+    rc = H2B_ERR_CUDA;
+  const uint64_t nsing = (uint64_t) cnt[1] + cnt[2] + cnt[3];
+  if (rc == H2B_OK) {
+    // base offsets of the cases in cnt[4..7]
+    cnt[4] = 0;
+    cnt[5] = 0;
+    cnt[6] = cnt[1];
+    cnt[7] = cnt[1] + cnt[2];
+    h->nsing = (uint32_t) nsing;
+    for (int c = 1; c <= 3; c++) h->pairs[c] = cnt[c];
+    h->pairs[0] = all_pairs - nsing;
+    if (cudaMalloc(&h->d_sing, sizeof(h2b_sing) * std::max<uint64_t>(nsing, 1)) != cudaSuccess ||
+        cudaMemsetAsync(d_cur, 0, sizeof(uint32_t) * 4, h->st) != cudaSuccess ||
+        cudaMemcpyAsync(d_cur + 4, cnt + 4, sizeof(uint32_t) * 4, cudaMemcpyHostToDevice, h->st) !=
+            cudaSuccess)
+      rc = H2B_ERR_CUDA;
+  }
+  if (rc == H2B_OK && nsing)
+    rc = h2b_near_classify(h->bem->s->d_tri, h->d_refs, h->d_tiles, h->ntiles, d_cur, d_cur + 4,
+                           h->d_sing, h->st);
+  if (rc == H2B_OK && cudaStreamSynchronize(h->st) != cudaSuccess) rc = H2B_ERR_CUDA;
+  if (rc == H2B_ERR_CUDA)
+    h2b_set_error("h2matrix singular-pair classification: %s",
+                  cudaGetErrorString(cudaGetLastError()));
+  cudaFree(d_cur);
+  return rc;
+}
+
 extern "C" h2b_h2matrix *h2b_h2matrix_new(const h2b_bem *bem, const h2b_tree *tree, uint32_t m) {
   if (!bem || !tree) {
     h2b_set_error("h2b_h2matrix_new: NULL operator or tree");
@@ -180,6 +290,7 @@ extern "C" h2b_h2matrix *h2b_h2matrix_new(const h2b_bem *bem, const h2b_tree *tr
   uint64_t ntot = 0;
   h2b_nearplan plan;
   h2b_nearplan_init(&plan);
+  plan.skip_sing = 1;  // singular pairs are found on the device below
   for (uint32_t b = 0; rc == H2B_OK && b < tree->blocks.n; b++) {
     const uint32_t r = tree->blocks.rc[b], c = tree->blocks.cc[b];
     if (tree->blocks.adm[b]) {
@@ -196,14 +307,10 @@ extern "C" h2b_h2matrix *h2b_h2matrix_new(const h2b_bem *bem, const h2b_tree *tr
       ntot += (uint64_t) rows * cols;
     }
   }
-  if (rc == H2B_OK) rc = h2b_nearplan_finalize(&plan);
-  if (rc == H2B_OK) {
-    uint64_t all = 0;
+  uint64_t all_pairs = 0;
+  if (rc == H2B_OK)
     for (uint32_t t = 0; t < plan.ntiles; t++)
-      all += (uint64_t) plan.tiles[t].tr_len * plan.tiles[t].sc_len;
-    for (int c = 1; c <= 3; c++) h->pairs[c] = plan.case_start[c + 1] - plan.case_start[c];
-    h->pairs[0] = all - plan.nsing;
-  }
+      all_pairs += (uint64_t) plan.tiles[t].tr_len * plan.tiles[t].sc_len;
   for (int e = 0; rc == H2B_OK && e < 12; e++)
     if (cudaEventCreate(&h->ev[e]) != cudaSuccess) {
       h2b_set_error("h2b_h2matrix_new: %s", cudaGetErrorString(cudaGetLastError()));
@@ -213,16 +320,15 @@ extern "C" h2b_h2matrix *h2b_h2matrix_new(const h2b_bem *bem, const h2b_tree *tr
   h->nnear = (uint32_t) nrc.size();
   h->near_total = ntot;
   h->ntiles = plan.ntiles;
-  h->nsing = plan.nsing;
   if (rc == H2B_OK) {
     const size_t W = h->cx ? 2 : 1;
     std::vector<h2b_tile> tiles(plan.tiles, plan.tiles + plan.ntiles);
     std::vector<h2b_triref> refs(plan.refs, plan.refs + plan.nrefs);
-    std::vector<h2b_sing> sing(plan.sing, plan.sing + plan.nsing);
     if ((rc = upload(&h->d_adm_rc, arc, h->st)) || (rc = upload(&h->d_adm_cc, acc, h->st)) ||
         (rc = upload(&h->d_near_rc, nrc, h->st)) || (rc = upload(&h->d_near_cc, ncc, h->st)) ||
         (rc = upload(&h->d_near_off, noff, h->st)) || (rc = upload(&h->d_tiles, tiles, h->st)) ||
-        (rc = upload(&h->d_refs, refs, h->st)) || (rc = upload(&h->d_sing, sing, h->st))) {
+        (rc = upload(&h->d_refs, refs, h->st)) ||
+        (rc = classify_singular(h, all_pairs))) {
     } else if (cudaMalloc(&h->d_S, sizeof(double) * W * std::max<uint64_t>((uint64_t) h->nadm * h->k * h->k, 1)) != cudaSuccess ||
                cudaMalloc(&h->d_N, sizeof(double) * W * std::max<uint64_t>(ntot, 1)) != cudaSuccess ||
                cudaMalloc(&h->d_xp, sizeof(double) * W * nc) != cudaSuccess ||
@@ -237,6 +343,13 @@ extern "C" h2b_h2matrix *h2b_h2matrix_new(const h2b_bem *bem, const h2b_tree *tr
     }
   }
   h2b_nearplan_free(&plan);
+  // flattened bases over the admissible clusters (unless the nested transforms are requested)
+  {
+    const char *e = getenv("H2B_MVM_NESTED");
+    h->flat = !(e && e[0] == '1');
+  }
+  if (rc == H2B_OK && h->flat) rc = devtree_flat_setup(h->rt, tree->row, arc, h->k, h->st);
+  if (rc == H2B_OK && h->flat) rc = devtree_flat_setup(h->ct, tree->col, acc, h->k, h->st);
   // single-triangle rule (raw and linear-basis weighted)
   if (rc == H2B_OK) {
     const h2b_quad &qd = bem->quad;
@@ -284,6 +397,12 @@ void h2b_h2_fill_mvm_plan(h2b_h2matrix *h) {
   p.down = MvmDownArgs{nullptr, h->rt.d_father, h->rt.d_E, h->d_yt, (int) h->k};
   p.bwd = MvmBackArgs{h->rt.d_leaves, h->rt.d_size, h->rt.d_off, h->rt.d_voff, h->rt.d_V,
                       h->d_yt, h->d_yp, h->rt.nleaves, (int) h->k};
+  p.flat = h->flat;
+  p.ncol_clusters = h->ct.n;
+  p.ffwd = MvmFlatArgs{h->ct.d_mitems, h->ct.d_off, h->ct.d_size, h->ct.d_woff, h->ct.d_W,
+                       h->ct.nmitems, (int) h->k};
+  p.fbwd = MvmFlatArgs{h->rt.d_mitems, h->rt.d_off, h->rt.d_size, h->rt.d_woff, h->rt.d_W,
+                       h->rt.nmitems, (int) h->k};
   p.level_list = h->rt.d_levels;
   p.rdepth = std::min<uint32_t>(h->rt.depth, 64);
   for (uint32_t l = 0; l <= p.rdepth; l++) p.level_start[l] = h->rt.level_start[l];
@@ -320,7 +439,9 @@ static int assemble_basis(h2b_h2matrix *h, DevCTree &t, int basis, int dn) {
   if (rc != H2B_OK) return rc;
   FarTransferArgs ta{t.d_nonroot, t.d_father, t.d_pts, t.d_E, t.n - 1, (int) h->m, (int) h->k,
                      transposed};
-  return h2b_far_transfer(&ta, h->st);
+  rc = h2b_far_transfer(&ta, h->st);
+  if (rc == H2B_OK && h->flat) rc = devtree_flatten(t, h->k, transposed, h->st);
+  return rc;
 }
 
 // Phase timings: events 2i / 2i+1 bracket phase i (0 row basis, 1 column basis, 2 coupling,

@@ -23,6 +23,15 @@ struct DevCTree {
   TriRef *d_refs = nullptr;
   uint32_t *d_tr_off = nullptr, *d_tr_len = nullptr;
   std::vector<uint32_t> leaves, level_start;
+  // flattened bases (flatbasis.cu): W_t for every cluster of an admissible block and below
+  double *d_W = nullptr;
+  uint64_t *d_woff = nullptr;
+  uint64_t wtotal = 0;
+  uint32_t *d_fitems = nullptr;  // flatten items (4 uint32 each), grouped by father level
+  uint32_t *d_wleaves = nullptr; // leaves that carry a W (W_leaf = V_leaf)
+  uint32_t *d_mitems = nullptr;  // matvec items (3 uint32 each) over the admissible clusters
+  std::vector<uint32_t> fitem_start, fitem_count;  // flatten items of father level l
+  uint32_t nwleaves = 0, nmitems = 0;
 };
 
 struct h2b_h2matrix {
@@ -30,6 +39,7 @@ struct h2b_h2matrix {
   const h2b_tree *tree = nullptr;
   uint32_t m = 0, k = 0, ns = 0;
   int cx = 0, num_sms = 148;
+  int flat = 1;  // matvec through flattened bases (W_t) instead of the nested transforms
   cudaStream_t st = nullptr;
   DevCTree rt, ct;
   uint32_t nadm = 0, nnear = 0, ntiles = 0, nsing = 0;

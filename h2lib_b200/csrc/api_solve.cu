@@ -2,6 +2,7 @@
 // (L2 projection of the harmonic Dirichlet datum, L2 error of the Neumann trace).
 #include <cuda_runtime.h>
 #include <math.h>
+#include <stdlib.h>
 #include <string.h>
 
 #include <vector>
@@ -123,26 +124,46 @@ extern "C" int h2b_solve_gmres(uint32_t nterms, const h2b_h2matrix *const *ops,
     ~HostFree() { cudaFreeHost(p); }
   } hf{hs};
 
+  // Default: the whole iteration runs inside one graph (WHILE/IF conditional nodes, the loop
+  // condition set on the device).  H2B_GMRES_HOSTLOOP=1 selects a host loop that launches a
+  // captured single step and reads the residual estimate after each one.
+  cudaGraphExec_t loop_exec = nullptr;
+  {
+    const char *e = getenv("H2B_GMRES_HOSTLOOP");
+    if (!(e && e[0] == '1') && (rc = h2b_gmres_loop_graph(&g, &op, db, dx, st, &loop_exec)) != H2B_OK)
+      return rc;
+  }
+  struct LoopFree {
+    cudaGraphExec_t e;
+    ~LoopFree() {
+      if (e) cudaGraphExecDestroy(e);
+    }
+  } lf{loop_exec};
   // the step is identical for every k (k is read on the device): capture it once
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
-  H2B_CUDA_TRY(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-  rc = h2b_gmres_step(&g, &op, st);
-  cudaError_t ce = cudaStreamEndCapture(st, &graph);
-  if (rc != H2B_OK || ce != cudaSuccess) {
-    if (graph) cudaGraphDestroy(graph);
-    if (rc == H2B_OK) h2b_set_error("h2b_solve_gmres: graph capture failed: %s", cudaGetErrorString(ce));
-    return rc == H2B_OK ? H2B_ERR_CUDA : rc;
-  }
-  ce = cudaGraphInstantiate(&exec, graph, 0);
-  cudaGraphDestroy(graph);
-  if (ce != cudaSuccess) {
-    h2b_set_error("h2b_solve_gmres: graph instantiation failed: %s", cudaGetErrorString(ce));
-    return H2B_ERR_CUDA;
+  if (!loop_exec) {
+    H2B_CUDA_TRY(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    rc = h2b_gmres_step(&g, &op, st);
+    cudaError_t ce = cudaStreamEndCapture(st, &graph);
+    if (rc != H2B_OK || ce != cudaSuccess) {
+      if (graph) cudaGraphDestroy(graph);
+      if (rc == H2B_OK)
+        h2b_set_error("h2b_solve_gmres: graph capture failed: %s", cudaGetErrorString(ce));
+      return rc == H2B_OK ? H2B_ERR_CUDA : rc;
+    }
+    ce = cudaGraphInstantiate(&exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (ce != cudaSuccess) {
+      h2b_set_error("h2b_solve_gmres: graph instantiation failed: %s", cudaGetErrorString(ce));
+      return H2B_ERR_CUDA;
+    }
   }
   struct ExecFree {
     cudaGraphExec_t e;
-    ~ExecFree() { cudaGraphExecDestroy(e); }
+    ~ExecFree() {
+      if (e) cudaGraphExecDestroy(e);
+    }
   } ef{exec};
 
   auto read_state = [&]() -> int {
@@ -157,7 +178,32 @@ extern "C" int h2b_solve_gmres(uint32_t nterms, const h2b_h2matrix *const *ops,
   const double bnorm = hs->bnorm;
   double err = hs->err;
   uint32_t k = 0, iter = 0;
-  while (err > eps * bnorm && iter + 1 != maxiter) {
+  if (loop_exec) {
+    // graph-resident loop: launches of at most kLoopBudget steps until the device stops it
+    constexpr uint32_t kLoopBudget = 512;
+    hs->tol = eps * bnorm;
+    hs->iter = 0;
+    hs->maxiter = maxiter;
+    hs->nan = 0;
+    while (true) {
+      hs->budget = kLoopBudget;
+      H2B_CUDA_TRY(cudaMemcpyAsync(g.state, hs, sizeof(GmresState), cudaMemcpyHostToDevice, st));
+      H2B_CUDA_TRY(cudaGraphLaunch(loop_exec, st));
+      if ((rc = read_state()) != H2B_OK) return rc;
+      if (hs->nan) {
+        h2b_set_error("h2b_solve_gmres: residual estimate is NaN after %u iterations", hs->iter);
+        return H2B_ERR_INTERNAL;
+      }
+      if (!(hs->err > hs->tol) || (maxiter != 0 && hs->iter + 1 == maxiter)) break;
+      if (hs->budget != 0) {
+        h2b_set_error("h2b_solve_gmres: device loop stopped early at iteration %u", hs->iter);
+        return H2B_ERR_INTERNAL;
+      }
+    }
+    iter = hs->iter;
+    err = hs->err;
+  }
+  while (!loop_exec && err > eps * bnorm && iter + 1 != maxiter) {
     if (k + 1 >= kmax) {
       if ((rc = h2b_gmres_finish(&g, &op, db, dx, st)) != H2B_OK) return rc;
       k = 0;

@@ -42,6 +42,31 @@ struct FarCouplingArgs {
   double kconst, k_re, k_imn;
 };
 
+// Flattened bases (flatbasis.cu): items of at most H2B_FLAT_ROWS rows of one son.
+#define H2B_FLAT_ROWS 64
+struct FlatArgs {
+  const uint32_t *items;     // 4 per item: father, son, first row in the son, rows
+  const uint32_t *off, *size;
+  const uint64_t *woff;      // per cluster: offset of W_t (doubles)
+  const double *E;           // transfer matrices (E or E^T), cluster c at (c-1)*k*k
+  double *W;
+  uint32_t nitems;
+  int k;
+  int transposed;            // column side: W^T stored k x |t|
+};
+
+struct FlatLeafArgs {
+  const uint32_t *leaves, *size;
+  const uint64_t *voff, *woff;
+  const double *V;
+  double *W;
+  uint32_t nleaves;
+  int k;
+};
+
+extern "C" int h2b_flat_leaves(const FlatLeafArgs *a, cudaStream_t st);
+extern "C" int h2b_flat_level(const FlatArgs *a, cudaStream_t st);
+
 extern "C" int h2b_far_leaf_basis(const FarLeafArgs *a, int linear, int dn, cudaStream_t st);
 extern "C" int h2b_far_transfer(const FarTransferArgs *a, cudaStream_t st);
 extern "C" int h2b_far_coupling(const FarCouplingArgs *a, int cx, cudaStream_t st);

@@ -1,0 +1,95 @@
+// Flattened cluster bases for the H2 matvec (sm_100a, FP64).
+//
+// For every cluster t that needs one, W_t is the |t| x k matrix that the nested basis represents
+// on t's indices: W_leaf = V_leaf and, for a father f with sons s,
+//   W_f restricted to the rows of s = W_s E_s
+// (the recursion of the reference's forward/backward transforms, Library/clusterbasis.c:524/749,
+// multiplied out once after assembly).  With W the forward transform is xt_t = W_t^T x_t and the
+// backward transform y_t += W_t yt_t for all clusters at once: no level-to-level dependence, so
+// the matvec streams W at HBM bandwidth instead of climbing the tree one level per step.
+// Row bases are stored like V (|t| x k, column-major, ld = |t|); column bases transposed like V^T
+// (k x |t|, ld = k), the layouts the matvec reads with consecutive threads on consecutive
+// addresses.
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "device_common.cuh"
+#include "farfield.h"
+
+namespace {
+
+constexpr int FLAT_TPB = 256;
+
+// One CTA per item (father f, son s, first row r0 of s, rows nr <= FLAT_ROWS): the nr rows of
+// W_s times E_s land in the rows of s inside W_f.
+__global__ void __launch_bounds__(FLAT_TPB) flatten_kernel(FlatArgs a) {
+  extern __shared__ double sm[];
+  const uint32_t *it = a.items + 4 * (size_t) blockIdx.x;
+  const uint32_t f = it[0], s = it[1], r0 = it[2], nr = it[3];
+  const uint32_t k = (uint32_t) a.k;
+  double *sE = sm;             // k x k
+  double *sW = sm + k * k;     // nr rows of W_s (layout of the side)
+  const double *E = a.E + (size_t) (s - 1) * k * k;
+  for (uint32_t e = threadIdx.x; e < k * k; e += blockDim.x) sE[e] = E[e];
+  const uint32_t ns = a.size[s], nf = a.size[f];
+  const uint32_t rf = a.off[s] - a.off[f] + r0;  // first row inside f
+  const double *Ws = a.W + a.woff[s];
+  double *Wf = a.W + a.woff[f];
+  if (!a.transposed) {
+    // sW[i + mu nr] = W_s[r0 + i, mu]
+    for (uint32_t e = threadIdx.x; e < nr * k; e += blockDim.x) {
+      const uint32_t i = e % nr, mu = e / nr;
+      sW[e] = Ws[r0 + i + (size_t) mu * ns];
+    }
+    __syncthreads();
+    // W_f[rf + i, nu] = sum_mu W_s[r0 + i, mu] E_s[mu, nu]   (E_s column-major k x k)
+    for (uint32_t e = threadIdx.x; e < nr * k; e += blockDim.x) {
+      const uint32_t i = e % nr, nu = e / nr;
+      double acc = 0.0;
+      for (uint32_t mu = 0; mu < k; mu++) acc = fma(sW[i + mu * nr], sE[mu + nu * k], acc);
+      Wf[rf + i + (size_t) nu * nf] = acc;
+    }
+  } else {
+    // sW[mu + i k] = W_s^T[mu, r0 + i]
+    for (uint32_t e = threadIdx.x; e < nr * k; e += blockDim.x) sW[e] = Ws[(size_t) r0 * k + e];
+    __syncthreads();
+    // W_f^T[nu, rf + i] = sum_mu E_s^T[nu, mu] W_s^T[mu, r0 + i]   (E_s^T column-major k x k)
+    for (uint32_t e = threadIdx.x; e < nr * k; e += blockDim.x) {
+      const uint32_t nu = e % k, i = e / k;
+      double acc = 0.0;
+      for (uint32_t mu = 0; mu < k; mu++) acc = fma(sE[nu + mu * k], sW[mu + i * k], acc);
+      Wf[(size_t) (rf + i) * k + nu] = acc;
+    }
+  }
+}
+
+// W_leaf = V_leaf (same layout on both sides).
+__global__ void __launch_bounds__(FLAT_TPB) leaf_copy_kernel(FlatLeafArgs a) {
+  const uint32_t l = a.leaves[blockIdx.x];
+  const size_t n = (size_t) a.size[l] * a.k;
+  const double *src = a.V + a.voff[l];
+  double *dst = a.W + a.woff[l];
+  for (size_t e = threadIdx.x; e < n; e += blockDim.x) dst[e] = src[e];
+}
+
+}  // namespace
+
+extern "C" int h2b_flat_leaves(const FlatLeafArgs *a, cudaStream_t st) {
+  if (a->nleaves) leaf_copy_kernel<<<a->nleaves, FLAT_TPB, 0, st>>>(*a);
+  H2B_CUDA_TRY(cudaGetLastError());
+  return H2B_OK;
+}
+
+extern "C" int h2b_flat_level(const FlatArgs *a, cudaStream_t st) {
+  if (a->nitems == 0) return H2B_OK;
+  const size_t smem = sizeof(double) * ((size_t) a->k * a->k + (size_t) H2B_FLAT_ROWS * a->k);
+  static size_t attr = 0;
+  if (smem > 48 * 1024 && smem > attr) {
+    H2B_CUDA_TRY(cudaFuncSetAttribute(flatten_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int) smem));
+    attr = smem;
+  }
+  flatten_kernel<<<a->nitems, FLAT_TPB, smem, st>>>(*a);
+  H2B_CUDA_TRY(cudaGetLastError());
+  return H2B_OK;
+}

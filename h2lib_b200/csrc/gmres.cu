@@ -525,7 +525,99 @@ int bnorm_impl(const GmresDev &g, const double *b, cudaStream_t st) {
   return H2B_OK;
 }
 
+// Loop control of the graph-resident iteration (one thread each).
+__global__ void precheck_kernel(GmresDev g, cudaGraphConditionalHandle hw) {
+  const GmresState *s = g.state;
+  const bool go = s->err > s->tol && (s->maxiter == 0 || s->iter + 1 != s->maxiter) &&
+                  s->budget > 0 && !s->nan;
+  cudaGraphSetConditional(hw, go ? 1u : 0u);
+}
+
+__global__ void decide_kernel(GmresDev g, cudaGraphConditionalHandle hi) {
+  cudaGraphSetConditional(hi, g.state->k + 1 >= g.kmax ? 1u : 0u);
+}
+
+__global__ void control_kernel(GmresDev g, cudaGraphConditionalHandle hw) {
+  GmresState *s = g.state;
+  s->iter++;
+  s->budget--;
+  if (!(s->err == s->err)) s->nan = 1;
+  const bool go = s->err > s->tol && (s->maxiter == 0 || s->iter + 1 != s->maxiter) &&
+                  s->budget > 0 && !s->nan;
+  cudaGraphSetConditional(hw, go ? 1u : 0u);
+}
+
 }  // namespace
+
+extern "C" int h2b_gmres_loop_graph(const GmresDev *g, const GmresOp *op, const double *b,
+                                    double *x, cudaStream_t st, cudaGraphExec_t *exec) {
+  cudaGraph_t top = nullptr;
+  *exec = nullptr;
+  H2B_CUDA_TRY(cudaGraphCreate(&top, 0));
+  struct GraphFree {
+    cudaGraph_t gr;
+    ~GraphFree() { cudaGraphDestroy(gr); }
+  } gf{top};
+  cudaGraphConditionalHandle hw, hi;
+  H2B_CUDA_TRY(cudaGraphConditionalHandleCreate(&hw, top, 0, 0));
+  GmresDev gv = *g;
+  // top: precheck -> WHILE
+  cudaGraphNode_t pre, wnode, dec, inode;
+  {
+    void *args[] = {&gv, &hw};
+    cudaKernelNodeParams kp = {};
+    kp.func = (void *) precheck_kernel;
+    kp.gridDim = dim3(1);
+    kp.blockDim = dim3(1);
+    kp.kernelParams = args;
+    H2B_CUDA_TRY(cudaGraphAddKernelNode(&pre, top, nullptr, 0, &kp));
+  }
+  cudaGraphNodeParams wp = {};
+  wp.type = cudaGraphNodeTypeConditional;
+  wp.conditional.handle = hw;
+  wp.conditional.type = cudaGraphCondTypeWhile;
+  wp.conditional.size = 1;
+  H2B_CUDA_TRY(cudaGraphAddNode(&wnode, top, &pre, 1, &wp));
+  cudaGraph_t body = wp.conditional.phGraph_out[0];
+  // body: decide -> IF(restart) -> step -> control
+  H2B_CUDA_TRY(cudaGraphConditionalHandleCreate(&hi, body, 0, 0));
+  {
+    void *args[] = {&gv, &hi};
+    cudaKernelNodeParams kp = {};
+    kp.func = (void *) decide_kernel;
+    kp.gridDim = dim3(1);
+    kp.blockDim = dim3(1);
+    kp.kernelParams = args;
+    H2B_CUDA_TRY(cudaGraphAddKernelNode(&dec, body, nullptr, 0, &kp));
+  }
+  cudaGraphNodeParams ip = {};
+  ip.type = cudaGraphNodeTypeConditional;
+  ip.conditional.handle = hi;
+  ip.conditional.type = cudaGraphCondTypeIf;
+  ip.conditional.size = 1;
+  H2B_CUDA_TRY(cudaGraphAddNode(&inode, body, &dec, 1, &ip));
+  cudaGraph_t ifbody = ip.conditional.phGraph_out[0];
+  int rc;
+  H2B_CUDA_TRY(cudaStreamBeginCaptureToGraph(st, ifbody, nullptr, nullptr, 0,
+                                             cudaStreamCaptureModeThreadLocal));
+  rc = g->cx ? finish_impl<true>(*g, *op, b, x, st) : finish_impl<false>(*g, *op, b, x, st);
+  cudaGraph_t captured = nullptr;
+  cudaError_t ce = cudaStreamEndCapture(st, &captured);
+  if (rc != H2B_OK) return rc;
+  H2B_CUDA_TRY(ce);
+  H2B_CUDA_TRY(cudaStreamBeginCaptureToGraph(st, body, &inode, nullptr, 1,
+                                             cudaStreamCaptureModeThreadLocal));
+  rc = g->cx ? step_impl<true>(*g, *op, st) : step_impl<false>(*g, *op, st);
+  if (rc == H2B_OK) {
+    control_kernel<<<1, 1, 0, st>>>(gv, hw);
+    if (cudaGetLastError() != cudaSuccess) rc = H2B_ERR_CUDA;
+  }
+  ce = cudaStreamEndCapture(st, &captured);
+  if (rc != H2B_OK) return rc;
+  H2B_CUDA_TRY(ce);
+  H2B_CUDA_TRY(cudaGraphInstantiate(exec, top, 0));
+  return H2B_OK;
+}
 
 extern "C" int h2b_gmres_step(const GmresDev *g, const GmresOp *op, cudaStream_t st) {
   return g->cx ? step_impl<true>(*g, *op, st) : step_impl<false>(*g, *op, st);

@@ -10,6 +10,12 @@ struct GmresState {
   uint32_t k, pad;
   double err, bnorm;
   double gamma_re, gamma_im, alpha_re, alpha_im;
+  // loop control of the graph-resident iteration (h2b_gmres_loop_graph)
+  double tol;          // eps * |b|
+  uint32_t iter;       // steps taken (the reference's loop counter)
+  uint32_t maxiter;    // stop when iter + 1 == maxiter (0: no limit)
+  uint32_t budget;     // steps left in the current graph launch
+  uint32_t nan;        // 1: the residual estimate became NaN
 };
 
 struct GmresDev {
@@ -38,3 +44,9 @@ extern "C" int h2b_gmres_init(const GmresDev *g, const GmresOp *op, const double
 extern "C" int h2b_gmres_finish(const GmresDev *g, const GmresOp *op, const double *b, double *x,
                                 cudaStream_t st);
 extern "C" int h2b_gmres_bnorm(const GmresDev *g, const double *b, cudaStream_t st);
+// One graph that runs restarted GMRES steps until the residual estimate reaches state->tol, the
+// step counter reaches maxiter or state->budget steps have run: a WHILE conditional node whose
+// body restarts (finish + init, an IF conditional node) when k + 1 == kmax, takes one step and
+// updates the loop condition on the device.  b and x are the device right-hand side and iterate.
+extern "C" int h2b_gmres_loop_graph(const GmresDev *g, const GmresOp *op, const double *b,
+                                    double *x, cudaStream_t st, cudaGraphExec_t *exec);

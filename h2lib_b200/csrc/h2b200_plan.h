@@ -47,6 +47,13 @@ typedef struct {
   uint32_t nsing;
   size_t csing;
   uint32_t case_start[5];   /* after finalize: singular pairs of case c in [case_start[c], [c+1]) */
+  /* triangle lists already in `refs`, keyed by (index pointer, length, basis): the tiles of one
+   * cluster share a single list (open addressing, capacity a power of two) */
+  const uint32_t **lkey;
+  uint32_t *lkn, *loff, *llen;
+  size_t lcap, lcount;
+  /* 1: leave the singular pairs to the device classification (h2b_near_classify) */
+  int skip_sing;
 } h2b_nearplan;
 
 /* Vertex -> triangle adjacency plus scratch stamps for the plan builder. */

@@ -22,6 +22,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <algorithm>
+
 #include "device_common.cuh"
 #include "h2mvm.h"
 
@@ -246,6 +248,66 @@ __global__ void __launch_bounds__(TPB) backward_chain_kernel(MvmBackArgs a, cons
   }
 }
 
+// Flattened-basis path.  xp = x[idx] and the accumulators are cleared in one launch.
+template <bool CX>
+__global__ void gather_zero_kernel(const double *__restrict__ x, const uint32_t *__restrict__ idx,
+                                   double *__restrict__ xp, uint32_t n, double *__restrict__ z0,
+                                   size_t n0, double *__restrict__ z1, size_t n1,
+                                   double *__restrict__ z2, size_t n2) {
+  const size_t i0 = blockIdx.x * (size_t) blockDim.x + threadIdx.x, st = (size_t) gridDim.x * blockDim.x;
+  for (size_t i = i0; i < n; i += st) {
+    const uint32_t j = idx[i];
+    if (CX) {
+      xp[2 * i] = x[2 * j];
+      xp[2 * i + 1] = x[2 * j + 1];
+    } else {
+      xp[i] = x[j];
+    }
+  }
+  for (size_t i = i0; i < n0; i += st) z0[i] = 0.0;
+  for (size_t i = i0; i < n1; i += st) z1[i] = 0.0;
+  for (size_t i = i0; i < n2; i += st) z2[i] = 0.0;
+}
+
+// Launch 1 (flat): xt_c += W_c^T x over rows [r0, r0 + nr) of c (CTAs < items; W_c^T is k x |c|,
+// ld = k), and the nearfield blocks (the other CTAs).
+template <bool CX>
+__global__ void __launch_bounds__(TPB) forward_flat_near_kernel(MvmFlatArgs f, MvmCoupleArgs c) {
+  constexpr int W = CX ? 2 : 1;
+  __shared__ double red[TPB * W];
+  __shared__ double tmp[KMAXW];
+  if (blockIdx.x >= f.nitems) {
+    const uint32_t nb = blockIdx.x - f.nitems;
+    const uint32_t r = c.near_rc[nb], cc = c.near_cc[nb];
+    panel_mv_atomic<CX>(c.N + (size_t) W * c.near_off[nb], c.rsize[r], c.csize[cc],
+                        c.xp + (size_t) W * c.coff[cc], c.yp + (size_t) W * c.roff[r], red);
+    return;
+  }
+  const uint32_t *it = f.items + 3 * (size_t) blockIdx.x;
+  const uint32_t cl = it[0], r0 = it[1], nr = it[2];
+  const uint32_t k = (uint32_t) f.k;
+  gemv_split<CX, false>(f.W + f.woff[cl] + (size_t) r0 * k, k, k, nr,
+                        c.xp + (size_t) W * (f.off[cl] + r0), red, tmp);
+  for (uint32_t e = threadIdx.x; e < W * k; e += blockDim.x)
+    atomicAdd(const_cast<double *>(&c.xt[(size_t) W * k * cl + e]), tmp[e]);
+}
+
+// Launch 3 (flat): yp[rows r0 .. r0 + nr of c] += W_c[r0:, :] yt_c (W_c is |c| x k, ld = |c|).
+template <bool CX>
+__global__ void __launch_bounds__(TPB) backward_flat_kernel(MvmFlatArgs f, const double *yt,
+                                                            double *yp) {
+  constexpr int W = CX ? 2 : 1;
+  __shared__ double red[TPB * W];
+  __shared__ double tmp[H2B_MVM_FLAT_ROWS * W];
+  const uint32_t *it = f.items + 3 * (size_t) blockIdx.x;
+  const uint32_t cl = it[0], r0 = it[1], nr = it[2];
+  const uint32_t k = (uint32_t) f.k;
+  gemv_split<CX, false>(f.W + f.woff[cl] + r0, f.size[cl], nr, k, yt + (size_t) W * k * cl, red,
+                        tmp);
+  double *y = yp + (size_t) W * (f.off[cl] + r0);
+  for (uint32_t e = threadIdx.x; e < W * nr; e += blockDim.x) atomicAdd(&y[e], tmp[e]);
+}
+
 }  // namespace
 
 extern "C" int h2b_mvm_launch(const MvmPlan *p, const double *x, double *y, double ar, double ai,
@@ -257,10 +319,36 @@ extern "C" int h2b_mvm_launch(const MvmPlan *p, const double *x, double *y, doub
     h2b_set_error("matvec: rank %d > 128", p->k);
     return H2B_ERR_ARG;
   }
-  H2B_CUDA_TRY(cudaMemsetAsync(p->yp, 0, sizeof(double) * W * p->nrow, st));
-  H2B_CUDA_TRY(cudaMemsetAsync(p->yt, 0, sizeof(double) * W * p->k * p->nrow_clusters, st));
   const uint32_t gg = (p->ncol + 255) / 256 < (uint32_t) (4 * sms) ? (p->ncol + 255) / 256
                                                                    : (uint32_t) (4 * sms);
+  if (p->flat) {
+    const MvmCoupleArgs &ca = p->cpl;
+    const uint32_t zn = p->nrow > p->ncol ? p->nrow : p->ncol;
+    const uint32_t gz = std::min<uint32_t>((zn + 255) / 256 + 1, (uint32_t) (4 * sms));
+    const size_t nyp = W * p->nrow, nxt = W * (size_t) p->k * p->ncol_clusters,
+                 nyt = W * (size_t) p->k * p->nrow_clusters;
+    if (cx) {
+      gather_zero_kernel<true><<<gz, 256, 0, st>>>(x, p->cidx, p->xp, p->ncol, p->yp, nyp, p->xt,
+                                                   nxt, p->yt, nyt);
+      if (p->ffwd.nitems + ca.nnear)
+        forward_flat_near_kernel<true><<<p->ffwd.nitems + ca.nnear, TPB, 0, st>>>(p->ffwd, ca);
+      if (ca.nadm) coupling_mv_kernel<true><<<ca.nadm, TPB, 0, st>>>(ca);
+      if (p->fbwd.nitems) backward_flat_kernel<true><<<p->fbwd.nitems, TPB, 0, st>>>(p->fbwd, p->yt, p->yp);
+      scatter_kernel<true><<<gz, 256, 0, st>>>(p->yp, p->ridx, y, p->nrow, ar, ai);
+    } else {
+      gather_zero_kernel<false><<<gz, 256, 0, st>>>(x, p->cidx, p->xp, p->ncol, p->yp, nyp, p->xt,
+                                                    nxt, p->yt, nyt);
+      if (p->ffwd.nitems + ca.nnear)
+        forward_flat_near_kernel<false><<<p->ffwd.nitems + ca.nnear, TPB, 0, st>>>(p->ffwd, ca);
+      if (ca.nadm) coupling_mv_kernel<false><<<ca.nadm, TPB, 0, st>>>(ca);
+      if (p->fbwd.nitems) backward_flat_kernel<false><<<p->fbwd.nitems, TPB, 0, st>>>(p->fbwd, p->yt, p->yp);
+      scatter_kernel<false><<<gz, 256, 0, st>>>(p->yp, p->ridx, y, p->nrow, ar, ai);
+    }
+    H2B_CUDA_TRY(cudaGetLastError());
+    return H2B_OK;
+  }
+  H2B_CUDA_TRY(cudaMemsetAsync(p->yp, 0, sizeof(double) * W * p->nrow, st));
+  H2B_CUDA_TRY(cudaMemsetAsync(p->yt, 0, sizeof(double) * W * p->k * p->nrow_clusters, st));
   const MvmForwardArgs &fa = p->fwd;
   const MvmCoupleArgs &ca = p->cpl;
   const MvmBackArgs &ba = p->bwd;

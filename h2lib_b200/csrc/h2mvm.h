@@ -49,10 +49,23 @@ struct MvmBackArgs {
   int k;
 };
 
+// Flattened-basis transforms (flatbasis.cu builds W): one item = rows [r0, r0 + nr) of cluster c.
+#define H2B_MVM_FLAT_ROWS 128
+struct MvmFlatArgs {
+  const uint32_t *items;      // 3 per item: cluster, first row, rows
+  const uint32_t *off, *size; // per cluster
+  const uint64_t *woff;       // per cluster: offset of W_t
+  const double *W;            // row side |t| x k (ld |t|); column side k x |t| (ld k)
+  uint32_t nitems;
+  int k;
+};
+
 struct MvmPlan {
   int cx, num_sms;
+  int flat;                      // 1: flattened-basis transforms (ffwd / fbwd)
+  MvmFlatArgs ffwd, fbwd;
   int k;
-  uint32_t nrow, ncol, nrow_clusters;
+  uint32_t nrow, ncol, nrow_clusters, ncol_clusters;
   const uint32_t *ridx, *cidx;   // device index arrays of the row / column tree
   double *xp, *yp, *xt, *yt;     // work vectors
   MvmForwardArgs fwd;

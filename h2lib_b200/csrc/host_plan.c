@@ -10,6 +10,7 @@
  * Classification and vertex permutation restate select_quadrature_singquad2d
  * (Library/singquad2d.c:549): the shared vertices come first, in the row triangle's order.
  */
+#include <stdint.h>
 #include <stdlib.h>
 #include <string.h>
 
@@ -85,7 +86,46 @@ void
 h2b_nearplan_free(h2b_nearplan *p)
 {
   free(p->tiles); free(p->refs); free(p->sing);
+  free((void *) p->lkey); free(p->lkn); free(p->loff); free(p->llen);
   memset(p, 0, sizeof(*p));
+}
+
+static size_t
+list_slot(const h2b_nearplan *p, const uint32_t *idx, uint32_t kn)
+{
+  size_t h = ((size_t) (uintptr_t) idx >> 2) * 0x9E3779B97F4A7C15ull ^ (size_t) kn * 0xC2B2AE3D27D4EB4Full;
+  size_t m = p->lcap - 1, i = (h >> 17) & m;
+  while (p->lkey[i] && !(p->lkey[i] == idx && p->lkn[i] == kn))
+    i = (i + 1) & m;
+  return i;
+}
+
+/* Grow the list table to keep it at most half full. */
+static int
+list_reserve(h2b_nearplan *p)
+{
+  size_t i, oc = p->lcap;
+  const uint32_t **ok = p->lkey;
+  uint32_t *okn = p->lkn, *ooff = p->loff, *olen = p->llen;
+  if (2 * (p->lcount + 1) <= p->lcap)
+    return H2B_OK;
+  p->lcap = oc ? 2 * oc : 1024;
+  p->lkey = (const uint32_t **) calloc(p->lcap, sizeof(*p->lkey));
+  p->lkn = (uint32_t *) calloc(p->lcap, sizeof(uint32_t));
+  p->loff = (uint32_t *) calloc(p->lcap, sizeof(uint32_t));
+  p->llen = (uint32_t *) calloc(p->lcap, sizeof(uint32_t));
+  if (!p->lkey || !p->lkn || !p->loff || !p->llen)
+    return H2B_ERR_NOMEM;
+  for (i = 0; i < oc; i++)
+    if (ok[i]) {
+      size_t j = list_slot(p, ok[i], okn[i]);
+      p->lkey[j] = ok[i];
+      p->lkn[j] = okn[i];
+      p->loff[j] = ooff[i];
+      p->llen[j] = olen[i];
+    }
+  free((void *) ok); free(okn); free(ooff); free(olen);
+  return H2B_OK;
 }
 
 static uint32_t
@@ -193,6 +233,32 @@ h2b_pair_code(const uint32_t *tv, const uint32_t *sv)
          | (sp[2] << 12);
 }
 
+/* add_reflist, reusing the list of an index range seen before. */
+static int
+cached_reflist(h2b_nearplan *p, h2b_adjacency *adj, int linear, const uint32_t *idx, uint32_t n,
+               uint32_t *off, uint32_t *len)
+{
+  const uint32_t kn = (n << 1) | (linear ? 1u : 0u);
+  size_t i;
+  int rc;
+  if ((rc = list_reserve(p)) != H2B_OK)
+    return rc;
+  i = list_slot(p, idx, kn);
+  if (p->lkey[i]) {
+    *off = p->loff[i];
+    *len = p->llen[i];
+    return H2B_OK;
+  }
+  if ((rc = add_reflist(p, adj, linear, idx, n, off, len)) != H2B_OK)
+    return rc;
+  p->lkey[i] = idx;
+  p->lkn[i] = kn;
+  p->loff[i] = *off;
+  p->llen[i] = *len;
+  p->lcount++;
+  return H2B_OK;
+}
+
 static int
 add_tile(h2b_nearplan *p, h2b_adjacency *adj, int row_linear, int col_linear,
          const uint32_t *ridx, uint32_t rows, const uint32_t *cidx, uint32_t cols,
@@ -206,9 +272,9 @@ add_tile(h2b_nearplan *p, h2b_adjacency *adj, int row_linear, int col_linear,
     tr_off = reuse_tr_off;
     tr_len = reuse_tr_len;
   }
-  else if ((rc = add_reflist(p, adj, row_linear, ridx, rows, &tr_off, &tr_len)) != H2B_OK)
+  else if ((rc = cached_reflist(p, adj, row_linear, ridx, rows, &tr_off, &tr_len)) != H2B_OK)
     return rc;
-  if ((rc = add_reflist(p, adj, col_linear, cidx, cols, &sc_off, &sc_len)) != H2B_OK)
+  if ((rc = cached_reflist(p, adj, col_linear, cidx, cols, &sc_off, &sc_len)) != H2B_OK)
     return rc;
 
   GROW(p->tiles, p->ntiles, p->ctiles, 1, h2b_tile);
@@ -224,6 +290,10 @@ add_tile(h2b_nearplan *p, h2b_adjacency *adj, int row_linear, int col_linear,
   tl->flags = ntrans ? 1u : 0u;
   tl->pad = 0;
 
+  if (p->skip_sing) {
+    p->ntiles++;
+    return H2B_OK;
+  }
   /* singular pairs: row triangles sharing a vertex with a column triangle */
   gt = next_gen(adj);
   for (i = 0; i < tr_len; i++) {

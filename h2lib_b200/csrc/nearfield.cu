@@ -21,6 +21,7 @@
 // the reference's A(1-t) + B(t-s) + C s map on both triangles, without forming x and y first.
 #include <cuda_runtime.h>
 #include <stdint.h>
+#include <string.h>
 
 #include "device_common.cuh"
 #include "h2b200_plan.h"
@@ -48,19 +49,29 @@ __host__ __device__ constexpr int dist_off(int q) {
 }
 __constant__ double c_dist[5][DIST_TOTAL];
 
-// Kernel values at difference d = x - y; ns = unit normal of the column triangle.
+// The distant rule is the tensor product of one q^2-point rule per triangle (the single-triangle
+// rule of Library/singquad2d.c:25: t = g_i, s = g_i g_j, w = gw_i gw_j g_i), so its weight
+// factors as w = w_x w_y.  Per order q and point p < q^2: rows t, s, w, w (1-t), w (t-s), w s
+// (the raw weight and the three linear nodal functions times the weight).
+constexpr int SIDE_MAXP = 25;
+// 1: distant pairs of the specialised orders use the factored sum (dist_pair_tensor); 0: the
+// point-by-point sum over the q^4 table.
+#ifndef H2B_DIST_TENSOR
+#define H2B_DIST_TENSOR 1
+#endif
+__constant__ double c_side[5][6][SIDE_MAXP];
+
+// Kernel values from r^2 = |x - y|^2 and dot = <x - y, n_y> (n_y: unit normal of the column
+// triangle; read only by the double layer kernels).
 template <int KK>
-__device__ __forceinline__ void eval_kernel(double dx, double dy, double dz, double n0, double n1,
-                                            double n2, double k_re, double k_imn, double kv[2]) {
-  double r2 = fma(dx, dx, fma(dy, dy, dz * dz));
+__device__ __forceinline__ void eval_kernel(double r2, double dot, double k_re, double k_imn,
+                                            double kv[2]) {
   double rinv = rsqrt_nr(r2);
   if constexpr (KK == KK_LSLP) {
     kv[0] = rinv;
   } else if constexpr (KK == KK_LDLP) {
-    double dot = fma(dx, n0, fma(dy, n1, dz * n2));
     kv[0] = dot * (rinv * rinv * rinv);
   } else if constexpr (KK == KK_LBOTH) {
-    double dot = fma(dx, n0, fma(dy, n1, dz * n2));
     kv[0] = rinv;
     kv[1] = dot * (rinv * rinv * rinv);
   } else if constexpr (KK == KK_HSLP) {
@@ -70,7 +81,6 @@ __device__ __forceinline__ void eval_kernel(double dx, double dy, double dz, dou
     kv[0] = rn * c;
     kv[1] = rn * s;
   } else {  // KK_HDLP
-    double dot = fma(dx, n0, fma(dy, n1, dz * n2));
     double re = (rinv * rinv * rinv) * dot, r = r2 * rinv, s, c;
     if (k_imn != 0.0) re *= exp(k_imn * r);
     double kr = k_re * r;
@@ -78,6 +88,11 @@ __device__ __forceinline__ void eval_kernel(double dx, double dy, double dz, dou
     kv[0] = fma(kr, s, c) * re;
     kv[1] = fma(-c, kr, s) * re;
   }
+}
+
+template <int KK>
+constexpr bool uses_normal() {
+  return KK == KK_LDLP || KK == KK_LBOTH || KK == KK_HDLP;
 }
 
 __device__ __forceinline__ double vtx(const TriRec &T, int i, int d) {
@@ -125,7 +140,9 @@ __device__ __forceinline__ void quad_point(const PairGeo &g, double tx, double s
   double dy = fma(-sy, g.q2[1], fma(-ty, g.q1[1], fma(sx, g.p2[1], fma(tx, g.p1[1], g.d0[1]))));
   double dz = fma(-sy, g.q2[2], fma(-ty, g.q1[2], fma(sx, g.p2[2], fma(tx, g.p1[2], g.d0[2]))));
   double kv[2];
-  eval_kernel<KK>(dx, dy, dz, n0, n1, n2, k_re, k_imn, kv);
+  const double r2 = fma(dx, dx, fma(dy, dy, dz * dz));
+  const double dot = uses_normal<KK>() ? fma(dx, n0, fma(dy, n1, dz * n2)) : 0.0;
+  eval_kernel<KK>(r2, dot, k_re, k_imn, kv);
   if constexpr (!RL && !CL) {
 #pragma unroll
     for (int c = 0; c < NCH; c++) acc[c][0][0] = fma(w, kv[c], acc[c][0][0]);
@@ -143,6 +160,58 @@ __device__ __forceinline__ void quad_point(const PairGeo &g, double tx, double s
         for (int j = 0; j < (CL ? 3 : 1); j++)
           acc[c][i][j] = RL ? fma(pr[i], u[j], acc[c][i][j]) : acc[c][i][j] + u[j];
     }
+  }
+}
+
+// One distant pair with the q^4 tensor rule, summed column side first:
+//   acc[c][i][j] = sum_a w_a phi_i(x_a) sum_b w_b phi_j(y_b) k_c(x_a, y_b).
+// With X_a = x_a - A_s and Y_b = y_b - A_s the difference is x_a - y_b = X_a - Y_b and the double
+// layer's <x - y, n_y> = <X_a, n_y> - <Y_b, n_y>; X_a, Y_b and their normal components are formed
+// once per point instead of once per point pair.  Same sum as quad_point over the q^4 points, in
+// another order (differences at rounding level).
+template <int Q, int KK, bool RL, bool CL>
+__device__ __forceinline__ void dist_pair_tensor(const PairGeo &g, double n0, double n1, double n2,
+                                                 double k_re, double k_imn,
+                                                 double (&acc)[KT<KK>::NCH][RL ? 3 : 1][CL ? 3 : 1]) {
+  constexpr int NCH = KT<KK>::NCH, NC = CL ? 3 : 1, NR = RL ? 3 : 1, P = Q * Q;
+  constexpr bool DOT = uses_normal<KK>();
+  const double(&sd)[6][SIDE_MAXP] = c_side[Q - 1];
+  double yb[P][3], nyb[P];
+#pragma unroll
+  for (int b = 0; b < P; b++) {
+#pragma unroll
+    for (int d = 0; d < 3; d++) yb[b][d] = fma(sd[1][b], g.q2[d], sd[0][b] * g.q1[d]);
+    nyb[b] = DOT ? fma(yb[b][0], n0, fma(yb[b][1], n1, yb[b][2] * n2)) : 0.0;
+  }
+#pragma unroll
+  for (int a = 0; a < P; a++) {
+    double xa[3];
+#pragma unroll
+    for (int d = 0; d < 3; d++) xa[d] = fma(sd[1][a], g.p2[d], fma(sd[0][a], g.p1[d], g.d0[d]));
+    const double nxa = DOT ? fma(xa[0], n0, fma(xa[1], n1, xa[2] * n2)) : 0.0;
+    double in[NCH][NC];
+#pragma unroll
+    for (int c = 0; c < NCH; c++)
+#pragma unroll
+      for (int j = 0; j < NC; j++) in[c][j] = 0.0;
+#pragma unroll
+    for (int b = 0; b < P; b++) {
+      const double dx = xa[0] - yb[b][0], dy = xa[1] - yb[b][1], dz = xa[2] - yb[b][2];
+      const double r2 = fma(dx, dx, fma(dy, dy, dz * dz));
+      double kv[2];
+      eval_kernel<KK>(r2, nxa - nyb[b], k_re, k_imn, kv);
+#pragma unroll
+      for (int c = 0; c < NCH; c++)
+#pragma unroll
+        for (int j = 0; j < NC; j++) in[c][j] = fma(sd[CL ? 3 + j : 2][b], kv[c], in[c][j]);
+    }
+#pragma unroll
+    for (int c = 0; c < NCH; c++)
+#pragma unroll
+      for (int i = 0; i < NR; i++)
+#pragma unroll
+        for (int j = 0; j < NC; j++)
+          acc[c][i][j] = fma(sd[RL ? 3 + i : 2][a], in[c][j], acc[c][i][j]);
   }
 }
 
@@ -213,10 +282,14 @@ __global__ void __launch_bounds__(256, H2B_DIST_MINBLOCKS) near_dist_kernel(Dist
         for (int j = 0; j < NC; j++) acc[c][i][j] = 0.0;
 
     if constexpr (Q > 0) {
+#if H2B_DIST_TENSOR
+      dist_pair_tensor<Q, KK, RL, CL>(g, n0, n1, n2, a.k_re, a.k_imn, acc);
+#else
 #pragma unroll
       for (int k = 0; k < Q * Q * Q * Q; k++)
         quad_point<KK, RL, CL>(g, cx0[k], cx1[k], cy0[k], cy1[k], cw[k], n0, n1, n2, a.k_re,
                                a.k_imn, acc);
+#endif
     } else {
       for (int k = 0; k < nq; k++)
         quad_point<KK, RL, CL>(g, cx0[k], cx1[k], cy0[k], cy1[k], cw[k], n0, n1, n2, a.k_re,
@@ -522,7 +595,104 @@ int launch_kk(const h2b_near_launch *L, cudaStream_t st) {
   return launch_kk_basis<KK, false, false>(L, st);
 }
 
+// Vertex permutation of a pair, the device twin of h2b_pair_code (host_plan.c): number of shared
+// vertices in bits 0-1, the row triangle's order (shared vertices first) in bits 2-7, the column
+// triangle's in bits 8-13 (select_quadrature_singquad2d, Library/singquad2d.c:549).
+__device__ uint32_t pair_code_dev(const uint32_t tv[3], const uint32_t sv[3]) {
+  uint32_t p = 0, tp[3] = {0, 1, 2}, sp[3] = {0, 1, 2};
+  for (int i = 0; i < 3; i++)
+    for (int j = 0; j < 3; j++) p += (tv[i] == sv[j]);
+  if (p == 1 || p == 2) {
+    uint32_t c = 0;
+    for (uint32_t i = 0; i < 3; i++)
+      for (uint32_t j = 0; j < 3; j++)
+        if (tv[i] == sv[j]) {
+          tp[c] = i;
+          sp[c] = j;
+          c++;
+          break;
+        }
+    uint32_t q = c;
+    for (uint32_t i = 0; i < 3; i++) {
+      uint32_t j = 0;
+      while (j < q && tv[i] != tv[tp[j]]) j++;
+      if (j == q) tp[q++] = i;
+    }
+    q = c;
+    for (uint32_t i = 0; i < 3; i++) {
+      uint32_t j = 0;
+      while (j < q && sv[i] != sv[sp[j]]) j++;
+      if (j == q) sp[q++] = i;
+    }
+  }
+  if (p > 3) p = 3;
+  return p | (tp[0] << 2) | (tp[1] << 4) | (tp[2] << 6) | (sp[0] << 8) | (sp[1] << 10) |
+         (sp[2] << 12);
+}
+
+// One CTA per tile, a thread per triangle pair; warp-aggregated atomics per case.
+template <bool WRITE>
+__global__ void __launch_bounds__(256) classify_kernel(const TriRec *tri, const TriRef *refs,
+                                                       const h2b_tile *tiles, uint32_t *cursor,
+                                                       const uint32_t *base, h2b_sing *out) {
+  const h2b_tile tl = tiles[blockIdx.x];
+  const uint32_t ntr = tl.tr_len, npairs = tl.tr_len * tl.sc_len;
+  const uint32_t lane = threadIdx.x & 31;
+  for (uint32_t p0 = 0; p0 < npairs; p0 += blockDim.x) {
+    const uint32_t p = p0 + threadIdx.x;
+    uint32_t code = 0, cs = 0, is = 0, it = 0;
+    if (p < npairs) {
+      is = p / ntr;
+      it = p - is * ntr;
+      const TriRec &T = tri[refs[tl.tr_off + it].t];
+      const TriRec &S = tri[refs[tl.sc_off + is].t];
+      const uint32_t tv[3] = {T.v[0], T.v[1], T.v[2]}, sv[3] = {S.v[0], S.v[1], S.v[2]};
+      bool shared = false;
+#pragma unroll
+      for (int i = 0; i < 3; i++)
+#pragma unroll
+        for (int j = 0; j < 3; j++) shared |= tv[i] == sv[j];
+      if (shared) {
+        code = pair_code_dev(tv, sv);
+        cs = code & 3u;
+      }
+    }
+    // every thread of the warp reaches the ballots (the loop bound is uniform per CTA)
+#pragma unroll
+    for (uint32_t c = 1; c <= 3; c++) {
+      const unsigned m = __ballot_sync(0xffffffffu, cs == c);
+      if (m == 0) continue;
+      const uint32_t leader = __ffs(m) - 1;
+      uint32_t b = 0;
+      if (lane == leader) b = atomicAdd(&cursor[c], (uint32_t) __popc(m));
+      b = __shfl_sync(0xffffffffu, b, leader);
+      if (WRITE && cs == c) {
+        h2b_sing sg;
+        sg.tile = blockIdx.x;
+        sg.tr = tl.tr_off + it;
+        sg.sc = tl.sc_off + is;
+        sg.code = code;
+        out[base[c] + b + __popc(m & ((1u << lane) - 1u))] = sg;
+      }
+    }
+  }
+}
+
 }  // namespace
+
+extern "C" int h2b_near_classify(const void *tri, const void *refs, const h2b_tile *tiles,
+                                 uint32_t ntiles, uint32_t *cursor, const uint32_t *base,
+                                 h2b_sing *sing, cudaStream_t st) {
+  if (ntiles == 0) return H2B_OK;
+  if (sing)
+    classify_kernel<true><<<ntiles, 256, 0, st>>>((const TriRec *) tri, (const TriRef *) refs,
+                                                  tiles, cursor, base, sing);
+  else
+    classify_kernel<false><<<ntiles, 256, 0, st>>>((const TriRec *) tri, (const TriRef *) refs,
+                                                   tiles, cursor, nullptr, nullptr);
+  H2B_CUDA_TRY(cudaGetLastError());
+  return H2B_OK;
+}
 
 extern "C" int h2b_near_upload_dist_rules(void) {
   static double host[5][DIST_TOTAL];
@@ -541,6 +711,25 @@ extern "C" int h2b_near_upload_dist_rules(void) {
     h2b_quad_free(&qd);
   }
   H2B_CUDA_TRY(cudaMemcpyToSymbol(c_dist, host, sizeof(host)));
+
+  static double side[5][6][SIDE_MAXP];
+  memset(side, 0, sizeof(side));
+  for (int q = 1; q <= 5; q++) {
+    double g[8], gw[8];
+    int rc = h2b_gauss_legendre01((uint32_t) q, g, gw);
+    if (rc != H2B_OK) return rc;
+    for (int i = 0, p = 0; i < q; i++)
+      for (int j = 0; j < q; j++, p++) {
+        const double t = g[i], s = g[i] * g[j], w = gw[i] * gw[j] * g[i];
+        side[q - 1][0][p] = t;
+        side[q - 1][1][p] = s;
+        side[q - 1][2][p] = w;
+        side[q - 1][3][p] = w * (1.0 - t);
+        side[q - 1][4][p] = w * (t - s);
+        side[q - 1][5][p] = w * s;
+      }
+  }
+  H2B_CUDA_TRY(cudaMemcpyToSymbol(c_side, side, sizeof(side)));
   return H2B_OK;
 }
 

@@ -40,6 +40,12 @@ typedef struct {
 } h2b_near_launch;
 
 int h2b_near_upload_dist_rules(void);
+/* Singular pairs of a tile list on the device (the pairs that share a vertex, with the vertex
+ * permutation code of h2b_pair_code).  sing == NULL: add the number of pairs of each case c to
+ * cursor[c] (c = 1 vertex, 2 edge, 3 identical).  Otherwise write the pairs of case c to
+ * sing[base[c] + cursor[c]++] (cursor zeroed by the caller); the order inside a case is not fixed. */
+int h2b_near_classify(const void *tri, const void *refs, const h2b_tile *tiles, uint32_t ntiles,
+                      uint32_t *cursor, const uint32_t *base, h2b_sing *sing, cudaStream_t st);
 int h2b_near_launch_kernels(const h2b_near_launch *L, cudaStream_t st);
 
 #ifdef __cplusplus
