@@ -43,6 +43,8 @@ _SIGS = {
     "h2b_tree_new_flat": (vp, [C.c_uint32, _u32p, _u32p, _u32p, _f64p, C.c_uint32, _u32p,
                                C.c_uint32, _u32p, _u32p, _u32p, _f64p, C.c_uint32, _u32p,
                                C.c_uint32, _u32p, _u32p, _u8p]),
+    "h2b_tree_new_forest": (vp, [C.c_uint32, _u32p, _u32p, _f64p, _u32p, C.c_int, C.c_int,
+                                 C.c_uint32, C.c_double]),
     "h2b_tree_del": (None, [vp]),
     "h2b_tree_info": (C.c_int, [vp, _u64p]),
     "h2b_tree_export_clusters": (C.c_int, [vp, C.c_int, vp, vp, vp]),
@@ -73,12 +75,22 @@ _SIGS = {
                                              C.c_uint64, vp, C.c_uint64]),
     "h2b_solve_gmres": (C.c_int, [C.c_uint32, vp, _f64p, vp, vp, C.c_double, C.c_uint32,
                                   C.c_uint32]),
+    "h2b_solve_gmres_batch": (C.c_int, [C.c_uint32, vp, _f64p, C.c_uint32, _u32p, C.c_uint32,
+                                        vp, vp, C.c_double, C.c_uint32, C.c_uint32, C.c_uint32,
+                                        _u32p]),
+    "h2b_solve_gmres_mixed": (C.c_int, [C.c_uint32, vp, _f64p, vp, vp, C.c_double, C.c_uint32,
+                                        C.c_uint32]),
+    "h2b_h2matrix_make_single": (C.c_int, [vp]),
+    "h2b_h2matrix_addeval_single": (C.c_int, [C.c_double, C.c_double, vp, vp, vp]),
     "h2b_residual_norm": (C.c_int, [C.c_uint32, vp, _f64p, vp, vp, C.POINTER(C.c_double)]),
     "h2b_solve_gmres_noalloc": (C.c_int, [C.c_uint32, vp, _f64p, vp, vp, C.c_double,
                                           C.c_uint32, C.c_uint32]),
     "h2b_project_l2_harmonic": (C.c_int, [vp, _f64p, vp]),
     "h2b_l2_error_harmonic": (C.c_int, [vp, _f64p, vp, C.POINTER(C.c_double),
                                         C.POINTER(C.c_double)]),
+    "h2b_project_l2_harmonic_multi": (C.c_int, [vp, C.c_uint32, _u32p, C.c_uint32, _f64p, vp]),
+    "h2b_l2_error_harmonic_multi": (C.c_int, [vp, C.c_uint32, _u32p, C.c_uint32, _f64p, vp,
+                                              _f64p, _f64p]),
     "h2b_integrate_plane_wave": (C.c_int, [vp, _f64p, _f64p, C.c_double, C.c_double, vp]),
 }
 

@@ -96,6 +96,21 @@ def new_ellipsoid_surface3d(split, axes):
     return Surface3d(x, t)
 
 
+def union_surface3d(surfaces):
+    """One Surface3d holding several disjoint surfaces (vertices and triangles concatenated, the
+    triangles' vertex ids shifted).  Returns (surface, vertex_off, triangle_off): surface m owns
+    vertices [vertex_off[m], vertex_off[m+1]) and triangles [triangle_off[m], triangle_off[m+1])."""
+    voff = np.zeros(len(surfaces) + 1, dtype=np.uint32)
+    toff = np.zeros(len(surfaces) + 1, dtype=np.uint32)
+    for m, gr in enumerate(surfaces):
+        voff[m + 1] = voff[m] + gr.vertices
+        toff[m + 1] = toff[m] + gr.triangles
+    x = np.concatenate([gr.x for gr in surfaces])
+    t = np.concatenate([gr.t.astype(np.uint64) + int(voff[m])
+                        for m, gr in enumerate(surfaces)]).astype(np.uint32)
+    return Surface3d(x, t), voff, toff
+
+
 class Bem3d:
     """Operator handle: the counterpart of H2Lib's pbem3d (Library/bem3d.h:290)."""
 
@@ -211,6 +226,16 @@ def build_tree(gr, row_basis, col_basis, clf, eta):
                                         col_basis, clf, eta), "h2b_tree_new"))
 
 
+def build_forest(gr, vertex_off, triangle_off, row_basis, col_basis, clf, eta):
+    """Cluster and block trees of every surface of a union (union_surface3d), side by side: the
+    H2 matrix on this forest is block diagonal, one block per surface."""
+    return Tree(checkp(lib.h2b_tree_new_forest(len(vertex_off) - 1,
+                                               np.ascontiguousarray(vertex_off, dtype=np.uint32),
+                                               np.ascontiguousarray(triangle_off, dtype=np.uint32),
+                                               gr.x, gr.t, row_basis, col_basis, clf, eta),
+                       "h2b_tree_new_forest"))
+
+
 class H2Matrix:
     """Device H2 matrix with Chebyshev interpolation (setup_h2matrix_aprx_inter_bem3d,
     Library/bem3d.c:9658)."""
@@ -223,6 +248,11 @@ class H2Matrix:
     def assemble(self):
         """assemble_bem3d_h2matrix_row/col_clusterbasis + assemble_bem3d_h2matrix."""
         check(lib.h2b_h2matrix_assemble_all(self.handle), "h2matrix_assemble_all")
+        return self
+
+    def make_single(self):
+        """FP32 copies of N, S and the flattened bases for mixed-precision products."""
+        check(lib.h2b_h2matrix_make_single(self.handle), "h2matrix_make_single")
         return self
 
     def info(self):
@@ -266,6 +296,14 @@ class H2Matrix:
             self.handle = None
 
 
+def addeval_h2matrix_avector_single(alpha, h2, x, y):
+    """y += alpha * A x from the FP32 copies of the matrix (H2Matrix.make_single)."""
+    alpha = complex(alpha)
+    check(lib.h2b_h2matrix_addeval_single(alpha.real, alpha.imag, h2.handle, _ptr(x), _ptr(y)),
+          "addeval_h2matrix_avector_single")
+    return y
+
+
 def addeval_h2matrix_avector(alpha, h2, x, y):
     """y += alpha * A x (Library/h2matrix.c:1269)."""
     alpha = complex(alpha)
@@ -282,6 +320,39 @@ def solve_gmres(ops, coefs, b, x, eps, maxiter, kmax):
         cf[2 * i], cf[2 * i + 1] = complex(c).real, complex(c).imag
     return check(lib.h2b_solve_gmres(len(ops), C.cast(arr, C.c_void_p), cf, _ptr(b), _ptr(x),
                                      eps, maxiter, kmax), "solve_gmres")
+
+
+SOLVE_MIXED = 1
+
+
+def _coefs(ops, coefs):
+    arr = (C.c_void_p * len(ops))(*[o.handle for o in ops])
+    cf = np.zeros(2 * len(ops))
+    for i, c in enumerate(coefs):
+        cf[2 * i], cf[2 * i + 1] = complex(c).real, complex(c).imag
+    return C.cast(arr, C.c_void_p), cf, arr
+
+
+def solve_gmres_batch(ops, coefs, system_off, b, x, eps, maxiter, kmax, nrhs=1, mixed=False):
+    """Independent GMRES solves of the diagonal blocks [system_off[s], system_off[s+1]) of a block
+    diagonal operator (an H2 matrix on a forest), all in one device loop; with nrhs > 1, b and x
+    hold nrhs columns.  mixed: FP32 Arnoldi steps, FP64 residuals (make_single first).  Returns
+    the iteration counts, shape (nrhs, systems)."""
+    ptr, cf, _keep = _coefs(ops, coefs)
+    off = np.ascontiguousarray(system_off, dtype=np.uint32)
+    iters = np.zeros(nrhs * (off.size - 1), dtype=np.uint32)
+    check(lib.h2b_solve_gmres_batch(len(ops), ptr, cf, off.size - 1, off, nrhs, _ptr(b),
+                                    _ptr(x), eps, maxiter, kmax, SOLVE_MIXED if mixed else 0,
+                                    iters), "solve_gmres_batch")
+    return iters.reshape(nrhs, off.size - 1)
+
+
+def solve_gmres_mixed(ops, coefs, b, x, eps, maxiter, kmax):
+    """solve_gmres with FP32 Arnoldi steps and FP64 residuals (iterative refinement); the
+    operators need their FP32 copies (H2Matrix.make_single)."""
+    ptr, cf, _keep = _coefs(ops, coefs)
+    return check(lib.h2b_solve_gmres_mixed(len(ops), ptr, cf, _ptr(b), _ptr(x), eps, maxiter,
+                                           kmax), "solve_gmres_mixed")
 
 
 def solve_gmres_h2matrix_avector(A, b, x, eps, maxiter, kmax):
@@ -316,6 +387,33 @@ def l2_error_harmonic(bem, z, u):
     check(lib.h2b_l2_error_harmonic(bem.handle, np.asarray(z, dtype=np.float64), _ptr(u),
                                     C.byref(e), C.byref(n)), "l2_error_harmonic")
     return e.value, n.value
+
+
+def project_l2_harmonic_multi(bem, triangle_off, zs, w=None):
+    """project_l2_harmonic on a union of surfaces with one source per (column, surface):
+    zs has shape (nrhs, surfaces, 3); returns w of shape (nrhs, vertices)."""
+    zs = np.ascontiguousarray(zs, dtype=np.float64)
+    nrhs, nseg = zs.shape[0], zs.shape[1]
+    if w is None:
+        w = np.zeros((nrhs, bem.gr.vertices))
+    check(lib.h2b_project_l2_harmonic_multi(bem.handle, nseg,
+                                            np.ascontiguousarray(triangle_off, dtype=np.uint32),
+                                            nrhs, zs.reshape(-1), _ptr(w)),
+          "project_l2_harmonic_multi")
+    return w
+
+
+def l2_error_harmonic_multi(bem, triangle_off, zs, u):
+    """l2_error_harmonic per (column, surface); returns (err, norm), each (nrhs, surfaces)."""
+    zs = np.ascontiguousarray(zs, dtype=np.float64)
+    nrhs, nseg = zs.shape[0], zs.shape[1]
+    err = np.zeros(nrhs * nseg)
+    nrm = np.zeros(nrhs * nseg)
+    check(lib.h2b_l2_error_harmonic_multi(bem.handle, nseg,
+                                          np.ascontiguousarray(triangle_off, dtype=np.uint32),
+                                          nrhs, zs.reshape(-1), _ptr(u), err, nrm),
+          "l2_error_harmonic_multi")
+    return err.reshape(nrhs, nseg), nrm.reshape(nrhs, nseg)
 
 
 def integrate_plane_wave(bem, kvec, src=(0.0, 0.0, 0.0), coef=1.0, b=None):

@@ -135,10 +135,11 @@ static int devtree_build(DevCTree &t, const h2b_ctree &c, int basis, uint32_t m,
       vtot += (uint64_t) c.size[i] * k;
       t.max_rows = std::max(t.max_rows, c.size[i]);
     }
-    if (i > 0) nonroot.push_back(i);
+    if (c.father[i] != UINT32_MAX) nonroot.push_back(i);  // every root of a forest excluded
     box_points(c.bmin + 3 * (size_t) i, c.bmax + 3 * (size_t) i, m, pts.data() + (size_t) i * 3 * m);
   }
   t.vtotal = vtot;
+  t.nnonroot = (uint32_t) nonroot.size();
   t.nleaves = (uint32_t) leaves.size();
   t.leaves = leaves;
   // clusters by level
@@ -196,6 +197,7 @@ extern "C" void h2b_h2matrix_del(h2b_h2matrix *h) {
   if (h->st) cudaStreamSynchronize(h->st);
   devtree_free(h->rt);
   devtree_free(h->ct);
+  dfree(h->rt.f_W); dfree(h->ct.f_W); dfree(h->f_N); dfree(h->f_S);
   dfree(h->d_adm_rc); dfree(h->d_adm_cc); dfree(h->d_S);
   dfree(h->d_near_rc); dfree(h->d_near_cc); dfree(h->d_near_off); dfree(h->d_N);
   dfree(h->d_tiles); dfree(h->d_refs); dfree(h->d_sing);
@@ -390,19 +392,44 @@ void h2b_h2_fill_mvm_plan(h2b_h2matrix *h) {
   p.fwd = MvmForwardArgs{h->ct.d_leaves, h->ct.d_father, h->ct.d_son0, h->ct.d_son1,
                          h->ct.d_size, h->ct.d_off, h->ct.d_voff, h->ct.d_V, h->ct.d_E, h->d_xp,
                          h->d_xt, h->ct.d_counter, h->ct.nleaves, (int) h->k};
-  p.cpl = MvmCoupleArgs{h->d_adm_rc, h->d_adm_cc, h->d_S, h->d_near_rc, h->d_near_cc,
-                        h->d_near_off, h->d_N, h->rt.d_size, h->ct.d_size, h->rt.d_off,
-                        h->ct.d_off, h->d_xt, h->d_xp, h->d_yt, h->d_yp, h->nadm, h->nnear,
-                        (int) h->k};
+  MvmCoupleArgs &c = p.cpl;
+  c.adm_rc = h->d_adm_rc;
+  c.adm_cc = h->d_adm_cc;
+  c.S = h->d_S;
+  c.near_rc = h->d_near_rc;
+  c.near_cc = h->d_near_cc;
+  c.near_off = h->d_near_off;
+  c.N = h->d_N;
+  c.Ss = h->f_S;
+  c.Ns = h->f_N;
+  c.rsize = h->rt.d_size;
+  c.csize = h->ct.d_size;
+  c.roff = h->rt.d_off;
+  c.coff = h->ct.d_off;
+  c.xt = h->d_xt;
+  c.xp = h->d_xp;
+  c.yt = h->d_yt;
+  c.yp = h->d_yp;
+  c.nadm = h->nadm;
+  c.nnear = h->nnear;
+  c.k = (int) h->k;
   p.down = MvmDownArgs{nullptr, h->rt.d_father, h->rt.d_E, h->d_yt, (int) h->k};
   p.bwd = MvmBackArgs{h->rt.d_leaves, h->rt.d_size, h->rt.d_off, h->rt.d_voff, h->rt.d_V,
                       h->d_yt, h->d_yp, h->rt.nleaves, (int) h->k};
   p.flat = h->flat;
   p.ncol_clusters = h->ct.n;
-  p.ffwd = MvmFlatArgs{h->ct.d_mitems, h->ct.d_off, h->ct.d_size, h->ct.d_woff, h->ct.d_W,
-                       h->ct.nmitems, (int) h->k};
-  p.fbwd = MvmFlatArgs{h->rt.d_mitems, h->rt.d_off, h->rt.d_size, h->rt.d_woff, h->rt.d_W,
-                       h->rt.nmitems, (int) h->k};
+  for (int side = 0; side < 2; side++) {
+    const DevCTree &t = side ? h->rt : h->ct;
+    MvmFlatArgs &f = side ? p.fbwd : p.ffwd;
+    f.items = t.d_mitems;
+    f.off = t.d_off;
+    f.size = t.d_size;
+    f.woff = t.d_woff;
+    f.W = t.d_W;
+    f.Ws = t.f_W;
+    f.nitems = t.nmitems;
+    f.k = (int) h->k;
+  }
   p.level_list = h->rt.d_levels;
   p.rdepth = std::min<uint32_t>(h->rt.depth, 64);
   for (uint32_t l = 0; l <= p.rdepth; l++) p.level_start[l] = h->rt.level_start[l];
@@ -437,7 +464,7 @@ static int assemble_basis(h2b_h2matrix *h, DevCTree &t, int basis, int dn) {
   la.ns = (int) h->ns;
   int rc = h2b_far_leaf_basis(&la, basis == H2B_BASIS_LINEAR, dn, h->st);
   if (rc != H2B_OK) return rc;
-  FarTransferArgs ta{t.d_nonroot, t.d_father, t.d_pts, t.d_E, t.n - 1, (int) h->m, (int) h->k,
+  FarTransferArgs ta{t.d_nonroot, t.d_father, t.d_pts, t.d_E, t.nnonroot, (int) h->m, (int) h->k,
                      transposed};
   rc = h2b_far_transfer(&ta, h->st);
   if (rc == H2B_OK && h->flat) rc = devtree_flatten(t, h->k, transposed, h->st);
@@ -448,7 +475,53 @@ static int assemble_basis(h2b_h2matrix *h, DevCTree &t, int basis, int dn) {
 // 3 nearfield; event 7 separates the distant and singular nearfield kernels; 9/10 the matvec).
 static void mark(h2b_h2matrix *h, int e) { cudaEventRecord(h->ev[e], h->st); }
 
+// Free the FP32 copies (they no longer match the matrix once any part is reassembled).
+static void drop_single(h2b_h2matrix *h) {
+  if (!h->f_N && !h->f_S && !h->rt.f_W && !h->ct.f_W) return;
+  cudaStreamSynchronize(h->st);
+  dfree(h->f_N);
+  dfree(h->f_S);
+  dfree(h->rt.f_W);
+  dfree(h->ct.f_W);
+  h2b_h2_fill_mvm_plan(h);
+}
+
+extern "C" int h2b_h2matrix_make_single(h2b_h2matrix *h) {
+  if (!h) return H2B_ERR_ARG;
+  if (!h->flat) {
+    h2b_set_error("h2b_h2matrix_make_single: needs the flattened-basis matvec");
+    return H2B_ERR_STATE;
+  }
+  drop_single(h);
+  const uint64_t W = h->cx ? 2 : 1;
+  const uint64_t nN = W * h->near_total, nS = W * (uint64_t) h->nadm * h->k * h->k;
+  if (cudaMalloc(&h->f_N, sizeof(float) * std::max<uint64_t>(nN, 1)) != cudaSuccess ||
+      cudaMalloc(&h->f_S, sizeof(float) * std::max<uint64_t>(nS, 1)) != cudaSuccess ||
+      cudaMalloc(&h->rt.f_W, sizeof(float) * std::max<uint64_t>(h->rt.wtotal, 1)) != cudaSuccess ||
+      cudaMalloc(&h->ct.f_W, sizeof(float) * std::max<uint64_t>(h->ct.wtotal, 1)) != cudaSuccess) {
+    cudaGetLastError();
+    drop_single(h);
+    h2b_set_error("h2b_h2matrix_make_single: device allocation failed");
+    return H2B_ERR_NOMEM;
+  }
+  int rc = h2b_to_single(h->d_N, h->f_N, nN, h->num_sms, h->st);
+  if (rc == H2B_OK) rc = h2b_to_single(h->d_S, h->f_S, nS, h->num_sms, h->st);
+  if (rc == H2B_OK) rc = h2b_to_single(h->rt.d_W, h->rt.f_W, h->rt.wtotal, h->num_sms, h->st);
+  if (rc == H2B_OK) rc = h2b_to_single(h->ct.d_W, h->ct.f_W, h->ct.wtotal, h->num_sms, h->st);
+  if (rc == H2B_OK && cudaStreamSynchronize(h->st) != cudaSuccess) {
+    h2b_set_error("h2b_h2matrix_make_single: %s", cudaGetErrorString(cudaGetLastError()));
+    rc = H2B_ERR_CUDA;
+  }
+  if (rc != H2B_OK) {
+    drop_single(h);
+    return rc;
+  }
+  h2b_h2_fill_mvm_plan(h);
+  return H2B_OK;
+}
+
 static int finish(h2b_h2matrix *h, int rc, unsigned phases) {
+  drop_single(h);
   if (rc != H2B_OK) return rc;
   if (cudaStreamSynchronize(h->st) != cudaSuccess) {
     h2b_set_error("h2matrix: %s", cudaGetErrorString(cudaGetLastError()));
@@ -700,8 +773,21 @@ extern "C" int h2b_h2matrix_addeval_multi(double alpha_re, double alpha_im,
   return H2B_OK;
 }
 
+static int addeval_prec(double alpha_re, double alpha_im, const h2b_h2matrix *h, const double *x,
+                        double *y, int single);
+
 extern "C" int h2b_h2matrix_addeval(double alpha_re, double alpha_im, const h2b_h2matrix *h,
                                     const double *x, double *y) {
+  return addeval_prec(alpha_re, alpha_im, h, x, y, 0);
+}
+
+extern "C" int h2b_h2matrix_addeval_single(double alpha_re, double alpha_im,
+                                           const h2b_h2matrix *h, const double *x, double *y) {
+  return addeval_prec(alpha_re, alpha_im, h, x, y, 1);
+}
+
+static int addeval_prec(double alpha_re, double alpha_im, const h2b_h2matrix *h, const double *x,
+                        double *y, int single) {
   if (!h || !x || !y) {
     h2b_set_error("h2b_h2matrix_addeval: NULL argument");
     return H2B_ERR_ARG;
@@ -721,7 +807,8 @@ extern "C" int h2b_h2matrix_addeval(double alpha_re, double alpha_im, const h2b_
     yd = h->d_yio;
   }
   cudaEventRecord(h->ev[9], h->st);
-  int rc = h2b_h2_addeval_dev(h, alpha_re, alpha_im, xd, yd, h->st);
+  int rc = single ? h2b_mvm_launch_single(&h->mvm, xd, yd, alpha_re, alpha_im, h->st)
+                  : h2b_h2_addeval_dev(h, alpha_re, alpha_im, xd, yd, h->st);
   cudaEventRecord(h->ev[10], h->st);
   if (rc == H2B_OK && !dy) {
     if (cudaMemcpyAsync(y, yd, sizeof(double) * W * h->rt.nidx, cudaMemcpyDeviceToHost,

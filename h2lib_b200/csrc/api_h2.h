@@ -12,7 +12,7 @@
 #include "h2mvm.h"
 
 struct DevCTree {
-  uint32_t n = 0, nidx = 0, depth = 0, nleaves = 0, max_rows = 0;
+  uint32_t n = 0, nidx = 0, depth = 0, nleaves = 0, max_rows = 0, nnonroot = 0;
   uint64_t vtotal = 0;
   uint32_t *d_off = nullptr, *d_size = nullptr, *d_father = nullptr, *d_son0 = nullptr,
            *d_son1 = nullptr, *d_idx = nullptr, *d_leaves = nullptr, *d_nonroot = nullptr,
@@ -32,6 +32,7 @@ struct DevCTree {
   uint32_t *d_mitems = nullptr;  // matvec items (3 uint32 each) over the admissible clusters
   std::vector<uint32_t> fitem_start, fitem_count;  // flatten items of father level l
   uint32_t nwleaves = 0, nmitems = 0;
+  float *f_W = nullptr;  // FP32 copy of W (h2b_h2matrix_make_single)
 };
 
 struct h2b_h2matrix {
@@ -49,6 +50,7 @@ struct h2b_h2matrix {
   uint32_t *d_near_rc = nullptr, *d_near_cc = nullptr;
   uint64_t *d_near_off = nullptr;
   double *d_N = nullptr;
+  float *f_S = nullptr, *f_N = nullptr;  // FP32 copies (h2b_h2matrix_make_single)
   h2b_tile *d_tiles = nullptr;
   h2b_triref *d_refs = nullptr;
   h2b_sing *d_sing = nullptr;

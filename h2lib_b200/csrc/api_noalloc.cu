@@ -14,6 +14,8 @@
 #include <cuda_runtime.h>
 #include <string.h>
 
+#include <vector>
+
 #include "api_h2.h"
 #include "gmres.h"
 
@@ -93,17 +95,10 @@ extern "C" int h2b_solve_gmres_noalloc(uint32_t nterms, const h2b_h2matrix *cons
   const uint32_t n = A0->rt.nidx;
   const size_t W = A0->cx ? 2 : 1;
 
-  GmresDev g;
-  memset(&g, 0, sizeof(g));
-  g.cx = A0->cx;
-  g.n = n;
-  g.kmax = kmax;
-  g.nblocks = (n + 255) / 256;
-  g.ldpart = kmax + 1;
-  const size_t nq = W * (size_t) n * kmax, nT = 2 * (size_t) kmax * kmax,
-               nsm = 2 * (size_t) (kmax + 1), npart = 2 * (size_t) g.nblocks * g.ldpart;
-  const size_t ndoubles = nq + 2 * (size_t) kmax + nT + 3 * nsm + 4 * W * (size_t) n + npart;
-  const size_t need = sizeof(double) * ndoubles + 256 + sizeof(GmresState);
+  const uint32_t sizes[1] = {n};
+  uint32_t nblocks = 0;
+  const size_t ndoubles = h2b_gmres_workspace(A0->cx, 1, sizes, kmax, &nblocks) + 2 * W * (size_t) n;
+  const size_t need = sizeof(double) * ndoubles + 512;
   if (need > H2B_NOALLOC_SCRATCH_BYTES) {
     h2b_set_error("h2b_solve_gmres_noalloc: needs %zu bytes of work space for n = %u, kmax = %u; "
                   "the fixed work space holds %u bytes (use h2b_solve_gmres)",
@@ -113,26 +108,24 @@ extern "C" int h2b_solve_gmres_noalloc(uint32_t nterms, const h2b_h2matrix *cons
   void *base = nullptr;
   int rc = scratch_address(&base);
   if (rc != H2B_OK) return rc;
-  double *p = (double *) base;
-  g.qr = p; p += nq;
-  g.tau = p; p += 2 * kmax;
-  g.T = p; p += nT;
-  g.rhat = p; p += nsm;
-  g.w = p; p += nsm;
-  g.u = p; p += nsm;
-  g.q = p; p += W * n;
-  g.abuf = p; p += W * n;
-  double *db = p; p += W * n;
-  double *dx = p; p += W * n;
-  g.part = p; p += npart;
-  g.state = (GmresState *) (((uintptr_t) p + 255) & ~(uintptr_t) 255);
+  double *db = (double *) base, *dx = db + W * n;
+  GmresDev g;
+  memset(&g, 0, sizeof(g));
+  GmresSys sys;
+  std::vector<uint32_t> blk(nblocks);  // host table, copied into the work space
+  h2b_gmres_layout(&g, dx + W * n, A0->cx, 1, sizes, kmax, &sys, blk.data());
+  g.eps = eps;
   // the scratch keeps the previous call's contents: clear what must start at zero
-  H2B_CUDA_TRY(cudaMemsetAsync(g.T, 0, sizeof(double) * nT, st));
+  H2B_CUDA_TRY(cudaMemsetAsync(g.T, 0, sizeof(double) * 2 * (size_t) kmax * kmax, st));
   H2B_CUDA_TRY(cudaMemsetAsync(g.state, 0, sizeof(GmresState), st));
+  H2B_CUDA_TRY(cudaMemcpyAsync((void *) g.sys, &sys, sizeof(GmresSys), cudaMemcpyHostToDevice, st));
+  H2B_CUDA_TRY(cudaMemcpyAsync((void *) g.blk, blk.data(), sizeof(uint32_t) * nblocks,
+                               cudaMemcpyHostToDevice, st));
   H2B_CUDA_TRY(cudaMemcpyAsync(db, b, sizeof(double) * W * n, cudaMemcpyDefault, st));
   H2B_CUDA_TRY(cudaMemcpyAsync(dx, x, sizeof(double) * W * n, cudaMemcpyDefault, st));
 
-  GmresOp op{&combo, combo_apply_na};
+  // host-driven loop: one step launch sequence per iteration, the residual estimate read back
+  GmresOp op{&combo, combo_apply_na, nullptr};
   GmresState hs;
   auto read_state = [&]() -> int {
     H2B_CUDA_TRY(cudaMemcpyAsync(&hs, g.state, sizeof(GmresState), cudaMemcpyDeviceToHost, st));
@@ -140,14 +133,14 @@ extern "C" int h2b_solve_gmres_noalloc(uint32_t nterms, const h2b_h2matrix *cons
     return H2B_OK;
   };
   if ((rc = h2b_gmres_bnorm(&g, db, st)) != H2B_OK) return rc;
-  if ((rc = h2b_gmres_init(&g, &op, db, dx, st)) != H2B_OK) return rc;
+  if ((rc = h2b_gmres_init(&g, &op, db, dx, GMRES_SEL_ALL, st)) != H2B_OK) return rc;
   if ((rc = read_state()) != H2B_OK) return rc;
   const double bnorm = hs.bnorm;
   double err = hs.err;
   uint32_t k = 0, iter = 0;
   while (err > eps * bnorm && iter + 1 != maxiter) {
     if (k + 1 >= kmax) {
-      if ((rc = h2b_gmres_finish(&g, &op, db, dx, st)) != H2B_OK) return rc;
+      if ((rc = h2b_gmres_finish(&g, &op, db, dx, GMRES_SEL_ALL, st)) != H2B_OK) return rc;
       k = 0;
     }
     if ((rc = h2b_gmres_step(&g, &op, st)) != H2B_OK) return rc;
@@ -161,7 +154,7 @@ extern "C" int h2b_solve_gmres_noalloc(uint32_t nterms, const h2b_h2matrix *cons
     err = hs.err;
     iter++;
   }
-  if ((rc = h2b_gmres_finish(&g, &op, db, dx, st)) != H2B_OK) return rc;
+  if ((rc = h2b_gmres_update(&g, dx, GMRES_SEL_ALL, st)) != H2B_OK) return rc;
   H2B_CUDA_TRY(cudaMemcpyAsync(x, dx, sizeof(double) * W * n, cudaMemcpyDefault, st));
   H2B_CUDA_TRY(cudaStreamSynchronize(st));
   return (int) iter;

@@ -16,16 +16,29 @@ struct Combo {
   uint32_t nterms;
   const h2b_h2matrix *ops[16];
   double cre[16], cim[16];
+  uint32_t nrhs = 1;  // vectors hold nrhs columns of the operator size, each multiplied alone
 };
 
-int combo_apply(void *ctx, const double *x, double *y, double ar, double ai, cudaStream_t st) {
+template <bool SINGLE>
+int combo_apply_t(void *ctx, const double *x, double *y, double ar, double ai, cudaStream_t st) {
   const Combo *c = (const Combo *) ctx;
-  for (uint32_t i = 0; i < c->nterms; i++) {
-    const double br = ar * c->cre[i] - ai * c->cim[i], bi = ar * c->cim[i] + ai * c->cre[i];
-    int rc = h2b_mvm_launch(&c->ops[i]->mvm, x, y, br, bi, st);
-    if (rc != H2B_OK) return rc;
-  }
+  const size_t col = (size_t) (c->ops[0]->cx ? 2 : 1) * c->ops[0]->rt.nidx;
+  for (uint32_t r = 0; r < c->nrhs; r++)
+    for (uint32_t i = 0; i < c->nterms; i++) {
+      const double br = ar * c->cre[i] - ai * c->cim[i], bi = ar * c->cim[i] + ai * c->cre[i];
+      int rc = SINGLE ? h2b_mvm_launch_single(&c->ops[i]->mvm, x + r * col, y + r * col, br, bi, st)
+                      : h2b_mvm_launch(&c->ops[i]->mvm, x + r * col, y + r * col, br, bi, st);
+      if (rc != H2B_OK) return rc;
+    }
   return H2B_OK;
+}
+
+int combo_apply(void *ctx, const double *x, double *y, double ar, double ai, cudaStream_t st) {
+  return combo_apply_t<false>(ctx, x, y, ar, ai, st);
+}
+int combo_apply_single(void *ctx, const double *x, double *y, double ar, double ai,
+                       cudaStream_t st) {
+  return combo_apply_t<true>(ctx, x, y, ar, ai, st);
 }
 
 int check_ops(uint32_t nterms, const h2b_h2matrix *const *ops, const double *coef, Combo *c) {
@@ -61,6 +74,84 @@ struct DevBuf {
 
 }  // namespace
 
+// Solve a batch of independent systems that share the operator (ops, coef) on the row ranges
+// seg_off[s] .. seg_off[s+1] of the vectors (each segment must be closed under the operator:
+// a forest H2 matrix, one block per surface).  iters[s] receives the step count of system s.
+// With nrhs > 1 the vectors hold nrhs columns and system (s, r) is segment s of column r
+// (iters[s + r * nseg]).  mixed: Arnoldi steps with the FP32 copies of the matrices, (re)start
+// residuals and the final stopping test in FP64.
+static int solve_segments(Combo &combo, uint32_t nseg, const uint32_t *seg_off, uint32_t nrhs,
+                          const double *b, double *x, double eps, uint32_t maxiter,
+                          uint32_t kmax, int mixed, uint32_t *iters, const char *who) {
+  const h2b_h2matrix *A0 = combo.ops[0];
+  cudaStream_t st = A0->st;
+  const uint32_t n1 = A0->rt.nidx;
+  const size_t W = A0->cx ? 2 : 1;
+  if (nrhs == 0 || (uint64_t) n1 * nrhs > 0xFFFFFFFFull) {
+    h2b_set_error("%s: %u right-hand sides of size %u", who, nrhs, n1);
+    return H2B_ERR_ARG;
+  }
+  const uint32_t n = n1 * nrhs;
+  combo.nrhs = nrhs;
+  if (mixed)
+    for (uint32_t i = 0; i < combo.nterms; i++)
+      if (!combo.ops[i]->mvm.cpl.Ss) {
+        h2b_set_error("%s: operator %u has no FP32 copy (h2b_h2matrix_make_single)", who, i);
+        return H2B_ERR_ARG;
+      }
+  if (kmax < 2 || kmax >= GMRES_KMAX) {
+    h2b_set_error("%s: kmax %u outside 2..%d", who, kmax, GMRES_KMAX - 1);
+    return H2B_ERR_ARG;
+  }
+  if (nseg == 0 || !seg_off || seg_off[0] != 0 || seg_off[nseg] != n1) {
+    h2b_set_error("%s: segments must start at 0 and end at the operator size %u", who, n1);
+    return H2B_ERR_ARG;
+  }
+  std::vector<uint32_t> sizes((size_t) nseg * nrhs);
+  for (uint32_t s = 0; s < nseg; s++) {
+    if (seg_off[s + 1] <= seg_off[s]) {
+      h2b_set_error("%s: segment %u is empty or the offsets decrease", who, s);
+      return H2B_ERR_ARG;
+    }
+    for (uint32_t r = 0; r < nrhs; r++) sizes[s + (size_t) r * nseg] = seg_off[s + 1] - seg_off[s];
+  }
+  const uint32_t nsys = nseg * nrhs;
+  uint32_t nblocks = 0;
+  const size_t nws = h2b_gmres_workspace(A0->cx, nsys, sizes.data(), kmax, &nblocks);
+  DevBuf buf;
+  buf.st = st;
+  H2B_CUDA_TRY(cudaMallocAsync(&buf.p, sizeof(double) * (nws + 2 * W * (size_t) n) + 512, st));
+  GmresDev g;
+  memset(&g, 0, sizeof(g));
+  std::vector<GmresSys> sys(nsys);
+  std::vector<uint32_t> blk(nblocks);
+  double *db = (double *) buf.p, *dx = db + W * n;
+  h2b_gmres_layout(&g, dx + W * n, A0->cx, nsys, sizes.data(), kmax, sys.data(), blk.data());
+  g.eps = eps;
+  g.mixed = mixed;
+  H2B_CUDA_TRY(cudaMemcpyAsync((void *) g.sys, sys.data(), sizeof(GmresSys) * nsys,
+                               cudaMemcpyHostToDevice, st));
+  H2B_CUDA_TRY(cudaMemcpyAsync((void *) g.blk, blk.data(), sizeof(uint32_t) * nblocks,
+                               cudaMemcpyHostToDevice, st));
+  H2B_CUDA_TRY(cudaMemcpyAsync(db, b, sizeof(double) * W * n, cudaMemcpyDefault, st));
+  H2B_CUDA_TRY(cudaMemcpyAsync(dx, x, sizeof(double) * W * n, cudaMemcpyDefault, st));
+  GmresOp op{(void *) &combo, combo_apply, mixed ? combo_apply_single : nullptr};
+  std::vector<GmresState> hs(nsys);
+  int rc = h2b_gmres_run(&g, &op, db, dx, maxiter, st, hs.data());
+  if (rc != H2B_OK) return rc;
+  for (uint32_t s = 0; s < nsys; s++) {
+    if (hs[s].nan) {
+      h2b_set_error("%s: residual estimate of system %u is NaN after %u iterations", who, s,
+                    hs[s].iter);
+      return H2B_ERR_INTERNAL;
+    }
+    if (iters) iters[s] = hs[s].iter;
+  }
+  H2B_CUDA_TRY(cudaMemcpyAsync(x, dx, sizeof(double) * W * n, cudaMemcpyDefault, st));
+  H2B_CUDA_TRY(cudaStreamSynchronize(st));
+  return H2B_OK;
+}
+
 extern "C" int h2b_solve_gmres(uint32_t nterms, const h2b_h2matrix *const *ops,
                                const double *coef, const double *b, double *x, double eps,
                                uint32_t maxiter, uint32_t kmax) {
@@ -71,162 +162,43 @@ extern "C" int h2b_solve_gmres(uint32_t nterms, const h2b_h2matrix *const *ops,
     h2b_set_error("h2b_solve_gmres: NULL vector");
     return H2B_ERR_ARG;
   }
-  if (kmax < 2 || kmax >= GMRES_KMAX) {
-    h2b_set_error("h2b_solve_gmres: kmax %u outside 2..%d", kmax, GMRES_KMAX - 1);
+  const uint32_t seg[2] = {0, ops[0]->rt.nidx};
+  uint32_t iter = 0;
+  rc = solve_segments(combo, 1, seg, 1, b, x, eps, maxiter, kmax, 0, &iter, "h2b_solve_gmres");
+  return rc == H2B_OK ? (int) iter : rc;
+}
+
+extern "C" int h2b_solve_gmres_mixed(uint32_t nterms, const h2b_h2matrix *const *ops,
+                                     const double *coef, const double *b, double *x, double eps,
+                                     uint32_t maxiter, uint32_t kmax) {
+  Combo combo;
+  int rc = check_ops(nterms, ops, coef, &combo);
+  if (rc != H2B_OK) return rc;
+  if (!b || !x) {
+    h2b_set_error("h2b_solve_gmres_mixed: NULL vector");
     return H2B_ERR_ARG;
   }
-  const h2b_h2matrix *A0 = ops[0];
-  cudaStream_t st = A0->st;
-  const uint32_t n = A0->rt.nidx;
-  const size_t W = A0->cx ? 2 : 1;
+  const uint32_t seg[2] = {0, ops[0]->rt.nidx};
+  uint32_t iter = 0;
+  rc = solve_segments(combo, 1, seg, 1, b, x, eps, maxiter, kmax, 1, &iter,
+                      "h2b_solve_gmres_mixed");
+  return rc == H2B_OK ? (int) iter : rc;
+}
 
-  GmresDev g;
-  memset(&g, 0, sizeof(g));
-  g.cx = A0->cx;
-  g.n = n;
-  g.kmax = kmax;
-  g.nblocks = (n + 255) / 256;
-  g.ldpart = kmax + 1;
-  // one allocation for all device state
-  const size_t nq = W * (size_t) n * kmax, nT = 2 * (size_t) kmax * kmax, nsm = 2 * (size_t) (kmax + 1);
-  const size_t npart = 2 * (size_t) g.nblocks * g.ldpart;
-  const size_t total = nq + 2 * kmax + nT + 3 * nsm + 4 * W * (size_t) n + npart + 16;
-  DevBuf buf;
-  buf.st = st;
-  H2B_CUDA_TRY(cudaMallocAsync(&buf.p, sizeof(double) * total + sizeof(GmresState) + 256, st));
-  double *p = (double *) buf.p;
-  g.qr = p; p += nq;
-  g.tau = p; p += 2 * kmax;
-  g.T = p; p += nT;
-  g.rhat = p; p += nsm;
-  g.w = p; p += nsm;
-  g.u = p; p += nsm;
-  g.q = p; p += W * n;
-  g.abuf = p; p += W * n;
-  double *db = p; p += W * n;
-  double *dx = p; p += W * n;
-  g.part = p; p += npart;
-  g.state = (GmresState *) (((uintptr_t) p + 255) & ~(uintptr_t) 255);
-  H2B_CUDA_TRY(cudaMemsetAsync(g.T, 0, sizeof(double) * nT, st));
-  H2B_CUDA_TRY(cudaMemsetAsync(g.state, 0, sizeof(GmresState), st));
-
-  const bool bdev = h2b_is_device_ptr(b), xdev = h2b_is_device_ptr(x);
-  H2B_CUDA_TRY(cudaMemcpyAsync(db, b, sizeof(double) * W * n,
-                               bdev ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, st));
-  H2B_CUDA_TRY(cudaMemcpyAsync(dx, x, sizeof(double) * W * n,
-                               xdev ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, st));
-
-  GmresOp op{&combo, combo_apply};
-  GmresState *hs = nullptr;
-  H2B_CUDA_TRY(cudaMallocHost(&hs, sizeof(GmresState)));
-  struct HostFree {
-    GmresState *p;
-    ~HostFree() { cudaFreeHost(p); }
-  } hf{hs};
-
-  // Default: the whole iteration runs inside one graph (WHILE/IF conditional nodes, the loop
-  // condition set on the device).  H2B_GMRES_HOSTLOOP=1 selects a host loop that launches a
-  // captured single step and reads the residual estimate after each one.
-  cudaGraphExec_t loop_exec = nullptr;
-  {
-    const char *e = getenv("H2B_GMRES_HOSTLOOP");
-    if (!(e && e[0] == '1') && (rc = h2b_gmres_loop_graph(&g, &op, db, dx, st, &loop_exec)) != H2B_OK)
-      return rc;
+extern "C" int h2b_solve_gmres_batch(uint32_t nterms, const h2b_h2matrix *const *ops,
+                                     const double *coef, uint32_t systems,
+                                     const uint32_t *system_off, uint32_t nrhs, const double *b,
+                                     double *x, double eps, uint32_t maxiter, uint32_t kmax,
+                                     uint32_t flags, uint32_t *iterations) {
+  Combo combo;
+  int rc = check_ops(nterms, ops, coef, &combo);
+  if (rc != H2B_OK) return rc;
+  if (!b || !x) {
+    h2b_set_error("h2b_solve_gmres_batch: NULL vector");
+    return H2B_ERR_ARG;
   }
-  struct LoopFree {
-    cudaGraphExec_t e;
-    ~LoopFree() {
-      if (e) cudaGraphExecDestroy(e);
-    }
-  } lf{loop_exec};
-  // the step is identical for every k (k is read on the device): capture it once
-  cudaGraph_t graph = nullptr;
-  cudaGraphExec_t exec = nullptr;
-  if (!loop_exec) {
-    H2B_CUDA_TRY(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-    rc = h2b_gmres_step(&g, &op, st);
-    cudaError_t ce = cudaStreamEndCapture(st, &graph);
-    if (rc != H2B_OK || ce != cudaSuccess) {
-      if (graph) cudaGraphDestroy(graph);
-      if (rc == H2B_OK)
-        h2b_set_error("h2b_solve_gmres: graph capture failed: %s", cudaGetErrorString(ce));
-      return rc == H2B_OK ? H2B_ERR_CUDA : rc;
-    }
-    ce = cudaGraphInstantiate(&exec, graph, 0);
-    cudaGraphDestroy(graph);
-    if (ce != cudaSuccess) {
-      h2b_set_error("h2b_solve_gmres: graph instantiation failed: %s", cudaGetErrorString(ce));
-      return H2B_ERR_CUDA;
-    }
-  }
-  struct ExecFree {
-    cudaGraphExec_t e;
-    ~ExecFree() {
-      if (e) cudaGraphExecDestroy(e);
-    }
-  } ef{exec};
-
-  auto read_state = [&]() -> int {
-    H2B_CUDA_TRY(cudaMemcpyAsync(hs, g.state, sizeof(GmresState), cudaMemcpyDeviceToHost, st));
-    H2B_CUDA_TRY(cudaStreamSynchronize(st));
-    return H2B_OK;
-  };
-
-  if ((rc = h2b_gmres_bnorm(&g, db, st)) != H2B_OK) return rc;
-  if ((rc = h2b_gmres_init(&g, &op, db, dx, st)) != H2B_OK) return rc;
-  if ((rc = read_state()) != H2B_OK) return rc;
-  const double bnorm = hs->bnorm;
-  double err = hs->err;
-  uint32_t k = 0, iter = 0;
-  if (loop_exec) {
-    // graph-resident loop: launches of at most kLoopBudget steps until the device stops it
-    constexpr uint32_t kLoopBudget = 512;
-    hs->tol = eps * bnorm;
-    hs->iter = 0;
-    hs->maxiter = maxiter;
-    hs->nan = 0;
-    while (true) {
-      hs->budget = kLoopBudget;
-      H2B_CUDA_TRY(cudaMemcpyAsync(g.state, hs, sizeof(GmresState), cudaMemcpyHostToDevice, st));
-      H2B_CUDA_TRY(cudaGraphLaunch(loop_exec, st));
-      if ((rc = read_state()) != H2B_OK) return rc;
-      if (hs->nan) {
-        h2b_set_error("h2b_solve_gmres: residual estimate is NaN after %u iterations", hs->iter);
-        return H2B_ERR_INTERNAL;
-      }
-      if (!(hs->err > hs->tol) || (maxiter != 0 && hs->iter + 1 == maxiter)) break;
-      if (hs->budget != 0) {
-        h2b_set_error("h2b_solve_gmres: device loop stopped early at iteration %u", hs->iter);
-        return H2B_ERR_INTERNAL;
-      }
-    }
-    iter = hs->iter;
-    err = hs->err;
-  }
-  while (!loop_exec && err > eps * bnorm && iter + 1 != maxiter) {
-    if (k + 1 >= kmax) {
-      if ((rc = h2b_gmres_finish(&g, &op, db, dx, st)) != H2B_OK) return rc;
-      k = 0;
-    }
-    H2B_CUDA_TRY(cudaGraphLaunch(exec, st));
-    k++;
-    if ((rc = read_state()) != H2B_OK) return rc;
-    if (hs->k != k) {
-      h2b_set_error("h2b_solve_gmres: device step counter %u != %u", hs->k, k);
-      return H2B_ERR_INTERNAL;
-    }
-    err = hs->err;
-    if (!(err == err)) {
-      h2b_set_error("h2b_solve_gmres: residual estimate is NaN after %u iterations", iter + 1);
-      return H2B_ERR_INTERNAL;
-    }
-    iter++;
-  }
-  if ((rc = h2b_gmres_finish(&g, &op, db, dx, st)) != H2B_OK) return rc;
-  H2B_CUDA_TRY(cudaMemcpyAsync(x, dx, sizeof(double) * W * n,
-                               xdev ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, st));
-  H2B_CUDA_TRY(cudaStreamSynchronize(st));
-  return (int) iter;
+  return solve_segments(combo, systems, system_off, nrhs, b, x, eps, maxiter, kmax,
+                        (flags & H2B_SOLVE_MIXED) ? 1 : 0, iterations, "h2b_solve_gmres_batch");
 }
 
 // ------------------------------------------------------------------------------------------
@@ -399,6 +371,78 @@ __global__ void plane_wave_kernel(HarmArgs a, double k0, double k1, double k2, d
   b[2 * t + 1] = cre * si + cim * sr;
 }
 
+// Several surfaces (triangle ranges tri_off[s] .. tri_off[s+1]) and right-hand sides: the source
+// of (surface s, column r) is zs[3 (s + r nseg)].  Columns of the vertex vectors are nv long.
+struct MultiZ {
+  const uint32_t *tri_off;
+  const double *zs;
+  uint32_t nseg, nv;
+};
+
+__device__ __forceinline__ uint32_t segment_of(const MultiZ &m, uint32_t t) {
+  uint32_t lo = 0, hi = m.nseg;  // tri_off[lo] <= t < tri_off[hi]
+  while (hi - lo > 1) {
+    const uint32_t mid = (lo + hi) / 2;
+    if (m.tri_off[mid] <= t) lo = mid; else hi = mid;
+  }
+  return lo;
+}
+
+// project_rhs_kernel with the source of the triangle's surface; blockIdx.y = column
+__global__ void project_rhs_multi_kernel(HarmArgs a, MultiZ m, double *v) {
+  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x, r = blockIdx.y;
+  if (t >= a.nt) return;
+  const double *z = m.zs + 3 * ((size_t) segment_of(m, t) + (size_t) r * m.nseg);
+  const TriRec &T = a.tri[t];
+  double s[3] = {0.0, 0.0, 0.0};
+  for (int q = 0; q < a.ns; q++) {
+    double X[3];
+    tri_point(T, a.xs[q], a.ys[q], X);
+    const double d0 = X[0] - z[0], d1 = X[1] - z[1], d2 = X[2] - z[2];
+    const double f = 1.0 / sqrt(d0 * d0 + d1 * d1 + d2 * d2);
+    for (int l = 0; l < 3; l++) s[l] += a.wsl[l * a.ns + q] * f;
+  }
+  for (int l = 0; l < 3; l++) atomicAdd(&v[(size_t) r * m.nv + T.v[l]], s[l] * T.g);
+}
+
+// mass_kernel on every column (blockIdx.y)
+__global__ void mass_multi_kernel(const TriRec *tri, uint32_t nt, uint32_t nv, const double *x,
+                                  double *y) {
+  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nt) return;
+  const size_t o = (size_t) blockIdx.y * nv;
+  const TriRec &T = tri[t];
+  const double x0 = x[o + T.v[0]], x1 = x[o + T.v[1]], x2 = x[o + T.v[2]];
+  const double c1 = T.g / 24.0, c2 = T.g / 12.0;
+  atomicAdd(&y[o + T.v[0]], c2 * x0 + c1 * (x1 + x2));
+  atomicAdd(&y[o + T.v[1]], c2 * x1 + c1 * (x0 + x2));
+  atomicAdd(&y[o + T.v[2]], c2 * x2 + c1 * (x0 + x1));
+}
+
+// l2err_kernel per (surface, column): out[2 (s + r nseg)] += (error^2, norm^2)
+__global__ void l2err_multi_kernel(HarmArgs a, MultiZ m, const double *u, double *out) {
+  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x, r = blockIdx.y;
+  if (t >= a.nt) return;
+  const uint32_t sg = segment_of(m, t);
+  const double *z = m.zs + 3 * ((size_t) sg + (size_t) r * m.nseg);
+  const double *ur = u + (size_t) r * m.nv;
+  const TriRec &T = a.tri[t];
+  double e = 0.0, nn = 0.0;
+  for (int q = 0; q < a.ns; q++) {
+    double X[3];
+    const double tx = a.xs[q], sx = a.ys[q];
+    tri_point(T, tx, sx, X);
+    const double d0 = X[0] - z[0], d1 = X[1] - z[1], d2 = X[2] - z[2];
+    const double r2 = d0 * d0 + d1 * d1 + d2 * d2;
+    const double f = -(d0 * T.n[0] + d1 * T.n[1] + d2 * T.n[2]) / (r2 * sqrt(r2));
+    const double bf = ur[T.v[0]] * (1.0 - tx) + ur[T.v[1]] * (tx - sx) + ur[T.v[2]] * sx;
+    e += a.ws[q] * (f - bf) * (f - bf);
+    nn += a.ws[q] * f * f;
+  }
+  atomicAdd(&out[2 * ((size_t) sg + (size_t) r * m.nseg)], e * T.g);
+  atomicAdd(&out[2 * ((size_t) sg + (size_t) r * m.nseg) + 1], nn * T.g);
+}
+
 int harm_args(const h2b_bem *bem, const double z[3], double *scratch, HarmArgs *a,
               cudaStream_t st) {
   const h2b_quad &qd = bem->quad;
@@ -497,6 +541,126 @@ extern "C" int h2b_l2_error_harmonic(const h2b_bem *bem, const double z[3], cons
   H2B_CUDA_TRY(cudaStreamSynchronize(st));
   *err = sqrt(h[0]);
   *norm = sqrt(h[1]);
+  return H2B_OK;
+}
+
+// Device copies of the surface offsets and sources of a multi-surface call.
+static int multi_args(const h2b_bem *bem, uint32_t nseg, const uint32_t *tri_off, uint32_t nrhs,
+                      const double *zs, void *dev, MultiZ *m, cudaStream_t st) {
+  if (nseg == 0 || nrhs == 0 || !tri_off || !zs || tri_off[0] != 0 ||
+      tri_off[nseg] != bem->s->nt) {
+    h2b_set_error("harmonic data: triangle offsets must run from 0 to %u", bem->s->nt);
+    return H2B_ERR_ARG;
+  }
+  for (uint32_t s = 0; s < nseg; s++)
+    if (tri_off[s + 1] < tri_off[s]) {
+      h2b_set_error("harmonic data: triangle offsets decrease at surface %u", s);
+      return H2B_ERR_ARG;
+    }
+  uint32_t *doff = (uint32_t *) dev;
+  double *dz = (double *) (((uintptr_t) (doff + nseg + 1) + 15) & ~(uintptr_t) 15);
+  H2B_CUDA_TRY(cudaMemcpyAsync(doff, tri_off, sizeof(uint32_t) * (nseg + 1),
+                               cudaMemcpyHostToDevice, st));
+  H2B_CUDA_TRY(cudaMemcpyAsync(dz, zs, sizeof(double) * 3 * (size_t) nseg * nrhs,
+                               cudaMemcpyHostToDevice, st));
+  m->tri_off = doff;
+  m->zs = dz;
+  m->nseg = nseg;
+  m->nv = bem->s->nv;
+  return H2B_OK;
+}
+
+static size_t multi_bytes(uint32_t nseg, uint32_t nrhs) {
+  return sizeof(uint32_t) * (nseg + 1) + 16 + sizeof(double) * 3 * (size_t) nseg * nrhs;
+}
+
+extern "C" int h2b_project_l2_harmonic_multi(const h2b_bem *bem, uint32_t surfaces,
+                                             const uint32_t *triangle_off, uint32_t nrhs,
+                                             const double *zs, double *w) {
+  if (!bem || !w || bem->row_basis != H2B_BASIS_LINEAR) {
+    h2b_set_error("h2b_project_l2_harmonic_multi: needs an operator with a linear row basis");
+    return H2B_ERR_ARG;
+  }
+  const h2b_surface *s = bem->s;
+  cudaStream_t st = s->stream;
+  const uint32_t nv = s->nv, nt = s->nt;
+  const size_t n = (size_t) nv * (nrhs ? nrhs : 1);
+  DevBuf buf;
+  buf.st = st;
+  H2B_CUDA_TRY(cudaMallocAsync(&buf.p, sizeof(double) * (5 * n + 6 * 64 + 4) +
+                                           multi_bytes(surfaces, nrhs) + 64, st));
+  double *v = (double *) buf.p, *x = v + n, *r = x + n, *p = r + n, *ap = p + n,
+         *rule = ap + n, *sc = rule + 6 * 64;
+  HarmArgs a;
+  MultiZ m;
+  const double z0[3] = {0.0, 0.0, 0.0};
+  int rc = harm_args(bem, z0, rule, &a, st);
+  if (rc == H2B_OK) rc = multi_args(bem, surfaces, triangle_off, nrhs, zs, sc + 4, &m, st);
+  if (rc != H2B_OK) return rc;
+  H2B_CUDA_TRY(cudaMemsetAsync(v, 0, sizeof(double) * 2 * n, st));
+  project_rhs_multi_kernel<<<dim3((nt + 127) / 128, nrhs), 128, 0, st>>>(a, m, v);
+  // CG on the stacked block-diagonal mass system (as h2b_project_l2_harmonic per column)
+  H2B_CUDA_TRY(cudaMemcpyAsync(r, v, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
+  H2B_CUDA_TRY(cudaMemcpyAsync(p, v, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
+  double hsc[4];
+  H2B_CUDA_TRY(cudaMemsetAsync(sc, 0, sizeof(double) * 4, st));
+  const uint32_t un = (uint32_t) n;
+  dot_kernel<<<64, 256, 0, st>>>(r, r, un, sc);
+  H2B_CUDA_TRY(cudaMemcpyAsync(hsc, sc, sizeof(double), cudaMemcpyDeviceToHost, st));
+  H2B_CUDA_TRY(cudaStreamSynchronize(st));
+  const double norm = sqrt(hsc[0]);
+  double rr = hsc[0];
+  for (uint32_t it = 0; sqrt(rr) > 1e-15 * norm && it + 1 < 500; it++) {
+    H2B_CUDA_TRY(cudaMemsetAsync(ap, 0, sizeof(double) * n, st));
+    mass_multi_kernel<<<dim3((nt + 127) / 128, nrhs), 128, 0, st>>>(s->d_tri, nt, nv, p, ap);
+    H2B_CUDA_TRY(cudaMemsetAsync(sc + 1, 0, sizeof(double) * 2, st));
+    dot_kernel<<<64, 256, 0, st>>>(p, ap, un, sc + 1);
+    cg_update_kernel<<<64, 256, 0, st>>>(x, r, p, ap, un, sc);
+    dot_kernel<<<64, 256, 0, st>>>(r, r, un, sc + 2);
+    cg_dir_kernel<<<64, 256, 0, st>>>(p, r, un, sc);
+    H2B_CUDA_TRY(cudaMemcpyAsync(sc, sc + 2, sizeof(double), cudaMemcpyDeviceToDevice, st));
+    H2B_CUDA_TRY(cudaMemcpyAsync(hsc, sc, sizeof(double), cudaMemcpyDeviceToHost, st));
+    H2B_CUDA_TRY(cudaStreamSynchronize(st));
+    rr = hsc[0];
+  }
+  H2B_CUDA_TRY(cudaMemcpyAsync(w, x, sizeof(double) * n, cudaMemcpyDefault, st));
+  H2B_CUDA_TRY(cudaStreamSynchronize(st));
+  return H2B_OK;
+}
+
+extern "C" int h2b_l2_error_harmonic_multi(const h2b_bem *bem, uint32_t surfaces,
+                                           const uint32_t *triangle_off, uint32_t nrhs,
+                                           const double *zs, const double *u, double *err,
+                                           double *norm) {
+  if (!bem || !u || !err || !norm) {
+    h2b_set_error("h2b_l2_error_harmonic_multi: NULL argument");
+    return H2B_ERR_ARG;
+  }
+  const h2b_surface *s = bem->s;
+  cudaStream_t st = s->stream;
+  const size_t n = (size_t) s->nv * (nrhs ? nrhs : 1), nsys = (size_t) surfaces * nrhs;
+  DevBuf buf;
+  buf.st = st;
+  H2B_CUDA_TRY(cudaMallocAsync(&buf.p, sizeof(double) * (n + 6 * 64 + 2 * nsys) +
+                                           multi_bytes(surfaces, nrhs) + 64, st));
+  double *du = (double *) buf.p, *rule = du + n, *out = rule + 6 * 64;
+  HarmArgs a;
+  MultiZ m;
+  const double z0[3] = {0.0, 0.0, 0.0};
+  int rc = harm_args(bem, z0, rule, &a, st);
+  if (rc == H2B_OK) rc = multi_args(bem, surfaces, triangle_off, nrhs, zs, out + 2 * nsys, &m, st);
+  if (rc != H2B_OK) return rc;
+  H2B_CUDA_TRY(cudaMemcpyAsync(du, u, sizeof(double) * n, cudaMemcpyDefault, st));
+  H2B_CUDA_TRY(cudaMemsetAsync(out, 0, sizeof(double) * 2 * nsys, st));
+  l2err_multi_kernel<<<dim3((s->nt + 127) / 128, nrhs), 128, 0, st>>>(a, m, du, out);
+  std::vector<double> h(2 * nsys);
+  H2B_CUDA_TRY(cudaMemcpyAsync(h.data(), out, sizeof(double) * 2 * nsys, cudaMemcpyDeviceToHost,
+                               st));
+  H2B_CUDA_TRY(cudaStreamSynchronize(st));
+  for (size_t i = 0; i < nsys; i++) {
+    err[i] = sqrt(h[2 * i]);
+    norm[i] = sqrt(h[2 * i + 1]);
+  }
   return H2B_OK;
 }
 

@@ -65,6 +65,8 @@ struct FlatLeafArgs {
 };
 
 extern "C" int h2b_flat_leaves(const FlatLeafArgs *a, cudaStream_t st);
+extern "C" int h2b_to_single(const double *in, float *out, size_t n, int num_sms,
+                             cudaStream_t st);
 extern "C" int h2b_flat_level(const FlatArgs *a, cudaStream_t st);
 
 extern "C" int h2b_far_leaf_basis(const FarLeafArgs *a, int linear, int dn, cudaStream_t st);

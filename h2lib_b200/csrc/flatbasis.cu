@@ -35,6 +35,9 @@ __global__ void __launch_bounds__(FLAT_TPB) flatten_kernel(FlatArgs a) {
   const uint32_t rf = a.off[s] - a.off[f] + r0;  // first row inside f
   const double *Ws = a.W + a.woff[s];
   double *Wf = a.W + a.woff[f];
+  // Each thread computes a 4 x 4 tile of the nr x k product (16 x 16 threads cover 64 x 64
+  // per pass), reading 4 + 4 shared-memory values per 16 FMAs.
+  const uint32_t tr = threadIdx.x % 16, tc = threadIdx.x / 16;
   if (!a.transposed) {
     // sW[i + mu nr] = W_s[r0 + i, mu]
     for (uint32_t e = threadIdx.x; e < nr * k; e += blockDim.x) {
@@ -43,22 +46,66 @@ __global__ void __launch_bounds__(FLAT_TPB) flatten_kernel(FlatArgs a) {
     }
     __syncthreads();
     // W_f[rf + i, nu] = sum_mu W_s[r0 + i, mu] E_s[mu, nu]   (E_s column-major k x k)
-    for (uint32_t e = threadIdx.x; e < nr * k; e += blockDim.x) {
-      const uint32_t i = e % nr, nu = e / nr;
-      double acc = 0.0;
-      for (uint32_t mu = 0; mu < k; mu++) acc = fma(sW[i + mu * nr], sE[mu + nu * k], acc);
-      Wf[rf + i + (size_t) nu * nf] = acc;
+    for (uint32_t c0 = 0; c0 < k; c0 += 64) {
+      double acc[4][4] = {};
+      uint32_t ii[4], nn[4];
+#pragma unroll
+      for (int q = 0; q < 4; q++) {
+        ii[q] = min(4 * tr + q, nr - 1);
+        nn[q] = min(c0 + 4 * tc + q, k - 1);
+      }
+      for (uint32_t mu = 0; mu < k; mu++) {
+        double x[4], y[4];
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+          x[q] = sW[ii[q] + mu * nr];
+          y[q] = sE[mu + nn[q] * k];
+        }
+#pragma unroll
+        for (int p = 0; p < 4; p++)
+#pragma unroll
+          for (int q = 0; q < 4; q++) acc[p][q] = fma(x[p], y[q], acc[p][q]);
+      }
+#pragma unroll
+      for (int p = 0; p < 4; p++)
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+          const uint32_t i = 4 * tr + p, nu = c0 + 4 * tc + q;
+          if (i < nr && nu < k) Wf[rf + i + (size_t) nu * nf] = acc[p][q];
+        }
     }
   } else {
     // sW[mu + i k] = W_s^T[mu, r0 + i]
     for (uint32_t e = threadIdx.x; e < nr * k; e += blockDim.x) sW[e] = Ws[(size_t) r0 * k + e];
     __syncthreads();
     // W_f^T[nu, rf + i] = sum_mu E_s^T[nu, mu] W_s^T[mu, r0 + i]   (E_s^T column-major k x k)
-    for (uint32_t e = threadIdx.x; e < nr * k; e += blockDim.x) {
-      const uint32_t nu = e % k, i = e / k;
-      double acc = 0.0;
-      for (uint32_t mu = 0; mu < k; mu++) acc = fma(sE[nu + mu * k], sW[mu + i * k], acc);
-      Wf[(size_t) (rf + i) * k + nu] = acc;
+    for (uint32_t c0 = 0; c0 < k; c0 += 64) {
+      double acc[4][4] = {};
+      uint32_t nn[4], ii[4];
+#pragma unroll
+      for (int q = 0; q < 4; q++) {
+        nn[q] = min(c0 + 4 * tr + q, k - 1);
+        ii[q] = min(4 * tc + q, nr - 1);
+      }
+      for (uint32_t mu = 0; mu < k; mu++) {
+        double x[4], y[4];
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+          x[q] = sE[nn[q] + mu * k];
+          y[q] = sW[mu + ii[q] * k];
+        }
+#pragma unroll
+        for (int p = 0; p < 4; p++)
+#pragma unroll
+          for (int q = 0; q < 4; q++) acc[p][q] = fma(x[p], y[q], acc[p][q]);
+      }
+#pragma unroll
+      for (int p = 0; p < 4; p++)
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+          const uint32_t nu = c0 + 4 * tr + p, i = 4 * tc + q;
+          if (i < nr && nu < k) Wf[(size_t) (rf + i) * k + nu] = acc[p][q];
+        }
     }
   }
 }
@@ -72,7 +119,23 @@ __global__ void __launch_bounds__(FLAT_TPB) leaf_copy_kernel(FlatLeafArgs a) {
   for (size_t e = threadIdx.x; e < n; e += blockDim.x) dst[e] = src[e];
 }
 
+// out[i] = (float) in[i] (round to nearest)
+__global__ void to_single_kernel(const double *__restrict__ in, float *__restrict__ out, size_t n) {
+  for (size_t i = blockIdx.x * (size_t) blockDim.x + threadIdx.x; i < n;
+       i += (size_t) gridDim.x * blockDim.x)
+    out[i] = __double2float_rn(in[i]);
+}
+
 }  // namespace
+
+extern "C" int h2b_to_single(const double *in, float *out, size_t n, int num_sms,
+                             cudaStream_t st) {
+  if (n == 0) return H2B_OK;
+  const size_t want = (n + FLAT_TPB - 1) / FLAT_TPB, cap = (size_t) 8 * (num_sms > 0 ? num_sms : 148);
+  to_single_kernel<<<(unsigned) (want < cap ? want : cap), FLAT_TPB, 0, st>>>(in, out, n);
+  H2B_CUDA_TRY(cudaGetLastError());
+  return H2B_OK;
+}
 
 extern "C" int h2b_flat_leaves(const FlatLeafArgs *a, cudaStream_t st) {
   if (a->nleaves) leaf_copy_kernel<<<a->nleaves, FLAT_TPB, 0, st>>>(*a);

@@ -1,4 +1,5 @@
-// Restarted GMRES with Householder QR on the device (sm_100a).
+// Restarted GMRES with Householder QR on the device (sm_100a), for one system or a batch of
+// independent systems.
 //
 // Algorithm of init_gmres / step_gmres / finish_gmres (Library/krylov.c:612/659/725) and the
 // driver solve_gmres_avector (Library/krylovsolvers.c:183): the Krylov basis is orthogonalised by
@@ -10,9 +11,13 @@
 // GEMV passes over V instead of j dependent dot/axpy pairs.  This is the same operator as the
 // reference's sequential application; only the rounding order differs.
 //
-// All state (k, tau, T, rhat, scalars) lives on the device; kernels read the current dimension k
-// from device memory, so the kernel sequence of one step is identical for every step and is
-// captured once into a CUDA graph.
+// A batch holds nsys systems on disjoint row ranges of the global vectors (the block-diagonal
+// operator of a forest H2 matrix, or one system per right-hand side): each system has its own
+// qr, reflectors, Hessenberg data, residual estimate, restart and stopping decision, exactly as
+// if it were solved alone; only the operator application is shared.  Vector kernels run one CTA
+// per block of GMRES_TPB rows of one system; the bookkeeping kernel runs one CTA per system.
+// All state lives on the device and kernels read it there, so the kernel sequence of one step
+// is the same for every step and the whole iteration is one CUDA graph (h2b_gmres_loop_graph).
 #include <cuda_runtime.h>
 #include <math.h>
 #include <stdint.h>
@@ -22,7 +27,7 @@
 
 namespace {
 
-constexpr int TPB = 256;
+constexpr int TPB = GMRES_TPB;
 
 struct cd {
   double re, im;
@@ -50,6 +55,50 @@ template <bool CX> __device__ __forceinline__ void st(double *p, size_t i, cd v)
   }
 }
 
+// The arrays of one system.
+struct Sys {
+  uint32_t n, nblk, s;
+  double *qr, *tau, *T, *rhat, *w, *u, *q, *abuf, *part;
+  GmresState *state;
+};
+
+template <bool CX>
+__device__ __forceinline__ Sys sys_view(const GmresDev &g, uint32_t s) {
+  constexpr size_t W = CX ? 2 : 1;
+  const GmresSys y = g.sys[s];
+  Sys v;
+  v.n = y.n;
+  v.nblk = y.nblk;
+  v.s = s;
+  v.qr = g.qr + W * y.qoff;
+  v.tau = g.tau + 2 * (size_t) s * g.kmax;
+  v.T = g.T + 2 * (size_t) s * g.kmax * g.kmax;
+  v.rhat = g.rhat + 2 * (size_t) s * (g.kmax + 1);
+  v.w = g.w + 2 * (size_t) s * (g.kmax + 1);
+  v.u = g.u + 2 * (size_t) s * (g.kmax + 1);
+  v.q = g.q + W * y.row0;
+  v.abuf = g.abuf + W * y.row0;
+  v.part = g.part + 2 * (size_t) y.blk0 * g.ldpart;
+  v.state = g.state + s;
+  return v;
+}
+
+__device__ __forceinline__ bool selected(const GmresState *s, int sel) {
+  return sel == GMRES_SEL_ALL || (sel == GMRES_SEL_ACTIVE ? s->active != 0 : s->restart != 0);
+}
+
+// Vector kernels: CTA -> (system, local row i).  Returns false (uniformly per CTA) when the
+// system is not selected.
+template <bool CX>
+__device__ __forceinline__ bool vec_view(const GmresDev &g, int sel, Sys &v, uint32_t &i,
+                                         uint32_t &lb) {
+  const uint32_t s = g.blk[blockIdx.x];
+  v = sys_view<CX>(g, s);
+  lb = blockIdx.x - g.sys[s].blk0;
+  i = lb * TPB + threadIdx.x;
+  return selected(v.state, sel);
+}
+
 __device__ __forceinline__ double block_sum(double v, double *red) {
   v = warp_sum(v);
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
@@ -66,34 +115,38 @@ __device__ __forceinline__ double block_sum(double v, double *red) {
 
 // element (i, j) of the reflector matrix V (unit lower trapezoidal)
 template <bool CX>
-__device__ __forceinline__ cd vij(const GmresDev &g, uint32_t i, uint32_t j) {
+__device__ __forceinline__ cd vij(const Sys &v, uint32_t i, uint32_t j) {
   if (i < j) return {0.0, 0.0};
   if (i == j) return {1.0, 0.0};
-  return ld<CX>(g.qr, (size_t) i + (size_t) j * g.n);
+  return ld<CX>(v.qr, (size_t) i + (size_t) j * v.n);
 }
 
-// The new Krylov vector a = A q (in g.abuf) is moved into column k+1 of qr, and the partial sums
-// part[b][j] = sum_{i in chunk b} conj(V[i,j]) a[i] (j <= k) of w = V_{0..k}^H a are formed.
+__device__ __forceinline__ void put_part(const GmresDev &g, const Sys &v, uint32_t lb, uint32_t j,
+                                         double re, double im) {
+  v.part[(size_t) lb * g.ldpart * 2 + 2 * j] = re;
+  v.part[(size_t) lb * g.ldpart * 2 + 2 * j + 1] = im;
+}
+
+// The new Krylov vector a = A q (in abuf) is moved into column k+1 of qr, and the partial sums
+// part[b][j] = sum_{i in block b} conj(V[i,j]) a[i] (j <= k) of w = V_{0..k}^H a are formed.
 template <bool CX>
 __global__ void __launch_bounds__(TPB) vth_kernel(GmresDev g) {
   __shared__ double red[2][TPB / 32];
-  const uint32_t k = g.state->k;
-  const uint32_t ncols = k + 1;
-  double *col = g.qr + (size_t) (CX ? 2 : 1) * (k + 1) * g.n;
-  const uint32_t i = blockIdx.x * TPB + threadIdx.x;
-  const bool in = i < g.n;
-  const cd x = in ? ld<CX>(g.abuf, i) : cd{0.0, 0.0};
+  Sys v;
+  uint32_t i, lb;
+  if (!vec_view<CX>(g, GMRES_SEL_ACTIVE, v, i, lb)) return;
+  const uint32_t k = v.state->k;
+  double *col = v.qr + (size_t) (CX ? 2 : 1) * (k + 1) * v.n;
+  const bool in = i < v.n;
+  const cd x = in ? ld<CX>(v.abuf, i) : cd{0.0, 0.0};
   if (in) st<CX>(col, i, x);
-  for (uint32_t j = 0; j < ncols; j++) {
+  for (uint32_t j = 0; j <= k; j++) {
     cd p = {0.0, 0.0};
-    if (in) p = cmul(cconj(vij<CX>(g, i, j)), x);
+    if (in) p = cmul(cconj(vij<CX>(v, i, j)), x);
     const double sr = block_sum(p.re, red[0]);
     double si = 0.0;
     if (CX) si = block_sum(p.im, red[1]);
-    if (threadIdx.x == 0) {
-      g.part[(size_t) blockIdx.x * g.ldpart * 2 + 2 * j] = sr;
-      g.part[(size_t) blockIdx.x * g.ldpart * 2 + 2 * j + 1] = si;
-    }
+    if (threadIdx.x == 0) put_part(g, v, lb, j, sr, si);
   }
 }
 
@@ -102,51 +155,52 @@ template <bool CX>
 __global__ void __launch_bounds__(TPB) apply_v_norm_kernel(GmresDev g) {
   __shared__ double red[TPB / 32];
   __shared__ double us[2 * GMRES_KMAX];
-  const uint32_t k = g.state->k;
+  Sys v;
+  uint32_t i, lb;
+  if (!vec_view<CX>(g, GMRES_SEL_ACTIVE, v, i, lb)) return;
+  const uint32_t k = v.state->k;
   for (uint32_t j = threadIdx.x; j <= k; j += TPB) {
-    us[2 * j] = g.u[2 * j];
-    us[2 * j + 1] = g.u[2 * j + 1];
+    us[2 * j] = v.u[2 * j];
+    us[2 * j + 1] = v.u[2 * j + 1];
   }
   __syncthreads();
-  double *a = g.qr + (size_t) (CX ? 2 : 1) * (k + 1) * g.n;
-  const uint32_t i = blockIdx.x * TPB + threadIdx.x;
+  double *a = v.qr + (size_t) (CX ? 2 : 1) * (k + 1) * v.n;
   double nrm = 0.0;
-  if (i < g.n) {
+  if (i < v.n) {
     cd ai = ld<CX>(a, i);
     const uint32_t jmax = i < k ? i : k;  // V[i, j] = 0 for j > i
     for (uint32_t j = 0; j <= jmax; j++)
-      ai = csub(ai, cmul(vij<CX>(g, i, j), cd{us[2 * j], us[2 * j + 1]}));
+      ai = csub(ai, cmul(vij<CX>(v, i, j), cd{us[2 * j], us[2 * j + 1]}));
     st<CX>(a, i, ai);
     if (i >= k + 1) nrm = cabs2(ai);
   }
   const double s = block_sum(nrm, red);
-  if (threadIdx.x == 0) g.part[(size_t) blockIdx.x * g.ldpart * 2] = s;
+  if (threadIdx.x == 0) put_part(g, v, lb, 0, s, 0.0);
 }
 
 // scale a[i > k+1] *= gamma, a[k+1] = alpha; partial z_j = sum_{i>k+1} conj(V[i,j]) a[i]
 template <bool CX>
 __global__ void __launch_bounds__(TPB) scale_vth_kernel(GmresDev g) {
   __shared__ double red[2][TPB / 32];
-  const uint32_t k = g.state->k;
-  const cd gamma = {g.state->gamma_re, g.state->gamma_im};
-  double *a = g.qr + (size_t) (CX ? 2 : 1) * (k + 1) * g.n;
-  const uint32_t i = blockIdx.x * TPB + threadIdx.x;
+  Sys v;
+  uint32_t i, lb;
+  if (!vec_view<CX>(g, GMRES_SEL_ACTIVE, v, i, lb)) return;
+  const uint32_t k = v.state->k;
+  const cd gamma = {v.state->gamma_re, v.state->gamma_im};
+  double *a = v.qr + (size_t) (CX ? 2 : 1) * (k + 1) * v.n;
   cd x = {0.0, 0.0};
-  if (i < g.n && i > k + 1) {
+  if (i < v.n && i > k + 1) {
     x = cmul(ld<CX>(a, i), gamma);
     st<CX>(a, i, x);
   }
-  if (i == k + 1) st<CX>(a, i, cd{g.state->alpha_re, g.state->alpha_im});
+  if (i == k + 1 && i < v.n) st<CX>(a, i, cd{v.state->alpha_re, v.state->alpha_im});
   for (uint32_t j = 0; j <= k; j++) {
     cd p = {0.0, 0.0};
-    if (i < g.n && i > k + 1) p = cmul(cconj(vij<CX>(g, i, j)), x);
+    if (i < v.n && i > k + 1) p = cmul(cconj(vij<CX>(v, i, j)), x);
     const double sr = block_sum(p.re, red[0]);
     double si = 0.0;
     if (CX) si = block_sum(p.im, red[1]);
-    if (threadIdx.x == 0) {
-      g.part[(size_t) blockIdx.x * g.ldpart * 2 + 2 * j] = sr;
-      g.part[(size_t) blockIdx.x * g.ldpart * 2 + 2 * j + 1] = si;
-    }
+    if (threadIdx.x == 0) put_part(g, v, lb, j, sr, si);
   }
 }
 
@@ -154,48 +208,50 @@ __global__ void __launch_bounds__(TPB) scale_vth_kernel(GmresDev g) {
 template <bool CX>
 __global__ void __launch_bounds__(TPB) make_q_kernel(GmresDev g) {
   __shared__ double us[2 * GMRES_KMAX];
-  const uint32_t k = g.state->k;
+  Sys v;
+  uint32_t i, lb;
+  if (!vec_view<CX>(g, GMRES_SEL_ACTIVE, v, i, lb)) return;
+  const uint32_t k = v.state->k;
   for (uint32_t j = threadIdx.x; j <= k; j += TPB) {
-    us[2 * j] = g.u[2 * j];
-    us[2 * j + 1] = g.u[2 * j + 1];
+    us[2 * j] = v.u[2 * j];
+    us[2 * j + 1] = v.u[2 * j + 1];
   }
   __syncthreads();
-  const uint32_t i = blockIdx.x * TPB + threadIdx.x;
-  if (i >= g.n) return;
+  if (i >= v.n) return;
   cd q = {i == k ? 1.0 : 0.0, 0.0};
   const uint32_t jmax = i < k ? i : k;
-  for (uint32_t j = 0; j <= jmax; j++) q = csub(q, cmul(vij<CX>(g, i, j), cd{us[2 * j], us[2 * j + 1]}));
-  st<CX>(g.q, i, q);
+  for (uint32_t j = 0; j <= jmax; j++) q = csub(q, cmul(vij<CX>(v, i, j), cd{us[2 * j], us[2 * j + 1]}));
+  st<CX>(v.q, i, q);
 }
 
-__device__ cd sum_parts(const GmresDev &g, uint32_t j, uint32_t nb) {
+__device__ cd sum_parts(const GmresDev &g, const Sys &v, uint32_t j) {
   cd s = {0.0, 0.0};
-  for (uint32_t b = 0; b < nb; b++) {
-    s.re += g.part[(size_t) b * g.ldpart * 2 + 2 * j];
-    s.im += g.part[(size_t) b * g.ldpart * 2 + 2 * j + 1];
+  for (uint32_t b = 0; b < v.nblk; b++) {
+    s.re += v.part[(size_t) b * g.ldpart * 2 + 2 * j];
+    s.im += v.part[(size_t) b * g.ldpart * 2 + 2 * j + 1];
   }
   return s;
 }
 
-__device__ __forceinline__ cd Tij(const GmresDev &g, uint32_t i, uint32_t j) {
-  return {g.T[2 * ((size_t) i + (size_t) j * g.kmax)], g.T[2 * ((size_t) i + (size_t) j * g.kmax) + 1]};
+__device__ __forceinline__ cd Tij(const GmresDev &g, const Sys &v, uint32_t i, uint32_t j) {
+  return {v.T[2 * ((size_t) i + (size_t) j * g.kmax)], v.T[2 * ((size_t) i + (size_t) j * g.kmax) + 1]};
 }
-__device__ __forceinline__ void setT(const GmresDev &g, uint32_t i, uint32_t j, cd v) {
-  g.T[2 * ((size_t) i + (size_t) j * g.kmax)] = v.re;
-  g.T[2 * ((size_t) i + (size_t) j * g.kmax) + 1] = v.im;
+__device__ __forceinline__ void setT(const GmresDev &g, const Sys &v, uint32_t i, uint32_t j, cd x) {
+  v.T[2 * ((size_t) i + (size_t) j * g.kmax)] = x.re;
+  v.T[2 * ((size_t) i + (size_t) j * g.kmax) + 1] = x.im;
 }
 
 // Householder scalars of a column with entries diag (first) and squared norm norm2
 // (qrdecomp_amatrix, Library/factorizations.c:2179).
-__device__ void householder(cd diag, double norm2, GmresState *s, uint32_t col, const GmresDev &g) {
+__device__ void householder(cd diag, double norm2, GmresState *s, uint32_t col, const Sys &v) {
   const double norm = sqrt(norm2);
   if (norm2 <= 1e-300) {
     s->gamma_re = 1.0;
     s->gamma_im = 0.0;
     s->alpha_re = diag.re;
     s->alpha_im = diag.im;
-    g.tau[2 * col] = 0.0;
-    g.tau[2 * col + 1] = 0.0;
+    v.tau[2 * col] = 0.0;
+    v.tau[2 * col + 1] = 0.0;
     return;
   }
   const double ad = sqrt(cabs2(diag));
@@ -208,8 +264,8 @@ __device__ void householder(cd diag, double norm2, GmresState *s, uint32_t col, 
   s->gamma_im = gamma.im;
   s->alpha_re = -sgn.re * norm;
   s->alpha_im = -sgn.im * norm;
-  g.tau[2 * col] = beta;
-  g.tau[2 * col + 1] = 0.0;
+  v.tau[2 * col] = beta;
+  v.tau[2 * col + 1] = 0.0;
 }
 
 // Givens rotations of Library/krylov.c:551 / :587 (complex form as in the reference).
@@ -253,8 +309,9 @@ __device__ void apply_givens(cd rho, cd *a, cd *b) {
   *b = csub(cmul(c, bb), cmul(s, aa));
 }
 
-// Bookkeeping kernels: one CTA of SMALL_THREADS threads (>= kmax); O(k) work per thread for the
-// triangular products, sequential only where the algorithm is (Givens, triangular solve).
+// Bookkeeping kernels: one CTA of SMALL_THREADS threads (>= kmax) per system; O(k) work per
+// thread for the triangular products, sequential only where the algorithm is (Givens, triangular
+// solve).
 constexpr int SMALL_THREADS = GMRES_KMAX;
 
 __device__ double block_sum_small(double v, double *red) {
@@ -268,69 +325,71 @@ __device__ double block_sum_small(double v, double *red) {
 }
 
 template <bool CX>
-__global__ void __launch_bounds__(SMALL_THREADS) small_kernel(GmresDev g, int phase) {
+__global__ void __launch_bounds__(SMALL_THREADS) small_kernel(GmresDev g, int phase, int sel) {
   __shared__ double zr[GMRES_KMAX], zi[GMRES_KMAX], red[SMALL_THREADS / 32];
-  GmresState *s = g.state;
+  __shared__ double wr[GMRES_KMAX], wi[GMRES_KMAX];
+  const Sys v = sys_view<CX>(g, blockIdx.x);
+  GmresState *s = v.state;
+  if (!selected(s, sel)) return;
   const uint32_t k = s->k;
-  const uint32_t nb = g.nblocks;
   const uint32_t t = threadIdx.x;
   __syncthreads();  // every thread has read k before anyone may change it
   if (phase == 0) {
     // after vth: w = V^H a; u = T^H w
     if (t <= k) {
-      cd w = sum_parts(g, t, nb);
+      cd w = sum_parts(g, v, t);
       zr[t] = w.re;
       zi[t] = w.im;
-      g.w[2 * t] = w.re;
-      g.w[2 * t + 1] = w.im;
+      v.w[2 * t] = w.re;
+      v.w[2 * t + 1] = w.im;
     }
     __syncthreads();
     if (t <= k) {
       cd u = {0.0, 0.0};
-      for (uint32_t i = 0; i <= t; i++) u = cadd(u, cmul(cconj(Tij(g, i, t)), cd{zr[i], zi[i]}));
-      g.u[2 * t] = u.re;
-      g.u[2 * t + 1] = u.im;
+      for (uint32_t i = 0; i <= t; i++) u = cadd(u, cmul(cconj(Tij(g, v, i, t)), cd{zr[i], zi[i]}));
+      v.u[2 * t] = u.re;
+      v.u[2 * t + 1] = u.im;
     }
   } else if (phase == 1) {
     // after apply_v_norm: Householder scalars of column k+1, rows >= k+1
     double part = 0.0;
-    for (uint32_t b = t; b < nb; b += SMALL_THREADS) part += g.part[(size_t) b * g.ldpart * 2];
+    for (uint32_t b = t; b < v.nblk; b += SMALL_THREADS) part += v.part[(size_t) b * g.ldpart * 2];
     const double norm2 = block_sum_small(part, red);
     if (t == 0) {
-      const double *a = g.qr + (size_t) (CX ? 2 : 1) * (k + 1) * g.n;
-      householder(ld<CX>(a, k + 1), norm2, s, k + 1, g);
+      const double *a = v.qr + (size_t) (CX ? 2 : 1) * (k + 1) * v.n;
+      householder(k + 1 < v.n ? ld<CX>(a, k + 1) : cd{0.0, 0.0}, norm2, s, k + 1, v);
     }
   } else if (phase == 2) {
     // after scale_vth: T column k+1; u for q; Givens; k += 1
-    const cd tau = {g.tau[2 * (k + 1)], g.tau[2 * (k + 1) + 1]};
+    const cd tau = {v.tau[2 * (k + 1)], v.tau[2 * (k + 1) + 1]};
     if (t <= k) {
-      const cd z = cadd(sum_parts(g, t, nb), cconj(vij<CX>(g, k + 1, t)));  // + conj(v_t[k+1])
+      const cd z = cadd(sum_parts(g, v, t), cconj(vij<CX>(v, k + 1, t)));  // + conj(v_t[k+1])
       zr[t] = z.re;
       zi[t] = z.im;
     }
     __syncthreads();
     if (t <= k) {
       cd acc = {0.0, 0.0};
-      for (uint32_t j = t; j <= k; j++) acc = cadd(acc, cmul(Tij(g, t, j), cd{zr[j], zi[j]}));
-      setT(g, t, k + 1, cmul(cd{-tau.re, -tau.im}, acc));
+      for (uint32_t j = t; j <= k; j++) acc = cadd(acc, cmul(Tij(g, v, t, j), cd{zr[j], zi[j]}));
+      setT(g, v, t, k + 1, cmul(cd{-tau.re, -tau.im}, acc));
     }
-    if (t == 0) setT(g, k + 1, k + 1, tau);
+    if (t == 0) setT(g, v, k + 1, k + 1, tau);
     __syncthreads();
     // u = T y, y_j = conj(V[k+1, j]) (j <= k), y_{k+1} = 1
     if (t <= k + 1) {
       cd acc = {0.0, 0.0};
       for (uint32_t j = t; j <= k + 1; j++) {
-        const cd y = j == k + 1 ? cd{1.0, 0.0} : cconj(vij<CX>(g, k + 1, j));
-        acc = cadd(acc, cmul(Tij(g, t, j), y));
+        const cd y = j == k + 1 ? cd{1.0, 0.0} : cconj(vij<CX>(v, k + 1, j));
+        acc = cadd(acc, cmul(Tij(g, v, t, j), y));
       }
-      g.u[2 * t] = acc.re;
-      g.u[2 * t + 1] = acc.im;
+      v.u[2 * t] = acc.re;
+      v.u[2 * t + 1] = acc.im;
     }
     if (t != 0) return;
     // Givens rotations on the new Hessenberg column (rows 0..k+1 of column k+1)
-    double *col = g.qr + (size_t) (CX ? 2 : 1) * (k + 1) * g.n;
+    double *col = v.qr + (size_t) (CX ? 2 : 1) * (k + 1) * v.n;
     for (uint32_t i = 0; i < k; i++) {
-      const cd rho = ld<CX>(g.qr + (size_t) (CX ? 2 : 1) * (i + 1) * g.n, i + 1);
+      const cd rho = ld<CX>(v.qr + (size_t) (CX ? 2 : 1) * (i + 1) * v.n, i + 1);
       cd a = ld<CX>(col, i), b = ld<CX>(col, i + 1);
       apply_givens(rho, &a, &b);
       st<CX>(col, i, a);
@@ -340,137 +399,161 @@ __global__ void __launch_bounds__(SMALL_THREADS) small_kernel(GmresDev g, int ph
     const cd rho = findapply_givens(&a, &b);
     st<CX>(col, k, a);
     st<CX>(col, k + 1, rho);
-    cd r0 = {g.rhat[2 * k], g.rhat[2 * k + 1]}, r1 = {g.rhat[2 * (k + 1)], g.rhat[2 * (k + 1) + 1]};
+    cd r0 = {v.rhat[2 * k], v.rhat[2 * k + 1]}, r1 = {v.rhat[2 * (k + 1)], v.rhat[2 * (k + 1) + 1]};
     apply_givens(rho, &r0, &r1);
-    g.rhat[2 * k] = r0.re;
-    g.rhat[2 * k + 1] = r0.im;
-    g.rhat[2 * (k + 1)] = r1.re;
-    g.rhat[2 * (k + 1) + 1] = r1.im;
+    v.rhat[2 * k] = r0.re;
+    v.rhat[2 * k + 1] = r0.im;
+    v.rhat[2 * (k + 1)] = r1.re;
+    v.rhat[2 * (k + 1) + 1] = r1.im;
     s->k = k + 1;
     s->err = sqrt(cabs2(r1));
   } else if (phase == 3) {
     // finish: rhat_k = R^{-1} rhat_k (back substitution, row by row); z = V_k^H rhat;
     // u = T_k z
     if (t < k) {
-      zr[t] = g.rhat[2 * t];
-      zi[t] = g.rhat[2 * t + 1];
+      zr[t] = v.rhat[2 * t];
+      zi[t] = v.rhat[2 * t + 1];
     }
     __syncthreads();
     for (uint32_t jj = k; jj-- > 0;) {
       if (t == 0) {
-        const cd r = cdiv(cd{zr[jj], zi[jj]}, ld<CX>(g.qr + (size_t) (CX ? 2 : 1) * (jj + 1) * g.n, jj));
+        const cd r = cdiv(cd{zr[jj], zi[jj]}, ld<CX>(v.qr + (size_t) (CX ? 2 : 1) * (jj + 1) * v.n, jj));
         zr[jj] = r.re;
         zi[jj] = r.im;
       }
       __syncthreads();
       // eliminate the solved unknown from the rows above (column jj+1 of R)
       if (t < jj) {
-        const cd v = cmul(ld<CX>(g.qr + (size_t) (CX ? 2 : 1) * (jj + 1) * g.n, t), cd{zr[jj], zi[jj]});
-        zr[t] -= v.re;
-        zi[t] -= v.im;
+        const cd x = cmul(ld<CX>(v.qr + (size_t) (CX ? 2 : 1) * (jj + 1) * v.n, t), cd{zr[jj], zi[jj]});
+        zr[t] -= x.re;
+        zi[t] -= x.im;
       }
       __syncthreads();
     }
     if (t < k) {
-      g.rhat[2 * t] = zr[t];
-      g.rhat[2 * t + 1] = zi[t];
+      v.rhat[2 * t] = zr[t];
+      v.rhat[2 * t + 1] = zi[t];
     }
-    __shared__ double wr[GMRES_KMAX], wi[GMRES_KMAX];
     if (t < k) {
       cd acc = {zr[t], zi[t]};
-      for (uint32_t i = t + 1; i < k; i++) acc = cadd(acc, cmul(cconj(vij<CX>(g, i, t)), cd{zr[i], zi[i]}));
+      for (uint32_t i = t + 1; i < k; i++) acc = cadd(acc, cmul(cconj(vij<CX>(v, i, t)), cd{zr[i], zi[i]}));
       wr[t] = acc.re;
       wi[t] = acc.im;
     }
     __syncthreads();
     if (t < k) {
       cd acc = {0.0, 0.0};
-      for (uint32_t j = t; j < k; j++) acc = cadd(acc, cmul(Tij(g, t, j), cd{wr[j], wi[j]}));
-      g.u[2 * t] = acc.re;
-      g.u[2 * t + 1] = acc.im;
+      for (uint32_t j = t; j < k; j++) acc = cadd(acc, cmul(Tij(g, v, t, j), cd{wr[j], wi[j]}));
+      v.u[2 * t] = acc.re;
+      v.u[2 * t + 1] = acc.im;
     }
   } else if (phase == 4 || phase == 6) {
     // ||r||^2 (init, Householder of column 0) or ||b||^2, from part[b][0]
     double part = 0.0;
-    for (uint32_t b = t; b < nb; b += SMALL_THREADS) part += g.part[(size_t) b * g.ldpart * 2];
+    for (uint32_t b = t; b < v.nblk; b += SMALL_THREADS) part += v.part[(size_t) b * g.ldpart * 2];
     const double norm2 = block_sum_small(part, red);
     if (t == 0) {
-      if (phase == 4)
-        householder(ld<CX>(g.qr, 0), norm2, s, 0, g);
-      else
+      if (phase == 4) {
+        householder(ld<CX>(v.qr, 0), norm2, s, 0, v);
+      } else {
         s->bnorm = sqrt(norm2);
+        s->tol = g.eps * s->bnorm;
+      }
     }
   } else if (phase == 5) {
     // init, after scaling column 0: T, rhat, k, err
-    for (uint32_t i = t; i < 2 * (g.kmax + 1); i += SMALL_THREADS) g.rhat[i] = 0.0;
+    for (uint32_t i = t; i < 2 * (g.kmax + 1); i += SMALL_THREADS) v.rhat[i] = 0.0;
     __syncthreads();
     if (t == 0) {
-      g.rhat[0] = s->alpha_re;
-      g.rhat[1] = s->alpha_im;
-      setT(g, 0, 0, cd{g.tau[0], g.tau[1]});
+      v.rhat[0] = s->alpha_re;
+      v.rhat[1] = s->alpha_im;
+      setT(g, v, 0, 0, cd{v.tau[0], v.tau[1]});
       s->k = 0;
       s->err = sqrt(s->alpha_re * s->alpha_re + s->alpha_im * s->alpha_im);
+      // FP64: the reference steps after every restart.  Mixed: err is the FP64 residual of the
+      // new start, an exact stopping test.
+      s->active = g.mixed ? (s->err > s->tol ? 1u : 0u) : 1u;
+      s->verify = 0;
     }
   }
 }
 
 // x += rhat_(k) - V_k u (finish); vector kernels
 template <bool CX>
-__global__ void __launch_bounds__(TPB) update_x_kernel(GmresDev g, double *x) {
+__global__ void __launch_bounds__(TPB) update_x_kernel(GmresDev g, double *x, int sel) {
   __shared__ double us[2 * GMRES_KMAX];
-  const uint32_t k = g.state->k;
+  Sys v;
+  uint32_t i, lb;
+  if (!vec_view<CX>(g, sel, v, i, lb)) return;
+  const uint32_t k = v.state->k;
   for (uint32_t j = threadIdx.x; j < k; j += TPB) {
-    us[2 * j] = g.u[2 * j];
-    us[2 * j + 1] = g.u[2 * j + 1];
+    us[2 * j] = v.u[2 * j];
+    us[2 * j + 1] = v.u[2 * j + 1];
   }
   __syncthreads();
-  const uint32_t i = blockIdx.x * TPB + threadIdx.x;
-  if (i >= g.n || k == 0) return;
-  cd d = i < k ? cd{g.rhat[2 * i], g.rhat[2 * i + 1]} : cd{0.0, 0.0};
+  if (i >= v.n || k == 0) return;
+  double *xs = x + (size_t) (CX ? 2 : 1) * g.sys[v.s].row0;
+  cd d = i < k ? cd{v.rhat[2 * i], v.rhat[2 * i + 1]} : cd{0.0, 0.0};
   const uint32_t jmax = i < k - 1 ? i : k - 1;
-  for (uint32_t j = 0; j <= jmax; j++) d = csub(d, cmul(vij<CX>(g, i, j), cd{us[2 * j], us[2 * j + 1]}));
-  st<CX>(x, i, cadd(ld<CX>(x, i), d));
+  for (uint32_t j = 0; j <= jmax; j++) d = csub(d, cmul(vij<CX>(v, i, j), cd{us[2 * j], us[2 * j + 1]}));
+  st<CX>(xs, i, cadd(ld<CX>(xs, i), d));
 }
 
-// qr[:,0] = b; also partial ||b||^2 (for phase 6)
+// abuf = 0 over the whole vector
 template <bool CX>
-__global__ void __launch_bounds__(TPB) copy_b_kernel(GmresDev g, const double *b) {
+__global__ void __launch_bounds__(TPB) zero_abuf_kernel(GmresDev g) {
+  const size_t n = (size_t) (CX ? 2 : 1) * g.n;
+  for (size_t i = blockIdx.x * (size_t) TPB + threadIdx.x; i < n; i += (size_t) gridDim.x * TPB)
+    g.abuf[i] = 0.0;
+}
+
+// partial ||b||^2 (for phase 6)
+template <bool CX>
+__global__ void __launch_bounds__(TPB) bnorm_kernel(GmresDev g, const double *b) {
   __shared__ double red[TPB / 32];
-  const uint32_t i = blockIdx.x * TPB + threadIdx.x;
-  double v = 0.0;
-  if (i < g.n) {
-    const cd bi = ld<CX>(b, i);
-    st<CX>(g.qr, i, bi);
-    v = cabs2(bi);
+  Sys v;
+  uint32_t i, lb;
+  vec_view<CX>(g, GMRES_SEL_ALL, v, i, lb);
+  const double *bs = b + (size_t) (CX ? 2 : 1) * g.sys[v.s].row0;
+  const double x = i < v.n ? cabs2(ld<CX>(bs, i)) : 0.0;
+  const double s = block_sum(x, red);
+  if (threadIdx.x == 0) put_part(g, v, lb, 0, s, 0.0);
+}
+
+// qr[:,0] = b - A x (A x in abuf) and its partial norm^2
+template <bool CX>
+__global__ void __launch_bounds__(TPB) init0_kernel(GmresDev g, const double *b, int sel) {
+  __shared__ double red[TPB / 32];
+  Sys v;
+  uint32_t i, lb;
+  if (!vec_view<CX>(g, sel, v, i, lb)) return;
+  const double *bs = b + (size_t) (CX ? 2 : 1) * g.sys[v.s].row0;
+  double x = 0.0;
+  if (i < v.n) {
+    const cd r = csub(ld<CX>(bs, i), ld<CX>(v.abuf, i));
+    st<CX>(v.qr, i, r);
+    x = cabs2(r);
   }
-  const double s = block_sum(v, red);
-  if (threadIdx.x == 0) g.part[(size_t) blockIdx.x * g.ldpart * 2] = s;
-}
-
-// partial ||qr[:,0]||^2
-template <bool CX>
-__global__ void __launch_bounds__(TPB) norm0_kernel(GmresDev g) {
-  __shared__ double red[TPB / 32];
-  const uint32_t i = blockIdx.x * TPB + threadIdx.x;
-  const double v = i < g.n ? cabs2(ld<CX>(g.qr, i)) : 0.0;
-  const double s = block_sum(v, red);
-  if (threadIdx.x == 0) g.part[(size_t) blockIdx.x * g.ldpart * 2] = s;
+  const double s = block_sum(x, red);
+  if (threadIdx.x == 0) put_part(g, v, lb, 0, s, 0.0);
 }
 
 // column 0: scale rows > 0 by gamma, row 0 = alpha; q = H_0 e_0 = e_0 - tau_0 v_0
 template <bool CX>
-__global__ void __launch_bounds__(TPB) scale0_kernel(GmresDev g) {
-  const uint32_t i = blockIdx.x * TPB + threadIdx.x;
-  if (i >= g.n) return;
-  const cd gamma = {g.state->gamma_re, g.state->gamma_im};
-  const cd tau = {g.tau[0], g.tau[1]};
+__global__ void __launch_bounds__(TPB) scale0_kernel(GmresDev g, int sel) {
+  Sys v;
+  uint32_t i, lb;
+  if (!vec_view<CX>(g, sel, v, i, lb)) return;
+  if (i >= v.n) return;
+  const cd gamma = {v.state->gamma_re, v.state->gamma_im};
+  const cd tau = {v.tau[0], v.tau[1]};
   if (i == 0) {
-    st<CX>(g.qr, 0, cd{g.state->alpha_re, g.state->alpha_im});
-    st<CX>(g.q, 0, csub(cd{1.0, 0.0}, tau));
+    st<CX>(v.qr, 0, cd{v.state->alpha_re, v.state->alpha_im});
+    st<CX>(v.q, 0, csub(cd{1.0, 0.0}, tau));
   } else {
-    const cd v = cmul(ld<CX>(g.qr, i), gamma);
-    st<CX>(g.qr, i, v);
-    st<CX>(g.q, i, cmul(cd{-tau.re, -tau.im}, v));
+    const cd x = cmul(ld<CX>(v.qr, i), gamma);
+    st<CX>(v.qr, i, x);
+    st<CX>(v.q, i, cmul(cd{-tau.re, -tau.im}, x));
   }
 }
 
@@ -478,76 +561,220 @@ template <bool CX>
 int step_impl(const GmresDev &g, const GmresOp &op, cudaStream_t st) {
   const uint32_t nb = g.nblocks;
   // a = A q into the staging vector, then into column k+1 of qr (k is read on the device)
-  H2B_CUDA_TRY(cudaMemsetAsync(g.abuf, 0, sizeof(double) * (CX ? 2 : 1) * g.n, st));
-  int rc = op.apply(op.ctx, g.q, g.abuf, 1.0, 0.0, st);
+  zero_abuf_kernel<CX><<<nb, TPB, 0, st>>>(g);
+  int rc = (op.apply_lo ? op.apply_lo : op.apply)(op.ctx, g.q, g.abuf, 1.0, 0.0, st);
   if (rc != H2B_OK) return rc;
   vth_kernel<CX><<<nb, TPB, 0, st>>>(g);
-  small_kernel<CX><<<1, SMALL_THREADS, 0, st>>>(g, 0);
+  small_kernel<CX><<<g.nsys, SMALL_THREADS, 0, st>>>(g, 0, GMRES_SEL_ACTIVE);
   apply_v_norm_kernel<CX><<<nb, TPB, 0, st>>>(g);
-  small_kernel<CX><<<1, SMALL_THREADS, 0, st>>>(g, 1);
+  small_kernel<CX><<<g.nsys, SMALL_THREADS, 0, st>>>(g, 1, GMRES_SEL_ACTIVE);
   scale_vth_kernel<CX><<<nb, TPB, 0, st>>>(g);
-  small_kernel<CX><<<1, SMALL_THREADS, 0, st>>>(g, 2);
+  small_kernel<CX><<<g.nsys, SMALL_THREADS, 0, st>>>(g, 2, GMRES_SEL_ACTIVE);
   make_q_kernel<CX><<<nb, TPB, 0, st>>>(g);
   H2B_CUDA_TRY(cudaGetLastError());
   return H2B_OK;
 }
 
 template <bool CX>
-int init_impl(const GmresDev &g, const GmresOp &op, const double *b, double *x, cudaStream_t st) {
+int init_impl(const GmresDev &g, const GmresOp &op, const double *b, double *x, int sel,
+              cudaStream_t st) {
   const uint32_t nb = g.nblocks;
-  copy_b_kernel<CX><<<nb, TPB, 0, st>>>(g, b);
   // qr[:,0] = b - A x
-  int rc = op.apply(op.ctx, x, g.qr, -1.0, 0.0, st);
+  zero_abuf_kernel<CX><<<nb, TPB, 0, st>>>(g);
+  int rc = op.apply(op.ctx, x, g.abuf, 1.0, 0.0, st);
   if (rc != H2B_OK) return rc;
-  norm0_kernel<CX><<<nb, TPB, 0, st>>>(g);
-  small_kernel<CX><<<1, SMALL_THREADS, 0, st>>>(g, 4);
-  scale0_kernel<CX><<<nb, TPB, 0, st>>>(g);
-  small_kernel<CX><<<1, SMALL_THREADS, 0, st>>>(g, 5);
+  init0_kernel<CX><<<nb, TPB, 0, st>>>(g, b, sel);
+  small_kernel<CX><<<g.nsys, SMALL_THREADS, 0, st>>>(g, 4, sel);
+  scale0_kernel<CX><<<nb, TPB, 0, st>>>(g, sel);
+  small_kernel<CX><<<g.nsys, SMALL_THREADS, 0, st>>>(g, 5, sel);
   H2B_CUDA_TRY(cudaGetLastError());
   return H2B_OK;
 }
 
 template <bool CX>
-int finish_impl(const GmresDev &g, const GmresOp &op, const double *b, double *x,
-                cudaStream_t st) {
-  const uint32_t nb = g.nblocks;
-  small_kernel<CX><<<1, SMALL_THREADS, 0, st>>>(g, 3);
-  update_x_kernel<CX><<<nb, TPB, 0, st>>>(g, x);
+int finish_only(const GmresDev &g, double *x, int sel, cudaStream_t st) {
+  small_kernel<CX><<<g.nsys, SMALL_THREADS, 0, st>>>(g, 3, sel);
+  update_x_kernel<CX><<<g.nblocks, TPB, 0, st>>>(g, x, sel);
   H2B_CUDA_TRY(cudaGetLastError());
-  return init_impl<CX>(g, op, b, x, st);
+  return H2B_OK;
+}
+
+template <bool CX>
+int finish_impl(const GmresDev &g, const GmresOp &op, const double *b, double *x, int sel,
+                cudaStream_t st) {
+  int rc = finish_only<CX>(g, x, sel, st);
+  if (rc != H2B_OK) return rc;
+  return init_impl<CX>(g, op, b, x, sel, st);
 }
 
 template <bool CX>
 int bnorm_impl(const GmresDev &g, const double *b, cudaStream_t st) {
-  copy_b_kernel<CX><<<g.nblocks, TPB, 0, st>>>(g, b);
-  small_kernel<CX><<<1, SMALL_THREADS, 0, st>>>(g, 6);
+  bnorm_kernel<CX><<<g.nblocks, TPB, 0, st>>>(g, b);
+  small_kernel<CX><<<g.nsys, SMALL_THREADS, 0, st>>>(g, 6, GMRES_SEL_ALL);
   H2B_CUDA_TRY(cudaGetLastError());
   return H2B_OK;
 }
 
-// Loop control of the graph-resident iteration (one thread each).
+// Loop control of the graph-resident iteration (one CTA each, threads stride over the systems).
+__device__ __forceinline__ bool keeps_going(const GmresState *s, uint32_t maxiter) {
+  return s->err > s->tol && (maxiter == 0 || s->iter + 1 != maxiter) && !s->nan;
+}
+
 __global__ void precheck_kernel(GmresDev g, cudaGraphConditionalHandle hw) {
-  const GmresState *s = g.state;
-  const bool go = s->err > s->tol && (s->maxiter == 0 || s->iter + 1 != s->maxiter) &&
-                  s->budget > 0 && !s->nan;
-  cudaGraphSetConditional(hw, go ? 1u : 0u);
+  __shared__ int any;
+  if (threadIdx.x == 0) any = 0;
+  __syncthreads();
+  for (uint32_t s = threadIdx.x; s < g.nsys; s += blockDim.x) {
+    GmresState *y = g.state + s;
+    y->active = keeps_going(y, g.ctl->maxiter) ? 1u : 0u;
+    y->restart = 0;
+    if (y->active) any = 1;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    g.ctl->any_active = any;
+    cudaGraphSetConditional(hw, (any && g.ctl->budget > 0) ? 1u : 0u);
+  }
 }
 
 __global__ void decide_kernel(GmresDev g, cudaGraphConditionalHandle hi) {
-  cudaGraphSetConditional(hi, g.state->k + 1 >= g.kmax ? 1u : 0u);
+  __shared__ int any;
+  if (threadIdx.x == 0) any = 0;
+  __syncthreads();
+  for (uint32_t s = threadIdx.x; s < g.nsys; s += blockDim.x) {
+    GmresState *y = g.state + s;
+    y->restart = (y->active && (y->k + 1 >= g.kmax || y->verify)) ? 1u : 0u;
+    if (y->restart) any = 1;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    g.ctl->any_restart = any;
+    cudaGraphSetConditional(hi, any ? 1u : 0u);
+  }
 }
 
 __global__ void control_kernel(GmresDev g, cudaGraphConditionalHandle hw) {
-  GmresState *s = g.state;
-  s->iter++;
-  s->budget--;
-  if (!(s->err == s->err)) s->nan = 1;
-  const bool go = s->err > s->tol && (s->maxiter == 0 || s->iter + 1 != s->maxiter) &&
-                  s->budget > 0 && !s->nan;
-  cudaGraphSetConditional(hw, go ? 1u : 0u);
+  __shared__ int any;
+  if (threadIdx.x == 0) any = 0;
+  __syncthreads();
+  for (uint32_t s = threadIdx.x; s < g.nsys; s += blockDim.x) {
+    GmresState *y = g.state + s;
+    y->restart = 0;
+    if (!y->active) continue;
+    y->iter++;
+    if (!(y->err == y->err)) y->nan = 1;
+    y->active = keeps_going(y, g.ctl->maxiter) ? 1u : 0u;
+    // mixed precision: an estimate below tol is checked by a restart with the FP64 residual
+    if (g.mixed && !y->active && !y->nan && !(y->err > y->tol) &&
+        (g.ctl->maxiter == 0 || y->iter + 1 != g.ctl->maxiter)) {
+      y->active = 1;
+      y->verify = 1;
+    }
+    if (y->active) any = 1;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    g.ctl->budget--;
+    g.ctl->any_active = any;
+    cudaGraphSetConditional(hw, (any && g.ctl->budget > 0) ? 1u : 0u);
+  }
+}
+
+constexpr int CTL_THREADS = 256;
+
+int add_ctl_node(cudaGraphNode_t *node, cudaGraph_t graph, const cudaGraphNode_t *dep,
+                 size_t ndep, void *func, GmresDev *g, cudaGraphConditionalHandle *h) {
+  void *args[] = {g, h};
+  cudaKernelNodeParams kp = {};
+  kp.func = func;
+  kp.gridDim = dim3(1);
+  kp.blockDim = dim3(CTL_THREADS);
+  kp.kernelParams = args;
+  H2B_CUDA_TRY(cudaGraphAddKernelNode(node, graph, dep, ndep, &kp));
+  return H2B_OK;
 }
 
 }  // namespace
+
+size_t h2b_gmres_workspace(int cx, uint32_t nsys, const uint32_t *sizes, uint32_t kmax,
+                           uint32_t *nblocks) {
+  const size_t W = cx ? 2 : 1;
+  uint64_t n = 0, nb = 0;
+  for (uint32_t s = 0; s < nsys; s++) {
+    n += sizes[s];
+    nb += (sizes[s] + TPB - 1) / TPB;
+  }
+  if (nblocks) *nblocks = (uint32_t) nb;
+  const size_t ld = kmax + 1;
+  return W * n * kmax                       // qr
+         + 2 * (size_t) nsys * kmax          // tau
+         + 2 * (size_t) nsys * kmax * kmax   // T
+         + 3 * 2 * (size_t) nsys * ld        // rhat, w, u
+         + 2 * W * n                         // q, abuf
+         + 2 * nb * ld                       // part
+         + (sizeof(GmresState) * nsys + sizeof(GmresCtl) + sizeof(GmresSys) * nsys +
+            sizeof(uint32_t) * nb) / sizeof(double) + 64;
+}
+
+void h2b_gmres_layout(GmresDev *g, double *p, int cx, uint32_t nsys, const uint32_t *sizes,
+                      uint32_t kmax, GmresSys *sys_host, uint32_t *blk_host) {
+  const size_t W = cx ? 2 : 1;
+  uint64_t n = 0, q = 0;
+  uint32_t nb = 0;
+  for (uint32_t s = 0; s < nsys; s++) {
+    sys_host[s].n = sizes[s];
+    sys_host[s].row0 = (uint32_t) n;
+    sys_host[s].qoff = q;
+    sys_host[s].blk0 = nb;
+    sys_host[s].nblk = (sizes[s] + TPB - 1) / TPB;
+    for (uint32_t b = 0; b < sys_host[s].nblk; b++) blk_host[nb + b] = s;
+    nb += sys_host[s].nblk;
+    n += sizes[s];
+    q += (uint64_t) sizes[s] * kmax;
+  }
+  const size_t ld = kmax + 1;
+  g->cx = cx;
+  g->nsys = nsys;
+  g->n = (uint32_t) n;
+  g->kmax = kmax;
+  g->nblocks = nb;
+  g->ldpart = (uint32_t) ld;
+  g->qr = p; p += W * n * kmax;
+  g->tau = p; p += 2 * (size_t) nsys * kmax;
+  g->T = p; p += 2 * (size_t) nsys * kmax * kmax;
+  g->rhat = p; p += 2 * (size_t) nsys * ld;
+  g->w = p; p += 2 * (size_t) nsys * ld;
+  g->u = p; p += 2 * (size_t) nsys * ld;
+  g->q = p; p += W * n;
+  g->abuf = p; p += W * n;
+  g->part = p; p += 2 * (size_t) nb * ld;
+  char *c = (char *) (((uintptr_t) p + 255) & ~(uintptr_t) 255);
+  g->state = (GmresState *) c; c += sizeof(GmresState) * nsys;
+  g->ctl = (GmresCtl *) c; c += sizeof(GmresCtl);
+  c = (char *) (((uintptr_t) c + 15) & ~(uintptr_t) 15);
+  g->sys = (const GmresSys *) c; c += sizeof(GmresSys) * nsys;
+  g->blk = (const uint32_t *) c;
+}
+
+extern "C" int h2b_gmres_step(const GmresDev *g, const GmresOp *op, cudaStream_t st) {
+  return g->cx ? step_impl<true>(*g, *op, st) : step_impl<false>(*g, *op, st);
+}
+extern "C" int h2b_gmres_init(const GmresDev *g, const GmresOp *op, const double *b, double *x,
+                              int sel, cudaStream_t st) {
+  return g->cx ? init_impl<true>(*g, *op, b, x, sel, st) : init_impl<false>(*g, *op, b, x, sel, st);
+}
+extern "C" int h2b_gmres_finish(const GmresDev *g, const GmresOp *op, const double *b, double *x,
+                                int sel, cudaStream_t st) {
+  return g->cx ? finish_impl<true>(*g, *op, b, x, sel, st)
+               : finish_impl<false>(*g, *op, b, x, sel, st);
+}
+extern "C" int h2b_gmres_bnorm(const GmresDev *g, const double *b, cudaStream_t st) {
+  return g->cx ? bnorm_impl<true>(*g, b, st) : bnorm_impl<false>(*g, b, st);
+}
+
+extern "C" int h2b_gmres_update(const GmresDev *g, double *x, int sel, cudaStream_t st) {
+  return g->cx ? finish_only<true>(*g, x, sel, st) : finish_only<false>(*g, x, sel, st);
+}
 
 extern "C" int h2b_gmres_loop_graph(const GmresDev *g, const GmresOp *op, const double *b,
                                     double *x, cudaStream_t st, cudaGraphExec_t *exec) {
@@ -561,17 +788,11 @@ extern "C" int h2b_gmres_loop_graph(const GmresDev *g, const GmresOp *op, const 
   cudaGraphConditionalHandle hw, hi;
   H2B_CUDA_TRY(cudaGraphConditionalHandleCreate(&hw, top, 0, 0));
   GmresDev gv = *g;
+  int rc;
   // top: precheck -> WHILE
   cudaGraphNode_t pre, wnode, dec, inode;
-  {
-    void *args[] = {&gv, &hw};
-    cudaKernelNodeParams kp = {};
-    kp.func = (void *) precheck_kernel;
-    kp.gridDim = dim3(1);
-    kp.blockDim = dim3(1);
-    kp.kernelParams = args;
-    H2B_CUDA_TRY(cudaGraphAddKernelNode(&pre, top, nullptr, 0, &kp));
-  }
+  if ((rc = add_ctl_node(&pre, top, nullptr, 0, (void *) precheck_kernel, &gv, &hw)) != H2B_OK)
+    return rc;
   cudaGraphNodeParams wp = {};
   wp.type = cudaGraphNodeTypeConditional;
   wp.conditional.handle = hw;
@@ -581,15 +802,8 @@ extern "C" int h2b_gmres_loop_graph(const GmresDev *g, const GmresOp *op, const 
   cudaGraph_t body = wp.conditional.phGraph_out[0];
   // body: decide -> IF(restart) -> step -> control
   H2B_CUDA_TRY(cudaGraphConditionalHandleCreate(&hi, body, 0, 0));
-  {
-    void *args[] = {&gv, &hi};
-    cudaKernelNodeParams kp = {};
-    kp.func = (void *) decide_kernel;
-    kp.gridDim = dim3(1);
-    kp.blockDim = dim3(1);
-    kp.kernelParams = args;
-    H2B_CUDA_TRY(cudaGraphAddKernelNode(&dec, body, nullptr, 0, &kp));
-  }
+  if ((rc = add_ctl_node(&dec, body, nullptr, 0, (void *) decide_kernel, &gv, &hi)) != H2B_OK)
+    return rc;
   cudaGraphNodeParams ip = {};
   ip.type = cudaGraphNodeTypeConditional;
   ip.conditional.handle = hi;
@@ -597,10 +811,10 @@ extern "C" int h2b_gmres_loop_graph(const GmresDev *g, const GmresOp *op, const 
   ip.conditional.size = 1;
   H2B_CUDA_TRY(cudaGraphAddNode(&inode, body, &dec, 1, &ip));
   cudaGraph_t ifbody = ip.conditional.phGraph_out[0];
-  int rc;
   H2B_CUDA_TRY(cudaStreamBeginCaptureToGraph(st, ifbody, nullptr, nullptr, 0,
                                              cudaStreamCaptureModeThreadLocal));
-  rc = g->cx ? finish_impl<true>(*g, *op, b, x, st) : finish_impl<false>(*g, *op, b, x, st);
+  rc = g->cx ? finish_impl<true>(*g, *op, b, x, GMRES_SEL_RESTART, st)
+             : finish_impl<false>(*g, *op, b, x, GMRES_SEL_RESTART, st);
   cudaGraph_t captured = nullptr;
   cudaError_t ce = cudaStreamEndCapture(st, &captured);
   if (rc != H2B_OK) return rc;
@@ -609,7 +823,7 @@ extern "C" int h2b_gmres_loop_graph(const GmresDev *g, const GmresOp *op, const 
                                              cudaStreamCaptureModeThreadLocal));
   rc = g->cx ? step_impl<true>(*g, *op, st) : step_impl<false>(*g, *op, st);
   if (rc == H2B_OK) {
-    control_kernel<<<1, 1, 0, st>>>(gv, hw);
+    control_kernel<<<1, CTL_THREADS, 0, st>>>(gv, hw);
     if (cudaGetLastError() != cudaSuccess) rc = H2B_ERR_CUDA;
   }
   ce = cudaStreamEndCapture(st, &captured);
@@ -619,17 +833,44 @@ extern "C" int h2b_gmres_loop_graph(const GmresDev *g, const GmresOp *op, const 
   return H2B_OK;
 }
 
-extern "C" int h2b_gmres_step(const GmresDev *g, const GmresOp *op, cudaStream_t st) {
-  return g->cx ? step_impl<true>(*g, *op, st) : step_impl<false>(*g, *op, st);
-}
-extern "C" int h2b_gmres_init(const GmresDev *g, const GmresOp *op, const double *b, double *x,
-                              cudaStream_t st) {
-  return g->cx ? init_impl<true>(*g, *op, b, x, st) : init_impl<false>(*g, *op, b, x, st);
-}
-extern "C" int h2b_gmres_finish(const GmresDev *g, const GmresOp *op, const double *b, double *x,
-                                cudaStream_t st) {
-  return g->cx ? finish_impl<true>(*g, *op, b, x, st) : finish_impl<false>(*g, *op, b, x, st);
-}
-extern "C" int h2b_gmres_bnorm(const GmresDev *g, const double *b, cudaStream_t st) {
-  return g->cx ? bnorm_impl<true>(*g, b, st) : bnorm_impl<false>(*g, b, st);
+extern "C" int h2b_gmres_run(const GmresDev *g, const GmresOp *op, const double *b, double *x,
+                             uint32_t maxiter, cudaStream_t st, GmresState *host_state) {
+  constexpr uint32_t kLoopBudget = 512;
+  cudaGraphExec_t exec = nullptr;
+  int rc = h2b_gmres_loop_graph(g, op, b, x, st, &exec);
+  if (rc != H2B_OK) return rc;
+  struct ExecFree {
+    cudaGraphExec_t e;
+    ~ExecFree() {
+      if (e) cudaGraphExecDestroy(e);
+    }
+  } ef{exec};
+  H2B_CUDA_TRY(cudaMemsetAsync(g->state, 0, sizeof(GmresState) * g->nsys, st));
+  H2B_CUDA_TRY(cudaMemsetAsync(g->T, 0, sizeof(double) * 2 * (size_t) g->nsys * g->kmax * g->kmax, st));
+  if ((rc = h2b_gmres_bnorm(g, b, st)) != H2B_OK) return rc;
+  if ((rc = h2b_gmres_init(g, op, b, x, GMRES_SEL_ALL, st)) != H2B_OK) return rc;
+  GmresCtl ctl = {maxiter, kLoopBudget, 0, 0};
+  while (true) {
+    ctl.budget = kLoopBudget;
+    H2B_CUDA_TRY(cudaMemcpyAsync(g->ctl, &ctl, sizeof(GmresCtl), cudaMemcpyHostToDevice, st));
+    H2B_CUDA_TRY(cudaGraphLaunch(exec, st));
+    GmresCtl out;
+    H2B_CUDA_TRY(cudaMemcpyAsync(&out, g->ctl, sizeof(GmresCtl), cudaMemcpyDeviceToHost, st));
+    H2B_CUDA_TRY(cudaStreamSynchronize(st));
+    if (!out.any_active) break;
+    if (out.budget != 0) {
+      h2b_set_error("GMRES: device loop stopped with active systems and budget %u left",
+                    out.budget);
+      return H2B_ERR_INTERNAL;
+    }
+  }
+  if ((rc = g->cx ? finish_only<true>(*g, x, GMRES_SEL_ALL, st)
+                  : finish_only<false>(*g, x, GMRES_SEL_ALL, st)) != H2B_OK)
+    return rc;
+  if (host_state) {
+    H2B_CUDA_TRY(cudaMemcpyAsync(host_state, g->state, sizeof(GmresState) * g->nsys,
+                                 cudaMemcpyDeviceToHost, st));
+  }
+  H2B_CUDA_TRY(cudaStreamSynchronize(st));
+  return H2B_OK;
 }

@@ -69,8 +69,8 @@ __global__ void scatter_kernel(const double *__restrict__ yp, const uint32_t *__
 // All threads of the CTA must call it (it synchronises).  With VGLOBAL, `v` is a global array
 // read through L2 (it may have been written by another CTA of the same launch); otherwise `v`
 // is in shared memory.
-template <bool CX, bool VGLOBAL>
-__device__ __forceinline__ void gemv_split(const double *__restrict__ P, uint32_t ld,
+template <bool CX, bool VGLOBAL, typename TP = double>
+__device__ __forceinline__ void gemv_split(const TP *__restrict__ P, uint32_t ld,
                                            uint32_t nrows, uint32_t ncols,
                                            const double *__restrict__ v, double *red,
                                            double *out) {
@@ -81,7 +81,7 @@ __device__ __forceinline__ void gemv_split(const double *__restrict__ P, uint32_
   if (g < G) {
 #pragma unroll 4
     for (uint32_t c = g; c < ncols; c += G) {
-      const double p = P[r + (size_t) c * ld];
+      const double p = (double) P[r + (size_t) c * ld];
       const double vr = VGLOBAL ? __ldcg(v + W * c) : v[W * c];
       sr = fma(p, vr, sr);
       if (CX) si = fma(p, VGLOBAL ? __ldcg(v + W * c + 1) : v[W * c + 1], si);
@@ -105,8 +105,8 @@ __device__ __forceinline__ void gemv_split(const double *__restrict__ P, uint32_
 // y_rows += M x_cols for a column-major rows x cols panel M (ld = rows, complex if CX).  The
 // column groups' partial sums are combined in shared memory (`red`, blockDim * W doubles), so
 // each output row receives one atomic addition per block.  All threads must call it.
-template <bool CX>
-__device__ __forceinline__ void panel_mv_atomic(const double *__restrict__ M, uint32_t rows,
+template <bool CX, typename TM = double>
+__device__ __forceinline__ void panel_mv_atomic(const TM *__restrict__ M, uint32_t rows,
                                                 uint32_t cols, const double *__restrict__ xv,
                                                 double *__restrict__ yv, double *red) {
   constexpr int W = CX ? 2 : 1;
@@ -120,11 +120,12 @@ __device__ __forceinline__ void panel_mv_atomic(const double *__restrict__ M, ui
       for (uint32_t j = g; j < cols; j += groups) {
         const size_t e = (size_t) r + (size_t) j * rows;
         if (CX) {
-          const double mr = M[2 * e], mi = M[2 * e + 1], xr = xv[2 * j], xi = xv[2 * j + 1];
+          const double mr = (double) M[2 * e], mi = (double) M[2 * e + 1], xr = xv[2 * j],
+                       xi = xv[2 * j + 1];
           sr = fma(mr, xr, fma(-mi, xi, sr));
           si = fma(mr, xi, fma(mi, xr, si));
         } else {
-          sr = fma(M[e], xv[j], sr);
+          sr = fma((double) M[e], xv[j], sr);
         }
       }
       red[W * (g * rb + rl)] = sr;
@@ -190,14 +191,18 @@ __global__ void __launch_bounds__(TPB) forward_near_kernel(MvmForwardArgs a, Mvm
 }
 
 // Launch 2: coupling blocks yt_r += S_b xt_c.
-template <bool CX>
+template <bool CX, bool SINGLE = false>
 __global__ void __launch_bounds__(TPB) coupling_mv_kernel(MvmCoupleArgs a) {
   constexpr int W = CX ? 2 : 1;
   __shared__ double red[TPB * W];
   const uint32_t b = blockIdx.x;
   const uint32_t k = (uint32_t) a.k;
-  panel_mv_atomic<CX>(a.S + (size_t) W * k * k * b, k, k, a.xt + (size_t) W * k * a.adm_cc[b],
-                      a.yt + (size_t) W * k * a.adm_rc[b], red);
+  if (SINGLE)
+    panel_mv_atomic<CX>(a.Ss + (size_t) W * k * k * b, k, k, a.xt + (size_t) W * k * a.adm_cc[b],
+                        a.yt + (size_t) W * k * a.adm_rc[b], red);
+  else
+    panel_mv_atomic<CX>(a.S + (size_t) W * k * k * b, k, k, a.xt + (size_t) W * k * a.adm_cc[b],
+                        a.yt + (size_t) W * k * a.adm_rc[b], red);
 }
 
 // Launch 3: backward transform, a CTA per row leaf walking root -> leaf:
@@ -271,7 +276,7 @@ __global__ void gather_zero_kernel(const double *__restrict__ x, const uint32_t 
 
 // Launch 1 (flat): xt_c += W_c^T x over rows [r0, r0 + nr) of c (CTAs < items; W_c^T is k x |c|,
 // ld = k), and the nearfield blocks (the other CTAs).
-template <bool CX>
+template <bool CX, bool SINGLE = false>
 __global__ void __launch_bounds__(TPB) forward_flat_near_kernel(MvmFlatArgs f, MvmCoupleArgs c) {
   constexpr int W = CX ? 2 : 1;
   __shared__ double red[TPB * W];
@@ -279,21 +284,29 @@ __global__ void __launch_bounds__(TPB) forward_flat_near_kernel(MvmFlatArgs f, M
   if (blockIdx.x >= f.nitems) {
     const uint32_t nb = blockIdx.x - f.nitems;
     const uint32_t r = c.near_rc[nb], cc = c.near_cc[nb];
-    panel_mv_atomic<CX>(c.N + (size_t) W * c.near_off[nb], c.rsize[r], c.csize[cc],
-                        c.xp + (size_t) W * c.coff[cc], c.yp + (size_t) W * c.roff[r], red);
+    if (SINGLE)
+      panel_mv_atomic<CX>(c.Ns + (size_t) W * c.near_off[nb], c.rsize[r], c.csize[cc],
+                          c.xp + (size_t) W * c.coff[cc], c.yp + (size_t) W * c.roff[r], red);
+    else
+      panel_mv_atomic<CX>(c.N + (size_t) W * c.near_off[nb], c.rsize[r], c.csize[cc],
+                          c.xp + (size_t) W * c.coff[cc], c.yp + (size_t) W * c.roff[r], red);
     return;
   }
   const uint32_t *it = f.items + 3 * (size_t) blockIdx.x;
   const uint32_t cl = it[0], r0 = it[1], nr = it[2];
   const uint32_t k = (uint32_t) f.k;
-  gemv_split<CX, false>(f.W + f.woff[cl] + (size_t) r0 * k, k, k, nr,
-                        c.xp + (size_t) W * (f.off[cl] + r0), red, tmp);
+  if (SINGLE)
+    gemv_split<CX, false>(f.Ws + f.woff[cl] + (size_t) r0 * k, k, k, nr,
+                          c.xp + (size_t) W * (f.off[cl] + r0), red, tmp);
+  else
+    gemv_split<CX, false>(f.W + f.woff[cl] + (size_t) r0 * k, k, k, nr,
+                          c.xp + (size_t) W * (f.off[cl] + r0), red, tmp);
   for (uint32_t e = threadIdx.x; e < W * k; e += blockDim.x)
     atomicAdd(const_cast<double *>(&c.xt[(size_t) W * k * cl + e]), tmp[e]);
 }
 
 // Launch 3 (flat): yp[rows r0 .. r0 + nr of c] += W_c[r0:, :] yt_c (W_c is |c| x k, ld = |c|).
-template <bool CX>
+template <bool CX, bool SINGLE = false>
 __global__ void __launch_bounds__(TPB) backward_flat_kernel(MvmFlatArgs f, const double *yt,
                                                             double *yp) {
   constexpr int W = CX ? 2 : 1;
@@ -302,13 +315,53 @@ __global__ void __launch_bounds__(TPB) backward_flat_kernel(MvmFlatArgs f, const
   const uint32_t *it = f.items + 3 * (size_t) blockIdx.x;
   const uint32_t cl = it[0], r0 = it[1], nr = it[2];
   const uint32_t k = (uint32_t) f.k;
-  gemv_split<CX, false>(f.W + f.woff[cl] + r0, f.size[cl], nr, k, yt + (size_t) W * k * cl, red,
-                        tmp);
+  if (SINGLE)
+    gemv_split<CX, false>(f.Ws + f.woff[cl] + r0, f.size[cl], nr, k, yt + (size_t) W * k * cl,
+                          red, tmp);
+  else
+    gemv_split<CX, false>(f.W + f.woff[cl] + r0, f.size[cl], nr, k, yt + (size_t) W * k * cl,
+                          red, tmp);
   double *y = yp + (size_t) W * (f.off[cl] + r0);
   for (uint32_t e = threadIdx.x; e < W * nr; e += blockDim.x) atomicAdd(&y[e], tmp[e]);
 }
 
+template <bool CX, bool SINGLE>
+int launch_flat(const MvmPlan *p, const double *x, double *y, double ar, double ai,
+                cudaStream_t st) {
+  const size_t W = CX ? 2 : 1;
+  const int sms = p->num_sms > 0 ? p->num_sms : 148;
+  const MvmCoupleArgs &ca = p->cpl;
+  const uint32_t zn = p->nrow > p->ncol ? p->nrow : p->ncol;
+  const uint32_t gz = std::min<uint32_t>((zn + 255) / 256 + 1, (uint32_t) (4 * sms));
+  const size_t nyp = W * p->nrow, nxt = W * (size_t) p->k * p->ncol_clusters,
+               nyt = W * (size_t) p->k * p->nrow_clusters;
+  gather_zero_kernel<CX><<<gz, 256, 0, st>>>(x, p->cidx, p->xp, p->ncol, p->yp, nyp, p->xt, nxt,
+                                             p->yt, nyt);
+  if (p->ffwd.nitems + ca.nnear)
+    forward_flat_near_kernel<CX, SINGLE><<<p->ffwd.nitems + ca.nnear, TPB, 0, st>>>(p->ffwd, ca);
+  if (ca.nadm) coupling_mv_kernel<CX, SINGLE><<<ca.nadm, TPB, 0, st>>>(ca);
+  if (p->fbwd.nitems)
+    backward_flat_kernel<CX, SINGLE><<<p->fbwd.nitems, TPB, 0, st>>>(p->fbwd, p->yt, p->yp);
+  scatter_kernel<CX><<<gz, 256, 0, st>>>(p->yp, p->ridx, y, p->nrow, ar, ai);
+  H2B_CUDA_TRY(cudaGetLastError());
+  return H2B_OK;
+}
+
 }  // namespace
+
+extern "C" int h2b_mvm_launch_single(const MvmPlan *p, const double *x, double *y, double ar,
+                                     double ai, cudaStream_t st) {
+  if (!p->flat || !p->cpl.Ss || !p->cpl.Ns || !p->ffwd.Ws || !p->fbwd.Ws) {
+    h2b_set_error("matvec: no FP32 copy of the H2 matrix (h2b_h2matrix_make_single)");
+    return H2B_ERR_ARG;
+  }
+  if (p->k > 128) {
+    h2b_set_error("matvec: rank %d > 128", p->k);
+    return H2B_ERR_ARG;
+  }
+  return p->cx ? launch_flat<true, true>(p, x, y, ar, ai, st)
+               : launch_flat<false, true>(p, x, y, ar, ai, st);
+}
 
 extern "C" int h2b_mvm_launch(const MvmPlan *p, const double *x, double *y, double ar, double ai,
                               cudaStream_t st) {
@@ -321,32 +374,8 @@ extern "C" int h2b_mvm_launch(const MvmPlan *p, const double *x, double *y, doub
   }
   const uint32_t gg = (p->ncol + 255) / 256 < (uint32_t) (4 * sms) ? (p->ncol + 255) / 256
                                                                    : (uint32_t) (4 * sms);
-  if (p->flat) {
-    const MvmCoupleArgs &ca = p->cpl;
-    const uint32_t zn = p->nrow > p->ncol ? p->nrow : p->ncol;
-    const uint32_t gz = std::min<uint32_t>((zn + 255) / 256 + 1, (uint32_t) (4 * sms));
-    const size_t nyp = W * p->nrow, nxt = W * (size_t) p->k * p->ncol_clusters,
-                 nyt = W * (size_t) p->k * p->nrow_clusters;
-    if (cx) {
-      gather_zero_kernel<true><<<gz, 256, 0, st>>>(x, p->cidx, p->xp, p->ncol, p->yp, nyp, p->xt,
-                                                   nxt, p->yt, nyt);
-      if (p->ffwd.nitems + ca.nnear)
-        forward_flat_near_kernel<true><<<p->ffwd.nitems + ca.nnear, TPB, 0, st>>>(p->ffwd, ca);
-      if (ca.nadm) coupling_mv_kernel<true><<<ca.nadm, TPB, 0, st>>>(ca);
-      if (p->fbwd.nitems) backward_flat_kernel<true><<<p->fbwd.nitems, TPB, 0, st>>>(p->fbwd, p->yt, p->yp);
-      scatter_kernel<true><<<gz, 256, 0, st>>>(p->yp, p->ridx, y, p->nrow, ar, ai);
-    } else {
-      gather_zero_kernel<false><<<gz, 256, 0, st>>>(x, p->cidx, p->xp, p->ncol, p->yp, nyp, p->xt,
-                                                    nxt, p->yt, nyt);
-      if (p->ffwd.nitems + ca.nnear)
-        forward_flat_near_kernel<false><<<p->ffwd.nitems + ca.nnear, TPB, 0, st>>>(p->ffwd, ca);
-      if (ca.nadm) coupling_mv_kernel<false><<<ca.nadm, TPB, 0, st>>>(ca);
-      if (p->fbwd.nitems) backward_flat_kernel<false><<<p->fbwd.nitems, TPB, 0, st>>>(p->fbwd, p->yt, p->yp);
-      scatter_kernel<false><<<gz, 256, 0, st>>>(p->yp, p->ridx, y, p->nrow, ar, ai);
-    }
-    H2B_CUDA_TRY(cudaGetLastError());
-    return H2B_OK;
-  }
+  if (p->flat) return p->cx ? launch_flat<true, false>(p, x, y, ar, ai, st)
+                            : launch_flat<false, false>(p, x, y, ar, ai, st);
   H2B_CUDA_TRY(cudaMemsetAsync(p->yp, 0, sizeof(double) * W * p->nrow, st));
   H2B_CUDA_TRY(cudaMemsetAsync(p->yt, 0, sizeof(double) * W * p->k * p->nrow_clusters, st));
   const MvmForwardArgs &fa = p->fwd;

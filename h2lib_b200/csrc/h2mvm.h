@@ -23,6 +23,7 @@ struct MvmCoupleArgs {
   const uint32_t *near_rc, *near_cc;
   const uint64_t *near_off;
   const double *N;
+  const float *Ss, *Ns;       // FP32 copies of S and N (NULL until made)
   const uint32_t *rsize, *csize, *roff, *coff;
   const double *xt, *xp;
   double *yt, *yp;
@@ -56,6 +57,7 @@ struct MvmFlatArgs {
   const uint32_t *off, *size; // per cluster
   const uint64_t *woff;       // per cluster: offset of W_t
   const double *W;            // row side |t| x k (ld |t|); column side k x |t| (ld k)
+  const float *Ws;            // FP32 copy of W (NULL until made)
   uint32_t nitems;
   int k;
 };
@@ -79,3 +81,7 @@ struct MvmPlan {
 
 extern "C" int h2b_mvm_launch(const MvmPlan *p, const double *x, double *y, double ar, double ai,
                               cudaStream_t st);
+// The same product from the FP32 copies of N, S and W (flattened path only): matrix entries are
+// read as FP32 and widened, vectors and sums stay FP64, so the product reads half the bytes.
+extern "C" int h2b_mvm_launch_single(const MvmPlan *p, const double *x, double *y, double ar,
+                                     double ai, cudaStream_t st);

@@ -55,6 +55,151 @@ h2b_tree_new(uint32_t vertices, const double *x, uint32_t triangles, const uint3
   return tr;
 }
 
+/* Append the clusters of `src` to `dst` with cluster ids shifted by dst->n, index positions by
+ * dst->nidx and index values by `ioff`. */
+static int
+ctree_append(h2b_ctree *dst, const h2b_ctree *src, uint32_t ioff)
+{
+  const uint32_t c0 = dst->n, i0 = dst->nidx, n = dst->n + src->n, ni = dst->nidx + src->nidx;
+  uint32_t i;
+#define H2B_RE(f, type, cnt)                                                   \
+  do {                                                                        \
+    type *p_ = (type *) realloc(dst->f, sizeof(type) * (size_t) (cnt));      \
+    if (!p_)                                                                  \
+      return H2B_ERR_NOMEM;                                                   \
+    dst->f = p_;                                                              \
+  } while (0)
+  H2B_RE(off, uint32_t, n); H2B_RE(size, uint32_t, n); H2B_RE(sons, uint32_t, n);
+  H2B_RE(son0, uint32_t, n); H2B_RE(son1, uint32_t, n); H2B_RE(father, uint32_t, n);
+  H2B_RE(level, uint32_t, n); H2B_RE(bmin, double, 3 * (size_t) n);
+  H2B_RE(bmax, double, 3 * (size_t) n); H2B_RE(idx, uint32_t, ni);
+#undef H2B_RE
+  for (i = 0; i < src->n; i++) {
+    dst->off[c0 + i] = src->off[i] + i0;
+    dst->size[c0 + i] = src->size[i];
+    dst->sons[c0 + i] = src->sons[i];
+    dst->son0[c0 + i] = src->son0[i] == UINT32_MAX ? UINT32_MAX : src->son0[i] + c0;
+    dst->son1[c0 + i] = src->son1[i] == UINT32_MAX ? UINT32_MAX : src->son1[i] + c0;
+    dst->father[c0 + i] = src->father[i] == UINT32_MAX ? UINT32_MAX : src->father[i] + c0;
+    dst->level[c0 + i] = src->level[i];
+  }
+  memcpy(dst->bmin + 3 * (size_t) c0, src->bmin, sizeof(double) * 3 * src->n);
+  memcpy(dst->bmax + 3 * (size_t) c0, src->bmax, sizeof(double) * 3 * src->n);
+  for (i = 0; i < src->nidx; i++)
+    dst->idx[i0 + i] = src->idx[i] + ioff;
+  dst->n = n;
+  dst->nidx = ni;
+  if (src->depth > dst->depth)
+    dst->depth = src->depth;
+  return H2B_OK;
+}
+
+h2b_tree *
+h2b_tree_new_forest(uint32_t surfaces, const uint32_t *vertex_off, const uint32_t *triangle_off,
+                    const double *x, const uint32_t *t, int row_basis, int col_basis, uint32_t clf,
+                    double eta)
+{
+  h2b_tree *tr;
+  uint32_t m, i;
+  uint32_t *tl = NULL;
+  size_t tcap = 0;
+  if (!vertex_off || !triangle_off || !x || !t || surfaces == 0) {
+    h2b_set_error("h2b_tree_new_forest: empty input");
+    return NULL;
+  }
+  if ((row_basis != H2B_BASIS_CONSTANT && row_basis != H2B_BASIS_LINEAR)
+      || (col_basis != H2B_BASIS_CONSTANT && col_basis != H2B_BASIS_LINEAR) || !(eta > 0.0)) {
+    h2b_set_error("h2b_tree_new_forest: invalid basis or eta");
+    return NULL;
+  }
+  tr = (h2b_tree *) calloc(1, sizeof(h2b_tree));
+  if (!tr) {
+    h2b_set_error("h2b_tree_new_forest: out of host memory");
+    return NULL;
+  }
+  tr->row_basis = row_basis;
+  tr->col_basis = col_basis;
+  for (m = 0; m < surfaces; m++) {
+    const uint32_t v0 = vertex_off[m], nv = vertex_off[m + 1] - vertex_off[m];
+    const uint32_t t0 = triangle_off[m], nt = triangle_off[m + 1] - triangle_off[m];
+    h2b_tree one;
+    const uint32_t rc0 = tr->row.n, cc0 = tr->col.n, b0 = tr->blocks.n;
+    int rc;
+    if (vertex_off[m + 1] < vertex_off[m] || triangle_off[m + 1] < triangle_off[m] || nv == 0
+        || nt == 0) {
+      h2b_set_error("h2b_tree_new_forest: surface %u is empty or its offsets decrease", m);
+      free(tl);
+      h2b_tree_del(tr);
+      return NULL;
+    }
+    /* the surface's triangles with local vertex ids */
+    if (3 * (size_t) nt > tcap) {
+      uint32_t *p = (uint32_t *) realloc(tl, sizeof(uint32_t) * 3 * (size_t) nt);
+      if (!p) {
+        free(tl);
+        h2b_tree_del(tr);
+        h2b_set_error("h2b_tree_new_forest: out of host memory");
+        return NULL;
+      }
+      tl = p;
+      tcap = 3 * (size_t) nt;
+    }
+    for (i = 0; i < 3 * nt; i++) {
+      const uint32_t v = t[3 * (size_t) t0 + i];
+      if (v < v0 || v >= v0 + nv) {
+        free(tl);
+        h2b_tree_del(tr);
+        h2b_set_error("h2b_tree_new_forest: triangle %u of surface %u has a vertex outside it",
+                      t0 + i / 3, m);
+        return NULL;
+      }
+      tl[i] = v - v0;
+    }
+    memset(&one, 0, sizeof(one));
+    rc = h2b_ctree_build(nv, x + 3 * (size_t) v0, nt, tl, row_basis, clf, &one.row);
+    if (rc == H2B_OK)
+      rc = h2b_ctree_build(nv, x + 3 * (size_t) v0, nt, tl, col_basis, clf, &one.col);
+    if (rc == H2B_OK)
+      rc = h2b_blist_build(&one.row, &one.col, eta, &one.blocks);
+    if (rc == H2B_OK)
+      rc = ctree_append(&tr->row, &one.row, row_basis == H2B_BASIS_LINEAR ? v0 : t0);
+    if (rc == H2B_OK)
+      rc = ctree_append(&tr->col, &one.col, col_basis == H2B_BASIS_LINEAR ? v0 : t0);
+    if (rc == H2B_OK) {
+      const uint32_t nb = b0 + one.blocks.n;
+      uint32_t *prc = (uint32_t *) realloc(tr->blocks.rc, sizeof(uint32_t) * nb);
+      uint32_t *pcc = prc ? (uint32_t *) realloc(tr->blocks.cc, sizeof(uint32_t) * nb) : NULL;
+      uint8_t *padm = pcc ? (uint8_t *) realloc(tr->blocks.adm, nb) : NULL;
+      if (prc) tr->blocks.rc = prc;
+      if (pcc) tr->blocks.cc = pcc;
+      if (padm) tr->blocks.adm = padm;
+      if (!prc || !pcc || !padm)
+        rc = H2B_ERR_NOMEM;
+      else {
+        for (i = 0; i < one.blocks.n; i++) {
+          tr->blocks.rc[b0 + i] = one.blocks.rc[i] + rc0;
+          tr->blocks.cc[b0 + i] = one.blocks.cc[i] + cc0;
+          tr->blocks.adm[b0 + i] = one.blocks.adm[i];
+        }
+        tr->blocks.n = nb;
+      }
+    }
+    h2b_ctree_free(&one.row);
+    h2b_ctree_free(&one.col);
+    h2b_blist_free(&one.blocks);
+    if (rc != H2B_OK) {
+      free(tl);
+      h2b_tree_del(tr);
+      if (rc == H2B_ERR_NOMEM)
+        h2b_set_error("h2b_tree_new_forest: out of host memory");
+      return NULL;
+    }
+  }
+  free(tl);
+  finish_tree(tr);
+  return tr;
+}
+
 /* Rebuild son/father/level links of a pre-order tree given only (off, size, sons). */
 static int
 link_tree(h2b_ctree *t)

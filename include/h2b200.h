@@ -129,6 +129,15 @@ h2b_tree *h2b_tree_new_flat(uint32_t row_clusters, const uint32_t *row_off,
                             uint32_t blocks, const uint32_t *block_rc,
                             const uint32_t *block_cc, const uint8_t *block_adm);
 
+/* A forest of independent surfaces: surface m owns vertices [vertex_off[m], vertex_off[m+1]) and
+ * triangles [triangle_off[m], triangle_off[m+1]) of x / t (t holds global vertex ids).  Each
+ * surface gets its own cluster trees and block tree (as h2b_tree_new on that surface alone);
+ * the forest concatenates them, so an H2 matrix on it is block diagonal: one assembly and one
+ * matvec serve all surfaces.  No H2Lib counterpart (H2Lib builds one tree per surface). */
+h2b_tree *h2b_tree_new_forest(uint32_t surfaces, const uint32_t *vertex_off,
+                              const uint32_t *triangle_off, const double *x, const uint32_t *t,
+                              int row_basis, int col_basis, uint32_t clf, double eta);
+
 void h2b_tree_del(h2b_tree *tree);
 
 /* Counts: clusters of the row/column tree, index-set sizes, leaf blocks, admissible blocks,
@@ -210,6 +219,16 @@ int h2b_h2matrix_assemble_nearfield_pair(h2b_h2matrix *a, h2b_h2matrix *b);
  * [7] rank k. */
 int h2b_h2matrix_info(const h2b_h2matrix *h2, uint64_t info[8]);
 
+/* FP32 copies of the nearfield blocks, coupling matrices and flattened cluster bases, read by the
+ * mixed-precision matvec (half the bytes of the FP64 product).  Call after assembly; any later
+ * assembly call drops the copies.  No counterpart in the reference (FP64 only). */
+int h2b_h2matrix_make_single(h2b_h2matrix *h2);
+
+/* y += alpha A x read from the FP32 copies (FP64 vectors and sums); same arguments as
+ * h2b_h2matrix_addeval.  Needs h2b_h2matrix_make_single. */
+int h2b_h2matrix_addeval_single(double alpha_re, double alpha_im, const h2b_h2matrix *h2,
+                                const double *x, double *y);
+
 /* Device time (ms, CUDA events on the matrix's stream) of the last run of each phase:
  * [0] row basis, [1] column basis, [2] coupling, [3] nearfield distant pairs, [4] nearfield
  * singular pairs, [5] last matvec.  No reference counterpart (diagnostics). */
@@ -256,6 +275,31 @@ int h2b_h2matrix_addeval_multi(double alpha_re, double alpha_im, const h2b_h2mat
 int h2b_solve_gmres(uint32_t nterms, const h2b_h2matrix *const *ops, const double *coef,
                     const double *b, double *x, double eps, uint32_t maxiter, uint32_t kmax);
 
+/* Many independent systems at once: the operator must be block diagonal with diagonal blocks on
+ * the row ranges [system_off[s], system_off[s+1]) (an H2 matrix on a forest, h2b_tree_new_forest;
+ * system_off[0] = 0, system_off[systems] = the operator size).  Each system runs the GMRES of
+ * h2b_solve_gmres on its own rows — own Krylov basis, residual estimate, restarts and stop at
+ * eps * ||b_s|| or maxiter — while one operator application per step serves all of them.
+ * iterations[s] (may be NULL) receives each system's step count.  No counterpart in the
+ * reference, which solves one system per solve_gmres_avector call. */
+#define H2B_SOLVE_MIXED 1u
+int h2b_solve_gmres_batch(uint32_t nterms, const h2b_h2matrix *const *ops, const double *coef,
+                          uint32_t systems, const uint32_t *system_off, uint32_t nrhs,
+                          const double *b, double *x, double eps, uint32_t maxiter, uint32_t kmax,
+                          uint32_t flags, uint32_t *iterations);
+/* With nrhs > 1, b and x hold nrhs columns of the operator size (column r at r * size) and
+ * system (s, r) is segment s of column r; iterations has systems * nrhs entries (s + r * systems).
+ * flags: H2B_SOLVE_MIXED runs the Arnoldi steps on the FP32 copies of the matrices
+ * (h2b_h2matrix_make_single) and keeps residuals in FP64: every (re)start computes the FP64
+ * residual b - A x, and a system whose residual estimate reaches eps * ||b|| restarts once more
+ * to confirm it with the FP64 residual, so the returned x meets eps in FP64 — restarted GMRES
+ * as iterative refinement with a single-precision inner operator. */
+
+/* h2b_solve_gmres with the mixed-precision iteration of H2B_SOLVE_MIXED (one system). */
+int h2b_solve_gmres_mixed(uint32_t nterms, const h2b_h2matrix *const *ops, const double *coef,
+                          const double *b, double *x, double eps, uint32_t maxiter,
+                          uint32_t kmax);
+
 /* GMRES that allocates nothing.  No counterpart in the reference (H2Lib allocates its Krylov work
  * space with new_avector / new_amatrix in solve_gmres_avector).  For callers that cannot allocate
  * device memory during a solve — a device-memory budget fixed at start-up, an allocator owned by
@@ -294,6 +338,17 @@ int h2b_project_l2_harmonic(const h2b_bem *bem, const double z[3], double *w);
  * itself (normL2_bem3d, :8704). */
 int h2b_l2_error_harmonic(const h2b_bem *bem, const double z[3], const double *u, double *err,
                           double *norm);
+
+/* The same for an operator on a union of surfaces (triangle ranges triangle_off[s] ..
+ * triangle_off[s+1], triangle_off[surfaces] = all triangles) and nrhs columns: the source of
+ * surface s in column r is zs[3 (s + r surfaces)]; w and u hold nrhs columns of the vertex count;
+ * err / norm receive surfaces * nrhs values (s + r surfaces). */
+int h2b_project_l2_harmonic_multi(const h2b_bem *bem, uint32_t surfaces,
+                                  const uint32_t *triangle_off, uint32_t nrhs, const double *zs,
+                                  double *w);
+int h2b_l2_error_harmonic_multi(const h2b_bem *bem, uint32_t surfaces,
+                                const uint32_t *triangle_off, uint32_t nrhs, const double *zs,
+                                const double *u, double *err, double *norm);
 
 /* b[t] = coef * int_{triangle t} exp(i kvec . (x - src)) dx for the constant basis (a plane wave
  * as Dirichlet datum).  Replaces integrate_bem3d_c_avector (Library/bem3d.c:8579) with
