@@ -5,6 +5,8 @@
 #include <stdlib.h>
 #include <string.h>
 
+#include <atomic>
+#include <mutex>
 #include <vector>
 
 #include "api_internal.h"
@@ -26,7 +28,10 @@ extern "C" const char *h2b_last_error(void) { return g_err; }
 
 extern "C" const char *h2b_version(void) { return "h2b200 0.1 (sm_100a)"; }
 
-static int g_inited_device = -1;
+// Device whose constant tables are loaded; written under g_init_mutex (handles may be created
+// from several host threads, e.g. the workers of a solve server).
+static std::atomic<int> g_inited_device{-1};
+static std::mutex g_init_mutex;
 
 extern "C" int h2b_device_init(int device) {
   int n = 0;
@@ -47,9 +52,17 @@ extern "C" int h2b_device_init(int device) {
                   prop.major, prop.minor);
     return H2B_ERR_CUDA;
   }
+  std::lock_guard<std::mutex> lock(g_init_mutex);
   if (g_inited_device != device) {
     int rc = h2b_near_upload_dist_rules();
     if (rc != H2B_OK) return rc;
+    // keep freed stream-ordered memory in the device pool for reuse by later handles
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+      uint64_t keep = UINT64_MAX;
+      cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    }
+    cudaGetLastError();
     g_inited_device = device;
   }
   return H2B_OK;
@@ -123,12 +136,13 @@ extern "C" h2b_surface *h2b_surface_new(uint32_t vertices, const double *x, uint
   cudaDeviceProp prop;
   if (cudaGetDevice(&dev) != cudaSuccess || cudaGetDeviceProperties(&prop, dev) != cudaSuccess ||
       cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) != cudaSuccess ||
-      cudaMalloc(&s->d_tri, sizeof(TriRec) * triangles) != cudaSuccess ||
-      cudaMalloc(&s->d_x, sizeof(double) * 3ull * vertices) != cudaSuccess ||
-      cudaMemcpy(s->d_tri, rec.data(), sizeof(TriRec) * triangles, cudaMemcpyHostToDevice) !=
-          cudaSuccess ||
-      cudaMemcpy(s->d_x, x, sizeof(double) * 3ull * vertices, cudaMemcpyHostToDevice) !=
-          cudaSuccess) {
+      cudaMallocAsync(&s->d_tri, sizeof(TriRec) * triangles, s->stream) != cudaSuccess ||
+      cudaMallocAsync(&s->d_x, sizeof(double) * 3ull * vertices, s->stream) != cudaSuccess ||
+      cudaMemcpyAsync(s->d_tri, rec.data(), sizeof(TriRec) * triangles, cudaMemcpyHostToDevice,
+                      s->stream) != cudaSuccess ||
+      cudaMemcpyAsync(s->d_x, x, sizeof(double) * 3ull * vertices, cudaMemcpyHostToDevice,
+                      s->stream) != cudaSuccess ||
+      cudaStreamSynchronize(s->stream) != cudaSuccess) {
     h2b_set_error("h2b_surface_new: %s", cudaGetErrorString(cudaGetLastError()));
     h2b_surface_del(s);
     return NULL;
@@ -140,8 +154,10 @@ extern "C" h2b_surface *h2b_surface_new(uint32_t vertices, const double *x, uint
 
 extern "C" void h2b_surface_del(h2b_surface *s) {
   if (!s) return;
-  if (s->d_tri) cudaFree(s->d_tri);
-  if (s->d_x) cudaFree(s->d_x);
+  // every entry point ends synchronised, so no kernel still reads these arrays; stream-ordered
+  // frees do not synchronise the device (other handles keep running)
+  if (s->d_tri) cudaFreeAsync(s->d_tri, s->stream);
+  if (s->d_x) cudaFreeAsync(s->d_x, s->stream);
   if (s->stream) cudaStreamDestroy(s->stream);
   h2b_adjacency_free(&s->adj);
   delete s;
@@ -215,11 +231,13 @@ extern "C" h2b_bem *h2b_bem_new(const h2b_surface *s, int pde, int layer, int ro
   }
   // every field must start on a 16-byte boundary: n is a multiple of 2 (2 q2^4 and 6 q2^4)
   b->rule_total = (uint32_t) pack.size();
-  if (cudaMalloc(&b->d_rule, sizeof(double) * pack.size()) != cudaSuccess ||
-      cudaMemcpy(b->d_rule, pack.data(), sizeof(double) * pack.size(), cudaMemcpyHostToDevice) !=
-          cudaSuccess ||
-      cudaMalloc(&b->d_err, sizeof(int)) != cudaSuccess ||
-      cudaMemset(b->d_err, 0, sizeof(int)) != cudaSuccess) {
+  cudaStream_t st = b->s->stream;
+  if (cudaMallocAsync(&b->d_rule, sizeof(double) * pack.size(), st) != cudaSuccess ||
+      cudaMemcpyAsync(b->d_rule, pack.data(), sizeof(double) * pack.size(),
+                      cudaMemcpyHostToDevice, st) != cudaSuccess ||
+      cudaMallocAsync(&b->d_err, sizeof(int), st) != cudaSuccess ||
+      cudaMemsetAsync(b->d_err, 0, sizeof(int), st) != cudaSuccess ||
+      cudaStreamSynchronize(st) != cudaSuccess) {
     h2b_set_error("h2b_bem_new: %s", cudaGetErrorString(cudaGetLastError()));
     h2b_bem_del(b);
     return NULL;
@@ -229,8 +247,9 @@ extern "C" h2b_bem *h2b_bem_new(const h2b_surface *s, int pde, int layer, int ro
 
 extern "C" void h2b_bem_del(h2b_bem *b) {
   if (!b) return;
-  if (b->d_rule) cudaFree(b->d_rule);
-  if (b->d_err) cudaFree(b->d_err);
+  // the operator must be deleted before its surface (the frees are ordered on its stream)
+  if (b->d_rule) cudaFreeAsync(b->d_rule, b->s->stream);
+  if (b->d_err) cudaFreeAsync(b->d_err, b->s->stream);
   h2b_quad_free(&b->quad);
   delete b;
 }

@@ -17,15 +17,18 @@ template <typename T>
 static int upload(T **dst, const std::vector<T> &src, cudaStream_t st) {
   *dst = nullptr;
   if (src.empty()) return H2B_OK;
-  H2B_CUDA_TRY(cudaMalloc((void **) dst, sizeof(T) * src.size()));
+  H2B_CUDA_TRY(cudaMallocAsync((void **) dst, sizeof(T) * src.size(), st));
   H2B_CUDA_TRY(cudaMemcpyAsync(*dst, src.data(), sizeof(T) * src.size(), cudaMemcpyHostToDevice,
                                st));
   return H2B_OK;
 }
 
+// Device memory of the H2 structures is stream-ordered (cudaMallocAsync / cudaFreeAsync on the
+// matrix's stream, served from the device's memory pool): creating and releasing matrices never
+// synchronises the device, so matrices of concurrent requests do not stall each other.
 template <typename T>
-static void dfree(T *&p) {
-  if (p) cudaFree((void *) p);
+static void dfree(T *&p, cudaStream_t st) {
+  if (p) cudaFreeAsync((void *) p, st);
   p = nullptr;
 }
 
@@ -45,12 +48,12 @@ static void box_points(const double *bmin, const double *bmax, uint32_t m, doubl
   }
 }
 
-static void devtree_free(DevCTree &t) {
-  dfree(t.d_off); dfree(t.d_size); dfree(t.d_father); dfree(t.d_son0); dfree(t.d_son1);
-  dfree(t.d_idx); dfree(t.d_leaves); dfree(t.d_nonroot); dfree(t.d_levels); dfree(t.d_voff);
-  dfree(t.d_pts); dfree(t.d_V); dfree(t.d_E); dfree(t.d_counter); dfree(t.d_refs);
-  dfree(t.d_tr_off); dfree(t.d_tr_len);
-  dfree(t.d_W); dfree(t.d_woff); dfree(t.d_fitems); dfree(t.d_wleaves); dfree(t.d_mitems);
+static void devtree_free(DevCTree &t, cudaStream_t st) {
+  dfree(t.d_off, st); dfree(t.d_size, st); dfree(t.d_father, st); dfree(t.d_son0, st); dfree(t.d_son1, st);
+  dfree(t.d_idx, st); dfree(t.d_leaves, st); dfree(t.d_nonroot, st); dfree(t.d_levels, st); dfree(t.d_voff, st);
+  dfree(t.d_pts, st); dfree(t.d_V, st); dfree(t.d_E, st); dfree(t.d_counter, st); dfree(t.d_refs, st);
+  dfree(t.d_tr_off, st); dfree(t.d_tr_len, st);
+  dfree(t.d_W, st); dfree(t.d_woff, st); dfree(t.d_fitems, st); dfree(t.d_wleaves, st); dfree(t.d_mitems, st);
 }
 
 // Flattened bases: W_t for the clusters of admissible blocks (`adm`, ids of this tree) and all
@@ -102,7 +105,7 @@ static int devtree_flat_setup(DevCTree &t, const h2b_ctree &c, const std::vector
   if ((rc = upload(&t.d_woff, woff, st)) || (rc = upload(&t.d_wleaves, wleaves, st)) ||
       (rc = upload(&t.d_fitems, fitems, st)) || (rc = upload(&t.d_mitems, mitems, st)))
     return rc;
-  H2B_CUDA_TRY(cudaMalloc(&t.d_W, sizeof(double) * std::max<uint64_t>(tot, 1)));
+  H2B_CUDA_TRY(cudaMallocAsync(&t.d_W, sizeof(double) * std::max<uint64_t>(tot, 1), st));
   return H2B_OK;
 }
 
@@ -181,9 +184,9 @@ static int devtree_build(DevCTree &t, const h2b_ctree &c, int basis, uint32_t m,
       (rc = upload(&t.d_pts, pts, st)) || (rc = upload(&t.d_refs, refs, st)) ||
       (rc = upload(&t.d_tr_off, tr_off, st)) || (rc = upload(&t.d_tr_len, tr_len, st)))
     return rc;
-  H2B_CUDA_TRY(cudaMalloc(&t.d_V, sizeof(double) * std::max<uint64_t>(vtot, 1)));
-  H2B_CUDA_TRY(cudaMalloc(&t.d_E, sizeof(double) * std::max<uint64_t>((uint64_t) (c.n - 1) * k * k, 1)));
-  H2B_CUDA_TRY(cudaMalloc(&t.d_counter, sizeof(unsigned) * c.n));
+  H2B_CUDA_TRY(cudaMallocAsync(&t.d_V, sizeof(double) * std::max<uint64_t>(vtot, 1), st));
+  H2B_CUDA_TRY(cudaMallocAsync(&t.d_E, sizeof(double) * std::max<uint64_t>((uint64_t) (c.n - 1) * k * k, 1), st));
+  H2B_CUDA_TRY(cudaMallocAsync(&t.d_counter, sizeof(unsigned) * c.n, st));
   H2B_CUDA_TRY(cudaMemsetAsync(t.d_counter, 0, sizeof(unsigned) * c.n, st));
   return H2B_OK;
 }
@@ -194,16 +197,17 @@ static int devtree_build(DevCTree &t, const h2b_ctree &c, int basis, uint32_t m,
 
 extern "C" void h2b_h2matrix_del(h2b_h2matrix *h) {
   if (!h) return;
-  if (h->st) cudaStreamSynchronize(h->st);
-  devtree_free(h->rt);
-  devtree_free(h->ct);
-  dfree(h->rt.f_W); dfree(h->ct.f_W); dfree(h->f_N); dfree(h->f_S);
-  dfree(h->d_adm_rc); dfree(h->d_adm_cc); dfree(h->d_S);
-  dfree(h->d_near_rc); dfree(h->d_near_cc); dfree(h->d_near_off); dfree(h->d_N);
-  dfree(h->d_tiles); dfree(h->d_refs); dfree(h->d_sing);
-  dfree(h->d_xp); dfree(h->d_yp); dfree(h->d_xt); dfree(h->d_yt);
-  dfree(h->d_xs); dfree(h->d_ys); dfree(h->d_ws); dfree(h->d_wsl);
-  dfree(h->d_xio); dfree(h->d_yio);
+  cudaStream_t st = h->st;
+  if (st) cudaStreamSynchronize(st);
+  devtree_free(h->rt, st);
+  devtree_free(h->ct, st);
+  dfree(h->rt.f_W, st); dfree(h->ct.f_W, st); dfree(h->f_N, st); dfree(h->f_S, st);
+  dfree(h->d_adm_rc, st); dfree(h->d_adm_cc, st); dfree(h->d_S, st);
+  dfree(h->d_near_rc, st); dfree(h->d_near_cc, st); dfree(h->d_near_off, st); dfree(h->d_N, st);
+  dfree(h->d_tiles, st); dfree(h->d_refs, st); dfree(h->d_sing, st);
+  dfree(h->d_xp, st); dfree(h->d_yp, st); dfree(h->d_xt, st); dfree(h->d_yt, st);
+  dfree(h->d_xs, st); dfree(h->d_ys, st); dfree(h->d_ws, st); dfree(h->d_wsl, st);
+  dfree(h->d_xio, st); dfree(h->d_yio, st);
   for (int e = 0; e < 12; e++)
     if (h->ev[e]) cudaEventDestroy(h->ev[e]);
   if (h->st) cudaStreamDestroy(h->st);
@@ -214,7 +218,7 @@ extern "C" void h2b_h2matrix_del(h2b_h2matrix *h) {
 // grouped by Sauter-Schwab case: vertex, edge, identical), and the pair counts per case.
 static int classify_singular(h2b_h2matrix *h, uint64_t all_pairs) {
   uint32_t *d_cur = nullptr;
-  H2B_CUDA_TRY(cudaMalloc(&d_cur, sizeof(uint32_t) * 8));
+  H2B_CUDA_TRY(cudaMallocAsync(&d_cur, sizeof(uint32_t) * 8, h->st));
   int rc = H2B_OK;
   uint32_t cnt[8] = {0, 0, 0, 0, 0, 0, 0, 0};
   if (cudaMemsetAsync(d_cur, 0, sizeof(uint32_t) * 8, h->st) != cudaSuccess) rc = H2B_ERR_CUDA;
@@ -236,7 +240,7 @@ static int classify_singular(h2b_h2matrix *h, uint64_t all_pairs) {
     h->nsing = (uint32_t) nsing;
     for (int c = 1; c <= 3; c++) h->pairs[c] = cnt[c];
     h->pairs[0] = all_pairs - nsing;
-    if (cudaMalloc(&h->d_sing, sizeof(h2b_sing) * std::max<uint64_t>(nsing, 1)) != cudaSuccess ||
+    if (cudaMallocAsync(&h->d_sing, sizeof(h2b_sing) * std::max<uint64_t>(nsing, 1), h->st) != cudaSuccess ||
         cudaMemsetAsync(d_cur, 0, sizeof(uint32_t) * 4, h->st) != cudaSuccess ||
         cudaMemcpyAsync(d_cur + 4, cnt + 4, sizeof(uint32_t) * 4, cudaMemcpyHostToDevice, h->st) !=
             cudaSuccess)
@@ -249,7 +253,7 @@ static int classify_singular(h2b_h2matrix *h, uint64_t all_pairs) {
   if (rc == H2B_ERR_CUDA)
     h2b_set_error("h2matrix singular-pair classification: %s",
                   cudaGetErrorString(cudaGetLastError()));
-  cudaFree(d_cur);
+  cudaFreeAsync(d_cur, h->st);
   return rc;
 }
 
@@ -331,14 +335,14 @@ extern "C" h2b_h2matrix *h2b_h2matrix_new(const h2b_bem *bem, const h2b_tree *tr
         (rc = upload(&h->d_near_off, noff, h->st)) || (rc = upload(&h->d_tiles, tiles, h->st)) ||
         (rc = upload(&h->d_refs, refs, h->st)) ||
         (rc = classify_singular(h, all_pairs))) {
-    } else if (cudaMalloc(&h->d_S, sizeof(double) * W * std::max<uint64_t>((uint64_t) h->nadm * h->k * h->k, 1)) != cudaSuccess ||
-               cudaMalloc(&h->d_N, sizeof(double) * W * std::max<uint64_t>(ntot, 1)) != cudaSuccess ||
-               cudaMalloc(&h->d_xp, sizeof(double) * W * nc) != cudaSuccess ||
-               cudaMalloc(&h->d_yp, sizeof(double) * W * nr) != cudaSuccess ||
-               cudaMalloc(&h->d_xt, sizeof(double) * W * h->k * tree->col.n) != cudaSuccess ||
-               cudaMalloc(&h->d_yt, sizeof(double) * W * h->k * tree->row.n) != cudaSuccess ||
-               cudaMalloc(&h->d_xio, sizeof(double) * W * nc) != cudaSuccess ||
-               cudaMalloc(&h->d_yio, sizeof(double) * W * nr) != cudaSuccess) {
+    } else if (cudaMallocAsync(&h->d_S, sizeof(double) * W * std::max<uint64_t>((uint64_t) h->nadm * h->k * h->k, 1), h->st) != cudaSuccess ||
+               cudaMallocAsync(&h->d_N, sizeof(double) * W * std::max<uint64_t>(ntot, 1), h->st) != cudaSuccess ||
+               cudaMallocAsync(&h->d_xp, sizeof(double) * W * nc, h->st) != cudaSuccess ||
+               cudaMallocAsync(&h->d_yp, sizeof(double) * W * nr, h->st) != cudaSuccess ||
+               cudaMallocAsync(&h->d_xt, sizeof(double) * W * h->k * tree->col.n, h->st) != cudaSuccess ||
+               cudaMallocAsync(&h->d_yt, sizeof(double) * W * h->k * tree->row.n, h->st) != cudaSuccess ||
+               cudaMallocAsync(&h->d_xio, sizeof(double) * W * nc, h->st) != cudaSuccess ||
+               cudaMallocAsync(&h->d_yio, sizeof(double) * W * nr, h->st) != cudaSuccess) {
       h2b_set_error("h2b_h2matrix_new: device allocation failed: %s",
                     cudaGetErrorString(cudaGetLastError()));
       rc = H2B_ERR_NOMEM;
@@ -478,11 +482,11 @@ static void mark(h2b_h2matrix *h, int e) { cudaEventRecord(h->ev[e], h->st); }
 // Free the FP32 copies (they no longer match the matrix once any part is reassembled).
 static void drop_single(h2b_h2matrix *h) {
   if (!h->f_N && !h->f_S && !h->rt.f_W && !h->ct.f_W) return;
-  cudaStreamSynchronize(h->st);
-  dfree(h->f_N);
-  dfree(h->f_S);
-  dfree(h->rt.f_W);
-  dfree(h->ct.f_W);
+  cudaStream_t st = h->st;
+  dfree(h->f_N, st);
+  dfree(h->f_S, st);
+  dfree(h->rt.f_W, st);
+  dfree(h->ct.f_W, st);
   h2b_h2_fill_mvm_plan(h);
 }
 
@@ -495,10 +499,10 @@ extern "C" int h2b_h2matrix_make_single(h2b_h2matrix *h) {
   drop_single(h);
   const uint64_t W = h->cx ? 2 : 1;
   const uint64_t nN = W * h->near_total, nS = W * (uint64_t) h->nadm * h->k * h->k;
-  if (cudaMalloc(&h->f_N, sizeof(float) * std::max<uint64_t>(nN, 1)) != cudaSuccess ||
-      cudaMalloc(&h->f_S, sizeof(float) * std::max<uint64_t>(nS, 1)) != cudaSuccess ||
-      cudaMalloc(&h->rt.f_W, sizeof(float) * std::max<uint64_t>(h->rt.wtotal, 1)) != cudaSuccess ||
-      cudaMalloc(&h->ct.f_W, sizeof(float) * std::max<uint64_t>(h->ct.wtotal, 1)) != cudaSuccess) {
+  if (cudaMallocAsync(&h->f_N, sizeof(float) * std::max<uint64_t>(nN, 1), h->st) != cudaSuccess ||
+      cudaMallocAsync(&h->f_S, sizeof(float) * std::max<uint64_t>(nS, 1), h->st) != cudaSuccess ||
+      cudaMallocAsync(&h->rt.f_W, sizeof(float) * std::max<uint64_t>(h->rt.wtotal, 1), h->st) != cudaSuccess ||
+      cudaMallocAsync(&h->ct.f_W, sizeof(float) * std::max<uint64_t>(h->ct.wtotal, 1), h->st) != cudaSuccess) {
     cudaGetLastError();
     drop_single(h);
     h2b_set_error("h2b_h2matrix_make_single: device allocation failed");

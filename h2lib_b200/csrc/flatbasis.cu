@@ -20,6 +20,26 @@ namespace {
 
 constexpr int FLAT_TPB = 256;
 
+// dst[e] = src(e) for e < n by the whole CTA, eight loads in flight per thread before the
+// stores (a plain strided loop issues one global load per iteration and waits on each).
+template <typename F>
+__device__ __forceinline__ void cta_copy(double *dst, size_t n, F src) {
+  constexpr int U = 8;
+  for (size_t e0 = threadIdx.x; e0 < n; e0 += (size_t) blockDim.x * U) {
+    double v[U];
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+      const size_t e = e0 + (size_t) u * blockDim.x;
+      v[u] = e < n ? src(e) : 0.0;
+    }
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+      const size_t e = e0 + (size_t) u * blockDim.x;
+      if (e < n) dst[e] = v[u];
+    }
+  }
+}
+
 // One CTA per item (father f, son s, first row r0 of s, rows nr <= FLAT_ROWS): the nr rows of
 // W_s times E_s land in the rows of s inside W_f.
 __global__ void __launch_bounds__(FLAT_TPB) flatten_kernel(FlatArgs a) {
@@ -30,7 +50,7 @@ __global__ void __launch_bounds__(FLAT_TPB) flatten_kernel(FlatArgs a) {
   double *sE = sm;             // k x k
   double *sW = sm + k * k;     // nr rows of W_s (layout of the side)
   const double *E = a.E + (size_t) (s - 1) * k * k;
-  for (uint32_t e = threadIdx.x; e < k * k; e += blockDim.x) sE[e] = E[e];
+  cta_copy(sE, (size_t) k * k, [&](size_t e) { return E[e]; });
   const uint32_t ns = a.size[s], nf = a.size[f];
   const uint32_t rf = a.off[s] - a.off[f] + r0;  // first row inside f
   const double *Ws = a.W + a.woff[s];
@@ -40,10 +60,10 @@ __global__ void __launch_bounds__(FLAT_TPB) flatten_kernel(FlatArgs a) {
   const uint32_t tr = threadIdx.x % 16, tc = threadIdx.x / 16;
   if (!a.transposed) {
     // sW[i + mu nr] = W_s[r0 + i, mu]
-    for (uint32_t e = threadIdx.x; e < nr * k; e += blockDim.x) {
-      const uint32_t i = e % nr, mu = e / nr;
-      sW[e] = Ws[r0 + i + (size_t) mu * ns];
-    }
+    cta_copy(sW, (size_t) nr * k, [&](size_t e) {
+      const uint32_t i = (uint32_t) (e % nr), mu = (uint32_t) (e / nr);
+      return Ws[r0 + i + (size_t) mu * ns];
+    });
     __syncthreads();
     // W_f[rf + i, nu] = sum_mu W_s[r0 + i, mu] E_s[mu, nu]   (E_s column-major k x k)
     for (uint32_t c0 = 0; c0 < k; c0 += 64) {
@@ -76,7 +96,7 @@ __global__ void __launch_bounds__(FLAT_TPB) flatten_kernel(FlatArgs a) {
     }
   } else {
     // sW[mu + i k] = W_s^T[mu, r0 + i]
-    for (uint32_t e = threadIdx.x; e < nr * k; e += blockDim.x) sW[e] = Ws[(size_t) r0 * k + e];
+    cta_copy(sW, (size_t) nr * k, [&](size_t e) { return Ws[(size_t) r0 * k + e]; });
     __syncthreads();
     // W_f^T[nu, rf + i] = sum_mu E_s^T[nu, mu] W_s^T[mu, r0 + i]   (E_s^T column-major k x k)
     for (uint32_t c0 = 0; c0 < k; c0 += 64) {
@@ -116,7 +136,7 @@ __global__ void __launch_bounds__(FLAT_TPB) leaf_copy_kernel(FlatLeafArgs a) {
   const size_t n = (size_t) a.size[l] * a.k;
   const double *src = a.V + a.voff[l];
   double *dst = a.W + a.woff[l];
-  for (size_t e = threadIdx.x; e < n; e += blockDim.x) dst[e] = src[e];
+  cta_copy(dst, n, [&](size_t e) { return src[e]; });
 }
 
 // out[i] = (float) in[i] (round to nearest)

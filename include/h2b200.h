@@ -357,6 +357,50 @@ int h2b_l2_error_harmonic_multi(const h2b_bem *bem, uint32_t surfaces,
 int h2b_integrate_plane_wave(const h2b_bem *bem, const double kvec[3], const double src[3],
                              double coef_re, double coef_im, double *b);
 
+/* ------------------------------------------------------------------------------------------
+ * Solve server: continuous admission of Dirichlet solves (no counterpart in the reference,
+ * which solves one problem per program run)
+ * ------------------------------------------------------------------------------------------ */
+
+typedef struct h2b_server h2b_server;
+
+/* One request.  pde = H2B_LAPLACE: interior Dirichlet problem of 1/|x - src| (src outside the
+ * surface), V du/dn = (K + M/2) g_D with the linear basis (m = 4); the solution has `vertices`
+ * entries.  pde = H2B_HELMHOLTZ: Brakhage-Werner ((K + M/2) - i k V) u = -int exp(i k src.x)
+ * for the plane wave of unit direction src and wavenumber k, constant basis (m = 5); the solution
+ * has `triangles` complex (interleaved) entries.  Both use q = 2/4, leaf size 64, eta = 1.4 and
+ * GMRES(kmax) to eps (flags: H2B_SOLVE_MIXED for FP32 Arnoldi steps with FP64 residuals). */
+typedef struct {
+  uint32_t vertices, triangles;
+  const double *x;
+  const uint32_t *t;
+  int pde;
+  double k;
+  double src[3];
+  double eps;
+  uint32_t maxiter, kmax, flags;
+} h2b_request;
+
+typedef struct {
+  int status;                /* H2B_OK or the error of the request */
+  uint32_t iterations, unknowns;
+  double rel_residual;       /* FP64 ||b - A u|| / ||b|| after the solve */
+  double t_submit, t_start, t_done;  /* seconds since the server started */
+  uint64_t bytes_reserved;   /* device-memory estimate charged against the budget */
+} h2b_request_result;
+
+/* A server with `slots` worker threads on `device` admitting requests while their estimated
+ * device memory fits hbm_budget_bytes.  Requests run concurrently on their own streams. */
+h2b_server *h2b_server_new(int device, uint32_t slots, uint64_t hbm_budget_bytes);
+/* Queue a request (the mesh is copied); returns its id (> 0) or a negative error. */
+int64_t h2b_server_submit(h2b_server *server, const h2b_request *request);
+/* Block until request `id` is done; copy its solution (may be NULL) and result, then forget it. */
+int h2b_server_wait(h2b_server *server, int64_t id, double *solution, h2b_request_result *res);
+/* queued, running, completed requests and reserved bytes */
+int h2b_server_stats(h2b_server *server, uint64_t out[4]);
+/* Finish running requests, drop queued ones, stop the workers. */
+void h2b_server_del(h2b_server *server);
+
 #ifdef __cplusplus
 }
 #endif
