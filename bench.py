@@ -52,6 +52,9 @@ def parse():
     p.add_argument("--no-batched", action="store_true")
     p.add_argument("--batched-meshes", type=int, default=256)
     p.add_argument("--plain-sample", type=int, default=16)
+    p.add_argument("--no-serving", action="store_true")
+    p.add_argument("--serve-requests", type=int, default=48)
+    p.add_argument("--serve-rates", default="50,200,1000,2000")
     return p.parse_args()
 
 
@@ -494,6 +497,81 @@ def run_batched(a):
     }
 
 
+def serving_workload(n, seed):
+    """Request stream: geometry uniform over sphere / cube / ellipsoid (semi-axes U[0.5, 2]^3),
+    triangle counts log-uniform in [512, 32768], Laplace (point source at 3x the extent) or
+    Helmholtz (k ~ U[1, 6], random plane-wave direction) with equal probability."""
+    from h2lib_b200 import bem3d as hb
+    from h2lib_b200.serve import HELMHOLTZ, LAPLACE
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(n):
+        kind = int(rng.integers(3))
+        tri = float(np.exp(rng.uniform(np.log(512.0), np.log(32768.0))))
+        axes = rng.uniform(0.5, 2.0, 3)
+        if kind == 1:
+            g = hb.new_cube_surface3d(max(3, int(round(np.sqrt(tri / 12.0)))))
+            ext = np.sqrt(3.0)
+        elif kind == 0:
+            g = hb.new_sphere_surface3d(max(4, int(round(np.sqrt(tri / 8.0)))))
+            ext = 1.0
+        else:
+            g = hb.new_ellipsoid_surface3d(max(4, int(round(np.sqrt(tri / 8.0)))), axes)
+            ext = float(axes.max())
+        d = rng.standard_normal(3)
+        d /= np.linalg.norm(d)
+        if rng.random() < 0.5:
+            out.append((g, LAPLACE, 3.0 * ext * d, 0.0))
+        else:
+            out.append((g, HELMHOLTZ, d, float(rng.uniform(1.0, 6.0))))
+    return out
+
+
+def run_serving(a):
+    """Poisson request streams through the solve server (8 slots, 150 GB budget, mixed
+    precision), then the plain FP64 form (one slot, FP64) on the same requests."""
+    from h2lib_b200.serve import Server
+    rates = [float(r) for r in a.serve_rates.split(",")]
+    reqs = serving_workload(a.serve_requests, BATCH_SEED + 1)
+    rng = np.random.default_rng(BATCH_SEED + 2)
+
+    def serve(requests, slots, mixed, rate):
+        srv = Server(slots=slots, hbm_budget=150 << 30)
+        try:
+            for g, pde, src, k in requests[:2]:  # warm-up of the code paths
+                srv.wait(srv.submit(g, pde, src, k=k, mixed=mixed))
+            gaps = rng.exponential(1.0 / rate, len(requests)) if rate else np.zeros(len(requests))
+            t0 = time.perf_counter()
+            ids, due = [], 0.0
+            for (g, pde, src, k), gap in zip(requests, gaps):
+                due += gap
+                dt = t0 + due - time.perf_counter()
+                if dt > 0:
+                    time.sleep(dt)
+                ids.append(srv.submit(g, pde, src, k=k, mixed=mixed))
+            res = [srv.wait(i)[1] for i in ids]
+        finally:
+            srv.close()
+        lat = np.array([r["t_done"] - r["t_submit"] for r in res])
+        span = max(r["t_done"] for r in res) - min(r["t_submit"] for r in res)
+        return {"rate_req_s": rate, "requests": len(res), "solves_per_s": len(res) / span,
+                "latency_p50_s": float(np.percentile(lat, 50)),
+                "latency_p99_s": float(np.percentile(lat, 99)),
+                "max_rel_residual_fp64": float(max(r["rel_residual"] for r in res)),
+                "iterations_median": float(np.median([r["iterations"] for r in res]))}
+
+    sweep = [serve(reqs, 8, True, r) for r in rates]
+    plain = serve(reqs[:a.plain_sample], 1, False, 0.0)
+    best = max(s["solves_per_s"] for s in sweep)
+    return {"workload": f"{len(reqs)} requests per rate: sphere/cube/ellipsoid, 512..32768 "
+                        f"triangles, Laplace (linear, m 4) or Helmholtz BW (k 1..6, constant, m 5),"
+                        f" GMRES to 1e-8 (FP64 residual); seed {BATCH_SEED + 1}",
+            "server": "8 slots, 150 GB HBM budget, FP32 Arnoldi steps + FP64 residuals",
+            "sweep": sweep,
+            "plain_fp64": dict(plain, path="1 slot, FP64, requests back to back"),
+            "speedup_vs_plain_fp64": best / plain["solves_per_s"]}
+
+
 def main():
     a = parse()
     rank, world, local = dist_init(a.gpus)
@@ -529,6 +607,11 @@ def main():
                 res["batched"] = run_batched(a)
             except Exception as e:  # reported, never hides the headline line
                 res["batched"] = {"error": str(e)[:300]}
+        if not a.no_serving:
+            try:
+                res["serving"] = run_serving(a)
+            except Exception as e:  # reported, never hides the headline line
+                res["serving"] = {"error": str(e)[:300]}
         if not a.no_cpu_baseline:
             try:
                 res["cpu_baseline"] = cpu_baseline(a)

@@ -88,6 +88,11 @@ _SIGS = {
     "h2b_project_l2_harmonic": (C.c_int, [vp, _f64p, vp]),
     "h2b_l2_error_harmonic": (C.c_int, [vp, _f64p, vp, C.POINTER(C.c_double),
                                         C.POINTER(C.c_double)]),
+    "h2b_server_new": (vp, [C.c_int, C.c_uint32, C.c_uint64]),
+    "h2b_server_submit": (C.c_int64, [vp, vp]),
+    "h2b_server_wait": (C.c_int, [vp, C.c_int64, vp, vp]),
+    "h2b_server_stats": (C.c_int, [vp, _u64p]),
+    "h2b_server_del": (None, [vp]),
     "h2b_project_l2_harmonic_multi": (C.c_int, [vp, C.c_uint32, _u32p, C.c_uint32, _f64p, vp]),
     "h2b_l2_error_harmonic_multi": (C.c_int, [vp, C.c_uint32, _u32p, C.c_uint32, _f64p, vp,
                                               _f64p, _f64p]),

@@ -120,3 +120,14 @@ def test_tree_rejects_bad_input():
     gr = hb.new_sphere_surface3d(2)
     assert not lib.h2b_tree_new(gr.vertices, gr.x, gr.triangles, gr.t, L, L, 16, -1.0)
     assert "eta" in hb.__dict__["check"].__globals__["last_error"]()
+
+
+def test_server_needs_a_device():
+    """Without a CUDA device the server refuses to start (no CPU fallback)."""
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    from h2lib_b200.serve import Server
+    with pytest.raises(H2BError):
+        Server(slots=2)
+from h2lib_b200._lib import H2BError  # noqa: E402
