@@ -34,6 +34,14 @@ Z = (1.2, 1.2, 1.2)
 # algorithmic FP64 operations per quadrature point (reference source, + - * / sqrt counted as 1):
 # linear-basis single layer 64, double layer 72
 FLOPS_PER_POINT = {"slp": 64, "dlp": 72}
+# flops the tensor-factored distant-pair sum executes per triangle pair for SLP+DLP, linear basis,
+# q = 2 (FMA = 2): 16 point pairs x 37 (difference 3, r^2 5, rsqrt 13, normal part 4, three
+# column weights per channel 12) + 4 row points x 53 (x_a 12, <x_a, n> 5, 3 x 3 x 2 outer FMAs
+# 36) + 4 column points x 17 (y_b 12, <y_b, n> 5) + 20 for the scaling
+EXECUTED_FLOPS_PER_PAIR = 16 * 37 + 4 * 53 + 4 * 17 + 20
+# DRAM bytes (read + write) of one near_dist_kernel launch on this workload from an ncu capture
+# of the full-size run (dram__bytes_read.sum + dram__bytes_write.sum); None until captured
+NEAR_DIST_TRAFFIC = None
 
 
 def parse():
@@ -260,9 +268,13 @@ def run_ours(a, rank, world, local):
     sing_points = pc["vertex"] * 512 + pc["edge"] * 1536 + pc["identical"] * 1536
     peak = fp64_peak_tflops(torch)
     achieved = dist_flops / (near_dist_ms * 1e-3) / 1e12
+    executed = pc["distant"] * EXECUTED_FLOPS_PER_PAIR
     roofline = {"bound": "fp64", "kernel": "near_dist_kernel (fused SLP+DLP, linear basis)",
                 "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
-                "traffic": None,
+                "traffic": NEAR_DIST_TRAFFIC,
+                "executed_flops_per_launch": executed,
+                "executed_tflops": executed / (near_dist_ms * 1e-3) / 1e12,
+                "executed_frac": executed / (near_dist_ms * 1e-3) / 1e12 / peak,
                 "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (MEASURED_PEAKS.json "
                                "has no FP64 figure)",
                 "flops_per_launch": dist_flops, "launch_ms": near_dist_ms}
@@ -557,11 +569,14 @@ def run_serving(a):
         return {"rate_req_s": rate, "requests": len(res), "solves_per_s": len(res) / span,
                 "latency_p50_s": float(np.percentile(lat, 50)),
                 "latency_p99_s": float(np.percentile(lat, 99)),
+                "queue_wait_p50_s": float(np.median([r["t_start"] - r["t_submit"] for r in res])),
+                "mean_phase_s": {p: float(np.mean([r["t_" + p] for r in res]))
+                                 for p in ("setup", "assembly", "rhs", "solve")},
                 "max_rel_residual_fp64": float(max(r["rel_residual"] for r in res)),
                 "iterations_median": float(np.median([r["iterations"] for r in res]))}
 
     sweep = [serve(reqs, 8, True, r) for r in rates]
-    plain = serve(reqs[:a.plain_sample], 1, False, 0.0)
+    plain = serve(reqs, 1, False, 0.0)
     best = max(s["solves_per_s"] for s in sweep)
     return {"workload": f"{len(reqs)} requests per rate: sphere/cube/ellipsoid, 512..32768 "
                         f"triangles, Laplace (linear, m 4) or Helmholtz BW (k 1..6, constant, m 5),"

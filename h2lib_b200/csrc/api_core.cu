@@ -61,6 +61,9 @@ extern "C" int h2b_device_init(int device) {
     if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
       uint64_t keep = UINT64_MAX;
       cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+      // never make one handle's stream wait for another's to reuse a freed block
+      int no = 0;
+      cudaMemPoolSetAttribute(pool, cudaMemPoolReuseAllowInternalDependencies, &no);
     }
     cudaGetLastError();
     g_inited_device = device;

@@ -54,6 +54,7 @@ static void devtree_free(DevCTree &t, cudaStream_t st) {
   dfree(t.d_pts, st); dfree(t.d_V, st); dfree(t.d_E, st); dfree(t.d_counter, st); dfree(t.d_refs, st);
   dfree(t.d_tr_off, st); dfree(t.d_tr_len, st);
   dfree(t.d_W, st); dfree(t.d_woff, st); dfree(t.d_fitems, st); dfree(t.d_wleaves, st); dfree(t.d_mitems, st);
+  dfree(t.d_seg, st);
 }
 
 // Flattened bases: W_t for the clusters of admissible blocks (`adm`, ids of this tree) and all
@@ -126,7 +127,11 @@ static int devtree_build(DevCTree &t, const h2b_ctree &c, int basis, uint32_t m,
   t.n = c.n;
   t.nidx = c.nidx;
   t.depth = c.depth;
-  std::vector<uint32_t> leaves, nonroot;
+  std::vector<uint32_t> leaves, nonroot, seg(c.n, 0);
+  t.roots.clear();
+  t.h_idx = c.idx;
+  t.h_off = c.off;
+  t.h_size = c.size;
   std::vector<uint64_t> voff(c.n, 0);
   std::vector<double> pts((size_t) c.n * 3 * m);
   uint64_t vtot = 0;
@@ -139,6 +144,8 @@ static int devtree_build(DevCTree &t, const h2b_ctree &c, int basis, uint32_t m,
       t.max_rows = std::max(t.max_rows, c.size[i]);
     }
     if (c.father[i] != UINT32_MAX) nonroot.push_back(i);  // every root of a forest excluded
+    else t.roots.push_back(i);
+    seg[i] = (uint32_t) t.roots.size() - 1;  // pre-order: a surface's clusters follow its root
     box_points(c.bmin + 3 * (size_t) i, c.bmax + 3 * (size_t) i, m, pts.data() + (size_t) i * 3 * m);
   }
   t.vtotal = vtot;
@@ -182,7 +189,8 @@ static int devtree_build(DevCTree &t, const h2b_ctree &c, int basis, uint32_t m,
       (rc = upload(&t.d_leaves, leaves, st)) || (rc = upload(&t.d_nonroot, nonroot, st)) ||
       (rc = upload(&t.d_levels, levels, st)) || (rc = upload(&t.d_voff, voff, st)) ||
       (rc = upload(&t.d_pts, pts, st)) || (rc = upload(&t.d_refs, refs, st)) ||
-      (rc = upload(&t.d_tr_off, tr_off, st)) || (rc = upload(&t.d_tr_len, tr_len, st)))
+      (rc = upload(&t.d_tr_off, tr_off, st)) || (rc = upload(&t.d_tr_len, tr_len, st)) ||
+      (rc = upload(&t.d_seg, seg, st)))
     return rc;
   H2B_CUDA_TRY(cudaMallocAsync(&t.d_V, sizeof(double) * std::max<uint64_t>(vtot, 1), st));
   H2B_CUDA_TRY(cudaMallocAsync(&t.d_E, sizeof(double) * std::max<uint64_t>((uint64_t) (c.n - 1) * k * k, 1), st));
@@ -421,6 +429,8 @@ void h2b_h2_fill_mvm_plan(h2b_h2matrix *h) {
   p.bwd = MvmBackArgs{h->rt.d_leaves, h->rt.d_size, h->rt.d_off, h->rt.d_voff, h->rt.d_V,
                       h->d_yt, h->d_yp, h->rt.nleaves, (int) h->k};
   p.flat = h->flat;
+  p.rseg = h->rt.d_seg;
+  p.cseg = h->ct.d_seg;
   p.ncol_clusters = h->ct.n;
   for (int side = 0; side < 2; side++) {
     const DevCTree &t = side ? h->rt : h->ct;

@@ -33,6 +33,10 @@ struct DevCTree {
   std::vector<uint32_t> fitem_start, fitem_count;  // flatten items of father level l
   uint32_t nwleaves = 0, nmitems = 0;
   float *f_W = nullptr;  // FP32 copy of W (h2b_h2matrix_make_single)
+  // surfaces of a forest: the surface of every cluster (device) and the roots (host)
+  uint32_t *d_seg = nullptr;
+  std::vector<uint32_t> roots;
+  const uint32_t *h_idx = nullptr, *h_off = nullptr, *h_size = nullptr;  // the host tree
 };
 
 struct h2b_h2matrix {

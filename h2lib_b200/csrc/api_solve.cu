@@ -16,13 +16,27 @@ struct Combo {
   uint32_t nterms;
   const h2b_h2matrix *ops[16];
   double cre[16], cim[16];
-  uint32_t nrhs = 1;  // vectors hold nrhs columns of the operator size, each multiplied alone
+  uint32_t nrhs = 1;  // vectors hold nrhs columns of the operator size
+  // batched form: all columns in one launch sequence per term (work: h2b_mvm_work_doubles),
+  // optionally skipping the columns of finished systems (mask[segment + r * nseg])
+  double *work = nullptr;
+  const uint32_t *mask = nullptr;
+  uint32_t nseg = 1;
 };
 
 template <bool SINGLE>
 int combo_apply_t(void *ctx, const double *x, double *y, double ar, double ai, cudaStream_t st) {
   const Combo *c = (const Combo *) ctx;
   const size_t col = (size_t) (c->ops[0]->cx ? 2 : 1) * c->ops[0]->rt.nidx;
+  if (c->work) {
+    for (uint32_t i = 0; i < c->nterms; i++) {
+      const double br = ar * c->cre[i] - ai * c->cim[i], bi = ar * c->cim[i] + ai * c->cre[i];
+      int rc = h2b_mvm_launch_batch(&c->ops[i]->mvm, SINGLE ? 1 : 0, c->nrhs, x, col, y, col, br,
+                                    bi, c->work, c->mask, c->nseg, st);
+      if (rc != H2B_OK) return rc;
+    }
+    return H2B_OK;
+  }
   for (uint32_t r = 0; r < c->nrhs; r++)
     for (uint32_t i = 0; i < c->nterms; i++) {
       const double br = ar * c->cre[i] - ai * c->cim[i], bi = ar * c->cim[i] + ai * c->cre[i];
@@ -80,6 +94,20 @@ struct DevBuf {
 // With nrhs > 1 the vectors hold nrhs columns and system (s, r) is segment s of column r
 // (iters[s + r * nseg]).  mixed: Arnoldi steps with the FP32 copies of the matrices, (re)start
 // residuals and the final stopping test in FP64.
+// True when the tree is a forest whose surfaces (roots, in order) hold exactly the index ranges
+// seg_off[m] .. seg_off[m+1]: then the operator is block diagonal on the segments and a surface's
+// blocks only touch its own segment.
+static bool forest_matches(const DevCTree &t, uint32_t nseg, const uint32_t *seg_off) {
+  if (t.roots.size() != nseg || !t.h_idx) return false;
+  for (uint32_t m = 0; m < nseg; m++) {
+    const uint32_t r = t.roots[m], lo = seg_off[m], hi = seg_off[m + 1];
+    if (t.h_off[r] != lo || t.h_size[r] != hi - lo) return false;
+    for (uint32_t i = lo; i < hi; i++)
+      if (t.h_idx[i] < lo || t.h_idx[i] >= hi) return false;
+  }
+  return true;
+}
+
 static int solve_segments(Combo &combo, uint32_t nseg, const uint32_t *seg_off, uint32_t nrhs,
                           const double *b, double *x, double eps, uint32_t maxiter,
                           uint32_t kmax, int mixed, uint32_t *iters, const char *who) {
@@ -135,6 +163,24 @@ static int solve_segments(Combo &combo, uint32_t nseg, const uint32_t *seg_off, 
                                cudaMemcpyHostToDevice, st));
   H2B_CUDA_TRY(cudaMemcpyAsync(db, b, sizeof(double) * W * n, cudaMemcpyDefault, st));
   H2B_CUDA_TRY(cudaMemcpyAsync(dx, x, sizeof(double) * W * n, cudaMemcpyDefault, st));
+  // All columns of a term in one launch sequence; on a forest whose surfaces are exactly the
+  // segments, the products skip the columns of systems that have stopped.
+  DevBuf work;
+  work.st = st;
+  bool flat = true, forest = nseg > 1;
+  size_t nwork = 0;
+  for (uint32_t i = 0; i < combo.nterms; i++) {
+    const h2b_h2matrix *h = combo.ops[i];
+    flat = flat && h->flat;
+    forest = forest && forest_matches(h->rt, nseg, seg_off) && forest_matches(h->ct, nseg, seg_off);
+    nwork = std::max(nwork, h2b_mvm_work_doubles(&h->mvm, nrhs));
+  }
+  if (flat) {
+    H2B_CUDA_TRY(cudaMallocAsync(&work.p, sizeof(double) * nwork, st));
+    combo.work = (double *) work.p;
+    combo.mask = forest ? g.mask : nullptr;
+    combo.nseg = nseg;
+  }
   GmresOp op{(void *) &combo, combo_apply, mixed ? combo_apply_single : nullptr};
   std::vector<GmresState> hs(nsys);
   int rc = h2b_gmres_run(&g, &op, db, dx, maxiter, st, hs.data());

@@ -628,6 +628,7 @@ __global__ void precheck_kernel(GmresDev g, cudaGraphConditionalHandle hw) {
     GmresState *y = g.state + s;
     y->active = keeps_going(y, g.ctl->maxiter) ? 1u : 0u;
     y->restart = 0;
+    if (g.mask) g.mask[s] = y->active;
     if (y->active) any = 1;
   }
   __syncthreads();
@@ -660,7 +661,10 @@ __global__ void control_kernel(GmresDev g, cudaGraphConditionalHandle hw) {
   for (uint32_t s = threadIdx.x; s < g.nsys; s += blockDim.x) {
     GmresState *y = g.state + s;
     y->restart = 0;
-    if (!y->active) continue;
+    if (!y->active) {  // stopped earlier, or by the FP64 residual of a restart in this step
+      if (g.mask) g.mask[s] = 0;
+      continue;
+    }
     y->iter++;
     if (!(y->err == y->err)) y->nan = 1;
     y->active = keeps_going(y, g.ctl->maxiter) ? 1u : 0u;
@@ -670,6 +674,7 @@ __global__ void control_kernel(GmresDev g, cudaGraphConditionalHandle hw) {
       y->active = 1;
       y->verify = 1;
     }
+    if (g.mask) g.mask[s] = y->active;
     if (y->active) any = 1;
   }
   __syncthreads();
@@ -713,7 +718,7 @@ size_t h2b_gmres_workspace(int cx, uint32_t nsys, const uint32_t *sizes, uint32_
          + 2 * W * n                         // q, abuf
          + 2 * nb * ld                       // part
          + (sizeof(GmresState) * nsys + sizeof(GmresCtl) + sizeof(GmresSys) * nsys +
-            sizeof(uint32_t) * nb) / sizeof(double) + 64;
+            sizeof(uint32_t) * (nb + nsys)) / sizeof(double) + 64;
 }
 
 void h2b_gmres_layout(GmresDev *g, double *p, int cx, uint32_t nsys, const uint32_t *sizes,
@@ -754,6 +759,7 @@ void h2b_gmres_layout(GmresDev *g, double *p, int cx, uint32_t nsys, const uint3
   c = (char *) (((uintptr_t) c + 15) & ~(uintptr_t) 15);
   g->sys = (const GmresSys *) c; c += sizeof(GmresSys) * nsys;
   g->blk = (const uint32_t *) c;
+  g->mask = (uint32_t *) c + nb;
 }
 
 extern "C" int h2b_gmres_step(const GmresDev *g, const GmresOp *op, cudaStream_t st) {
@@ -846,6 +852,8 @@ extern "C" int h2b_gmres_run(const GmresDev *g, const GmresOp *op, const double 
     }
   } ef{exec};
   H2B_CUDA_TRY(cudaMemsetAsync(g->state, 0, sizeof(GmresState) * g->nsys, st));
+  // the first residual needs every system's product
+  H2B_CUDA_TRY(cudaMemsetAsync(g->mask, 1, sizeof(uint32_t) * g->nsys, st));
   H2B_CUDA_TRY(cudaMemsetAsync(g->T, 0, sizeof(double) * 2 * (size_t) g->nsys * g->kmax * g->kmax, st));
   if ((rc = h2b_gmres_bnorm(g, b, st)) != H2B_OK) return rc;
   if ((rc = h2b_gmres_init(g, op, b, x, GMRES_SEL_ALL, st)) != H2B_OK) return rc;

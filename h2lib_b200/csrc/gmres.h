@@ -54,6 +54,7 @@ struct GmresDev {
   double *part;              // nblocks x ldpart (complex pairs)
   GmresState *state;         // nsys
   GmresCtl *ctl;
+  uint32_t *mask;            // nsys: 1 while the system is active (read by a masked operator)
 };
 
 // y += alpha * A x on stream st (x, y: the global vectors).  apply_lo (optional) is a cheaper,

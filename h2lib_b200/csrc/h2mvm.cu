@@ -253,81 +253,154 @@ __global__ void __launch_bounds__(TPB) backward_chain_kernel(MvmBackArgs a, cons
   }
 }
 
-// Flattened-basis path.  xp = x[idx] and the accumulators are cleared in one launch.
+// Flattened-basis path, for nrhs right-hand sides at once.  Every CTA loads its matrix panel
+// once per column it multiplies; the columns after the first find the panel in L1/L2, so HBM
+// reads the matrix about once per product of all columns.  With a mask (batched solves on a
+// forest: mask[surface + r * nseg] for column r) a CTA skips the columns whose system is done.
+struct MvmVecs {
+  double *xp, *yp, *xt, *yt;      // work vectors, column r at r * stride
+  size_t sxp, syp, sxt, syt;
+  uint32_t nrhs, nseg;
+  const uint32_t *mask;           // NULL: every column
+  const uint32_t *rseg, *cseg;    // surface of each row / column cluster
+};
+
+__device__ __forceinline__ bool col_on(const MvmVecs &v, uint32_t seg, uint32_t r) {
+  return !v.mask || v.mask[seg + r * v.nseg] != 0;
+}
+
+// xp = x[idx] per column; the accumulators yp, xt, yt are cleared.
 template <bool CX>
-__global__ void gather_zero_kernel(const double *__restrict__ x, const uint32_t *__restrict__ idx,
-                                   double *__restrict__ xp, uint32_t n, double *__restrict__ z0,
-                                   size_t n0, double *__restrict__ z1, size_t n1,
-                                   double *__restrict__ z2, size_t n2) {
+__global__ void gather_zero_kernel(const double *__restrict__ x, size_t ldx,
+                                   const uint32_t *__restrict__ idx, uint32_t n, MvmVecs v,
+                                   size_t nyp, size_t nxt, size_t nyt) {
   const size_t i0 = blockIdx.x * (size_t) blockDim.x + threadIdx.x, st = (size_t) gridDim.x * blockDim.x;
-  for (size_t i = i0; i < n; i += st) {
-    const uint32_t j = idx[i];
-    if (CX) {
-      xp[2 * i] = x[2 * j];
-      xp[2 * i + 1] = x[2 * j + 1];
-    } else {
-      xp[i] = x[j];
+  for (uint32_t r = 0; r < v.nrhs; r++) {
+    const double *xr = x + r * ldx;
+    double *xp = v.xp + r * v.sxp;
+    for (size_t i = i0; i < n; i += st) {
+      const uint32_t j = idx[i];
+      if (CX) {
+        xp[2 * i] = xr[2 * j];
+        xp[2 * i + 1] = xr[2 * j + 1];
+      } else {
+        xp[i] = xr[j];
+      }
+    }
+    for (size_t i = i0; i < nyp; i += st) v.yp[r * v.syp + i] = 0.0;
+    for (size_t i = i0; i < nxt; i += st) v.xt[r * v.sxt + i] = 0.0;
+    for (size_t i = i0; i < nyt; i += st) v.yt[r * v.syt + i] = 0.0;
+  }
+}
+
+// y[idx[i]] += alpha * yp[i] per column
+template <bool CX>
+__global__ void scatter_multi_kernel(MvmVecs v, const uint32_t *__restrict__ idx,
+                                     double *__restrict__ y, size_t ldy, uint32_t n, double ar,
+                                     double ai) {
+  for (uint32_t r = 0; r < v.nrhs; r++) {
+    const double *yp = v.yp + r * v.syp;
+    double *yr = y + r * ldy;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+      const uint32_t j = idx[i];
+      if (CX) {
+        const double re = yp[2 * i], im = yp[2 * i + 1];
+        yr[2 * j] += ar * re - ai * im;
+        yr[2 * j + 1] += ar * im + ai * re;
+      } else {
+        yr[j] += ar * yp[i];
+      }
     }
   }
-  for (size_t i = i0; i < n0; i += st) z0[i] = 0.0;
-  for (size_t i = i0; i < n1; i += st) z1[i] = 0.0;
-  for (size_t i = i0; i < n2; i += st) z2[i] = 0.0;
 }
 
 // Launch 1 (flat): xt_c += W_c^T x over rows [r0, r0 + nr) of c (CTAs < items; W_c^T is k x |c|,
 // ld = k), and the nearfield blocks (the other CTAs).
 template <bool CX, bool SINGLE = false>
-__global__ void __launch_bounds__(TPB) forward_flat_near_kernel(MvmFlatArgs f, MvmCoupleArgs c) {
+__global__ void __launch_bounds__(TPB) forward_flat_near_kernel(MvmFlatArgs f, MvmCoupleArgs c,
+                                                                MvmVecs v) {
   constexpr int W = CX ? 2 : 1;
   __shared__ double red[TPB * W];
   __shared__ double tmp[KMAXW];
   if (blockIdx.x >= f.nitems) {
     const uint32_t nb = blockIdx.x - f.nitems;
     const uint32_t r = c.near_rc[nb], cc = c.near_cc[nb];
-    if (SINGLE)
-      panel_mv_atomic<CX>(c.Ns + (size_t) W * c.near_off[nb], c.rsize[r], c.csize[cc],
-                          c.xp + (size_t) W * c.coff[cc], c.yp + (size_t) W * c.roff[r], red);
-    else
-      panel_mv_atomic<CX>(c.N + (size_t) W * c.near_off[nb], c.rsize[r], c.csize[cc],
-                          c.xp + (size_t) W * c.coff[cc], c.yp + (size_t) W * c.roff[r], red);
+    const uint32_t seg = v.rseg ? v.rseg[r] : 0;
+    for (uint32_t q = 0; q < v.nrhs; q++) {
+      if (!col_on(v, seg, q)) continue;
+      const double *xp = v.xp + q * v.sxp + (size_t) W * c.coff[cc];
+      double *yp = v.yp + q * v.syp + (size_t) W * c.roff[r];
+      if (SINGLE)
+        panel_mv_atomic<CX>(c.Ns + (size_t) W * c.near_off[nb], c.rsize[r], c.csize[cc], xp, yp,
+                            red);
+      else
+        panel_mv_atomic<CX>(c.N + (size_t) W * c.near_off[nb], c.rsize[r], c.csize[cc], xp, yp,
+                            red);
+    }
     return;
   }
   const uint32_t *it = f.items + 3 * (size_t) blockIdx.x;
   const uint32_t cl = it[0], r0 = it[1], nr = it[2];
   const uint32_t k = (uint32_t) f.k;
-  if (SINGLE)
-    gemv_split<CX, false>(f.Ws + f.woff[cl] + (size_t) r0 * k, k, k, nr,
-                          c.xp + (size_t) W * (f.off[cl] + r0), red, tmp);
-  else
-    gemv_split<CX, false>(f.W + f.woff[cl] + (size_t) r0 * k, k, k, nr,
-                          c.xp + (size_t) W * (f.off[cl] + r0), red, tmp);
-  for (uint32_t e = threadIdx.x; e < W * k; e += blockDim.x)
-    atomicAdd(const_cast<double *>(&c.xt[(size_t) W * k * cl + e]), tmp[e]);
+  const uint32_t seg = v.cseg ? v.cseg[cl] : 0;
+  for (uint32_t q = 0; q < v.nrhs; q++) {
+    if (!col_on(v, seg, q)) continue;
+    const double *xp = v.xp + q * v.sxp + (size_t) W * (f.off[cl] + r0);
+    if (SINGLE)
+      gemv_split<CX, false>(f.Ws + f.woff[cl] + (size_t) r0 * k, k, k, nr, xp, red, tmp);
+    else
+      gemv_split<CX, false>(f.W + f.woff[cl] + (size_t) r0 * k, k, k, nr, xp, red, tmp);
+    double *xt = v.xt + q * v.sxt + (size_t) W * k * cl;
+    for (uint32_t e = threadIdx.x; e < W * k; e += blockDim.x) atomicAdd(&xt[e], tmp[e]);
+    __syncthreads();  // tmp is reused by the next column
+  }
+}
+
+// Launch 2 (flat): coupling blocks yt_r += S_b xt_c per column.
+template <bool CX, bool SINGLE>
+__global__ void __launch_bounds__(TPB) coupling_flat_kernel(MvmCoupleArgs a, MvmVecs v) {
+  constexpr int W = CX ? 2 : 1;
+  __shared__ double red[TPB * W];
+  const uint32_t b = blockIdx.x;
+  const uint32_t k = (uint32_t) a.k;
+  const uint32_t seg = v.rseg ? v.rseg[a.adm_rc[b]] : 0;
+  for (uint32_t q = 0; q < v.nrhs; q++) {
+    if (!col_on(v, seg, q)) continue;
+    const double *xt = v.xt + q * v.sxt + (size_t) W * k * a.adm_cc[b];
+    double *yt = v.yt + q * v.syt + (size_t) W * k * a.adm_rc[b];
+    if (SINGLE)
+      panel_mv_atomic<CX>(a.Ss + (size_t) W * k * k * b, k, k, xt, yt, red);
+    else
+      panel_mv_atomic<CX>(a.S + (size_t) W * k * k * b, k, k, xt, yt, red);
+  }
 }
 
 // Launch 3 (flat): yp[rows r0 .. r0 + nr of c] += W_c[r0:, :] yt_c (W_c is |c| x k, ld = |c|).
 template <bool CX, bool SINGLE = false>
-__global__ void __launch_bounds__(TPB) backward_flat_kernel(MvmFlatArgs f, const double *yt,
-                                                            double *yp) {
+__global__ void __launch_bounds__(TPB) backward_flat_kernel(MvmFlatArgs f, MvmVecs v) {
   constexpr int W = CX ? 2 : 1;
   __shared__ double red[TPB * W];
   __shared__ double tmp[H2B_MVM_FLAT_ROWS * W];
   const uint32_t *it = f.items + 3 * (size_t) blockIdx.x;
   const uint32_t cl = it[0], r0 = it[1], nr = it[2];
   const uint32_t k = (uint32_t) f.k;
-  if (SINGLE)
-    gemv_split<CX, false>(f.Ws + f.woff[cl] + r0, f.size[cl], nr, k, yt + (size_t) W * k * cl,
-                          red, tmp);
-  else
-    gemv_split<CX, false>(f.W + f.woff[cl] + r0, f.size[cl], nr, k, yt + (size_t) W * k * cl,
-                          red, tmp);
-  double *y = yp + (size_t) W * (f.off[cl] + r0);
-  for (uint32_t e = threadIdx.x; e < W * nr; e += blockDim.x) atomicAdd(&y[e], tmp[e]);
+  const uint32_t seg = v.rseg ? v.rseg[cl] : 0;
+  for (uint32_t q = 0; q < v.nrhs; q++) {
+    if (!col_on(v, seg, q)) continue;
+    const double *yt = v.yt + q * v.syt + (size_t) W * k * cl;
+    if (SINGLE)
+      gemv_split<CX, false>(f.Ws + f.woff[cl] + r0, f.size[cl], nr, k, yt, red, tmp);
+    else
+      gemv_split<CX, false>(f.W + f.woff[cl] + r0, f.size[cl], nr, k, yt, red, tmp);
+    double *y = v.yp + q * v.syp + (size_t) W * (f.off[cl] + r0);
+    for (uint32_t e = threadIdx.x; e < W * nr; e += blockDim.x) atomicAdd(&y[e], tmp[e]);
+    __syncthreads();  // tmp is reused by the next column
+  }
 }
 
 template <bool CX, bool SINGLE>
-int launch_flat(const MvmPlan *p, const double *x, double *y, double ar, double ai,
-                cudaStream_t st) {
+int launch_flat(const MvmPlan *p, const double *x, size_t ldx, double *y, size_t ldy, double ar,
+                double ai, const MvmVecs &v, cudaStream_t st) {
   const size_t W = CX ? 2 : 1;
   const int sms = p->num_sms > 0 ? p->num_sms : 148;
   const MvmCoupleArgs &ca = p->cpl;
@@ -335,16 +408,31 @@ int launch_flat(const MvmPlan *p, const double *x, double *y, double ar, double 
   const uint32_t gz = std::min<uint32_t>((zn + 255) / 256 + 1, (uint32_t) (4 * sms));
   const size_t nyp = W * p->nrow, nxt = W * (size_t) p->k * p->ncol_clusters,
                nyt = W * (size_t) p->k * p->nrow_clusters;
-  gather_zero_kernel<CX><<<gz, 256, 0, st>>>(x, p->cidx, p->xp, p->ncol, p->yp, nyp, p->xt, nxt,
-                                             p->yt, nyt);
+  gather_zero_kernel<CX><<<gz, 256, 0, st>>>(x, ldx, p->cidx, p->ncol, v, nyp, nxt, nyt);
   if (p->ffwd.nitems + ca.nnear)
-    forward_flat_near_kernel<CX, SINGLE><<<p->ffwd.nitems + ca.nnear, TPB, 0, st>>>(p->ffwd, ca);
-  if (ca.nadm) coupling_mv_kernel<CX, SINGLE><<<ca.nadm, TPB, 0, st>>>(ca);
+    forward_flat_near_kernel<CX, SINGLE><<<p->ffwd.nitems + ca.nnear, TPB, 0, st>>>(p->ffwd, ca,
+                                                                                     v);
+  if (ca.nadm) coupling_flat_kernel<CX, SINGLE><<<ca.nadm, TPB, 0, st>>>(ca, v);
   if (p->fbwd.nitems)
-    backward_flat_kernel<CX, SINGLE><<<p->fbwd.nitems, TPB, 0, st>>>(p->fbwd, p->yt, p->yp);
-  scatter_kernel<CX><<<gz, 256, 0, st>>>(p->yp, p->ridx, y, p->nrow, ar, ai);
+    backward_flat_kernel<CX, SINGLE><<<p->fbwd.nitems, TPB, 0, st>>>(p->fbwd, v);
+  scatter_multi_kernel<CX><<<gz, 256, 0, st>>>(v, p->ridx, y, ldy, p->nrow, ar, ai);
   H2B_CUDA_TRY(cudaGetLastError());
   return H2B_OK;
+}
+
+// The plan's own work vectors (one column, no mask).
+MvmVecs plan_vecs(const MvmPlan *p) {
+  MvmVecs v;
+  v.xp = p->xp;
+  v.yp = p->yp;
+  v.xt = p->xt;
+  v.yt = p->yt;
+  v.sxp = v.syp = v.sxt = v.syt = 0;
+  v.nrhs = 1;
+  v.nseg = 1;
+  v.mask = nullptr;
+  v.rseg = v.cseg = nullptr;
+  return v;
 }
 
 }  // namespace
@@ -359,8 +447,9 @@ extern "C" int h2b_mvm_launch_single(const MvmPlan *p, const double *x, double *
     h2b_set_error("matvec: rank %d > 128", p->k);
     return H2B_ERR_ARG;
   }
-  return p->cx ? launch_flat<true, true>(p, x, y, ar, ai, st)
-               : launch_flat<false, true>(p, x, y, ar, ai, st);
+  const MvmVecs v = plan_vecs(p);
+  return p->cx ? launch_flat<true, true>(p, x, 0, y, 0, ar, ai, v, st)
+               : launch_flat<false, true>(p, x, 0, y, 0, ar, ai, v, st);
 }
 
 extern "C" int h2b_mvm_launch(const MvmPlan *p, const double *x, double *y, double ar, double ai,
@@ -374,8 +463,11 @@ extern "C" int h2b_mvm_launch(const MvmPlan *p, const double *x, double *y, doub
   }
   const uint32_t gg = (p->ncol + 255) / 256 < (uint32_t) (4 * sms) ? (p->ncol + 255) / 256
                                                                    : (uint32_t) (4 * sms);
-  if (p->flat) return p->cx ? launch_flat<true, false>(p, x, y, ar, ai, st)
-                            : launch_flat<false, false>(p, x, y, ar, ai, st);
+  if (p->flat) {
+    const MvmVecs v = plan_vecs(p);
+    return p->cx ? launch_flat<true, false>(p, x, 0, y, 0, ar, ai, v, st)
+                 : launch_flat<false, false>(p, x, 0, y, 0, ar, ai, v, st);
+  }
   H2B_CUDA_TRY(cudaMemsetAsync(p->yp, 0, sizeof(double) * W * p->nrow, st));
   H2B_CUDA_TRY(cudaMemsetAsync(p->yt, 0, sizeof(double) * W * p->k * p->nrow_clusters, st));
   const MvmForwardArgs &fa = p->fwd;
@@ -396,4 +488,49 @@ extern "C" int h2b_mvm_launch(const MvmPlan *p, const double *x, double *y, doub
   }
   H2B_CUDA_TRY(cudaGetLastError());
   return H2B_OK;
+}
+
+extern "C" size_t h2b_mvm_work_doubles(const MvmPlan *p, uint32_t nrhs) {
+  const size_t W = p->cx ? 2 : 1;
+  return nrhs * W * ((size_t) p->ncol + p->nrow +
+                     (size_t) p->k * (p->ncol_clusters + p->nrow_clusters));
+}
+
+extern "C" int h2b_mvm_launch_batch(const MvmPlan *p, int single, uint32_t nrhs, const double *x,
+                                    size_t ldx, double *y, size_t ldy, double ar, double ai,
+                                    double *work, const uint32_t *mask, uint32_t nseg,
+                                    cudaStream_t st) {
+  if (!p->flat || (single && (!p->cpl.Ss || !p->cpl.Ns || !p->ffwd.Ws || !p->fbwd.Ws))) {
+    h2b_set_error("batched matvec: needs the flattened path%s",
+                  single ? " and the FP32 copies (h2b_h2matrix_make_single)" : "");
+    return H2B_ERR_ARG;
+  }
+  if (p->k > 128 || nrhs == 0) {
+    h2b_set_error("batched matvec: rank %d > 128 or no columns", p->k);
+    return H2B_ERR_ARG;
+  }
+  const size_t W = p->cx ? 2 : 1;
+  MvmVecs v;
+  v.sxp = W * p->ncol;
+  v.syp = W * p->nrow;
+  v.sxt = W * (size_t) p->k * p->ncol_clusters;
+  v.syt = W * (size_t) p->k * p->nrow_clusters;
+  v.xp = work;
+  v.yp = v.xp + nrhs * v.sxp;
+  v.xt = v.yp + nrhs * v.syp;
+  v.yt = v.xt + nrhs * v.sxt;
+  v.nrhs = nrhs;
+  v.nseg = nseg;
+  v.mask = mask;
+  v.rseg = mask ? p->rseg : nullptr;
+  v.cseg = mask ? p->cseg : nullptr;
+  if (mask && (!p->rseg || !p->cseg)) {
+    h2b_set_error("batched matvec: masking needs the surface of every cluster");
+    return H2B_ERR_ARG;
+  }
+  if (p->cx)
+    return single ? launch_flat<true, true>(p, x, ldx, y, ldy, ar, ai, v, st)
+                  : launch_flat<true, false>(p, x, ldx, y, ldy, ar, ai, v, st);
+  return single ? launch_flat<false, true>(p, x, ldx, y, ldy, ar, ai, v, st)
+                : launch_flat<false, false>(p, x, ldx, y, ldy, ar, ai, v, st);
 }

@@ -66,6 +66,7 @@ struct MvmPlan {
   int cx, num_sms;
   int flat;                      // 1: flattened-basis transforms (ffwd / fbwd)
   MvmFlatArgs ffwd, fbwd;
+  const uint32_t *rseg, *cseg;   // surface of every row / column cluster (forest trees)
   int k;
   uint32_t nrow, ncol, nrow_clusters, ncol_clusters;
   const uint32_t *ridx, *cidx;   // device index arrays of the row / column tree
@@ -85,3 +86,12 @@ extern "C" int h2b_mvm_launch(const MvmPlan *p, const double *x, double *y, doub
 // read as FP32 and widened, vectors and sums stay FP64, so the product reads half the bytes.
 extern "C" int h2b_mvm_launch_single(const MvmPlan *p, const double *x, double *y, double ar,
                                      double ai, cudaStream_t st);
+// y[:, r] += alpha A x[:, r] for nrhs columns (leading dimensions ldx, ldy in doubles) in one
+// launch sequence that reads the matrix about once; `work` holds h2b_mvm_work_doubles(p, nrhs)
+// doubles.  mask (optional, forest matrices): column r of surface s is computed only when
+// mask[s + r * nseg] != 0 (the others receive nothing).  single: the FP32 copies.
+extern "C" size_t h2b_mvm_work_doubles(const MvmPlan *p, uint32_t nrhs);
+extern "C" int h2b_mvm_launch_batch(const MvmPlan *p, int single, uint32_t nrhs, const double *x,
+                                    size_t ldx, double *y, size_t ldy, double ar, double ai,
+                                    double *work, const uint32_t *mask, uint32_t nseg,
+                                    cudaStream_t st);

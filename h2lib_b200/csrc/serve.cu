@@ -85,6 +85,11 @@ uint64_t estimate_bytes(const h2b_request &r) {
 
 // Run one request to the end on the calling (worker) thread.
 int run_request(Req *q) {
+  auto tick = [] { return Clock::now(); };
+  auto secs = [](Clock::time_point a, Clock::time_point b) {
+    return std::chrono::duration<double>(b - a).count();
+  };
+  const auto c0 = tick();
   const h2b_request &d = q->desc;
   const bool helm = d.pde == H2B_HELMHOLTZ;
   const uint32_t nv = d.vertices, nt = d.triangles;
@@ -104,6 +109,7 @@ int run_request(Req *q) {
                               : nullptr;
   h2b_h2matrix *V = tr ? h2b_h2matrix_new(slp, tr, m) : nullptr;
   h2b_h2matrix *K = tr ? h2b_h2matrix_new(dlp, tr, m) : nullptr;
+  const auto c1 = tick();
   const uint32_t nd = helm ? nt : nv;
   const size_t W = helm ? 2 : 1;
   std::vector<double> b(W * nd, 0.0), u(W * nd, 0.0), gD;
@@ -120,6 +126,7 @@ int run_request(Req *q) {
       if (rc == H2B_OK) rc = h2b_h2matrix_assemble_nearfield_pair(V, K);
     }
   }
+  const auto c2 = tick();
   const h2b_h2matrix *ops[2];
   double coef[4];
   uint32_t nterms = 1;
@@ -144,6 +151,7 @@ int run_request(Req *q) {
       coef[1] = 0.0;
     }
   }
+  const auto c3 = tick();
   const bool mixed = (d.flags & H2B_SOLVE_MIXED) != 0;
   if (rc == H2B_OK && mixed)
     for (uint32_t i = 0; i < nterms && rc == H2B_OK; i++)
@@ -156,6 +164,11 @@ int run_request(Req *q) {
                                  d.kmax);
     if (it < 0) rc = it;
   }
+  const auto c4 = tick();
+  q->res.t_setup = secs(c0, c1);
+  q->res.t_assembly = secs(c1, c2);
+  q->res.t_rhs = secs(c2, c3);
+  q->res.t_solve = secs(c3, c4);
   double relres = 0.0;
   if (rc == H2B_OK) rc = h2b_residual_norm(nterms, ops, coef, b.data(), u.data(), &relres);
   if (rc == H2B_OK) {

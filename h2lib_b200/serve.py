@@ -23,7 +23,9 @@ class Request(C.Structure):
 class Result(C.Structure):
     _fields_ = [("status", C.c_int), ("iterations", C.c_uint32), ("unknowns", C.c_uint32),
                 ("rel_residual", C.c_double), ("t_submit", C.c_double), ("t_start", C.c_double),
-                ("t_done", C.c_double), ("bytes_reserved", C.c_uint64)]
+                ("t_done", C.c_double), ("bytes_reserved", C.c_uint64),
+                ("t_setup", C.c_double), ("t_assembly", C.c_double), ("t_rhs", C.c_double),
+                ("t_solve", C.c_double)]
 
 
 class Server:

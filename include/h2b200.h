@@ -387,6 +387,8 @@ typedef struct {
   double rel_residual;       /* FP64 ||b - A u|| / ||b|| after the solve */
   double t_submit, t_start, t_done;  /* seconds since the server started */
   uint64_t bytes_reserved;   /* device-memory estimate charged against the budget */
+  /* seconds spent in: surface + trees + H2 structure, assembly, right-hand side, solve */
+  double t_setup, t_assembly, t_rhs, t_solve;
 } h2b_request_result;
 
 /* A server with `slots` worker threads on `device` admitting requests while their estimated
