@@ -61,6 +61,7 @@ def parse():
     p.add_argument("--batched-meshes", type=int, default=256)
     p.add_argument("--plain-sample", type=int, default=16)
     p.add_argument("--no-serving", action="store_true")
+    p.add_argument("--no-helmholtz", action="store_true")
     p.add_argument("--serve-requests", type=int, default=48)
     p.add_argument("--serve-rates", default="50,200,1000,2000")
     return p.parse_args()
@@ -509,6 +510,51 @@ def run_batched(a):
     }
 
 
+def run_helmholtz(a):
+    """Brakhage-Werner solves of config 3: unit cube split 64 (49152 triangles), constant basis,
+    q 2/4, leaf 64, eta 1.4, m 5, plane wave along (1,1,1)/sqrt(3), GMRES(80) to 1e-8, k = 2
+    and 8; FP64 and mixed precision."""
+    import torch
+    from h2lib_b200 import bem3d as hb
+    C = hb.BASIS_CONSTANT_BEM3D
+    d = np.ones(3) / np.sqrt(3.0)
+    out = []
+    gr = hb.new_cube_surface3d(64)
+    tree = hb.build_tree(gr, C, C, 64, 1.4)
+    for k in (2.0, 8.0):
+        slp = hb.new_slp_helmholtz_bem3d(k, gr, 2, 4, C, C)
+        dlp = hb.new_dlp_helmholtz_bem3d(k, gr, 2, 4, C, C, 0.5)
+        V, K = hb.H2Matrix(slp, tree, 5), hb.H2Matrix(dlp, tree, 5)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        V.assemble()
+        K.assemble()
+        t_asm = time.perf_counter() - t0
+        b = hb.integrate_plane_wave(slp, k * d, coef=-1.0)
+        u64 = np.zeros(V.rows, dtype=np.complex128)
+        t0 = time.perf_counter()
+        it64 = hb.solve_gmres([K, V], [1.0, -1j * k], b, u64, 1e-8, 1000, 80)
+        t64 = time.perf_counter() - t0
+        V.make_single()
+        K.make_single()
+        u32 = np.zeros(V.rows, dtype=np.complex128)
+        t0 = time.perf_counter()
+        it32 = hb.solve_gmres_mixed([K, V], [1.0, -1j * k], b, u32, 1e-8, 1000, 80)
+        t32 = time.perf_counter() - t0
+        ent = V.info()["near_entries"] + K.info()["near_entries"]
+        out.append({"k": k, "assembly_s": t_asm, "near_entries_per_s": ent / t_asm,
+                    "fp64": {"iterations": it64, "seconds": t64,
+                             "rel_residual": hb.residual_norm([K, V], [1.0, -1j * k], b, u64)},
+                    "mixed": {"iterations": it32, "seconds": t32,
+                              "rel_residual": hb.residual_norm([K, V], [1.0, -1j * k], b, u32),
+                              "rel_diff_to_fp64": float(np.linalg.norm(u32 - u64) /
+                                                        np.linalg.norm(u64))},
+                    "reference_iterations": {2.0: 22, 8.0: 32}[k]})
+        del V, K, slp, dlp
+    return {"workload": "config 3: cube 49152 triangles, Helmholtz Brakhage-Werner, constant "
+                        "basis, m 5, GMRES(80) to 1e-8", "runs": out}
+
+
 def serving_workload(n, seed):
     """Request stream: geometry uniform over sphere / cube / ellipsoid (semi-axes U[0.5, 2]^3),
     triangle counts log-uniform in [512, 32768], Laplace (point source at 3x the extent) or
@@ -622,6 +668,11 @@ def main():
                 res["batched"] = run_batched(a)
             except Exception as e:  # reported, never hides the headline line
                 res["batched"] = {"error": str(e)[:300]}
+        if not a.no_helmholtz:
+            try:
+                res["helmholtz"] = run_helmholtz(a)
+            except Exception as e:  # reported, never hides the headline line
+                res["helmholtz"] = {"error": str(e)[:300]}
         if not a.no_serving:
             try:
                 res["serving"] = run_serving(a)
