@@ -24,6 +24,8 @@ finish_tree(h2b_tree *tr)
   return H2B_OK;
 }
 
+static int ctree_append(h2b_ctree *dst, const h2b_ctree *src, uint32_t ioff);
+
 h2b_tree *
 h2b_tree_new(uint32_t vertices, const double *x, uint32_t triangles, const uint32_t *t,
              int row_basis, int col_basis, uint32_t clf, double eta)
@@ -45,8 +47,11 @@ h2b_tree_new(uint32_t vertices, const double *x, uint32_t triangles, const uint3
   }
   tr->row_basis = row_basis;
   tr->col_basis = col_basis;
+  /* equal bases give equal trees: build the row tree once and copy it */
   if (h2b_ctree_build(vertices, x, triangles, t, row_basis, clf, &tr->row) != H2B_OK
-      || h2b_ctree_build(vertices, x, triangles, t, col_basis, clf, &tr->col) != H2B_OK
+      || (col_basis == row_basis ? ctree_append(&tr->col, &tr->row, 0)
+                                 : h2b_ctree_build(vertices, x, triangles, t, col_basis, clf,
+                                                   &tr->col)) != H2B_OK
       || h2b_blist_build(&tr->row, &tr->col, eta, &tr->blocks) != H2B_OK) {
     h2b_tree_del(tr);
     return NULL;
