@@ -39,9 +39,10 @@ FLOPS_PER_POINT = {"slp": 64, "dlp": 72}
 # column weights per channel 12) + 4 row points x 53 (x_a 12, <x_a, n> 5, 3 x 3 x 2 outer FMAs
 # 36) + 4 column points x 17 (y_b 12, <y_b, n> 5) + 20 for the scaling
 EXECUTED_FLOPS_PER_PAIR = 16 * 37 + 4 * 53 + 4 * 17 + 20
-# DRAM bytes (read + write) of one near_dist_kernel launch on this workload from an ncu capture
-# of the full-size run (dram__bytes_read.sum + dram__bytes_write.sum); None until captured
-NEAR_DIST_TRAFFIC = None
+# DRAM bytes (read 7,302,656 + write 215,154,688) of one near_dist_kernel launch on the default
+# workload (sphere split 64), from an ncu capture of the full-size run (single-pass metrics
+# dram__bytes_read.sum + dram__bytes_write.sum)
+NEAR_DIST_TRAFFIC = 7302656 + 215154688
 
 
 def parse():
@@ -272,7 +273,7 @@ def run_ours(a, rank, world, local):
     executed = pc["distant"] * EXECUTED_FLOPS_PER_PAIR
     roofline = {"bound": "fp64", "kernel": "near_dist_kernel (fused SLP+DLP, linear basis)",
                 "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
-                "traffic": NEAR_DIST_TRAFFIC,
+                "traffic": NEAR_DIST_TRAFFIC if (a.split, a.clf, a.m) == (64, 64, 4) else None,
                 "executed_flops_per_launch": executed,
                 "executed_tflops": executed / (near_dist_ms * 1e-3) / 1e12,
                 "executed_frac": executed / (near_dist_ms * 1e-3) / 1e12 / peak,
