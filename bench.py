@@ -63,6 +63,7 @@ def parse():
     p.add_argument("--plain-sample", type=int, default=16)
     p.add_argument("--no-serving", action="store_true")
     p.add_argument("--no-helmholtz", action="store_true")
+    p.add_argument("--no-mixed", action="store_true")
     p.add_argument("--serve-requests", type=int, default=48)
     p.add_argument("--serve-rates", default="50,200,1000,2000")
     return p.parse_args()
@@ -327,6 +328,45 @@ def run_ours(a, rank, world, local):
                  "rel_residual": hb.residual_norm([V], [1.0], b, u),
                  "reference_iterations": 161, "reference_rel_l2_error": 2.297e-2}
 
+    # ---- mixed precision: the same assembly with FP32 distant-pair quadrature (singular pairs,
+    # bases and coupling FP64), then GMRES with FP32 Arnoldi products and FP64 residuals
+    mixed = None
+    if not a.no_mixed:
+        for h in (V, K):
+            h.set_precision(True)
+        for _ in range(a.warmup):
+            step()
+        mdev = []
+        for _ in range(a.steps):
+            flush.fill_(1.0)
+            torch.cuda.synchronize()
+            mdev.append(step()[0])
+        m_ms = dist_max(statistics.mean(mdev), world)
+        tv, tk = V.timings(), K.timings()
+        mixed = {"value": world * entries / (m_ms * 1e-3), "unit": UNIT, "ms_per_step": m_ms,
+                 "near_distant_ms": tv["near_distant"] + tk["near_distant"],
+                 "quadrature": "distant pairs FP32 (q=2), singular pairs / bases / coupling FP64"}
+        if not a.no_solve:
+            gD = hb.project_l2_harmonic(dlp, Z)
+            bm = hb.addeval_h2matrix_avector(1.0, K, gD, np.zeros(K.rows))
+            V.make_single()
+            um = np.zeros(V.rows)
+            hb.solve_gmres_mixed([V], [1.0], bm, um, 1e-8, 1000, 50)  # warm-up
+            um[:] = 0.0
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            itm = hb.solve_gmres_mixed([V], [1.0], bm, um, 1e-8, 1000, 50)
+            t_m = time.perf_counter() - t0
+            err, nrm = hb.l2_error_harmonic(slp, Z, um)
+            mixed["solve"] = {"seconds": t_m, "solves_per_s": 1.0 / t_m, "iterations": itm,
+                              "rel_residual_fp64": hb.residual_norm([V], [1.0], bm, um),
+                              "rel_l2_error_neumann": err / nrm,
+                              "rel_diff_to_fp64_solution":
+                                  float(np.linalg.norm(um - u) / np.linalg.norm(u))
+                                  if solve else None}
+        for h in (V, K):
+            h.set_precision(False)
+
     # ---- e2e: the same assembly through the C ABI from host arrays, results copied to host
     e2e = None
     if not a.no_e2e:
@@ -387,7 +427,8 @@ def run_ours(a, rank, world, local):
                      for k in ("row_basis", "col_basis", "coupling")} |
                     {"near_distant_fused": near_dist_ms, "near_singular_fused": near_sing_ms},
         "pairs_per_operator": pc, "singular_points": sing_points,
-        "roofline": roofline, "roofline_matvec": roof_mv, "solve": solve, "e2e": e2e,
+        "roofline": roofline, "roofline_matvec": roof_mv, "solve": solve, "mixed": mixed,
+        "e2e": e2e,
         "clocks": clocks.summary(),
         "gpu_launches": a.steps * 12,
     }

@@ -250,6 +250,11 @@ class H2Matrix:
         check(lib.h2b_h2matrix_assemble_all(self.handle), "h2matrix_assemble_all")
         return self
 
+    def set_precision(self, fp32):
+        """FP32 (True) or FP64 (False, default) distant-pair quadrature for later assembly."""
+        check(lib.h2b_h2matrix_set_precision(self.handle, 1 if fp32 else 0), "set_precision")
+        return self
+
     def make_single(self):
         """FP32 copies of N, S and the flattened bases for mixed-precision products."""
         check(lib.h2b_h2matrix_make_single(self.handle), "h2matrix_make_single")

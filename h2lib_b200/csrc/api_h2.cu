@@ -500,6 +500,19 @@ static void drop_single(h2b_h2matrix *h) {
   h2b_h2_fill_mvm_plan(h);
 }
 
+extern "C" int h2b_h2matrix_set_precision(h2b_h2matrix *h, int precision) {
+  if (!h || (precision != H2B_FP64 && precision != H2B_FP32)) {
+    h2b_set_error("h2b_h2matrix_set_precision: precision must be H2B_FP64 or H2B_FP32");
+    return H2B_ERR_ARG;
+  }
+  if (precision == H2B_FP32 && h->bem->q != 2) {
+    h2b_set_error("h2b_h2matrix_set_precision: FP32 quadrature needs the regular order q = 2");
+    return H2B_ERR_ARG;
+  }
+  h->quad_fp32 = precision == H2B_FP32;
+  return H2B_OK;
+}
+
 extern "C" int h2b_h2matrix_make_single(h2b_h2matrix *h) {
   if (!h) return H2B_ERR_ARG;
   if (!h->flat) {
@@ -588,6 +601,7 @@ static int launch_near(h2b_h2matrix *h, h2b_h2matrix *h2) {
   L.nsing = h->nsing;
   L.out0 = h->d_N;
   L.ev_between = h->ev[7];
+  L.fp32 = h->quad_fp32;
   if (h2) {
     L.kk = H2B_KK_LBOTH;
     L.out1 = h2->d_N;

@@ -45,6 +45,7 @@ struct h2b_h2matrix {
   uint32_t m = 0, k = 0, ns = 0;
   int cx = 0, num_sms = 148;
   int flat = 1;  // matvec through flattened bases (W_t) instead of the nested transforms
+  int quad_fp32 = 0;  // distant-pair quadrature in FP32 (h2b_h2matrix_set_precision)
   cudaStream_t st = nullptr;
   DevCTree rt, ct;
   uint32_t nadm = 0, nnear = 0, ntiles = 0, nsing = 0;

@@ -31,6 +31,11 @@ namespace {
 
 constexpr int TPB = 256;
 constexpr int KMAXW = 2 * 128;  // k <= 128 complex coefficients
+// independent matrix loads in flight per thread in the GEMV loops
+#ifndef H2B_MVM_UNROLL
+#define H2B_MVM_UNROLL 8
+#endif
+constexpr int MVM_UNROLL = H2B_MVM_UNROLL;
 
 // xp = x[idx] (cluster order)
 template <bool CX>
@@ -79,7 +84,7 @@ __device__ __forceinline__ void gemv_split(const TP *__restrict__ P, uint32_t ld
   const uint32_t t = threadIdx.x, r = t % nrows, g = t / nrows;
   double sr = 0.0, si = 0.0;
   if (g < G) {
-#pragma unroll 4
+#pragma unroll MVM_UNROLL
     for (uint32_t c = g; c < ncols; c += G) {
       const double p = (double) P[r + (size_t) c * ld];
       const double vr = VGLOBAL ? __ldcg(v + W * c) : v[W * c];
@@ -116,7 +121,7 @@ __device__ __forceinline__ void panel_mv_atomic(const TM *__restrict__ M, uint32
     const uint32_t rl = threadIdx.x % rb, r = r0 + rl, g = threadIdx.x / rb;
     if (g < groups && r < rows) {
       double sr = 0.0, si = 0.0;
-#pragma unroll 4
+#pragma unroll MVM_UNROLL
       for (uint32_t j = g; j < cols; j += groups) {
         const size_t e = (size_t) r + (size_t) j * rows;
         if (CX) {

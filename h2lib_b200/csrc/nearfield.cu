@@ -215,6 +215,109 @@ __device__ __forceinline__ void dist_pair_tensor(const PairGeo &g, double n0, do
   }
 }
 
+// FP32 variant of dist_pair_tensor (mixed-precision assembly): the pair geometry is formed in
+// FP64 relative to the column triangle's first vertex and rounded once; points, kernel values
+// (rsqrtf, sincosf, expf) and the q^4 sums run in FP32; the pair's sums are widened to FP64
+// before they are added to the tile.  Entries carry FP32 accuracy (~1e-7 relative).
+__constant__ float c_side_f[5][6][SIDE_MAXP];
+
+template <int KK>
+__device__ __forceinline__ void eval_kernel_f(float r2, float dot, float k_re, float k_imn,
+                                              float kv[2]) {
+  const float rinv = rsqrtf(r2);
+  if constexpr (KK == KK_LSLP) {
+    kv[0] = rinv;
+  } else if constexpr (KK == KK_LDLP) {
+    kv[0] = dot * (rinv * rinv * rinv);
+  } else if constexpr (KK == KK_LBOTH) {
+    kv[0] = rinv;
+    kv[1] = dot * (rinv * rinv * rinv);
+  } else if constexpr (KK == KK_HSLP) {
+    float r = r2 * rinv, rn = rinv, s, c;
+    if (k_imn != 0.0f) rn *= expf(k_imn * r);
+    sincosf(k_re * r, &s, &c);
+    kv[0] = rn * c;
+    kv[1] = rn * s;
+  } else {  // KK_HDLP
+    float re = (rinv * rinv * rinv) * dot, r = r2 * rinv, s, c;
+    if (k_imn != 0.0f) re *= expf(k_imn * r);
+    const float kr = k_re * r;
+    sincosf(kr, &s, &c);
+    kv[0] = fmaf(kr, s, c) * re;
+    kv[1] = fmaf(-c, kr, s) * re;
+  }
+}
+
+template <int Q, int KK, bool RL, bool CL>
+__device__ __forceinline__ void dist_pair_tensor_f32(const PairGeo &g, double n0d, double n1d,
+                                                     double n2d, double k_re, double k_imn,
+                                                     double (&acc)[KT<KK>::NCH][RL ? 3 : 1][CL ? 3 : 1]) {
+  constexpr int NCH = KT<KK>::NCH, NC = CL ? 3 : 1, NR = RL ? 3 : 1, P = Q * Q;
+  constexpr bool DOT = uses_normal<KK>();
+  const float(&sd)[6][SIDE_MAXP] = c_side_f[Q - 1];
+  const float n0 = (float) n0d, n1 = (float) n1d, n2 = (float) n2d;
+  const float kr = (float) k_re, ki = (float) k_imn;
+  float d0[3], p1[3], p2[3], q1[3], q2[3];
+#pragma unroll
+  for (int d = 0; d < 3; d++) {
+    d0[d] = (float) g.d0[d];
+    p1[d] = (float) g.p1[d];
+    p2[d] = (float) g.p2[d];
+    q1[d] = (float) g.q1[d];
+    q2[d] = (float) g.q2[d];
+  }
+  float yb[P][3], nyb[P];
+#pragma unroll
+  for (int b = 0; b < P; b++) {
+#pragma unroll
+    for (int d = 0; d < 3; d++) yb[b][d] = fmaf(sd[1][b], q2[d], sd[0][b] * q1[d]);
+    nyb[b] = DOT ? fmaf(yb[b][0], n0, fmaf(yb[b][1], n1, yb[b][2] * n2)) : 0.0f;
+  }
+  float accf[NCH][NR][NC];
+#pragma unroll
+  for (int c = 0; c < NCH; c++)
+#pragma unroll
+    for (int i = 0; i < NR; i++)
+#pragma unroll
+      for (int j = 0; j < NC; j++) accf[c][i][j] = 0.0f;
+#pragma unroll
+  for (int a = 0; a < P; a++) {
+    float xa[3];
+#pragma unroll
+    for (int d = 0; d < 3; d++) xa[d] = fmaf(sd[1][a], p2[d], fmaf(sd[0][a], p1[d], d0[d]));
+    const float nxa = DOT ? fmaf(xa[0], n0, fmaf(xa[1], n1, xa[2] * n2)) : 0.0f;
+    float in[NCH][NC];
+#pragma unroll
+    for (int c = 0; c < NCH; c++)
+#pragma unroll
+      for (int j = 0; j < NC; j++) in[c][j] = 0.0f;
+#pragma unroll
+    for (int b = 0; b < P; b++) {
+      const float dx = xa[0] - yb[b][0], dy = xa[1] - yb[b][1], dz = xa[2] - yb[b][2];
+      const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+      float kv[2];
+      eval_kernel_f<KK>(r2, nxa - nyb[b], kr, ki, kv);
+#pragma unroll
+      for (int c = 0; c < NCH; c++)
+#pragma unroll
+        for (int j = 0; j < NC; j++) in[c][j] = fmaf(sd[CL ? 3 + j : 2][b], kv[c], in[c][j]);
+    }
+#pragma unroll
+    for (int c = 0; c < NCH; c++)
+#pragma unroll
+      for (int i = 0; i < NR; i++)
+#pragma unroll
+        for (int j = 0; j < NC; j++)
+          accf[c][i][j] = fmaf(sd[RL ? 3 + i : 2][a], in[c][j], accf[c][i][j]);
+  }
+#pragma unroll
+  for (int c = 0; c < NCH; c++)
+#pragma unroll
+    for (int i = 0; i < NR; i++)
+#pragma unroll
+      for (int j = 0; j < NC; j++) acc[c][i][j] = (double) accf[c][i][j];
+}
+
 struct DistArgs {
   const TriRec *tri;
   const TriRef *refs;
@@ -225,10 +328,10 @@ struct DistArgs {
 };
 
 // Shared-memory accumulator tile: [NOUT*(CPLX?2:1)][64*64] doubles.
-template <int Q, int KK, bool RL, bool CL>
 #ifndef H2B_DIST_MINBLOCKS
 #define H2B_DIST_MINBLOCKS 2
 #endif
+template <int Q, int KK, bool RL, bool CL, bool F32 = false>
 __global__ void __launch_bounds__(256, H2B_DIST_MINBLOCKS) near_dist_kernel(DistArgs a) {
   constexpr int NCH = KT<KK>::NCH;
   constexpr int NR = RL ? 3 : 1, NC = CL ? 3 : 1;
@@ -283,7 +386,10 @@ __global__ void __launch_bounds__(256, H2B_DIST_MINBLOCKS) near_dist_kernel(Dist
 
     if constexpr (Q > 0) {
 #if H2B_DIST_TENSOR
-      dist_pair_tensor<Q, KK, RL, CL>(g, n0, n1, n2, a.k_re, a.k_imn, acc);
+      if constexpr (F32)
+        dist_pair_tensor_f32<Q, KK, RL, CL>(g, n0, n1, n2, a.k_re, a.k_imn, acc);
+      else
+        dist_pair_tensor<Q, KK, RL, CL>(g, n0, n1, n2, a.k_re, a.k_imn, acc);
 #else
 #pragma unroll
       for (int k = 0; k < Q * Q * Q * Q; k++)
@@ -508,13 +614,13 @@ __global__ void __launch_bounds__(SING_THREADS, 1) near_sing_kernel(SingArgs a) 
   }
 }
 
-template <int Q, int KK, bool RL, bool CL>
+template <int Q, int KK, bool RL, bool CL, bool F32 = false>
 int launch_dist(const h2b_near_launch *L, cudaStream_t st) {
   constexpr int PLANES = KT<KK>::CPLX ? 2 : KT<KK>::NOUT;
   const size_t smem = sizeof(double) * PLANES * H2B_TILE_MAX * H2B_TILE_MAX;
   static bool attr_set = false;
   if (!attr_set) {
-    H2B_CUDA_TRY(cudaFuncSetAttribute(near_dist_kernel<Q, KK, RL, CL>,
+    H2B_CUDA_TRY(cudaFuncSetAttribute(near_dist_kernel<Q, KK, RL, CL, F32>,
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem));
     attr_set = true;
   }
@@ -528,7 +634,7 @@ int launch_dist(const h2b_near_launch *L, cudaStream_t st) {
   a.k_re = L->k_re;
   a.k_imn = L->k_imn;
   a.q = (int) L->q;
-  if (L->ntiles > 0) near_dist_kernel<Q, KK, RL, CL><<<L->ntiles, 256, smem, st>>>(a);
+  if (L->ntiles > 0) near_dist_kernel<Q, KK, RL, CL, F32><<<L->ntiles, 256, smem, st>>>(a);
   H2B_CUDA_TRY(cudaGetLastError());
   return H2B_OK;
 }
@@ -578,7 +684,9 @@ int launch_sing(const h2b_near_launch *L, cudaStream_t st) {
 template <int KK, bool RL, bool CL>
 int launch_kk_basis(const h2b_near_launch *L, cudaStream_t st) {
   int rc;
-  if (L->q == 2)
+  if (L->q == 2 && L->fp32)
+    rc = launch_dist<2, KK, RL, CL, true>(L, st);
+  else if (L->q == 2)
     rc = launch_dist<2, KK, RL, CL>(L, st);
   else
     rc = launch_dist<0, KK, RL, CL>(L, st);
@@ -730,6 +838,11 @@ extern "C" int h2b_near_upload_dist_rules(void) {
       }
   }
   H2B_CUDA_TRY(cudaMemcpyToSymbol(c_side, side, sizeof(side)));
+  static float side_f[5][6][SIDE_MAXP];
+  for (int q = 0; q < 5; q++)
+    for (int r = 0; r < 6; r++)
+      for (int p = 0; p < SIDE_MAXP; p++) side_f[q][r][p] = (float) side[q][r][p];
+  H2B_CUDA_TRY(cudaMemcpyToSymbol(c_side_f, side_f, sizeof(side_f)));
   return H2B_OK;
 }
 

@@ -37,6 +37,7 @@ typedef struct {
   int num_sms;
   int *err;                      /* device flag */
   cudaEvent_t ev_between;        /* optional: recorded between the distant and singular kernels */
+  int fp32;                      /* 1: distant pairs in FP32 (q = 2 only); singular pairs stay FP64 */
 } h2b_near_launch;
 
 int h2b_near_upload_dist_rules(void);

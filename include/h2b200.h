@@ -219,6 +219,13 @@ int h2b_h2matrix_assemble_nearfield_pair(h2b_h2matrix *a, h2b_h2matrix *b);
  * [7] rank k. */
 int h2b_h2matrix_info(const h2b_h2matrix *h2, uint64_t info[8]);
 
+/* Precision of the regular (distant-pair) nearfield quadrature of later assembly calls:
+ * H2B_FP64 (default; entries match the reference to 1e-12) or H2B_FP32 (points, kernel values
+ * and sums in FP32 for q = 2, about 1e-7 relative in those entries; singular pairs, bases and
+ * coupling matrices stay FP64).  The mixed-precision assembly of a solve whose FP64 residual is
+ * driven to 1e-8 on this operator; no counterpart in the reference (FP64 only). */
+int h2b_h2matrix_set_precision(h2b_h2matrix *h2, int precision);
+
 /* FP32 copies of the nearfield blocks, coupling matrices and flattened cluster bases, read by the
  * mixed-precision matvec (half the bytes of the FP64 product).  Call after assembly; any later
  * assembly call drops the copies.  No counterpart in the reference (FP64 only). */

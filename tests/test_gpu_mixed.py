@@ -83,3 +83,36 @@ def test_batched_mixed_multi_rhs():
                                             np.zeros(n))
             res = np.linalg.norm(B[r, lo:hi] - y[lo:hi]) / np.linalg.norm(B[r, lo:hi])
             assert res <= 1.0001e-8
+
+
+def test_fp32_quadrature_operator():
+    """FP32 distant-pair quadrature: entries within FP32 accuracy of the FP64 ones, and the
+    mixed solve on that operator meets the FP64 tolerance with a solution close to the FP64
+    one and the same analytic error."""
+    gr = hb.new_sphere_surface3d(16)
+    slp = hb.new_slp_laplace_bem3d(gr, 2, 4, L, L)
+    dlp = hb.new_dlp_laplace_bem3d(gr, 2, 4, L, L, 0.5)
+    tree = hb.build_tree(gr, L, L, 64, 1.4)
+    V64 = hb.H2Matrix(slp, tree, 4).assemble()
+    K64 = hb.H2Matrix(dlp, tree, 4).assemble()
+    V32 = hb.H2Matrix(slp, tree, 4).set_precision(True).assemble()
+    K32 = hb.H2Matrix(dlp, tree, 4).set_precision(True).assemble()
+    for a, b in ((V32, V64), (K32, K64)):
+        n32, n64 = a.export(5), b.export(5)
+        d = relerr(n32, n64)
+        assert 1e-11 < d < 1e-6
+        np.testing.assert_array_equal(a.export(4), b.export(4))  # coupling stays FP64
+    gD = hb.project_l2_harmonic(dlp, Z)
+    b64 = hb.addeval_h2matrix_avector(1.0, K64, gD, np.zeros(K64.rows))
+    b32 = hb.addeval_h2matrix_avector(1.0, K32, gD, np.zeros(K32.rows))
+    assert relerr(b32, b64) < 1e-6
+    u64 = np.zeros(V64.rows)
+    hb.solve_gmres_h2matrix_avector(V64, b64, u64, 1e-8, 1000, 50)
+    V32.make_single()
+    u = np.zeros(V32.rows)
+    hb.solve_gmres_mixed([V32], [1.0], b32, u, 1e-8, 1000, 50)
+    assert hb.residual_norm([V32], [1.0], b32, u) <= 1.0001e-8
+    assert relerr(u, u64) < 1e-5
+    e32, nrm = hb.l2_error_harmonic(slp, Z, u)
+    e64, _ = hb.l2_error_harmonic(slp, Z, u64)
+    assert abs(e32 - e64) < 1e-4 * nrm
