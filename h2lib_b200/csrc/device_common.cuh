@@ -73,6 +73,18 @@ __device__ __forceinline__ double rsqrt_nr(double x) {
 #endif
 }
 
+// Allow kernel K up to H2B_MAX_DYN_SMEM bytes of dynamic shared memory, once per process
+// (thread-safe static initialisation).  Launches pass the size they need; the attribute never
+// changes afterwards, so launches from several host threads (a solve server's workers) cannot
+// race on it.
+#define H2B_MAX_DYN_SMEM (200u * 1024u)
+template <auto K>
+inline cudaError_t h2b_allow_smem() {
+  static const cudaError_t rc = cudaFuncSetAttribute(
+      K, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) H2B_MAX_DYN_SMEM);
+  return rc;
+}
+
 struct dcomplex {
   double re, im;
 };

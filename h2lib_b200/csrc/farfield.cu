@@ -197,8 +197,7 @@ extern "C" int h2b_far_leaf_basis(const FarLeafArgs *a, int linear, int dn, cuda
   }
 #define LAUNCH(L, D)                                                                        \
   do {                                                                                      \
-    H2B_CUDA_TRY(cudaFuncSetAttribute(leaf_basis_kernel<L, D>,                             \
-                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem)); \
+    H2B_CUDA_TRY((h2b_allow_smem<leaf_basis_kernel<L, D>>()));                             \
     leaf_basis_kernel<L, D><<<a->nleaves, 256, smem, st>>>(*a);                             \
   } while (0)
   if (linear && dn) LAUNCH(true, true);

@@ -166,12 +166,11 @@ extern "C" int h2b_flat_leaves(const FlatLeafArgs *a, cudaStream_t st) {
 extern "C" int h2b_flat_level(const FlatArgs *a, cudaStream_t st) {
   if (a->nitems == 0) return H2B_OK;
   const size_t smem = sizeof(double) * ((size_t) a->k * a->k + (size_t) H2B_FLAT_ROWS * a->k);
-  static size_t attr = 0;
-  if (smem > 48 * 1024 && smem > attr) {
-    H2B_CUDA_TRY(cudaFuncSetAttribute(flatten_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int) smem));
-    attr = smem;
+  if (smem > H2B_MAX_DYN_SMEM) {
+    h2b_set_error("flattened bases: rank %d needs %zu bytes of shared memory", a->k, smem);
+    return H2B_ERR_ARG;
   }
+  H2B_CUDA_TRY(h2b_allow_smem<flatten_kernel>());
   flatten_kernel<<<a->nitems, FLAT_TPB, smem, st>>>(*a);
   H2B_CUDA_TRY(cudaGetLastError());
   return H2B_OK;

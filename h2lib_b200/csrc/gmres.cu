@@ -127,11 +127,38 @@ __device__ __forceinline__ void put_part(const GmresDev &g, const Sys &v, uint32
   v.part[(size_t) lb * g.ldpart * 2 + 2 * j + 1] = im;
 }
 
+// part[lb][j] = sum over this CTA's rows of pj(j), for j = 0..k: one warp reduction per j into
+// shared memory and a single barrier, instead of a block-wide reduction (two barriers) per j.
+template <bool CX, typename F>
+__device__ __forceinline__ void block_dots(const GmresDev &g, const Sys &v, uint32_t lb,
+                                           uint32_t k, F pj) {
+  __shared__ double ws[2][TPB / 32][GMRES_KMAX + 1];
+  const uint32_t lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  for (uint32_t j = 0; j <= k; j++) {
+    const cd p = pj(j);
+    const double sr = warp_sum(p.re);
+    const double si = CX ? warp_sum(p.im) : 0.0;
+    if (lane == 0) {
+      ws[0][w][j] = sr;
+      ws[1][w][j] = si;
+    }
+  }
+  __syncthreads();
+  for (uint32_t j = threadIdx.x; j <= k; j += blockDim.x) {
+    double sr = 0.0, si = 0.0;
+#pragma unroll
+    for (int q = 0; q < TPB / 32; q++) {
+      sr += ws[0][q][j];
+      si += ws[1][q][j];
+    }
+    put_part(g, v, lb, j, sr, si);
+  }
+}
+
 // The new Krylov vector a = A q (in abuf) is moved into column k+1 of qr, and the partial sums
 // part[b][j] = sum_{i in block b} conj(V[i,j]) a[i] (j <= k) of w = V_{0..k}^H a are formed.
 template <bool CX>
 __global__ void __launch_bounds__(TPB) vth_kernel(GmresDev g) {
-  __shared__ double red[2][TPB / 32];
   Sys v;
   uint32_t i, lb;
   if (!vec_view<CX>(g, GMRES_SEL_ACTIVE, v, i, lb)) return;
@@ -140,14 +167,9 @@ __global__ void __launch_bounds__(TPB) vth_kernel(GmresDev g) {
   const bool in = i < v.n;
   const cd x = in ? ld<CX>(v.abuf, i) : cd{0.0, 0.0};
   if (in) st<CX>(col, i, x);
-  for (uint32_t j = 0; j <= k; j++) {
-    cd p = {0.0, 0.0};
-    if (in) p = cmul(cconj(vij<CX>(v, i, j)), x);
-    const double sr = block_sum(p.re, red[0]);
-    double si = 0.0;
-    if (CX) si = block_sum(p.im, red[1]);
-    if (threadIdx.x == 0) put_part(g, v, lb, j, sr, si);
-  }
+  block_dots<CX>(g, v, lb, k, [&](uint32_t j) {
+    return in ? cmul(cconj(vij<CX>(v, i, j)), x) : cd{0.0, 0.0};
+  });
 }
 
 // a -= V u over rows (columns 0..k), then partial norm^2 of a[k+1..n)
@@ -181,7 +203,6 @@ __global__ void __launch_bounds__(TPB) apply_v_norm_kernel(GmresDev g) {
 // scale a[i > k+1] *= gamma, a[k+1] = alpha; partial z_j = sum_{i>k+1} conj(V[i,j]) a[i]
 template <bool CX>
 __global__ void __launch_bounds__(TPB) scale_vth_kernel(GmresDev g) {
-  __shared__ double red[2][TPB / 32];
   Sys v;
   uint32_t i, lb;
   if (!vec_view<CX>(g, GMRES_SEL_ACTIVE, v, i, lb)) return;
@@ -189,19 +210,15 @@ __global__ void __launch_bounds__(TPB) scale_vth_kernel(GmresDev g) {
   const cd gamma = {v.state->gamma_re, v.state->gamma_im};
   double *a = v.qr + (size_t) (CX ? 2 : 1) * (k + 1) * v.n;
   cd x = {0.0, 0.0};
-  if (i < v.n && i > k + 1) {
+  const bool below = i < v.n && i > k + 1;
+  if (below) {
     x = cmul(ld<CX>(a, i), gamma);
     st<CX>(a, i, x);
   }
   if (i == k + 1 && i < v.n) st<CX>(a, i, cd{v.state->alpha_re, v.state->alpha_im});
-  for (uint32_t j = 0; j <= k; j++) {
-    cd p = {0.0, 0.0};
-    if (i < v.n && i > k + 1) p = cmul(cconj(vij<CX>(v, i, j)), x);
-    const double sr = block_sum(p.re, red[0]);
-    double si = 0.0;
-    if (CX) si = block_sum(p.im, red[1]);
-    if (threadIdx.x == 0) put_part(g, v, lb, j, sr, si);
-  }
+  block_dots<CX>(g, v, lb, k, [&](uint32_t j) {
+    return below ? cmul(cconj(vij<CX>(v, i, j)), x) : cd{0.0, 0.0};
+  });
 }
 
 // q = e_{k} - V_{0..k} u  (k = current dimension after the step)
@@ -385,28 +402,48 @@ __global__ void __launch_bounds__(SMALL_THREADS) small_kernel(GmresDev g, int ph
       v.u[2 * t] = acc.re;
       v.u[2 * t + 1] = acc.im;
     }
-    if (t != 0) return;
-    // Givens rotations on the new Hessenberg column (rows 0..k+1 of column k+1)
+    // Givens rotations on the new Hessenberg column (rows 0..k+1 of column k+1): the column and
+    // the stored rotations (diagonal of the previous columns) are staged in shared memory, so the
+    // sequential sweep by one thread never waits on global memory.
     double *col = v.qr + (size_t) (CX ? 2 : 1) * (k + 1) * v.n;
-    for (uint32_t i = 0; i < k; i++) {
-      const cd rho = ld<CX>(v.qr + (size_t) (CX ? 2 : 1) * (i + 1) * v.n, i + 1);
-      cd a = ld<CX>(col, i), b = ld<CX>(col, i + 1);
-      apply_givens(rho, &a, &b);
-      st<CX>(col, i, a);
-      st<CX>(col, i + 1, b);
+    if (t <= k + 1) {
+      const cd c = ld<CX>(col, t);
+      wr[t] = c.re;
+      wi[t] = c.im;
     }
-    cd a = ld<CX>(col, k), b = ld<CX>(col, k + 1);
-    const cd rho = findapply_givens(&a, &b);
-    st<CX>(col, k, a);
-    st<CX>(col, k + 1, rho);
-    cd r0 = {v.rhat[2 * k], v.rhat[2 * k + 1]}, r1 = {v.rhat[2 * (k + 1)], v.rhat[2 * (k + 1) + 1]};
-    apply_givens(rho, &r0, &r1);
-    v.rhat[2 * k] = r0.re;
-    v.rhat[2 * k + 1] = r0.im;
-    v.rhat[2 * (k + 1)] = r1.re;
-    v.rhat[2 * (k + 1) + 1] = r1.im;
-    s->k = k + 1;
-    s->err = sqrt(cabs2(r1));
+    if (t < k) {
+      const cd r = ld<CX>(v.qr + (size_t) (CX ? 2 : 1) * (t + 1) * v.n, t + 1);
+      zr[t] = r.re;
+      zi[t] = r.im;
+    }
+    __syncthreads();
+    if (t == 0) {
+      for (uint32_t i = 0; i < k; i++) {
+        cd a = {wr[i], wi[i]}, b = {wr[i + 1], wi[i + 1]};
+        apply_givens(cd{zr[i], zi[i]}, &a, &b);
+        wr[i] = a.re;
+        wi[i] = a.im;
+        wr[i + 1] = b.re;
+        wi[i + 1] = b.im;
+      }
+      cd a = {wr[k], wi[k]}, b = {wr[k + 1], wi[k + 1]};
+      const cd rho = findapply_givens(&a, &b);
+      wr[k] = a.re;
+      wi[k] = a.im;
+      wr[k + 1] = rho.re;  // the rotation is stored below the diagonal
+      wi[k + 1] = rho.im;
+      cd r0 = {v.rhat[2 * k], v.rhat[2 * k + 1]},
+         r1 = {v.rhat[2 * (k + 1)], v.rhat[2 * (k + 1) + 1]};
+      apply_givens(rho, &r0, &r1);
+      v.rhat[2 * k] = r0.re;
+      v.rhat[2 * k + 1] = r0.im;
+      v.rhat[2 * (k + 1)] = r1.re;
+      v.rhat[2 * (k + 1) + 1] = r1.im;
+      s->k = k + 1;
+      s->err = sqrt(cabs2(r1));
+    }
+    __syncthreads();
+    if (t <= k + 1) st<CX>(col, t, cd{wr[t], wi[t]});
   } else if (phase == 3) {
     // finish: rhat_k = R^{-1} rhat_k (back substitution, row by row); z = V_k^H rhat;
     // u = T_k z

@@ -618,12 +618,7 @@ template <int Q, int KK, bool RL, bool CL, bool F32 = false>
 int launch_dist(const h2b_near_launch *L, cudaStream_t st) {
   constexpr int PLANES = KT<KK>::CPLX ? 2 : KT<KK>::NOUT;
   const size_t smem = sizeof(double) * PLANES * H2B_TILE_MAX * H2B_TILE_MAX;
-  static bool attr_set = false;
-  if (!attr_set) {
-    H2B_CUDA_TRY(cudaFuncSetAttribute(near_dist_kernel<Q, KK, RL, CL, F32>,
-                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem));
-    attr_set = true;
-  }
+  H2B_CUDA_TRY((h2b_allow_smem<near_dist_kernel<Q, KK, RL, CL, F32>>()));
   DistArgs a;
   a.tri = (const TriRec *) L->tri;
   a.refs = (const TriRef *) L->refs;
@@ -644,12 +639,7 @@ int launch_sing(const h2b_near_launch *L, cudaStream_t st) {
   if (L->nsing == 0) return H2B_OK;
   const int staged = sizeof(double) * L->rule_total <= 200u * 1024u;
   const size_t smem = staged ? sizeof(double) * L->rule_total : 0;
-  static size_t attr_set = 0;
-  if (smem > attr_set) {
-    H2B_CUDA_TRY(cudaFuncSetAttribute(near_sing_kernel<KK, RL, CL>,
-                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem));
-    attr_set = smem;
-  }
+  H2B_CUDA_TRY((h2b_allow_smem<near_sing_kernel<KK, RL, CL>>()));
   SingArgs a;
   a.tri = (const TriRec *) L->tri;
   a.refs = (const TriRef *) L->refs;

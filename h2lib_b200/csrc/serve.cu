@@ -109,6 +109,11 @@ int run_request(Req *q) {
                               : nullptr;
   h2b_h2matrix *V = tr ? h2b_h2matrix_new(slp, tr, m) : nullptr;
   h2b_h2matrix *K = tr ? h2b_h2matrix_new(dlp, tr, m) : nullptr;
+  // mixed precision: FP32 distant-pair quadrature too (singular pairs stay FP64)
+  if (V && K && (d.flags & H2B_SOLVE_MIXED)) {
+    h2b_h2matrix_set_precision(V, H2B_FP32);
+    h2b_h2matrix_set_precision(K, H2B_FP32);
+  }
   const auto c1 = tick();
   const uint32_t nd = helm ? nt : nv;
   const size_t W = helm ? 2 : 1;
