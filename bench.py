@@ -393,13 +393,19 @@ def run_ours(a, rank, world, local):
                 check(lib.h2b_h2matrix_assemble_row_clusterbasis(h.handle), "row basis")
                 check(lib.h2b_h2matrix_assemble_col_clusterbasis(h.handle), "col basis")
                 check(lib.h2b_h2matrix_assemble_farfield(h.handle), "coupling")
+            # the coupling matrices travel to the host while the nearfield is assembled
+            for name, h in (("Vs", V2), ("Ks", K2)):
+                check(lib.h2b_h2matrix_export_async(h.handle, 4, 0xFFFFFFFF,
+                                                    ctypes.c_void_p(pin[name].data_ptr())),
+                      "export")
             check(lib.h2b_h2matrix_assemble_nearfield_pair(V2.handle, K2.handle), "near pair")
             t4 = time.perf_counter()
-            nd = ctypes.c_uint64()
-            for name, h, part in (("Vn", V2, 5), ("Kn", K2, 5), ("Vs", V2, 4), ("Ks", K2, 4)):
-                check(lib.h2b_h2matrix_export(h.handle, part, 0xFFFFFFFF,
-                                              ctypes.c_void_p(pin[name].data_ptr()),
-                                              ctypes.byref(nd)), "export")
+            for name, h in (("Vn", V2), ("Kn", K2)):
+                check(lib.h2b_h2matrix_export_async(h.handle, 5, 0xFFFFFFFF,
+                                                    ctypes.c_void_p(pin[name].data_ptr())),
+                      "export")
+            for h in (V2, K2):
+                check(lib.h2b_h2matrix_export_wait(h.handle), "export wait")
             t5 = time.perf_counter()
             e2e_times.append(t5 - t0)
             e2e_phases.append({"surface_and_operators": t1 - t0, "trees": t2 - t1,
@@ -413,7 +419,8 @@ def run_ours(a, rank, world, local):
                "d2h_bytes_per_step": int(d2h),
                "includes": "mesh upload, operators, cluster/block trees (host C), H2 structure "
                            "upload, assembly of V and K, copy of all nearfield and coupling "
-                           "blocks to pinned host memory",
+                           "blocks to pinned host memory (coupling copies overlap the nearfield "
+                           "assembly; 'assembly' then includes that overlap)",
                "phase_ms": {k: 1e3 * e2e_phases[e2e_times.index(min(e2e_times))][k]
                             for k in e2e_phases[0]}}
 

@@ -70,6 +70,8 @@ _SIGS = {
     "h2b_h2matrix_timings": (C.c_int, [vp, _f64p]),
     "h2b_h2matrix_pair_counts": (C.c_int, [vp, _u64p]),
     "h2b_h2matrix_export": (C.c_int, [vp, C.c_int, C.c_uint32, vp, C.POINTER(C.c_uint64)]),
+    "h2b_h2matrix_export_async": (C.c_int, [vp, C.c_int, C.c_uint32, vp]),
+    "h2b_h2matrix_export_wait": (C.c_int, [vp]),
     "h2b_h2matrix_addeval": (C.c_int, [C.c_double, C.c_double, vp, vp, vp]),
     "h2b_h2matrix_addeval_multi": (C.c_int, [C.c_double, C.c_double, vp, C.c_uint32, vp,
                                              C.c_uint64, vp, C.c_uint64]),

@@ -207,6 +207,7 @@ extern "C" void h2b_h2matrix_del(h2b_h2matrix *h) {
   if (!h) return;
   cudaStream_t st = h->st;
   if (st) cudaStreamSynchronize(st);
+  if (h->cst) cudaStreamSynchronize(h->cst);  // pending asynchronous exports read the blocks
   devtree_free(h->rt, st);
   devtree_free(h->ct, st);
   dfree(h->rt.f_W, st); dfree(h->ct.f_W, st); dfree(h->f_N, st); dfree(h->f_S, st);
@@ -218,6 +219,11 @@ extern "C" void h2b_h2matrix_del(h2b_h2matrix *h) {
   dfree(h->d_xio, st); dfree(h->d_yio, st);
   for (int e = 0; e < 12; e++)
     if (h->ev[e]) cudaEventDestroy(h->ev[e]);
+  if (h->cst) {
+    cudaStreamSynchronize(h->cst);
+    cudaStreamDestroy(h->cst);
+  }
+  if (h->ev_copy) cudaEventDestroy(h->ev_copy);
   if (h->st) cudaStreamDestroy(h->st);
   delete h;
 }
@@ -770,6 +776,31 @@ extern "C" int h2b_h2matrix_export(const h2b_h2matrix *h, int part, uint32_t cou
       }
     }
   }
+  return H2B_OK;
+}
+
+extern "C" int h2b_h2matrix_export_async(h2b_h2matrix *h, int part, uint32_t count,
+                                         double *out) {
+  if (!h || !out || part == 2 || part == 3 || part < 0 || part > 5) {
+    h2b_set_error("h2b_h2matrix_export_async: parts 0, 1, 4, 5 into a non-NULL buffer");
+    return H2B_ERR_ARG;
+  }
+  uint64_t n = 0;
+  int rc = h2b_h2matrix_export(h, part, count, nullptr, &n);
+  if (rc != H2B_OK || n == 0) return rc;
+  const double *src = part == 0 ? h->rt.d_V : part == 1 ? h->rt.d_E : part == 4 ? h->d_S : h->d_N;
+  if (!h->cst) H2B_CUDA_TRY(cudaStreamCreateWithFlags(&h->cst, cudaStreamNonBlocking));
+  if (!h->ev_copy) H2B_CUDA_TRY(cudaEventCreateWithFlags(&h->ev_copy, cudaEventDisableTiming));
+  // after everything already queued on the matrix's stream, on the copy stream
+  H2B_CUDA_TRY(cudaEventRecord(h->ev_copy, h->st));
+  H2B_CUDA_TRY(cudaStreamWaitEvent(h->cst, h->ev_copy, 0));
+  H2B_CUDA_TRY(cudaMemcpyAsync(out, src, sizeof(double) * n, cudaMemcpyDeviceToHost, h->cst));
+  return H2B_OK;
+}
+
+extern "C" int h2b_h2matrix_export_wait(h2b_h2matrix *h) {
+  if (!h) return H2B_ERR_ARG;
+  if (h->cst) H2B_CUDA_TRY(cudaStreamSynchronize(h->cst));
   return H2B_OK;
 }
 

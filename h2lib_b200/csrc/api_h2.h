@@ -68,6 +68,8 @@ struct h2b_h2matrix {
   // device timings of the last assembly phases (ms): row basis, column basis, coupling,
   // nearfield distant, nearfield singular, matvec
   cudaEvent_t ev[12] = {};
+  cudaStream_t cst = nullptr;     // copy stream of h2b_h2matrix_export_async
+  cudaEvent_t ev_copy = nullptr;
   float ms[6] = {0, 0, 0, 0, 0, 0};
 };
 

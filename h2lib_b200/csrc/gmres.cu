@@ -241,14 +241,26 @@ __global__ void __launch_bounds__(TPB) make_q_kernel(GmresDev g) {
   st<CX>(v.q, i, q);
 }
 
-__device__ cd sum_parts(const GmresDev &g, const Sys &v, uint32_t j) {
-  cd s = {0.0, 0.0};
-  for (uint32_t b = 0; b < v.nblk; b++) {
-    s.re += v.part[(size_t) b * g.ldpart * 2 + 2 * j];
-    s.im += v.part[(size_t) b * g.ldpart * 2 + 2 * j + 1];
+// z[j] = sum over the system's blocks of part[b][j], j <= k: a warp per column, its lanes over
+// the blocks (the blocks' partial sums are read in parallel, not one after another).
+__device__ void sum_parts_all(const GmresDev &g, const Sys &v, uint32_t k, double *zr,
+                              double *zi) {
+  const uint32_t lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  for (uint32_t j = w; j <= k; j += nw) {
+    double sr = 0.0, si = 0.0;
+    for (uint32_t b = lane; b < v.nblk; b += 32) {
+      sr += v.part[(size_t) b * g.ldpart * 2 + 2 * j];
+      si += v.part[(size_t) b * g.ldpart * 2 + 2 * j + 1];
+    }
+    sr = warp_sum(sr);
+    si = warp_sum(si);
+    if (lane == 0) {
+      zr[j] = sr;
+      zi[j] = si;
+    }
   }
-  return s;
 }
+
 
 __device__ __forceinline__ cd Tij(const GmresDev &g, const Sys &v, uint32_t i, uint32_t j) {
   return {v.T[2 * ((size_t) i + (size_t) j * g.kmax)], v.T[2 * ((size_t) i + (size_t) j * g.kmax) + 1]};
@@ -353,14 +365,12 @@ __global__ void __launch_bounds__(SMALL_THREADS) small_kernel(GmresDev g, int ph
   __syncthreads();  // every thread has read k before anyone may change it
   if (phase == 0) {
     // after vth: w = V^H a; u = T^H w
-    if (t <= k) {
-      cd w = sum_parts(g, v, t);
-      zr[t] = w.re;
-      zi[t] = w.im;
-      v.w[2 * t] = w.re;
-      v.w[2 * t + 1] = w.im;
-    }
+    sum_parts_all(g, v, k, zr, zi);
     __syncthreads();
+    if (t <= k) {
+      v.w[2 * t] = zr[t];
+      v.w[2 * t + 1] = zi[t];
+    }
     if (t <= k) {
       cd u = {0.0, 0.0};
       for (uint32_t i = 0; i <= t; i++) u = cadd(u, cmul(cconj(Tij(g, v, i, t)), cd{zr[i], zi[i]}));
@@ -379,8 +389,10 @@ __global__ void __launch_bounds__(SMALL_THREADS) small_kernel(GmresDev g, int ph
   } else if (phase == 2) {
     // after scale_vth: T column k+1; u for q; Givens; k += 1
     const cd tau = {v.tau[2 * (k + 1)], v.tau[2 * (k + 1) + 1]};
-    if (t <= k) {
-      const cd z = cadd(sum_parts(g, v, t), cconj(vij<CX>(v, k + 1, t)));  // + conj(v_t[k+1])
+    sum_parts_all(g, v, k, zr, zi);
+    __syncthreads();
+    if (t <= k) {  // + conj(v_t[k+1])
+      const cd z = cadd(cd{zr[t], zi[t]}, cconj(vij<CX>(v, k + 1, t)));
       zr[t] = z.re;
       zi[t] = z.im;
     }

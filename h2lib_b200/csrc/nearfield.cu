@@ -59,6 +59,10 @@ constexpr int SIDE_MAXP = 25;
 #ifndef H2B_DIST_TENSOR
 #define H2B_DIST_TENSOR 1
 #endif
+// 1: the lanes of a warp visit row triangles spread over the tile's list (see near_dist_kernel)
+#ifndef H2B_DIST_PERMUTE
+#define H2B_DIST_PERMUTE 1
+#endif
 __constant__ double c_side[5][6][SIDE_MAXP];
 
 // Kernel values from r^2 = |x - y|^2 and dot = <x - y, n_y> (n_y: unit normal of the column
@@ -361,8 +365,18 @@ __global__ void __launch_bounds__(256, H2B_DIST_MINBLOCKS) near_dist_kernel(Dist
     cw = &c_dist[4][dist_off(q)];
   }
 
+  // Lanes of a warp take consecutive row positions q of one column triangle.  The row triangles
+  // are visited as it = q * mult mod ntr (a bijection, mult prime and not dividing ntr): the
+  // triangle lists follow the vertex order, so neighbours share vertices, and spreading a warp
+  // over the list keeps its lanes' shared-memory atomics off common entries.
+#if H2B_DIST_PERMUTE
+  const uint32_t mult = (ntr % 17u) ? 17u : 19u;
+#else
+  const uint32_t mult = 1u;
+#endif
   for (uint32_t p = threadIdx.x; p < npairs; p += blockDim.x) {
-    const uint32_t is = p / ntr, it = p - is * ntr;
+    const uint32_t is = p / ntr, q = p - is * ntr;
+    const uint32_t it = (uint32_t) (((uint64_t) q * mult) % ntr);
     const TriRef rt = a.refs[tl.tr_off + it];
     const TriRef st = a.refs[tl.sc_off + is];
     const TriRec &T = a.tri[rt.t];

@@ -255,6 +255,13 @@ int h2b_h2matrix_pair_counts(const h2b_h2matrix *h2, uint64_t counts[4]);
 int h2b_h2matrix_export(const h2b_h2matrix *h2, int part, uint32_t count, double *out,
                         uint64_t *ndoubles);
 
+/* The same copy for parts 0, 1, 4 and 5, queued on the matrix's own copy stream and returning at
+ * once, so that an H2Lib host matrix can be filled while later assembly calls run (for example the
+ * coupling matrices while the nearfield is assembled).  `out` should be pinned host memory for the
+ * copy to overlap; it must stay valid until h2b_h2matrix_export_wait returns. */
+int h2b_h2matrix_export_async(h2b_h2matrix *h2, int part, uint32_t count, double *out);
+int h2b_h2matrix_export_wait(h2b_h2matrix *h2);
+
 /* y += alpha * A x.  Replaces addeval_h2matrix_avector (Library/h2matrix.c:1269): forward
  * transform (Library/clusterbasis.c:524), coupling and nearfield (fastaddeval, Library/h2matrix.c:
  * 1211), backward transform (Library/clusterbasis.c:749).  x has columns, y rows entries of the
