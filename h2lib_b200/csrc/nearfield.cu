@@ -59,9 +59,10 @@ constexpr int SIDE_MAXP = 25;
 #ifndef H2B_DIST_TENSOR
 #define H2B_DIST_TENSOR 1
 #endif
-// 1: the lanes of a warp visit row triangles spread over the tile's list (see near_dist_kernel)
+// 1: the lanes of a warp visit row triangles spread over the tile's list (see near_dist_kernel);
+// measured 3% slower on config 2 than consecutive rows (0, the default), kept as an option
 #ifndef H2B_DIST_PERMUTE
-#define H2B_DIST_PERMUTE 1
+#define H2B_DIST_PERMUTE 0
 #endif
 __constant__ double c_side[5][6][SIDE_MAXP];
 
