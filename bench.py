@@ -228,7 +228,7 @@ def run_ours(a, rank, world, local):
     dlp = hb.new_dlp_laplace_bem3d(gr, 2, 4, L, L, 0.5)
     tree = hb.build_tree(gr, L, L, a.clf, a.eta)
     V = hb.H2Matrix(slp, tree, a.m)
-    K = hb.H2Matrix(dlp, tree, a.m)
+    K = hb.H2Matrix(dlp, tree, a.m, like=V)  # shares V's device structure
     entries = V.info()["near_entries"] + K.info()["near_entries"]
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
 
@@ -387,7 +387,8 @@ def run_ours(a, rank, world, local):
             t1 = time.perf_counter()
             tr2 = hb.build_tree(g2, L, L, a.clf, a.eta)
             t2 = time.perf_counter()
-            V2, K2 = hb.H2Matrix(s2, tr2, a.m), hb.H2Matrix(d2, tr2, a.m)
+            V2 = hb.H2Matrix(s2, tr2, a.m)
+            K2 = hb.H2Matrix(d2, tr2, a.m, like=V2)
             t3 = time.perf_counter()
             for h in (V2, K2):
                 check(lib.h2b_h2matrix_assemble_row_clusterbasis(h.handle), "row basis")
@@ -480,7 +481,8 @@ def run_batched(a):
         slp = hb.new_slp_laplace_bem3d(gu, 2, 4, L, L)
         dlp = hb.new_dlp_laplace_bem3d(gu, 2, 4, L, L, 0.5)
         forest = hb.build_forest(gu, voff, toff, L, L, a.clf, a.eta)
-        V, K = hb.H2Matrix(slp, forest, a.m), hb.H2Matrix(dlp, forest, a.m)
+        V = hb.H2Matrix(slp, forest, a.m)
+        K = hb.H2Matrix(dlp, forest, a.m, like=V)
         V.set_precision(True)   # FP32 distant-pair quadrature (singular pairs FP64)
         K.set_precision(True)
         t1 = time.perf_counter()
@@ -527,7 +529,7 @@ def run_batched(a):
         dlp = hb.new_dlp_laplace_bem3d(g, 2, 4, L, L, 0.5)
         tree = hb.build_tree(g, L, L, a.clf, a.eta)
         V = hb.H2Matrix(slp, tree, a.m).assemble()
-        K = hb.H2Matrix(dlp, tree, a.m).assemble()
+        K = hb.H2Matrix(dlp, tree, a.m, like=V).assemble()
         for r in range(nrhs):
             gD = hb.project_l2_harmonic(dlp, zs[r])
             rhs = hb.addeval_h2matrix_avector(1.0, K, gD, np.zeros(K.rows))

@@ -58,6 +58,7 @@ _SIGS = {
                                     C.c_uint64]),
     "h2b_bem_assemble_amatrix": (C.c_int, [vp, vp, C.c_uint64]),
     "h2b_h2matrix_new": (vp, [vp, vp, C.c_uint32]),
+    "h2b_h2matrix_new_like": (vp, [vp, vp]),
     "h2b_h2matrix_del": (None, [vp]),
     "h2b_h2matrix_assemble_row_clusterbasis": (C.c_int, [vp]),
     "h2b_h2matrix_assemble_col_clusterbasis": (C.c_int, [vp]),

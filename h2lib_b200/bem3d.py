@@ -240,9 +240,16 @@ class H2Matrix:
     """Device H2 matrix with Chebyshev interpolation (setup_h2matrix_aprx_inter_bem3d,
     Library/bem3d.c:9658)."""
 
-    def __init__(self, bem, tree, m):
-        self.bem, self.tree, self.m = bem, tree, m
-        self.handle = checkp(lib.h2b_h2matrix_new(bem.handle, tree.handle, m), "h2matrix_new")
+    def __init__(self, bem, tree, m, like=None):
+        """like: an H2Matrix on the same surface, trees, bases and quadrature whose device
+        structure this one shares (h2b_h2matrix_new_like); it is kept alive by this object."""
+        self.bem, self.tree, self.m, self._like = bem, tree, m, like
+        if like is not None:
+            self.handle = checkp(lib.h2b_h2matrix_new_like(bem.handle, like.handle),
+                                 "h2matrix_new_like")
+        else:
+            self.handle = checkp(lib.h2b_h2matrix_new(bem.handle, tree.handle, m),
+                                 "h2matrix_new")
         self.rows, self.cols, self.dtype = bem.rows, bem.cols, bem.dtype
 
     def assemble(self):

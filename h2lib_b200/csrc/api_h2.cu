@@ -208,15 +208,23 @@ extern "C" void h2b_h2matrix_del(h2b_h2matrix *h) {
   cudaStream_t st = h->st;
   if (st) cudaStreamSynchronize(st);
   if (h->cst) cudaStreamSynchronize(h->cst);  // pending asynchronous exports read the blocks
-  devtree_free(h->rt, st);
-  devtree_free(h->ct, st);
-  dfree(h->rt.f_W, st); dfree(h->ct.f_W, st); dfree(h->f_N, st); dfree(h->f_S, st);
-  dfree(h->d_adm_rc, st); dfree(h->d_adm_cc, st); dfree(h->d_S, st);
-  dfree(h->d_near_rc, st); dfree(h->d_near_cc, st); dfree(h->d_near_off, st); dfree(h->d_N, st);
-  dfree(h->d_tiles, st); dfree(h->d_refs, st); dfree(h->d_sing, st);
+  // the operator's own data
+  for (DevCTree *t : {&h->rt, &h->ct}) {
+    dfree(t->d_V, st); dfree(t->d_E, st); dfree(t->d_W, st); dfree(t->d_counter, st);
+    dfree(t->f_W, st);
+  }
+  dfree(h->f_N, st); dfree(h->f_S, st); dfree(h->d_S, st); dfree(h->d_N, st);
   dfree(h->d_xp, st); dfree(h->d_yp, st); dfree(h->d_xt, st); dfree(h->d_yt, st);
-  dfree(h->d_xs, st); dfree(h->d_ys, st); dfree(h->d_ws, st); dfree(h->d_wsl, st);
   dfree(h->d_xio, st); dfree(h->d_yio, st);
+  // the structure, unless it belongs to the matrix this one was made like
+  if (!h->shared) {
+    devtree_free(h->rt, st);
+    devtree_free(h->ct, st);
+    dfree(h->d_adm_rc, st); dfree(h->d_adm_cc, st);
+    dfree(h->d_near_rc, st); dfree(h->d_near_cc, st); dfree(h->d_near_off, st);
+    dfree(h->d_tiles, st); dfree(h->d_refs, st); dfree(h->d_sing, st);
+    dfree(h->d_xs, st); dfree(h->d_ys, st); dfree(h->d_ws, st); dfree(h->d_wsl, st);
+  }
   for (int e = 0; e < 12; e++)
     if (h->ev[e]) cudaEventDestroy(h->ev[e]);
   if (h->cst) {
@@ -385,6 +393,71 @@ extern "C" h2b_h2matrix *h2b_h2matrix_new(const h2b_bem *bem, const h2b_tree *tr
     rc = H2B_ERR_CUDA;
   }
   if (rc != H2B_OK) {
+    h2b_h2matrix_del(h);
+    return NULL;
+  }
+  h2b_h2_fill_mvm_plan(h);
+  return h;
+}
+
+extern "C" h2b_h2matrix *h2b_h2matrix_new_like(const h2b_bem *bem, const h2b_h2matrix *like) {
+  if (!bem || !like) {
+    h2b_set_error("h2b_h2matrix_new_like: NULL operator or matrix");
+    return NULL;
+  }
+  const h2b_bem *b0 = like->bem;
+  if (bem->s != b0->s || bem->row_basis != b0->row_basis || bem->col_basis != b0->col_basis ||
+      bem->q != b0->q || bem->pde != b0->pde) {
+    h2b_set_error("h2b_h2matrix_new_like: the operator must share the surface, bases, quadrature "
+                  "order and PDE of the model matrix");
+    return NULL;
+  }
+  if (h2b_ensure_device() != H2B_OK) return NULL;
+  // copy every field, then replace what belongs to the new operator
+  h2b_h2matrix *h = new h2b_h2matrix(*like);
+  h->bem = bem;
+  h->shared = 1;
+  h->st = nullptr;
+  h->cst = nullptr;
+  h->ev_copy = nullptr;
+  for (int e = 0; e < 12; e++) h->ev[e] = nullptr;
+  for (int i = 0; i < 6; i++) h->ms[i] = 0.0f;
+  h->quad_fp32 = 0;
+  h->f_S = h->f_N = nullptr;
+  h->d_S = h->d_N = h->d_xp = h->d_yp = h->d_xt = h->d_yt = h->d_xio = h->d_yio = nullptr;
+  for (DevCTree *t : {&h->rt, &h->ct}) t->d_V = t->d_E = t->d_W = nullptr, t->f_W = nullptr,
+                                       t->d_counter = nullptr;
+  int rc = H2B_OK;
+  if (cudaStreamCreateWithFlags(&h->st, cudaStreamNonBlocking) != cudaSuccess) rc = H2B_ERR_CUDA;
+  for (int e = 0; rc == H2B_OK && e < 12; e++)
+    if (cudaEventCreate(&h->ev[e]) != cudaSuccess) rc = H2B_ERR_CUDA;
+  const size_t W = h->cx ? 2 : 1;
+  const uint64_t kk = (uint64_t) h->k * h->k;
+  const uint32_t nr = h->rt.nidx, nc = h->ct.nidx;
+  for (DevCTree *t : {&h->rt, &h->ct}) {
+    if (rc != H2B_OK) break;
+    if (cudaMallocAsync(&t->d_V, sizeof(double) * std::max<uint64_t>(t->vtotal, 1), h->st) ||
+        cudaMallocAsync(&t->d_E, sizeof(double) * std::max<uint64_t>((uint64_t) (t->n - 1) * kk, 1),
+                        h->st) ||
+        cudaMallocAsync(&t->d_counter, sizeof(unsigned) * t->n, h->st) ||
+        cudaMemsetAsync(t->d_counter, 0, sizeof(unsigned) * t->n, h->st) ||
+        (h->flat && cudaMallocAsync(&t->d_W, sizeof(double) * std::max<uint64_t>(t->wtotal, 1),
+                                    h->st)))
+      rc = H2B_ERR_NOMEM;
+  }
+  if (rc == H2B_OK &&
+      (cudaMallocAsync(&h->d_S, sizeof(double) * W * std::max<uint64_t>(h->nadm * kk, 1), h->st) ||
+       cudaMallocAsync(&h->d_N, sizeof(double) * W * std::max<uint64_t>(h->near_total, 1), h->st) ||
+       cudaMallocAsync(&h->d_xp, sizeof(double) * W * nc, h->st) ||
+       cudaMallocAsync(&h->d_yp, sizeof(double) * W * nr, h->st) ||
+       cudaMallocAsync(&h->d_xt, sizeof(double) * W * h->k * h->ct.n, h->st) ||
+       cudaMallocAsync(&h->d_yt, sizeof(double) * W * h->k * h->rt.n, h->st) ||
+       cudaMallocAsync(&h->d_xio, sizeof(double) * W * nc, h->st) ||
+       cudaMallocAsync(&h->d_yio, sizeof(double) * W * nr, h->st)))
+    rc = H2B_ERR_NOMEM;
+  if (rc == H2B_OK && cudaStreamSynchronize(h->st) != cudaSuccess) rc = H2B_ERR_CUDA;
+  if (rc != H2B_OK) {
+    h2b_set_error("h2b_h2matrix_new_like: %s", cudaGetErrorString(cudaGetLastError()));
     h2b_h2matrix_del(h);
     return NULL;
   }

@@ -46,6 +46,9 @@ struct h2b_h2matrix {
   int cx = 0, num_sms = 148;
   int flat = 1;  // matvec through flattened bases (W_t) instead of the nested transforms
   int quad_fp32 = 0;  // distant-pair quadrature in FP32 (h2b_h2matrix_set_precision)
+  // 1: the tree, block and nearfield-plan arrays belong to another matrix (h2b_h2matrix_new_like);
+  // only the operator's own data (bases, transfers, W, S, N, work vectors) are freed here
+  int shared = 0;
   cudaStream_t st = nullptr;
   DevCTree rt, ct;
   uint32_t nadm = 0, nnear = 0, ntiles = 0, nsing = 0;

@@ -108,7 +108,7 @@ int run_request(Req *q) {
                                              1.4)
                               : nullptr;
   h2b_h2matrix *V = tr ? h2b_h2matrix_new(slp, tr, m) : nullptr;
-  h2b_h2matrix *K = tr ? h2b_h2matrix_new(dlp, tr, m) : nullptr;
+  h2b_h2matrix *K = V ? h2b_h2matrix_new_like(dlp, V) : nullptr;  // shares V's structure
   // mixed precision: FP32 distant-pair quadrature too (singular pairs stay FP64)
   if (V && K && (d.flags & H2B_SOLVE_MIXED)) {
     h2b_h2matrix_set_precision(V, H2B_FP32);

@@ -197,6 +197,12 @@ int h2b_bem_assemble_amatrix(const h2b_bem *bem, double *G, uint64_t ld);
  * build_from_block_h2matrix (Library/h2matrix.c:438) + setup_h2matrix_aprx_inter_bem3d
  * (Library/bem3d.c:9658).  All storage is FP64. */
 h2b_h2matrix *h2b_h2matrix_new(const h2b_bem *bem, const h2b_tree *tree, uint32_t m);
+/* A second operator on the structure of `like` (same surface, trees, bases, quadrature order and
+ * PDE, e.g. the double layer beside the single layer of a Dirichlet problem): the device trees,
+ * block lists and nearfield plan are shared, not rebuilt; only the operator's own bases,
+ * coupling and nearfield storage are allocated.  `like` must outlive the new matrix.  No
+ * reference counterpart (H2Lib builds the cluster bases of each operator separately). */
+h2b_h2matrix *h2b_h2matrix_new_like(const h2b_bem *bem, const h2b_h2matrix *like);
 void h2b_h2matrix_del(h2b_h2matrix *h2);
 
 /* Assembly.  Replace assemble_bem3d_h2matrix_row_clusterbasis (Library/bem3d.c:10407),

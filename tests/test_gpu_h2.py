@@ -131,3 +131,50 @@ def test_config2_matvec_and_solve(gold):
     assert hb.residual_norm([V], [1.0], b, u) < 1.05e-8
     err, nrm = hb.l2_error_harmonic(slp, Z, u)
     assert abs(err / nrm - g["c2_l2err"][0] / g["c2_l2norm"][0]) < 1e-6
+
+
+def test_async_export_equals_export(s8):
+    """h2b_h2matrix_export_async (copy stream, pinned buffers) returns the same bytes as the
+    synchronous export, also when queued before a later assembly call of the matrix."""
+    import ctypes
+    import torch
+    from h2lib_b200._lib import check, lib
+    slp, dlp, tree, V, K = build_pair(s8, L, 16, 3)
+    V.assemble()
+    K.assemble()
+    want = {p: V.export(p) for p in (0, 1, 4, 5)}
+    bufs = {p: torch.empty(want[p].size, dtype=torch.float64, pin_memory=True)
+            for p in (0, 1, 4, 5)}
+    for p in (4, 0, 1):
+        check(lib.h2b_h2matrix_export_async(V.handle, p, 0xFFFFFFFF,
+                                            ctypes.c_void_p(bufs[p].data_ptr())), "async")
+    check(lib.h2b_h2matrix_assemble_nearfield(V.handle), "nearfield")  # reassembles N only
+    check(lib.h2b_h2matrix_export_async(V.handle, 5, 0xFFFFFFFF,
+                                        ctypes.c_void_p(bufs[5].data_ptr())), "async")
+    check(lib.h2b_h2matrix_export_wait(V.handle), "wait")
+    for p in (0, 1, 4):
+        np.testing.assert_array_equal(bufs[p].numpy(), want[p])
+    # the reassembled nearfield sums with atomics: equal up to rounding
+    assert relerr(bufs[5].numpy(), want[5]) < 1e-14
+    with pytest.raises(hb.H2BError):
+        check(lib.h2b_h2matrix_export_async(V.handle, 2, 0xFFFFFFFF,
+                                            ctypes.c_void_p(bufs[0].data_ptr())), "async")
+
+
+def test_new_like_shares_structure(s8):
+    """An operator made with H2Matrix(..., like=V) shares V's trees and nearfield plan and
+    assembles the same matrix as one built on its own."""
+    slp, dlp, tree, V, K = build_pair(s8, L, 16, 3)
+    V.assemble()
+    K.assemble()
+    K2 = hb.H2Matrix(dlp, tree, 3, like=V).assemble()
+    for p in (0, 1, 2, 3, 4):
+        np.testing.assert_array_equal(K2.export(p), K.export(p))
+    assert relerr(K2.export(5), K.export(5)) < 1e-14
+    x = np.random.default_rng(5).standard_normal(K.cols)
+    y1 = hb.addeval_h2matrix_avector(1.0, K, x, np.zeros(K.rows))
+    y2 = hb.addeval_h2matrix_avector(1.0, K2, x, np.zeros(K.rows))
+    assert relerr(y2, y1) < 1e-13
+    del K2  # the shared structure stays with V
+    y3 = hb.addeval_h2matrix_avector(1.0, V, x, np.zeros(V.rows))
+    assert np.all(np.isfinite(y3))
