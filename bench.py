@@ -567,7 +567,8 @@ def run_batched(a):
 def run_helmholtz(a):
     """Brakhage-Werner solves of config 3: unit cube split 64 (49152 triangles), constant basis,
     q 2/4, leaf 64, eta 1.4, m 5, plane wave along (1,1,1)/sqrt(3), GMRES(80) to 1e-8, k = 2
-    and 8; FP64 and mixed precision."""
+    and 8; FP64 with the reference's Givens rotations, FP64 with unitary rotations, and mixed
+    precision (unitary)."""
     import torch
     from h2lib_b200 import bem3d as hb
     C = hb.BASIS_CONSTANT_BEM3D
@@ -589,6 +590,11 @@ def run_helmholtz(a):
         t0 = time.perf_counter()
         it64 = hb.solve_gmres([K, V], [1.0, -1j * k], b, u64, 1e-8, 1000, 80)
         t64 = time.perf_counter() - t0
+        # unitary complex Givens rotations: the stop at 1e-8 holds for the true residual
+        uu = np.zeros(V.rows, dtype=np.complex128)
+        t0 = time.perf_counter()
+        itu = hb.solve_gmres([K, V], [1.0, -1j * k], b, uu, 1e-8, 1000, 80, unitary=True)
+        tu = time.perf_counter() - t0
         V.make_single()
         K.make_single()
         u32 = np.zeros(V.rows, dtype=np.complex128)
@@ -599,6 +605,9 @@ def run_helmholtz(a):
         out.append({"k": k, "assembly_s": t_asm, "near_entries_per_s": ent / t_asm,
                     "fp64": {"iterations": it64, "seconds": t64,
                              "rel_residual": hb.residual_norm([K, V], [1.0, -1j * k], b, u64)},
+                    "fp64_unitary": {"iterations": itu, "seconds": tu,
+                                     "rel_residual": hb.residual_norm([K, V], [1.0, -1j * k], b,
+                                                                      uu)},
                     "mixed": {"iterations": it32, "seconds": t32,
                               "rel_residual": hb.residual_norm([K, V], [1.0, -1j * k], b, u32),
                               "rel_diff_to_fp64": float(np.linalg.norm(u32 - u64) /

@@ -324,8 +324,15 @@ def addeval_h2matrix_avector(alpha, h2, x, y):
     return y
 
 
-def solve_gmres(ops, coefs, b, x, eps, maxiter, kmax):
-    """GMRES on sum_i coefs[i] * ops[i] (solve_gmres_avector, Library/krylovsolvers.c:183)."""
+def solve_gmres(ops, coefs, b, x, eps, maxiter, kmax, unitary=False):
+    """GMRES on sum_i coefs[i] * ops[i] (solve_gmres_avector, Library/krylovsolvers.c:183).
+    unitary: complex Givens rotations in unitary form (H2B_SOLVE_UNITARY), so that the stop at
+    eps holds for the true residual of a complex system; the default keeps the reference's
+    rotations and iteration counts."""
+    if unitary:
+        n = ops[0].rows
+        it = solve_gmres_batch(ops, coefs, [0, n], b, x, eps, maxiter, kmax, unitary=True)
+        return int(it[0, 0])
     arr = (C.c_void_p * len(ops))(*[o.handle for o in ops])
     cf = np.zeros(2 * len(ops))
     for i, c in enumerate(coefs):
@@ -335,6 +342,7 @@ def solve_gmres(ops, coefs, b, x, eps, maxiter, kmax):
 
 
 SOLVE_MIXED = 1
+SOLVE_UNITARY = 2
 
 
 def _coefs(ops, coefs):
@@ -345,17 +353,21 @@ def _coefs(ops, coefs):
     return C.cast(arr, C.c_void_p), cf, arr
 
 
-def solve_gmres_batch(ops, coefs, system_off, b, x, eps, maxiter, kmax, nrhs=1, mixed=False):
+def solve_gmres_batch(ops, coefs, system_off, b, x, eps, maxiter, kmax, nrhs=1, mixed=False,
+                      unitary=False):
     """Independent GMRES solves of the diagonal blocks [system_off[s], system_off[s+1]) of a block
     diagonal operator (an H2 matrix on a forest), all in one device loop; with nrhs > 1, b and x
-    hold nrhs columns.  mixed: FP32 Arnoldi steps, FP64 residuals (make_single first).  Returns
-    the iteration counts, shape (nrhs, systems)."""
+    hold nrhs columns.  mixed: FP32 Arnoldi steps, FP64 residuals (make_single first; implies
+    unitary).  unitary: unitary complex Givens rotations.  Returns the iteration counts, shape
+    (nrhs, systems)."""
     ptr, cf, _keep = _coefs(ops, coefs)
     off = np.ascontiguousarray(system_off, dtype=np.uint32)
     iters = np.zeros(nrhs * (off.size - 1), dtype=np.uint32)
     check(lib.h2b_solve_gmres_batch(len(ops), ptr, cf, off.size - 1, off, nrhs, _ptr(b),
-                                    _ptr(x), eps, maxiter, kmax, SOLVE_MIXED if mixed else 0,
-                                    iters), "solve_gmres_batch")
+                                    _ptr(x), eps, maxiter, kmax,
+                                    (SOLVE_MIXED if mixed else 0) |
+                                    (SOLVE_UNITARY if unitary else 0), iters),
+          "solve_gmres_batch")
     return iters.reshape(nrhs, off.size - 1)
 
 

@@ -45,11 +45,12 @@ extern "C" int h2b_device_init(int device) {
     return H2B_ERR_ARG;
   }
   H2B_CUDA_TRY(cudaSetDevice(device));
-  cudaDeviceProp prop;
-  H2B_CUDA_TRY(cudaGetDeviceProperties(&prop, device));
-  if (prop.major != 10) {
+  int major = 0, minor = 0;
+  H2B_CUDA_TRY(cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, device));
+  H2B_CUDA_TRY(cudaDeviceGetAttribute(&minor, cudaDevAttrComputeCapabilityMinor, device));
+  if (major != 10) {
     h2b_set_error("device %d is sm_%d%d; this library is built for sm_100a only", device,
-                  prop.major, prop.minor);
+                  major, minor);
     return H2B_ERR_CUDA;
   }
   std::lock_guard<std::mutex> lock(g_init_mutex);
@@ -135,9 +136,10 @@ extern "C" h2b_surface *h2b_surface_new(uint32_t vertices, const double *x, uint
     }
     r.g = g[i];
   }
-  int dev = 0;
-  cudaDeviceProp prop;
-  if (cudaGetDevice(&dev) != cudaSuccess || cudaGetDeviceProperties(&prop, dev) != cudaSuccess ||
+  // (an attribute query, not cudaGetDeviceProperties, which costs milliseconds per call)
+  int dev = 0, sms = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess ||
+      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
       cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) != cudaSuccess ||
       cudaMallocAsync(&s->d_tri, sizeof(TriRec) * triangles, s->stream) != cudaSuccess ||
       cudaMallocAsync(&s->d_x, sizeof(double) * 3ull * vertices, s->stream) != cudaSuccess ||
@@ -151,7 +153,7 @@ extern "C" h2b_surface *h2b_surface_new(uint32_t vertices, const double *x, uint
     return NULL;
   }
   s->device = dev;
-  s->num_sms = prop.multiProcessorCount;
+  s->num_sms = sms;
   return s;
 }
 

@@ -110,7 +110,8 @@ static bool forest_matches(const DevCTree &t, uint32_t nseg, const uint32_t *seg
 
 static int solve_segments(Combo &combo, uint32_t nseg, const uint32_t *seg_off, uint32_t nrhs,
                           const double *b, double *x, double eps, uint32_t maxiter,
-                          uint32_t kmax, int mixed, uint32_t *iters, const char *who) {
+                          uint32_t kmax, int mixed, int unitary, uint32_t *iters,
+                          const char *who) {
   const h2b_h2matrix *A0 = combo.ops[0];
   cudaStream_t st = A0->st;
   const uint32_t n1 = A0->rt.nidx;
@@ -157,6 +158,7 @@ static int solve_segments(Combo &combo, uint32_t nseg, const uint32_t *seg_off, 
   h2b_gmres_layout(&g, dx + W * n, A0->cx, nsys, sizes.data(), kmax, sys.data(), blk.data());
   g.eps = eps;
   g.mixed = mixed;
+  g.unitary = unitary;
   H2B_CUDA_TRY(cudaMemcpyAsync((void *) g.sys, sys.data(), sizeof(GmresSys) * nsys,
                                cudaMemcpyHostToDevice, st));
   H2B_CUDA_TRY(cudaMemcpyAsync((void *) g.blk, blk.data(), sizeof(uint32_t) * nblocks,
@@ -210,7 +212,8 @@ extern "C" int h2b_solve_gmres(uint32_t nterms, const h2b_h2matrix *const *ops,
   }
   const uint32_t seg[2] = {0, ops[0]->rt.nidx};
   uint32_t iter = 0;
-  rc = solve_segments(combo, 1, seg, 1, b, x, eps, maxiter, kmax, 0, &iter, "h2b_solve_gmres");
+  rc = solve_segments(combo, 1, seg, 1, b, x, eps, maxiter, kmax, 0, 0, &iter,
+                      "h2b_solve_gmres");
   return rc == H2B_OK ? (int) iter : rc;
 }
 
@@ -226,7 +229,7 @@ extern "C" int h2b_solve_gmres_mixed(uint32_t nterms, const h2b_h2matrix *const 
   }
   const uint32_t seg[2] = {0, ops[0]->rt.nidx};
   uint32_t iter = 0;
-  rc = solve_segments(combo, 1, seg, 1, b, x, eps, maxiter, kmax, 1, &iter,
+  rc = solve_segments(combo, 1, seg, 1, b, x, eps, maxiter, kmax, 1, 1, &iter,
                       "h2b_solve_gmres_mixed");
   return rc == H2B_OK ? (int) iter : rc;
 }
@@ -243,8 +246,16 @@ extern "C" int h2b_solve_gmres_batch(uint32_t nterms, const h2b_h2matrix *const 
     h2b_set_error("h2b_solve_gmres_batch: NULL vector");
     return H2B_ERR_ARG;
   }
-  return solve_segments(combo, systems, system_off, nrhs, b, x, eps, maxiter, kmax,
-                        (flags & H2B_SOLVE_MIXED) ? 1 : 0, iterations, "h2b_solve_gmres_batch");
+  if (flags & ~(H2B_SOLVE_MIXED | H2B_SOLVE_UNITARY)) {
+    h2b_set_error("h2b_solve_gmres_batch: unknown flags 0x%x", flags);
+    return H2B_ERR_ARG;
+  }
+  // the mixed iteration always uses the unitary rotations: its restarts compare the estimate
+  // with the FP64 residual, which only an exact estimate makes cheap
+  const int mixed = (flags & H2B_SOLVE_MIXED) ? 1 : 0;
+  const int unitary = (mixed || (flags & H2B_SOLVE_UNITARY)) ? 1 : 0;
+  return solve_segments(combo, systems, system_off, nrhs, b, x, eps, maxiter, kmax, mixed,
+                        unitary, iterations, "h2b_solve_gmres_batch");
 }
 
 // ------------------------------------------------------------------------------------------

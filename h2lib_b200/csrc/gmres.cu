@@ -297,31 +297,38 @@ __device__ void householder(cd diag, double norm2, GmresState *s, uint32_t col, 
   v.tau[2 * col + 1] = 0.0;
 }
 
-// Givens rotations of Library/krylov.c:551 / :587 (complex form as in the reference).
-__device__ cd findapply_givens(cd *a, cd *b) {
+// Givens rotations of Library/krylov.c:551 / :587.  A rotation is stored as one number rho:
+// |rho| < 1: s = rho, c = sqrt(1 - |s|^2) real; |rho| > 1: c = 1 / rho, s = sqrt(1 - |c|^2) real.
+// unitary = false is the reference's complex form, (a, b) -> (c a + s b, c b - s a) with
+// s = c b / a (or c = s a / b): for complex entries that matrix is not unitary, so |rhat_k| is no
+// longer the residual norm (for real entries both forms coincide).  unitary = true uses
+// s = c conj(b / a) (or c = s conj(a / b)) and (a, b) -> (c a + s b, conj(c) b - conj(s) a),
+// a unitary matrix that eliminates b the same way, so |rhat_k| stays the residual norm.
+__device__ cd findapply_givens(cd *a, cd *b, bool unitary) {
   const cd aa = *a, bb = *b;
   cd s, c, rho;
-  if (cabs2(bb) < cabs2(aa)) {
+  const double a2 = cabs2(aa), b2 = cabs2(bb);
+  if (b2 < a2 || (unitary && b2 == a2 && a2 > 0.0)) {
     const cd t = cdiv(bb, aa);
     c = {1.0 / sqrt(cabs2(t) + 1.0), 0.0};
-    s = cmul(t, c);
+    s = cmul(unitary ? cconj(t) : t, c);
     rho = s;
-  } else if (cabs2(aa) < cabs2(bb)) {
+  } else if (a2 < b2) {
     const cd t = cdiv(aa, bb);
     s = {1.0 / sqrt(cabs2(t) + 1.0), 0.0};
-    c = cmul(t, s);
+    c = cmul(unitary ? cconj(t) : t, s);
     rho = cdiv(cd{1.0, 0.0}, c);
   } else {
     c = {1.0, 0.0};
     s = {0.0, 0.0};
-    rho = {1.0, 0.0};
+    rho = unitary ? cd{0.0, 0.0} : cd{1.0, 0.0};
   }
   *a = cadd(cmul(c, aa), cmul(s, bb));
   *b = {0.0, 0.0};
   return rho;
 }
 
-__device__ void apply_givens(cd rho, cd *a, cd *b) {
+__device__ void apply_givens(cd rho, cd *a, cd *b, bool unitary) {
   const cd aa = *a, bb = *b;
   cd s, c;
   if (cabs2(rho) < 1.0) {
@@ -335,7 +342,7 @@ __device__ void apply_givens(cd rho, cd *a, cd *b) {
     s = {0.0, 0.0};
   }
   *a = cadd(cmul(c, aa), cmul(s, bb));
-  *b = csub(cmul(c, bb), cmul(s, aa));
+  *b = unitary ? csub(cmul(cconj(c), bb), cmul(cconj(s), aa)) : csub(cmul(c, bb), cmul(s, aa));
 }
 
 // Bookkeeping kernels: one CTA of SMALL_THREADS threads (>= kmax) per system; O(k) work per
@@ -432,21 +439,21 @@ __global__ void __launch_bounds__(SMALL_THREADS) small_kernel(GmresDev g, int ph
     if (t == 0) {
       for (uint32_t i = 0; i < k; i++) {
         cd a = {wr[i], wi[i]}, b = {wr[i + 1], wi[i + 1]};
-        apply_givens(cd{zr[i], zi[i]}, &a, &b);
+        apply_givens(cd{zr[i], zi[i]}, &a, &b, g.unitary != 0);
         wr[i] = a.re;
         wi[i] = a.im;
         wr[i + 1] = b.re;
         wi[i + 1] = b.im;
       }
       cd a = {wr[k], wi[k]}, b = {wr[k + 1], wi[k + 1]};
-      const cd rho = findapply_givens(&a, &b);
+      const cd rho = findapply_givens(&a, &b, g.unitary != 0);
       wr[k] = a.re;
       wi[k] = a.im;
       wr[k + 1] = rho.re;  // the rotation is stored below the diagonal
       wi[k + 1] = rho.im;
       cd r0 = {v.rhat[2 * k], v.rhat[2 * k + 1]},
          r1 = {v.rhat[2 * (k + 1)], v.rhat[2 * (k + 1) + 1]};
-      apply_givens(rho, &r0, &r1);
+      apply_givens(rho, &r0, &r1, g.unitary != 0);
       v.rhat[2 * k] = r0.re;
       v.rhat[2 * k + 1] = r0.im;
       v.rhat[2 * (k + 1)] = r1.re;

@@ -40,6 +40,7 @@ enum { GMRES_SEL_ALL = 0, GMRES_SEL_ACTIVE = 1, GMRES_SEL_RESTART = 2 };
 struct GmresDev {
   int cx;
   int mixed;                 // 1: steps use op.apply_lo, restarts measure the FP64 residual
+  int unitary;               // 1: unitary complex Givens rotations (see findapply_givens)
   uint32_t nsys, n, kmax, nblocks, ldpart;
   double eps;
   const GmresSys *sys;       // nsys

@@ -163,11 +163,13 @@ int run_request(Req *q) {
       rc = h2b_h2matrix_make_single(const_cast<h2b_h2matrix *>(ops[i]));
   int it = 0;
   if (rc == H2B_OK) {
-    it = mixed ? h2b_solve_gmres_mixed(nterms, ops, coef, b.data(), u.data(), d.eps, d.maxiter,
-                                       d.kmax)
-               : h2b_solve_gmres(nterms, ops, coef, b.data(), u.data(), d.eps, d.maxiter,
-                                 d.kmax);
-    if (it < 0) rc = it;
+    // unitary rotations: the stop is decided by the true residual, also for complex systems
+    const uint32_t seg[2] = {0, nd};
+    uint32_t iters = 0;
+    rc = h2b_solve_gmres_batch(nterms, ops, coef, 1, seg, 1, b.data(), u.data(), d.eps,
+                               d.maxiter, d.kmax,
+                               H2B_SOLVE_UNITARY | (mixed ? H2B_SOLVE_MIXED : 0u), &iters);
+    it = (int) iters;
   }
   const auto c4 = tick();
   q->res.t_setup = secs(c0, c1);

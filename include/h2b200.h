@@ -303,6 +303,13 @@ int h2b_solve_gmres(uint32_t nterms, const h2b_h2matrix *const *ops, const doubl
  * iterations[s] (may be NULL) receives each system's step count.  No counterpart in the
  * reference, which solves one system per solve_gmres_avector call. */
 #define H2B_SOLVE_MIXED 1u
+/* Complex systems: Givens rotations in unitary form.  The reference's complex rotation
+ * (Library/krylov.c:551/587) is not a unitary matrix, so for Helmholtz operators its residual
+ * estimate |rhat_k| can lie orders of magnitude below the true residual and the solve stops
+ * early; h2b_solve_gmres keeps that behaviour (same iteration counts as the reference).  With
+ * this flag the rotation is unitary and |rhat_k| is the residual norm.  Real systems are
+ * unaffected (both forms coincide); H2B_SOLVE_MIXED implies it. */
+#define H2B_SOLVE_UNITARY 2u
 int h2b_solve_gmres_batch(uint32_t nterms, const h2b_h2matrix *const *ops, const double *coef,
                           uint32_t systems, const uint32_t *system_off, uint32_t nrhs,
                           const double *b, double *x, double eps, uint32_t maxiter, uint32_t kmax,
@@ -315,7 +322,8 @@ int h2b_solve_gmres_batch(uint32_t nterms, const h2b_h2matrix *const *ops, const
  * to confirm it with the FP64 residual, so the returned x meets eps in FP64 — restarted GMRES
  * as iterative refinement with a single-precision inner operator. */
 
-/* h2b_solve_gmres with the mixed-precision iteration of H2B_SOLVE_MIXED (one system). */
+/* h2b_solve_gmres with the mixed-precision iteration of H2B_SOLVE_MIXED (one system; unitary
+ * rotations). */
 int h2b_solve_gmres_mixed(uint32_t nterms, const h2b_h2matrix *const *ops, const double *coef,
                           const double *b, double *x, double eps, uint32_t maxiter,
                           uint32_t kmax);
@@ -389,7 +397,9 @@ typedef struct h2b_server h2b_server;
  * entries.  pde = H2B_HELMHOLTZ: Brakhage-Werner ((K + M/2) - i k V) u = -int exp(i k src.x)
  * for the plane wave of unit direction src and wavenumber k, constant basis (m = 5); the solution
  * has `triangles` complex (interleaved) entries.  Both use q = 2/4, leaf size 64, eta = 1.4 and
- * GMRES(kmax) to eps (flags: H2B_SOLVE_MIXED for FP32 Arnoldi steps with FP64 residuals). */
+ * GMRES(kmax) to eps (flags: H2B_SOLVE_MIXED for FP32 Arnoldi steps with FP64 residuals).  The
+ * server always uses the unitary rotations of H2B_SOLVE_UNITARY, so every result meets eps in
+ * the true residual. */
 typedef struct {
   uint32_t vertices, triangles;
   const double *x;

@@ -1081,14 +1081,27 @@ qr_apply(const cplx *qr, uint32_t n, const cplx *tau, uint32_t refl, int qtrans,
   }
 }
 
+/* Givens rotations of Library/krylov.c:551/587, one number rho per rotation.  g_unitary = 0
+ * restates the reference's complex form ((a, b) -> (c a + s b, c b - s a), s = c b / a), which
+ * is not unitary for complex entries; g_unitary = 1 uses s = c conj(b / a) and
+ * (a, b) -> (c a + s b, conj(c) b - conj(s) a), unitary, for checking the library's
+ * H2B_SOLVE_UNITARY mode.  Both coincide for real entries. */
+static int g_unitary = 0;
+
 static cplx
 findapply_givens(cplx *a, cplx *b)
 {
   cplx aa = *a, bb = *b, s, c, t, rho;
   double a2 = creal(aa * conj(aa)), b2 = creal(bb * conj(bb));
-  if (b2 < a2) { t = bb / aa; c = 1.0 / sqrt(creal(t * conj(t)) + 1.0); s = t * c; rho = s; }
-  else if (a2 < b2) { t = aa / bb; s = 1.0 / sqrt(creal(t * conj(t)) + 1.0); c = t * s; rho = 1.0 / c; }
-  else { c = 1.0; s = 0.0; rho = 1.0; }
+  if (b2 < a2 || (g_unitary && b2 == a2 && a2 > 0.0)) {
+    t = bb / aa; c = 1.0 / sqrt(creal(t * conj(t)) + 1.0); s = (g_unitary ? conj(t) : t) * c;
+    rho = s;
+  }
+  else if (a2 < b2) {
+    t = aa / bb; s = 1.0 / sqrt(creal(t * conj(t)) + 1.0); c = (g_unitary ? conj(t) : t) * s;
+    rho = 1.0 / c;
+  }
+  else { c = 1.0; s = 0.0; rho = g_unitary ? 0.0 : 1.0; }
   *a = c * aa + s * bb;
   *b = 0.0;
   return rho;
@@ -1103,7 +1116,7 @@ apply_givens(cplx rho, cplx *a, cplx *b)
   else if (r2 > 1.0) { c = 1.0 / rho; s = sqrt(1.0 - creal(c * conj(c))); }
   else { c = 1.0; s = 0.0; }
   *a = c * aa + s * bb;
-  *b = c * bb - s * aa;
+  *b = g_unitary ? conj(c) * bb - conj(s) * aa : c * bb - s * aa;
 }
 
 typedef struct {
@@ -1166,6 +1179,17 @@ gm_finish(const combo_t *A, const cplx *b, cplx *x, gm_t *g)
   qr_apply(g->qr, n, g->tau, k, 0, g->rhat);
   for (i = 0; i < n; i++) x[i] += g->rhat[i];
   gm_init(A, b, x, g);
+}
+
+int
+orc_gmres_unitary(uint32_t nterms, orc_h2 *const *ops, const double *coef, const double *b,
+                  double *x, double eps, uint32_t maxiter, uint32_t kmax)
+{
+  int it;
+  g_unitary = 1;
+  it = orc_gmres(nterms, ops, coef, b, x, eps, maxiter, kmax);
+  g_unitary = 0;
+  return it;
 }
 
 int

@@ -47,6 +47,8 @@ def _load():
         d.orc_h2_addeval.argtypes = [vp, C.c_double, C.c_double, vp, vp]
         d.orc_gmres.argtypes = [C.c_uint32, vp, _f64p, vp, vp, C.c_double, C.c_uint32,
                                 C.c_uint32]
+        d.orc_gmres_unitary.argtypes = [C.c_uint32, vp, _f64p, vp, vp, C.c_double,
+                                        C.c_uint32, C.c_uint32]
         d.orc_project_l2_harmonic.argtypes = [C.c_uint32, _f64p, C.c_uint32, _u32p, _f64p,
                                               C.c_uint32, _f64p, _f64p]
         d.orc_l2_error_harmonic.argtypes = [C.c_uint32, _f64p, C.c_uint32, _u32p, _f64p, _f64p,
@@ -150,13 +152,15 @@ class H2:
             self.handle = None
 
 
-def gmres(ops, coefs, b, x, eps, maxiter, kmax):
+def gmres(ops, coefs, b, x, eps, maxiter, kmax, unitary=False):
+    """unitary: complex Givens rotations in unitary form (the reference's form otherwise)."""
     arr = (C.c_void_p * len(ops))(*[o.handle for o in ops])
     cf = np.zeros(2 * len(ops))
     for i, c in enumerate(coefs):
         cf[2 * i], cf[2 * i + 1] = complex(c).real, complex(c).imag
-    return _load().orc_gmres(len(ops), C.cast(arr, C.c_void_p), cf, _p(np.ascontiguousarray(b)),
-                             _p(x), eps, maxiter, kmax)
+    fn = _load().orc_gmres_unitary if unitary else _load().orc_gmres
+    return fn(len(ops), C.cast(arr, C.c_void_p), cf, _p(np.ascontiguousarray(b)), _p(x), eps,
+              maxiter, kmax)
 
 
 def project_l2_harmonic(mesh, z, q=2):

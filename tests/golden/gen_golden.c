@@ -7,7 +7,7 @@
  *
  * Usage: gen_golden <outdir> <section> [...]
  * Sections (real build):    quad sphere8 sphere4 h2small config2 cube
- * Sections (complex build): helm_sphere4 helm_h2small
+ * Sections (complex build): helm_sphere4 helm_h2small config3 helm_gmres
  */
 #include <math.h>
 #include <stdio.h>
@@ -830,6 +830,76 @@ section_config3(void)
   del_stopwatch(sw);
 }
 
+/* The reference's complex GMRES on a small Brakhage-Werner system: sphere refined x10 (800
+ * triangles), constant basis, k = 5, leaf 32, eta 1.4, m = 4, seeded right-hand side, GMRES(80)
+ * to 1e-8.  Records the iteration count, the solution and its true relative residual
+ * |b - A u| / |b| (the reference stops on its residual estimate). */
+static void
+section_helm_gmres(void)
+{
+  pmacrosurface3d mg = new_sphere_macrosurface3d();
+  psurface3d gr = build_from_macrosurface3d_surface3d(mg, 10);
+  field k = 5.0;
+  real eta = 1.4;
+  pbem3d slp, dlp;
+  pcluster root;
+  pblock broot;
+  pclusterbasis Vrb, Vcb, Krb, Kcb;
+  ph2matrix V, K;
+  pavector b, u, r;
+  bw_t bw;
+  uint iter;
+
+  slp = new_slp_helmholtz_bem3d(k, gr, 2, 4, BASIS_CONSTANT_BEM3D, BASIS_CONSTANT_BEM3D);
+  dlp = new_dlp_helmholtz_bem3d(k, gr, 2, 4, BASIS_CONSTANT_BEM3D, BASIS_CONSTANT_BEM3D, 0.5);
+  root = build_bem3d_cluster(slp, 32, BASIS_CONSTANT_BEM3D);
+  broot = build_strict_block(root, root, &eta, admissible_max_cluster);
+  dump_mesh("hg", gr);
+  dump_cluster("hg", root);
+  dump_block("hg", broot, root, root);
+  Vrb = build_from_cluster_clusterbasis(root);
+  Vcb = build_from_cluster_clusterbasis(root);
+  Krb = build_from_cluster_clusterbasis(root);
+  Kcb = build_from_cluster_clusterbasis(root);
+  V = build_from_block_h2matrix(broot, Vrb, Vcb);
+  K = build_from_block_h2matrix(broot, Krb, Kcb);
+  setup_h2matrix_aprx_inter_bem3d(slp, Vrb, Vcb, broot, 4);
+  setup_h2matrix_aprx_inter_bem3d(dlp, Krb, Kcb, broot, 4);
+  assemble_bem3d_h2matrix_row_clusterbasis(slp, Vrb);
+  assemble_bem3d_h2matrix_col_clusterbasis(slp, Vcb);
+  assemble_bem3d_h2matrix(slp, V);
+  assemble_bem3d_h2matrix_row_clusterbasis(dlp, Krb);
+  assemble_bem3d_h2matrix_col_clusterbasis(dlp, Kcb);
+  assemble_bem3d_h2matrix(dlp, K);
+
+  b = new_avector(gr->triangles);
+  u = new_avector(gr->triangles);
+  r = new_avector(gr->triangles);
+  seeded_avector(b, 4);
+  dump_avector("hg_b", b);
+  bw.V = V;
+  bw.KM = K;
+  bw.eta = k;
+  clear_avector(u);
+  iter = solve_gmres_avector(&bw, addeval_bw, b, u, 1.0e-8, 1000, 80);
+  dump_scalar("hg_gmres_iter", (double) iter);
+  dump_avector("hg_u", u);
+  copy_avector(b, r);
+  addeval_bw(-1.0, &bw, u, r);
+  dump_scalar("hg_true_residual", norm2_avector(r) / norm2_avector(b));
+
+  del_avector(b); del_avector(u); del_avector(r);
+  del_h2matrix(V);
+  del_h2matrix(K);
+  del_block(broot);
+  freemem(root->idx);
+  del_cluster(root);
+  del_helmholtz_bem3d(slp);
+  del_helmholtz_bem3d(dlp);
+  del_surface3d(gr);
+  del_macrosurface3d(mg);
+}
+
 #endif
 
 int
@@ -871,6 +941,8 @@ main(int argc, char **argv)
       section_helm_h2small();
     else if (!strcmp(argv[i], "config3"))
       section_config3();
+    else if (!strcmp(argv[i], "helm_gmres"))
+      section_helm_gmres();
 #endif
     else {
       fprintf(stderr, "unknown section %s\n", argv[i]);

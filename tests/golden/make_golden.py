@@ -7,7 +7,7 @@ read the committed .npz files.
 
     python tests/golden/make_golden.py [section ...]
 
-Sections: quad sphere8 sphere4 h2small config2 cube helm_sphere4 helm_h2small
+Sections: quad sphere8 sphere4 h2small config2 cube helm_sphere4 helm_h2small config3 helm_gmres
 """
 import os
 import subprocess
@@ -22,7 +22,7 @@ REF = os.environ.get("REF", "/root/reference")
 REFOUT = os.path.join(ROOT, "oracle", "_ref")
 
 REAL_SECTIONS = ["quad", "sphere8", "sphere4", "h2small", "config2", "cube"]
-COMPLEX_SECTIONS = ["helm_sphere4", "helm_h2small", "config3"]
+COMPLEX_SECTIONS = ["helm_sphere4", "helm_h2small", "config3", "helm_gmres"]
 DTYPES = {"f8": np.float64, "u4": np.uint32, "c16": np.complex128}
 # Arrays stored only in part, to keep the fixtures small: name -> number of leading columns kept
 # (matrices are written column-major, i.e. shape (cols, rows)).

@@ -168,9 +168,12 @@ def test_new_like_shares_structure(s8):
     V.assemble()
     K.assemble()
     K2 = hb.H2Matrix(dlp, tree, 3, like=V).assemble()
-    for p in (0, 1, 2, 3, 4):
-        np.testing.assert_array_equal(K2.export(p), K.export(p))
-    assert relerr(K2.export(5), K.export(5)) < 1e-14
+    i1, i2 = K.info(), K2.info()
+    assert all(i1[f] == i2[f] for f in i1 if f != "bytes")
+    # linear-basis leaf bases and nearfield entries sum over triangles with atomics: equal up
+    # to rounding, not bitwise
+    for p in (0, 1, 2, 3, 4, 5):
+        assert relerr(K2.export(p), K.export(p)) < 1e-14
     x = np.random.default_rng(5).standard_normal(K.cols)
     y1 = hb.addeval_h2matrix_avector(1.0, K, x, np.zeros(K.rows))
     y2 = hb.addeval_h2matrix_avector(1.0, K2, x, np.zeros(K.rows))

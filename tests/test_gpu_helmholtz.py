@@ -43,3 +43,32 @@ def test_config3_brakhage_werner(gold):
     assert abs(it - int(g["c3_gmres_iter"][0])) <= 1
     assert relerr(u, g["c3_u"]) < 1e-6
     assert hb.residual_norm([K, V], [1.0, -1j * k], b, u) < 1.05e-8
+
+
+def test_complex_gmres_givens(gold):
+    """Brakhage-Werner on the sphere refined x10 (800 triangles), k = 5, GMRES(80) to 1e-8 against
+    the reference's run: h2b_solve_gmres keeps the reference's complex Givens rotation (same
+    steps, same solution, whose true residual misses eps); H2B_SOLVE_UNITARY takes as many steps
+    and meets eps in the true residual."""
+    g = gold("helm_gmres")
+    k = 5.0
+    gr = hb.Surface3d(g["hg_x"], g["hg_t"])
+    slp = hb.new_slp_helmholtz_bem3d(k, gr, 2, 4, C, C)
+    dlp = hb.new_dlp_helmholtz_bem3d(k, gr, 2, 4, C, C, 0.5)
+    tree = hb.build_tree(gr, C, C, 32, 1.4)
+    rec, box, idx = tree.clusters(0)
+    np.testing.assert_array_equal(rec, g["hg_ctree"])
+    np.testing.assert_array_equal(idx, g["hg_idx"])
+    V = hb.H2Matrix(slp, tree, 4).assemble()
+    K = hb.H2Matrix(dlp, tree, 4, like=V).assemble()
+    ops, coefs = [K, V], [1.0, -1j * k]
+    b = np.ascontiguousarray(g["hg_b"])
+    u = np.zeros_like(b)
+    it = hb.solve_gmres(ops, coefs, b, u, 1e-8, 1000, 80)
+    assert abs(it - int(g["hg_gmres_iter"][0])) <= 1
+    assert relerr(u, g["hg_u"]) < 1e-6
+    assert abs(hb.residual_norm(ops, coefs, b, u) / g["hg_true_residual"][0] - 1.0) < 0.05
+    u2 = np.zeros_like(b)
+    it2 = hb.solve_gmres(ops, coefs, b, u2, 1e-8, 1000, 80, unitary=True)
+    assert abs(it2 - it) <= 1
+    assert hb.residual_norm(ops, coefs, b, u2) <= 1.0e-8

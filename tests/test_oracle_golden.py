@@ -156,3 +156,33 @@ def test_helmholtz_h2_matvec(gold):
     assert relerr(y, g["hh2_ySLP"]) < 1e-12
     y = K.addeval(1.0, x, np.zeros(2 * K.rows)).view(np.complex128)
     assert relerr(y, g["hh2_yDLP"]) < 1e-12
+
+
+def test_complex_gmres_givens(gold):
+    """The reference's GMRES on a complex (Brakhage-Werner) system: the oracle takes the same
+    steps and returns the same solution, whose true residual misses eps, because the reference's
+    complex Givens rotation (Library/krylov.c:551/587) is not unitary.  The unitary rotation
+    (the library's H2B_SOLVE_UNITARY) takes the same number of steps and meets eps."""
+    g = gold("helm_gmres")
+    mesh = mesh_from(g, "hg")
+    tree, blocks = tree_arrays(g, "hg")
+    k = 5.0
+    V = orc.H2(mesh, orc.HELMHOLTZ, orc.SLP, C, C, 4, tree, tree, blocks, k=k)
+    K = orc.H2(mesh, orc.HELMHOLTZ, orc.DLP, C, C, 4, tree, tree, blocks, k=k, alpha=0.5)
+    b = g["hg_b"]
+
+    def true_residual(u):
+        r = b.copy()
+        K.addeval(-1.0, u, r)
+        V.addeval(1j * k, u, r)
+        return float(np.linalg.norm(r) / np.linalg.norm(b))
+
+    u = np.zeros_like(b)
+    it = orc.gmres([K, V], [1.0, -1j * k], b, u, 1e-8, 1000, 80)
+    assert it == int(g["hg_gmres_iter"][0])
+    assert relerr(u, g["hg_u"]) < 1e-9
+    assert abs(true_residual(u) / g["hg_true_residual"][0] - 1.0) < 1e-3
+    assert g["hg_true_residual"][0] > 1.2e-8  # the reference's answer misses eps
+    u2 = np.zeros_like(b)
+    assert orc.gmres([K, V], [1.0, -1j * k], b, u2, 1e-8, 1000, 80, unitary=True) == it
+    assert true_residual(u2) <= 1e-8
