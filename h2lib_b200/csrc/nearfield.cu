@@ -336,6 +336,22 @@ struct DistArgs {
 #ifndef H2B_DIST_MINBLOCKS
 #define H2B_DIST_MINBLOCKS 2
 #endif
+// 1: the tile's row and column triangles are staged in shared memory, structure of arrays, in
+// chunks of DIST_CHUNK triangles per side (the pair loop then reads consecutive words per warp
+// instead of one 128-byte record per lane from L1); 0: records read per pair from global memory.
+#ifndef H2B_DIST_STAGE
+#define H2B_DIST_STAGE 1
+#endif
+constexpr int DIST_CHUNK = 128;
+
+// Staged triangles of one chunk pair.  Edge vectors are formed once per triangle here (the same
+// subtractions pair_geo_id makes per pair, so the pair geometry is bitwise the same).
+struct DistStage {
+  double r[10][DIST_CHUNK];  // row triangles: A (3), B - A (3), C - B (3), Gram determinant
+  double c[13][DIST_CHUNK];  // column triangles: A, B - A, C - B, Gram determinant * kconst, n
+  uint32_t rv[3][DIST_CHUNK], cv[3][DIST_CHUNK];  // vertex ids
+  int32_t rl[3][DIST_CHUNK], cl[3][DIST_CHUNK];   // local output row / column per vertex
+};
 template <int Q, int KK, bool RL, bool CL, bool F32 = false>
 __global__ void __launch_bounds__(256, H2B_DIST_MINBLOCKS) near_dist_kernel(DistArgs a) {
   constexpr int NCH = KT<KK>::NCH;
@@ -366,6 +382,125 @@ __global__ void __launch_bounds__(256, H2B_DIST_MINBLOCKS) near_dist_kernel(Dist
     cw = &c_dist[4][dist_off(q)];
   }
 
+#if H2B_DIST_STAGE
+  // Chunk pairs (column chunk outer): rows are restaged per chunk pair only when the tile has
+  // more than one row chunk.  Lanes of a warp take consecutive row triangles of one column
+  // triangle: the row arrays are read as consecutive words, the column arrays as a broadcast.
+  DistStage &sg = *reinterpret_cast<DistStage *>(sacc + PLANES * TS);
+  for (uint32_t c0 = 0; c0 < nsc; c0 += DIST_CHUNK) {
+    const uint32_t nc = min((uint32_t) DIST_CHUNK, nsc - c0);
+    for (uint32_t r0 = 0; r0 < ntr; r0 += DIST_CHUNK) {
+      const uint32_t nr = min((uint32_t) DIST_CHUNK, ntr - r0);
+      if (r0 == 0 || ntr > (uint32_t) DIST_CHUNK) {
+        if (c0 + r0 > 0) __syncthreads();  // the previous chunk pair is done with the stage
+        if (r0 == 0) {
+          for (uint32_t e = threadIdx.x; e < nc; e += blockDim.x) {
+            const TriRef st = a.refs[tl.sc_off + c0 + e];
+            const TriRec &S = a.tri[st.t];
+#pragma unroll
+            for (int d = 0; d < 3; d++) {
+              sg.c[d][e] = S.a[d];
+              sg.c[3 + d][e] = S.b[d] - S.a[d];
+              sg.c[6 + d][e] = S.c[d] - S.b[d];
+              sg.c[10 + d][e] = S.n[d];
+              sg.cv[d][e] = S.v[d];
+              sg.cl[d][e] = st.l[d];
+            }
+            sg.c[9][e] = S.g * a.kconst;
+          }
+        }
+        if (c0 == 0 || ntr > (uint32_t) DIST_CHUNK) {
+          for (uint32_t e = threadIdx.x; e < nr; e += blockDim.x) {
+            const TriRef rt = a.refs[tl.tr_off + r0 + e];
+            const TriRec &T = a.tri[rt.t];
+#pragma unroll
+            for (int d = 0; d < 3; d++) {
+              sg.r[d][e] = T.a[d];
+              sg.r[3 + d][e] = T.b[d] - T.a[d];
+              sg.r[6 + d][e] = T.c[d] - T.b[d];
+              sg.rv[d][e] = T.v[d];
+              sg.rl[d][e] = rt.l[d];
+            }
+            sg.r[9][e] = T.g;
+          }
+        }
+        __syncthreads();
+      }
+      // pair p = is * nr + it; the step of blockDim.x pairs advances (is, it) by (dq, dr)
+      const uint32_t np = nr * nc, dq = blockDim.x / nr, dr = blockDim.x - dq * nr;
+      uint32_t is = threadIdx.x / nr, it = threadIdx.x - is * nr;
+      for (uint32_t p = threadIdx.x; p < np; p += blockDim.x) {
+        const uint32_t ci = is, ri = it;
+        is += dq;
+        it += dr;
+        if (it >= nr) {
+          it -= nr;
+          is++;
+        }
+        const uint32_t tv0 = sg.rv[0][ri], tv1 = sg.rv[1][ri], tv2 = sg.rv[2][ri];
+        const uint32_t sv0 = sg.cv[0][ci], sv1 = sg.cv[1][ci], sv2 = sg.cv[2][ci];
+        const bool singular = tv0 == sv0 || tv0 == sv1 || tv0 == sv2 || tv1 == sv0 ||
+                              tv1 == sv1 || tv1 == sv2 || tv2 == sv0 || tv2 == sv1 || tv2 == sv2;
+        if (singular) continue;
+        PairGeo g;
+#pragma unroll
+        for (int d = 0; d < 3; d++) {
+          g.d0[d] = sg.r[d][ri] - sg.c[d][ci];
+          g.p1[d] = sg.r[3 + d][ri];
+          g.p2[d] = sg.r[6 + d][ri];
+          g.q1[d] = sg.c[3 + d][ci];
+          g.q2[d] = sg.c[6 + d][ci];
+        }
+        const double n0 = sg.c[10][ci], n1 = sg.c[11][ci], n2 = sg.c[12][ci];
+        double acc[NCH][NR][NC];
+#pragma unroll
+        for (int c = 0; c < NCH; c++)
+#pragma unroll
+          for (int i = 0; i < NR; i++)
+#pragma unroll
+            for (int j = 0; j < NC; j++) acc[c][i][j] = 0.0;
+
+        if constexpr (Q > 0) {
+#if H2B_DIST_TENSOR
+          if constexpr (F32)
+            dist_pair_tensor_f32<Q, KK, RL, CL>(g, n0, n1, n2, a.k_re, a.k_imn, acc);
+          else
+            dist_pair_tensor<Q, KK, RL, CL>(g, n0, n1, n2, a.k_re, a.k_imn, acc);
+#else
+#pragma unroll
+          for (int k = 0; k < Q * Q * Q * Q; k++)
+            quad_point<KK, RL, CL>(g, cx0[k], cx1[k], cy0[k], cy1[k], cw[k], n0, n1, n2, a.k_re,
+                                   a.k_imn, acc);
+#endif
+        } else {
+          for (int k = 0; k < nq; k++)
+            quad_point<KK, RL, CL>(g, cx0[k], cx1[k], cy0[k], cy1[k], cw[k], n0, n1, n2, a.k_re,
+                                   a.k_imn, acc);
+        }
+
+        const double f2 = sg.c[9][ci] * sg.r[9][ri];
+#pragma unroll
+        for (int i = 0; i < NR; i++) {
+          const int lr = sg.rl[i][ri];
+#pragma unroll
+          for (int j = 0; j < NC; j++) {
+            const int lc = sg.cl[j][ci];
+            if (lr < 0 || lc < 0) continue;
+            const int e = lr + H2B_TILE_MAX * lc;
+#pragma unroll
+            for (int c = 0; c < NCH; c++) {
+              const double v = acc[c][i][j] * f2;
+              if constexpr (RL || CL)
+                atomicAdd(&sacc[c * TS + e], v);
+              else
+                sacc[c * TS + e] = v;
+            }
+          }
+        }
+      }
+    }
+  }
+#else
   // Lanes of a warp take consecutive row positions q of one column triangle.  The row triangles
   // are visited as it = q * mult mod ntr (a bijection, mult prime and not dividing ntr): the
   // triangle lists follow the vertex order, so neighbours share vertices, and spreading a warp
@@ -437,6 +572,7 @@ __global__ void __launch_bounds__(256, H2B_DIST_MINBLOCKS) near_dist_kernel(Dist
       }
     }
   }
+#endif
   __syncthreads();
 
   const bool ntrans = tl.flags & 1u;
@@ -632,7 +768,8 @@ __global__ void __launch_bounds__(SING_THREADS, 1) near_sing_kernel(SingArgs a) 
 template <int Q, int KK, bool RL, bool CL, bool F32 = false>
 int launch_dist(const h2b_near_launch *L, cudaStream_t st) {
   constexpr int PLANES = KT<KK>::CPLX ? 2 : KT<KK>::NOUT;
-  const size_t smem = sizeof(double) * PLANES * H2B_TILE_MAX * H2B_TILE_MAX;
+  const size_t smem = sizeof(double) * PLANES * H2B_TILE_MAX * H2B_TILE_MAX +
+                      (H2B_DIST_STAGE ? sizeof(DistStage) : 0);
   H2B_CUDA_TRY((h2b_allow_smem<near_dist_kernel<Q, KK, RL, CL, F32>>()));
   DistArgs a;
   a.tri = (const TriRec *) L->tri;
