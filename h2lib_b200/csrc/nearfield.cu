@@ -59,8 +59,8 @@ constexpr int SIDE_MAXP = 25;
 #ifndef H2B_DIST_TENSOR
 #define H2B_DIST_TENSOR 1
 #endif
-// 1: the lanes of a warp visit row triangles spread over the tile's list (see near_dist_kernel);
-// measured 3% slower on config 2 than consecutive rows (0, the default), kept as an option
+// 1: the lanes of a warp visit row triangles spread over the tile's list (stage position e holds
+// list entry e * 17 mod n), so that fewer lanes add to the same tile entry at once; 0: list order
 #ifndef H2B_DIST_PERMUTE
 #define H2B_DIST_PERMUTE 0
 #endif
@@ -410,8 +410,16 @@ __global__ void __launch_bounds__(256, H2B_DIST_MINBLOCKS) near_dist_kernel(Dist
           }
         }
         if (c0 == 0 || ntr > (uint32_t) DIST_CHUNK) {
+#if H2B_DIST_PERMUTE
+          const uint32_t rmul = (nr % 17u) ? 17u : 19u;  // prime, coprime to nr <= 128
+#endif
           for (uint32_t e = threadIdx.x; e < nr; e += blockDim.x) {
-            const TriRef rt = a.refs[tl.tr_off + r0 + e];
+#if H2B_DIST_PERMUTE
+            const uint32_t src = (e * rmul) % nr;
+#else
+            const uint32_t src = e;
+#endif
+            const TriRef rt = a.refs[tl.tr_off + r0 + src];
             const TriRec &T = a.tri[rt.t];
 #pragma unroll
             for (int d = 0; d < 3; d++) {
