@@ -17,7 +17,7 @@ H2B_OK = 0
 BASIS_CONSTANT = ord("c")
 BASIS_LINEAR = ord("l")
 LAPLACE, HELMHOLTZ = 0, 1
-SLP, DLP = 0, 1
+SLP, DLP, ADLP = 0, 1, 2
 MESH_SPHERE, MESH_CUBE = 0, 1
 
 _u32p = np.ctypeslib.ndpointer(np.uint32, flags="C_CONTIGUOUS")

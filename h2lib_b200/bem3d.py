@@ -8,13 +8,14 @@ import ctypes as C
 
 import numpy as np
 
-from ._lib import (BASIS_CONSTANT, BASIS_LINEAR, DLP, HELMHOLTZ, LAPLACE, MESH_CUBE,
+from ._lib import (ADLP, BASIS_CONSTANT, BASIS_LINEAR, DLP, HELMHOLTZ, LAPLACE, MESH_CUBE,
                    MESH_SPHERE, SLP, H2BError, check, checkp, lib)
 
 __all__ = [
     "BASIS_CONSTANT_BEM3D", "BASIS_LINEAR_BEM3D", "Surface3d", "new_sphere_surface3d",
     "new_cube_surface3d", "new_slp_laplace_bem3d", "new_dlp_laplace_bem3d",
-    "new_slp_helmholtz_bem3d", "new_dlp_helmholtz_bem3d", "assemble_bem3d_amatrix",
+    "new_slp_helmholtz_bem3d", "new_dlp_helmholtz_bem3d", "new_adlp_laplace_bem3d",
+    "new_adlp_helmholtz_bem3d", "assemble_bem3d_amatrix",
     "nearfield", "Tree", "build_tree", "H2Matrix", "addeval_h2matrix_avector",
     "solve_gmres_h2matrix_avector", "solve_gmres", "quad_export",
 ]
@@ -156,6 +157,17 @@ def new_slp_helmholtz_bem3d(k, gr, q_regular, q_singular, row_basis, col_basis):
 def new_dlp_helmholtz_bem3d(k, gr, q_regular, q_singular, row_basis, col_basis, alpha):
     """Library/helmholtzbem3d.c:1177"""
     return Bem3d(gr, HELMHOLTZ, DLP, q_regular, q_singular, row_basis, col_basis, k=k,
+                 alpha=alpha)
+
+
+def new_adlp_laplace_bem3d(gr, q_regular, q_singular, row_basis, col_basis, alpha):
+    """Adjoint double layer K' + alpha M (Library/laplacebem3d.c:1180)"""
+    return Bem3d(gr, LAPLACE, ADLP, q_regular, q_singular, row_basis, col_basis, alpha=alpha)
+
+
+def new_adlp_helmholtz_bem3d(k, gr, q_regular, q_singular, row_basis, col_basis, alpha):
+    """Library/helmholtzbem3d.c:1346"""
+    return Bem3d(gr, HELMHOLTZ, ADLP, q_regular, q_singular, row_basis, col_basis, k=k,
                  alpha=alpha)
 
 

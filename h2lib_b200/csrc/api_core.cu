@@ -179,7 +179,8 @@ extern "C" h2b_bem *h2b_bem_new(const h2b_surface *s, int pde, int layer, int ro
     h2b_set_error("h2b_bem_new: NULL surface");
     return NULL;
   }
-  if ((pde != H2B_LAPLACE && pde != H2B_HELMHOLTZ) || (layer != H2B_SLP && layer != H2B_DLP) ||
+  if ((pde != H2B_LAPLACE && pde != H2B_HELMHOLTZ) ||
+      (layer != H2B_SLP && layer != H2B_DLP && layer != H2B_ADLP) ||
       (row_basis != H2B_BASIS_CONSTANT && row_basis != H2B_BASIS_LINEAR) ||
       (col_basis != H2B_BASIS_CONSTANT && col_basis != H2B_BASIS_LINEAR)) {
     h2b_set_error("h2b_bem_new: unknown pde/layer/basis (%d, %d, %d, %d)", pde, layer,
@@ -260,8 +261,9 @@ extern "C" void h2b_bem_del(h2b_bem *b) {
 }
 
 int h2b_bem_kernel_kind(const h2b_bem *b) {
-  if (b->pde == H2B_LAPLACE) return b->layer == H2B_SLP ? H2B_KK_LSLP : H2B_KK_LDLP;
-  return b->layer == H2B_SLP ? H2B_KK_HSLP : H2B_KK_HDLP;
+  if (b->pde == H2B_LAPLACE)
+    return b->layer == H2B_SLP ? H2B_KK_LSLP : b->layer == H2B_DLP ? H2B_KK_LDLP : H2B_KK_LADLP;
+  return b->layer == H2B_SLP ? H2B_KK_HSLP : b->layer == H2B_DLP ? H2B_KK_HDLP : H2B_KK_HADLP;
 }
 
 void h2b_fill_launch(const h2b_bem *b, h2b_near_launch *L) {

@@ -647,8 +647,9 @@ static int finish(h2b_h2matrix *h, int rc, unsigned phases) {
 
 static int row_basis(h2b_h2matrix *h) {
   mark(h, 0);
-  // row side: Lagrange polynomials (assemble_bem3d_lagrange_{c,l}_amatrix)
-  int rc = assemble_basis(h, h->rt, h->bem->row_basis, 0);
+  // row side: Lagrange polynomials (assemble_bem3d_lagrange_{c,l}_amatrix); normal derivatives
+  // for the adjoint double layer (assemble_bem3d_dn_lagrange_*, Library/laplacebem3d.c:1180)
+  int rc = assemble_basis(h, h->rt, h->bem->row_basis, h->bem->layer == H2B_ADLP);
   mark(h, 1);
   return rc;
 }

@@ -34,6 +34,8 @@ constexpr int KK_LDLP = H2B_KK_LDLP;
 constexpr int KK_LBOTH = H2B_KK_LBOTH;
 constexpr int KK_HSLP = H2B_KK_HSLP;
 constexpr int KK_HDLP = H2B_KK_HDLP;
+constexpr int KK_LADLP = H2B_KK_LADLP;
+constexpr int KK_HADLP = H2B_KK_HADLP;
 
 template <int KK> struct KT;
 template <> struct KT<KK_LSLP> { static constexpr int NCH = 1, NOUT = 1; static constexpr bool CPLX = false; };
@@ -41,6 +43,8 @@ template <> struct KT<KK_LDLP> { static constexpr int NCH = 1, NOUT = 1; static 
 template <> struct KT<KK_LBOTH> { static constexpr int NCH = 2, NOUT = 2; static constexpr bool CPLX = false; };
 template <> struct KT<KK_HSLP> { static constexpr int NCH = 2, NOUT = 1; static constexpr bool CPLX = true; };
 template <> struct KT<KK_HDLP> { static constexpr int NCH = 2, NOUT = 1; static constexpr bool CPLX = true; };
+template <> struct KT<KK_LADLP> { static constexpr int NCH = 1, NOUT = 1; static constexpr bool CPLX = false; };
+template <> struct KT<KK_HADLP> { static constexpr int NCH = 2, NOUT = 1; static constexpr bool CPLX = true; };
 
 // Distant tensor rules for q = 1..5 (q^4 points each): x0, x1, y0, y1, w.
 constexpr int DIST_TOTAL = 1 + 16 + 81 + 256 + 625;
@@ -66,8 +70,9 @@ constexpr int SIDE_MAXP = 25;
 #endif
 __constant__ double c_side[5][6][SIDE_MAXP];
 
-// Kernel values from r^2 = |x - y|^2 and dot = <x - y, n_y> (n_y: unit normal of the column
-// triangle; read only by the double layer kernels).
+// Kernel values from r^2 = |x - y|^2 and dot = <x - y, n> with n the unit normal of the column
+// triangle (double layer) or of the row triangle (adjoint double layer, whose kernels take
+// <y - x, n_x> = -dot: Library/laplacebem3d.c:136, Library/helmholtzbem3d.c:209).
 template <int KK>
 __device__ __forceinline__ void eval_kernel(double r2, double dot, double k_re, double k_imn,
                                             double kv[2]) {
@@ -76,6 +81,8 @@ __device__ __forceinline__ void eval_kernel(double r2, double dot, double k_re, 
     kv[0] = rinv;
   } else if constexpr (KK == KK_LDLP) {
     kv[0] = dot * (rinv * rinv * rinv);
+  } else if constexpr (KK == KK_LADLP) {
+    kv[0] = -dot * (rinv * rinv * rinv);
   } else if constexpr (KK == KK_LBOTH) {
     kv[0] = rinv;
     kv[1] = dot * (rinv * rinv * rinv);
@@ -85,8 +92,8 @@ __device__ __forceinline__ void eval_kernel(double r2, double dot, double k_re, 
     sincos(k_re * r, &s, &c);
     kv[0] = rn * c;
     kv[1] = rn * s;
-  } else {  // KK_HDLP
-    double re = (rinv * rinv * rinv) * dot, r = r2 * rinv, s, c;
+  } else {  // KK_HDLP, KK_HADLP
+    double re = (rinv * rinv * rinv) * (KK == KK_HADLP ? -dot : dot), r = r2 * rinv, s, c;
     if (k_imn != 0.0) re *= exp(k_imn * r);
     double kr = k_re * r;
     sincos(kr, &s, &c);
@@ -97,7 +104,13 @@ __device__ __forceinline__ void eval_kernel(double r2, double dot, double k_re, 
 
 template <int KK>
 constexpr bool uses_normal() {
-  return KK == KK_LDLP || KK == KK_LBOTH || KK == KK_HDLP;
+  return KK == KK_LDLP || KK == KK_LBOTH || KK == KK_HDLP || KK == KK_LADLP || KK == KK_HADLP;
+}
+
+// the adjoint double layer differentiates in the row triangle's normal direction
+template <int KK>
+constexpr bool row_normal() {
+  return KK == KK_LADLP || KK == KK_HADLP;
 }
 
 __device__ __forceinline__ double vtx(const TriRec &T, int i, int d) {
@@ -234,6 +247,8 @@ __device__ __forceinline__ void eval_kernel_f(float r2, float dot, float k_re, f
     kv[0] = rinv;
   } else if constexpr (KK == KK_LDLP) {
     kv[0] = dot * (rinv * rinv * rinv);
+  } else if constexpr (KK == KK_LADLP) {
+    kv[0] = -dot * (rinv * rinv * rinv);
   } else if constexpr (KK == KK_LBOTH) {
     kv[0] = rinv;
     kv[1] = dot * (rinv * rinv * rinv);
@@ -243,8 +258,8 @@ __device__ __forceinline__ void eval_kernel_f(float r2, float dot, float k_re, f
     sincosf(k_re * r, &s, &c);
     kv[0] = rn * c;
     kv[1] = rn * s;
-  } else {  // KK_HDLP
-    float re = (rinv * rinv * rinv) * dot, r = r2 * rinv, s, c;
+  } else {  // KK_HDLP, KK_HADLP
+    float re = (rinv * rinv * rinv) * (KK == KK_HADLP ? -dot : dot), r = r2 * rinv, s, c;
     if (k_imn != 0.0f) re *= expf(k_imn * r);
     const float kr = k_re * r;
     sincosf(kr, &s, &c);
@@ -347,7 +362,7 @@ constexpr int DIST_CHUNK = 128;
 // Staged triangles of one chunk pair.  Edge vectors are formed once per triangle here (the same
 // subtractions pair_geo_id makes per pair, so the pair geometry is bitwise the same).
 struct DistStage {
-  double r[10][DIST_CHUNK];  // row triangles: A (3), B - A (3), C - B (3), Gram determinant
+  double r[13][DIST_CHUNK];  // row triangles: A (3), B - A (3), C - B (3), Gram determinant, n
   double c[13][DIST_CHUNK];  // column triangles: A, B - A, C - B, Gram determinant * kconst, n
   uint32_t rv[3][DIST_CHUNK], cv[3][DIST_CHUNK];  // vertex ids
   int32_t rl[3][DIST_CHUNK], cl[3][DIST_CHUNK];   // local output row / column per vertex
@@ -426,6 +441,7 @@ __global__ void __launch_bounds__(256, H2B_DIST_MINBLOCKS) near_dist_kernel(Dist
               sg.r[d][e] = T.a[d];
               sg.r[3 + d][e] = T.b[d] - T.a[d];
               sg.r[6 + d][e] = T.c[d] - T.b[d];
+              sg.r[10 + d][e] = T.n[d];
               sg.rv[d][e] = T.v[d];
               sg.rl[d][e] = rt.l[d];
             }
@@ -459,7 +475,9 @@ __global__ void __launch_bounds__(256, H2B_DIST_MINBLOCKS) near_dist_kernel(Dist
           g.q1[d] = sg.c[3 + d][ci];
           g.q2[d] = sg.c[6 + d][ci];
         }
-        const double n0 = sg.c[10][ci], n1 = sg.c[11][ci], n2 = sg.c[12][ci];
+        const double(&nn)[13][DIST_CHUNK] = row_normal<KK>() ? sg.r : sg.c;
+        const uint32_t ni = row_normal<KK>() ? ri : ci;
+        const double n0 = nn[10][ni], n1 = nn[11][ni], n2 = nn[12][ni];
         double acc[NCH][NR][NC];
 #pragma unroll
         for (int c = 0; c < NCH; c++)
@@ -533,7 +551,8 @@ __global__ void __launch_bounds__(256, H2B_DIST_MINBLOCKS) near_dist_kernel(Dist
 
     PairGeo g;
     pair_geo_id(T, S, g);
-    const double n0 = S.n[0], n1 = S.n[1], n2 = S.n[2];
+    const TriRec &NT = row_normal<KK>() ? T : S;  // triangle whose normal the kernel uses
+    const double n0 = NT.n[0], n1 = NT.n[1], n2 = NT.n[2];
     double acc[NCH][NR][NC];
 #pragma unroll
     for (int c = 0; c < NCH; c++)
@@ -685,7 +704,8 @@ __global__ void __launch_bounds__(SING_THREADS, 1) near_sing_kernel(SingArgs a) 
     const TriRec &S = a.tri[st.t];
     PairGeo g;
     pair_geo(T, S, tp, sq, g);
-    const double n0 = S.n[0], n1 = S.n[1], n2 = S.n[2];
+    const TriRec &NT = row_normal<KK>() ? T : S;  // triangle whose normal the kernel uses
+    const double n0 = NT.n[0], n1 = NT.n[1], n2 = NT.n[2];
     const uint32_t n = a.rule_n[cs];
     const double *rx0 = rules + a.rule_off[cs];
     const double *rx1 = rx0 + n, *ry0 = rx0 + 2 * n, *ry1 = rx0 + 3 * n, *rw = rx0 + 4 * n;
@@ -1007,6 +1027,8 @@ extern "C" int h2b_near_launch_kernels(const h2b_near_launch *L, cudaStream_t st
     case KK_LBOTH: return launch_kk<KK_LBOTH>(L, st);
     case KK_HSLP: return launch_kk<KK_HSLP>(L, st);
     case KK_HDLP: return launch_kk<KK_HDLP>(L, st);
+    case KK_LADLP: return launch_kk<KK_LADLP>(L, st);
+    case KK_HADLP: return launch_kk<KK_HADLP>(L, st);
     default: h2b_set_error("unknown kernel kind %d", L->kk); return H2B_ERR_ARG;
   }
 }

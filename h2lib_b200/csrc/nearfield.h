@@ -17,6 +17,8 @@ extern "C" {
 #define H2B_KK_LBOTH 2  /* Laplace single and double layer together (two real outputs) */
 #define H2B_KK_HSLP 3   /* Helmholtz single layer, complex */
 #define H2B_KK_HDLP 4   /* Helmholtz double layer, complex */
+#define H2B_KK_LADLP 5  /* Laplace adjoint double layer (row normal), real */
+#define H2B_KK_HADLP 6  /* Helmholtz adjoint double layer (row normal), complex */
 
 typedef struct {
   int kk;

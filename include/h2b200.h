@@ -49,6 +49,7 @@ extern "C" {
 
 #define H2B_SLP 0
 #define H2B_DLP 1
+#define H2B_ADLP 2 /* adjoint double layer K' (normal derivative in x) */
 
 #define H2B_MESH_SPHERE 0
 #define H2B_MESH_CUBE 1
@@ -167,10 +168,13 @@ void h2b_surface_del(h2b_surface *s);
  *   new_dlp_laplace_bem3d(gr, q_regular, q_singular, row, col, alpha) Library/laplacebem3d.c:1012
  *   new_slp_helmholtz_bem3d(k, gr, q_regular, q_singular, row, col)   Library/helmholtzbem3d.c:1008
  *   new_dlp_helmholtz_bem3d(k, gr, ..., alpha)                        Library/helmholtzbem3d.c:1177
- * pde H2B_LAPLACE / H2B_HELMHOLTZ, layer H2B_SLP / H2B_DLP; (k_re, k_im) the wave number
- * (Helmholtz only; H2Lib's convention e^{i k r} with damping for Im k > 0); (alpha_re, alpha_im)
- * the coefficient of the identity added to the DLP (H2Lib's bem->alpha: 0.5*alpha*g on the cc
- * diagonal, alpha*mass*g for linear bases). */
+ *   new_adlp_laplace_bem3d(gr, q_regular, q_singular, row, col, alpha) Library/laplacebem3d.c:1180
+ *   new_adlp_helmholtz_bem3d(k, gr, ..., alpha)                       Library/helmholtzbem3d.c:1346
+ * pde H2B_LAPLACE / H2B_HELMHOLTZ, layer H2B_SLP / H2B_DLP / H2B_ADLP; (k_re, k_im) the wave
+ * number (Helmholtz only; H2Lib's convention e^{i k r} with damping for Im k > 0); (alpha_re,
+ * alpha_im) the coefficient of the identity added to the DLP or adjoint DLP (H2Lib's bem->alpha:
+ * 0.5*alpha*g on the cc diagonal, alpha*mass*g for linear bases).  The adjoint double layer's
+ * H2 row basis carries the normal derivative of the interpolation polynomials. */
 h2b_bem *h2b_bem_new(const h2b_surface *s, int pde, int layer, int row_basis, int col_basis,
                      uint32_t q_regular, uint32_t q_singular, double k_re, double k_im,
                      double alpha_re, double alpha_im);

@@ -6,8 +6,8 @@
  *                                     :549 pair classification / vertex permutation
  *   Library/bem3d.c:1151              assemble_cc_near_bem3d
  *   Library/bem3d.c:1798/2394/3038    assemble_{cl,lc,ll}_near_bem3d
- *   Library/laplacebem3d.c:36/84      Laplace single / double layer kernels
- *   Library/helmholtzbem3d.c:27/140   Helmholtz single / double layer kernels
+ *   Library/laplacebem3d.c:36/84/136      Laplace single / double / adjoint double layer kernels
+ *   Library/helmholtzbem3d.c:27/140/209   Helmholtz single / double / adjoint double layer
  *   Library/bem3d.c:4978/5179/5236    Chebyshev points and interpolation boxes
  *   Library/bem3d.c:7555-8540         Lagrange polynomials, leaf bases (c/l, normal derivative),
  *                                     transfer matrices
@@ -260,18 +260,23 @@ op_init(op_t *o, uint32_t nv, const double *x, uint32_t nt, const uint32_t *t, c
   return 0;
 }
 
-/* kernel at (x, y) with column normal ny */
+/* kernel at (x, y) with row normal nx and column normal ny; layer 0 single, 1 double, 2 adjoint
+ * double layer (Library/laplacebem3d.c:36/84/136, Library/helmholtzbem3d.c:27/140/209) */
 static cplx
-kernel(const op_t *o, const double *xx, const double *yy, const double *ny)
+kernel(const op_t *o, const double *xx, const double *yy, const double *nx, const double *ny)
 {
   double d[3] = {xx[0] - yy[0], xx[1] - yy[1], xx[2] - yy[2]};
   double n2 = d[0] * d[0] + d[1] * d[1] + d[2] * d[2];
-  double rn = 1.0 / sqrt(n2);
+  double rn = 1.0 / sqrt(n2), dot = 0.0;
+  if (o->layer == 1)
+    dot = d[0] * ny[0] + d[1] * ny[1] + d[2] * ny[2];
+  else if (o->layer == 2)  /* <y - x, n_x> */
+    dot = (yy[0] - xx[0]) * nx[0] + (yy[1] - xx[1]) * nx[1] + (yy[2] - xx[2]) * nx[2];
   if (o->pde == 0) {
     if (o->layer == 0)
       return rn;
     rn = rn * rn * rn;
-    return (d[0] * ny[0] + d[1] * ny[1] + d[2] * ny[2]) * rn;
+    return dot * rn;
   }
   if (o->layer == 0) {
     double norm = n2 * rn;
@@ -281,7 +286,7 @@ kernel(const op_t *o, const double *xx, const double *yy, const double *ny)
     return rn * cos(norm) + (sin(norm) * rn) * I;
   }
   {
-    double re = (rn * rn * rn) * (d[0] * ny[0] + d[1] * ny[1] + d[2] * ny[2]);
+    double re = (rn * rn * rn) * dot;
     double norm = n2 * rn, s, c;
     if (o->k_imn != 0.0)
       re *= exp(o->k_imn * norm);
@@ -346,7 +351,7 @@ pair_integrals(const op_t *o, uint32_t tt, uint32_t ss, cplx *res, uint32_t *tp,
                *Ct = o->x + 3 * (size_t) tv[tp[2]];
   const double *As = o->x + 3 * (size_t) sv[sp[0]], *Bs = o->x + 3 * (size_t) sv[sp[1]],
                *Cs = o->x + 3 * (size_t) sv[sp[2]];
-  const double *ny = o->n + 3 * (size_t) ss;
+  const double *nx = o->n + 3 * (size_t) tt, *ny = o->n + 3 * (size_t) ss;
   int rl = o->rb == ORC_BASIS_LINEAR, cl = o->cb == ORC_BASIS_LINEAR;
   for (l = 0; l < 9; l++)
     res[l] = 0.0;
@@ -360,7 +365,7 @@ pair_integrals(const op_t *o, uint32_t tt, uint32_t ss, cplx *res, uint32_t *tp,
       xx[d] = At[d] * Ax + Bt[d] * Bx + Ct[d] * Cx;
       yy[d] = As[d] * Ay + Bs[d] * By + Cs[d] * Cy;
     }
-    kv = kernel(o, xx, yy, ny);
+    kv = kernel(o, xx, yy, nx, ny);
     for (k = 0; k < (cl ? 3u : 1u); k++)
       for (l = 0; l < (rl ? 3u : 1u); l++)
         res[l + 3 * k] += (r->w[q] * nodal(rl, l, tx, sx) * nodal(cl, k, ty, sy)) * kv;
@@ -628,7 +633,8 @@ ctree_init(ctree_t *c, uint32_t nc, const uint32_t *rec, const double *box, uint
 }
 
 /* Leaf basis of cluster c: V[i, nu] (size x k, column-major), row basis or column basis
- * (dn selects the normal-derivative version used for the DLP column side). */
+ * (dn selects the normal-derivative version: the double layer's column side, the adjoint double
+ * layer's row side). */
 static void
 leaf_basis(const orc_h2 *h, const ctree_t *c, uint32_t cid, int linear, int dn, cplx *V)
 {
@@ -766,7 +772,7 @@ coupling(const orc_h2 *h, uint32_t r, uint32_t c, cplx *S)
   }
   for (j = 0; j < k; j++)
     for (i = 0; i < k; i++)
-      S[i + (size_t) j * k] = KCONST * kernel(&slp, X[i], Y[j], NULL);
+      S[i + (size_t) j * k] = KCONST * kernel(&slp, X[i], Y[j], NULL, NULL);
   free(X);
   free(Y);
 }
@@ -816,9 +822,9 @@ orc_h2_new(uint32_t nv, const double *x, uint32_t nt, const uint32_t *t, const d
   h->boff = malloc(8 * nb);
   if (!h->brc || !h->bcc || !h->badm || !h->boff) goto fail;
   memcpy(h->brc, brc, 4 * nb); memcpy(h->bcc, bcc, 4 * nb); memcpy(h->badm, badm, nb);
-  /* row basis: plain Lagrange (normal derivative for the adjoint DLP, not used here);
-   * column basis: normal derivative for the double layer operator */
-  if (build_basis(h, &h->rt, row_basis == ORC_BASIS_LINEAR, 0)
+  /* row basis: normal derivative for the adjoint double layer operator; column basis: normal
+   * derivative for the double layer operator (assemble_bem3d_dn_lagrange_*) */
+  if (build_basis(h, &h->rt, row_basis == ORC_BASIS_LINEAR, layer == 2)
       || build_basis(h, &h->ct, col_basis == ORC_BASIS_LINEAR, layer == 1)) goto fail;
   for (b = 0; b < nb; b++) {
     if (badm[b]) { h->boff[b] = stot; stot += (uint64_t) h->k * h->k; }

@@ -86,7 +86,7 @@ class Mesh:
         self.nv, self.nt = self.x.shape[0], self.t.shape[0]
 
 
-LAPLACE, HELMHOLTZ, SLP, DLP = 0, 1, 0, 1
+LAPLACE, HELMHOLTZ, SLP, DLP, ADLP = 0, 1, 0, 1, 2
 
 
 def nearfield(mesh, pde, layer, rb, cb, ridx=None, cidx=None, q=2, q2=4, k=0.0, alpha=0.0,

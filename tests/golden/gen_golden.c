@@ -6,8 +6,8 @@
  * Built twice: without USE_COMPLEX (Laplace, real field) and with it (Helmholtz, complex field).
  *
  * Usage: gen_golden <outdir> <section> [...]
- * Sections (real build):    quad sphere8 sphere4 h2small config2 cube
- * Sections (complex build): helm_sphere4 helm_h2small config3 helm_gmres
+ * Sections (real build):    quad sphere8 sphere4 h2small config2 cube adlp
+ * Sections (complex build): helm_sphere4 helm_h2small config3 helm_gmres helm_adlp
  */
 #include <math.h>
 #include <stdio.h>
@@ -335,6 +335,82 @@ dump_h2parts(const char *prefix, pch2matrix G, uint limit)
   free(N.v);
 }
 
+/* Dense nearfield matrix of an operator on the whole mesh (all pairs), and for the linear-linear
+ * case a ragged sub-block and its transposed write. */
+static void
+dense_op(const char *prefix, psurface3d gr, pbem3d op, basisfunctionbem3d rb,
+         basisfunctionbem3d cb, int with_block)
+{
+  uint n = (rb == BASIS_LINEAR_BEM3D) ? gr->vertices : gr->triangles;
+  uint m = (cb == BASIS_LINEAR_BEM3D) ? gr->vertices : gr->triangles;
+  pamatrix A = new_amatrix(n, m);
+  char name[256];
+
+  op->nearfield(NULL, NULL, op, false, A);
+  dump_amatrix(prefix, A);
+  del_amatrix(A);
+  if (with_block) {
+    uint ridx[7] = { 5, 9, 20, 33, 2, 61, 40 };
+    uint cidx[5] = { 1, 40, 2, 60, 65 };
+    pamatrix B = new_amatrix(7, 5), Bt = new_amatrix(5, 7);
+    op->nearfield(ridx, cidx, op, false, B);
+    snprintf(name, sizeof(name), "%s_block", prefix);
+    dump_amatrix(name, B);
+    op->nearfield(ridx, cidx, op, true, Bt);
+    snprintf(name, sizeof(name), "%s_block_trans", prefix);
+    dump_amatrix(name, Bt);
+    del_amatrix(B);
+    del_amatrix(Bt);
+  }
+}
+
+/* H2 matrix of one operator on the mesh: trees, row and column bases, the first coupling and
+ * nearfield blocks, and a matvec with a seeded vector. */
+static void
+h2_op(const char *prefix, psurface3d gr, pbem3d op, basisfunctionbem3d basis, uint clf,
+      real eta, uint m, uint parts_limit)
+{
+  pcluster root;
+  pblock broot;
+  pclusterbasis rb, cb;
+  ph2matrix G;
+  pavector x, y;
+  char name[256];
+
+  root = build_bem3d_cluster(op, clf, basis);
+  broot = build_strict_block(root, root, &eta, admissible_max_cluster);
+  dump_cluster(prefix, root);
+  dump_block(prefix, broot, root, root);
+  rb = build_from_cluster_clusterbasis(root);
+  cb = build_from_cluster_clusterbasis(root);
+  G = build_from_block_h2matrix(broot, rb, cb);
+  setup_h2matrix_aprx_inter_bem3d(op, rb, cb, broot, m);
+  assemble_bem3d_h2matrix_row_clusterbasis(op, rb);
+  assemble_bem3d_h2matrix_col_clusterbasis(op, cb);
+  assemble_bem3d_h2matrix(op, G);
+  snprintf(name, sizeof(name), "%s_row", prefix);
+  dump_basis(name, rb);
+  snprintf(name, sizeof(name), "%s_col", prefix);
+  dump_basis(name, cb);
+  snprintf(name, sizeof(name), "%s_parts", prefix);
+  dump_h2parts(name, G, parts_limit);
+  x = new_avector(G->cb->t->size);
+  y = new_avector(G->rb->t->size);
+  seeded_avector(x, 5);
+  snprintf(name, sizeof(name), "%s_x", prefix);
+  dump_avector(name, x);
+  clear_avector(y);
+  addeval_h2matrix_avector(1.0, G, x, y);
+  snprintf(name, sizeof(name), "%s_y", prefix);
+  dump_avector(name, y);
+  del_avector(x);
+  del_avector(y);
+  del_h2matrix(G);
+  del_block(broot);
+  freemem(root->idx);
+  del_cluster(root);
+}
+
 /* ---------- sections ---------- */
 
 #ifndef USE_COMPLEX
@@ -636,6 +712,40 @@ section_cube(void)
   del_macrosurface3d(mg);
 }
 
+/* Adjoint double layer K' + M/2 (new_adlp_laplace_bem3d, Library/laplacebem3d.c:1180): dense on
+ * the sphere refined x4 for the four basis pairs, and H2 matrices on the sphere refined x8. */
+static void
+section_adlp(void)
+{
+  pmacrosurface3d mg = new_sphere_macrosurface3d();
+  psurface3d g4 = build_from_macrosurface3d_surface3d(mg, 4);
+  psurface3d g8 = build_from_macrosurface3d_surface3d(mg, 8);
+  basisfunctionbem3d C = BASIS_CONSTANT_BEM3D, L = BASIS_LINEAR_BEM3D;
+  pbem3d op;
+
+  op = new_adlp_laplace_bem3d(g4, 2, 4, C, C, 0.5);
+  dense_op("ad4cc", g4, op, C, C, 0);
+  del_laplace_bem3d(op);
+  op = new_adlp_laplace_bem3d(g4, 2, 4, L, L, 0.5);
+  dense_op("ad4ll", g4, op, L, L, 1);
+  del_laplace_bem3d(op);
+  op = new_adlp_laplace_bem3d(g4, 2, 4, C, L, 0.5);
+  dense_op("ad4cl", g4, op, C, L, 0);
+  del_laplace_bem3d(op);
+  op = new_adlp_laplace_bem3d(g4, 2, 4, L, C, 0.5);
+  dense_op("ad4lc", g4, op, L, C, 0);
+  del_laplace_bem3d(op);
+  op = new_adlp_laplace_bem3d(g8, 2, 4, L, L, 0.5);
+  h2_op("adh2ll", g8, op, L, 16, 1.4, 3, 24);
+  del_laplace_bem3d(op);
+  op = new_adlp_laplace_bem3d(g8, 2, 4, C, C, 0.5);
+  h2_op("adh2cc", g8, op, C, 16, 1.4, 3, 24);
+  del_laplace_bem3d(op);
+  del_surface3d(g4);
+  del_surface3d(g8);
+  del_macrosurface3d(mg);
+}
+
 #else /* USE_COMPLEX */
 
 static void
@@ -830,6 +940,32 @@ section_config3(void)
   del_stopwatch(sw);
 }
 
+/* Helmholtz adjoint double layer K' + M/2 (new_adlp_helmholtz_bem3d, Library/helmholtzbem3d.c:
+ * 1346), constant basis: dense on the sphere refined x4 (k = 2 and the damped k = 2 + 0.5i) and
+ * the H2 matrix on the sphere refined x8 (k = 2). */
+static void
+section_helm_adlp(void)
+{
+  pmacrosurface3d mg = new_sphere_macrosurface3d();
+  psurface3d g4 = build_from_macrosurface3d_surface3d(mg, 4);
+  psurface3d g8 = build_from_macrosurface3d_surface3d(mg, 8);
+  basisfunctionbem3d C = BASIS_CONSTANT_BEM3D;
+  pbem3d op;
+
+  op = new_adlp_helmholtz_bem3d(2.0, g4, 2, 4, C, C, 0.5);
+  dense_op("had4cc", g4, op, C, C, 0);
+  del_helmholtz_bem3d(op);
+  op = new_adlp_helmholtz_bem3d(2.0 + 0.5 * I, g4, 2, 4, C, C, 0.5);
+  dense_op("had4cc_damped", g4, op, C, C, 0);
+  del_helmholtz_bem3d(op);
+  op = new_adlp_helmholtz_bem3d(2.0, g8, 2, 4, C, C, 0.5);
+  h2_op("hadh2cc", g8, op, C, 16, 1.4, 3, 24);
+  del_helmholtz_bem3d(op);
+  del_surface3d(g4);
+  del_surface3d(g8);
+  del_macrosurface3d(mg);
+}
+
 /* The reference's complex GMRES on a small Brakhage-Werner system: sphere refined x10 (800
  * triangles), constant basis, k = 5, leaf 32, eta 1.4, m = 4, seeded right-hand side, GMRES(80)
  * to 1e-8.  Records the iteration count, the solution and its true relative residual
@@ -934,6 +1070,8 @@ main(int argc, char **argv)
       section_config2();
     else if (!strcmp(argv[i], "cube"))
       section_cube();
+    else if (!strcmp(argv[i], "adlp"))
+      section_adlp();
 #else
     if (!strcmp(argv[i], "helm_sphere4"))
       section_helm_sphere4();
@@ -943,6 +1081,8 @@ main(int argc, char **argv)
       section_config3();
     else if (!strcmp(argv[i], "helm_gmres"))
       section_helm_gmres();
+    else if (!strcmp(argv[i], "helm_adlp"))
+      section_helm_adlp();
 #endif
     else {
       fprintf(stderr, "unknown section %s\n", argv[i]);

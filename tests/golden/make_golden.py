@@ -7,7 +7,8 @@ read the committed .npz files.
 
     python tests/golden/make_golden.py [section ...]
 
-Sections: quad sphere8 sphere4 h2small config2 cube helm_sphere4 helm_h2small config3 helm_gmres
+Sections: quad sphere8 sphere4 h2small config2 cube adlp helm_sphere4 helm_h2small config3
+helm_gmres helm_adlp
 """
 import os
 import subprocess
@@ -21,12 +22,16 @@ ROOT = os.path.dirname(os.path.dirname(HERE))
 REF = os.environ.get("REF", "/root/reference")
 REFOUT = os.path.join(ROOT, "oracle", "_ref")
 
-REAL_SECTIONS = ["quad", "sphere8", "sphere4", "h2small", "config2", "cube"]
-COMPLEX_SECTIONS = ["helm_sphere4", "helm_h2small", "config3", "helm_gmres"]
+REAL_SECTIONS = ["quad", "sphere8", "sphere4", "h2small", "config2", "cube", "adlp"]
+COMPLEX_SECTIONS = ["helm_sphere4", "helm_h2small", "config3", "helm_gmres", "helm_adlp"]
 DTYPES = {"f8": np.float64, "u4": np.uint32, "c16": np.complex128}
 # Arrays stored only in part, to keep the fixtures small: name -> number of leading columns kept
 # (matrices are written column-major, i.e. shape (cols, rows)).
 CROP = {"c1_dlp": 128}
+# Arrays not stored: the adjoint double layer's transfer matrices and column bases equal the single
+# layer's, which other fixtures pin already.
+DROP = {f"{p}_{part}" for p in ("adh2ll", "adh2cc", "hadh2cc")
+        for part in ("row_E", "col_E", "col_V")}
 
 
 def build():
@@ -51,6 +56,8 @@ def run_section(exe, section):
             for line in fh:
                 parts = line.split()
                 name, dt, shape = parts[0], DTYPES[parts[1]], tuple(int(s) for s in parts[2:])
+                if name in DROP:
+                    continue
                 data = np.fromfile(os.path.join(tmp, name + ".bin"), dtype=dt)
                 data = data.reshape(shape)
                 if name in CROP:

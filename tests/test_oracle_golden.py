@@ -186,3 +186,47 @@ def test_complex_gmres_givens(gold):
     u2 = np.zeros_like(b)
     assert orc.gmres([K, V], [1.0, -1j * k], b, u2, 1e-8, 1000, 80, unitary=True) == it
     assert true_residual(u2) <= 1e-8
+
+
+@pytest.mark.parametrize("basis", ["cc", "ll", "cl", "lc"])
+def test_adjoint_double_layer_dense(gold, basis):
+    """K' + M/2 (new_adlp_laplace_bem3d, Library/laplacebem3d.c:1180) on the sphere refined x4."""
+    g, mesh = gold("adlp"), mesh_from(gold("sphere4"), "sphere4")
+    rb, cb = (L if basis[0] == "l" else C), (L if basis[1] == "l" else C)
+    A = orc.nearfield(mesh, orc.LAPLACE, orc.ADLP, rb, cb, alpha=0.5)
+    assert rel_entry_err(A, fortran(g[f"ad4{basis}"])) < 1e-12
+    if basis == "ll":
+        s4 = gold("sphere4")
+        ridx, cidx = s4["block_ridx"], s4["block_cidx"]
+        A = orc.nearfield(mesh, orc.LAPLACE, orc.ADLP, L, L, ridx, cidx, alpha=0.5)
+        assert rel_entry_err(A, fortran(g["ad4ll_block"])) < 1e-12
+        A = orc.nearfield(mesh, orc.LAPLACE, orc.ADLP, L, L, ridx, cidx, alpha=0.5, ntrans=True)
+        assert rel_entry_err(A, fortran(g["ad4ll_block_trans"])) < 1e-12
+
+
+@pytest.mark.parametrize("prefix,basis", [("adh2ll", L), ("adh2cc", C)])
+def test_adjoint_double_layer_h2(gold, prefix, basis):
+    """H2 matrix of K' + M/2: the row basis carries the normal derivative of the Lagrange
+    polynomials (assemble_bem3d_dn_lagrange_*); coupling, nearfield and the matvec."""
+    g, mesh = gold("adlp"), mesh_from(gold("sphere8"), "sphere8")
+    tree, blocks = tree_arrays(g, prefix)
+    A = orc.H2(mesh, orc.LAPLACE, orc.ADLP, basis, basis, 3, tree, tree, blocks, alpha=0.5)
+    assert relerr(A.export(0), g[f"{prefix}_row_V"]) < 1e-12
+    assert relerr(A.export(4, 24), g[f"{prefix}_parts_S"]) < 1e-12
+    assert relerr(A.export(5, 24), g[f"{prefix}_parts_N"]) < 1e-12
+    y = A.addeval(1.0, g[f"{prefix}_x"], np.zeros(A.rows))
+    assert relerr(y, g[f"{prefix}_y"]) < 1e-12
+
+
+def test_adjoint_double_layer_helmholtz(gold):
+    g, mesh = gold("helm_adlp"), mesh_from(gold("sphere4"), "sphere4")
+    for name, k in (("had4cc", 2.0), ("had4cc_damped", 2.0 + 0.5j)):
+        A = orc.nearfield(mesh, orc.HELMHOLTZ, orc.ADLP, C, C, k=k, alpha=0.5)
+        assert rel_entry_err(A, fortran(g[name])) < 1e-12
+    mesh8 = mesh_from(gold("sphere8"), "sphere8")
+    tree, blocks = tree_arrays(g, "hadh2cc")
+    A = orc.H2(mesh8, orc.HELMHOLTZ, orc.ADLP, C, C, 3, tree, tree, blocks, k=2.0, alpha=0.5)
+    assert relerr(A.export(0), g["hadh2cc_row_V"]) < 1e-12
+    assert relerr(A.export(5, 24), g["hadh2cc_parts_N"]) < 1e-12
+    y = A.addeval(1.0, np.ascontiguousarray(g["hadh2cc_x"]), np.zeros(A.rows, dtype=np.complex128))
+    assert relerr(y, g["hadh2cc_y"]) < 1e-12
