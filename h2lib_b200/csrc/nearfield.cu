@@ -136,7 +136,8 @@ __device__ __forceinline__ void pair_geo(const TriRec &T, const TriRec &S, const
   }
 }
 
-__device__ __forceinline__ void pair_geo_id(const TriRec &T, const TriRec &S, PairGeo &g) {
+[[maybe_unused]] __device__ __forceinline__ void pair_geo_id(const TriRec &T, const TriRec &S,
+                                                             PairGeo &g) {
 #pragma unroll
   for (int d = 0; d < 3; d++) {
     g.d0[d] = T.a[d] - S.a[d];
@@ -381,7 +382,6 @@ __global__ void __launch_bounds__(256, H2B_DIST_MINBLOCKS) near_dist_kernel(Dist
   __syncthreads();
 
   const uint32_t ntr = tl.tr_len, nsc = tl.sc_len;
-  const uint32_t npairs = ntr * nsc;
   const int q = Q > 0 ? Q : a.q;
   const int nq = q * q * q * q;
   const double *cx0 = &c_dist[0][dist_off(Q > 0 ? Q : 1)];
@@ -536,6 +536,7 @@ __global__ void __launch_bounds__(256, H2B_DIST_MINBLOCKS) near_dist_kernel(Dist
 #else
   const uint32_t mult = 1u;
 #endif
+  const uint32_t npairs = ntr * nsc;
   for (uint32_t p = threadIdx.x; p < npairs; p += blockDim.x) {
     const uint32_t is = p / ntr, q = p - is * ntr;
     const uint32_t it = (uint32_t) (((uint64_t) q * mult) % ntr);
@@ -636,6 +637,12 @@ struct SingArgs {
   int *err;                   // set to 1 if the staging copy did not complete
 };
 
+// Points per lane in flight in the singular kernel's point loop (unroll factor).
+#ifndef H2B_SING_UNROLL
+#define H2B_SING_UNROLL 1
+#endif
+constexpr int SING_UNROLL = H2B_SING_UNROLL;
+
 // One warp per singular pair.  The three rules are copied into shared memory once per CTA.
 // 512 threads: one CTA per SM holds the staged rules, 16 warps hide the FP64 latencies.
 constexpr int SING_THREADS = 512;
@@ -717,6 +724,7 @@ __global__ void __launch_bounds__(SING_THREADS, 1) near_sing_kernel(SingArgs a) 
       for (int i = 0; i < NR; i++)
 #pragma unroll
         for (int j = 0; j < NC; j++) acc[c][i][j] = 0.0;
+#pragma unroll SING_UNROLL
     for (uint32_t k = lane; k < n; k += 32)
       quad_point<KK, RL, CL>(g, rx0[k], rx1[k], ry0[k], ry1[k], rw[k], n0, n1, n2, a.k_re, a.k_imn,
                              acc);
