@@ -403,6 +403,212 @@ __global__ void __launch_bounds__(TPB) backward_flat_kernel(MvmFlatArgs f, MvmVe
   }
 }
 
+// ------------------------------------------------------------------------------------------
+// Warp-per-item variant of the three flattened-path launches.  Every work item is a small dense
+// GEMV y_rows += P x_cols (a coupling block, a nearfield block, or a slice of a flattened basis)
+// and one warp does it alone: lane l owns rows l, l + 32, ... (WG_R per pass) and walks the
+// columns with WG_U columns' loads in flight; each row's sum reaches its output with one atomic
+// addition.  No shared memory and no barriers, so an SM keeps 64 warps' loads in flight, and a
+// panel serves up to WG_Q right-hand sides per read (the others are re-read from L2).
+// ------------------------------------------------------------------------------------------
+#ifndef H2B_MVM_WARP
+#define H2B_MVM_WARP 1
+#endif
+constexpr int WG_R = 4;  // rows per lane per pass (128 rows)
+constexpr int WG_U = 4;  // columns unrolled (loads in flight per row)
+constexpr int WG_Q = 4;  // right-hand sides per pass
+
+// One matrix entry, widened to FP64: (re, im) of P[e] (complex P interleaved).
+template <bool PCX, typename TP>
+__device__ __forceinline__ void load_entry(const TP *__restrict__ P, size_t e, double &re,
+                                           double &im) {
+  if constexpr (PCX) {
+    if constexpr (sizeof(TP) == 8) {
+      const double2 t = __ldg(reinterpret_cast<const double2 *>(P) + e);
+      re = t.x;
+      im = t.y;
+    } else {
+      const float2 t = __ldg(reinterpret_cast<const float2 *>(P) + e);
+      re = (double) t.x;
+      im = (double) t.y;
+    }
+  } else {
+    re = (double) __ldg(P + e);
+    im = 0.0;
+  }
+}
+
+// y_q[rows] += P x_q for the nq (<= NQ) right-hand sides given, P column-major (ld), real or
+// complex (PCX); x, y complex when CX.  Called by all lanes of one warp.
+template <bool CX, bool PCX, int NQ, typename TP>
+__device__ __forceinline__ void warp_gemv(const TP *__restrict__ P, uint32_t ld, uint32_t nrows,
+                                          uint32_t ncols, const double *const (&xq)[NQ],
+                                          double *const (&yq)[NQ], int nq) {
+  constexpr int WV = CX ? 2 : 1;
+  const uint32_t lane = threadIdx.x & 31u;
+  for (uint32_t r0 = 0; r0 < nrows; r0 += 32 * WG_R) {
+    double sr[NQ][WG_R], si[NQ][WG_R];
+#pragma unroll
+    for (int q = 0; q < NQ; q++)
+#pragma unroll
+      for (int i = 0; i < WG_R; i++) sr[q][i] = si[q][i] = 0.0;
+#pragma unroll WG_U
+    for (uint32_t c = 0; c < ncols; c++) {
+      double xr[NQ], xi[NQ];
+#pragma unroll
+      for (int q = 0; q < NQ; q++) {
+        xr[q] = q < nq ? __ldg(xq[q] + WV * c) : 0.0;
+        xi[q] = (CX && q < nq) ? __ldg(xq[q] + WV * c + 1) : 0.0;
+      }
+#pragma unroll
+      for (int i = 0; i < WG_R; i++) {
+        const uint32_t r = r0 + lane + 32u * i;
+        if (r < nrows) {
+          double pr, pi;
+          load_entry<PCX>(P, (size_t) r + (size_t) c * ld, pr, pi);
+#pragma unroll
+          for (int q = 0; q < NQ; q++) {
+            if (PCX) {
+              sr[q][i] = fma(pr, xr[q], fma(-pi, xi[q], sr[q][i]));
+              si[q][i] = fma(pr, xi[q], fma(pi, xr[q], si[q][i]));
+            } else {
+              sr[q][i] = fma(pr, xr[q], sr[q][i]);
+              if (CX) si[q][i] = fma(pr, xi[q], si[q][i]);
+            }
+          }
+        }
+      }
+    }
+#pragma unroll
+    for (int i = 0; i < WG_R; i++) {
+      const uint32_t r = r0 + lane + 32u * i;
+      if (r < nrows) {
+#pragma unroll
+        for (int q = 0; q < NQ; q++) {
+          if (q < nq) {
+            atomicAdd(yq[q] + WV * r, sr[q][i]);
+            if (CX) atomicAdd(yq[q] + WV * r + 1, si[q][i]);
+          }
+        }
+      }
+    }
+  }
+}
+
+// The item's work, applied to the unmasked right-hand sides in groups of NQ.  off_x / off_y:
+// offsets (in doubles) of the item's vector slices inside one column of the x / y work vector.
+template <bool CX, bool PCX, int NQ, typename TP>
+__device__ __forceinline__ void warp_item(const TP *__restrict__ P, uint32_t ld, uint32_t nrows,
+                                          uint32_t ncols, const MvmVecs &v, uint32_t seg,
+                                          const double *x0, size_t sx, double *y0, size_t sy) {
+  for (uint32_t q0 = 0; q0 < v.nrhs; q0 += NQ) {
+    const double *xq[NQ];
+    double *yq[NQ];
+    int nq = 0;
+#pragma unroll
+    for (int q = 0; q < NQ; q++) {
+      xq[q] = x0;
+      yq[q] = y0;
+    }
+    for (uint32_t q = q0; q < v.nrhs && q < q0 + NQ; q++)
+      if (col_on(v, seg, q)) {
+        // (nq < NQ: at most NQ columns per group)
+#pragma unroll
+        for (int s = 0; s < NQ; s++)
+          if (s == nq) {
+            xq[s] = x0 + q * sx;
+            yq[s] = y0 + q * sy;
+          }
+        nq++;
+      }
+    if (nq > 0) warp_gemv<CX, PCX, NQ>(P, ld, nrows, ncols, xq, yq, nq);
+  }
+}
+
+// Launch 1: forward items xt_c += W_c^T x[rows r0 .. r0 + nr of c] (W_c^T: k x |c|, ld k) and
+// the nearfield blocks yp_r += N_b xp_c, one warp each.
+template <bool CX, bool SINGLE, int NQ>
+__global__ void __launch_bounds__(TPB) forward_near_warp_kernel(MvmFlatArgs f, MvmCoupleArgs c,
+                                                                MvmVecs v) {
+  constexpr int W = CX ? 2 : 1;
+  const uint32_t item = blockIdx.x * (TPB / 32) + (threadIdx.x >> 5);
+  if (item < f.nitems) {
+    const uint32_t *it = f.items + 3 * (size_t) item;
+    const uint32_t cl = it[0], r0 = it[1], nr = it[2];
+    const uint32_t k = (uint32_t) f.k;
+    const uint32_t seg = v.cseg ? v.cseg[cl] : 0;
+    const double *x0 = v.xp + (size_t) W * (f.off[cl] + r0);
+    double *y0 = v.xt + (size_t) W * k * cl;
+    if (SINGLE)
+      warp_item<CX, false, NQ>(f.Ws + f.woff[cl] + (size_t) r0 * k, k, k, nr, v, seg, x0, v.sxp,
+                               y0, v.sxt);
+    else
+      warp_item<CX, false, NQ>(f.W + f.woff[cl] + (size_t) r0 * k, k, k, nr, v, seg, x0, v.sxp,
+                               y0, v.sxt);
+  } else if (item < f.nitems + c.nnear) {
+    const uint32_t nb = item - f.nitems;
+    const uint32_t r = c.near_rc[nb], cc = c.near_cc[nb];
+    const uint32_t seg = v.rseg ? v.rseg[r] : 0;
+    const uint32_t rows = c.rsize[r];
+    const double *x0 = v.xp + (size_t) W * c.coff[cc];
+    double *y0 = v.yp + (size_t) W * c.roff[r];
+    if (SINGLE)
+      warp_item<CX, CX, NQ>(c.Ns + (size_t) W * c.near_off[nb], rows, rows, c.csize[cc], v, seg,
+                            x0, v.sxp, y0, v.syp);
+    else
+      warp_item<CX, CX, NQ>(c.N + (size_t) W * c.near_off[nb], rows, rows, c.csize[cc], v, seg,
+                            x0, v.sxp, y0, v.syp);
+  }
+}
+
+// Launch 2: coupling blocks yt_r += S_b xt_c, one warp each.
+template <bool CX, bool SINGLE, int NQ>
+__global__ void __launch_bounds__(TPB) coupling_warp_kernel(MvmCoupleArgs a, MvmVecs v) {
+  constexpr int W = CX ? 2 : 1;
+  const uint32_t b = blockIdx.x * (TPB / 32) + (threadIdx.x >> 5);
+  if (b >= a.nadm) return;
+  const uint32_t k = (uint32_t) a.k;
+  const uint32_t seg = v.rseg ? v.rseg[a.adm_rc[b]] : 0;
+  const double *x0 = v.xt + (size_t) W * k * a.adm_cc[b];
+  double *y0 = v.yt + (size_t) W * k * a.adm_rc[b];
+  if (SINGLE)
+    warp_item<CX, CX, NQ>(a.Ss + (size_t) W * k * k * b, k, k, k, v, seg, x0, v.sxt, y0, v.syt);
+  else
+    warp_item<CX, CX, NQ>(a.S + (size_t) W * k * k * b, k, k, k, v, seg, x0, v.sxt, y0, v.syt);
+}
+
+// Launch 3: backward items yp[rows r0 .. r0 + nr of c] += W_c[r0:, :] yt_c (W_c: |c| x k,
+// ld |c|), one warp each.
+template <bool CX, bool SINGLE, int NQ>
+__global__ void __launch_bounds__(TPB) backward_warp_kernel(MvmFlatArgs f, MvmVecs v) {
+  constexpr int W = CX ? 2 : 1;
+  const uint32_t item = blockIdx.x * (TPB / 32) + (threadIdx.x >> 5);
+  if (item >= f.nitems) return;
+  const uint32_t *it = f.items + 3 * (size_t) item;
+  const uint32_t cl = it[0], r0 = it[1], nr = it[2];
+  const uint32_t k = (uint32_t) f.k;
+  const uint32_t seg = v.rseg ? v.rseg[cl] : 0;
+  const double *x0 = v.yt + (size_t) W * k * cl;
+  double *y0 = v.yp + (size_t) W * (f.off[cl] + r0);
+  if (SINGLE)
+    warp_item<CX, false, NQ>(f.Ws + f.woff[cl] + r0, f.size[cl], nr, k, v, seg, x0, v.syt, y0,
+                             v.syp);
+  else
+    warp_item<CX, false, NQ>(f.W + f.woff[cl] + r0, f.size[cl], nr, k, v, seg, x0, v.syt, y0,
+                             v.syp);
+}
+
+template <bool CX, bool SINGLE, int NQ>
+void launch_warp_items(const MvmPlan *p, const MvmVecs &v, cudaStream_t st) {
+  constexpr uint32_t WPB = TPB / 32;
+  const MvmCoupleArgs &ca = p->cpl;
+  const uint32_t n1 = p->ffwd.nitems + ca.nnear;
+  if (n1) forward_near_warp_kernel<CX, SINGLE, NQ><<<(n1 + WPB - 1) / WPB, TPB, 0, st>>>(p->ffwd, ca, v);
+  if (ca.nadm) coupling_warp_kernel<CX, SINGLE, NQ><<<(ca.nadm + WPB - 1) / WPB, TPB, 0, st>>>(ca, v);
+  if (p->fbwd.nitems)
+    backward_warp_kernel<CX, SINGLE, NQ><<<(p->fbwd.nitems + WPB - 1) / WPB, TPB, 0, st>>>(p->fbwd, v);
+}
+
 template <bool CX, bool SINGLE>
 int launch_flat(const MvmPlan *p, const double *x, size_t ldx, double *y, size_t ldy, double ar,
                 double ai, const MvmVecs &v, cudaStream_t st) {
@@ -414,12 +620,19 @@ int launch_flat(const MvmPlan *p, const double *x, size_t ldx, double *y, size_t
   const size_t nyp = W * p->nrow, nxt = W * (size_t) p->k * p->ncol_clusters,
                nyt = W * (size_t) p->k * p->nrow_clusters;
   gather_zero_kernel<CX><<<gz, 256, 0, st>>>(x, ldx, p->cidx, p->ncol, v, nyp, nxt, nyt);
-  if (p->ffwd.nitems + ca.nnear)
-    forward_flat_near_kernel<CX, SINGLE><<<p->ffwd.nitems + ca.nnear, TPB, 0, st>>>(p->ffwd, ca,
-                                                                                     v);
-  if (ca.nadm) coupling_flat_kernel<CX, SINGLE><<<ca.nadm, TPB, 0, st>>>(ca, v);
-  if (p->fbwd.nitems)
-    backward_flat_kernel<CX, SINGLE><<<p->fbwd.nitems, TPB, 0, st>>>(p->fbwd, v);
+  if (H2B_MVM_WARP) {
+    if (v.nrhs == 1)
+      launch_warp_items<CX, SINGLE, 1>(p, v, st);
+    else
+      launch_warp_items<CX, SINGLE, WG_Q>(p, v, st);
+  } else {
+    if (p->ffwd.nitems + ca.nnear)
+      forward_flat_near_kernel<CX, SINGLE><<<p->ffwd.nitems + ca.nnear, TPB, 0, st>>>(p->ffwd,
+                                                                                       ca, v);
+    if (ca.nadm) coupling_flat_kernel<CX, SINGLE><<<ca.nadm, TPB, 0, st>>>(ca, v);
+    if (p->fbwd.nitems)
+      backward_flat_kernel<CX, SINGLE><<<p->fbwd.nitems, TPB, 0, st>>>(p->fbwd, v);
+  }
   scatter_multi_kernel<CX><<<gz, 256, 0, st>>>(v, p->ridx, y, ldy, p->nrow, ar, ai);
   H2B_CUDA_TRY(cudaGetLastError());
   return H2B_OK;
