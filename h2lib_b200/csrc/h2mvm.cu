@@ -414,6 +414,10 @@ __global__ void __launch_bounds__(TPB) backward_flat_kernel(MvmFlatArgs f, MvmVe
 #ifndef H2B_MVM_WARP
 #define H2B_MVM_WARP 1
 #endif
+// resident CTAs per SM the warp kernels are compiled for (register budget 65536 / (256 * this))
+#ifndef H2B_MVM_WARP_MINB
+#define H2B_MVM_WARP_MINB 1
+#endif
 constexpr int WG_R = 4;  // rows per lane per pass (128 rows)
 constexpr int WG_U = 4;  // columns unrolled (loads in flight per row)
 constexpr int WG_Q = 4;  // right-hand sides per pass
@@ -528,7 +532,7 @@ __device__ __forceinline__ void warp_item(const TP *__restrict__ P, uint32_t ld,
 // Launch 1: forward items xt_c += W_c^T x[rows r0 .. r0 + nr of c] (W_c^T: k x |c|, ld k) and
 // the nearfield blocks yp_r += N_b xp_c, one warp each.
 template <bool CX, bool SINGLE, int NQ>
-__global__ void __launch_bounds__(TPB) forward_near_warp_kernel(MvmFlatArgs f, MvmCoupleArgs c,
+__global__ void __launch_bounds__(TPB, H2B_MVM_WARP_MINB) forward_near_warp_kernel(MvmFlatArgs f, MvmCoupleArgs c,
                                                                 MvmVecs v) {
   constexpr int W = CX ? 2 : 1;
   const uint32_t item = blockIdx.x * (TPB / 32) + (threadIdx.x >> 5);
@@ -563,7 +567,7 @@ __global__ void __launch_bounds__(TPB) forward_near_warp_kernel(MvmFlatArgs f, M
 
 // Launch 2: coupling blocks yt_r += S_b xt_c, one warp each.
 template <bool CX, bool SINGLE, int NQ>
-__global__ void __launch_bounds__(TPB) coupling_warp_kernel(MvmCoupleArgs a, MvmVecs v) {
+__global__ void __launch_bounds__(TPB, H2B_MVM_WARP_MINB) coupling_warp_kernel(MvmCoupleArgs a, MvmVecs v) {
   constexpr int W = CX ? 2 : 1;
   const uint32_t b = blockIdx.x * (TPB / 32) + (threadIdx.x >> 5);
   if (b >= a.nadm) return;
@@ -580,7 +584,7 @@ __global__ void __launch_bounds__(TPB) coupling_warp_kernel(MvmCoupleArgs a, Mvm
 // Launch 3: backward items yp[rows r0 .. r0 + nr of c] += W_c[r0:, :] yt_c (W_c: |c| x k,
 // ld |c|), one warp each.
 template <bool CX, bool SINGLE, int NQ>
-__global__ void __launch_bounds__(TPB) backward_warp_kernel(MvmFlatArgs f, MvmVecs v) {
+__global__ void __launch_bounds__(TPB, H2B_MVM_WARP_MINB) backward_warp_kernel(MvmFlatArgs f, MvmVecs v) {
   constexpr int W = CX ? 2 : 1;
   const uint32_t item = blockIdx.x * (TPB / 32) + (threadIdx.x >> 5);
   if (item >= f.nitems) return;
