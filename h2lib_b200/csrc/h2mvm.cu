@@ -404,12 +404,12 @@ __global__ void __launch_bounds__(TPB) backward_flat_kernel(MvmFlatArgs f, MvmVe
 }
 
 // ------------------------------------------------------------------------------------------
-// Warp-per-item variant of the three flattened-path launches.  Every work item is a small dense
-// GEMV y_rows += P x_cols (a coupling block, a nearfield block, or a slice of a flattened basis)
-// and one warp does it alone: lane l owns rows l, l + 32, ... (WG_R per pass) and walks the
-// columns with WG_U columns' loads in flight; each row's sum reaches its output with one atomic
-// addition.  No shared memory and no barriers, so an SM keeps 64 warps' loads in flight, and a
-// panel serves up to WG_Q right-hand sides per read (the others are re-read from L2).
+// Warp-per-item variant of the three flattened-path launches (used for the FP32 copies).  Every
+// work item is a small dense GEMV y_rows += P x_cols (a coupling block, a nearfield block, or a
+// slice of a flattened basis) and one warp does it alone: lane l owns rows l, l + 32, ... (WG_R
+// per pass) and walks the columns with WG_U columns' loads in flight; each row's sum reaches its
+// output with one atomic addition.  No shared memory and no barriers, and a panel serves up to
+// WG_Q right-hand sides per read (the others are re-read from L2).
 // ------------------------------------------------------------------------------------------
 #ifndef H2B_MVM_WARP
 #define H2B_MVM_WARP 1
@@ -624,7 +624,9 @@ int launch_flat(const MvmPlan *p, const double *x, size_t ldx, double *y, size_t
   const size_t nyp = W * p->nrow, nxt = W * (size_t) p->k * p->ncol_clusters,
                nyt = W * (size_t) p->k * p->nrow_clusters;
   gather_zero_kernel<CX><<<gz, 256, 0, st>>>(x, ldx, p->cidx, p->ncol, v, nyp, nxt, nyt);
-  if (H2B_MVM_WARP) {
+  // FP32-stored products run one warp per item (measured faster); FP64 ones one CTA per item
+  // (measured faster: the warp form's registers halve its occupancy for 8-byte entries)
+  if (H2B_MVM_WARP && SINGLE) {
     if (v.nrhs == 1)
       launch_warp_items<CX, SINGLE, 1>(p, v, st);
     else
