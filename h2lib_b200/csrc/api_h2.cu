@@ -508,6 +508,10 @@ void h2b_h2_fill_mvm_plan(h2b_h2matrix *h) {
   p.bwd = MvmBackArgs{h->rt.d_leaves, h->rt.d_size, h->rt.d_off, h->rt.d_voff, h->rt.d_V,
                       h->d_yt, h->d_yp, h->rt.nleaves, (int) h->k};
   p.flat = h->flat;
+  p.max_rows = 0;
+  for (uint32_t b = 0; b < h->tree->blocks.n; b++)
+    if (!h->tree->blocks.adm[b])
+      p.max_rows = std::max(p.max_rows, h->tree->row.size[h->tree->blocks.rc[b]]);
   p.rseg = h->rt.d_seg;
   p.cseg = h->ct.d_seg;
   p.ncol_clusters = h->ct.n;

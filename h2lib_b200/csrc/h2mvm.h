@@ -65,6 +65,7 @@ struct MvmFlatArgs {
 struct MvmPlan {
   int cx, num_sms;
   int flat;                      // 1: flattened-basis transforms (ffwd / fbwd)
+  uint32_t max_rows;             // most rows of any nearfield block (the pipelined kernels' limit)
   MvmFlatArgs ffwd, fbwd;
   const uint32_t *rseg, *cseg;   // surface of every row / column cluster (forest trees)
   int k;
