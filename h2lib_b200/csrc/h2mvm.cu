@@ -628,6 +628,7 @@ void launch_warp_items(const MvmPlan *p, const MvmVecs &v, cudaStream_t st) {
 constexpr int PL_NS = 4;            // stages
 constexpr int PL_STAGE = 2048;      // doubles per stage (16 KB)
 constexpr int PL_MAXROWS = 256;     // rows per item (4 passes of 64)
+constexpr int PL_MAXCOLS = 128;     // columns per chunk (the staged slice of x)
 constexpr int PL_CTAS_PER_SM = 2;
 
 __device__ __forceinline__ void cp_async8(double *smem, const double *gmem) {
@@ -707,11 +708,20 @@ __device__ __forceinline__ PlItem pl_item(int kind, uint32_t i, const MvmFlatArg
 // columns of one chunk of an item
 __device__ __forceinline__ uint32_t pl_chunk_cols(const PlItem &it) {
   const uint32_t per = (uint32_t) PL_STAGE / (it.rows * (it.pcx ? 2u : 1u));
-  return per > 0 ? per : 1;
+  return per > (uint32_t) PL_MAXCOLS ? (uint32_t) PL_MAXCOLS : (per > 0 ? per : 1u);
 }
 
-// Issue the copies of columns [c0, c0 + nc) of item `it` into stage `buf` (all threads).
-__device__ __forceinline__ void pl_issue(const PlItem &it, uint32_t c0, uint32_t nc, double *buf) {
+// Issue the copies of columns [c0, c0 + nc) of item `it` into stage `buf`, and of the matching
+// slice of x into `xbuf` (all threads).
+template <bool CX>
+__device__ __forceinline__ void pl_issue(const PlItem &it, uint32_t c0, uint32_t nc, double *buf,
+                                         double *xbuf) {
+  for (uint32_t j = threadIdx.x; j < nc; j += blockDim.x) {
+    if (CX)
+      cp_async16(xbuf + 2 * j, it.x + 2 * (size_t) (c0 + j));
+    else
+      cp_async8(xbuf + j, it.x + c0 + j);
+  }
   const uint32_t rows = it.rows, n = rows * nc;
   const uint32_t dq = blockDim.x / rows, dr = blockDim.x - dq * rows;
   uint32_t j = threadIdx.x / rows, r = threadIdx.x - j * rows;
@@ -739,7 +749,8 @@ __global__ void __launch_bounds__(TPB, PL_CTAS_PER_SM) pipe_gemv_kernel(int kind
   constexpr int NP = PL_MAXROWS / 64;  // row passes
   extern __shared__ __align__(16) double pl_smem[];
   double *stage = pl_smem;                          // PL_NS x PL_STAGE
-  double *red = pl_smem + PL_NS * PL_STAGE;         // TPB x NP x W
+  double *xst = pl_smem + PL_NS * PL_STAGE;         // PL_NS x PL_MAXCOLS x W
+  double *red = xst + PL_NS * PL_MAXCOLS * W;       // TPB x NP x W
   const uint32_t G = gridDim.x;
   // producer cursor (item, first column of the next chunk to issue)
   uint32_t pi = blockIdx.x, pc = 0;
@@ -748,7 +759,7 @@ __global__ void __launch_bounds__(TPB, PL_CTAS_PER_SM) pipe_gemv_kernel(int kind
   auto issue_next = [&](int s) {
     if (pi < nitems) {
       const uint32_t nc = min(pl_chunk_cols(pit), pit.cols - pc);
-      pl_issue(pit, pc, nc, stage + (size_t) s * PL_STAGE);
+      pl_issue<CX>(pit, pc, nc, stage + (size_t) s * PL_STAGE, xst + (size_t) s * PL_MAXCOLS * W);
       pc += nc;
       if (pc >= pit.cols) {
         pi += G;
@@ -776,6 +787,7 @@ __global__ void __launch_bounds__(TPB, PL_CTAS_PER_SM) pipe_gemv_kernel(int kind
     __syncthreads();  // chunk visible to all; the stage consumed last round is free again
     issue_next((s + PL_NS - 1) % PL_NS);
     const double *buf = stage + (size_t) s * PL_STAGE;
+    const double *xb = xst + (size_t) s * PL_MAXCOLS * W;
     const uint32_t rows = it.rows, rb = rows < 64 ? rows : 64, groups = blockDim.x / rb;
     const uint32_t rl = threadIdx.x % rb, g = threadIdx.x / rb;
     if (g < groups) {
@@ -783,9 +795,10 @@ __global__ void __launch_bounds__(TPB, PL_CTAS_PER_SM) pipe_gemv_kernel(int kind
       for (int p = 0; p < NP; p++) {
         const uint32_t r = rl + 64u * p;
         if (p * 64u < rows && r < rows) {
+#pragma unroll 4
           for (uint32_t j = g; j < nc; j += groups) {
-            const double xr = it.x[W * (cc + j)];
-            const double xi = CX ? it.x[W * (cc + j) + 1] : 0.0;
+            const double xr = xb[W * j];
+            const double xi = CX ? xb[W * j + 1] : 0.0;
             if (it.pcx) {
               const double mr = buf[2 * ((size_t) r + (size_t) j * rows)],
                            mi = buf[2 * ((size_t) r + (size_t) j * rows) + 1];
@@ -836,7 +849,8 @@ __global__ void __launch_bounds__(TPB, PL_CTAS_PER_SM) pipe_gemv_kernel(int kind
 
 template <bool CX>
 int launch_pipe(const MvmPlan *p, const MvmVecs &v, cudaStream_t st) {
-  const size_t smem = sizeof(double) * ((size_t) PL_NS * PL_STAGE + (size_t) TPB * (PL_MAXROWS / 64) * (CX ? 2 : 1));
+  const size_t smem = sizeof(double) * ((size_t) PL_NS * (PL_STAGE + PL_MAXCOLS * (CX ? 2 : 1)) +
+                                        (size_t) TPB * (PL_MAXROWS / 64) * (CX ? 2 : 1));
   H2B_CUDA_TRY((h2b_allow_smem<pipe_gemv_kernel<CX>>()));
   const uint32_t sms = p->num_sms > 0 ? (uint32_t) p->num_sms : 148u;
   const MvmCoupleArgs &ca = p->cpl;
