@@ -60,9 +60,9 @@ static void devtree_free(DevCTree &t, cudaStream_t st) {
 // Flattened bases: W_t for the clusters of admissible blocks (`adm`, ids of this tree) and all
 // their descendants (which the products W_f = [W_s E_s] pass through).  Flatten items are
 // grouped by father level, deepest first; matvec items cover the admissible clusters in pieces
-// of at most H2B_MVM_FLAT_ROWS rows.
+// of at most `item_rows` rows.
 static int devtree_flat_setup(DevCTree &t, const h2b_ctree &c, const std::vector<uint32_t> &adm,
-                              uint32_t k, cudaStream_t st) {
+                              uint32_t k, uint32_t item_rows, cudaStream_t st) {
   std::vector<char> in_adm(c.n, 0), need(c.n, 0);
   for (uint32_t a : adm) in_adm[a] = 1;
   // pre-order: a father precedes its sons
@@ -98,8 +98,8 @@ static int devtree_flat_setup(DevCTree &t, const h2b_ctree &c, const std::vector
   }
   for (uint32_t i = 0; i < c.n; i++)
     if (in_adm[i])
-      for (uint32_t r0 = 0; r0 < c.size[i]; r0 += H2B_MVM_FLAT_ROWS)
-        mitems.insert(mitems.end(), {i, r0, std::min<uint32_t>(H2B_MVM_FLAT_ROWS, c.size[i] - r0)});
+      for (uint32_t r0 = 0; r0 < c.size[i]; r0 += item_rows)
+        mitems.insert(mitems.end(), {i, r0, std::min<uint32_t>(item_rows, c.size[i] - r0)});
   t.nwleaves = (uint32_t) wleaves.size();
   t.nmitems = (uint32_t) (mitems.size() / 3);
   int rc;
@@ -376,8 +376,13 @@ extern "C" h2b_h2matrix *h2b_h2matrix_new(const h2b_bem *bem, const h2b_tree *tr
     const char *e = getenv("H2B_MVM_NESTED");
     h->flat = !(e && e[0] == '1');
   }
-  if (rc == H2B_OK && h->flat) rc = devtree_flat_setup(h->rt, tree->row, arc, h->k, h->st);
-  if (rc == H2B_OK && h->flat) rc = devtree_flat_setup(h->ct, tree->col, acc, h->k, h->st);
+  // backward items (row side) in short slices: y rows take one atomic addition per item, and
+  // the slices give the backward launch enough CTAs; forward items (column side) in long ones,
+  // since each adds k entries of xt atomically
+  if (rc == H2B_OK && h->flat)
+    rc = devtree_flat_setup(h->rt, tree->row, arc, h->k, H2B_MVM_BACK_ROWS, h->st);
+  if (rc == H2B_OK && h->flat)
+    rc = devtree_flat_setup(h->ct, tree->col, acc, h->k, H2B_MVM_FLAT_ROWS, h->st);
   // single-triangle rule (raw and linear-basis weighted)
   if (rc == H2B_OK) {
     const h2b_quad &qd = bem->quad;
@@ -508,10 +513,6 @@ void h2b_h2_fill_mvm_plan(h2b_h2matrix *h) {
   p.bwd = MvmBackArgs{h->rt.d_leaves, h->rt.d_size, h->rt.d_off, h->rt.d_voff, h->rt.d_V,
                       h->d_yt, h->d_yp, h->rt.nleaves, (int) h->k};
   p.flat = h->flat;
-  p.max_rows = 0;
-  for (uint32_t b = 0; b < h->tree->blocks.n; b++)
-    if (!h->tree->blocks.adm[b])
-      p.max_rows = std::max(p.max_rows, h->tree->row.size[h->tree->blocks.rc[b]]);
   p.rseg = h->rt.d_seg;
   p.cseg = h->ct.d_seg;
   p.ncol_clusters = h->ct.n;

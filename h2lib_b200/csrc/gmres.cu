@@ -241,26 +241,37 @@ __global__ void __launch_bounds__(TPB) make_q_kernel(GmresDev g) {
   st<CX>(v.q, i, q);
 }
 
-// z[j] = sum over the system's blocks of part[b][j], j <= k: a warp per column, its lanes over
-// the blocks (the blocks' partial sums are read in parallel, not one after another).
+// z[j] = sum over the system's blocks of part[b][j], j <= k.  Lanes take consecutive columns
+// (coalesced reads of a block's partial sums), warps take interleaved blocks, so every thread has
+// all its loads in flight at once; the warps' sums are combined in shared memory.  The caller
+// synchronises before reading z.
 __device__ void sum_parts_all(const GmresDev &g, const Sys &v, uint32_t k, double *zr,
                               double *zi) {
-  const uint32_t lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  for (uint32_t j = w; j <= k; j += nw) {
+  constexpr int NW = GMRES_KMAX / 32;  // warps of the bookkeeping CTA (GMRES_KMAX threads)
+  __shared__ double wsr[NW][GMRES_KMAX], wsi[NW][GMRES_KMAX];
+  const uint32_t lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  for (uint32_t j = lane; j <= k; j += 32) {
     double sr = 0.0, si = 0.0;
-    for (uint32_t b = lane; b < v.nblk; b += 32) {
+#pragma unroll 8
+    for (uint32_t b = w; b < v.nblk; b += NW) {
       sr += v.part[(size_t) b * g.ldpart * 2 + 2 * j];
       si += v.part[(size_t) b * g.ldpart * 2 + 2 * j + 1];
     }
-    sr = warp_sum(sr);
-    si = warp_sum(si);
-    if (lane == 0) {
-      zr[j] = sr;
-      zi[j] = si;
+    wsr[w][j] = sr;
+    wsi[w][j] = si;
+  }
+  __syncthreads();
+  for (uint32_t j = threadIdx.x; j <= k; j += blockDim.x) {
+    double sr = 0.0, si = 0.0;
+#pragma unroll
+    for (int q = 0; q < NW; q++) {
+      sr += wsr[q][j];
+      si += wsi[q][j];
     }
+    zr[j] = sr;
+    zi[j] = si;
   }
 }
-
 
 __device__ __forceinline__ cd Tij(const GmresDev &g, const Sys &v, uint32_t i, uint32_t j) {
   return {v.T[2 * ((size_t) i + (size_t) j * g.kmax)], v.T[2 * ((size_t) i + (size_t) j * g.kmax) + 1]};

@@ -613,257 +613,6 @@ void launch_warp_items(const MvmPlan *p, const MvmVecs &v, cudaStream_t st) {
     backward_warp_kernel<CX, SINGLE, NQ><<<(p->fbwd.nitems + WPB - 1) / WPB, TPB, 0, st>>>(p->fbwd, v);
 }
 
-// ------------------------------------------------------------------------------------------
-// Pipelined variant for the FP64 single-column product.  A CTA (resident for the whole launch)
-// walks its share of the work items (item i, i + grid, ...), cut into chunks of whole columns of
-// at most PL_STAGE doubles, and streams the chunks through PL_NS shared-memory stages with
-// asynchronous copies (cp.async, global -> shared, no registers held while in flight): while
-// the CTA multiplies chunk t, the copies of chunks t+1 .. t+PL_NS-1 are under way.  Rows are
-// split over the threads as in panel_mv_atomic (rows per pass <= 64, the column groups' sums
-// combined in shared memory at the end of each item, one atomic addition per row).
-// ------------------------------------------------------------------------------------------
-#ifndef H2B_MVM_PIPE
-#define H2B_MVM_PIPE 1
-#endif
-constexpr int PL_NS = 4;            // stages
-constexpr int PL_STAGE = 2048;      // doubles per stage (16 KB)
-constexpr int PL_MAXROWS = 256;     // rows per item (4 passes of 64)
-constexpr int PL_MAXCOLS = 128;     // columns per chunk (the staged slice of x)
-constexpr int PL_CTAS_PER_SM = 2;
-
-__device__ __forceinline__ void cp_async8(double *smem, const double *gmem) {
-  const unsigned s = (unsigned) __cvta_generic_to_shared(smem);
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem) : "memory");
-}
-__device__ __forceinline__ void cp_async16(double *smem, const double *gmem) {
-  const unsigned s = (unsigned) __cvta_generic_to_shared(smem);
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() {
-  asm volatile("cp.async.commit_group;\n" ::: "memory");
-}
-template <int N>
-__device__ __forceinline__ void cp_async_wait() {
-  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
-}
-
-// One work item: y[0 .. rows) += P x (P: rows x cols, column-major with ld; complex if pcx).
-struct PlItem {
-  const double *P;
-  const double *x;
-  double *y;
-  uint32_t rows, cols, ld;
-  int pcx;
-};
-
-// kind 0: forward items then nearfield blocks; 1: coupling blocks; 2: backward items.
-template <bool CX>
-__device__ __forceinline__ PlItem pl_item(int kind, uint32_t i, const MvmFlatArgs &f,
-                                          const MvmCoupleArgs &c, const MvmVecs &v) {
-  constexpr int W = CX ? 2 : 1;
-  PlItem it;
-  const uint32_t k = (uint32_t) c.k;
-  if (kind == 0 && i < f.nitems) {
-    const uint32_t *m = f.items + 3 * (size_t) i;
-    const uint32_t cl = m[0], r0 = m[1], nr = m[2];
-    it.P = f.W + f.woff[cl] + (size_t) r0 * k;
-    it.x = v.xp + (size_t) W * (f.off[cl] + r0);
-    it.y = v.xt + (size_t) W * k * cl;
-    it.rows = k;
-    it.cols = nr;
-    it.ld = k;
-    it.pcx = 0;
-  } else if (kind == 0) {
-    const uint32_t nb = i - f.nitems;
-    const uint32_t r = c.near_rc[nb], cc = c.near_cc[nb];
-    it.P = c.N + (size_t) W * c.near_off[nb];
-    it.x = v.xp + (size_t) W * c.coff[cc];
-    it.y = v.yp + (size_t) W * c.roff[r];
-    it.rows = c.rsize[r];
-    it.cols = c.csize[cc];
-    it.ld = it.rows;
-    it.pcx = CX;
-  } else if (kind == 1) {
-    it.P = c.S + (size_t) W * k * k * i;
-    it.x = v.xt + (size_t) W * k * c.adm_cc[i];
-    it.y = v.yt + (size_t) W * k * c.adm_rc[i];
-    it.rows = k;
-    it.cols = k;
-    it.ld = k;
-    it.pcx = CX;
-  } else {
-    const uint32_t *m = f.items + 3 * (size_t) i;
-    const uint32_t cl = m[0], r0 = m[1], nr = m[2];
-    it.P = f.W + f.woff[cl] + r0;
-    it.x = v.yt + (size_t) W * k * cl;
-    it.y = v.yp + (size_t) W * (f.off[cl] + r0);
-    it.rows = nr;
-    it.cols = k;
-    it.ld = f.size[cl];
-    it.pcx = 0;
-  }
-  return it;
-}
-
-// columns of one chunk of an item
-__device__ __forceinline__ uint32_t pl_chunk_cols(const PlItem &it) {
-  const uint32_t per = (uint32_t) PL_STAGE / (it.rows * (it.pcx ? 2u : 1u));
-  return per > (uint32_t) PL_MAXCOLS ? (uint32_t) PL_MAXCOLS : (per > 0 ? per : 1u);
-}
-
-// Issue the copies of columns [c0, c0 + nc) of item `it` into stage `buf`, and of the matching
-// slice of x into `xbuf` (all threads).
-template <bool CX>
-__device__ __forceinline__ void pl_issue(const PlItem &it, uint32_t c0, uint32_t nc, double *buf,
-                                         double *xbuf) {
-  for (uint32_t j = threadIdx.x; j < nc; j += blockDim.x) {
-    if (CX)
-      cp_async16(xbuf + 2 * j, it.x + 2 * (size_t) (c0 + j));
-    else
-      cp_async8(xbuf + j, it.x + c0 + j);
-  }
-  const uint32_t rows = it.rows, n = rows * nc;
-  const uint32_t dq = blockDim.x / rows, dr = blockDim.x - dq * rows;
-  uint32_t j = threadIdx.x / rows, r = threadIdx.x - j * rows;
-  for (uint32_t e = threadIdx.x; e < n; e += blockDim.x) {
-    const size_t src = (size_t) r + (size_t) (c0 + j) * it.ld;
-    if (it.pcx)
-      cp_async16(buf + 2 * (size_t) e, it.P + 2 * src);
-    else
-      cp_async8(buf + e, it.P + src);
-    j += dq;
-    r += dr;
-    if (r >= rows) {
-      r -= rows;
-      j++;
-    }
-  }
-}
-
-template <bool CX>
-__global__ void __launch_bounds__(TPB, PL_CTAS_PER_SM) pipe_gemv_kernel(int kind, uint32_t nitems,
-                                                                        MvmFlatArgs f,
-                                                                        MvmCoupleArgs c,
-                                                                        MvmVecs v) {
-  constexpr int W = CX ? 2 : 1;
-  constexpr int NP = PL_MAXROWS / 64;  // row passes
-  extern __shared__ __align__(16) double pl_smem[];
-  double *stage = pl_smem;                          // PL_NS x PL_STAGE
-  double *xst = pl_smem + PL_NS * PL_STAGE;         // PL_NS x PL_MAXCOLS x W
-  double *red = xst + PL_NS * PL_MAXCOLS * W;       // TPB x NP x W
-  const uint32_t G = gridDim.x;
-  // producer cursor (item, first column of the next chunk to issue)
-  uint32_t pi = blockIdx.x, pc = 0;
-  PlItem pit;
-  if (pi < nitems) pit = pl_item<CX>(kind, pi, f, c, v);
-  auto issue_next = [&](int s) {
-    if (pi < nitems) {
-      const uint32_t nc = min(pl_chunk_cols(pit), pit.cols - pc);
-      pl_issue<CX>(pit, pc, nc, stage + (size_t) s * PL_STAGE, xst + (size_t) s * PL_MAXCOLS * W);
-      pc += nc;
-      if (pc >= pit.cols) {
-        pi += G;
-        pc = 0;
-        if (pi < nitems) pit = pl_item<CX>(kind, pi, f, c, v);
-      }
-    }
-    cp_async_commit();  // (an empty group when nothing is left keeps the wait counts uniform)
-  };
-#pragma unroll
-  for (int s = 0; s < PL_NS - 1; s++) issue_next(s);
-
-  // consumer cursor
-  uint32_t ci = blockIdx.x, cc = 0;
-  int s = 0;
-  double acc[NP][W];
-#pragma unroll
-  for (int p = 0; p < NP; p++)
-#pragma unroll
-    for (int w = 0; w < W; w++) acc[p][w] = 0.0;
-  while (ci < nitems) {
-    const PlItem it = pl_item<CX>(kind, ci, f, c, v);
-    const uint32_t nc = min(pl_chunk_cols(it), it.cols - cc);
-    cp_async_wait<PL_NS - 2>();
-    __syncthreads();  // chunk visible to all; the stage consumed last round is free again
-    issue_next((s + PL_NS - 1) % PL_NS);
-    const double *buf = stage + (size_t) s * PL_STAGE;
-    const double *xb = xst + (size_t) s * PL_MAXCOLS * W;
-    const uint32_t rows = it.rows, rb = rows < 64 ? rows : 64, groups = blockDim.x / rb;
-    const uint32_t rl = threadIdx.x % rb, g = threadIdx.x / rb;
-    if (g < groups) {
-#pragma unroll
-      for (int p = 0; p < NP; p++) {
-        const uint32_t r = rl + 64u * p;
-        if (p * 64u < rows && r < rows) {
-#pragma unroll 4
-          for (uint32_t j = g; j < nc; j += groups) {
-            const double xr = xb[W * j];
-            const double xi = CX ? xb[W * j + 1] : 0.0;
-            if (it.pcx) {
-              const double mr = buf[2 * ((size_t) r + (size_t) j * rows)],
-                           mi = buf[2 * ((size_t) r + (size_t) j * rows) + 1];
-              acc[p][0] = fma(mr, xr, fma(-mi, xi, acc[p][0]));
-              acc[p][W - 1] = fma(mr, xi, fma(mi, xr, acc[p][W - 1]));
-            } else {
-              const double m = buf[(size_t) r + (size_t) j * rows];
-              acc[p][0] = fma(m, xr, acc[p][0]);
-              if (CX) acc[p][W - 1] = fma(m, xi, acc[p][W - 1]);
-            }
-          }
-        }
-      }
-    }
-    s = (s + 1) % PL_NS;
-    cc += nc;
-    if (cc >= it.cols) {
-      // item done: combine the column groups, one atomic addition per row
-      if (g < groups) {
-#pragma unroll
-        for (int p = 0; p < NP; p++)
-#pragma unroll
-          for (int w = 0; w < W; w++) red[(size_t) W * (p * TPB + threadIdx.x) + w] = acc[p][w];
-      }
-      __syncthreads();
-      for (uint32_t r = threadIdx.x; r < rows; r += blockDim.x) {
-        const uint32_t p = r / 64, l = r % 64;
-        double sr = 0.0, si = 0.0;
-        for (uint32_t h = 0; h < groups; h++) {
-          const size_t o = (size_t) W * (p * TPB + h * rb + l);
-          sr += red[o];
-          if (CX) si += red[o + 1];
-        }
-        atomicAdd(it.y + W * r, sr);
-        if (CX) atomicAdd(it.y + W * r + 1, si);
-      }
-#pragma unroll
-      for (int p = 0; p < NP; p++)
-#pragma unroll
-        for (int w = 0; w < W; w++) acc[p][w] = 0.0;
-      ci += G;
-      cc = 0;
-      // (the next round's barrier orders these reads of red before its next writes)
-    }
-  }
-  cp_async_wait<0>();
-}
-
-template <bool CX>
-int launch_pipe(const MvmPlan *p, const MvmVecs &v, cudaStream_t st) {
-  const size_t smem = sizeof(double) * ((size_t) PL_NS * (PL_STAGE + PL_MAXCOLS * (CX ? 2 : 1)) +
-                                        (size_t) TPB * (PL_MAXROWS / 64) * (CX ? 2 : 1));
-  H2B_CUDA_TRY((h2b_allow_smem<pipe_gemv_kernel<CX>>()));
-  const uint32_t sms = p->num_sms > 0 ? (uint32_t) p->num_sms : 148u;
-  const MvmCoupleArgs &ca = p->cpl;
-  const uint32_t n[3] = {p->ffwd.nitems + ca.nnear, ca.nadm, p->fbwd.nitems};
-  for (int kind = 0; kind < 3; kind++) {
-    if (!n[kind]) continue;
-    const uint32_t grid = std::min<uint32_t>(n[kind], PL_CTAS_PER_SM * sms);
-    pipe_gemv_kernel<CX><<<grid, TPB, smem, st>>>(kind, n[kind], kind == 2 ? p->fbwd : p->ffwd,
-                                                  ca, v);
-  }
-  return H2B_OK;
-}
-
 template <bool CX, bool SINGLE>
 int launch_flat(const MvmPlan *p, const double *x, size_t ldx, double *y, size_t ldy, double ar,
                 double ai, const MvmVecs &v, cudaStream_t st) {
@@ -877,11 +626,7 @@ int launch_flat(const MvmPlan *p, const double *x, size_t ldx, double *y, size_t
   gather_zero_kernel<CX><<<gz, 256, 0, st>>>(x, ldx, p->cidx, p->ncol, v, nyp, nxt, nyt);
   // FP32-stored products run one warp per item (measured faster); FP64 ones one CTA per item
   // (measured faster: the warp form's registers halve its occupancy for 8-byte entries)
-  if (H2B_MVM_PIPE && !SINGLE && v.nrhs == 1 && !v.mask && p->max_rows <= (uint32_t) PL_MAXROWS &&
-      p->k <= PL_MAXROWS) {
-    const int rc = launch_pipe<CX>(p, v, st);
-    if (rc != H2B_OK) return rc;
-  } else if (H2B_MVM_WARP && SINGLE) {
+  if (H2B_MVM_WARP && SINGLE) {
     if (v.nrhs == 1)
       launch_warp_items<CX, SINGLE, 1>(p, v, st);
     else

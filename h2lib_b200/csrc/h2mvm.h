@@ -52,6 +52,9 @@ struct MvmBackArgs {
 
 // Flattened-basis transforms (flatbasis.cu builds W): one item = rows [r0, r0 + nr) of cluster c.
 #define H2B_MVM_FLAT_ROWS 128
+#ifndef H2B_MVM_BACK_ROWS
+#define H2B_MVM_BACK_ROWS 32
+#endif
 struct MvmFlatArgs {
   const uint32_t *items;      // 3 per item: cluster, first row, rows
   const uint32_t *off, *size; // per cluster
@@ -65,7 +68,6 @@ struct MvmFlatArgs {
 struct MvmPlan {
   int cx, num_sms;
   int flat;                      // 1: flattened-basis transforms (ffwd / fbwd)
-  uint32_t max_rows;             // most rows of any nearfield block (the pipelined kernels' limit)
   MvmFlatArgs ffwd, fbwd;
   const uint32_t *rseg, *cseg;   // surface of every row / column cluster (forest trees)
   int k;
