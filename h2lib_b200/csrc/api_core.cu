@@ -222,16 +222,36 @@ extern "C" h2b_bem *h2b_bem_new(const h2b_surface *s, int pde, int layer, int ro
     delete b;
     return NULL;
   }
-  // Packed singular rules for the device: per case c = 1..3: x0, x1, y0, y1, w (raw), each n_c
-  // doubles, every block padded to an even number of doubles (16-byte alignment).
+  // Packed singular rules for the device, every block padded to an even number of doubles
+  // (16-byte alignment).  Case 1 (common vertex): x0, x1, y0, y1, w (raw), n_1 doubles each.
+  // Cases 2 and 3 (common edge, identical): the reduced rules of h2b_quad_reduce, a, b, c and
+  // the basis-weighted weight rows (i + NR j) for the row / column basis functions i < NR,
+  // j < NC (NR, NC = 3 for a linear basis, 1 for a constant one), n_c' doubles each.
   std::vector<double> pack;
   b->rule_n[0] = b->rule_off[0] = 0;
+  const int NR = row_basis == H2B_BASIS_LINEAR ? 3 : 1, NC = col_basis == H2B_BASIS_LINEAR ? 3 : 1;
   for (int c = 1; c <= 3; c++) {
     const h2b_rule &r = b->quad.rule[c];
-    b->rule_n[c] = r.n;
     b->rule_off[c] = (uint32_t) pack.size();
-    const double *src[5] = {r.x0, r.x1, r.y0, r.y1, r.w + 9ull * r.n};
-    for (int f = 0; f < 5; f++) pack.insert(pack.end(), src[f], src[f] + r.n);
+    if (c == 1) {
+      b->rule_n[c] = r.n;
+      const double *src[5] = {r.x0, r.x1, r.y0, r.y1, r.w + 9ull * r.n};
+      for (int f = 0; f < 5; f++) pack.insert(pack.end(), src[f], src[f] + r.n);
+    } else {
+      uint32_t n = 0;
+      double *abc = nullptr, *w9 = nullptr;
+      if (h2b_quad_reduce(&r, c, q_singular, &n, &abc, &w9) != H2B_OK) {
+        h2b_bem_del(b);
+        return NULL;
+      }
+      b->rule_n[c] = n;
+      pack.insert(pack.end(), abc, abc + 3ull * n);
+      for (int j = 0; j < NC; j++)
+        for (int i = 0; i < NR; i++)
+          pack.insert(pack.end(), w9 + (size_t) (i + 3 * j) * n, w9 + (size_t) (i + 3 * j + 1) * n);
+      free(abc);
+      free(w9);
+    }
     // offsets inside the block are multiples of n; keep n even by padding the whole block
     if (pack.size() & 1) pack.push_back(0.0);
   }

@@ -38,6 +38,10 @@ typedef struct {
 int h2b_gauss_legendre01(uint32_t m, double *x, double *w);
 int h2b_quad_build(uint32_t q, uint32_t q2, int row_basis, int col_basis, h2b_quad *out);
 void h2b_quad_free(h2b_quad *qd);
+/* Edge (which = 2) or identical (3) rule with the points that share a kernel argument merged:
+ * (a, b, c) per point in abc[3 n'], summed basis-weighted weight rows in w9[9 n'] (malloc'ed). */
+int h2b_quad_reduce(const h2b_rule *r, int which, uint32_t q2, uint32_t *n_out, double **abc,
+                    double **w9);
 
 /* ---------------- cluster / block trees (host) ---------------- */
 

@@ -246,6 +246,62 @@ h2b_quad_build(uint32_t q, uint32_t q2, int row_basis, int col_basis, h2b_quad *
   return H2B_OK;
 }
 
+/* Reduced edge / identical rule.  With the shared vertices first in both triangles (the
+ * permutation of select_quadrature_singquad2d), X - Y depends on fewer variables than the rule
+ * has: for a common edge (A, B shared) X - Y = (x0 - y0)(B - A) + x1 (C_t - B) - y1 (C_s - B),
+ * and in each sub-simplex of build_edge x0 - y0, x1 and y1 do not depend on the innermost Gauss
+ * variable (xi2, loop l); for identical triangles X - Y = (x0 - y0)(B - A) + (x1 - y1)(C - B),
+ * and x0 - y0, x1 - y1 depend on neither xi2 nor xi3 (loops k, l).  The points that differ only
+ * in those variables therefore share one kernel value, so they become one point whose
+ * basis-weighted weights are the sums of theirs: q2 (edge) or q2^2 (identical) times fewer
+ * kernel evaluations for the same quadrature sum (summed in another order).
+ * Output: n' points; abc[0..n'), abc[n'..2n'), abc[2n'..3n') = (a, b, c) with
+ * X - Y = (A_t - A_s) + a (B_t - A_t) + b (C_t - B_t) - c (C_s - B_s); w9[(i + 3 j) n' + g] the
+ * summed weight rows 0..8.  Points are ordered as build_edge / build_id order them: six
+ * sub-simplices innermost, then l, k, j, i. */
+int
+h2b_quad_reduce(const h2b_rule *r, int which, uint32_t q2, uint32_t *n_out, double **abc,
+                double **w9)
+{
+  const uint32_t merge = which == H2B_RULE_EDGE ? q2 : q2 * q2;
+  uint32_t n, p, g, i;
+  *abc = NULL;
+  *w9 = NULL;
+  if ((which != H2B_RULE_EDGE && which != H2B_RULE_ID) || r->n % (6 * merge)) {
+    h2b_set_error("h2b_quad_reduce: rule %d cannot be reduced", which);
+    return H2B_ERR_ARG;
+  }
+  n = r->n / merge;
+  *abc = (double *) calloc(3 * (size_t) n, sizeof(double));
+  *w9 = (double *) calloc(9 * (size_t) n, sizeof(double));
+  if (!*abc || !*w9) {
+    free(*abc);
+    free(*w9);
+    *abc = *w9 = NULL;
+    h2b_set_error("h2b_quad_reduce: out of host memory");
+    return H2B_ERR_NOMEM;
+  }
+  for (p = 0; p < r->n; p++) {
+    const uint32_t s = p % 6, rest = p / 6, m = rest % merge, outer = rest / merge;
+    g = outer * 6 + s;
+    if (m == 0) {  /* the group's first point defines its kernel argument */
+      (*abc)[g] = r->x0[p] - r->y0[p];
+      if (which == H2B_RULE_EDGE) {
+        (*abc)[n + g] = r->x1[p];
+        (*abc)[2 * (size_t) n + g] = r->y1[p];
+      }
+      else {
+        (*abc)[n + g] = r->x1[p] - r->y1[p];
+        (*abc)[2 * (size_t) n + g] = 0.0;
+      }
+    }
+    for (i = 0; i < 9; i++)
+      (*w9)[i * (size_t) n + g] += r->w[i * (size_t) r->n + p];
+  }
+  *n_out = n;
+  return H2B_OK;
+}
+
 void
 h2b_quad_free(h2b_quad *qd)
 {

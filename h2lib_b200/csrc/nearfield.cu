@@ -6,8 +6,10 @@
 //     triangle pair (no shared vertex, q^4 tensor points, fully unrolled with the rule in
 //     constant memory); pair results are accumulated in a shared-memory tile and the tile is
 //     written to HBM once with coalesced column-major stores.  Singular pairs are skipped here.
-//   * near_sing_kernel — one warp per singular pair (vertex: 2 q2^4, edge / identical: 6 q2^4
-//     points), lanes stride over the points, the three Sauter-Schwab rules are staged once per
+//   * near_sing_kernel — one warp per singular pair (vertex: 2 q2^4 points; edge: 6 q2^3 and
+//     identical: 6 q2^2 kernel evaluations, the rules reduced on the host because X - Y does not
+//     depend on the inner Gauss variables there, see h2b_quad_reduce), lanes stride over the
+//     points, the three Sauter-Schwab rules are staged once per
 //     CTA into shared memory with bulk asynchronous copies (cp.async.bulk, global -> shared,
 //     completion on an mbarrier), partial sums are combined with warp shuffles and the result is
 //     written (constant basis) or added (linear basis) to the entries of its pair.
@@ -180,6 +182,32 @@ __device__ __forceinline__ void quad_point(const PairGeo &g, double tx, double s
           acc[c][i][j] = RL ? fma(pr[i], u[j], acc[c][i][j]) : acc[c][i][j] + u[j];
     }
   }
+}
+
+// One point of a reduced singular rule (h2b_quad_reduce): X - Y = d0 + a p1 + b p2 - c q2, and
+// the basis-weighted weights are precomputed, w[(i + NR j) * ld] for the row / column basis
+// functions i, j.  Several points of the full rule share this kernel value.
+template <int KK, bool RL, bool CL>
+__device__ __forceinline__ void quad_point_red(const PairGeo &g, double ra, double rb, double rc,
+                                               const double *w, uint32_t ld, double n0, double n1,
+                                               double n2, double k_re, double k_imn,
+                                               double (&acc)[KT<KK>::NCH][RL ? 3 : 1][CL ? 3 : 1]) {
+  constexpr int NCH = KT<KK>::NCH, NR = RL ? 3 : 1, NC = CL ? 3 : 1;
+  const double dx = fma(-rc, g.q2[0], fma(rb, g.p2[0], fma(ra, g.p1[0], g.d0[0])));
+  const double dy = fma(-rc, g.q2[1], fma(rb, g.p2[1], fma(ra, g.p1[1], g.d0[1])));
+  const double dz = fma(-rc, g.q2[2], fma(rb, g.p2[2], fma(ra, g.p1[2], g.d0[2])));
+  double kv[2];
+  const double r2 = fma(dx, dx, fma(dy, dy, dz * dz));
+  const double dot = uses_normal<KK>() ? fma(dx, n0, fma(dy, n1, dz * n2)) : 0.0;
+  eval_kernel<KK>(r2, dot, k_re, k_imn, kv);
+#pragma unroll
+  for (int j = 0; j < NC; j++)
+#pragma unroll
+    for (int i = 0; i < NR; i++) {
+      const double wij = w[(size_t) (i + NR * j) * ld];
+#pragma unroll
+      for (int c = 0; c < NCH; c++) acc[c][i][j] = fma(wij, kv[c], acc[c][i][j]);
+    }
 }
 
 // One distant pair with the q^4 tensor rule, summed column side first:
@@ -629,7 +657,8 @@ struct SingArgs {
   double kconst, k_re, k_imn;
   double alpha_re, alpha_im;  // identity coefficient of the double layer output
   double mass[9];
-  const double *rule;         // packed singular rules: [case 1..3] x {x0,x1,y0,y1,w} x n_case
+  const double *rule;         // packed singular rules: case 1 {x0,x1,y0,y1,w} x n_1, cases 2, 3
+                              // {a,b,c, NR*NC weight rows} x n_c (reduced rules)
   uint32_t rule_n[4];         // points per case (index 1..3)
   uint32_t rule_off[4];       // offset (in doubles) of each case's block in `rule`
   uint32_t rule_total;        // doubles in `rule` (multiple of 2, 16-byte aligned)
@@ -715,7 +744,6 @@ __global__ void __launch_bounds__(SING_THREADS, 1) near_sing_kernel(SingArgs a) 
     const double n0 = NT.n[0], n1 = NT.n[1], n2 = NT.n[2];
     const uint32_t n = a.rule_n[cs];
     const double *rx0 = rules + a.rule_off[cs];
-    const double *rx1 = rx0 + n, *ry0 = rx0 + 2 * n, *ry1 = rx0 + 3 * n, *rw = rx0 + 4 * n;
 
     double acc[NCH][NR][NC];
 #pragma unroll
@@ -724,10 +752,21 @@ __global__ void __launch_bounds__(SING_THREADS, 1) near_sing_kernel(SingArgs a) 
       for (int i = 0; i < NR; i++)
 #pragma unroll
         for (int j = 0; j < NC; j++) acc[c][i][j] = 0.0;
+    if (cs == 1u) {
+      // common vertex: the full rule (x0, x1, y0, y1, raw weight)
+      const double *rx1 = rx0 + n, *ry0 = rx0 + 2 * n, *ry1 = rx0 + 3 * n, *rw = rx0 + 4 * n;
 #pragma unroll SING_UNROLL
-    for (uint32_t k = lane; k < n; k += 32)
-      quad_point<KK, RL, CL>(g, rx0[k], rx1[k], ry0[k], ry1[k], rw[k], n0, n1, n2, a.k_re, a.k_imn,
-                             acc);
+      for (uint32_t k = lane; k < n; k += 32)
+        quad_point<KK, RL, CL>(g, rx0[k], rx1[k], ry0[k], ry1[k], rw[k], n0, n1, n2, a.k_re,
+                               a.k_imn, acc);
+    } else {
+      // common edge / identical: the reduced rule (a, b, c, basis-weighted weights)
+      const double *rb = rx0 + n, *rc = rx0 + 2 * n, *rwt = rx0 + 3 * n;
+#pragma unroll SING_UNROLL
+      for (uint32_t k = lane; k < n; k += 32)
+        quad_point_red<KK, RL, CL>(g, rx0[k], rb[k], rc[k], rwt + k, n, n0, n1, n2, a.k_re,
+                                   a.k_imn, acc);
+    }
 #pragma unroll
     for (int c = 0; c < NCH; c++)
 #pragma unroll
