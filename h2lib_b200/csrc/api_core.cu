@@ -223,8 +223,9 @@ extern "C" h2b_bem *h2b_bem_new(const h2b_surface *s, int pde, int layer, int ro
     return NULL;
   }
   // Packed singular rules for the device, every block padded to an even number of doubles
-  // (16-byte alignment).  Case 1 (common vertex): x0, x1, y0, y1, w (raw), n_1 doubles each.
-  // Cases 2 and 3 (common edge, identical): the reduced rules of h2b_quad_reduce, a, b, c and
+  // (16-byte alignment).  Case 1 (common vertex): for q_singular = 4 the tensor form of
+  // h2b_quad_vert_tensor (rule_n[1] = groups), otherwise x0, x1, y0, y1, w (raw), n_1 doubles
+  // each.  Cases 2 and 3 (common edge, identical): the reduced rules of h2b_quad_reduce, a, b, c and
   // the basis-weighted weight rows (i + NR j) for the row / column basis functions i < NR,
   // j < NC (NR, NC = 3 for a linear basis, 1 for a constant one), n_c' doubles each.
   std::vector<double> pack;
@@ -233,7 +234,19 @@ extern "C" h2b_bem *h2b_bem_new(const h2b_surface *s, int pde, int layer, int ro
   for (int c = 1; c <= 3; c++) {
     const h2b_rule &r = b->quad.rule[c];
     b->rule_off[c] = (uint32_t) pack.size();
-    if (c == 1) {
+    if (c == 1 && q_singular == 4) {
+      // tensor form (h2b_quad_vert_tensor): the kernel's specialised path for q2 = 4
+      uint32_t ng = 0;
+      double *t = nullptr;
+      if (h2b_quad_vert_tensor(q_singular, row_basis, col_basis, &ng, &t) != H2B_OK) {
+        h2b_bem_del(b);
+        return NULL;
+      }
+      b->rule_n[c] = ng;
+      b->vert_tensor = 1;
+      pack.insert(pack.end(), t, t + (size_t) (4 + NR + NC) * q_singular * ng);
+      free(t);
+    } else if (c == 1) {
       b->rule_n[c] = r.n;
       const double *src[5] = {r.x0, r.x1, r.y0, r.y1, r.w + 9ull * r.n};
       for (int f = 0; f < 5; f++) pack.insert(pack.end(), src[f], src[f] + r.n);
@@ -305,6 +318,7 @@ void h2b_fill_launch(const h2b_bem *b, h2b_near_launch *L) {
     L->rule_off[i] = b->rule_off[i];
   }
   L->rule_total = b->rule_total;
+  L->vert_tensor = b->vert_tensor;
   L->num_sms = b->s->num_sms;
   L->err = b->d_err;
 }

@@ -32,6 +32,7 @@ struct h2b_bem {
   h2b_quad quad{};
   double *d_rule = nullptr;
   uint32_t rule_n[4], rule_off[4], rule_total = 0;
+  int vert_tensor = 0;  // 1: the common-vertex rule is packed in tensor form (q_singular == 4)
   int *d_err = nullptr;
 };
 

@@ -42,6 +42,9 @@ void h2b_quad_free(h2b_quad *qd);
  * (a, b, c) per point in abc[3 n'], summed basis-weighted weight rows in w9[9 n'] (malloc'ed). */
 int h2b_quad_reduce(const h2b_rule *r, int which, uint32_t q2, uint32_t *n_out, double **abc,
                     double **w9);
+/* Common-vertex rule in tensor form: 2 q2^2 groups of q2 row points x q2 column points. */
+int h2b_quad_vert_tensor(uint32_t q2, int row_basis, int col_basis, uint32_t *ngroups,
+                         double **out);
 
 /* ---------------- cluster / block trees (host) ---------------- */
 

@@ -302,6 +302,61 @@ h2b_quad_reduce(const h2b_rule *r, int which, uint32_t q2, uint32_t *n_out, doub
   return H2B_OK;
 }
 
+/* Common-vertex rule in tensor form.  build_vert's points with the same (eta1, xi, sub-simplex)
+ * form a q2 x q2 tensor product: in sub-simplex 0 the row point (xi, eta2 xi) runs over eta2 and
+ * the column point (eta1 xi, eta1 eta3 xi) over eta3, in sub-simplex 1 the roles swap, and the
+ * weight gw_i gw_j gw_k gw_l xi^3 eta1 factors into a group part, a row-point part and a
+ * column-point part.  A group therefore needs q2 row points and q2 column points instead of
+ * q2^2 point pairs, and the pair sum can be taken column side first (as for distant pairs).
+ * Output (ngroups = 2 q2^2 groups, each array ngroups long, group g = (i q2 + l) 2 + s):
+ *   row points a < q2:    x0, x1, then NR weights G w_a phi_r(x)   (NR = 3 linear, 1 constant)
+ *   column points b < q2: y0, y1, then NC weights w_b phi_c(y)
+ * i.e. (2 + NR) q2 + (2 + NC) q2 arrays. */
+int
+h2b_quad_vert_tensor(uint32_t q2, int row_basis, int col_basis, uint32_t *ngroups, double **out)
+{
+  double g[64], gw[64];
+  const uint32_t NR = row_basis == H2B_BASIS_LINEAR ? 3 : 1, NC = col_basis == H2B_BASIS_LINEAR ? 3 : 1;
+  const uint32_t G = 2 * q2 * q2, rstride = 2 + NR, cstride = 2 + NC;
+  uint32_t i, l, s, a, r;
+  double *o, *col;
+  *out = NULL;
+  if (h2b_gauss_legendre01(q2, g, gw))
+    return H2B_ERR_ARG;
+  o = (double *) calloc((size_t) (rstride + cstride) * q2 * G, sizeof(double));
+  if (!o) {
+    h2b_set_error("h2b_quad_vert_tensor: out of host memory");
+    return H2B_ERR_NOMEM;
+  }
+  col = o + (size_t) rstride * q2 * G;
+  for (i = 0; i < q2; i++)
+    for (l = 0; l < q2; l++)
+      for (s = 0; s < 2; s++) {
+        const uint32_t grp = (i * q2 + l) * 2 + s;
+        const double e1 = g[i], xi = g[l];
+        const double wg = gw[i] * gw[l] * xi * xi * xi * e1;
+        for (a = 0; a < q2; a++) {
+          /* the point that varies with eta2 (index j) or eta3 (index k) */
+          const double pa0 = xi, pa1 = g[a] * xi;                  /* (xi, eta xi) */
+          const double pb0 = e1 * xi, pb1 = e1 * g[a] * xi;        /* (eta1 xi, eta1 eta xi) */
+          const double x0 = s == 0 ? pa0 : pb0, x1 = s == 0 ? pa1 : pb1;
+          const double y0 = s == 0 ? pb0 : pa0, y1 = s == 0 ? pb1 : pa1;
+          double *rp = o + (size_t) a * rstride * G, *cp = col + (size_t) a * cstride * G;
+          rp[grp] = x0;
+          rp[G + grp] = x1;
+          for (r = 0; r < NR; r++)
+            rp[(2 + r) * (size_t) G + grp] = wg * gw[a] * nodal(row_basis, (int) r, x0, x1);
+          cp[grp] = y0;
+          cp[G + grp] = y1;
+          for (r = 0; r < NC; r++)
+            cp[(2 + r) * (size_t) G + grp] = gw[a] * nodal(col_basis, (int) r, y0, y1);
+        }
+      }
+  *ngroups = G;
+  *out = o;
+  return H2B_OK;
+}
+
 void
 h2b_quad_free(h2b_quad *qd)
 {

@@ -210,6 +210,62 @@ __device__ __forceinline__ void quad_point_red(const PairGeo &g, double ra, doub
     }
 }
 
+// One group of the common-vertex rule in tensor form (h2b_quad_vert_tensor, q2 = VT_Q): VT_Q row
+// points x VT_Q column points, summed column side first as for distant pairs, so the basis
+// weights are applied once per point instead of once per point pair.  With the shared vertex
+// first in both triangles, X_a - Y_b = (d0 + x0 p1 + x1 p2) - (y0 q1 + y1 q2).  `t` is the
+// packed group arrays (gn groups each), the row weights include the group weight.
+constexpr int VT_Q = 4;
+template <int KK, bool RL, bool CL>
+__device__ __forceinline__ void vert_group_tensor(const PairGeo &g, const double *t, uint32_t gn,
+                                                  uint32_t grp, double n0, double n1, double n2,
+                                                  double k_re, double k_imn,
+                                                  double (&acc)[KT<KK>::NCH][RL ? 3 : 1][CL ? 3 : 1]) {
+  constexpr int NCH = KT<KK>::NCH, NR = RL ? 3 : 1, NC = CL ? 3 : 1;
+  constexpr bool DOT = uses_normal<KK>();
+  const double *col = t + (size_t) (2 + NR) * VT_Q * gn;
+#pragma unroll 1
+  for (int a = 0; a < VT_Q; a++) {
+    const double *rp = t + (size_t) a * (2 + NR) * gn + grp;
+    const double x0 = rp[0], x1 = rp[gn];
+    double xa[3];
+#pragma unroll
+    for (int d = 0; d < 3; d++) xa[d] = fma(x0, g.p1[d], fma(x1, g.p2[d], g.d0[d]));
+    double in[NCH][NC];
+#pragma unroll
+    for (int c = 0; c < NCH; c++)
+#pragma unroll
+      for (int j = 0; j < NC; j++) in[c][j] = 0.0;
+#pragma unroll
+    for (int b = 0; b < VT_Q; b++) {
+      // column point formed here rather than kept for all a (register budget of 128)
+      const double *cp = col + (size_t) b * (2 + NC) * gn + grp;
+      const double y0 = cp[0], y1 = cp[gn];
+      const double dx = xa[0] - fma(y0, g.q1[0], y1 * g.q2[0]);
+      const double dy = xa[1] - fma(y0, g.q1[1], y1 * g.q2[1]);
+      const double dz = xa[2] - fma(y0, g.q1[2], y1 * g.q2[2]);
+      const double r2 = fma(dx, dx, fma(dy, dy, dz * dz));
+      const double dot = DOT ? fma(dx, n0, fma(dy, n1, dz * n2)) : 0.0;
+      double kv[2];
+      eval_kernel<KK>(r2, dot, k_re, k_imn, kv);
+#pragma unroll
+      for (int j = 0; j < NC; j++) {
+        const double w = cp[(size_t) (2 + j) * gn];
+#pragma unroll
+        for (int c = 0; c < NCH; c++) in[c][j] = fma(w, kv[c], in[c][j]);
+      }
+    }
+#pragma unroll
+    for (int i = 0; i < NR; i++) {
+      const double w = rp[(size_t) (2 + i) * gn];
+#pragma unroll
+      for (int c = 0; c < NCH; c++)
+#pragma unroll
+        for (int j = 0; j < NC; j++) acc[c][i][j] = fma(w, in[c][j], acc[c][i][j]);
+    }
+  }
+}
+
 // One distant pair with the q^4 tensor rule, summed column side first:
 //   acc[c][i][j] = sum_a w_a phi_i(x_a) sum_b w_b phi_j(y_b) k_c(x_a, y_b).
 // With X_a = x_a - A_s and Y_b = y_b - A_s the difference is x_a - y_b = X_a - Y_b and the double
@@ -662,6 +718,7 @@ struct SingArgs {
   uint32_t rule_n[4];         // points per case (index 1..3)
   uint32_t rule_off[4];       // offset (in doubles) of each case's block in `rule`
   uint32_t rule_total;        // doubles in `rule` (multiple of 2, 16-byte aligned)
+  int vert_tensor;            // 1: case 1 in tensor form (rule_n[1] groups, q2 = 4)
   int staged;                 // 1: copy `rule` into shared memory first
   int *err;                   // set to 1 if the staging copy did not complete
 };
@@ -752,7 +809,11 @@ __global__ void __launch_bounds__(SING_THREADS, 1) near_sing_kernel(SingArgs a) 
       for (int i = 0; i < NR; i++)
 #pragma unroll
         for (int j = 0; j < NC; j++) acc[c][i][j] = 0.0;
-    if (cs == 1u) {
+    if (cs == 1u && a.vert_tensor) {
+      // common vertex, tensor form: a group of VT_Q x VT_Q points per lane
+      for (uint32_t grp = lane; grp < n; grp += 32)
+        vert_group_tensor<KK, RL, CL>(g, rx0, n, grp, n0, n1, n2, a.k_re, a.k_imn, acc);
+    } else if (cs == 1u) {
       // common vertex: the full rule (x0, x1, y0, y1, raw weight)
       const double *rx1 = rx0 + n, *ry0 = rx0 + 2 * n, *ry1 = rx0 + 3 * n, *rw = rx0 + 4 * n;
 #pragma unroll SING_UNROLL
@@ -887,6 +948,7 @@ int launch_sing(const h2b_near_launch *L, cudaStream_t st) {
     a.rule_off[i] = L->rule_off[i];
   }
   a.rule_total = L->rule_total;
+  a.vert_tensor = L->vert_tensor;
   a.staged = staged;
   a.err = L->err;
   int sms = L->num_sms > 0 ? L->num_sms : 148;

@@ -36,6 +36,7 @@ typedef struct {
   double mass[9];                /* linear-basis mass matrix on the reference triangle */
   const double *rule;            /* packed singular rules (device) */
   uint32_t rule_n[4], rule_off[4], rule_total;
+  int vert_tensor;               /* 1: common-vertex rule in tensor form (groups in rule_n[1]) */
   int num_sms;
   int *err;                      /* device flag */
   cudaEvent_t ev_between;        /* optional: recorded between the distant and singular kernels */
