@@ -30,42 +30,70 @@ __device__ __forceinline__ double lagr1(double x, const double *xi, int mu, int 
   return v;
 }
 
-__device__ __forceinline__ double dlagr1(double x, const double *xi, int mu, int m) {
+// Lagrange polynomial mu of nodes xi[0..m) at x as wbar_mu prod_{l != mu} (x - xi_l), with the
+// barycentric weight wbar_mu = 1 / prod_{l != mu} (xi_mu - xi_l) computed once per node set,
+// and its derivative wbar_mu sum_{l != mu} prod_{l2 != mu, l} (x - xi_l2): the same polynomials
+// as lagr1 (and its derivative) without a division per evaluation.
+__device__ __forceinline__ double lagr_bar(double x, const double *xi, double wbar, int mu, int m) {
+  double v = wbar;
+  for (int l = 0; l < m; l++)
+    if (l != mu) v *= x - xi[l];
+  return v;
+}
+
+__device__ __forceinline__ double dlagr_bar(double x, const double *xi, double wbar, int mu,
+                                            int m) {
   double s = 0.0;
   for (int l = 0; l < m; l++) {
     if (l == mu) continue;
     double tmp = 1.0;
     for (int l2 = 0; l2 < m; l2++)
-      if (l2 != mu && l2 != l) tmp *= (x - xi[l2]) / (xi[mu] - xi[l2]);
-    s += tmp / (xi[mu] - xi[l]);
+      if (l2 != mu && l2 != l) tmp *= x - xi[l2];
+    s += tmp;
   }
-  return s;
+  return wbar * s;
 }
 
-// Leaf bases.  Rows of leaf c: its triangles (constant basis) or vertices (linear basis).
-// The CTA's triangle list (TriRef, local row indices) is processed in batches of BATCH
-// triangles: first the one-dimensional Lagrange values (and derivatives) at every quadrature
-// point of the batch are tabulated in shared memory (3 axes x m), then each (triangle, nu) work
-// item forms the tensor products from the table.  The cluster's V block (rows x k) is
-// accumulated in shared memory (atomics for the linear basis, where a vertex receives the
-// integrals of all triangles around it) and written once.
+// Leaf bases.  Rows of leaf c: its triangles (constant basis) or vertices (linear basis).  A
+// leaf's nu range is split over LEAF_SPLIT CTAs (CTA (leaf, part) computes the columns
+// [part k / LEAF_SPLIT, ...)), so that the launch has several CTAs per SM.  The CTA's triangle
+// list (TriRef, local row indices) is processed in batches of BATCH triangles: first the
+// one-dimensional Lagrange values (and derivatives) at every quadrature point of the batch are
+// tabulated in shared memory (3 axes x m), then each (triangle, nu) work item forms the tensor
+// products from the table.  The CTA's columns of V (rows x its nu) are accumulated in shared
+// memory (atomics for the linear basis, where a vertex receives the integrals of all triangles
+// around it) and written once.
 constexpr int BATCH = 32;
 constexpr int NSMAX = 64;   // single-triangle rule points (q^2, q <= 8)
+constexpr int LEAF_SPLIT = 4;
 
 template <bool LINEAR, bool DN>
 __global__ void __launch_bounds__(256) leaf_basis_kernel(FarLeafArgs a) {
   extern __shared__ double smem[];
-  const uint32_t leaf = blockIdx.x;
+  __shared__ double wbar[3][MMAX];
+  const uint32_t leaf = blockIdx.x / LEAF_SPLIT, part = blockIdx.x % LEAF_SPLIT;
   const uint32_t c = a.leaves[leaf];
   const int m = a.m, k = a.k;
+  const int nu0 = (int) ((part * (uint32_t) k) / LEAF_SPLIT);
+  const int nu1 = (int) (((part + 1) * (uint32_t) k) / LEAF_SPLIT);
+  const int kp = nu1 - nu0;
   const uint32_t rows = a.size[c];
   const uint32_t tr0 = a.tr_off[leaf], ntr = a.tr_len[leaf];
   const double *pts = a.pts + (size_t) c * 3 * m;
   const int ns = a.ns;
-  double *V = smem;                                   // rows * k
-  double *tab = V + (size_t) rows * k;                // BATCH * ns * 3 * m  (values)
+  const int kpmax = (k + LEAF_SPLIT - 1) / LEAF_SPLIT;
+  double *V = smem;                                   // rows * kp (the CTA's columns)
+  double *tab = V + (size_t) rows * kpmax;            // BATCH * ns * 3 * m
   double *dtab = tab + (size_t) BATCH * ns * 3 * m;   // same size (derivatives, DN only)
-  for (uint32_t e = threadIdx.x; e < rows * (uint32_t) k; e += blockDim.x) V[e] = 0.0;
+  for (uint32_t e = threadIdx.x; e < rows * (uint32_t) kp; e += blockDim.x) V[e] = 0.0;
+  if (threadIdx.x < 3u * (uint32_t) m) {
+    const int d = (int) threadIdx.x / m, mu = (int) threadIdx.x % m;
+    const double *xi = pts + d * m;
+    double p = 1.0;
+    for (int l = 0; l < m; l++)
+      if (l != mu) p *= xi[mu] - xi[l];
+    wbar[d][mu] = 1.0 / p;
+  }
 
   for (uint32_t b0 = 0; b0 < ntr; b0 += BATCH) {
     const uint32_t nb = ntr - b0 < (uint32_t) BATCH ? ntr - b0 : (uint32_t) BATCH;
@@ -78,14 +106,14 @@ __global__ void __launch_bounds__(256) leaf_basis_kernel(FarLeafArgs a) {
       const double tx = a.xs[q], sx = a.ys[q];
       const double x = T.a[d] * (1.0 - tx) + T.b[d] * (tx - sx) + T.c[d] * sx;
       const double *xi = pts + d * m;
-      tab[e] = lagr1(x, xi, mu, m);
-      if (DN) dtab[e] = dlagr1(x, xi, mu, m);
+      tab[e] = lagr_bar(x, xi, wbar[d][mu], mu, m);
+      if (DN) dtab[e] = dlagr_bar(x, xi, wbar[d][mu], mu, m);
     }
     __syncthreads();
-    // work item = (triangle in batch, nu)
-    for (uint32_t it = threadIdx.x; it < nb * (uint32_t) k; it += blockDim.x) {
-      const uint32_t s = it / (uint32_t) k;
-      const int nu = (int) (it - s * (uint32_t) k);
+    // work item = (triangle in batch, nu of this CTA)
+    for (uint32_t it = threadIdx.x; it < nb * (uint32_t) kp; it += blockDim.x) {
+      const uint32_t s = it / (uint32_t) kp;
+      const int lnu = (int) (it - s * (uint32_t) kp), nu = nu0 + lnu;
       const int jx = nu / (m * m), jy = (nu / m) % m, jz = nu % m;
       const TriRef r = a.refs[tr0 + b0 + s];
       const TriRec &T = a.tri[r.t];
@@ -112,10 +140,10 @@ __global__ void __launch_bounds__(256) leaf_basis_kernel(FarLeafArgs a) {
 #pragma unroll
         for (int l = 0; l < 3; l++) {
           const int row = r.l[l];
-          if (row >= 0) atomicAdd(&V[row + (uint32_t) nu * rows], sum[l] * T.g);
+          if (row >= 0) atomicAdd(&V[row + (uint32_t) lnu * rows], sum[l] * T.g);
         }
       } else {
-        V[r.l[0] + (uint32_t) nu * rows] = T.g * sum[0];
+        V[r.l[0] + (uint32_t) lnu * rows] = T.g * sum[0];
       }
     }
   }
@@ -123,12 +151,13 @@ __global__ void __launch_bounds__(256) leaf_basis_kernel(FarLeafArgs a) {
   double *out = a.V + a.voff[c];
   if (a.transposed) {
     // V^T, k x rows column-major: consecutive threads write consecutive nu
-    for (uint32_t e = threadIdx.x; e < rows * (uint32_t) k; e += blockDim.x) {
-      const uint32_t nu = e % (uint32_t) k, i = e / (uint32_t) k;
-      out[e] = V[i + nu * rows];
+    for (uint32_t e = threadIdx.x; e < rows * (uint32_t) kp; e += blockDim.x) {
+      const uint32_t lnu = e % (uint32_t) kp, i = e / (uint32_t) kp;
+      out[(size_t) nu0 + lnu + (size_t) i * k] = V[i + lnu * rows];
     }
   } else {
-    for (uint32_t e = threadIdx.x; e < rows * (uint32_t) k; e += blockDim.x) out[e] = V[e];
+    double *o = out + (size_t) nu0 * rows;
+    for (uint32_t e = threadIdx.x; e < rows * (uint32_t) kp; e += blockDim.x) o[e] = V[e];
   }
 }
 
@@ -157,12 +186,15 @@ __global__ void __launch_bounds__(256) transfer_kernel(FarTransferArgs a) {
   }
 }
 
-// Coupling matrices: S_b[i, j] = (1/4pi) g(xi^r_i, xi^c_j).
-template <bool CX>
+// Coupling matrices: S_b[i, j] = (1/4pi) g(xi^r_i, xi^c_j), i = (ix m + iy) m + iz.  Written as
+// one coalesced store stream per block (HBM bound: 8 or 16 bytes per entry).  M > 0 fixes the
+// interpolation order at compile time (the index arithmetic then uses constant divisors); the
+// reciprocal distance is the FP64 reciprocal square root of the nearfield kernels.
+template <bool CX, int M>
 __global__ void __launch_bounds__(256) coupling_kernel(FarCouplingArgs a) {
   const uint32_t b = blockIdx.x;
   const uint32_t rc = a.rc[b], cc = a.cc[b];
-  const int m = a.m, k = a.k;
+  const int m = M > 0 ? M : a.m, k = M > 0 ? M * M * M : a.k;
   const double *rp = a.rpts + (size_t) rc * 3 * m, *cp = a.cpts + (size_t) cc * 3 * m;
   double *S = a.S + (size_t) b * k * k * (CX ? 2 : 1);
   for (int e = threadIdx.x; e < k * k; e += blockDim.x) {
@@ -171,7 +203,7 @@ __global__ void __launch_bounds__(256) coupling_kernel(FarCouplingArgs a) {
     const double y0 = cp[j / (m * m)], y1 = cp[m + (j / m) % m], y2 = cp[2 * m + j % m];
     const double d0 = x0 - y0, d1 = x1 - y1, d2 = x2 - y2;
     const double r2 = d0 * d0 + d1 * d1 + d2 * d2;
-    const double rinv = 1.0 / sqrt(r2);
+    const double rinv = rsqrt_nr(r2);
     if (!CX) {
       S[e] = a.kconst * rinv;
     } else {
@@ -188,7 +220,7 @@ __global__ void __launch_bounds__(256) coupling_kernel(FarCouplingArgs a) {
 
 extern "C" int h2b_far_leaf_basis(const FarLeafArgs *a, int linear, int dn, cudaStream_t st) {
   if (a->nleaves == 0) return H2B_OK;
-  const size_t smem = sizeof(double) * ((size_t) a->max_rows * a->k +
+  const size_t smem = sizeof(double) * ((size_t) a->max_rows * ((a->k + LEAF_SPLIT - 1) / LEAF_SPLIT) +
                                         2 * (size_t) BATCH * a->ns * 3 * a->m);
   if (smem > 200u * 1024u || a->ns > NSMAX) {
     h2b_set_error("leaf basis block of %u x %d (rule of %d points) exceeds shared memory",
@@ -198,7 +230,7 @@ extern "C" int h2b_far_leaf_basis(const FarLeafArgs *a, int linear, int dn, cuda
 #define LAUNCH(L, D)                                                                        \
   do {                                                                                      \
     H2B_CUDA_TRY((h2b_allow_smem<leaf_basis_kernel<L, D>>()));                             \
-    leaf_basis_kernel<L, D><<<a->nleaves, 256, smem, st>>>(*a);                             \
+    leaf_basis_kernel<L, D><<<a->nleaves * LEAF_SPLIT, 256, smem, st>>>(*a);                \
   } while (0)
   if (linear && dn) LAUNCH(true, true);
   else if (linear) LAUNCH(true, false);
@@ -222,10 +254,17 @@ extern "C" int h2b_far_transfer(const FarTransferArgs *a, cudaStream_t st) {
 
 extern "C" int h2b_far_coupling(const FarCouplingArgs *a, int cx, cudaStream_t st) {
   if (a->n == 0) return H2B_OK;
-  if (cx)
-    coupling_kernel<true><<<a->n, 256, 0, st>>>(*a);
-  else
-    coupling_kernel<false><<<a->n, 256, 0, st>>>(*a);
+#define LAUNCH(CXV, MV) coupling_kernel<CXV, MV><<<a->n, 256, 0, st>>>(*a)
+  if (cx) {
+    if (a->m == 4) LAUNCH(true, 4);
+    else if (a->m == 5) LAUNCH(true, 5);
+    else LAUNCH(true, 0);
+  } else {
+    if (a->m == 4) LAUNCH(false, 4);
+    else if (a->m == 5) LAUNCH(false, 5);
+    else LAUNCH(false, 0);
+  }
+#undef LAUNCH
   H2B_CUDA_TRY(cudaGetLastError());
   return H2B_OK;
 }
