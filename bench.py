@@ -269,6 +269,9 @@ def run_ours(a, rank, world, local):
     near_sing_ms = statistics.mean(p[0]["near_singular"] for p in phases)
     dist_flops = pc["distant"] * 16 * (FLOPS_PER_POINT["slp"] + FLOPS_PER_POINT["dlp"])
     sing_points = pc["vertex"] * 512 + pc["edge"] * 1536 + pc["identical"] * 1536
+    # kernel evaluations the singular kernel executes for q2 = 4: the edge and identical rules
+    # merged to 384 and 96 points (the kernel argument does not depend on the merged variables)
+    sing_evals = pc["vertex"] * 512 + pc["edge"] * 384 + pc["identical"] * 96
     peak = fp64_peak_tflops(torch)
     # achieved: the flops the kernel's algorithm (tensor-factored pair sum) executes per launch;
     # the reference's point-by-point count of the same quadrature is reported beside it
@@ -440,6 +443,7 @@ def run_ours(a, rank, world, local):
                      for k in ("row_basis", "col_basis", "coupling")} |
                     {"near_distant_fused": near_dist_ms, "near_singular_fused": near_sing_ms},
         "pairs_per_operator": pc, "singular_points": sing_points,
+        "singular_kernel_evaluations": sing_evals,
         "roofline": roofline, "roofline_matvec": roof_mv, "solve": solve, "mixed": mixed,
         "e2e": e2e,
         "clocks": clocks.summary(),

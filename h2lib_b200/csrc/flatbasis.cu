@@ -40,92 +40,65 @@ __device__ __forceinline__ void cta_copy(double *dst, size_t n, F src) {
   }
 }
 
-// One CTA per item (father f, son s, first row r0 of s, rows nr <= FLAT_ROWS): the nr rows of
-// W_s times E_s land in the rows of s inside W_f.
+// CTA (item, part): item = (father f, son s, first row r0 of s, rows nr <= H2B_FLAT_ROWS), part =
+// FLAT_COLS consecutive columns nu of the product; the nr rows of W_s times those columns of E_s
+// land in the rows of s inside W_f.  Splitting the columns over several CTAs gives every level's
+// launch enough CTAs (a level has few items near the root) and keeps each CTA's shared memory
+// small; the son's rows are read by each part (from L2).
+constexpr int FLAT_COLS = 16;
 __global__ void __launch_bounds__(FLAT_TPB) flatten_kernel(FlatArgs a) {
   extern __shared__ double sm[];
-  const uint32_t *it = a.items + 4 * (size_t) blockIdx.x;
-  const uint32_t f = it[0], s = it[1], r0 = it[2], nr = it[3];
   const uint32_t k = (uint32_t) a.k;
-  double *sE = sm;             // k x k
-  double *sW = sm + k * k;     // nr rows of W_s (layout of the side)
+  const uint32_t nparts = (k + FLAT_COLS - 1) / FLAT_COLS;
+  const uint32_t item = blockIdx.x / nparts, part = blockIdx.x % nparts;
+  const uint32_t *it = a.items + 4 * (size_t) item;
+  const uint32_t f = it[0], s = it[1], r0 = it[2], nr = it[3];
+  const uint32_t c0 = part * FLAT_COLS, nc = min((uint32_t) FLAT_COLS, k - c0);
+  double *sE = sm;                  // k x FLAT_COLS: sE[mu + j k] = E_s[mu, c0 + j]
+  double *sW = sm + k * FLAT_COLS;  // nr x k: sW[i + mu nr] = W_s[r0 + i, mu]
   const double *E = a.E + (size_t) (s - 1) * k * k;
-  cta_copy(sE, (size_t) k * k, [&](size_t e) { return E[e]; });
   const uint32_t ns = a.size[s], nf = a.size[f];
   const uint32_t rf = a.off[s] - a.off[f] + r0;  // first row inside f
   const double *Ws = a.W + a.woff[s];
   double *Wf = a.W + a.woff[f];
-  // Each thread computes a 4 x 4 tile of the nr x k product (16 x 16 threads cover 64 x 64
-  // per pass), reading 4 + 4 shared-memory values per 16 FMAs.
-  const uint32_t tr = threadIdx.x % 16, tc = threadIdx.x / 16;
   if (!a.transposed) {
-    // sW[i + mu nr] = W_s[r0 + i, mu]
+    // E_s column-major: the part's columns are contiguous
+    cta_copy(sE, (size_t) k * nc, [&](size_t e) { return E[(size_t) c0 * k + e]; });
     cta_copy(sW, (size_t) nr * k, [&](size_t e) {
       const uint32_t i = (uint32_t) (e % nr), mu = (uint32_t) (e / nr);
       return Ws[r0 + i + (size_t) mu * ns];
     });
-    __syncthreads();
-    // W_f[rf + i, nu] = sum_mu W_s[r0 + i, mu] E_s[mu, nu]   (E_s column-major k x k)
-    for (uint32_t c0 = 0; c0 < k; c0 += 64) {
-      double acc[4][4] = {};
-      uint32_t ii[4], nn[4];
-#pragma unroll
-      for (int q = 0; q < 4; q++) {
-        ii[q] = min(4 * tr + q, nr - 1);
-        nn[q] = min(c0 + 4 * tc + q, k - 1);
-      }
-      for (uint32_t mu = 0; mu < k; mu++) {
-        double x[4], y[4];
-#pragma unroll
-        for (int q = 0; q < 4; q++) {
-          x[q] = sW[ii[q] + mu * nr];
-          y[q] = sE[mu + nn[q] * k];
-        }
-#pragma unroll
-        for (int p = 0; p < 4; p++)
-#pragma unroll
-          for (int q = 0; q < 4; q++) acc[p][q] = fma(x[p], y[q], acc[p][q]);
-      }
-#pragma unroll
-      for (int p = 0; p < 4; p++)
-#pragma unroll
-        for (int q = 0; q < 4; q++) {
-          const uint32_t i = 4 * tr + p, nu = c0 + 4 * tc + q;
-          if (i < nr && nu < k) Wf[rf + i + (size_t) nu * nf] = acc[p][q];
-        }
-    }
   } else {
-    // sW[mu + i k] = W_s^T[mu, r0 + i]
-    cta_copy(sW, (size_t) nr * k, [&](size_t e) { return Ws[(size_t) r0 * k + e]; });
-    __syncthreads();
-    // W_f^T[nu, rf + i] = sum_mu E_s^T[nu, mu] W_s^T[mu, r0 + i]   (E_s^T column-major k x k)
-    for (uint32_t c0 = 0; c0 < k; c0 += 64) {
-      double acc[4][4] = {};
-      uint32_t nn[4], ii[4];
+    // E_s^T column-major (k x k): E_s[mu, nu] = E^T[nu + mu k]
+    cta_copy(sE, (size_t) k * nc, [&](size_t e) {
+      const uint32_t mu = (uint32_t) (e % k), j = (uint32_t) (e / k);
+      return E[c0 + j + (size_t) mu * k];
+    });
+    // W_s^T (k x |s|, ld k): sW[i + mu nr] = W_s^T[mu, r0 + i]
+    cta_copy(sW, (size_t) nr * k, [&](size_t e) {
+      const uint32_t i = (uint32_t) (e % nr), mu = (uint32_t) (e / nr);
+      return Ws[(size_t) (r0 + i) * k + mu];
+    });
+  }
+  __syncthreads();
+  // thread: row i = t % 64 (<= H2B_FLAT_ROWS = 64 rows), columns j = 4 (t / 64) .. + 3
+  const uint32_t i = threadIdx.x % 64, jq = 4 * (threadIdx.x / 64);
+  if (i < nr && jq < nc) {
+    double acc[4] = {0.0, 0.0, 0.0, 0.0};
+    for (uint32_t mu = 0; mu < k; mu++) {
+      const double x = sW[i + mu * nr];
 #pragma unroll
-      for (int q = 0; q < 4; q++) {
-        nn[q] = min(c0 + 4 * tr + q, k - 1);
-        ii[q] = min(4 * tc + q, nr - 1);
+      for (int q = 0; q < 4; q++) acc[q] = fma(x, sE[mu + (jq + q) * k], acc[q]);
+    }
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      const uint32_t nu = c0 + jq + q;
+      if (jq + q < nc) {
+        if (a.transposed)
+          Wf[(size_t) (rf + i) * k + nu] = acc[q];
+        else
+          Wf[rf + i + (size_t) nu * nf] = acc[q];
       }
-      for (uint32_t mu = 0; mu < k; mu++) {
-        double x[4], y[4];
-#pragma unroll
-        for (int q = 0; q < 4; q++) {
-          x[q] = sE[nn[q] + mu * k];
-          y[q] = sW[mu + ii[q] * k];
-        }
-#pragma unroll
-        for (int p = 0; p < 4; p++)
-#pragma unroll
-          for (int q = 0; q < 4; q++) acc[p][q] = fma(x[p], y[q], acc[p][q]);
-      }
-#pragma unroll
-      for (int p = 0; p < 4; p++)
-#pragma unroll
-        for (int q = 0; q < 4; q++) {
-          const uint32_t nu = c0 + 4 * tr + p, i = 4 * tc + q;
-          if (i < nr && nu < k) Wf[(size_t) (rf + i) * k + nu] = acc[p][q];
-        }
     }
   }
 }
@@ -165,13 +138,14 @@ extern "C" int h2b_flat_leaves(const FlatLeafArgs *a, cudaStream_t st) {
 
 extern "C" int h2b_flat_level(const FlatArgs *a, cudaStream_t st) {
   if (a->nitems == 0) return H2B_OK;
-  const size_t smem = sizeof(double) * ((size_t) a->k * a->k + (size_t) H2B_FLAT_ROWS * a->k);
+  const size_t smem = sizeof(double) * ((size_t) a->k * FLAT_COLS + (size_t) H2B_FLAT_ROWS * a->k);
   if (smem > H2B_MAX_DYN_SMEM) {
     h2b_set_error("flattened bases: rank %d needs %zu bytes of shared memory", a->k, smem);
     return H2B_ERR_ARG;
   }
   H2B_CUDA_TRY(h2b_allow_smem<flatten_kernel>());
-  flatten_kernel<<<a->nitems, FLAT_TPB, smem, st>>>(*a);
+  const uint32_t nparts = ((uint32_t) a->k + FLAT_COLS - 1) / FLAT_COLS;
+  flatten_kernel<<<a->nitems * nparts, FLAT_TPB, smem, st>>>(*a);
   H2B_CUDA_TRY(cudaGetLastError());
   return H2B_OK;
 }
