@@ -55,7 +55,8 @@ __global__ void __launch_bounds__(FLAT_TPB) flatten_kernel(FlatArgs a) {
   const uint32_t f = it[0], s = it[1], r0 = it[2], nr = it[3];
   const uint32_t c0 = part * FLAT_COLS, nc = min((uint32_t) FLAT_COLS, k - c0);
   double *sE = sm;                  // k x FLAT_COLS: sE[mu + j k] = E_s[mu, c0 + j]
-  double *sW = sm + k * FLAT_COLS;  // nr x k: sW[i + mu nr] = W_s[r0 + i, mu]
+  double *sW = sm + k * FLAT_COLS;  // W_s[r0 + i, mu]: sW[i + mu nr] (row side), sW[mu + i (k + 1)]
+                                    // (column side)
   const double *E = a.E + (size_t) (s - 1) * k * k;
   const uint32_t ns = a.size[s], nf = a.size[f];
   const uint32_t rf = a.off[s] - a.off[f] + r0;  // first row inside f
@@ -69,24 +70,27 @@ __global__ void __launch_bounds__(FLAT_TPB) flatten_kernel(FlatArgs a) {
       return Ws[r0 + i + (size_t) mu * ns];
     });
   } else {
-    // E_s^T column-major (k x k): E_s[mu, nu] = E^T[nu + mu k]
-    cta_copy(sE, (size_t) k * nc, [&](size_t e) {
-      const uint32_t mu = (uint32_t) (e % k), j = (uint32_t) (e / k);
-      return E[c0 + j + (size_t) mu * k];
-    });
-    // W_s^T (k x |s|, ld k): sW[i + mu nr] = W_s^T[mu, r0 + i]
-    cta_copy(sW, (size_t) nr * k, [&](size_t e) {
-      const uint32_t i = (uint32_t) (e % nr), mu = (uint32_t) (e / nr);
-      return Ws[(size_t) (r0 + i) * k + mu];
-    });
+    // E_s^T column-major (k x k): E_s[mu, nu] = E^T[nu + mu k]; read the part's rows of each
+    // column of E^T contiguously
+    for (uint32_t e = threadIdx.x; e < k * nc; e += blockDim.x) {
+      const uint32_t j = e % nc, mu = e / nc;
+      sE[mu + j * k] = E[c0 + j + (size_t) mu * k];
+    }
+    // W_s^T (k x |s|, ld k) is contiguous over the item's rows: sW[mu + i (k + 1)] (padded
+    // stride, so that a warp's rows fall in different banks)
+    for (uint32_t e = threadIdx.x; e < nr * k; e += blockDim.x) {
+      const uint32_t mu = e % k, i = e / k;
+      sW[mu + i * (k + 1)] = Ws[(size_t) r0 * k + e];
+    }
   }
   __syncthreads();
   // thread: row i = t % 64 (<= H2B_FLAT_ROWS = 64 rows), columns j = 4 (t / 64) .. + 3
   const uint32_t i = threadIdx.x % 64, jq = 4 * (threadIdx.x / 64);
+  const uint32_t si = a.transposed ? i * (k + 1) : i, smu = a.transposed ? 1 : nr;
   if (i < nr && jq < nc) {
     double acc[4] = {0.0, 0.0, 0.0, 0.0};
     for (uint32_t mu = 0; mu < k; mu++) {
-      const double x = sW[i + mu * nr];
+      const double x = sW[si + mu * smu];
 #pragma unroll
       for (int q = 0; q < 4; q++) acc[q] = fma(x, sE[mu + (jq + q) * k], acc[q]);
     }
@@ -138,7 +142,7 @@ extern "C" int h2b_flat_leaves(const FlatLeafArgs *a, cudaStream_t st) {
 
 extern "C" int h2b_flat_level(const FlatArgs *a, cudaStream_t st) {
   if (a->nitems == 0) return H2B_OK;
-  const size_t smem = sizeof(double) * ((size_t) a->k * FLAT_COLS + (size_t) H2B_FLAT_ROWS * a->k);
+  const size_t smem = sizeof(double) * ((size_t) a->k * FLAT_COLS + (size_t) H2B_FLAT_ROWS * (a->k + 1));
   if (smem > H2B_MAX_DYN_SMEM) {
     h2b_set_error("flattened bases: rank %d needs %zu bytes of shared memory", a->k, smem);
     return H2B_ERR_ARG;

@@ -1018,48 +1018,73 @@ __device__ uint32_t pair_code_dev(const uint32_t tv[3], const uint32_t sv[3]) {
 }
 
 // One CTA per tile, a thread per triangle pair; warp-aggregated atomics per case.
+// The tile's vertex ids are staged in shared memory in chunks of CL_CHUNK triangles per side (a
+// warp then reads consecutive words, or one broadcast word, instead of one triangle record per
+// lane).
+constexpr int CL_CHUNK = 256;
 template <bool WRITE>
 __global__ void __launch_bounds__(256) classify_kernel(const TriRec *tri, const TriRef *refs,
                                                        const h2b_tile *tiles, uint32_t *cursor,
                                                        const uint32_t *base, h2b_sing *out) {
+  __shared__ uint32_t rv[3][CL_CHUNK], cv[3][CL_CHUNK];
   const h2b_tile tl = tiles[blockIdx.x];
-  const uint32_t ntr = tl.tr_len, npairs = tl.tr_len * tl.sc_len;
+  const uint32_t ntr = tl.tr_len, nsc = tl.sc_len;
   const uint32_t lane = threadIdx.x & 31;
-  for (uint32_t p0 = 0; p0 < npairs; p0 += blockDim.x) {
-    const uint32_t p = p0 + threadIdx.x;
-    uint32_t code = 0, cs = 0, is = 0, it = 0;
-    if (p < npairs) {
-      is = p / ntr;
-      it = p - is * ntr;
-      const TriRec &T = tri[refs[tl.tr_off + it].t];
-      const TriRec &S = tri[refs[tl.sc_off + is].t];
-      const uint32_t tv[3] = {T.v[0], T.v[1], T.v[2]}, sv[3] = {S.v[0], S.v[1], S.v[2]};
-      bool shared = false;
-#pragma unroll
-      for (int i = 0; i < 3; i++)
-#pragma unroll
-        for (int j = 0; j < 3; j++) shared |= tv[i] == sv[j];
-      if (shared) {
-        code = pair_code_dev(tv, sv);
-        cs = code & 3u;
+  for (uint32_t c0 = 0; c0 < nsc; c0 += CL_CHUNK) {
+    const uint32_t nc = min((uint32_t) CL_CHUNK, nsc - c0);
+    for (uint32_t r0 = 0; r0 < ntr; r0 += CL_CHUNK) {
+      const uint32_t nr = min((uint32_t) CL_CHUNK, ntr - r0);
+      __syncthreads();  // the previous chunk pair is done with the stage
+      for (uint32_t e = threadIdx.x; e < nr; e += blockDim.x) {
+        const TriRec &T = tri[refs[tl.tr_off + r0 + e].t];
+        rv[0][e] = T.v[0];
+        rv[1][e] = T.v[1];
+        rv[2][e] = T.v[2];
       }
-    }
-    // every thread of the warp reaches the ballots (the loop bound is uniform per CTA)
+      for (uint32_t e = threadIdx.x; e < nc; e += blockDim.x) {
+        const TriRec &S = tri[refs[tl.sc_off + c0 + e].t];
+        cv[0][e] = S.v[0];
+        cv[1][e] = S.v[1];
+        cv[2][e] = S.v[2];
+      }
+      __syncthreads();
+      const uint32_t np = nr * nc;
+      for (uint32_t p0 = 0; p0 < np; p0 += blockDim.x) {
+        const uint32_t p = p0 + threadIdx.x;
+        uint32_t code = 0, cs = 0, is = 0, it = 0;
+        if (p < np) {
+          is = p / nr;
+          it = p - is * nr;
+          const uint32_t tv[3] = {rv[0][it], rv[1][it], rv[2][it]};
+          const uint32_t sv[3] = {cv[0][is], cv[1][is], cv[2][is]};
+          bool shared = false;
 #pragma unroll
-    for (uint32_t c = 1; c <= 3; c++) {
-      const unsigned m = __ballot_sync(0xffffffffu, cs == c);
-      if (m == 0) continue;
-      const uint32_t leader = __ffs(m) - 1;
-      uint32_t b = 0;
-      if (lane == leader) b = atomicAdd(&cursor[c], (uint32_t) __popc(m));
-      b = __shfl_sync(0xffffffffu, b, leader);
-      if (WRITE && cs == c) {
-        h2b_sing sg;
-        sg.tile = blockIdx.x;
-        sg.tr = tl.tr_off + it;
-        sg.sc = tl.sc_off + is;
-        sg.code = code;
-        out[base[c] + b + __popc(m & ((1u << lane) - 1u))] = sg;
+          for (int i = 0; i < 3; i++)
+#pragma unroll
+            for (int j = 0; j < 3; j++) shared |= tv[i] == sv[j];
+          if (shared) {
+            code = pair_code_dev(tv, sv);
+            cs = code & 3u;
+          }
+        }
+        // every thread of the warp reaches the ballots (the loop bound is uniform per CTA)
+#pragma unroll
+        for (uint32_t c = 1; c <= 3; c++) {
+          const unsigned m = __ballot_sync(0xffffffffu, cs == c);
+          if (m == 0) continue;
+          const uint32_t leader = __ffs(m) - 1;
+          uint32_t b = 0;
+          if (lane == leader) b = atomicAdd(&cursor[c], (uint32_t) __popc(m));
+          b = __shfl_sync(0xffffffffu, b, leader);
+          if (WRITE && cs == c) {
+            h2b_sing sg;
+            sg.tile = blockIdx.x;
+            sg.tr = tl.tr_off + r0 + it;
+            sg.sc = tl.sc_off + c0 + is;
+            sg.code = code;
+            out[base[c] + b + __popc(m & ((1u << lane) - 1u))] = sg;
+          }
+        }
       }
     }
   }
