@@ -96,6 +96,7 @@ _SIGS = {
     "h2b_server_submit": (C.c_int64, [vp, vp]),
     "h2b_server_wait": (C.c_int, [vp, C.c_int64, vp, vp]),
     "h2b_server_stats": (C.c_int, [vp, _u64p]),
+    "h2b_server_set_batching": (C.c_int, [vp, C.c_uint32]),
     "h2b_server_del": (None, [vp]),
     "h2b_project_l2_harmonic_multi": (C.c_int, [vp, C.c_uint32, _u32p, C.c_uint32, _f64p, vp]),
     "h2b_l2_error_harmonic_multi": (C.c_int, [vp, C.c_uint32, _u32p, C.c_uint32, _f64p, vp,

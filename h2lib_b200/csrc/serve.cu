@@ -2,9 +2,12 @@
 //
 // Requests (a surface mesh, a PDE, boundary data, a tolerance) are queued on submission.  A pool
 // of `slots` worker threads takes them in arrival order as soon as a slot is free and the
-// request's device-memory estimate fits the remaining HBM budget; each admitted request builds
-// its trees on the host, then runs structure upload, assembly, right-hand side and GMRES on its
-// own CUDA streams.  Requests that arrive while others are running are admitted as slots and
+// request's device-memory estimate fits the remaining HBM budget.  A worker also takes the queued
+// requests that can share the first one's operator (Laplace problems with the same solver
+// settings, up to the budget and the batch limits): their meshes become one forest H2 matrix
+// (one assembly, one batched GMRES in which every request keeps its own Krylov space and stop).
+// Each admitted request (or batch) builds its trees on the host, then runs structure upload,
+// assembly, right-hand side and GMRES on its own CUDA streams.  Requests that arrive while others are running are admitted as slots and
 // memory free up, and the kernels of all running requests overlap on the device (every handle
 // owns a non-blocking stream; device memory is stream-ordered, so one request's allocations and
 // frees never synchronise the device under another).  The H2 matrices and the Krylov state of a
@@ -67,6 +70,7 @@ struct h2b_server {
   uint32_t running = 0;
   uint64_t done = 0;
   bool stop = false;
+  uint32_t batch_max = 64;  // most requests one worker takes at once (1: no batching)
 };
 
 namespace {
@@ -193,8 +197,113 @@ int run_request(Req *q) {
   return rc;
 }
 
+// Requests that can share one operator: Laplace problems with the same solver settings (their
+// meshes become one block-diagonal forest H2 matrix and one batched GMRES; each request keeps
+// its own Krylov space, restarts and stop, so it ends as it would alone).
+bool batchable(const Req *a, const Req *b) {
+  return a->desc.pde == H2B_LAPLACE && b->desc.pde == H2B_LAPLACE &&
+         a->desc.flags == b->desc.flags && a->desc.eps == b->desc.eps &&
+         a->desc.maxiter == b->desc.maxiter && a->desc.kmax == b->desc.kmax;
+}
+
+// Run a batch of batchable Laplace requests on the calling worker thread: union mesh, forest
+// trees, one assembly of V and K, per-surface right-hand sides, one batched GMRES.
+int run_batch(const std::vector<Req *> &qs) {
+  auto tick = [] { return Clock::now(); };
+  auto secs = [](Clock::time_point a, Clock::time_point b) {
+    return std::chrono::duration<double>(b - a).count();
+  };
+  const auto c0 = tick();
+  const uint32_t ns = (uint32_t) qs.size();
+  const h2b_request &d = qs[0]->desc;
+  std::vector<uint32_t> voff(ns + 1, 0), toff(ns + 1, 0);
+  for (uint32_t i = 0; i < ns; i++) {
+    voff[i + 1] = voff[i] + qs[i]->desc.vertices;
+    toff[i + 1] = toff[i] + qs[i]->desc.triangles;
+  }
+  const uint32_t nv = voff[ns], nt = toff[ns];
+  std::vector<double> x(3 * (size_t) nv), n(3 * (size_t) nt), g(nt), zs(3 * (size_t) ns);
+  std::vector<uint32_t> t(3 * (size_t) nt);
+  for (uint32_t i = 0; i < ns; i++) {
+    memcpy(x.data() + 3 * (size_t) voff[i], qs[i]->x.data(), sizeof(double) * qs[i]->x.size());
+    for (size_t e = 0; e < qs[i]->t.size(); e++) t[3 * (size_t) toff[i] + e] = qs[i]->t[e] + voff[i];
+    for (int c = 0; c < 3; c++) zs[3 * (size_t) i + c] = qs[i]->desc.src[c];
+  }
+  int rc = h2b_prepare_surface(nv, x.data(), nt, t.data(), n.data(), g.data(), nullptr);
+  if (rc != H2B_OK) return rc;
+  h2b_surface *s = h2b_surface_new(nv, x.data(), nt, t.data(), n.data(), g.data());
+  if (!s) return H2B_ERR_CUDA;
+  const int L = H2B_BASIS_LINEAR;
+  h2b_bem *slp = h2b_bem_new(s, H2B_LAPLACE, H2B_SLP, L, L, 2, 4, 0.0, 0.0, 0.0, 0.0);
+  h2b_bem *dlp = h2b_bem_new(s, H2B_LAPLACE, H2B_DLP, L, L, 2, 4, 0.0, 0.0, 0.5, 0.0);
+  h2b_tree *tr = (slp && dlp) ? h2b_tree_new_forest(ns, voff.data(), toff.data(), x.data(),
+                                                    t.data(), L, L, 64, 1.4)
+                              : nullptr;
+  h2b_h2matrix *V = tr ? h2b_h2matrix_new(slp, tr, 4) : nullptr;
+  h2b_h2matrix *K = V ? h2b_h2matrix_new_like(dlp, V) : nullptr;
+  const bool mixed = (d.flags & H2B_SOLVE_MIXED) != 0;
+  if (V && K && mixed) {
+    h2b_h2matrix_set_precision(V, H2B_FP32);
+    h2b_h2matrix_set_precision(K, H2B_FP32);
+  }
+  const auto c1 = tick();
+  rc = (V && K) ? H2B_OK : H2B_ERR_CUDA;
+  for (h2b_h2matrix *h : {V, K}) {
+    if (rc == H2B_OK) rc = h2b_h2matrix_assemble_row_clusterbasis(h);
+    if (rc == H2B_OK) rc = h2b_h2matrix_assemble_col_clusterbasis(h);
+    if (rc == H2B_OK) rc = h2b_h2matrix_assemble_farfield(h);
+  }
+  if (rc == H2B_OK) rc = h2b_h2matrix_assemble_nearfield_pair(V, K);
+  const auto c2 = tick();
+  std::vector<double> gD(nv, 0.0), b(nv, 0.0), u(nv, 0.0), y(nv, 0.0);
+  if (rc == H2B_OK) rc = h2b_project_l2_harmonic_multi(dlp, ns, toff.data(), 1, zs.data(), gD.data());
+  if (rc == H2B_OK) rc = h2b_h2matrix_addeval(1.0, 0.0, K, gD.data(), b.data());
+  const auto c3 = tick();
+  if (rc == H2B_OK && mixed) rc = h2b_h2matrix_make_single(V);
+  std::vector<uint32_t> iters(ns, 0);
+  const h2b_h2matrix *ops[1] = {V};
+  const double coef[2] = {1.0, 0.0};
+  if (rc == H2B_OK)
+    rc = h2b_solve_gmres_batch(1, ops, coef, ns, voff.data(), 1, b.data(), u.data(), d.eps,
+                               d.maxiter, d.kmax, H2B_SOLVE_UNITARY | (mixed ? H2B_SOLVE_MIXED : 0u),
+                               iters.data());
+  const auto c4 = tick();
+  // FP64 residual of every system: y = V u, |b_s - y_s| / |b_s|
+  if (rc == H2B_OK) rc = h2b_h2matrix_addeval(1.0, 0.0, V, u.data(), y.data());
+  if (rc == H2B_OK) {
+    for (uint32_t i = 0; i < ns; i++) {
+      double rr = 0.0, bb = 0.0;
+      for (uint32_t e = voff[i]; e < voff[i + 1]; e++) {
+        rr += (b[e] - y[e]) * (b[e] - y[e]);
+        bb += b[e] * b[e];
+      }
+      Req *q = qs[i];
+      q->solution.assign(u.begin() + voff[i], u.begin() + voff[i + 1]);
+      q->res.iterations = iters[i];
+      q->res.unknowns = voff[i + 1] - voff[i];
+      q->res.rel_residual = bb > 0.0 ? sqrt(rr / bb) : sqrt(rr);
+      q->res.t_setup = secs(c0, c1);
+      q->res.t_assembly = secs(c1, c2);
+      q->res.t_rhs = secs(c2, c3);
+      q->res.t_solve = secs(c3, c4);
+    }
+  }
+  h2b_h2matrix_del(K);
+  h2b_h2matrix_del(V);
+  h2b_tree_del(tr);
+  h2b_bem_del(dlp);
+  h2b_bem_del(slp);
+  h2b_surface_del(s);
+  return rc;
+}
+
+// Most requests one batch may take, and the most triangles of a batch.
+constexpr size_t BATCH_MAX_REQUESTS = 64;
+constexpr uint64_t BATCH_MAX_TRIANGLES = 1u << 20;
+
 void worker_main(h2b_server *sv) {
   if (h2b_device_init(sv->device) != H2B_OK) return;
+  std::vector<Req *> batch;
   while (true) {
     Req *q = nullptr;
     {
@@ -210,21 +319,44 @@ void worker_main(h2b_server *sv) {
       if (sv->stop) return;
       q = sv->queue.front();
       sv->queue.pop_front();
+      batch.assign(1, q);
       sv->reserved += q->est;
+      // continuous batching: queued requests that can share q's operator join it (in arrival
+      // order, while they fit the budget and the batch limits)
+      uint64_t tris = q->desc.triangles;
+      for (auto it = sv->queue.begin(); it != sv->queue.end() && batch.size() < sv->batch_max &&
+                                        batch.size() < BATCH_MAX_REQUESTS;) {
+        Req *r = *it;
+        if (batchable(q, r) && sv->reserved + r->est <= sv->budget &&
+            tris + r->desc.triangles <= BATCH_MAX_TRIANGLES) {
+          batch.push_back(r);
+          sv->reserved += r->est;
+          tris += r->desc.triangles;
+          it = sv->queue.erase(it);
+        } else {
+          ++it;
+        }
+      }
       sv->running++;
-      q->status = 2;
-      q->res.t_start = since(sv);
+      const double t = since(sv);
+      for (Req *r : batch) {
+        r->status = 2;
+        r->res.t_start = t;
+      }
     }
-    const int rc = run_request(q);
+    const int rc = batch.size() > 1 ? run_batch(batch) : run_request(q);
     {
       std::lock_guard<std::mutex> lk(sv->mu);
-      sv->reserved -= q->est;
       sv->running--;
-      sv->done++;
-      q->res.t_done = since(sv);
-      q->res.status = rc;
-      if (rc != H2B_OK) snprintf(q->err, sizeof(q->err), "%s", h2b_last_error());
-      q->status = rc == H2B_OK ? 0 : rc;
+      const double t = since(sv);
+      for (Req *r : batch) {
+        sv->reserved -= r->est;
+        sv->done++;
+        r->res.t_done = t;
+        r->res.status = rc;
+        if (rc != H2B_OK) snprintf(r->err, sizeof(r->err), "%s", h2b_last_error());
+        r->status = rc == H2B_OK ? 0 : rc;
+      }
     }
     sv->cv_done.notify_all();
     sv->cv_work.notify_all();
@@ -306,6 +438,16 @@ extern "C" int h2b_server_wait(h2b_server *sv, int64_t id, double *solution,
   if (rc != 0) h2b_set_error("request %lld: %s", (long long) id, q->err);
   delete q;
   return rc;
+}
+
+extern "C" int h2b_server_set_batching(h2b_server *sv, uint32_t max_requests) {
+  if (!sv || max_requests == 0) {
+    h2b_set_error("h2b_server_set_batching: NULL server or zero requests");
+    return H2B_ERR_ARG;
+  }
+  std::lock_guard<std::mutex> lk(sv->mu);
+  sv->batch_max = max_requests;
+  return H2B_OK;
 }
 
 extern "C" int h2b_server_stats(h2b_server *sv, uint64_t out[4]) {

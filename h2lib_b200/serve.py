@@ -2,7 +2,9 @@
 
 A Server admits Dirichlet BEM solve requests continuously: requests wait in arrival order until
 a worker slot is free and their device-memory estimate fits the HBM budget, then run on their
-own CUDA streams, overlapping on the device with the other running requests.
+own CUDA streams, overlapping on the device with the other running requests.  Queued Laplace
+requests with equal settings are batched: a worker solves them together as one forest H2 matrix
+with a batched GMRES (each request keeps its own Krylov space and stop).
 """
 import ctypes as C
 
@@ -29,8 +31,11 @@ class Result(C.Structure):
 
 
 class Server:
-    def __init__(self, slots=8, hbm_budget=150 << 30, device=0):
+    def __init__(self, slots=8, hbm_budget=150 << 30, device=0, batching=64):
+        """batching: most queued Laplace requests with equal settings one worker solves together
+        (one forest H2 matrix, one batched GMRES); 1 solves every request alone."""
         self.handle = checkp(lib.h2b_server_new(device, slots, hbm_budget), "h2b_server_new")
+        check(lib.h2b_server_set_batching(self.handle, batching), "server_set_batching")
         self._sizes = {}
 
     def submit(self, gr, pde, src, k=0.0, eps=1e-8, maxiter=1000, kmax=None, mixed=False):

@@ -434,6 +434,10 @@ int64_t h2b_server_submit(h2b_server *server, const h2b_request *request);
 int h2b_server_wait(h2b_server *server, int64_t id, double *solution, h2b_request_result *res);
 /* queued, running, completed requests and reserved bytes */
 int h2b_server_stats(h2b_server *server, uint64_t out[4]);
+/* Continuous batching: a worker takes up to max_requests queued requests that can share one
+ * operator (Laplace problems with equal flags, eps, maxiter and kmax) and solves them as one
+ * forest H2 matrix with a batched GMRES (default 64; 1 solves every request alone). */
+int h2b_server_set_batching(h2b_server *server, uint32_t max_requests);
 /* Finish running requests, drop queued ones, stop the workers. */
 void h2b_server_del(h2b_server *server);
 

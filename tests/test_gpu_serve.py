@@ -99,3 +99,27 @@ def test_tiny_budget_serialises():
     for (s0, e0), (s1, e1) in zip(spans, spans[1:]):
         assert s1 >= e0 - 1e-6
     assert all(r["rel_residual"] <= 1.05e-8 for r in res)
+
+
+def test_batched_requests_match_alone():
+    """Laplace requests queued behind a running one are solved as one batch (forest H2 matrix,
+    batched GMRES): each result matches the request solved alone through the direct API."""
+    gh = hb.new_cube_surface3d(6)
+    gs = [hb.new_sphere_surface3d(10), hb.new_ellipsoid_surface3d(8, (1.4, 0.9, 1.1)),
+          hb.new_cube_surface3d(5)]
+    zs = [(1.2, 1.2, 1.2), (0.0, 3.0, 0.5), (2.5, -2.5, 1.0)]
+    srv = Server(slots=1)
+    try:
+        first = srv.submit(gh, HELMHOLTZ, D, k=2.0)  # keeps the only worker busy meanwhile
+        ids = [srv.submit(g, LAPLACE, z) for g, z in zip(gs, zs)]
+        srv.wait(first)
+        out = [srv.wait(i) for i in ids]
+    finally:
+        srv.close()
+    starts = {r["t_start"] for _, r in out}
+    assert len(starts) == 1  # one admission took all three
+    for (sol, res), g, z in zip(out, gs, zs):
+        u, it = direct_laplace(g, z)
+        assert res["status"] == 0 and res["rel_residual"] <= 1.05e-8
+        assert abs(int(res["iterations"]) - it) <= 1
+        assert relerr(sol, u) < 1e-6
