@@ -39,10 +39,10 @@ FLOPS_PER_POINT = {"slp": 64, "dlp": 72}
 # column weights per channel 12) + 4 row points x 53 (x_a 12, <x_a, n> 5, 3 x 3 x 2 outer FMAs
 # 36) + 4 column points x 17 (y_b 12, <y_b, n> 5) + 20 for the scaling
 EXECUTED_FLOPS_PER_PAIR = 16 * 37 + 4 * 53 + 4 * 17 + 20
-# DRAM bytes (read 6,076,416 + write 214,800,128) of one near_dist_kernel launch on the default
+# DRAM bytes (read 5,998,336 + write 214,822,656) of one near_dist_kernel launch on the default
 # workload (sphere split 64), from an ncu capture of the full-size run (single-pass metrics
 # dram__bytes_read.sum + dram__bytes_write.sum)
-NEAR_DIST_TRAFFIC = 6076416 + 214800128
+NEAR_DIST_TRAFFIC = 5998336 + 214822656
 
 
 def parse():
