@@ -43,7 +43,7 @@ struct FarCouplingArgs {
 };
 
 // Flattened bases (flatbasis.cu): items of at most H2B_FLAT_ROWS rows of one son.
-#define H2B_FLAT_ROWS 64
+#define H2B_FLAT_ROWS 16
 struct FlatArgs {
   const uint32_t *items;     // 4 per item: father, son, first row in the son, rows
   const uint32_t *off, *size;

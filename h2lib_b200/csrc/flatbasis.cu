@@ -41,11 +41,11 @@ __device__ __forceinline__ void cta_copy(double *dst, size_t n, F src) {
 }
 
 // CTA (item, part): item = (father f, son s, first row r0 of s, rows nr <= H2B_FLAT_ROWS), part =
-// FLAT_COLS consecutive columns nu of the product; the nr rows of W_s times those columns of E_s
-// land in the rows of s inside W_f.  Splitting the columns over several CTAs gives every level's
-// launch enough CTAs (a level has few items near the root) and keeps each CTA's shared memory
-// small; the son's rows are read by each part (from L2).
-constexpr int FLAT_COLS = 16;
+// up to FLAT_COLS consecutive columns nu of the product (one part for k <= 64); the nr rows of
+// W_s times those columns of E_s land in the rows of s inside W_f.  Short row slices give every
+// level's launch enough CTAs and read each son's rows once; E_s is read by every slice of the son
+// (from L2).
+constexpr int FLAT_COLS = 64;
 __global__ void __launch_bounds__(FLAT_TPB) flatten_kernel(FlatArgs a) {
   extern __shared__ double sm[];
   const uint32_t k = (uint32_t) a.k;
@@ -84,8 +84,10 @@ __global__ void __launch_bounds__(FLAT_TPB) flatten_kernel(FlatArgs a) {
     }
   }
   __syncthreads();
-  // thread: row i = t % 64 (<= H2B_FLAT_ROWS = 64 rows), columns j = 4 (t / 64) .. + 3
-  const uint32_t i = threadIdx.x % 64, jq = 4 * (threadIdx.x / 64);
+  // thread: row i = t % H2B_FLAT_ROWS, columns j = 4 (t / H2B_FLAT_ROWS) .. + 3 (256 threads
+  // cover 16 rows x 64 columns)
+  static_assert(FLAT_TPB / H2B_FLAT_ROWS * 4 == FLAT_COLS, "thread mapping");
+  const uint32_t i = threadIdx.x % H2B_FLAT_ROWS, jq = 4 * (threadIdx.x / H2B_FLAT_ROWS);
   const uint32_t si = a.transposed ? i * (k + 1) : i, smu = a.transposed ? 1 : nr;
   if (i < nr && jq < nc) {
     double acc[4] = {0.0, 0.0, 0.0, 0.0};
