@@ -95,16 +95,41 @@ __global__ void __launch_bounds__(256) leaf_basis_kernel(FarLeafArgs a) {
     wbar[d][mu] = 1.0 / p;
   }
 
+  // the rule's weights, and per batch the triangles' vertices, normals, Gram determinants and
+  // local rows, are staged in shared memory (the loops below then read no global memory)
+  __shared__ double sw[4][NSMAX];          // rows 0..2 linear-basis weighted, 3 raw
+  __shared__ double sx[NSMAX], sy[NSMAX];
+  __shared__ double tv[BATCH][9], tn[BATCH][3], tg[BATCH];
+  __shared__ int tl[BATCH][3];
+  for (int q = (int) threadIdx.x; q < ns; q += (int) blockDim.x) {
+    sx[q] = a.xs[q];
+    sy[q] = a.ys[q];
+    sw[3][q] = a.ws[q];
+    if (LINEAR)
+      for (int l = 0; l < 3; l++) sw[l][q] = a.wsl[l * ns + q];
+  }
   for (uint32_t b0 = 0; b0 < ntr; b0 += BATCH) {
     const uint32_t nb = ntr - b0 < (uint32_t) BATCH ? ntr - b0 : (uint32_t) BATCH;
+    __syncthreads();
+    for (uint32_t e = threadIdx.x; e < nb; e += blockDim.x) {
+      const TriRef r = a.refs[tr0 + b0 + e];
+      const TriRec &T = a.tri[r.t];
+      for (int d = 0; d < 3; d++) {
+        tv[e][d] = T.a[d];
+        tv[e][3 + d] = T.b[d];
+        tv[e][6 + d] = T.c[d];
+        tn[e][d] = T.n[d];
+        tl[e][d] = r.l[d];
+      }
+      tg[e] = T.g;
+    }
     __syncthreads();
     // table: entry ((s * ns + q) * 3 + d) * m + mu
     for (uint32_t e = threadIdx.x; e < nb * ns * 3 * m; e += blockDim.x) {
       const int mu = (int) (e % m), d = (int) ((e / m) % 3);
       const uint32_t sq = e / (3 * m), s = sq / ns, q = sq % ns;
-      const TriRec &T = a.tri[a.refs[tr0 + b0 + s].t];
-      const double tx = a.xs[q], sx = a.ys[q];
-      const double x = T.a[d] * (1.0 - tx) + T.b[d] * (tx - sx) + T.c[d] * sx;
+      const double tx = sx[q], sy_ = sy[q];
+      const double x = tv[s][d] * (1.0 - tx) + tv[s][3 + d] * (tx - sy_) + tv[s][6 + d] * sy_;
       const double *xi = pts + d * m;
       tab[e] = lagr_bar(x, xi, wbar[d][mu], mu, m);
       if (DN) dtab[e] = dlagr_bar(x, xi, wbar[d][mu], mu, m);
@@ -115,8 +140,6 @@ __global__ void __launch_bounds__(256) leaf_basis_kernel(FarLeafArgs a) {
       const uint32_t s = it / (uint32_t) kp;
       const int lnu = (int) (it - s * (uint32_t) kp), nu = nu0 + lnu;
       const int jx = nu / (m * m), jy = (nu / m) % m, jz = nu % m;
-      const TriRef r = a.refs[tr0 + b0 + s];
-      const TriRec &T = a.tri[r.t];
       double sum[3] = {0.0, 0.0, 0.0};
       for (int q = 0; q < ns; q++) {
         const double *t3 = tab + ((size_t) s * ns + q) * 3 * m;
@@ -126,24 +149,24 @@ __global__ void __launch_bounds__(256) leaf_basis_kernel(FarLeafArgs a) {
           val = lx * ly * lz;
         } else {
           const double *d3 = dtab + ((size_t) s * ns + q) * 3 * m;
-          val = T.n[0] * (d3[jx] * ly * lz) + T.n[1] * (lx * d3[m + jy] * lz) +
-                T.n[2] * (lx * ly * d3[2 * m + jz]);
+          val = tn[s][0] * (d3[jx] * ly * lz) + tn[s][1] * (lx * d3[m + jy] * lz) +
+                tn[s][2] * (lx * ly * d3[2 * m + jz]);
         }
         if (LINEAR) {
 #pragma unroll
-          for (int l = 0; l < 3; l++) sum[l] += a.wsl[l * ns + q] * val;
+          for (int l = 0; l < 3; l++) sum[l] += sw[l][q] * val;
         } else {
-          sum[0] += a.ws[q] * val;
+          sum[0] += sw[3][q] * val;
         }
       }
       if (LINEAR) {
 #pragma unroll
         for (int l = 0; l < 3; l++) {
-          const int row = r.l[l];
-          if (row >= 0) atomicAdd(&V[row + (uint32_t) lnu * rows], sum[l] * T.g);
+          const int row = tl[s][l];
+          if (row >= 0) atomicAdd(&V[row + (uint32_t) lnu * rows], sum[l] * tg[s]);
         }
       } else {
-        V[r.l[0] + (uint32_t) lnu * rows] = T.g * sum[0];
+        V[tl[s][0] + (uint32_t) lnu * rows] = tg[s] * sum[0];
       }
     }
   }

@@ -70,11 +70,11 @@ __global__ void __launch_bounds__(FLAT_TPB) flatten_kernel(FlatArgs a) {
       return Ws[r0 + i + (size_t) mu * ns];
     });
   } else {
-    // E_s^T column-major (k x k): E_s[mu, nu] = E^T[nu + mu k]; read the part's rows of each
-    // column of E^T contiguously
+    // E_s^T column-major (k x k): E_s[mu, nu] = E^T[nu + mu k]; the part's rows of each column
+    // of E^T, kept nu-major: sE[j + mu nc] = E_s[mu, c0 + j]
     for (uint32_t e = threadIdx.x; e < k * nc; e += blockDim.x) {
       const uint32_t j = e % nc, mu = e / nc;
-      sE[mu + j * k] = E[c0 + j + (size_t) mu * k];
+      sE[j + mu * nc] = E[c0 + j + (size_t) mu * k];
     }
     // W_s^T (k x |s|, ld k) is contiguous over the item's rows: sW[mu + i (k + 1)] (padded
     // stride, so that a warp's rows fall in different banks)
@@ -84,26 +84,41 @@ __global__ void __launch_bounds__(FLAT_TPB) flatten_kernel(FlatArgs a) {
     }
   }
   __syncthreads();
-  // thread: row i = t % H2B_FLAT_ROWS, columns j = 4 (t / H2B_FLAT_ROWS) .. + 3 (256 threads
-  // cover 16 rows x 64 columns)
   static_assert(FLAT_TPB / H2B_FLAT_ROWS * 4 == FLAT_COLS, "thread mapping");
-  const uint32_t i = threadIdx.x % H2B_FLAT_ROWS, jq = 4 * (threadIdx.x / H2B_FLAT_ROWS);
-  const uint32_t si = a.transposed ? i * (k + 1) : i, smu = a.transposed ? 1 : nr;
-  if (i < nr && jq < nc) {
-    double acc[4] = {0.0, 0.0, 0.0, 0.0};
-    for (uint32_t mu = 0; mu < k; mu++) {
-      const double x = sW[si + mu * smu];
+  static_assert(FLAT_TPB / FLAT_COLS * 4 == H2B_FLAT_ROWS, "thread mapping");
+  if (!a.transposed) {
+    // row side: thread = row i = t % 16, columns 4 (t / 16) .. + 3; a warp writes 16
+    // consecutive rows of four columns
+    const uint32_t i = threadIdx.x % H2B_FLAT_ROWS, jq = 4 * (threadIdx.x / H2B_FLAT_ROWS);
+    if (i < nr && jq < nc) {
+      double acc[4] = {0.0, 0.0, 0.0, 0.0};
+      for (uint32_t mu = 0; mu < k; mu++) {
+        const double x = sW[i + mu * nr];
 #pragma unroll
-      for (int q = 0; q < 4; q++) acc[q] = fma(x, sE[mu + (jq + q) * k], acc[q]);
+        for (int q = 0; q < 4; q++) acc[q] = fma(x, sE[mu + (jq + q) * k], acc[q]);
+      }
+#pragma unroll
+      for (int q = 0; q < 4; q++)
+        if (jq + q < nc) Wf[rf + i + (size_t) (c0 + jq + q) * nf] = acc[q];
     }
+  } else {
+    // column side (W^T stored k x |t|): thread = column j = t % 64, rows ig + 4 r (ig = t / 64,
+    // r < 4); a warp writes 32 consecutive nu of one row
+    const uint32_t j = threadIdx.x % FLAT_COLS, ig = threadIdx.x / FLAT_COLS;
+    if (j < nc) {
+      double acc[4] = {0.0, 0.0, 0.0, 0.0};
+      for (uint32_t mu = 0; mu < k; mu++) {
+        const double y = sE[j + mu * nc];
 #pragma unroll
-    for (int q = 0; q < 4; q++) {
-      const uint32_t nu = c0 + jq + q;
-      if (jq + q < nc) {
-        if (a.transposed)
-          Wf[(size_t) (rf + i) * k + nu] = acc[q];
-        else
-          Wf[rf + i + (size_t) nu * nf] = acc[q];
+        for (int r = 0; r < 4; r++) {
+          const uint32_t i = ig + 4u * r;
+          if (i < nr) acc[r] = fma(sW[mu + i * (k + 1)], y, acc[r]);
+        }
+      }
+#pragma unroll
+      for (int r = 0; r < 4; r++) {
+        const uint32_t i = ig + 4u * r;
+        if (i < nr) Wf[(size_t) (rf + i) * k + c0 + j] = acc[r];
       }
     }
   }
