@@ -321,6 +321,7 @@ void h2b_fill_launch(const h2b_bem *b, h2b_near_launch *L) {
   L->vert_tensor = b->vert_tensor;
   L->num_sms = b->s->num_sms;
   L->err = b->d_err;
+  L->nvert = UINT32_MAX;
 }
 
 uint32_t h2b_bem_rows(const h2b_bem *b) {
@@ -335,6 +336,7 @@ int h2b_devplan_upload(const h2b_nearplan *p, cudaStream_t st, h2b_devplan *dp) 
   memset(dp, 0, sizeof(*dp));
   dp->ntiles = p->ntiles;
   dp->nsing = p->nsing;
+  dp->nvert = p->nsing ? p->case_start[2] - p->case_start[1] : 0;
   if (p->ntiles) {
     H2B_CUDA_TRY(cudaMallocAsync(&dp->tiles, sizeof(h2b_tile) * p->ntiles, st));
     H2B_CUDA_TRY(cudaMemcpyAsync(dp->tiles, p->tiles, sizeof(h2b_tile) * p->ntiles,
@@ -466,6 +468,7 @@ extern "C" int h2b_bem_nearfield(const h2b_bem *bem, const uint32_t *ridx, uint3
   L.ntiles = dp.ntiles;
   L.sing = dp.sing;
   L.nsing = dp.nsing;
+  L.nvert = dp.nvert;
   L.out0 = out;
   rc = h2b_near_launch_kernels(&L, st);
   if (rc == H2B_OK && !dev_out) {

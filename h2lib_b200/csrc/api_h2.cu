@@ -684,6 +684,7 @@ static int launch_near(h2b_h2matrix *h, h2b_h2matrix *h2) {
   L.ntiles = h->ntiles;
   L.sing = h->d_sing;
   L.nsing = h->nsing;
+  L.nvert = h->pairs[1];
   L.out0 = h->d_N;
   L.ev_between = h->ev[7];
   L.fp32 = h->quad_fp32;

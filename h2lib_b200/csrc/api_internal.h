@@ -41,6 +41,7 @@ struct h2b_devplan {
   h2b_triref *refs;
   h2b_sing *sing;
   uint32_t ntiles, nsing;
+  uint32_t nvert;  // common-vertex pairs at the start of sing (the plan sorts them by case)
 };
 
 int h2b_ensure_device(void);

@@ -216,6 +216,10 @@ __device__ __forceinline__ void quad_point_red(const PairGeo &g, double ra, doub
 // first in both triangles, X_a - Y_b = (d0 + x0 p1 + x1 p2) - (y0 q1 + y1 q2).  `t` is the
 // packed group arrays (gn groups each), the row weights include the group weight.
 constexpr int VT_Q = 4;
+#ifndef H2B_VT_UNROLL
+#define H2B_VT_UNROLL 4
+#endif
+constexpr int VT_UNROLL = H2B_VT_UNROLL;  // column points per unrolled step
 template <int KK, bool RL, bool CL>
 __device__ __forceinline__ void vert_group_tensor(const PairGeo &g, const double *t, uint32_t gn,
                                                   uint32_t grp, double n0, double n1, double n2,
@@ -236,7 +240,7 @@ __device__ __forceinline__ void vert_group_tensor(const PairGeo &g, const double
     for (int c = 0; c < NCH; c++)
 #pragma unroll
       for (int j = 0; j < NC; j++) in[c][j] = 0.0;
-#pragma unroll
+#pragma unroll VT_UNROLL
     for (int b = 0; b < VT_Q; b++) {
       // column point formed here rather than kept for all a (register budget of 128)
       const double *cp = col + (size_t) b * (2 + NC) * gn + grp;
@@ -732,7 +736,10 @@ constexpr int SING_UNROLL = H2B_SING_UNROLL;
 // One warp per singular pair.  The three rules are copied into shared memory once per CTA.
 // 512 threads: one CTA per SM holds the staged rules, 16 warps hide the FP64 latencies.
 constexpr int SING_THREADS = 512;
-template <int KK, bool RL, bool CL>
+// PART selects the pairs a launch takes and so the code it carries (fewer live registers per
+// launch): 0 every case, 1 common vertex in tensor form, 2 common edge / identical (reduced
+// rules), 3 common vertex with the full rule.  `a.sing` / `a.nsing` are the launch's pairs.
+template <int KK, bool RL, bool CL, int PART>
 __global__ void __launch_bounds__(SING_THREADS, 1) near_sing_kernel(SingArgs a) {
   constexpr int NCH = KT<KK>::NCH;
   constexpr int NR = RL ? 3 : 1, NC = CL ? 3 : 1;
@@ -809,18 +816,18 @@ __global__ void __launch_bounds__(SING_THREADS, 1) near_sing_kernel(SingArgs a) 
       for (int i = 0; i < NR; i++)
 #pragma unroll
         for (int j = 0; j < NC; j++) acc[c][i][j] = 0.0;
-    if (cs == 1u && a.vert_tensor) {
+    if ((PART == 0 || PART == 1) && cs == 1u && (PART == 1 || a.vert_tensor)) {
       // common vertex, tensor form: a group of VT_Q x VT_Q points per lane
       for (uint32_t grp = lane; grp < n; grp += 32)
         vert_group_tensor<KK, RL, CL>(g, rx0, n, grp, n0, n1, n2, a.k_re, a.k_imn, acc);
-    } else if (cs == 1u) {
+    } else if ((PART == 0 || PART == 3) && cs == 1u) {
       // common vertex: the full rule (x0, x1, y0, y1, raw weight)
       const double *rx1 = rx0 + n, *ry0 = rx0 + 2 * n, *ry1 = rx0 + 3 * n, *rw = rx0 + 4 * n;
 #pragma unroll SING_UNROLL
       for (uint32_t k = lane; k < n; k += 32)
         quad_point<KK, RL, CL>(g, rx0[k], rx1[k], ry0[k], ry1[k], rw[k], n0, n1, n2, a.k_re,
                                a.k_imn, acc);
-    } else {
+    } else if (PART == 0 || PART == 2) {
       // common edge / identical: the reduced rule (a, b, c, basis-weighted weights)
       const double *rb = rx0 + n, *rc = rx0 + 2 * n, *rwt = rx0 + 3 * n;
 #pragma unroll SING_UNROLL
@@ -922,18 +929,18 @@ int launch_dist(const h2b_near_launch *L, cudaStream_t st) {
   return H2B_OK;
 }
 
-template <int KK, bool RL, bool CL>
-int launch_sing(const h2b_near_launch *L, cudaStream_t st) {
-  if (L->nsing == 0) return H2B_OK;
+template <int KK, bool RL, bool CL, int PART>
+int launch_sing_part(const h2b_near_launch *L, uint32_t first, uint32_t count, cudaStream_t st) {
+  if (count == 0) return H2B_OK;
   const int staged = sizeof(double) * L->rule_total <= 200u * 1024u;
   const size_t smem = staged ? sizeof(double) * L->rule_total : 0;
-  H2B_CUDA_TRY((h2b_allow_smem<near_sing_kernel<KK, RL, CL>>()));
+  H2B_CUDA_TRY((h2b_allow_smem<near_sing_kernel<KK, RL, CL, PART>>()));
   SingArgs a;
   a.tri = (const TriRec *) L->tri;
   a.refs = (const TriRef *) L->refs;
   a.tiles = L->tiles;
-  a.sing = L->sing;
-  a.nsing = L->nsing;
+  a.sing = L->sing + first;
+  a.nsing = count;
   a.out0 = L->out0;
   a.out1 = L->out1;
   a.kconst = L->kconst;
@@ -953,11 +960,24 @@ int launch_sing(const h2b_near_launch *L, cudaStream_t st) {
   a.err = L->err;
   int sms = L->num_sms > 0 ? L->num_sms : 148;
   const uint32_t wpc = SING_THREADS / 32;
-  uint32_t want = (L->nsing + wpc - 1) / wpc;
+  uint32_t want = (count + wpc - 1) / wpc;
   uint32_t grid = want < (uint32_t) sms ? want : (uint32_t) sms;
-  near_sing_kernel<KK, RL, CL><<<grid, SING_THREADS, smem, st>>>(a);
+  near_sing_kernel<KK, RL, CL, PART><<<grid, SING_THREADS, smem, st>>>(a);
   H2B_CUDA_TRY(cudaGetLastError());
   return H2B_OK;
+}
+
+// The singular pairs are sorted by case (common vertex first).  When the number of vertex pairs
+// is known, the vertex pairs and the edge / identical pairs run as two launches of specialised
+// kernels; otherwise one launch handles every case.
+template <int KK, bool RL, bool CL>
+int launch_sing(const h2b_near_launch *L, cudaStream_t st) {
+  if (L->nsing == 0) return H2B_OK;
+  if (L->nvert > L->nsing) return launch_sing_part<KK, RL, CL, 0>(L, 0, L->nsing, st);
+  const int rc = L->vert_tensor ? launch_sing_part<KK, RL, CL, 1>(L, 0, L->nvert, st)
+                                : launch_sing_part<KK, RL, CL, 3>(L, 0, L->nvert, st);
+  if (rc != H2B_OK) return rc;
+  return launch_sing_part<KK, RL, CL, 2>(L, L->nvert, L->nsing - L->nvert, st);
 }
 
 template <int KK, bool RL, bool CL>

@@ -30,6 +30,7 @@ typedef struct {
   uint32_t ntiles;
   const h2b_sing *sing;          /* sorted by case */
   uint32_t nsing;
+  uint32_t nvert;                /* vertex pairs at the start of sing (UINT32_MAX: not known) */
   double *out0, *out1;           /* out1: double-layer output of H2B_KK_LBOTH */
   double kconst, k_re, k_imn;    /* 1/(4 pi); Re k; -Im k */
   double alpha_re, alpha_im;     /* identity coefficient of the double layer output */
