@@ -268,6 +268,22 @@ extern "C" h2b_bem *h2b_bem_new(const h2b_surface *s, int pde, int layer, int ro
     // offsets inside the block are multiples of n; keep n even by padding the whole block
     if (pack.size() & 1) pack.push_back(0.0);
   }
+  if (q_singular == 4) {
+    // slot 4: the common-vertex rule with the radial sum folded into moments
+    // (h2b_quad_vert_merged), used for the Laplace kernels
+    uint32_t nm = 0;
+    double *t = nullptr;
+    if (h2b_quad_vert_merged(q_singular, row_basis, col_basis, &nm, &t) != H2B_OK) {
+      h2b_bem_del(b);
+      return NULL;
+    }
+    b->rule_off[4] = (uint32_t) pack.size();
+    b->rule_n[4] = nm;
+    b->vert_merged = 1;
+    pack.insert(pack.end(), t, t + (size_t) (4 + 2 * NR + 4 * NC) * nm);
+    free(t);
+    if (pack.size() & 1) pack.push_back(0.0);
+  }
   // every field must start on a 16-byte boundary: n is a multiple of 2 (2 q2^4 and 6 q2^4)
   b->rule_total = (uint32_t) pack.size();
   cudaStream_t st = b->s->stream;
@@ -313,12 +329,13 @@ void h2b_fill_launch(const h2b_bem *b, h2b_near_launch *L) {
   L->alpha_im = b->alpha_im;
   for (int i = 0; i < 9; i++) L->mass[i] = b->mass[i];
   L->rule = b->d_rule;
-  for (int i = 0; i < 4; i++) {
+  for (int i = 0; i < 5; i++) {
     L->rule_n[i] = b->rule_n[i];
     L->rule_off[i] = b->rule_off[i];
   }
   L->rule_total = b->rule_total;
   L->vert_tensor = b->vert_tensor;
+  L->vert_merged = b->vert_merged;
   L->num_sms = b->s->num_sms;
   L->err = b->d_err;
   L->nvert = UINT32_MAX;

@@ -31,7 +31,8 @@ struct h2b_bem {
   double mass[9];
   h2b_quad quad{};
   double *d_rule = nullptr;
-  uint32_t rule_n[4], rule_off[4], rule_total = 0;
+  uint32_t rule_n[5] = {0, 0, 0, 0, 0}, rule_off[5] = {0, 0, 0, 0, 0}, rule_total = 0;
+  int vert_merged = 0;  // 1: slot 4 holds h2b_quad_vert_merged's rule (q_singular == 4)
   int vert_tensor = 0;  // 1: the common-vertex rule is packed in tensor form (q_singular == 4)
   int *d_err = nullptr;
 };

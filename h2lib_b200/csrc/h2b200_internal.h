@@ -45,6 +45,10 @@ int h2b_quad_reduce(const h2b_rule *r, int which, uint32_t q2, uint32_t *n_out, 
 /* Common-vertex rule in tensor form: 2 q2^2 groups of q2 row points x q2 column points. */
 int h2b_quad_vert_tensor(uint32_t q2, int row_basis, int col_basis, uint32_t *ngroups,
                          double **out);
+/* Common-vertex rule with the radial sum folded into moments (kernels homogeneous of degree -1
+ * or -2): 2 q2^2 items of one row point and q2 column points each. */
+int h2b_quad_vert_merged(uint32_t q2, int row_basis, int col_basis, uint32_t *n_out,
+                         double **out);
 
 /* ---------------- cluster / block trees (host) ---------------- */
 

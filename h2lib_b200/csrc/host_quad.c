@@ -357,6 +357,81 @@ h2b_quad_vert_tensor(uint32_t q2, int row_basis, int col_basis, uint32_t *ngroup
   return H2B_OK;
 }
 
+/* Common-vertex rule with the radial Gauss sum folded into moments (Laplace kernels only).  In
+ * h2b_quad_vert_tensor every row and column point of group (i, l, s) is xi = g[l] times a point
+ * that does not depend on l: x = xi xh, y = xi yh.  With the shared vertex first in both
+ * triangles, x - y = xi (xh - yh), so a kernel homogeneous of degree -p (p = 1 single layer,
+ * p = 2 double layer and its adjoint) gives k(x - y) = xi^-p k(xh - yh), and the linear basis
+ * functions are affine in xi: phi(xi xh) = phi(0) + xi (phi(xh) - phi(0)).  The sum over l then
+ * needs only the moments M_e = sum_l gw[l] g[l]^e:
+ *   sum_l gw[l] xi^(3-p) phi_r(xi xh) phi_c(xi yh)
+ *     = phi_r0 phi_c0 M_(3-p) + (phi_r0 C + R phi_c0) M_(4-p) + R C M_(5-p),
+ * R = phi_r(xh) - phi_r0, C = phi_c(yh) - phi_c0: one kernel evaluation per (i, s, a, b) instead
+ * of q2 of them.  Same quadrature sum as the point rule, in another order.
+ * Output: n = 2 q2^2 items k = (i 2 + s) q2 + a, arrays of n doubles each:
+ *   row point a of group (i, s):    xh0, xh1, U_r (NR), V_r (NR)
+ *       U_r = gw[i] eta1 gw[a] phi_r0,  V_r = gw[i] eta1 gw[a] R_r
+ *   column point b of group (i, s) (index (i 2 + s) q2 + b):  yh0, yh1, then for p = 1 and p = 2
+ *       A_c = gw[b] (phi_c0 M_(3-p) + C_c M_(4-p)),  B_c = gw[b] (phi_c0 M_(4-p) + C_c M_(5-p))
+ *   (NC each, p = 1 first), i.e. (2 + 2 NR) + (2 + 4 NC) arrays;
+ * the entry sum is  sum over (i, s, a, b) of  k_p(xh - yh) (U_r A_c + V_r B_c). */
+int
+h2b_quad_vert_merged(uint32_t q2, int row_basis, int col_basis, uint32_t *n_out, double **out)
+{
+  double g[64], gw[64], M[6] = {0, 0, 0, 0, 0, 0};
+  const uint32_t NR = row_basis == H2B_BASIS_LINEAR ? 3 : 1, NC = col_basis == H2B_BASIS_LINEAR ? 3 : 1;
+  const uint32_t n = 2 * q2 * q2, rs = 2 + 2 * NR, cs = 2 + 4 * NC;
+  uint32_t i, l, s, a, r, p, e;
+  double *o, *col;
+  *out = NULL;
+  if (h2b_gauss_legendre01(q2, g, gw))
+    return H2B_ERR_ARG;
+  for (e = 0; e < 6; e++)
+    for (l = 0; l < q2; l++) {
+      double pw = 1.0;
+      for (p = 0; p < e; p++)
+        pw *= g[l];
+      M[e] += gw[l] * pw;
+    }
+  o = (double *) calloc((size_t) (rs + cs) * n, sizeof(double));
+  if (!o) {
+    h2b_set_error("h2b_quad_vert_merged: out of host memory");
+    return H2B_ERR_NOMEM;
+  }
+  col = o + (size_t) rs * n;
+  for (i = 0; i < q2; i++)
+    for (s = 0; s < 2; s++) {
+      const double e1 = g[i], wg = gw[i] * e1;
+      for (a = 0; a < q2; a++) {
+        const uint32_t k = (i * 2 + s) * q2 + a;
+        /* (1, eta) and (eta1, eta1 eta): the tensor form's points divided by xi */
+        const double pa0 = 1.0, pa1 = g[a], pb0 = e1, pb1 = e1 * g[a];
+        const double x0 = s == 0 ? pa0 : pb0, x1 = s == 0 ? pa1 : pb1;
+        const double y0 = s == 0 ? pb0 : pa0, y1 = s == 0 ? pb1 : pa1;
+        o[k] = x0;
+        o[n + k] = x1;
+        for (r = 0; r < NR; r++) {
+          const double f0 = nodal(row_basis, (int) r, 0.0, 0.0);
+          o[(2 + r) * (size_t) n + k] = wg * gw[a] * f0;
+          o[(2 + NR + r) * (size_t) n + k] = wg * gw[a] * (nodal(row_basis, (int) r, x0, x1) - f0);
+        }
+        col[k] = y0;
+        col[n + k] = y1;
+        for (p = 1; p <= 2; p++)
+          for (r = 0; r < NC; r++) {
+            const double f0 = nodal(col_basis, (int) r, 0.0, 0.0);
+            const double C = nodal(col_basis, (int) r, y0, y1) - f0;
+            const size_t base = 2 + (p - 1) * 2 * NC;
+            col[(base + r) * n + k] = gw[a] * (f0 * M[3 - p] + C * M[4 - p]);
+            col[(base + NC + r) * n + k] = gw[a] * (f0 * M[4 - p] + C * M[5 - p]);
+          }
+      }
+    }
+  *n_out = n;
+  *out = o;
+  return H2B_OK;
+}
+
 void
 h2b_quad_free(h2b_quad *qd)
 {

@@ -270,6 +270,71 @@ __device__ __forceinline__ void vert_group_tensor(const PairGeo &g, const double
   }
 }
 
+// Laplace kernels are homogeneous in x - y: degree -1 (single layer) or -2 (double layer and
+// its adjoint), per output channel.
+template <int KK>
+__device__ __forceinline__ constexpr bool homogeneous_kk() {
+  return KK == KK_LSLP || KK == KK_LDLP || KK == KK_LBOTH || KK == KK_LADLP;
+}
+template <int KK>
+__device__ __forceinline__ constexpr int kk_degree(int c) {
+  return (KK == KK_LSLP || (KK == KK_LBOTH && c == 0)) ? 1 : 2;
+}
+
+// One item of the merged common-vertex rule (h2b_quad_vert_merged, q2 = VT_Q): row point a of
+// group (i, s) against the group's VT_Q column points.  The points are the tensor form's divided
+// by the radial variable xi; the radial Gauss sum is folded into the column weights, one set per
+// homogeneity degree of the kernel channel, so each point pair needs one kernel evaluation where
+// the tensor form needs VT_Q.  With the shared vertex the origin of both triangles, the scaled
+// difference is xh0 p1 + xh1 p2 - (yh0 q1 + yh1 q2).
+template <int KK, bool RL, bool CL>
+__device__ __forceinline__ void vert_item_merged(const PairGeo &g, const double *t, uint32_t n,
+                                                 uint32_t k, double n0, double n1, double n2,
+                                                 double (&acc)[KT<KK>::NCH][RL ? 3 : 1][CL ? 3 : 1]) {
+  constexpr int NCH = KT<KK>::NCH, NR = RL ? 3 : 1, NC = CL ? 3 : 1;
+  constexpr bool DOT = uses_normal<KK>();
+  const double *col = t + (size_t) (2 + 2 * NR) * n;
+  const uint32_t c0 = (k / VT_Q) * VT_Q;
+  const double x0 = t[k], x1 = t[n + k];
+  double xa[3];
+#pragma unroll
+  for (int d = 0; d < 3; d++) xa[d] = fma(x0, g.p1[d], x1 * g.p2[d]);
+  double in[NCH][2][NC];
+#pragma unroll
+  for (int c = 0; c < NCH; c++)
+#pragma unroll
+    for (int j = 0; j < NC; j++) in[c][0][j] = in[c][1][j] = 0.0;
+#pragma unroll
+  for (int b = 0; b < VT_Q; b++) {
+    const uint32_t cb = c0 + b;
+    const double y0 = col[cb], y1 = col[n + cb];
+    const double dx = xa[0] - fma(y0, g.q1[0], y1 * g.q2[0]);
+    const double dy = xa[1] - fma(y0, g.q1[1], y1 * g.q2[1]);
+    const double dz = xa[2] - fma(y0, g.q1[2], y1 * g.q2[2]);
+    const double r2 = fma(dx, dx, fma(dy, dy, dz * dz));
+    const double dot = DOT ? fma(dx, n0, fma(dy, n1, dz * n2)) : 0.0;
+    double kv[2];
+    eval_kernel<KK>(r2, dot, 0.0, 0.0, kv);
+#pragma unroll
+    for (int c = 0; c < NCH; c++) {
+      const double *wc = col + (size_t) (2 + (kk_degree<KK>(c) - 1) * 2 * NC) * n + cb;
+#pragma unroll
+      for (int j = 0; j < NC; j++) {
+        in[c][0][j] = fma(wc[(size_t) j * n], kv[c], in[c][0][j]);
+        in[c][1][j] = fma(wc[(size_t) (NC + j) * n], kv[c], in[c][1][j]);
+      }
+    }
+  }
+#pragma unroll
+  for (int i = 0; i < NR; i++) {
+    const double u = t[(size_t) (2 + i) * n + k], v = t[(size_t) (2 + NR + i) * n + k];
+#pragma unroll
+    for (int c = 0; c < NCH; c++)
+#pragma unroll
+      for (int j = 0; j < NC; j++) acc[c][i][j] = fma(u, in[c][0][j], fma(v, in[c][1][j], acc[c][i][j]));
+  }
+}
+
 // One distant pair with the q^4 tensor rule, summed column side first:
 //   acc[c][i][j] = sum_a w_a phi_i(x_a) sum_b w_b phi_j(y_b) k_c(x_a, y_b).
 // With X_a = x_a - A_s and Y_b = y_b - A_s the difference is x_a - y_b = X_a - Y_b and the double
@@ -719,8 +784,8 @@ struct SingArgs {
   double mass[9];
   const double *rule;         // packed singular rules: case 1 {x0,x1,y0,y1,w} x n_1, cases 2, 3
                               // {a,b,c, NR*NC weight rows} x n_c (reduced rules)
-  uint32_t rule_n[4];         // points per case (index 1..3)
-  uint32_t rule_off[4];       // offset (in doubles) of each case's block in `rule`
+  uint32_t rule_n[5];         // points per case (index 1..3; 4: merged common-vertex rule)
+  uint32_t rule_off[5];       // offset (in doubles) of each case's block in `rule`
   uint32_t rule_total;        // doubles in `rule` (multiple of 2, 16-byte aligned)
   int vert_tensor;            // 1: case 1 in tensor form (rule_n[1] groups, q2 = 4)
   int staged;                 // 1: copy `rule` into shared memory first
@@ -816,7 +881,12 @@ __global__ void __launch_bounds__(SING_THREADS, 1) near_sing_kernel(SingArgs a) 
       for (int i = 0; i < NR; i++)
 #pragma unroll
         for (int j = 0; j < NC; j++) acc[c][i][j] = 0.0;
-    if ((PART == 0 || PART == 1) && cs == 1u && (PART == 1 || a.vert_tensor)) {
+    if (PART == 4) {
+      // common vertex, Laplace kernel: the merged rule, one row point per lane
+      const double *rm = rules + a.rule_off[4];
+      for (uint32_t k = lane; k < a.rule_n[4]; k += 32)
+        vert_item_merged<KK, RL, CL>(g, rm, a.rule_n[4], k, n0, n1, n2, acc);
+    } else if ((PART == 0 || PART == 1) && cs == 1u && (PART == 1 || a.vert_tensor)) {
       // common vertex, tensor form: a group of VT_Q x VT_Q points per lane
       for (uint32_t grp = lane; grp < n; grp += 32)
         vert_group_tensor<KK, RL, CL>(g, rx0, n, grp, n0, n1, n2, a.k_re, a.k_imn, acc);
@@ -950,7 +1020,7 @@ int launch_sing_part(const h2b_near_launch *L, uint32_t first, uint32_t count, c
   a.alpha_im = L->alpha_im;
   for (int i = 0; i < 9; i++) a.mass[i] = L->mass[i];
   a.rule = L->rule;
-  for (int i = 0; i < 4; i++) {
+  for (int i = 0; i < 5; i++) {
     a.rule_n[i] = L->rule_n[i];
     a.rule_off[i] = L->rule_off[i];
   }
@@ -974,8 +1044,14 @@ template <int KK, bool RL, bool CL>
 int launch_sing(const h2b_near_launch *L, cudaStream_t st) {
   if (L->nsing == 0) return H2B_OK;
   if (L->nvert > L->nsing) return launch_sing_part<KK, RL, CL, 0>(L, 0, L->nsing, st);
-  const int rc = L->vert_tensor ? launch_sing_part<KK, RL, CL, 1>(L, 0, L->nvert, st)
-                                : launch_sing_part<KK, RL, CL, 3>(L, 0, L->nvert, st);
+  int rc;
+  if constexpr (homogeneous_kk<KK>())
+    rc = L->vert_merged   ? launch_sing_part<KK, RL, CL, 4>(L, 0, L->nvert, st)
+         : L->vert_tensor ? launch_sing_part<KK, RL, CL, 1>(L, 0, L->nvert, st)
+                          : launch_sing_part<KK, RL, CL, 3>(L, 0, L->nvert, st);
+  else
+    rc = L->vert_tensor ? launch_sing_part<KK, RL, CL, 1>(L, 0, L->nvert, st)
+                        : launch_sing_part<KK, RL, CL, 3>(L, 0, L->nvert, st);
   if (rc != H2B_OK) return rc;
   return launch_sing_part<KK, RL, CL, 2>(L, L->nvert, L->nsing - L->nvert, st);
 }

@@ -36,8 +36,9 @@ typedef struct {
   double alpha_re, alpha_im;     /* identity coefficient of the double layer output */
   double mass[9];                /* linear-basis mass matrix on the reference triangle */
   const double *rule;            /* packed singular rules (device) */
-  uint32_t rule_n[4], rule_off[4], rule_total;
+  uint32_t rule_n[5], rule_off[5], rule_total;  /* [4]: merged common-vertex rule (or 0) */
   int vert_tensor;               /* 1: common-vertex rule in tensor form (groups in rule_n[1]) */
+  int vert_merged;               /* 1: merged common-vertex rule in slot 4 (items in rule_n[4]) */
   int num_sms;
   int *err;                      /* device flag */
   cudaEvent_t ev_between;        /* optional: recorded between the distant and singular kernels */
