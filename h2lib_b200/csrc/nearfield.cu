@@ -855,9 +855,18 @@ __global__ void __launch_bounds__(SING_THREADS, 1) near_sing_kernel(SingArgs a) 
   const int lane = threadIdx.x & 31;
   const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+  // lanes per pair: a warp per pair, except for the merged vertex rule (32 items of 4 kernel
+  // evaluations each), where 8 lanes take a pair and a warp four pairs: the reduction over the
+  // lanes then takes 3 shuffle steps instead of 5 per value.  A group without a pair of its own
+  // repeats the warp's first pair and writes nothing, so every lane takes part in the shuffles.
+  constexpr int LPP = PART == 4 ? 8 : 32;
+  constexpr uint32_t PPW = 32 / LPP;
+  const int sub = lane % LPP;
 
-  for (uint32_t pi = warp; pi < a.nsing; pi += nwarps) {
-    const h2b_sing sp = a.sing[pi];
+  for (uint32_t base = warp * PPW; base < a.nsing; base += nwarps * PPW) {
+    const uint32_t pi = base + (uint32_t) (lane / LPP);
+    const bool valid = pi < a.nsing;
+    const h2b_sing sp = a.sing[valid ? pi : base];
     const uint32_t cs = sp.code & 3u;
     const int tp[3] = {(int) ((sp.code >> 2) & 3u), (int) ((sp.code >> 4) & 3u),
                        (int) ((sp.code >> 6) & 3u)};
@@ -884,7 +893,7 @@ __global__ void __launch_bounds__(SING_THREADS, 1) near_sing_kernel(SingArgs a) 
     if (PART == 4) {
       // common vertex, Laplace kernel: the merged rule, one row point per lane
       const double *rm = rules + a.rule_off[4];
-      for (uint32_t k = lane; k < a.rule_n[4]; k += 32)
+      for (uint32_t k = sub; k < a.rule_n[4]; k += LPP)
         vert_item_merged<KK, RL, CL>(g, rm, a.rule_n[4], k, n0, n1, n2, acc);
     } else if ((PART == 0 || PART == 1) && cs == 1u && (PART == 1 || a.vert_tensor)) {
       // common vertex, tensor form: a group of VT_Q x VT_Q points per lane
@@ -910,9 +919,13 @@ __global__ void __launch_bounds__(SING_THREADS, 1) near_sing_kernel(SingArgs a) 
 #pragma unroll
       for (int i = 0; i < NR; i++)
 #pragma unroll
-        for (int j = 0; j < NC; j++) acc[c][i][j] = warp_sum(acc[c][i][j]);
+        for (int j = 0; j < NC; j++) {
+#pragma unroll
+          for (int o = LPP / 2; o > 0; o >>= 1)
+            acc[c][i][j] += __shfl_xor_sync(0xffffffffu, acc[c][i][j], o);
+        }
 
-    if (lane == 0) {
+    if (sub == 0 && valid) {
       const h2b_tile tl = a.tiles[sp.tile];
       const bool ntrans = tl.flags & 1u;
       const double f2 = (S.g * a.kconst) * T.g;
