@@ -856,10 +856,11 @@ __global__ void __launch_bounds__(SING_THREADS, 1) near_sing_kernel(SingArgs a) 
   const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
   // lanes per pair: a warp per pair, except for the merged vertex rule (32 items of 4 kernel
-  // evaluations each), where 8 lanes take a pair and a warp four pairs: the reduction over the
-  // lanes then takes 3 shuffle steps instead of 5 per value.  A group without a pair of its own
-  // repeats the warp's first pair and writes nothing, so every lane takes part in the shuffles.
-  constexpr int LPP = PART == 4 ? 8 : 32;
+  // evaluations each) and the reduced edge / identical rules (384 / 96 items), where 8 lanes take
+  // a pair and a warp four pairs: the reduction over the lanes then takes 3 shuffle steps
+  // instead of 5 per value.  A group without a pair of its own repeats the warp's first pair and
+  // writes nothing, so every lane takes part in the shuffles.
+  constexpr int LPP = (PART == 4 || PART == 2) ? 8 : 32;
   constexpr uint32_t PPW = 32 / LPP;
   const int sub = lane % LPP;
 
@@ -910,7 +911,7 @@ __global__ void __launch_bounds__(SING_THREADS, 1) near_sing_kernel(SingArgs a) 
       // common edge / identical: the reduced rule (a, b, c, basis-weighted weights)
       const double *rb = rx0 + n, *rc = rx0 + 2 * n, *rwt = rx0 + 3 * n;
 #pragma unroll SING_UNROLL
-      for (uint32_t k = lane; k < n; k += 32)
+      for (uint32_t k = sub; k < n; k += LPP)
         quad_point_red<KK, RL, CL>(g, rx0[k], rb[k], rc[k], rwt + k, n, n0, n1, n2, a.k_re,
                                    a.k_imn, acc);
     }
