@@ -84,39 +84,60 @@ __global__ void __launch_bounds__(FLAT_TPB) flatten_kernel(FlatArgs a) {
     }
   }
   __syncthreads();
-  static_assert(FLAT_TPB / H2B_FLAT_ROWS * 4 == FLAT_COLS, "thread mapping");
-  static_assert(FLAT_TPB / FLAT_COLS * 4 == H2B_FLAT_ROWS, "thread mapping");
+  // row side: 16 row lanes x 16 column quads; column side: 64 column lanes x 4 row groups
+  static_assert(FLAT_TPB / 16 * 4 == FLAT_COLS && H2B_FLAT_ROWS % 16 == 0, "thread mapping");
+  static_assert(FLAT_TPB / FLAT_COLS == 4 && H2B_FLAT_ROWS % 4 == 0, "thread mapping");
   if (!a.transposed) {
-    // row side: thread = row i = t % 16, columns 4 (t / 16) .. + 3; a warp writes 16
-    // consecutive rows of four columns
-    const uint32_t i = threadIdx.x % H2B_FLAT_ROWS, jq = 4 * (threadIdx.x / H2B_FLAT_ROWS);
-    if (i < nr && jq < nc) {
-      double acc[4] = {0.0, 0.0, 0.0, 0.0};
-      for (uint32_t mu = 0; mu < k; mu++) {
-        const double x = sW[i + mu * nr];
+    // row side: thread = rows i0 + 16 r (i0 = t % 16), columns 4 (t / 16) .. + 3; a warp
+    // writes 16 consecutive rows of four columns per store
+    constexpr int RS = H2B_FLAT_ROWS / 16;
+    const uint32_t i0 = threadIdx.x % 16, jq = 4 * (threadIdx.x / 16);
+    if (i0 < nr && jq < nc) {
+      double acc[RS][4];
 #pragma unroll
-        for (int q = 0; q < 4; q++) acc[q] = fma(x, sE[mu + (jq + q) * k], acc[q]);
+      for (int r = 0; r < RS; r++)
+#pragma unroll
+        for (int q = 0; q < 4; q++) acc[r][q] = 0.0;
+      for (uint32_t mu = 0; mu < k; mu++) {
+        double e[4];
+#pragma unroll
+        for (int q = 0; q < 4; q++) e[q] = sE[mu + (jq + q) * k];
+#pragma unroll
+        for (int r = 0; r < RS; r++) {
+          const uint32_t i = i0 + 16u * r;
+          const double x = i < nr ? sW[i + mu * nr] : 0.0;
+#pragma unroll
+          for (int q = 0; q < 4; q++) acc[r][q] = fma(x, e[q], acc[r][q]);
+        }
       }
 #pragma unroll
-      for (int q = 0; q < 4; q++)
-        if (jq + q < nc) Wf[rf + i + (size_t) (c0 + jq + q) * nf] = acc[q];
+      for (int r = 0; r < RS; r++) {
+        const uint32_t i = i0 + 16u * r;
+        if (i < nr)
+#pragma unroll
+          for (int q = 0; q < 4; q++)
+            if (jq + q < nc) Wf[rf + i + (size_t) (c0 + jq + q) * nf] = acc[r][q];
+      }
     }
   } else {
-    // column side (W^T stored k x |t|): thread = column j = t % 64, rows ig + 4 r (ig = t / 64,
-    // r < 4); a warp writes 32 consecutive nu of one row
+    // column side (W^T stored k x |t|): thread = column j = t % 64, rows ig + 4 r (ig = t / 64);
+    // a warp writes 32 consecutive nu of one row
+    constexpr int RC = H2B_FLAT_ROWS / 4;
     const uint32_t j = threadIdx.x % FLAT_COLS, ig = threadIdx.x / FLAT_COLS;
     if (j < nc) {
-      double acc[4] = {0.0, 0.0, 0.0, 0.0};
+      double acc[RC];
+#pragma unroll
+      for (int r = 0; r < RC; r++) acc[r] = 0.0;
       for (uint32_t mu = 0; mu < k; mu++) {
         const double y = sE[j + mu * nc];
 #pragma unroll
-        for (int r = 0; r < 4; r++) {
+        for (int r = 0; r < RC; r++) {
           const uint32_t i = ig + 4u * r;
           if (i < nr) acc[r] = fma(sW[mu + i * (k + 1)], y, acc[r]);
         }
       }
 #pragma unroll
-      for (int r = 0; r < 4; r++) {
+      for (int r = 0; r < RC; r++) {
         const uint32_t i = ig + 4u * r;
         if (i < nr) Wf[(size_t) (rf + i) * k + c0 + j] = acc[r];
       }
