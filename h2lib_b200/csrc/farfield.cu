@@ -65,7 +65,10 @@ __device__ __forceinline__ double dlagr_bar(double x, const double *xi, double w
 // around it) and written once.
 constexpr int BATCH = 32;
 constexpr int NSMAX = 64;   // single-triangle rule points (q^2, q <= 8)
-constexpr int LEAF_SPLIT = 4;
+#ifndef H2B_LEAF_SPLIT
+#define H2B_LEAF_SPLIT 2
+#endif
+constexpr int LEAF_SPLIT = H2B_LEAF_SPLIT;
 
 template <bool LINEAR, bool DN>
 __global__ void __launch_bounds__(256) leaf_basis_kernel(FarLeafArgs a) {
