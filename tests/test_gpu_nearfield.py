@@ -124,3 +124,22 @@ def test_invalid_arguments_fail_loudly(s4):
         hb.nearfield(slp, np.array([0, 0], dtype=np.uint32), None)   # repeated index
     with pytest.raises(hb.H2BError):
         hb.nearfield(slp, np.array([4096], dtype=np.uint32), None)   # out of range
+
+
+@pytest.mark.parametrize("q,q2", [(1, 2), (3, 3), (4, 5)])
+def test_other_quadrature_orders_against_oracle(s4, q, q2):
+    """Orders other than the default 2 / 4: the generic distant kernel, the full common-vertex
+    rule (no tensor or merged form) and the reduced edge / identical rules for other q2."""
+    for rb, cb in ((L, L), (C, C), (L, C)):
+        for layer in ("slp", "dlp"):
+            bem = (hb.new_slp_laplace_bem3d(s4, q, q2, rb, cb) if layer == "slp"
+                   else hb.new_dlp_laplace_bem3d(s4, q, q2, rb, cb, 0.5))
+            A = hb.nearfield(bem, None, None)
+            ref = orc.nearfield(omesh(s4), orc.LAPLACE, orc.SLP if layer == "slp" else orc.DLP,
+                                rb, cb, q=q, q2=q2, alpha=0.0 if layer == "slp" else 0.5)
+            assert rel_entry_err(A, ref) < TOL, (q, q2, rb, cb, layer)
+    bem = hb.new_dlp_helmholtz_bem3d(2.0 + 0.5j, s4, q, q2, C, C, 0.5)
+    A = hb.nearfield(bem, None, None)
+    ref = orc.nearfield(omesh(s4), orc.HELMHOLTZ, orc.DLP, C, C, q=q, q2=q2, k=2.0 + 0.5j,
+                        alpha=0.5)
+    assert rel_entry_err(A, ref) < TOL
