@@ -855,12 +855,13 @@ __global__ void __launch_bounds__(SING_THREADS, 1) near_sing_kernel(SingArgs a) 
   const int lane = threadIdx.x & 31;
   const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
-  // lanes per pair: a warp per pair, except for the merged vertex rule (32 items of 4 kernel
-  // evaluations each) and the reduced edge / identical rules (384 / 96 items), where 8 lanes take
-  // a pair and a warp four pairs: the reduction over the lanes then takes 3 shuffle steps
-  // instead of 5 per value.  A group without a pair of its own repeats the warp's first pair and
-  // writes nothing, so every lane takes part in the shuffles.
-  constexpr int LPP = (PART == 4 || PART == 2) ? 8 : 32;
+  // lanes per pair: a warp per pair for the full point rule; for the vertex rules (32 items of 4
+  // kernel evaluations each in the merged form, 32 groups of 16 in the tensor form) and the
+  // reduced edge / identical rules (384 / 96 items) 8 lanes take a pair and a warp four pairs,
+  // so that the reduction over the lanes takes 3 shuffle steps instead of 5 per value.  A group
+  // without a pair of its own repeats the warp's first pair and writes nothing, so every lane
+  // takes part in the shuffles.
+  constexpr int LPP = (PART == 4 || PART == 2 || PART == 1) ? 8 : 32;
   constexpr uint32_t PPW = 32 / LPP;
   const int sub = lane % LPP;
 
@@ -898,7 +899,7 @@ __global__ void __launch_bounds__(SING_THREADS, 1) near_sing_kernel(SingArgs a) 
         vert_item_merged<KK, RL, CL>(g, rm, a.rule_n[4], k, n0, n1, n2, acc);
     } else if ((PART == 0 || PART == 1) && cs == 1u && (PART == 1 || a.vert_tensor)) {
       // common vertex, tensor form: a group of VT_Q x VT_Q points per lane
-      for (uint32_t grp = lane; grp < n; grp += 32)
+      for (uint32_t grp = sub; grp < n; grp += LPP)
         vert_group_tensor<KK, RL, CL>(g, rx0, n, grp, n0, n1, n2, a.k_re, a.k_imn, acc);
     } else if ((PART == 0 || PART == 3) && cs == 1u) {
       // common vertex: the full rule (x0, x1, y0, y1, raw weight)
