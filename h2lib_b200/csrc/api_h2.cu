@@ -50,8 +50,8 @@ static void box_points(const double *bmin, const double *bmax, uint32_t m, doubl
 
 static void devtree_free(DevCTree &t, cudaStream_t st) {
   dfree(t.d_off, st); dfree(t.d_size, st); dfree(t.d_father, st); dfree(t.d_son0, st); dfree(t.d_son1, st);
-  dfree(t.d_idx, st); dfree(t.d_leaves, st); dfree(t.d_nonroot, st); dfree(t.d_levels, st); dfree(t.d_voff, st);
-  dfree(t.d_pts, st); dfree(t.d_V, st); dfree(t.d_E, st); dfree(t.d_counter, st); dfree(t.d_refs, st);
+  dfree(t.d_idx, st); dfree(t.d_leaves, st); dfree(t.d_nonroot, st); dfree(t.d_voff, st);
+  dfree(t.d_pts, st); dfree(t.d_V, st); dfree(t.d_E, st); dfree(t.d_refs, st);
   dfree(t.d_tr_off, st); dfree(t.d_tr_len, st);
   dfree(t.d_W, st); dfree(t.d_woff, st); dfree(t.d_fitems, st); dfree(t.d_wleaves, st); dfree(t.d_mitems, st);
   dfree(t.d_seg, st);
@@ -152,16 +152,6 @@ static int devtree_build(DevCTree &t, const h2b_ctree &c, int basis, uint32_t m,
   t.nnonroot = (uint32_t) nonroot.size();
   t.nleaves = (uint32_t) leaves.size();
   t.leaves = leaves;
-  // clusters by level
-  std::vector<std::vector<uint32_t>> bylevel(c.depth);
-  for (uint32_t i = 0; i < c.n; i++) bylevel[c.level[i]].push_back(i);
-  std::vector<uint32_t> levels;
-  t.level_start.assign(c.depth + 1, 0);
-  for (uint32_t l = 0; l < c.depth; l++) {
-    t.level_start[l] = (uint32_t) levels.size();
-    levels.insert(levels.end(), bylevel[l].begin(), bylevel[l].end());
-  }
-  t.level_start[c.depth] = (uint32_t) levels.size();
   // triangle lists of the leaves (basis assembly)
   h2b_nearplan tmp;
   h2b_nearplan_init(&tmp);
@@ -187,15 +177,13 @@ static int devtree_build(DevCTree &t, const h2b_ctree &c, int basis, uint32_t m,
       (rc = upload(&t.d_father, father, st)) || (rc = upload(&t.d_son0, son0, st)) ||
       (rc = upload(&t.d_son1, son1, st)) || (rc = upload(&t.d_idx, idx, st)) ||
       (rc = upload(&t.d_leaves, leaves, st)) || (rc = upload(&t.d_nonroot, nonroot, st)) ||
-      (rc = upload(&t.d_levels, levels, st)) || (rc = upload(&t.d_voff, voff, st)) ||
+      (rc = upload(&t.d_voff, voff, st)) ||
       (rc = upload(&t.d_pts, pts, st)) || (rc = upload(&t.d_refs, refs, st)) ||
       (rc = upload(&t.d_tr_off, tr_off, st)) || (rc = upload(&t.d_tr_len, tr_len, st)) ||
       (rc = upload(&t.d_seg, seg, st)))
     return rc;
   H2B_CUDA_TRY(cudaMallocAsync(&t.d_V, sizeof(double) * std::max<uint64_t>(vtot, 1), st));
   H2B_CUDA_TRY(cudaMallocAsync(&t.d_E, sizeof(double) * std::max<uint64_t>((uint64_t) (c.n - 1) * k * k, 1), st));
-  H2B_CUDA_TRY(cudaMallocAsync(&t.d_counter, sizeof(unsigned) * c.n, st));
-  H2B_CUDA_TRY(cudaMemsetAsync(t.d_counter, 0, sizeof(unsigned) * c.n, st));
   return H2B_OK;
 }
 
@@ -210,7 +198,7 @@ extern "C" void h2b_h2matrix_del(h2b_h2matrix *h) {
   if (h->cst) cudaStreamSynchronize(h->cst);  // pending asynchronous exports read the blocks
   // the operator's own data
   for (DevCTree *t : {&h->rt, &h->ct}) {
-    dfree(t->d_V, st); dfree(t->d_E, st); dfree(t->d_W, st); dfree(t->d_counter, st);
+    dfree(t->d_V, st); dfree(t->d_E, st); dfree(t->d_W, st);
     dfree(t->f_W, st);
   }
   dfree(h->f_N, st); dfree(h->f_S, st); dfree(h->d_S, st); dfree(h->d_N, st);
@@ -371,17 +359,12 @@ extern "C" h2b_h2matrix *h2b_h2matrix_new(const h2b_bem *bem, const h2b_tree *tr
     }
   }
   h2b_nearplan_free(&plan);
-  // flattened bases over the admissible clusters (unless the nested transforms are requested)
-  {
-    const char *e = getenv("H2B_MVM_NESTED");
-    h->flat = !(e && e[0] == '1');
-  }
-  // backward items (row side) in short slices: y rows take one atomic addition per item, and
-  // the slices give the backward launch enough CTAs; forward items (column side) in long ones,
-  // since each adds k entries of xt atomically
-  if (rc == H2B_OK && h->flat)
+  // flattened bases over the admissible clusters.  Backward items (row side) in short slices:
+  // y rows take one atomic addition per item, and the slices give the backward launch enough
+  // CTAs; forward items (column side) in long ones, since each adds k entries of xt atomically
+  if (rc == H2B_OK)
     rc = devtree_flat_setup(h->rt, tree->row, arc, h->k, H2B_MVM_BACK_ROWS, h->st);
-  if (rc == H2B_OK && h->flat)
+  if (rc == H2B_OK)
     rc = devtree_flat_setup(h->ct, tree->col, acc, h->k, H2B_MVM_FLAT_ROWS, h->st);
   // single-triangle rule (raw and linear-basis weighted)
   if (rc == H2B_OK) {
@@ -430,8 +413,7 @@ extern "C" h2b_h2matrix *h2b_h2matrix_new_like(const h2b_bem *bem, const h2b_h2m
   h->quad_fp32 = 0;
   h->f_S = h->f_N = nullptr;
   h->d_S = h->d_N = h->d_xp = h->d_yp = h->d_xt = h->d_yt = h->d_xio = h->d_yio = nullptr;
-  for (DevCTree *t : {&h->rt, &h->ct}) t->d_V = t->d_E = t->d_W = nullptr, t->f_W = nullptr,
-                                       t->d_counter = nullptr;
+  for (DevCTree *t : {&h->rt, &h->ct}) t->d_V = t->d_E = t->d_W = nullptr, t->f_W = nullptr;
   int rc = H2B_OK;
   if (cudaStreamCreateWithFlags(&h->st, cudaStreamNonBlocking) != cudaSuccess) rc = H2B_ERR_CUDA;
   for (int e = 0; rc == H2B_OK && e < 12; e++)
@@ -444,10 +426,7 @@ extern "C" h2b_h2matrix *h2b_h2matrix_new_like(const h2b_bem *bem, const h2b_h2m
     if (cudaMallocAsync(&t->d_V, sizeof(double) * std::max<uint64_t>(t->vtotal, 1), h->st) ||
         cudaMallocAsync(&t->d_E, sizeof(double) * std::max<uint64_t>((uint64_t) (t->n - 1) * kk, 1),
                         h->st) ||
-        cudaMallocAsync(&t->d_counter, sizeof(unsigned) * t->n, h->st) ||
-        cudaMemsetAsync(t->d_counter, 0, sizeof(unsigned) * t->n, h->st) ||
-        (h->flat && cudaMallocAsync(&t->d_W, sizeof(double) * std::max<uint64_t>(t->wtotal, 1),
-                                    h->st)))
+        cudaMallocAsync(&t->d_W, sizeof(double) * std::max<uint64_t>(t->wtotal, 1), h->st))
       rc = H2B_ERR_NOMEM;
   }
   if (rc == H2B_OK &&
@@ -485,9 +464,6 @@ void h2b_h2_fill_mvm_plan(h2b_h2matrix *h) {
   p.yp = h->d_yp;
   p.xt = h->d_xt;
   p.yt = h->d_yt;
-  p.fwd = MvmForwardArgs{h->ct.d_leaves, h->ct.d_father, h->ct.d_son0, h->ct.d_son1,
-                         h->ct.d_size, h->ct.d_off, h->ct.d_voff, h->ct.d_V, h->ct.d_E, h->d_xp,
-                         h->d_xt, h->ct.d_counter, h->ct.nleaves, (int) h->k};
   MvmCoupleArgs &c = p.cpl;
   c.adm_rc = h->d_adm_rc;
   c.adm_cc = h->d_adm_cc;
@@ -509,10 +485,6 @@ void h2b_h2_fill_mvm_plan(h2b_h2matrix *h) {
   c.nadm = h->nadm;
   c.nnear = h->nnear;
   c.k = (int) h->k;
-  p.down = MvmDownArgs{nullptr, h->rt.d_father, h->rt.d_E, h->d_yt, (int) h->k};
-  p.bwd = MvmBackArgs{h->rt.d_leaves, h->rt.d_size, h->rt.d_off, h->rt.d_voff, h->rt.d_V,
-                      h->d_yt, h->d_yp, h->rt.nleaves, (int) h->k};
-  p.flat = h->flat;
   p.rseg = h->rt.d_seg;
   p.cseg = h->ct.d_seg;
   p.ncol_clusters = h->ct.n;
@@ -528,9 +500,6 @@ void h2b_h2_fill_mvm_plan(h2b_h2matrix *h) {
     f.nitems = t.nmitems;
     f.k = (int) h->k;
   }
-  p.level_list = h->rt.d_levels;
-  p.rdepth = std::min<uint32_t>(h->rt.depth, 64);
-  for (uint32_t l = 0; l <= p.rdepth; l++) p.level_start[l] = h->rt.level_start[l];
 }
 
 // ------------------------------------------------------------------------------------------
@@ -565,7 +534,7 @@ static int assemble_basis(h2b_h2matrix *h, DevCTree &t, int basis, int dn) {
   FarTransferArgs ta{t.d_nonroot, t.d_father, t.d_pts, t.d_E, t.nnonroot, (int) h->m, (int) h->k,
                      transposed};
   rc = h2b_far_transfer(&ta, h->st);
-  if (rc == H2B_OK && h->flat) rc = devtree_flatten(t, h->k, transposed, h->st);
+  if (rc == H2B_OK) rc = devtree_flatten(t, h->k, transposed, h->st);
   return rc;
 }
 
@@ -599,10 +568,6 @@ extern "C" int h2b_h2matrix_set_precision(h2b_h2matrix *h, int precision) {
 
 extern "C" int h2b_h2matrix_make_single(h2b_h2matrix *h) {
   if (!h) return H2B_ERR_ARG;
-  if (!h->flat) {
-    h2b_set_error("h2b_h2matrix_make_single: needs the flattened-basis matvec");
-    return H2B_ERR_STATE;
-  }
   drop_single(h);
   const uint64_t W = h->cx ? 2 : 1;
   const uint64_t nN = W * h->near_total, nS = W * (uint64_t) h->nadm * h->k * h->k;

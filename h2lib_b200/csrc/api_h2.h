@@ -15,14 +15,12 @@ struct DevCTree {
   uint32_t n = 0, nidx = 0, depth = 0, nleaves = 0, max_rows = 0, nnonroot = 0;
   uint64_t vtotal = 0;
   uint32_t *d_off = nullptr, *d_size = nullptr, *d_father = nullptr, *d_son0 = nullptr,
-           *d_son1 = nullptr, *d_idx = nullptr, *d_leaves = nullptr, *d_nonroot = nullptr,
-           *d_levels = nullptr;
+           *d_son1 = nullptr, *d_idx = nullptr, *d_leaves = nullptr, *d_nonroot = nullptr;
   uint64_t *d_voff = nullptr;
   double *d_pts = nullptr, *d_V = nullptr, *d_E = nullptr;
-  unsigned *d_counter = nullptr;
   TriRef *d_refs = nullptr;
   uint32_t *d_tr_off = nullptr, *d_tr_len = nullptr;
-  std::vector<uint32_t> leaves, level_start;
+  std::vector<uint32_t> leaves;
   // flattened bases (flatbasis.cu): W_t for every cluster of an admissible block and below
   double *d_W = nullptr;
   uint64_t *d_woff = nullptr;
@@ -44,7 +42,6 @@ struct h2b_h2matrix {
   const h2b_tree *tree = nullptr;
   uint32_t m = 0, k = 0, ns = 0;
   int cx = 0, num_sms = 148;
-  int flat = 1;  // matvec through flattened bases (W_t) instead of the nested transforms
   int quad_fp32 = 0;  // distant-pair quadrature in FP32 (h2b_h2matrix_set_precision)
   // 1: the tree, block and nearfield-plan arrays belong to another matrix (h2b_h2matrix_new_like);
   // only the operator's own data (bases, transfers, W, S, N, work vectors) are freed here

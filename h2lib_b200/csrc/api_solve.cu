@@ -169,20 +169,17 @@ static int solve_segments(Combo &combo, uint32_t nseg, const uint32_t *seg_off, 
   // segments, the products skip the columns of systems that have stopped.
   DevBuf work;
   work.st = st;
-  bool flat = true, forest = nseg > 1;
+  bool forest = nseg > 1;
   size_t nwork = 0;
   for (uint32_t i = 0; i < combo.nterms; i++) {
     const h2b_h2matrix *h = combo.ops[i];
-    flat = flat && h->flat;
     forest = forest && forest_matches(h->rt, nseg, seg_off) && forest_matches(h->ct, nseg, seg_off);
     nwork = std::max(nwork, h2b_mvm_work_doubles(&h->mvm, nrhs));
   }
-  if (flat) {
-    H2B_CUDA_TRY(cudaMallocAsync(&work.p, sizeof(double) * nwork, st));
-    combo.work = (double *) work.p;
-    combo.mask = forest ? g.mask : nullptr;
-    combo.nseg = nseg;
-  }
+  H2B_CUDA_TRY(cudaMallocAsync(&work.p, sizeof(double) * nwork, st));
+  combo.work = (double *) work.p;
+  combo.mask = forest ? g.mask : nullptr;
+  combo.nseg = nseg;
   GmresOp op{(void *) &combo, combo_apply, mixed ? combo_apply_single : nullptr};
   std::vector<GmresState> hs(nsys);
   int rc = h2b_gmres_run(&g, &op, db, dx, maxiter, st, hs.data());

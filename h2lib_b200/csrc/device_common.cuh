@@ -15,6 +15,10 @@
     }                                                                                         \
   } while (0)
 
+// Counts kernel launches made by the library (every host thread), read with h2b_launch_count.
+// Each direct launch site of the assembly, classification and matvec kernels calls it once.
+void h2b_note_launch(void);
+
 // 1/(4 pi): constant of the fundamental solutions of Laplace and Helmholtz
 // (KERNEL_CONST_LAPLACEBEM3D, Library/laplacebem3d.c:33; KERNEL_CONST_HELMHOLTZBEM3D,
 // Library/helmholtzbem3d.c:25).
@@ -47,30 +51,17 @@ static_assert(sizeof(TriRef) == 12, "TriRef must be 12 bytes");
 // error below 1e-6 measured on B200); two Newton-Raphson steps y <- y + y/2 (1 - x y^2) in FP64
 // (the classical iteration for x^{-1/2}; each step squares the relative error, so the result is
 // within 1.2 ulp, measured against 1/sqrt over 4M arguments in [1e-12, 16]).  Inputs are squared
-// distances of quadrature points: positive and normal.
-// Variant 0 seeds with the FP32 approximation (rsqrtf of the value rounded to FP32; same accuracy,
-// 4% slower in the nearfield kernel because of the two conversions); variant 2 calls CUDA's
-// rsqrt() (7% slower).
-#ifndef H2B_RSQRT
-#define H2B_RSQRT 1
-#endif
+// distances of quadrature points: positive and normal.  (Measured in the nearfield kernel: 4%
+// faster than an FP32 seed, which needs two conversions, and 7% faster than CUDA's rsqrt().)
 __device__ __forceinline__ double rsqrt_nr(double x) {
-#if H2B_RSQRT == 2
-  return rsqrt(x);
-#else
-#if H2B_RSQRT == 1
   double y;
   asm("rsqrt.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
-#else
-  double y = (double) rsqrtf((float) x);
-#endif
   double h = x * y;
   double e = fma(-h, y, 1.0);
   y = fma(0.5 * y, e, y);
   h = x * y;
   e = fma(-h, y, 1.0);
   return fma(0.5 * y, e, y);
-#endif
 }
 
 // Allow kernel K up to H2B_MAX_DYN_SMEM bytes of dynamic shared memory, once per process

@@ -257,6 +257,7 @@ extern "C" int h2b_far_leaf_basis(const FarLeafArgs *a, int linear, int dn, cuda
   do {                                                                                      \
     H2B_CUDA_TRY((h2b_allow_smem<leaf_basis_kernel<L, D>>()));                             \
     leaf_basis_kernel<L, D><<<a->nleaves * LEAF_SPLIT, 256, smem, st>>>(*a);                \
+    h2b_note_launch();                                                                      \
   } while (0)
   if (linear && dn) LAUNCH(true, true);
   else if (linear) LAUNCH(true, false);
@@ -274,6 +275,7 @@ extern "C" int h2b_far_transfer(const FarTransferArgs *a, cudaStream_t st) {
     return H2B_ERR_ARG;
   }
   transfer_kernel<<<a->n, 256, 0, st>>>(*a);
+  h2b_note_launch();
   H2B_CUDA_TRY(cudaGetLastError());
   return H2B_OK;
 }
@@ -291,6 +293,7 @@ extern "C" int h2b_far_coupling(const FarCouplingArgs *a, int cx, cudaStream_t s
     else LAUNCH(false, 0);
   }
 #undef LAUNCH
+  h2b_note_launch();
   H2B_CUDA_TRY(cudaGetLastError());
   return H2B_OK;
 }

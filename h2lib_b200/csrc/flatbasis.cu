@@ -168,12 +168,16 @@ extern "C" int h2b_to_single(const double *in, float *out, size_t n, int num_sms
   if (n == 0) return H2B_OK;
   const size_t want = (n + FLAT_TPB - 1) / FLAT_TPB, cap = (size_t) 8 * (num_sms > 0 ? num_sms : 148);
   to_single_kernel<<<(unsigned) (want < cap ? want : cap), FLAT_TPB, 0, st>>>(in, out, n);
+  h2b_note_launch();
   H2B_CUDA_TRY(cudaGetLastError());
   return H2B_OK;
 }
 
 extern "C" int h2b_flat_leaves(const FlatLeafArgs *a, cudaStream_t st) {
-  if (a->nleaves) leaf_copy_kernel<<<a->nleaves, FLAT_TPB, 0, st>>>(*a);
+  if (a->nleaves) {
+    leaf_copy_kernel<<<a->nleaves, FLAT_TPB, 0, st>>>(*a);
+    h2b_note_launch();
+  }
   H2B_CUDA_TRY(cudaGetLastError());
   return H2B_OK;
 }
@@ -188,6 +192,7 @@ extern "C" int h2b_flat_level(const FlatArgs *a, cudaStream_t st) {
   H2B_CUDA_TRY(h2b_allow_smem<flatten_kernel>());
   const uint32_t nparts = ((uint32_t) a->k + FLAT_COLS - 1) / FLAT_COLS;
   flatten_kernel<<<a->nitems * nparts, FLAT_TPB, smem, st>>>(*a);
+  h2b_note_launch();
   H2B_CUDA_TRY(cudaGetLastError());
   return H2B_OK;
 }

@@ -4,21 +4,21 @@
 //   forward transform   xt_t = V_t^T x_t (leaves), xt_t = sum_s E_s^T xt_s (Library/clusterbasis.c:524)
 //   coupling / near     yt_t += S_b xt_s,  y_t += N_b x_s      (fastaddeval, Library/h2matrix.c:1211)
 //   backward transform  yt_s += E_s yt_t,  y_t += V_t yt_t     (Library/clusterbasis.c:749)
+// The nested transforms are multiplied out once after assembly (flatbasis.cu): for every cluster
+// t of an admissible block, W_t = V_t (leaf) or [W_s E_s] over the sons s, the |t| x k basis on
+// t's own indices.  The forward transform is then xt_t = W_t^T x_t and the backward transform
+// y_t += W_t yt_t for every such cluster independently, with no dependence between levels.
 // Vectors are kept in cluster order (xp[i] = x[idx[i]]) so that every cluster's entries are
-// contiguous.  Three launches do the work:
-//   1. forward + nearfield: CTAs [0, leaves) compute xt of their leaf, and the CTA that finishes
-//      the last son of a cluster continues with the father (an atomic arrival counter per
-//      cluster, reset by that CTA), so no CTA ever waits for another; CTAs [leaves, leaves +
-//      nearfield blocks) add N_b x_s into yp meanwhile (the nearfield does not need xt);
-//   2. coupling: a CTA per admissible block adds S_b xt_s into yt (FP64 atomics);
-//   3. backward: a CTA per leaf walks its root-to-leaf path (upper transfers recomputed per leaf,
-//      read from L2) and adds V_t yt_t.
-// The column cluster basis is stored transposed (V^T: k x rows, E^T: k x k, both column-major)
-// so that the forward GEMVs read consecutive addresses with consecutive threads; the row basis is
-// stored as H2Lib does (V: rows x k, E: k x k).  Every GEMV splits its reduction over G = 256 / k
-// thread groups and combines the partial sums in shared memory, which keeps 256 loads in flight
-// per CTA instead of one dependent chain.
-// CX: complex coefficients (Helmholtz) — S, N, x, y complex (interleaved); V, E real.
+// contiguous.  A product is five launches:
+//   gather_zero   xp = x[idx], accumulators cleared;
+//   forward+near  CTAs [0, items): xt_t += W_t[rows]^T x[rows] for one slice of rows of t;
+//                 the other CTAs: y_r += N_b x_c for one nearfield block (independent of xt);
+//   coupling      yt_r += S_b xt_c per admissible block;
+//   backward      y[rows] += W_t[rows] yt_t per slice;
+//   scatter       y[idx] += alpha yp.
+// Partial sums reach their outputs with FP64 atomics.  The column side W^T is stored k x |t|
+// (column-major), so the forward GEMVs read consecutive addresses with consecutive threads.
+// CX: complex coefficients (Helmholtz) — S, N, x, y complex (interleaved); W real.
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -36,37 +36,6 @@ constexpr int KMAXW = 2 * 128;  // k <= 128 complex coefficients
 #define H2B_MVM_UNROLL 8
 #endif
 constexpr int MVM_UNROLL = H2B_MVM_UNROLL;
-
-// xp = x[idx] (cluster order)
-template <bool CX>
-__global__ void gather_kernel(const double *__restrict__ x, const uint32_t *__restrict__ idx,
-                              double *__restrict__ xp, uint32_t n) {
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    const uint32_t j = idx[i];
-    if (CX) {
-      xp[2 * i] = x[2 * j];
-      xp[2 * i + 1] = x[2 * j + 1];
-    } else {
-      xp[i] = x[j];
-    }
-  }
-}
-
-// y[idx[i]] += alpha * yp[i]
-template <bool CX>
-__global__ void scatter_kernel(const double *__restrict__ yp, const uint32_t *__restrict__ idx,
-                               double *__restrict__ y, uint32_t n, double ar, double ai) {
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    const uint32_t j = idx[i];
-    if (CX) {
-      const double re = yp[2 * i], im = yp[2 * i + 1];
-      y[2 * j] += ar * re - ai * im;
-      y[2 * j + 1] += ar * im + ai * re;
-    } else {
-      y[j] += ar * yp[i];
-    }
-  }
-}
 
 // out[r] = sum_{c < ncols} P[r + c*ld] * v[c] for r < nrows (P column-major, real), v complex if
 // CX.  Threads: r = t % nrows, group g = t / nrows takes the columns c = g mod G.  The result is
@@ -145,114 +114,6 @@ __device__ __forceinline__ void panel_mv_atomic(const TM *__restrict__ M, uint32
       }
       atomicAdd(&yv[W * (r0 + threadIdx.x)], ar);
       if (CX) atomicAdd(&yv[W * (r0 + threadIdx.x) + 1], ai);
-    }
-    __syncthreads();
-  }
-}
-
-// Launch 1: forward transform (CTAs < nleaves) and nearfield blocks (the other CTAs).
-template <bool CX>
-__global__ void __launch_bounds__(TPB) forward_near_kernel(MvmForwardArgs a, MvmCoupleArgs c) {
-  constexpr int W = CX ? 2 : 1;
-  __shared__ double red[TPB * W];
-  __shared__ double tmp[2 * KMAXW];
-  __shared__ int last;
-  if (blockIdx.x >= a.nleaves) {
-    const uint32_t nb = blockIdx.x - a.nleaves;
-    const uint32_t r = c.near_rc[nb], cc = c.near_cc[nb];
-    panel_mv_atomic<CX>(c.N + (size_t) W * c.near_off[nb], c.rsize[r], c.csize[cc],
-                        c.xp + (size_t) W * c.coff[cc], c.yp + (size_t) W * c.roff[r], red);
-    return;
-  }
-  const uint32_t k = (uint32_t) a.k;
-  uint32_t cl = a.leaves[blockIdx.x];
-  // leaf: xt_c = V_c^T xp[off .. off + size): V^T stored k x size (ld = k)
-  gemv_split<CX, true>(a.V + a.voff[cl], k, k, a.size[cl], a.xp + (size_t) W * a.off[cl], red,
-                       a.xt + (size_t) W * k * cl);
-  // climb while this CTA completes the last son of the father
-  while (true) {
-    const uint32_t f = a.father[cl];
-    if (f == UINT32_MAX) return;
-    __threadfence();  // this CTA's xt writes are visible device-wide before it arrives
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      const unsigned old = atomicAdd(&a.counter[f], 1u);
-      last = (old == 1u);
-      if (last) a.counter[f] = 0u;  // reset for the next product
-    }
-    __syncthreads();
-    if (!last) return;
-    __threadfence();
-    // xt_f = E_s0^T xt_s0 + E_s1^T xt_s1: both E^T panels are k x k (ld = k)
-    const uint32_t s0 = a.son0[f], s1 = a.son1[f];
-    gemv_split<CX, true>(a.E + (size_t) (s0 - 1) * k * k, k, k, k, a.xt + (size_t) W * k * s0,
-                         red, tmp);
-    gemv_split<CX, true>(a.E + (size_t) (s1 - 1) * k * k, k, k, k, a.xt + (size_t) W * k * s1,
-                         red, tmp + W * k);
-    for (uint32_t e = threadIdx.x; e < W * k; e += blockDim.x)
-      a.xt[(size_t) W * k * f + e] = tmp[e] + tmp[W * k + e];
-    cl = f;
-  }
-}
-
-// Launch 2: coupling blocks yt_r += S_b xt_c.
-template <bool CX, bool SINGLE = false>
-__global__ void __launch_bounds__(TPB) coupling_mv_kernel(MvmCoupleArgs a) {
-  constexpr int W = CX ? 2 : 1;
-  __shared__ double red[TPB * W];
-  const uint32_t b = blockIdx.x;
-  const uint32_t k = (uint32_t) a.k;
-  if (SINGLE)
-    panel_mv_atomic<CX>(a.Ss + (size_t) W * k * k * b, k, k, a.xt + (size_t) W * k * a.adm_cc[b],
-                        a.yt + (size_t) W * k * a.adm_rc[b], red);
-  else
-    panel_mv_atomic<CX>(a.S + (size_t) W * k * k * b, k, k, a.xt + (size_t) W * k * a.adm_cc[b],
-                        a.yt + (size_t) W * k * a.adm_rc[b], red);
-}
-
-// Launch 3: backward transform, a CTA per row leaf walking root -> leaf:
-// t_root = yt_root, t_c = yt_c + E_c t_father(c) (the recursion of backward_clusterbasis_avector,
-// Library/clusterbasis.c:749), then yp[leaf rows] += V_leaf t_leaf.
-template <bool CX>
-__global__ void __launch_bounds__(TPB) backward_chain_kernel(MvmBackArgs a, const uint32_t *father,
-                                                             const double *E) {
-  constexpr int W = CX ? 2 : 1;
-  __shared__ double red[TPB * W];
-  __shared__ double tcur[KMAXW], tnew[KMAXW];
-  __shared__ uint32_t path[64];
-  __shared__ int depth;
-  const uint32_t leaf = a.leaves[blockIdx.x];
-  const uint32_t k = (uint32_t) a.k;
-  if (threadIdx.x == 0) {
-    int d = 0;
-    uint32_t c = leaf;
-    while (c != UINT32_MAX && d < 64) {
-      path[d++] = c;
-      c = father[c];
-    }
-    depth = d;  // path[d-1] is the root
-  }
-  __syncthreads();
-  const int d = depth;
-  for (uint32_t e = threadIdx.x; e < W * k; e += blockDim.x)
-    tcur[e] = a.yt[(size_t) W * k * path[d - 1] + e];
-  __syncthreads();
-  for (int l = d - 2; l >= 0; l--) {
-    const uint32_t c = path[l];
-    gemv_split<CX, false>(E + (size_t) (c - 1) * k * k, k, k, k, tcur, red, tnew);
-    for (uint32_t e = threadIdx.x; e < W * k; e += blockDim.x)
-      tcur[e] = tnew[e] + a.yt[(size_t) W * k * c + e];
-    __syncthreads();
-  }
-  // yp[off + i] += sum_nu V[i, nu] t[nu]  (V: rows x k, ld = rows)
-  const uint32_t rows = a.size[leaf];
-  double *yp = a.yp + (size_t) W * a.off[leaf];
-  for (uint32_t r0 = 0; r0 < rows; r0 += TPB) {
-    const uint32_t nr = rows - r0 < (uint32_t) TPB ? rows - r0 : (uint32_t) TPB;
-    gemv_split<CX, false>(a.V + a.voff[leaf] + r0, rows, nr, k, tcur, red, tnew);
-    for (uint32_t i = threadIdx.x; i < nr; i += blockDim.x) {
-      yp[W * (r0 + i)] += tnew[W * i];
-      if (CX) yp[W * (r0 + i) + 1] += tnew[W * i + 1];
     }
     __syncthreads();
   }
@@ -607,10 +468,18 @@ void launch_warp_items(const MvmPlan *p, const MvmVecs &v, cudaStream_t st) {
   constexpr uint32_t WPB = TPB / 32;
   const MvmCoupleArgs &ca = p->cpl;
   const uint32_t n1 = p->ffwd.nitems + ca.nnear;
-  if (n1) forward_near_warp_kernel<CX, SINGLE, NQ><<<(n1 + WPB - 1) / WPB, TPB, 0, st>>>(p->ffwd, ca, v);
-  if (ca.nadm) coupling_warp_kernel<CX, SINGLE, NQ><<<(ca.nadm + WPB - 1) / WPB, TPB, 0, st>>>(ca, v);
-  if (p->fbwd.nitems)
+  if (n1) {
+    forward_near_warp_kernel<CX, SINGLE, NQ><<<(n1 + WPB - 1) / WPB, TPB, 0, st>>>(p->ffwd, ca, v);
+    h2b_note_launch();
+  }
+  if (ca.nadm) {
+    coupling_warp_kernel<CX, SINGLE, NQ><<<(ca.nadm + WPB - 1) / WPB, TPB, 0, st>>>(ca, v);
+    h2b_note_launch();
+  }
+  if (p->fbwd.nitems) {
     backward_warp_kernel<CX, SINGLE, NQ><<<(p->fbwd.nitems + WPB - 1) / WPB, TPB, 0, st>>>(p->fbwd, v);
+    h2b_note_launch();
+  }
 }
 
 template <bool CX, bool SINGLE>
@@ -624,6 +493,7 @@ int launch_flat(const MvmPlan *p, const double *x, size_t ldx, double *y, size_t
   const size_t nyp = W * p->nrow, nxt = W * (size_t) p->k * p->ncol_clusters,
                nyt = W * (size_t) p->k * p->nrow_clusters;
   gather_zero_kernel<CX><<<gz, 256, 0, st>>>(x, ldx, p->cidx, p->ncol, v, nyp, nxt, nyt);
+  h2b_note_launch();
   // FP32-stored products run one warp per item (measured faster); FP64 ones one CTA per item
   // (measured faster: the warp form's registers halve its occupancy for 8-byte entries)
   if (H2B_MVM_WARP && SINGLE) {
@@ -632,14 +502,22 @@ int launch_flat(const MvmPlan *p, const double *x, size_t ldx, double *y, size_t
     else
       launch_warp_items<CX, SINGLE, WG_Q>(p, v, st);
   } else {
-    if (p->ffwd.nitems + ca.nnear)
+    if (p->ffwd.nitems + ca.nnear) {
       forward_flat_near_kernel<CX, SINGLE><<<p->ffwd.nitems + ca.nnear, TPB, 0, st>>>(p->ffwd,
                                                                                        ca, v);
-    if (ca.nadm) coupling_flat_kernel<CX, SINGLE><<<ca.nadm, TPB, 0, st>>>(ca, v);
-    if (p->fbwd.nitems)
+      h2b_note_launch();
+    }
+    if (ca.nadm) {
+      coupling_flat_kernel<CX, SINGLE><<<ca.nadm, TPB, 0, st>>>(ca, v);
+      h2b_note_launch();
+    }
+    if (p->fbwd.nitems) {
       backward_flat_kernel<CX, SINGLE><<<p->fbwd.nitems, TPB, 0, st>>>(p->fbwd, v);
+      h2b_note_launch();
+    }
   }
   scatter_multi_kernel<CX><<<gz, 256, 0, st>>>(v, p->ridx, y, ldy, p->nrow, ar, ai);
+  h2b_note_launch();
   H2B_CUDA_TRY(cudaGetLastError());
   return H2B_OK;
 }
@@ -663,7 +541,7 @@ MvmVecs plan_vecs(const MvmPlan *p) {
 
 extern "C" int h2b_mvm_launch_single(const MvmPlan *p, const double *x, double *y, double ar,
                                      double ai, cudaStream_t st) {
-  if (!p->flat || !p->cpl.Ss || !p->cpl.Ns || !p->ffwd.Ws || !p->fbwd.Ws) {
+  if (!p->cpl.Ss || !p->cpl.Ns || !p->ffwd.Ws || !p->fbwd.Ws) {
     h2b_set_error("matvec: no FP32 copy of the H2 matrix (h2b_h2matrix_make_single)");
     return H2B_ERR_ARG;
   }
@@ -678,40 +556,13 @@ extern "C" int h2b_mvm_launch_single(const MvmPlan *p, const double *x, double *
 
 extern "C" int h2b_mvm_launch(const MvmPlan *p, const double *x, double *y, double ar, double ai,
                               cudaStream_t st) {
-  const int cx = p->cx;
-  const size_t W = cx ? 2 : 1;
-  const int sms = p->num_sms > 0 ? p->num_sms : 148;
   if (p->k > 128) {
     h2b_set_error("matvec: rank %d > 128", p->k);
     return H2B_ERR_ARG;
   }
-  const uint32_t gg = (p->ncol + 255) / 256 < (uint32_t) (4 * sms) ? (p->ncol + 255) / 256
-                                                                   : (uint32_t) (4 * sms);
-  if (p->flat) {
-    const MvmVecs v = plan_vecs(p);
-    return p->cx ? launch_flat<true, false>(p, x, 0, y, 0, ar, ai, v, st)
-                 : launch_flat<false, false>(p, x, 0, y, 0, ar, ai, v, st);
-  }
-  H2B_CUDA_TRY(cudaMemsetAsync(p->yp, 0, sizeof(double) * W * p->nrow, st));
-  H2B_CUDA_TRY(cudaMemsetAsync(p->yt, 0, sizeof(double) * W * p->k * p->nrow_clusters, st));
-  const MvmForwardArgs &fa = p->fwd;
-  const MvmCoupleArgs &ca = p->cpl;
-  const MvmBackArgs &ba = p->bwd;
-  if (cx) {
-    gather_kernel<true><<<gg, 256, 0, st>>>(x, p->cidx, p->xp, p->ncol);
-    forward_near_kernel<true><<<fa.nleaves + ca.nnear, TPB, 0, st>>>(fa, ca);
-    if (ca.nadm) coupling_mv_kernel<true><<<ca.nadm, TPB, 0, st>>>(ca);
-    backward_chain_kernel<true><<<ba.nleaves, TPB, 0, st>>>(ba, p->down.father, p->down.E);
-    scatter_kernel<true><<<gg, 256, 0, st>>>(p->yp, p->ridx, y, p->nrow, ar, ai);
-  } else {
-    gather_kernel<false><<<gg, 256, 0, st>>>(x, p->cidx, p->xp, p->ncol);
-    forward_near_kernel<false><<<fa.nleaves + ca.nnear, TPB, 0, st>>>(fa, ca);
-    if (ca.nadm) coupling_mv_kernel<false><<<ca.nadm, TPB, 0, st>>>(ca);
-    backward_chain_kernel<false><<<ba.nleaves, TPB, 0, st>>>(ba, p->down.father, p->down.E);
-    scatter_kernel<false><<<gg, 256, 0, st>>>(p->yp, p->ridx, y, p->nrow, ar, ai);
-  }
-  H2B_CUDA_TRY(cudaGetLastError());
-  return H2B_OK;
+  const MvmVecs v = plan_vecs(p);
+  return p->cx ? launch_flat<true, false>(p, x, 0, y, 0, ar, ai, v, st)
+               : launch_flat<false, false>(p, x, 0, y, 0, ar, ai, v, st);
 }
 
 extern "C" size_t h2b_mvm_work_doubles(const MvmPlan *p, uint32_t nrhs) {
@@ -724,9 +575,8 @@ extern "C" int h2b_mvm_launch_batch(const MvmPlan *p, int single, uint32_t nrhs,
                                     size_t ldx, double *y, size_t ldy, double ar, double ai,
                                     double *work, const uint32_t *mask, uint32_t nseg,
                                     cudaStream_t st) {
-  if (!p->flat || (single && (!p->cpl.Ss || !p->cpl.Ns || !p->ffwd.Ws || !p->fbwd.Ws))) {
-    h2b_set_error("batched matvec: needs the flattened path%s",
-                  single ? " and the FP32 copies (h2b_h2matrix_make_single)" : "");
+  if (single && (!p->cpl.Ss || !p->cpl.Ns || !p->ffwd.Ws || !p->fbwd.Ws)) {
+    h2b_set_error("batched matvec: needs the FP32 copies (h2b_h2matrix_make_single)");
     return H2B_ERR_ARG;
   }
   if (p->k > 128 || nrhs == 0) {

@@ -4,19 +4,6 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
-struct MvmForwardArgs {       // column cluster basis
-  const uint32_t *leaves;     // leaf ids
-  const uint32_t *father, *son0, *son1;
-  const uint32_t *size, *off;
-  const uint64_t *voff;
-  const double *V, *E;
-  const double *xp;
-  double *xt;
-  unsigned *counter;          // per cluster arrival counters (zero between products)
-  uint32_t nleaves;
-  int k;
-};
-
 struct MvmCoupleArgs {
   const uint32_t *adm_rc, *adm_cc;
   const double *S;
@@ -28,25 +15,6 @@ struct MvmCoupleArgs {
   const double *xt, *xp;
   double *yt, *yp;
   uint32_t nadm, nnear;
-  int k;
-};
-
-struct MvmDownArgs {          // row cluster basis
-  const uint32_t *clusters;   // clusters of one level
-  const uint32_t *father;
-  const double *E;
-  double *yt;
-  int k;
-};
-
-struct MvmBackArgs {
-  const uint32_t *leaves;
-  const uint32_t *size, *off;
-  const uint64_t *voff;
-  const double *V;
-  const double *yt;
-  double *yp;
-  uint32_t nleaves;
   int k;
 };
 
@@ -67,25 +35,18 @@ struct MvmFlatArgs {
 
 struct MvmPlan {
   int cx, num_sms;
-  int flat;                      // 1: flattened-basis transforms (ffwd / fbwd)
-  MvmFlatArgs ffwd, fbwd;
+  MvmFlatArgs ffwd, fbwd;        // forward (column side) and backward (row side) slices
   const uint32_t *rseg, *cseg;   // surface of every row / column cluster (forest trees)
   int k;
   uint32_t nrow, ncol, nrow_clusters, ncol_clusters;
   const uint32_t *ridx, *cidx;   // device index arrays of the row / column tree
   double *xp, *yp, *xt, *yt;     // work vectors
-  MvmForwardArgs fwd;
   MvmCoupleArgs cpl;
-  MvmDownArgs down;
-  MvmBackArgs bwd;
-  const uint32_t *level_list;    // row-tree clusters sorted by level (device)
-  uint32_t level_start[65];      // host copy of the level offsets
-  uint32_t rdepth;
 };
 
 extern "C" int h2b_mvm_launch(const MvmPlan *p, const double *x, double *y, double ar, double ai,
                               cudaStream_t st);
-// The same product from the FP32 copies of N, S and W (flattened path only): matrix entries are
+// The same product from the FP32 copies of N, S and W: matrix entries are
 // read as FP32 and widened, vectors and sums stay FP64, so the product reads half the bytes.
 extern "C" int h2b_mvm_launch_single(const MvmPlan *p, const double *x, double *y, double ar,
                                      double ai, cudaStream_t st);

@@ -216,10 +216,6 @@ __device__ __forceinline__ void quad_point_red(const PairGeo &g, double ra, doub
 // first in both triangles, X_a - Y_b = (d0 + x0 p1 + x1 p2) - (y0 q1 + y1 q2).  `t` is the
 // packed group arrays (gn groups each), the row weights include the group weight.
 constexpr int VT_Q = 4;
-#ifndef H2B_VT_UNROLL
-#define H2B_VT_UNROLL 4
-#endif
-constexpr int VT_UNROLL = H2B_VT_UNROLL;  // column points per unrolled step
 template <int KK, bool RL, bool CL>
 __device__ __forceinline__ void vert_group_tensor(const PairGeo &g, const double *t, uint32_t gn,
                                                   uint32_t grp, double n0, double n1, double n2,
@@ -240,7 +236,7 @@ __device__ __forceinline__ void vert_group_tensor(const PairGeo &g, const double
     for (int c = 0; c < NCH; c++)
 #pragma unroll
       for (int j = 0; j < NC; j++) in[c][j] = 0.0;
-#pragma unroll VT_UNROLL
+#pragma unroll
     for (int b = 0; b < VT_Q; b++) {
       // column point formed here rather than kept for all a (register budget of 128)
       const double *cp = col + (size_t) b * (2 + NC) * gn + grp;
@@ -792,11 +788,6 @@ struct SingArgs {
   int *err;                   // set to 1 if the staging copy did not complete
 };
 
-// Points per lane in flight in the singular kernel's point loop (unroll factor).
-#ifndef H2B_SING_UNROLL
-#define H2B_SING_UNROLL 1
-#endif
-constexpr int SING_UNROLL = H2B_SING_UNROLL;
 
 // One warp per singular pair.  The three rules are copied into shared memory once per CTA.
 // 512 threads: one CTA per SM holds the staged rules, 16 warps hide the FP64 latencies.
@@ -904,14 +895,14 @@ __global__ void __launch_bounds__(SING_THREADS, 1) near_sing_kernel(SingArgs a) 
     } else if ((PART == 0 || PART == 3) && cs == 1u) {
       // common vertex: the full rule (x0, x1, y0, y1, raw weight)
       const double *rx1 = rx0 + n, *ry0 = rx0 + 2 * n, *ry1 = rx0 + 3 * n, *rw = rx0 + 4 * n;
-#pragma unroll SING_UNROLL
+#pragma unroll 1
       for (uint32_t k = lane; k < n; k += 32)
         quad_point<KK, RL, CL>(g, rx0[k], rx1[k], ry0[k], ry1[k], rw[k], n0, n1, n2, a.k_re,
                                a.k_imn, acc);
     } else if (PART == 0 || PART == 2) {
       // common edge / identical: the reduced rule (a, b, c, basis-weighted weights)
       const double *rb = rx0 + n, *rc = rx0 + 2 * n, *rwt = rx0 + 3 * n;
-#pragma unroll SING_UNROLL
+#pragma unroll 1
       for (uint32_t k = sub; k < n; k += LPP)
         quad_point_red<KK, RL, CL>(g, rx0[k], rb[k], rc[k], rwt + k, n, n0, n1, n2, a.k_re,
                                    a.k_imn, acc);
@@ -1009,7 +1000,10 @@ int launch_dist(const h2b_near_launch *L, cudaStream_t st) {
   a.k_re = L->k_re;
   a.k_imn = L->k_imn;
   a.q = (int) L->q;
-  if (L->ntiles > 0) near_dist_kernel<Q, KK, RL, CL, F32><<<L->ntiles, 256, smem, st>>>(a);
+  if (L->ntiles > 0) {
+    near_dist_kernel<Q, KK, RL, CL, F32><<<L->ntiles, 256, smem, st>>>(a);
+    h2b_note_launch();
+  }
   H2B_CUDA_TRY(cudaGetLastError());
   return H2B_OK;
 }
@@ -1048,6 +1042,7 @@ int launch_sing_part(const h2b_near_launch *L, uint32_t first, uint32_t count, c
   uint32_t want = (count + wpc - 1) / wpc;
   uint32_t grid = want < (uint32_t) sms ? want : (uint32_t) sms;
   near_sing_kernel<KK, RL, CL, PART><<<grid, SING_THREADS, smem, st>>>(a);
+  h2b_note_launch();
   H2B_CUDA_TRY(cudaGetLastError());
   return H2B_OK;
 }
@@ -1213,6 +1208,7 @@ extern "C" int h2b_near_classify(const void *tri, const void *refs, const h2b_ti
   else
     classify_kernel<false><<<ntiles, 256, 0, st>>>((const TriRec *) tri, (const TriRef *) refs,
                                                    tiles, cursor, nullptr, nullptr);
+  h2b_note_launch();
   H2B_CUDA_TRY(cudaGetLastError());
   return H2B_OK;
 }
