@@ -31,6 +31,8 @@ _SIGS = {
     "h2b_last_error": (C.c_char_p, []),
     "h2b_version": (C.c_char_p, []),
     "h2b_device_init": (C.c_int, [C.c_int]),
+    "h2b_device_memory": (C.c_int, [_u64p]),
+    "h2b_launch_count": (C.c_int, [C.POINTER(C.c_uint64)]),
     "h2b_macro_mesh_size": (C.c_int, [C.c_int, C.c_uint32, C.POINTER(C.c_uint32),
                                       C.POINTER(C.c_uint32)]),
     "h2b_macro_mesh_build": (C.c_int, [C.c_int, C.c_uint32, _f64p, _u32p]),

@@ -84,6 +84,34 @@ int h2b_ensure_device(void) {
   return h2b_device_init(dev);
 }
 
+static std::atomic<unsigned long long> g_launches{0};
+
+void h2b_note_launch(void) { g_launches.fetch_add(1, std::memory_order_relaxed); }
+
+extern "C" int h2b_launch_count(uint64_t *n) {
+  if (!n) return H2B_ERR_ARG;
+  *n = g_launches.load(std::memory_order_relaxed);
+  return H2B_OK;
+}
+
+extern "C" int h2b_device_memory(uint64_t out[4]) {
+  if (!out) return H2B_ERR_ARG;
+  int dev = 0;
+  size_t fr = 0, tot = 0;
+  H2B_CUDA_TRY(cudaGetDevice(&dev));
+  H2B_CUDA_TRY(cudaMemGetInfo(&fr, &tot));
+  cudaMemPool_t pool;
+  uint64_t used = 0, reserved = 0;
+  H2B_CUDA_TRY(cudaDeviceGetDefaultMemPool(&pool, dev));
+  H2B_CUDA_TRY(cudaMemPoolGetAttribute(pool, cudaMemPoolAttrUsedMemCurrent, &used));
+  H2B_CUDA_TRY(cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReservedMemCurrent, &reserved));
+  out[0] = fr;
+  out[1] = tot;
+  out[2] = used;
+  out[3] = reserved;
+  return H2B_OK;
+}
+
 bool h2b_is_device_ptr(const void *p) {
   cudaPointerAttributes attr;
   if (cudaPointerGetAttributes(&attr, p) != cudaSuccess) {

@@ -10,7 +10,13 @@
 // The array is H2B_NOALLOC_SCRATCH_BYTES large; every GPU that loads the library holds it until
 // the process exits.  All calls share it and it keeps the last call's contents, so calls that
 // overlap on the GPU (different host threads, or different streams without ordering) race; the
-// entries that must start at zero (T and the solver state) are cleared by every call.
+// entries that must start at zero (T and the solver state) are cleared by every call.  Every call,
+// failed ones included, waits for its own GPU work before it returns.
+//
+// Cost: the loop is driven from the host, one launch sequence per Arnoldi step followed by a read
+// of the solver state (a device-to-host copy and a stream synchronisation), so each step pays a
+// host round trip that h2b_solve_gmres, which runs up to 512 steps per CUDA graph launch, does
+// not.  For small systems this makes the variant noticeably slower per step.
 #include <cuda_runtime.h>
 #include <string.h>
 
@@ -23,31 +29,31 @@ __device__ __align__(256) unsigned char g_noalloc_scratch[H2B_NOALLOC_SCRATCH_BY
 
 namespace {
 
-// Device address of g_noalloc_scratch per device.  In host code the symbol's name is only a
-// host-side stand-in, so the address is looked up once per device with that device current.
-constexpr int MAX_DEVICES = 64;
-void *g_scratch_addr[MAX_DEVICES] = {};
-
+// Device address of g_noalloc_scratch on the current device.  In host code the symbol's name is
+// only a host-side stand-in, so the address is looked up with the device current.  It is looked
+// up on every call (a cheap table lookup once the module is loaded): no cached address can go
+// stale after cudaDeviceReset, and concurrent first calls share no host state.
 int scratch_address(void **out) {
-  int dev = 0;
-  H2B_CUDA_TRY(cudaGetDevice(&dev));
-  if (dev < 0 || dev >= MAX_DEVICES) {
-    h2b_set_error("h2b_solve_gmres_noalloc: device %d out of range", dev);
-    return H2B_ERR_ARG;
+  void *p = nullptr;
+  const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+  if (e != cudaSuccess || !p) {
+    h2b_set_error("h2b_solve_gmres_noalloc: cudaGetSymbolAddress failed: %s",
+                  cudaGetErrorString(e));
+    return H2B_ERR_CUDA;
   }
-  if (!g_scratch_addr[dev]) {
-    void *p = nullptr;
-    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-    if (e != cudaSuccess || !p) {
-      h2b_set_error("h2b_solve_gmres_noalloc: cudaGetSymbolAddress failed: %s",
-                    cudaGetErrorString(e));
-      return H2B_ERR_CUDA;
-    }
-    g_scratch_addr[dev] = p;
-  }
-  *out = g_scratch_addr[dev];
+  *out = p;
   return H2B_OK;
 }
+
+// Waits for the stream when a call returns early, so that no queued work of a failed call keeps
+// using the shared array after the call has returned.
+struct StreamDrain {
+  cudaStream_t st;
+  bool armed = false;
+  ~StreamDrain() {
+    if (armed) cudaStreamSynchronize(st);
+  }
+};
 
 struct ComboNA {
   uint32_t nterms;
@@ -115,6 +121,8 @@ extern "C" int h2b_solve_gmres_noalloc(uint32_t nterms, const h2b_h2matrix *cons
   std::vector<uint32_t> blk(nblocks);  // host table, copied into the work space
   h2b_gmres_layout(&g, dx + W * n, A0->cx, 1, sizes, kmax, &sys, blk.data());
   g.eps = eps;
+  StreamDrain drain{st};
+  drain.armed = true;  // from here on, every return waits for the work queued on st
   // the scratch keeps the previous call's contents: clear what must start at zero
   H2B_CUDA_TRY(cudaMemsetAsync(g.T, 0, sizeof(double) * 2 * (size_t) kmax * kmax, st));
   H2B_CUDA_TRY(cudaMemsetAsync(g.state, 0, sizeof(GmresState), st));
@@ -157,5 +165,6 @@ extern "C" int h2b_solve_gmres_noalloc(uint32_t nterms, const h2b_h2matrix *cons
   if ((rc = h2b_gmres_update(&g, dx, GMRES_SEL_ALL, st)) != H2B_OK) return rc;
   H2B_CUDA_TRY(cudaMemcpyAsync(x, dx, sizeof(double) * W * n, cudaMemcpyDefault, st));
   H2B_CUDA_TRY(cudaStreamSynchronize(st));
+  drain.armed = false;
   return (int) iter;
 }

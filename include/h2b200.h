@@ -77,6 +77,16 @@ const char *h2b_version(void);
  * Returns H2B_ERR_CUDA if no sm_100 device is usable. */
 int h2b_device_init(int device);
 
+/* Device memory of the current device: out[0] free and out[1] total bytes (cudaMemGetInfo), out[2]
+ * bytes in use and out[3] bytes reserved by the device's default stream-ordered memory pool, from
+ * which every handle allocates.  Diagnostics; no reference counterpart. */
+int h2b_device_memory(uint64_t out[4]);
+
+/* Kernels the library has launched directly since it was loaded (all host threads): the
+ * assembly, classification and matrix-vector kernels (a GMRES CUDA-graph launch is not counted
+ * here).  Diagnostics; no reference counterpart. */
+int h2b_launch_count(uint64_t *n);
+
 /* ------------------------------------------------------------------------------------------
  * Host-side geometry (no GPU needed)
  * ------------------------------------------------------------------------------------------ */
@@ -339,12 +349,15 @@ int h2b_solve_gmres_mixed(uint32_t nterms, const h2b_h2matrix *const *ops, const
  * h2b_solve_gmres takes its work space (Householder vectors, compact-WY factor, staging vectors)
  * from a fixed device array of H2B_NOALLOC_SCRATCH_BYTES bytes compiled into the library, which
  * every GPU that loads the library holds until the process exits, and launches the step kernels
- * directly (no CUDA graph).  Problems whose work space, about 8 * (n * kmax + 4 n) bytes (twice
- * that for complex operators), exceeds the array are rejected with H2B_ERR_ARG.  Same algorithm,
- * arguments and result as h2b_solve_gmres; b and x may be host or device pointers.
- * The first call on a device looks up the array's device address (cudaGetSymbolAddress): make it
- * before any stream capture.  All calls share the array and it keeps the last call's contents;
- * calls that overlap on the GPU race, so serialise them. */
+ * directly (no CUDA graph, one host round trip per Arnoldi step).  Problems whose work space
+ * exceeds the array are rejected with H2B_ERR_ARG; the work space is slightly more than
+ * 8 * (n * kmax + 4 n) bytes (twice that for complex operators): it is
+ * 8 (W n (kmax + 4) + 2 kmax^2 + 8 kmax + 2 ceil(n / 256) (kmax + 1)) bytes plus about 1 KiB,
+ * W = 1 real, 2 complex.  Same algorithm, arguments and result as h2b_solve_gmres; b and x may be host
+ * or device pointers.  Every call looks up the array's device address (cudaGetSymbolAddress); the
+ * first call on a device loads the module, so make it before any stream capture.  All calls share
+ * the array and it keeps the last call's contents; calls that overlap on the GPU race, so
+ * serialise them.  Every call, a failed one included, waits for its GPU work before returning. */
 #define H2B_NOALLOC_SCRATCH_BYTES (24u << 20)
 int h2b_solve_gmres_noalloc(uint32_t nterms, const h2b_h2matrix *const *ops, const double *coef,
                             const double *b, double *x, double eps, uint32_t maxiter,

@@ -38,6 +38,12 @@ def solve_noalloc(ops, coefs, b, eps, maxiter, kmax):
     return it, x
 
 
+def device_memory():
+    out = np.zeros(4, dtype=np.uint64)
+    check(lib.h2b_device_memory(out), "h2b_device_memory")
+    return [int(v) for v in out]
+
+
 def test_noalloc_gmres_matches_allocating_gmres_laplace():
     check(lib.h2b_device_init(0), "device_init")
     gr = hb.new_sphere_surface3d(8)
@@ -47,10 +53,17 @@ def test_noalloc_gmres_matches_allocating_gmres_laplace():
     b = np.sin(0.37 * np.arange(V.rows)) + 0.5
     u = np.zeros(V.rows)
     it_ref = hb.solve_gmres_h2matrix_avector(V, b, u, 1e-8, 1000, 20)
-    for _ in range(2):  # two calls in a row share the fixed work space
+    for call in range(2):  # two calls in a row share the fixed work space
+        before = device_memory()
         it, x = solve_noalloc([V], [1.0], b, 1e-8, 1000, 20)
+        after = device_memory()
         assert it == it_ref
         assert relerr(x, u) < TOL
+        if call == 1:
+            # the second call allocates nothing: free device memory and the stream-ordered
+            # pool's used and reserved bytes are unchanged
+            assert after[0] == before[0]
+            assert after[2] == before[2] and after[3] == before[3]
 
 
 def test_noalloc_gmres_matches_allocating_gmres_helmholtz():
