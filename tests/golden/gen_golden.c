@@ -7,7 +7,7 @@
  *
  * Usage: gen_golden <outdir> <section> [...]
  * Sections (real build):    quad sphere8 sphere4 h2small config2 cube adlp
- * Sections (complex build): helm_sphere4 helm_h2small config3 helm_gmres helm_adlp
+ * Sections (complex build): helm_sphere4 helm_h2small config3 config3_k8 helm_gmres helm_adlp
  */
 #include <math.h>
 #include <stdio.h>
@@ -313,6 +313,100 @@ collect_near(pch2matrix G, fbuf_t *N, uint *count, uint limit)
         collect_near(G->son[i + j * G->rsons], N, count, limit);
 }
 
+/* The nearfield leaves in block-tree pre-order (sons column-major), as a flat list. */
+typedef struct {
+  pch2matrix *b;
+  uint n, cap;
+} nearlist_t;
+
+static void
+list_near(pch2matrix G, nearlist_t *l)
+{
+  uint i, j;
+  if (G->f) {
+    if (l->n == l->cap) {
+      l->cap = l->cap ? 2 * l->cap : 1024;
+      l->b = realloc(l->b, sizeof(pch2matrix) * l->cap);
+    }
+    l->b[l->n++] = G;
+    return;
+  }
+  if (G->son)
+    for (j = 0; j < G->csons; j++)
+      for (i = 0; i < G->rsons; i++)
+        list_near(G->son[i + j * G->rsons], l);
+}
+
+/* Three whole nearfield blocks of V and K for entrywise comparison: the largest block, the most
+ * ragged one (largest |rows - cols|) and the largest diagonal one (row cluster == column
+ * cluster).  <prefix>_nblk_idx holds their positions in the list of nearfield blocks. */
+static void
+dump_selected_near(const char *prefix, pch2matrix V, pch2matrix K)
+{
+  nearlist_t lv = { NULL, 0, 0 }, lk = { NULL, 0, 0 };
+  uint sel[3] = { 0, 0, 0 }, i, s;
+  size_t best[3] = { 0, 0, 0 };
+  char name[256];
+  list_near(V, &lv);
+  list_near(K, &lk);
+  for (i = 0; i < lv.n; i++) {
+    pamatrix f = lv.b[i]->f;
+    size_t sz = (size_t) f->rows * f->cols;
+    size_t rag = f->rows > f->cols ? f->rows - f->cols : f->cols - f->rows;
+    if (sz > best[0]) best[0] = sz, sel[0] = i;
+    if (rag > best[1]) best[1] = rag, sel[1] = i;
+    if (lv.b[i]->rb->t == lv.b[i]->cb->t && sz > best[2]) best[2] = sz, sel[2] = i;
+  }
+  snprintf(name, sizeof(name), "%s_nblk_idx", prefix);
+  dump_uint(name, sel, 1, 3, 0);
+  for (s = 0; s < 3; s++) {
+    snprintf(name, sizeof(name), "%s_nblkV_%u", prefix, s);
+    dump_amatrix(name, lv.b[sel[s]]->f);
+    snprintf(name, sizeof(name), "%s_nblkK_%u", prefix, s);
+    dump_amatrix(name, lk.b[sel[s]]->f);
+  }
+  free(lv.b);
+  free(lk.b);
+}
+
+/* solve_gmres_avector (Library/krylovsolvers.c:183) with the same calls in the same order, also
+ * recording the residual estimate |rhat_k| of every iteration: trace[0] after init_gmres,
+ * trace[i] after step i.  The caller's trace array holds maxiter entries. */
+static uint
+solve_gmres_traced(void *A, addeval_t addeval_A, pcavector b, pavector x, real eps,
+                   uint maxiter, uint kmax, real *trace, real *threshold)
+{
+  pavector rhat, q, tau;
+  pamatrix qr;
+  real norm, error;
+  uint n = x->dim, iter, k;
+
+  rhat = new_avector(n);
+  q = new_avector(n);
+  qr = new_amatrix(n, kmax);
+  tau = new_avector(kmax);
+  norm = norm2_avector(b);
+  init_gmres(addeval_A, A, b, x, rhat, q, &k, qr, tau);
+  error = residualnorm_gmres(rhat, k);
+  trace[0] = error;
+  iter = 0;
+  while (error > eps * norm && iter + 1 != maxiter) {
+    if (k + 1 >= kmax)
+      finish_gmres(addeval_A, A, b, x, rhat, q, &k, qr, tau);
+    step_gmres(addeval_A, A, b, x, rhat, q, &k, qr, tau);
+    error = residualnorm_gmres(rhat, k);
+    iter++;
+    trace[iter] = error;
+  }
+  finish_gmres(addeval_A, A, b, x, rhat, q, &k, qr, tau);
+  *threshold = eps * norm;
+  del_avector(tau);
+  del_amatrix(qr);
+  del_avector(q);
+  del_avector(rhat);
+  return iter;
+}
+
 static void
 dump_h2parts(const char *prefix, pch2matrix G, uint limit)
 {
@@ -611,6 +705,8 @@ h2_case(const char *prefix, psurface3d gr, basisfunctionbem3d basis, uint clf, r
     snprintf(name, sizeof(name), "%s_Kparts", prefix);
     dump_h2parts(name, K, parts_limit);
   }
+  if (!strcmp(prefix, "c2"))
+    dump_selected_near(prefix, V, K);
 
   x = new_avector(V->cb->t->size);
   y = new_avector(V->rb->t->size);
@@ -643,9 +739,19 @@ h2_case(const char *prefix, psurface3d gr, basisfunctionbem3d basis, uint clf, r
     snprintf(name, sizeof(name), "%s_b", prefix);
     dump_avector(name, b);
     clear_avector(u);
-    start_stopwatch(sw);
-    iter = solve_gmres_h2matrix_avector(V, b, u, 1.0e-8, 1000, 50);
-    t0 = stop_stopwatch(sw);
+    {
+      /* solve_gmres_h2matrix_avector (Library/krylovsolvers.c:254), with its residual trace */
+      real *trace = (real *) calloc(1000, sizeof(real)), thr = 0.0;
+      start_stopwatch(sw);
+      iter = solve_gmres_traced(V, (addeval_t) addeval_h2matrix_avector, b, u, 1.0e-8, 1000, 50,
+                                trace, &thr);
+      t0 = stop_stopwatch(sw);
+      snprintf(name, sizeof(name), "%s_gmres_trace", prefix);
+      dump_real(name, trace, 1, iter + 1, 0);
+      snprintf(name, sizeof(name), "%s_gmres_threshold", prefix);
+      dump_scalar(name, thr);
+      free(trace);
+    }
     snprintf(name, sizeof(name), "%s_time_gmres", prefix);
     dump_scalar(name, t0);
     snprintf(name, sizeof(name), "%s_gmres_iter", prefix);
@@ -852,15 +958,16 @@ addeval_bw(field alpha, void *matrix, pcavector x, pavector y)
   addeval_h2matrix_avector(-I * alpha * bw->eta, bw->V, x, y);
 }
 
-/* Config 3: cube refined to 49152 triangles, constant basis, k = 2, m = 5, leaf 64, eta 1.4;
- * plane wave along (1,1,1)/sqrt(3); Dirichlet data -u_inc; GMRES(80) to 1e-8. */
+/* Config 3: cube refined to 49152 triangles, constant basis, wavenumber k, m = 5, leaf 64,
+ * eta 1.4; plane wave along (1,1,1)/sqrt(3); Dirichlet data -u_inc; GMRES(80) to 1e-8.  The
+ * trees are dumped once (they do not depend on k); the solve records its residual trace. */
 static void
-section_config3(void)
+config3_case(const char *p, field k, int with_trees)
 {
   pmacrosurface3d mg = new_cube_macrosurface3d();
   psurface3d gr = build_from_macrosurface3d_surface3d(mg, 64);
-  field k = 2.0;
   real eta = 1.4;
+  char name[256];
   pbem3d slp, dlp;
   pcluster root;
   pblock broot;
@@ -877,8 +984,10 @@ section_config3(void)
   dlp = new_dlp_helmholtz_bem3d(k, gr, 2, 4, BASIS_CONSTANT_BEM3D, BASIS_CONSTANT_BEM3D, 0.5);
   root = build_bem3d_cluster(slp, 64, BASIS_CONSTANT_BEM3D);
   broot = build_strict_block(root, root, &eta, admissible_max_cluster);
-  dump_cluster("c3", root);
-  dump_block("c3", broot, root, root);
+  if (with_trees) {
+    dump_cluster(p, root);
+    dump_block(p, broot, root, root);
+  }
   Vrb = build_from_cluster_clusterbasis(root);
   Vcb = build_from_cluster_clusterbasis(root);
   Krb = build_from_cluster_clusterbasis(root);
@@ -894,18 +1003,22 @@ section_config3(void)
   assemble_bem3d_h2matrix_row_clusterbasis(dlp, Krb);
   assemble_bem3d_h2matrix_col_clusterbasis(dlp, Kcb);
   assemble_bem3d_h2matrix(dlp, K);
-  dump_scalar("c3_time_assembly", stop_stopwatch(sw));
+  snprintf(name, sizeof(name), "%s_time_assembly", p);
+  dump_scalar(name, stop_stopwatch(sw));
 
   x = new_avector(gr->triangles);
   y = new_avector(gr->triangles);
   seeded_avector(x, 3);
-  dump_avector("c3_x", x);
+  snprintf(name, sizeof(name), "%s_x", p);
+  dump_avector(name, x);
   clear_avector(y);
   addeval_h2matrix_avector(1.0, V, x, y);
-  dump_avector("c3_ySLP", y);
+  snprintf(name, sizeof(name), "%s_ySLP", p);
+  dump_avector(name, y);
   clear_avector(y);
   addeval_h2matrix_avector(1.0, K, x, y);
-  dump_avector("c3_yDLP", y);
+  snprintf(name, sizeof(name), "%s_yDLP", p);
+  dump_avector(name, y);
 
   for (i = 0; i < 3; i++)
     kvec[i] = REAL(k) / REAL_SQRT(3.0);
@@ -916,16 +1029,28 @@ section_config3(void)
   u = new_avector(gr->triangles);
   integrate_bem3d_c_avector(dlp, rhs_dirichlet_plane_helmholtzbem3d, b, (void *) &hdata);
   scale_avector(-1.0, b);
-  dump_avector("c3_b", b);
+  snprintf(name, sizeof(name), "%s_b", p);
+  dump_avector(name, b);
   bw.V = V;
   bw.KM = K;
   bw.eta = k;
   clear_avector(u);
-  start_stopwatch(sw);
-  iter = solve_gmres_avector(&bw, addeval_bw, b, u, 1.0e-8, 1000, 80);
-  dump_scalar("c3_time_gmres", stop_stopwatch(sw));
-  dump_scalar("c3_gmres_iter", (double) iter);
-  dump_avector("c3_u", u);
+  {
+    real *trace = (real *) calloc(1000, sizeof(real)), thr = 0.0;
+    start_stopwatch(sw);
+    iter = solve_gmres_traced(&bw, addeval_bw, b, u, 1.0e-8, 1000, 80, trace, &thr);
+    snprintf(name, sizeof(name), "%s_time_gmres", p);
+    dump_scalar(name, stop_stopwatch(sw));
+    snprintf(name, sizeof(name), "%s_gmres_trace", p);
+    dump_real(name, trace, 1, iter + 1, 0);
+    snprintf(name, sizeof(name), "%s_gmres_threshold", p);
+    dump_scalar(name, thr);
+    free(trace);
+  }
+  snprintf(name, sizeof(name), "%s_gmres_iter", p);
+  dump_scalar(name, (double) iter);
+  snprintf(name, sizeof(name), "%s_u", p);
+  dump_avector(name, u);
 
   del_avector(x); del_avector(y); del_avector(b); del_avector(u);
   del_h2matrix(V);
@@ -938,6 +1063,18 @@ section_config3(void)
   del_surface3d(gr);
   del_macrosurface3d(mg);
   del_stopwatch(sw);
+}
+
+static void
+section_config3(void)
+{
+  config3_case("c3", 2.0, 1);
+}
+
+static void
+section_config3_k8(void)
+{
+  config3_case("c8", 8.0, 0);
 }
 
 /* Helmholtz adjoint double layer K' + M/2 (new_adlp_helmholtz_bem3d, Library/helmholtzbem3d.c:
@@ -1079,6 +1216,8 @@ main(int argc, char **argv)
       section_helm_h2small();
     else if (!strcmp(argv[i], "config3"))
       section_config3();
+    else if (!strcmp(argv[i], "config3_k8"))
+      section_config3_k8();
     else if (!strcmp(argv[i], "helm_gmres"))
       section_helm_gmres();
     else if (!strcmp(argv[i], "helm_adlp"))

@@ -8,7 +8,7 @@ read the committed .npz files.
     python tests/golden/make_golden.py [section ...]
 
 Sections: quad sphere8 sphere4 h2small config2 cube adlp helm_sphere4 helm_h2small config3
-helm_gmres helm_adlp
+config3_k8 helm_gmres helm_adlp
 """
 import os
 import subprocess
@@ -23,7 +23,8 @@ REF = os.environ.get("REF", "/root/reference")
 REFOUT = os.path.join(ROOT, "oracle", "_ref")
 
 REAL_SECTIONS = ["quad", "sphere8", "sphere4", "h2small", "config2", "cube", "adlp"]
-COMPLEX_SECTIONS = ["helm_sphere4", "helm_h2small", "config3", "helm_gmres", "helm_adlp"]
+COMPLEX_SECTIONS = ["helm_sphere4", "helm_h2small", "config3", "config3_k8", "helm_gmres",
+                    "helm_adlp"]
 DTYPES = {"f8": np.float64, "u4": np.uint32, "c16": np.complex128}
 # Arrays stored only in part, to keep the fixtures small: name -> number of leading columns kept
 # (matrices are written column-major, i.e. shape (cols, rows)).

@@ -5,6 +5,7 @@ of GMRES iterations and reproduce the solution to 1e-9 relative)."""
 import numpy as np
 import pytest
 
+from conftest import fortran, rel_entry_err
 from h2lib_b200 import bem3d as hb
 
 pytestmark = pytest.mark.gpu
@@ -114,6 +115,22 @@ def test_config2_matvec_and_solve(gold):
     check(lib.h2b_h2matrix_assemble_col_clusterbasis(K.handle), "cb")
     check(lib.h2b_h2matrix_assemble_farfield(K.handle), "far")
     check(lib.h2b_h2matrix_assemble_nearfield_pair(V.handle, K.handle), "near pair")
+    # whole nearfield blocks, entrywise (row-scaled rule): the largest one (here also the
+    # largest diagonal one) and the most ragged one (64 x 26)
+    sel = [int(i) for i in g["c2_nblk_idx"]]
+    recs = tree.block_records()
+    near = recs[recs[:, 4] == 0]
+    sizes = near[:, 1].astype(np.int64) * near[:, 3]
+    starts = np.concatenate([[0], np.cumsum(sizes)])
+    nv = V.export(5, max(sel) + 1)
+    nk = K.export(5, max(sel) + 1)
+    for s, b in enumerate(sel):
+        rows, cols = int(near[b, 1]), int(near[b, 3])
+        for got, name in ((nv, "V"), (nk, "K")):
+            blk = got[starts[b]:starts[b + 1]].reshape(cols, rows).T
+            want = fortran(g[f"c2_nblk{name}_{s}"])
+            assert blk.shape == want.shape
+            assert rel_entry_err(blk, want) < 1e-12, (name, s)
     x = g["c2_x"]
     assert relerr(hb.addeval_h2matrix_avector(1.0, V, x, np.zeros(V.rows)), g["c2_ySLP"]) < 1e-12
     assert relerr(hb.addeval_h2matrix_avector(1.0, K, x, np.zeros(K.rows)), g["c2_yDLP"]) < 1e-12
@@ -122,11 +139,15 @@ def test_config2_matvec_and_solve(gold):
     b = hb.addeval_h2matrix_avector(1.0, K, gD, np.zeros(K.rows))
     u = np.zeros(V.rows)
     it = hb.solve_gmres_h2matrix_avector(V, b, u, 1e-8, 1000, 50)
-    # The reference stops after 161 iterations; its residual estimate after 160 iterations is
-    # 1.0196 x the threshold (CPU oracle trace of the same restarted Householder GMRES), a 2%
-    # margin that FP64 rounding differences of the operator (1e-15, amplified by the condition
-    # number of V) can cross.  Hence 160 or 161, and the solution agrees to the solver accuracy.
-    assert abs(it - int(g["c2_gmres_iter"][0])) <= 1
+    # The reference stops after 161 iterations.  Its own residual-estimate trace (fixture, from
+    # the reference's run) puts iteration 160 at 1.0189 x the threshold eps ||b||: a margin of
+    # under 2% that FP64 rounding differences of the operator (1e-15, amplified by the condition
+    # number of V) can cross.  Only then is one iteration fewer allowed.
+    ref_it = int(g["c2_gmres_iter"][0])
+    trace, thr = g["c2_gmres_trace"], g["c2_gmres_threshold"][0]
+    assert trace.size == ref_it + 1 and trace[-1] <= thr < trace[-2]
+    margin = trace[-2] / thr - 1.0
+    assert it == ref_it or (it == ref_it - 1 and margin < 0.02)
     assert relerr(u, g["c2_u"]) < 1e-6
     assert hb.residual_norm([V], [1.0], b, u) < 1.05e-8
     err, nrm = hb.l2_error_harmonic(slp, Z, u)

@@ -17,32 +17,51 @@ def relerr(a, b):
     return float(np.linalg.norm(a - b) / np.linalg.norm(b))
 
 
-def test_config3_brakhage_werner(gold):
-    g = gold("config3")
-    k = 2.0
+@pytest.fixture(scope="module")
+def cube64():
     gr = hb.new_cube_surface3d(64)
+    return gr, hb.build_tree(gr, C, C, 64, 1.4)
+
+
+def allowed_iterations(g, p):
+    """The reference's iteration count, and one fewer only where its own residual-estimate trace
+    (fixture) puts the previous iteration less than 2% above eps ||b|| (a margin that rounding
+    differences of the device operator can cross)."""
+    ref_it = int(g[f"{p}_gmres_iter"][0])
+    trace, thr = g[f"{p}_gmres_trace"], g[f"{p}_gmres_threshold"][0]
+    assert trace.size == ref_it + 1 and trace[-1] <= thr < trace[-2]
+    return {ref_it, ref_it - 1} if trace[-2] < 1.02 * thr else {ref_it}
+
+
+@pytest.mark.parametrize("section,p,k", [("config3", "c3", 2.0), ("config3_k8", "c8", 8.0)])
+def test_config3_brakhage_werner(gold, cube64, section, p, k):
+    """k = 2 and k = 8 (k diam = 27.7): products, right-hand side, iterations and solution against
+    the reference's run on the same trees."""
+    g = gold(section)
+    gr, tree = cube64
+    if p == "c3":
+        rec, box, idx = tree.clusters(0)
+        np.testing.assert_array_equal(rec, g["c3_ctree"])
+        np.testing.assert_array_equal(idx, g["c3_idx"])
+        np.testing.assert_array_equal(tree.block_records(), g["c3_blocks"])
     slp = hb.new_slp_helmholtz_bem3d(k, gr, 2, 4, C, C)
     dlp = hb.new_dlp_helmholtz_bem3d(k, gr, 2, 4, C, C, 0.5)
-    tree = hb.build_tree(gr, C, C, 64, 1.4)
-    rec, box, idx = tree.clusters(0)
-    np.testing.assert_array_equal(rec, g["c3_ctree"])
-    np.testing.assert_array_equal(idx, g["c3_idx"])
-    np.testing.assert_array_equal(tree.block_records(), g["c3_blocks"])
     V = hb.H2Matrix(slp, tree, 5).assemble()
     K = hb.H2Matrix(dlp, tree, 5).assemble()
-    x = np.ascontiguousarray(g["c3_x"])
+    x = np.ascontiguousarray(g[f"{p}_x"])
     y = hb.addeval_h2matrix_avector(1.0, V, x, np.zeros(V.rows, dtype=np.complex128))
-    assert relerr(y, g["c3_ySLP"]) < 1e-12
+    assert relerr(y, g[f"{p}_ySLP"]) < 1e-12
     y = hb.addeval_h2matrix_avector(1.0, K, x, np.zeros(K.rows, dtype=np.complex128))
-    assert relerr(y, g["c3_yDLP"]) < 1e-12
+    assert relerr(y, g[f"{p}_yDLP"]) < 1e-12
     d = np.ones(3) / np.sqrt(3.0)
     b = hb.integrate_plane_wave(slp, k * d, coef=-1.0)
-    assert relerr(b, g["c3_b"]) < 1e-12
+    assert relerr(b, g[f"{p}_b"]) < 1e-12
     u = np.zeros(V.rows, dtype=np.complex128)
     it = hb.solve_gmres([K, V], [1.0, -1j * k], b, u, 1e-8, 1000, 80)
-    assert abs(it - int(g["c3_gmres_iter"][0])) <= 1
-    assert relerr(u, g["c3_u"]) < 1e-6
-    assert hb.residual_norm([K, V], [1.0, -1j * k], b, u) < 1.05e-8
+    assert it in allowed_iterations(g, p)
+    assert relerr(u, g[f"{p}_u"]) < 1e-6
+    if p == "c3":
+        assert hb.residual_norm([K, V], [1.0, -1j * k], b, u) < 1.05e-8
 
 
 def test_complex_gmres_givens(gold):

@@ -230,3 +230,33 @@ def test_adjoint_double_layer_helmholtz(gold):
     assert relerr(A.export(5, 24), g["hadh2cc_parts_N"]) < 1e-12
     y = A.addeval(1.0, np.ascontiguousarray(g["hadh2cc_x"]), np.zeros(A.rows, dtype=np.complex128))
     assert relerr(y, g["hadh2cc_y"]) < 1e-12
+
+
+def test_config2_nearfield_blocks(gold):
+    """Whole nearfield blocks of the config-2 operators (sphere refined x64, linear basis, leaf 64,
+    eta 1.4): the oracle fills the reference's largest and most ragged blocks with the block's
+    own index sets, entrywise at 1e-12 (row-scaled rule)."""
+    from h2lib_b200 import bem3d as hb
+    g = gold("config2")
+    gr = hb.Surface3d(g["c2mesh_x"], g["c2mesh_t"])
+    mesh = orc.Mesh(gr.x, gr.t, gr.n, gr.g)
+    idx = g["c2_idx"]
+    near = g["c2_blocks"][g["c2_blocks"][:, 4] == 0]
+    for s, b in enumerate(int(i) for i in g["c2_nblk_idx"]):
+        ro, rs, co, cs = (int(v) for v in near[b, :4])
+        ridx = np.ascontiguousarray(idx[ro:ro + rs])
+        cidx = np.ascontiguousarray(idx[co:co + cs])
+        for layer, name, alpha in ((orc.SLP, "V", 0.0), (orc.DLP, "K", 0.5)):
+            A = orc.nearfield(mesh, orc.LAPLACE, layer, L, L, ridx, cidx, alpha=alpha)
+            assert rel_entry_err(A, fortran(g[f"c2_nblk{name}_{s}"])) < 1e-12, (name, s)
+
+
+def test_config2_gmres_trace_pins_the_iteration_allowance(gold):
+    """The reference's own residual-estimate trace of the config-2 solve: it stops after 161
+    iterations, and iteration 160 lies less than 2% above eps ||b|| (the margin that lets the
+    device solve, with another summation order, stop one iteration earlier)."""
+    g = gold("config2")
+    trace, thr, it = g["c2_gmres_trace"], g["c2_gmres_threshold"][0], int(g["c2_gmres_iter"][0])
+    assert it == 161 and trace.size == it + 1
+    assert trace[-1] <= thr < trace[-2] < 1.02 * thr
+    assert np.all(trace[:-1] > thr)
