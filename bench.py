@@ -65,6 +65,8 @@ def parse():
     p.add_argument("--no-helmholtz", action="store_true")
     p.add_argument("--no-mixed", action="store_true")
     p.add_argument("--serve-requests", type=int, default=48)
+    p.add_argument("--cpu-batch-sample", type=int, default=8)
+    p.add_argument("--cpu-serve-budget", type=float, default=60.0)
     p.add_argument("--serve-rates", default="50,200,1000,2000")
     return p.parse_args()
 
@@ -164,30 +166,112 @@ class ClockSampler:
 # --------------------------------------------------------------------------------------------
 
 REF_BENCH = os.path.join(ROOT, "oracle", "_ref", "ref_bench")
+REF_BENCH_CX = os.path.join(ROOT, "oracle", "_ref", "ref_bench_complex")
+# reference GMRES iteration counts of config 3 (the reference's own runs, tests/golden/config3*.npz)
+REF_BW_ITERATIONS = {2.0: 22, 8.0: 32}
 
 
-def run_reference(a, steps, warmup, stride):
-    if not os.path.exists(REF_BENCH):
+def run_ref(exe, args, timeout=1800):
+    """One run of the reference harness (oracle/ref_bench.c); None if it was not built."""
+    if not os.path.exists(exe):
         return None
-    out = subprocess.run([REF_BENCH, str(a.split), str(a.clf), str(a.eta), str(a.m), str(steps),
-                          str(warmup), str(stride)], capture_output=True, text=True, timeout=1800)
+    out = subprocess.run([exe, *[str(x) for x in args]], capture_output=True, text=True,
+                         timeout=timeout)
     if out.returncode != 0:
-        raise RuntimeError(f"ref_bench failed: {out.stderr[-2000:]}")
+        raise RuntimeError(f"{os.path.basename(exe)} failed: {out.stderr[-2000:]}")
     return json.loads(out.stdout)
 
 
+def run_reference_assembly(a, steps, warmup, solve=False):
+    return run_ref(REF_BENCH, ["assembly", a.split, a.clf, a.eta, a.m, steps, warmup] +
+                   (["--solve"] if solve else []))
+
+
+def write_requests(path, reqs):
+    """Request file of ref_bench's `requests` mode: (pde, kmax, k, srcs, x, t) per request."""
+    import struct
+    with open(path, "wb") as fh:
+        fh.write(struct.pack("<I", len(reqs)))
+        for pde, kmax, k, srcs, x, t in reqs:
+            srcs = np.ascontiguousarray(srcs, dtype=np.float64).reshape(-1, 3)
+            fh.write(struct.pack("<IIIddI", pde, kmax, 1000, k, 1e-8, srcs.shape[0]))
+            fh.write(srcs.tobytes())
+            fh.write(struct.pack("<II", x.shape[0], t.shape[0]))
+            fh.write(np.ascontiguousarray(x, dtype=np.float64).tobytes())
+            fh.write(np.ascontiguousarray(t, dtype=np.uint32).tobytes())
+
+
+def run_reference_requests(reqs, budget_s):
+    """Serve `reqs` one after the other with the reference (Laplace requests by the real build,
+    Helmholtz ones by the complex build); per request the set-up, assembly, right-hand side and
+    solve seconds, None for requests that the budget left unserved."""
+    import tempfile
+    out, threads = [None] * len(reqs), None
+    with tempfile.TemporaryDirectory() as tmp:
+        path = os.path.join(tmp, "requests.bin")
+        write_requests(path, reqs)
+        for exe in (REF_BENCH, REF_BENCH_CX):
+            if not any(r[0] == (exe == REF_BENCH_CX) for r in reqs):
+                continue
+            r = run_ref(exe, ["requests", path, budget_s])
+            if r is None:
+                continue
+            for q in r["requests"]:
+                out[q["index"]] = q
+            threads = r["threads"]
+    return out, threads
+
+
 def cpu_baseline(a):
-    """Bounded sample: every 8th nearfield block + all bases and coupling, one timed step."""
-    stride = 8
-    r = run_reference(a, 1, 0, stride)
+    """The reference on the host cores (OpenMP + AVX build, all threads): the config-2 assembly of
+    V and K with H2Lib's own drivers on every block (one warm-up step, one timed step) and the
+    GMRES(50) solve; config 3 (Helmholtz BW, k = 2 and 8) assembly and operator applications;
+    config 4 on a sample of the ellipsoids.  The serial config-5 stream is timed in run_serving."""
+    r = run_reference_assembly(a, 1, 1, solve=True)
     if r is None:
         return None
     s = r["steps"][0]
-    return {"value": s["entries"] / s["seconds"], "unit": UNIT, "cores": r["threads"],
-            "kind": "reference",
-            "sample": f"H2Lib (OpenMP+AVX build) assembling V and K on sphere split {a.split}: "
-                      f"all bases and coupling matrices, every {stride}th of {r['near_blocks']} "
-                      f"nearfield blocks ({s['entries']:.0f} entries in {s['seconds']:.2f} s)"}
+    sol = r["solve"]
+    out = {"value": r["entries_per_step"] / s["seconds"], "unit": UNIT, "cores": r["threads"],
+           "kind": "reference",
+           "sample": f"H2Lib OpenMP+AVX build, its own drivers (cluster bases, "
+                     f"assemble_bem3d_nearfield_h2matrix, assemble_bem3d_farfield_h2matrix) on "
+                     f"every block of V and K, sphere split {a.split}: one warm-up step, one timed "
+                     f"step ({r['entries_per_step']:.0f} entries in {s['seconds']:.2f} s)",
+           "phase_s": {k: s[k] for k in ("bases", "nearfield", "farfield")},
+           "solve": {"seconds": sol["seconds"], "solves_per_s": 1.0 / sol["seconds"],
+                     "iterations": sol["iterations"], "matvec_seconds": sol["matvec_seconds"],
+                     "what": "solve_gmres_h2matrix_avector, GMRES(50) to 1e-8 (config 2)"}}
+    if not a.no_helmholtz:
+        hel = []
+        for k in (2.0, 8.0):
+            h = run_ref(REF_BENCH_CX, ["helmholtz", 64, k, 64, 1.4, 5, 1])
+            if h is None:
+                break
+            it = REF_BW_ITERATIONS[k]
+            hel.append({"k": k, "assembly_s": h["assembly"]["seconds"],
+                        "near_entries_per_s": h["entries"] / h["assembly"]["seconds"],
+                        "application_s": h["application_seconds"],
+                        "solve_s_estimate": it * h["application_seconds"],
+                        "solves_per_s_estimate": 1.0 / (it * h["application_seconds"]),
+                        "estimate": f"{it} reference GMRES iterations x one timed "
+                                    "Brakhage-Werner operator application"})
+        out["helmholtz"] = hel
+    if not a.no_batched:
+        work = batched_workload(a.batched_meshes)[:a.cpu_batch_sample]
+        reqs = []
+        from h2lib_b200 import bem3d as hb
+        for split, axes, zs in work:
+            g = hb.new_ellipsoid_surface3d(split, axes)
+            reqs.append((0, 50, 0.0, zs, g.x, g.t))
+        res, _ = run_reference_requests(reqs, 1e9)
+        tot = sum(q["setup"] + q["assembly"] + q["rhs"] + q["solve"] for q in res)
+        ns = sum(q["solves"] for q in res)
+        out["batched"] = {"sample_meshes": len(res), "solves": ns, "seconds": tot,
+                          "solves_per_s": ns / tot,
+                          "what": "first meshes of the config-4 workload, one after the other: "
+                                  "per mesh set-up, assembly of V and K, and 4 GMRES(50) solves"}
+    return out
 
 
 # --------------------------------------------------------------------------------------------
@@ -247,9 +331,12 @@ def run_ours(a, rank, world, local):
         step()
     torch.cuda.synchronize()
     dev_ms, wall_ms, phases = [], [], []
+    import ctypes
+    launches = [ctypes.c_uint64(0), ctypes.c_uint64(0)]
     with ClockSampler(local) as clocks:
         dist_barrier(world)
         torch.cuda.synchronize()
+        check(lib.h2b_launch_count(ctypes.byref(launches[0])), "launch count")
         for _ in range(a.steps):
             flush.fill_(1.0)  # evict L2 between steps
             torch.cuda.synchronize()
@@ -258,6 +345,7 @@ def run_ours(a, rank, world, local):
             wall_ms.append((time.perf_counter() - t0) * 1e3)
             dev_ms.append(dev)
             phases.append((tv, tk))
+        check(lib.h2b_launch_count(ctypes.byref(launches[1])), "launch count")
         torch.cuda.synchronize()
         dist_barrier(world)
     step_ms = dist_max(statistics.mean(dev_ms), world)
@@ -447,7 +535,8 @@ def run_ours(a, rank, world, local):
         "roofline": roofline, "roofline_matvec": roof_mv, "solve": solve, "mixed": mixed,
         "e2e": e2e,
         "clocks": clocks.summary(),
-        "gpu_launches": a.steps * 12,
+        # kernels the library launched in the timed steps (its own launch counter)
+        "gpu_launches": int(launches[1].value - launches[0].value),
     }
     return res
 
@@ -701,6 +790,7 @@ def run_serving(a):
     sweep = [serve(reqs, 8, True, r) for r in rates]
     plain = serve(reqs, 1, False, 0.0, batching=1)
     best = max(s["solves_per_s"] for s in sweep)
+    cpu = None if a.no_cpu_baseline else cpu_serving(a, reqs, rates)
     return {"workload": f"{len(reqs)} requests per rate: sphere/cube/ellipsoid, 512..32768 "
                         f"triangles, Laplace (linear, m 4) or Helmholtz BW (k 1..6, constant, m 5),"
                         f" GMRES to 1e-8 (FP64 residual); seed {BATCH_SEED + 1}",
@@ -708,7 +798,47 @@ def run_serving(a):
                       "Laplace requests batched (forest H2 matrix, batched GMRES)",
             "sweep": sweep,
             "plain_fp64": dict(plain, path="1 slot, FP64, no batching, requests back to back"),
-            "speedup_vs_plain_fp64": best / plain["solves_per_s"]}
+            "speedup_vs_plain_fp64": best / plain["solves_per_s"],
+            "cpu_reference": cpu}
+
+
+def cpu_serving(a, reqs, rates):
+    """The same stream served one request at a time by the reference (OpenMP + AVX build, all
+    host threads): the requests of the stream in arrival order are served until the time budget
+    is spent, and first-in first-out queueing at each arrival rate is replayed from the measured
+    service times (seeded exponential gaps)."""
+    from h2lib_b200.serve import HELMHOLTZ
+    rr = [(1 if pde == HELMHOLTZ else 0, 80 if pde == HELMHOLTZ else 50, k, src, g.x, g.t)
+          for g, pde, src, k in reqs]
+    res, threads = run_reference_requests(rr, a.cpu_serve_budget)
+    served = [i for i, q in enumerate(res) if q is not None]
+    if not served:
+        return None
+    # requests before the first unserved one keep the stream's order
+    prefix = []
+    for i, q in enumerate(res):
+        if q is None:
+            break
+        prefix.append(q["setup"] + q["assembly"] + q["rhs"] + q["solve"])
+    rng = np.random.default_rng(BATCH_SEED + 3)
+    sweep = []
+    for rate in rates:
+        arr = np.cumsum(rng.exponential(1.0 / rate, len(prefix)))
+        done, free = [], 0.0
+        for t_arr, svc in zip(arr, prefix):
+            free = max(free, t_arr) + svc
+            done.append(free)
+        lat = np.array(done) - arr
+        sweep.append({"rate_req_s": rate, "requests": len(prefix),
+                      "solves_per_s": len(prefix) / (done[-1] - arr[0]),
+                      "latency_p50_s": float(np.percentile(lat, 50)),
+                      "latency_p99_s": float(np.percentile(lat, 99))})
+    return {"cores": threads, "kind": "reference", "served": len(served),
+            "service_s": {"median": float(np.median(prefix)), "max": float(np.max(prefix))},
+            "sample": f"the first {len(prefix)} requests of the stream (budget "
+                      f"{a.cpu_serve_budget:.0f} s), one after the other; FIFO queueing replayed "
+                      f"at each rate from the measured service times",
+            "sweep": sweep}
 
 
 def main():
@@ -717,15 +847,13 @@ def main():
     if a.impl == "reference":
         if rank != 0:
             return 0
-        stride = 4
-        r = run_reference(a, a.steps, a.warmup, stride)
+        r = run_reference_assembly(a, a.steps, a.warmup)
         if r is None:
             print(json.dumps({"impl": "reference", "unavailable":
                               "oracle/_ref/ref_bench not built (H2Lib sources absent at build)"}))
             return 0
         secs = [s["seconds"] for s in r["steps"]]
-        ent = r["steps"][0]["entries"]
-        value = ent / statistics.mean(secs)
+        value = r["entries_per_step"] / statistics.mean(secs)
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
                 "steps": a.steps, "warmup": a.warmup,
                 "ms_per_step": statistics.mean(secs) * 1e3, "higher_is_better": True,
@@ -733,8 +861,9 @@ def main():
                 "config": dict(workload(a), parallelism="cpu"), "impl": "reference",
                 "cpu_baseline": {"value": value, "unit": UNIT, "cores": r["threads"],
                                  "kind": "reference",
-                                 "sample": f"every {stride}th of {r['near_blocks']} nearfield "
-                                           f"blocks + all bases and coupling per step"},
+                                 "sample": "every block of V and K per step, H2Lib's own drivers "
+                                           "(cluster bases, assemble_bem3d_nearfield_h2matrix, "
+                                           "assemble_bem3d_farfield_h2matrix), OpenMP+AVX build"},
                 "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
                         "d2h_bytes_per_step": 0}}
         print(json.dumps(line))
