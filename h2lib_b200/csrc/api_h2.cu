@@ -53,16 +53,15 @@ static void devtree_free(DevCTree &t, cudaStream_t st) {
   dfree(t.d_idx, st); dfree(t.d_leaves, st); dfree(t.d_nonroot, st); dfree(t.d_voff, st);
   dfree(t.d_pts, st); dfree(t.d_V, st); dfree(t.d_E, st); dfree(t.d_refs, st);
   dfree(t.d_tr_off, st); dfree(t.d_tr_len, st);
-  dfree(t.d_W, st); dfree(t.d_woff, st); dfree(t.d_fitems, st); dfree(t.d_wleaves, st); dfree(t.d_mitems, st);
+  dfree(t.d_W, st); dfree(t.d_woff, st); dfree(t.d_fitems, st); dfree(t.d_wleaves, st);
   dfree(t.d_seg, st);
 }
 
 // Flattened bases: W_t for the clusters of admissible blocks (`adm`, ids of this tree) and all
 // their descendants (which the products W_f = [W_s E_s] pass through).  Flatten items are
-// grouped by father level, deepest first; matvec items cover the admissible clusters in pieces
-// of at most `item_rows` rows.
+// grouped by father level, deepest first.  W is allocated with H2B_MV_SLACK bytes at its end.
 static int devtree_flat_setup(DevCTree &t, const h2b_ctree &c, const std::vector<uint32_t> &adm,
-                              uint32_t k, uint32_t item_rows, cudaStream_t st) {
+                              uint32_t k, cudaStream_t st) {
   std::vector<char> in_adm(c.n, 0), need(c.n, 0);
   for (uint32_t a : adm) in_adm[a] = 1;
   // pre-order: a father precedes its sons
@@ -76,7 +75,7 @@ static int devtree_flat_setup(DevCTree &t, const h2b_ctree &c, const std::vector
       tot += (uint64_t) c.size[i] * k;
     }
   t.wtotal = tot;
-  std::vector<uint32_t> wleaves, fitems, mitems;
+  std::vector<uint32_t> wleaves, fitems;
   for (uint32_t i = 0; i < c.n; i++)
     if (need[i] && c.sons[i] == 0) wleaves.push_back(i);
   t.fitem_start.assign(c.depth + 1, 0);
@@ -96,23 +95,23 @@ static int devtree_flat_setup(DevCTree &t, const h2b_ctree &c, const std::vector
     }
     t.fitem_count[l] = nitems - t.fitem_start[l];
   }
-  for (uint32_t i = 0; i < c.n; i++)
-    if (in_adm[i])
-      for (uint32_t r0 = 0; r0 < c.size[i]; r0 += item_rows)
-        mitems.insert(mitems.end(), {i, r0, std::min<uint32_t>(item_rows, c.size[i] - r0)});
   t.nwleaves = (uint32_t) wleaves.size();
-  t.nmitems = (uint32_t) (mitems.size() / 3);
+  t.h_woff = woff;
+  t.h_adm = in_adm;
   int rc;
   if ((rc = upload(&t.d_woff, woff, st)) || (rc = upload(&t.d_wleaves, wleaves, st)) ||
-      (rc = upload(&t.d_fitems, fitems, st)) || (rc = upload(&t.d_mitems, mitems, st)))
+      (rc = upload(&t.d_fitems, fitems, st)))
     return rc;
-  H2B_CUDA_TRY(cudaMallocAsync(&t.d_W, sizeof(double) * std::max<uint64_t>(tot, 1), st));
+  H2B_CUDA_TRY(cudaMallocAsync(&t.d_W, sizeof(double) * std::max<uint64_t>(tot, 1) + H2B_MV_SLACK,
+                               st));
   return H2B_OK;
 }
 
-// W from V and E: leaves first, then the father levels from the deepest up.
+// W^T from V and E: leaves first, then the father levels from the deepest up.  `transposed`: the
+// basis stores V^T and E^T (column side); otherwise V and E (row side).
 static int devtree_flatten(DevCTree &t, uint32_t k, int transposed, cudaStream_t st) {
-  FlatLeafArgs la{t.d_wleaves, t.d_size, t.d_voff, t.d_woff, t.d_V, t.d_W, t.nwleaves, (int) k};
+  FlatLeafArgs la{t.d_wleaves, t.d_size, t.d_voff, t.d_woff, t.d_V, t.d_W, t.nwleaves, (int) k,
+                  !transposed};
   int rc = h2b_flat_leaves(&la, st);
   for (int l = (int) t.depth - 1; rc == H2B_OK && l >= 0; l--) {
     FlatArgs fa{t.d_fitems + 4 * (size_t) t.fitem_start[l], t.d_off, t.d_size, t.d_woff, t.d_E,
@@ -149,6 +148,7 @@ static int devtree_build(DevCTree &t, const h2b_ctree &c, int basis, uint32_t m,
     box_points(c.bmin + 3 * (size_t) i, c.bmax + 3 * (size_t) i, m, pts.data() + (size_t) i * 3 * m);
   }
   t.vtotal = vtot;
+  t.h_seg = seg;
   t.nnonroot = (uint32_t) nonroot.size();
   t.nleaves = (uint32_t) leaves.size();
   t.leaves = leaves;
@@ -203,9 +203,10 @@ extern "C" void h2b_h2matrix_del(h2b_h2matrix *h) {
   }
   dfree(h->f_N, st); dfree(h->f_S, st); dfree(h->d_S, st); dfree(h->d_N, st);
   dfree(h->d_xp, st); dfree(h->d_yp, st); dfree(h->d_xt, st); dfree(h->d_yt, st);
-  dfree(h->d_xio, st); dfree(h->d_yio, st);
+  dfree(h->d_xio, st); dfree(h->d_yio, st); dfree(h->d_mverr, st);
   // the structure, unless it belongs to the matrix this one was made like
   if (!h->shared) {
+    for (int i = 0; i < 3; i++) dfree(h->d_items[i], st);
     devtree_free(h->rt, st);
     devtree_free(h->ct, st);
     dfree(h->d_adm_rc, st); dfree(h->d_adm_cc, st);
@@ -345,8 +346,10 @@ extern "C" h2b_h2matrix *h2b_h2matrix_new(const h2b_bem *bem, const h2b_tree *tr
         (rc = upload(&h->d_near_off, noff, h->st)) || (rc = upload(&h->d_tiles, tiles, h->st)) ||
         (rc = upload(&h->d_refs, refs, h->st)) ||
         (rc = classify_singular(h, all_pairs))) {
-    } else if (cudaMallocAsync(&h->d_S, sizeof(double) * W * std::max<uint64_t>((uint64_t) h->nadm * h->k * h->k, 1), h->st) != cudaSuccess ||
-               cudaMallocAsync(&h->d_N, sizeof(double) * W * std::max<uint64_t>(ntot, 1), h->st) != cudaSuccess ||
+    } else if (cudaMallocAsync(&h->d_S, sizeof(double) * W * std::max<uint64_t>((uint64_t) h->nadm * h->k * h->k, 1) + H2B_MV_SLACK, h->st) != cudaSuccess ||
+               cudaMallocAsync(&h->d_N, sizeof(double) * W * std::max<uint64_t>(ntot, 1) + H2B_MV_SLACK, h->st) != cudaSuccess ||
+               cudaMallocAsync(&h->d_mverr, sizeof(int), h->st) != cudaSuccess ||
+               cudaMemsetAsync(h->d_mverr, 0, sizeof(int), h->st) != cudaSuccess ||
                cudaMallocAsync(&h->d_xp, sizeof(double) * W * nc, h->st) != cudaSuccess ||
                cudaMallocAsync(&h->d_yp, sizeof(double) * W * nr, h->st) != cudaSuccess ||
                cudaMallocAsync(&h->d_xt, sizeof(double) * W * h->k * tree->col.n, h->st) != cudaSuccess ||
@@ -359,13 +362,17 @@ extern "C" h2b_h2matrix *h2b_h2matrix_new(const h2b_bem *bem, const h2b_tree *tr
     }
   }
   h2b_nearplan_free(&plan);
-  // flattened bases over the admissible clusters.  Backward items (row side) in short slices:
-  // y rows take one atomic addition per item, and the slices give the backward launch enough
-  // CTAs; forward items (column side) in long ones, since each adds k entries of xt atomically
-  if (rc == H2B_OK)
-    rc = devtree_flat_setup(h->rt, tree->row, arc, h->k, H2B_MVM_BACK_ROWS, h->st);
-  if (rc == H2B_OK)
-    rc = devtree_flat_setup(h->ct, tree->col, acc, h->k, H2B_MVM_FLAT_ROWS, h->st);
+  // flattened bases over the admissible clusters, and the matvec work items
+  if (rc == H2B_OK) rc = devtree_flat_setup(h->rt, tree->row, arc, h->k, h->st);
+  if (rc == H2B_OK) rc = devtree_flat_setup(h->ct, tree->col, acc, h->k, h->st);
+  if (rc == H2B_OK) {
+    h->h_arc = arc;
+    h->h_acc = acc;
+    h->h_nrc = nrc;
+    h->h_ncc = ncc;
+    h->h_noff = noff;
+    rc = h2b_h2_build_mv_items(h);
+  }
   // single-triangle rule (raw and linear-basis weighted)
   if (rc == H2B_OK) {
     const h2b_quad &qd = bem->quad;
@@ -413,6 +420,7 @@ extern "C" h2b_h2matrix *h2b_h2matrix_new_like(const h2b_bem *bem, const h2b_h2m
   h->quad_fp32 = 0;
   h->f_S = h->f_N = nullptr;
   h->d_S = h->d_N = h->d_xp = h->d_yp = h->d_xt = h->d_yt = h->d_xio = h->d_yio = nullptr;
+  h->d_mverr = nullptr;
   for (DevCTree *t : {&h->rt, &h->ct}) t->d_V = t->d_E = t->d_W = nullptr, t->f_W = nullptr;
   int rc = H2B_OK;
   if (cudaStreamCreateWithFlags(&h->st, cudaStreamNonBlocking) != cudaSuccess) rc = H2B_ERR_CUDA;
@@ -426,12 +434,15 @@ extern "C" h2b_h2matrix *h2b_h2matrix_new_like(const h2b_bem *bem, const h2b_h2m
     if (cudaMallocAsync(&t->d_V, sizeof(double) * std::max<uint64_t>(t->vtotal, 1), h->st) ||
         cudaMallocAsync(&t->d_E, sizeof(double) * std::max<uint64_t>((uint64_t) (t->n - 1) * kk, 1),
                         h->st) ||
-        cudaMallocAsync(&t->d_W, sizeof(double) * std::max<uint64_t>(t->wtotal, 1), h->st))
+        cudaMallocAsync(&t->d_W, sizeof(double) * std::max<uint64_t>(t->wtotal, 1) + H2B_MV_SLACK,
+                        h->st))
       rc = H2B_ERR_NOMEM;
   }
   if (rc == H2B_OK &&
-      (cudaMallocAsync(&h->d_S, sizeof(double) * W * std::max<uint64_t>(h->nadm * kk, 1), h->st) ||
-       cudaMallocAsync(&h->d_N, sizeof(double) * W * std::max<uint64_t>(h->near_total, 1), h->st) ||
+      (cudaMallocAsync(&h->d_S, sizeof(double) * W * std::max<uint64_t>(h->nadm * kk, 1) + H2B_MV_SLACK, h->st) ||
+       cudaMallocAsync(&h->d_N, sizeof(double) * W * std::max<uint64_t>(h->near_total, 1) + H2B_MV_SLACK, h->st) ||
+       cudaMallocAsync(&h->d_mverr, sizeof(int), h->st) ||
+       cudaMemsetAsync(h->d_mverr, 0, sizeof(int), h->st) ||
        cudaMallocAsync(&h->d_xp, sizeof(double) * W * nc, h->st) ||
        cudaMallocAsync(&h->d_yp, sizeof(double) * W * nr, h->st) ||
        cudaMallocAsync(&h->d_xt, sizeof(double) * W * h->k * h->ct.n, h->st) ||
@@ -449,6 +460,81 @@ extern "C" h2b_h2matrix *h2b_h2matrix_new_like(const h2b_bem *bem, const h2b_h2m
   return h;
 }
 
+int h2b_h2_check_mv_error(const h2b_h2matrix *h) {
+  int flag = 0;
+  H2B_CUDA_TRY(cudaMemcpyAsync(&flag, h->d_mverr, sizeof(int), cudaMemcpyDeviceToHost, h->st));
+  H2B_CUDA_TRY(cudaStreamSynchronize(h->st));
+  if (flag) {
+    cudaMemsetAsync(h->d_mverr, 0, sizeof(int), h->st);
+    h2b_set_error("matvec: a panel copy to shared memory did not complete (bounded wait)");
+    return H2B_ERR_TIMEOUT;
+  }
+  return H2B_OK;
+}
+
+int h2b_h2_build_mv_items(h2b_h2matrix *h) {
+  const h2b_ctree &R = h->tree->row, &C = h->tree->col;
+  const uint32_t k = h->k, W = h->cx ? 2 : 1;
+  std::vector<MvItem> ph[3];
+  // rows per slice of a flattened basis: the knob, at most one panel of H2B_MV_PANEL_BYTES
+  auto slice_rows = [&](uint32_t want) {
+    const uint32_t cap = std::max<uint32_t>(1, H2B_MV_PANEL_BYTES / (8u * k));
+    return std::max<uint32_t>(1, std::min(want, cap));
+  };
+  // columns per panel of a block with `rows` rows and complex entries when W = 2
+  auto panel_cols = [&](uint32_t rows) {
+    return std::max<uint32_t>(1, H2B_MV_PANEL_BYTES / (8u * W * std::max<uint32_t>(rows, 1)));
+  };
+  // 1a: forward slices, x_t -> xt_t, over every admissible column cluster
+  const uint32_t fr = slice_rows(h->mv_fwd_rows), br = slice_rows(h->mv_back_rows);
+  for (uint32_t t = 0; t < C.n; t++) {
+    if (!h->ct.h_adm[t]) continue;
+    for (uint32_t r0 = 0; r0 < C.size[t]; r0 += fr)
+      ph[0].push_back(MvItem{h->ct.h_woff[t] + (uint64_t) r0 * k, k,
+                             std::min(fr, C.size[t] - r0), C.off[t] + r0, k * t, h->ct.h_seg[t],
+                             0u});
+  }
+  // 1b: nearfield blocks, in column panels
+  for (size_t b = 0; b < h->h_nrc.size(); b++) {
+    const uint32_t r = h->h_nrc[b], c = h->h_ncc[b], rows = R.size[r], cols = C.size[c];
+    const uint32_t pc = panel_cols(rows);
+    for (uint32_t c0 = 0; c0 < cols; c0 += pc)
+      ph[0].push_back(MvItem{h->h_noff[b] + (uint64_t) c0 * rows, rows, std::min(pc, cols - c0),
+                             C.off[c] + c0, R.off[r], h->rt.h_seg[r], H2B_MV_SRC1});
+  }
+  // 2: coupling blocks, in column panels
+  for (size_t b = 0; b < h->h_arc.size(); b++) {
+    const uint32_t r = h->h_arc[b], c = h->h_acc[b], pc = panel_cols(k);
+    for (uint32_t c0 = 0; c0 < k; c0 += pc)
+      ph[1].push_back(MvItem{(uint64_t) b * k * k + (uint64_t) c0 * k, k, std::min(pc, k - c0),
+                             k * c + c0, k * r, h->rt.h_seg[r], H2B_MV_SRC1});
+  }
+  // 3: backward slices, yt_t -> y_t (W_t^T transposed), over every admissible row cluster
+  for (uint32_t t = 0; t < R.n; t++) {
+    if (!h->rt.h_adm[t]) continue;
+    for (uint32_t r0 = 0; r0 < R.size[t]; r0 += br)
+      ph[2].push_back(MvItem{h->rt.h_woff[t] + (uint64_t) r0 * k, k,
+                             std::min(br, R.size[t] - r0), k * t, R.off[t] + r0, h->rt.h_seg[t],
+                             H2B_MV_TRANS});
+  }
+  for (int i = 0; i < 3; i++) {
+    dfree(h->d_items[i], h->st);
+    int rc = upload(&h->d_items[i], ph[i], h->st);
+    if (rc != H2B_OK) return rc;
+    MvPhase &m = h->mvph[i];
+    m.items = h->d_items[i];
+    m.n = (uint32_t) ph[i].size();
+    m.max_bytes = 0;
+    m.max_rows = 0;
+    for (const MvItem &it : ph[i]) {
+      const uint32_t esz = 8u * ((it.flags & H2B_MV_SRC1) ? W : 1u);
+      m.max_bytes = std::max<uint32_t>(m.max_bytes, it.rows * it.cols * esz);
+      if (!(it.flags & H2B_MV_TRANS)) m.max_rows = std::max(m.max_rows, it.rows);
+    }
+  }
+  return H2B_OK;
+}
+
 void h2b_h2_fill_mvm_plan(h2b_h2matrix *h) {
   MvmPlan &p = h->mvm;
   memset(&p, 0, sizeof(p));
@@ -458,48 +544,26 @@ void h2b_h2_fill_mvm_plan(h2b_h2matrix *h) {
   p.nrow = h->rt.nidx;
   p.ncol = h->ct.nidx;
   p.nrow_clusters = h->rt.n;
+  p.ncol_clusters = h->ct.n;
   p.ridx = h->rt.d_idx;
   p.cidx = h->ct.d_idx;
   p.xp = h->d_xp;
   p.yp = h->d_yp;
   p.xt = h->d_xt;
   p.yt = h->d_yt;
-  MvmCoupleArgs &c = p.cpl;
-  c.adm_rc = h->d_adm_rc;
-  c.adm_cc = h->d_adm_cc;
-  c.S = h->d_S;
-  c.near_rc = h->d_near_rc;
-  c.near_cc = h->d_near_cc;
-  c.near_off = h->d_near_off;
-  c.N = h->d_N;
-  c.Ss = h->f_S;
-  c.Ns = h->f_N;
-  c.rsize = h->rt.d_size;
-  c.csize = h->ct.d_size;
-  c.roff = h->rt.d_off;
-  c.coff = h->ct.d_off;
-  c.xt = h->d_xt;
-  c.xp = h->d_xp;
-  c.yt = h->d_yt;
-  c.yp = h->d_yp;
-  c.nadm = h->nadm;
-  c.nnear = h->nnear;
-  c.k = (int) h->k;
-  p.rseg = h->rt.d_seg;
-  p.cseg = h->ct.d_seg;
-  p.ncol_clusters = h->ct.n;
-  for (int side = 0; side < 2; side++) {
-    const DevCTree &t = side ? h->rt : h->ct;
-    MvmFlatArgs &f = side ? p.fbwd : p.ffwd;
-    f.items = t.d_mitems;
-    f.off = t.d_off;
-    f.size = t.d_size;
-    f.woff = t.d_woff;
-    f.W = t.d_W;
-    f.Ws = t.f_W;
-    f.nitems = t.nmitems;
-    f.k = (int) h->k;
-  }
+  for (int i = 0; i < 3; i++) p.ph[i] = h->mvph[i];
+  p.Wc = h->ct.d_W;
+  p.Wr = h->rt.d_W;
+  p.N = h->d_N;
+  p.S = h->d_S;
+  p.fWc = h->ct.f_W;
+  p.fWr = h->rt.f_W;
+  p.fN = h->f_N;
+  p.fS = h->f_S;
+  p.err = h->d_mverr;
+  p.ctas_per_sm = h->mv_ctas;
+  p.stages = h->mv_stages;
+  h2b_mvm_prepare();
 }
 
 // ------------------------------------------------------------------------------------------
@@ -571,10 +635,11 @@ extern "C" int h2b_h2matrix_make_single(h2b_h2matrix *h) {
   drop_single(h);
   const uint64_t W = h->cx ? 2 : 1;
   const uint64_t nN = W * h->near_total, nS = W * (uint64_t) h->nadm * h->k * h->k;
-  if (cudaMallocAsync(&h->f_N, sizeof(float) * std::max<uint64_t>(nN, 1), h->st) != cudaSuccess ||
-      cudaMallocAsync(&h->f_S, sizeof(float) * std::max<uint64_t>(nS, 1), h->st) != cudaSuccess ||
-      cudaMallocAsync(&h->rt.f_W, sizeof(float) * std::max<uint64_t>(h->rt.wtotal, 1), h->st) != cudaSuccess ||
-      cudaMallocAsync(&h->ct.f_W, sizeof(float) * std::max<uint64_t>(h->ct.wtotal, 1), h->st) != cudaSuccess) {
+  const size_t sl = H2B_MV_SLACK;
+  if (cudaMallocAsync(&h->f_N, sizeof(float) * std::max<uint64_t>(nN, 1) + sl, h->st) != cudaSuccess ||
+      cudaMallocAsync(&h->f_S, sizeof(float) * std::max<uint64_t>(nS, 1) + sl, h->st) != cudaSuccess ||
+      cudaMallocAsync(&h->rt.f_W, sizeof(float) * std::max<uint64_t>(h->rt.wtotal, 1) + sl, h->st) != cudaSuccess ||
+      cudaMallocAsync(&h->ct.f_W, sizeof(float) * std::max<uint64_t>(h->ct.wtotal, 1) + sl, h->st) != cudaSuccess) {
     cudaGetLastError();
     drop_single(h);
     h2b_set_error("h2b_h2matrix_make_single: device allocation failed");
@@ -925,6 +990,7 @@ static int addeval_prec(double alpha_re, double alpha_im, const h2b_h2matrix *h,
     h2b_set_error("h2b_h2matrix_addeval: %s", cudaGetErrorString(cudaGetLastError()));
     rc = H2B_ERR_CUDA;
   }
+  if (rc == H2B_OK) rc = h2b_h2_check_mv_error(h);
   float t;
   if (rc == H2B_OK && cudaEventElapsedTime(&t, h->ev[9], h->ev[10]) == cudaSuccess)
     const_cast<h2b_h2matrix *>(h)->ms[5] = t;

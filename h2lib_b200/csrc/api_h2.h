@@ -27,9 +27,11 @@ struct DevCTree {
   uint64_t wtotal = 0;
   uint32_t *d_fitems = nullptr;  // flatten items (4 uint32 each), grouped by father level
   uint32_t *d_wleaves = nullptr; // leaves that carry a W (W_leaf = V_leaf)
-  uint32_t *d_mitems = nullptr;  // matvec items (3 uint32 each) over the admissible clusters
   std::vector<uint32_t> fitem_start, fitem_count;  // flatten items of father level l
-  uint32_t nwleaves = 0, nmitems = 0;
+  uint32_t nwleaves = 0;
+  std::vector<uint64_t> h_woff;  // host copy of d_woff
+  std::vector<char> h_adm;       // 1: the cluster belongs to an admissible block
+  std::vector<uint32_t> h_seg;   // host copy of d_seg
   float *f_W = nullptr;  // FP32 copy of W (h2b_h2matrix_make_single)
   // surfaces of a forest: the surface of every cluster (device) and the roots (host)
   uint32_t *d_seg = nullptr;
@@ -43,6 +45,18 @@ struct h2b_h2matrix {
   uint32_t m = 0, k = 0, ns = 0;
   int cx = 0, num_sms = 148;
   int quad_fp32 = 0;  // distant-pair quadrature in FP32 (h2b_h2matrix_set_precision)
+  // matvec work items of the three launches (h2mvm.h), owned by the structure's owner, and the
+  // knobs they were built with: rows per forward / backward slice; CTAs per SM and stages of the
+  // item kernel
+  MvItem *d_items[3] = {nullptr, nullptr, nullptr};
+  MvPhase mvph[3] = {};
+  uint32_t mv_fwd_rows = 64, mv_back_rows = 64;
+  int mv_ctas = 2, mv_stages = 3;
+  int *d_mverr = nullptr;  // the item kernel's error flag (one per matrix)
+  // host copies of the block lists: admissible (row, column cluster), nearfield (row, column
+  // cluster, offset of the block in N)
+  std::vector<uint32_t> h_arc, h_acc, h_nrc, h_ncc;
+  std::vector<uint64_t> h_noff;
   // 1: the tree, block and nearfield-plan arrays belong to another matrix (h2b_h2matrix_new_like);
   // only the operator's own data (bases, transfers, W, S, N, work vectors) are freed here
   int shared = 0;
@@ -74,5 +88,11 @@ struct h2b_h2matrix {
 };
 
 void h2b_h2_fill_mvm_plan(h2b_h2matrix *h);
+// (Re)build the matvec work items from the structure and the matrix's slice knobs (owner only).
+int h2b_h2_build_mv_items(h2b_h2matrix *h);
+// H2B_ERR_TIMEOUT (and the flag cleared) if a matvec of h lost a panel copy; synchronises h->st.
+int h2b_h2_check_mv_error(const h2b_h2matrix *h);
+// Bytes of slack after every panel array: a panel copy may read up to 15 bytes past its panel.
+#define H2B_MV_SLACK 64
 int h2b_h2_addeval_dev(const h2b_h2matrix *h, double ar, double ai, const double *dx, double *dy,
                        cudaStream_t st);

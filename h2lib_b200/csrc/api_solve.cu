@@ -124,7 +124,7 @@ static int solve_segments(Combo &combo, uint32_t nseg, const uint32_t *seg_off, 
   combo.nrhs = nrhs;
   if (mixed)
     for (uint32_t i = 0; i < combo.nterms; i++)
-      if (!combo.ops[i]->mvm.cpl.Ss) {
+      if (!combo.ops[i]->mvm.fS) {
         h2b_set_error("%s: operator %u has no FP32 copy (h2b_h2matrix_make_single)", who, i);
         return H2B_ERR_ARG;
       }
@@ -194,6 +194,8 @@ static int solve_segments(Combo &combo, uint32_t nseg, const uint32_t *seg_off, 
   }
   H2B_CUDA_TRY(cudaMemcpyAsync(x, dx, sizeof(double) * W * n, cudaMemcpyDefault, st));
   H2B_CUDA_TRY(cudaStreamSynchronize(st));
+  for (uint32_t i = 0; i < combo.nterms; i++)
+    if ((rc = h2b_h2_check_mv_error(combo.ops[i])) != H2B_OK) return rc;
   return H2B_OK;
 }
 

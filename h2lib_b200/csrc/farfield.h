@@ -54,7 +54,7 @@ struct FlatArgs {
   double *W;
   uint32_t nitems;
   int k;
-  int transposed;            // column side: W^T stored k x |t|
+  int e_transposed;          // E stored transposed (column side: E^T); W^T is k x |t| always
 };
 
 struct FlatLeafArgs {
@@ -64,6 +64,7 @@ struct FlatLeafArgs {
   double *W;
   uint32_t nleaves;
   int k;
+  int transpose;             // V stored |t| x k (row side): W^T = V^T is written
 };
 
 extern "C" int h2b_flat_leaves(const FlatLeafArgs *a, cudaStream_t st);

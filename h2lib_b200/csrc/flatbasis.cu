@@ -7,9 +7,10 @@
 // multiplied out once after assembly).  With W the forward transform is xt_t = W_t^T x_t and the
 // backward transform y_t += W_t yt_t for all clusters at once: no level-to-level dependence, so
 // the matvec streams W at HBM bandwidth instead of climbing the tree one level per step.
-// Row bases are stored like V (|t| x k, column-major, ld = |t|); column bases transposed like V^T
-// (k x |t|, ld = k), the layouts the matvec reads with consecutive threads on consecutive
-// addresses.
+// Both sides store W transposed (W^T: k x |t|, column-major, ld = k), so that a slice of rows of
+// t is one contiguous panel that the matvec copies to shared memory in one bulk transfer.  The
+// column basis keeps V and E transposed as well (V^T, E^T); the row basis keeps them as H2Lib
+// does (V: |t| x k, E: k x k), and its leaves are transposed on the copy into W.
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -44,7 +45,7 @@ __device__ __forceinline__ void cta_copy(double *dst, size_t n, F src) {
 // up to FLAT_COLS consecutive columns nu of the product (one part for k <= 64); the nr rows of
 // W_s times those columns of E_s land in the rows of s inside W_f.  Short row slices give every
 // level's launch enough CTAs and read each son's rows once; E_s is read by every slice of the son
-// (from L2).
+// (from L2).  W^T is stored k x |t| (ld k) on both sides.
 constexpr int FLAT_COLS = 64;
 __global__ void __launch_bounds__(FLAT_TPB) flatten_kernel(FlatArgs a) {
   extern __shared__ double sm[];
@@ -54,104 +55,65 @@ __global__ void __launch_bounds__(FLAT_TPB) flatten_kernel(FlatArgs a) {
   const uint32_t *it = a.items + 4 * (size_t) item;
   const uint32_t f = it[0], s = it[1], r0 = it[2], nr = it[3];
   const uint32_t c0 = part * FLAT_COLS, nc = min((uint32_t) FLAT_COLS, k - c0);
-  double *sE = sm;                  // k x FLAT_COLS: sE[mu + j k] = E_s[mu, c0 + j]
-  double *sW = sm + k * FLAT_COLS;  // W_s[r0 + i, mu]: sW[i + mu nr] (row side), sW[mu + i (k + 1)]
-                                    // (column side)
+  double *sE = sm;                  // sE[j + mu nc] = E_s[mu, c0 + j]
+  double *sW = sm + k * FLAT_COLS;  // W_s[r0 + i, mu] at sW[mu + i (k + 1)]
   const double *E = a.E + (size_t) (s - 1) * k * k;
-  const uint32_t ns = a.size[s], nf = a.size[f];
   const uint32_t rf = a.off[s] - a.off[f] + r0;  // first row inside f
   const double *Ws = a.W + a.woff[s];
   double *Wf = a.W + a.woff[f];
-  if (!a.transposed) {
-    // E_s column-major: the part's columns are contiguous
-    cta_copy(sE, (size_t) k * nc, [&](size_t e) { return E[(size_t) c0 * k + e]; });
-    cta_copy(sW, (size_t) nr * k, [&](size_t e) {
-      const uint32_t i = (uint32_t) (e % nr), mu = (uint32_t) (e / nr);
-      return Ws[r0 + i + (size_t) mu * ns];
-    });
-  } else {
-    // E_s^T column-major (k x k): E_s[mu, nu] = E^T[nu + mu k]; the part's rows of each column
-    // of E^T, kept nu-major: sE[j + mu nc] = E_s[mu, c0 + j]
-    for (uint32_t e = threadIdx.x; e < k * nc; e += blockDim.x) {
-      const uint32_t j = e % nc, mu = e / nc;
-      sE[j + mu * nc] = E[c0 + j + (size_t) mu * k];
-    }
-    // W_s^T (k x |s|, ld k) is contiguous over the item's rows: sW[mu + i (k + 1)] (padded
-    // stride, so that a warp's rows fall in different banks)
-    for (uint32_t e = threadIdx.x; e < nr * k; e += blockDim.x) {
-      const uint32_t mu = e % k, i = e / k;
-      sW[mu + i * (k + 1)] = Ws[(size_t) r0 * k + e];
-    }
+  // E_s from E^T (column side: E_s[mu, nu] = E^T[nu + mu k]) or from E itself (row side:
+  // E_s[mu, nu] = E[mu + nu k])
+  for (uint32_t e = threadIdx.x; e < k * nc; e += blockDim.x) {
+    const uint32_t j = e % nc, mu = e / nc;
+    sE[j + mu * nc] = a.e_transposed ? E[c0 + j + (size_t) mu * k] : E[mu + (size_t) (c0 + j) * k];
+  }
+  // W_s^T (k x |s|, ld k) is contiguous over the item's rows: sW[mu + i (k + 1)] (padded stride,
+  // so that a warp's rows fall in different banks)
+  for (uint32_t e = threadIdx.x; e < nr * k; e += blockDim.x) {
+    const uint32_t mu = e % k, i = e / k;
+    sW[mu + i * (k + 1)] = Ws[(size_t) r0 * k + e];
   }
   __syncthreads();
-  // row side: 16 row lanes x 16 column quads; column side: 64 column lanes x 4 row groups
-  static_assert(FLAT_TPB / 16 * 4 == FLAT_COLS && H2B_FLAT_ROWS % 16 == 0, "thread mapping");
+  // thread = column j = t % 64, rows ig + 4 r (ig = t / 64); a warp writes 32 consecutive nu of
+  // one row of W_f^T
   static_assert(FLAT_TPB / FLAT_COLS == 4 && H2B_FLAT_ROWS % 4 == 0, "thread mapping");
-  if (!a.transposed) {
-    // row side: thread = rows i0 + 16 r (i0 = t % 16), columns 4 (t / 16) .. + 3; a warp
-    // writes 16 consecutive rows of four columns per store
-    constexpr int RS = H2B_FLAT_ROWS / 16;
-    const uint32_t i0 = threadIdx.x % 16, jq = 4 * (threadIdx.x / 16);
-    if (i0 < nr && jq < nc) {
-      double acc[RS][4];
+  constexpr int RC = H2B_FLAT_ROWS / 4;
+  const uint32_t j = threadIdx.x % FLAT_COLS, ig = threadIdx.x / FLAT_COLS;
+  if (j < nc) {
+    double acc[RC];
 #pragma unroll
-      for (int r = 0; r < RS; r++)
-#pragma unroll
-        for (int q = 0; q < 4; q++) acc[r][q] = 0.0;
-      for (uint32_t mu = 0; mu < k; mu++) {
-        double e[4];
-#pragma unroll
-        for (int q = 0; q < 4; q++) e[q] = sE[mu + (jq + q) * k];
-#pragma unroll
-        for (int r = 0; r < RS; r++) {
-          const uint32_t i = i0 + 16u * r;
-          const double x = i < nr ? sW[i + mu * nr] : 0.0;
-#pragma unroll
-          for (int q = 0; q < 4; q++) acc[r][q] = fma(x, e[q], acc[r][q]);
-        }
-      }
-#pragma unroll
-      for (int r = 0; r < RS; r++) {
-        const uint32_t i = i0 + 16u * r;
-        if (i < nr)
-#pragma unroll
-          for (int q = 0; q < 4; q++)
-            if (jq + q < nc) Wf[rf + i + (size_t) (c0 + jq + q) * nf] = acc[r][q];
-      }
-    }
-  } else {
-    // column side (W^T stored k x |t|): thread = column j = t % 64, rows ig + 4 r (ig = t / 64);
-    // a warp writes 32 consecutive nu of one row
-    constexpr int RC = H2B_FLAT_ROWS / 4;
-    const uint32_t j = threadIdx.x % FLAT_COLS, ig = threadIdx.x / FLAT_COLS;
-    if (j < nc) {
-      double acc[RC];
-#pragma unroll
-      for (int r = 0; r < RC; r++) acc[r] = 0.0;
-      for (uint32_t mu = 0; mu < k; mu++) {
-        const double y = sE[j + mu * nc];
-#pragma unroll
-        for (int r = 0; r < RC; r++) {
-          const uint32_t i = ig + 4u * r;
-          if (i < nr) acc[r] = fma(sW[mu + i * (k + 1)], y, acc[r]);
-        }
-      }
+    for (int r = 0; r < RC; r++) acc[r] = 0.0;
+    for (uint32_t mu = 0; mu < k; mu++) {
+      const double y = sE[j + mu * nc];
 #pragma unroll
       for (int r = 0; r < RC; r++) {
         const uint32_t i = ig + 4u * r;
-        if (i < nr) Wf[(size_t) (rf + i) * k + c0 + j] = acc[r];
+        if (i < nr) acc[r] = fma(sW[mu + i * (k + 1)], y, acc[r]);
       }
+    }
+#pragma unroll
+    for (int r = 0; r < RC; r++) {
+      const uint32_t i = ig + 4u * r;
+      if (i < nr) Wf[(size_t) (rf + i) * k + c0 + j] = acc[r];
     }
   }
 }
 
-// W_leaf = V_leaf (same layout on both sides).
+// W_leaf^T from V_leaf: a copy when V is stored transposed (column side), a transposition when V
+// is stored |t| x k (row side).
 __global__ void __launch_bounds__(FLAT_TPB) leaf_copy_kernel(FlatLeafArgs a) {
   const uint32_t l = a.leaves[blockIdx.x];
-  const size_t n = (size_t) a.size[l] * a.k;
+  const uint32_t nt = a.size[l], k = (uint32_t) a.k;
+  const size_t n = (size_t) nt * k;
   const double *src = a.V + a.voff[l];
   double *dst = a.W + a.woff[l];
-  cta_copy(dst, n, [&](size_t e) { return src[e]; });
+  if (a.transpose)
+    cta_copy(dst, n, [&](size_t e) {  // dst[nu + i k] = V[i + nu nt]
+      const uint32_t nu = (uint32_t) (e % k), i = (uint32_t) (e / k);
+      return src[i + (size_t) nu * nt];
+    });
+  else
+    cta_copy(dst, n, [&](size_t e) { return src[e]; });
 }
 
 // out[i] = (float) in[i] (round to nearest)

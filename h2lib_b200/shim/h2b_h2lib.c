@@ -479,7 +479,13 @@ static double *export_part(const h2b_h2matrix *h, int part, uint64_t *n) {
     fprintf(stderr, "h2b_h2lib: out of host memory\n");
     abort();
   }
-  check(h2b_h2matrix_export(h, part, UINT32_MAX, buf, NULL), "h2b_h2matrix_export");
+  uint64_t got = 0;
+  check(h2b_h2matrix_export(h, part, UINT32_MAX, buf, &got), "h2b_h2matrix_export");
+  if (got != *n) {
+    fprintf(stderr, "h2b_h2lib: export of part %d returned %llu of %llu values\n", part,
+            (unsigned long long) got, (unsigned long long) *n);
+    abort();
+  }
   return buf;
 }
 

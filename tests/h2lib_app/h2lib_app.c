@@ -9,8 +9,9 @@
  *
  * Real build (Laplace): sphere refined x8, dense cc single layer; linear-basis single and double
  * layer H2 matrices (leaf 16, eta 1.4, m 3), products, and the interior Dirichlet GMRES(50) solve.
- * Complex build (Helmholtz, k = 2): the same sphere, constant basis, single layer H2 matrix
- * (leaf 16, eta 1.4, m 3), products, a dense block fill and a GMRES solve of V.
+ * Complex build (Helmholtz, k = 2): the same sphere, constant basis: a single-layer block through
+ * the nearfield callback, the dense double layer, single and double layer H2 matrices (leaf 16,
+ * eta 1.4, m 3), products and a GMRES solve of V.
  *
  * usage: h2lib_app <outdir>
  */
@@ -200,12 +201,18 @@ int main(int argc, char **argv) {
         new_dlp_helmholtz_bem3d(k, gr, 2, 4, BASIS_CONSTANT_BEM3D, BASIS_CONSTANT_BEM3D, 0.5);
     ph2matrix V, K;
     pavector x, u;
-    pamatrix B = new_amatrix(7, 5);
+    pamatrix B = new_amatrix(7, 5), A = new_amatrix(gr->triangles, gr->triangles);
     uint ridx[7] = {5, 9, 20, 33, 2, 61, 40}, cidx[5] = {1, 40, 2, 60, 65};
-    /* one block through the nearfield callback (the plugin point) */
-    dlp->nearfield(ridx, cidx, dlp, false, B);
-    dump_mat("block_dlp", B);
+    /* one block of the single layer through the nearfield callback (the plugin point); the
+     * double layer's identity term is placed differently by H2Lib when a triangle appears at
+     * different positions of ridx and cidx (assemble_cc_near_bem3d writes aa[t + t ld]), so the
+     * double layer is compared on the whole matrix */
+    slp->nearfield(ridx, cidx, slp, false, B);
+    dump_mat("block_slp", B);
+    assemble_bem3d_amatrix(dlp, A);
+    dump_mat("dense_dlp_cc", A);
     del_amatrix(B);
+    del_amatrix(A);
     root = build_bem3d_cluster(slp, 16, BASIS_CONSTANT_BEM3D);
     broot = build_strict_block(root, root, &eta, admissible_max_cluster);
     V = h2_of(slp, root, broot, 3);

@@ -12,8 +12,8 @@ Compared (the tolerances of the other GPU parity tests):
   * solve_gmres_h2matrix_avector and solve_gmres_avector with addeval_h2matrix_avector: iteration
     count within one (the device GMRES applies the Householder reflectors in another order) and
     solution to 1e-6;
-  * the Helmholtz build: a block through the bem->nearfield plugin point, the products and a GMRES
-    solve of the single layer operator;
+  * the Helmholtz build: a single-layer block through the bem->nearfield plugin point, the dense
+    double layer matrix, the products and a GMRES solve of the single layer operator;
 and the shim's counters show that the device did the work.
 """
 import os
@@ -66,9 +66,12 @@ def test_h2lib_program_through_the_shim(field):
         assert abs(gpu["gmres_iter2"][0] - cpu["gmres_iter2"][0]) <= 1
         assert relerr(gpu["u2"], cpu["u2"]) < 1e-6
     else:
-        b = cpu["block_dlp"].reshape(5, 7).T
-        assert rel_entry_err(gpu["block_dlp"].reshape(5, 7).T, b) < 1e-12
+        b = cpu["block_slp"].reshape(5, 7).T
+        assert rel_entry_err(gpu["block_slp"].reshape(5, 7).T, b) < 1e-12
         assert counts[0] >= 1  # the nearfield callback ran on the device
+        n = int(np.sqrt(cpu["dense_dlp_cc"].size))
+        a = gpu["dense_dlp_cc"].reshape(n, n).T
+        assert rel_entry_err(a, cpu["dense_dlp_cc"].reshape(n, n).T) < 1e-12
     for op in ("V", "K"):
         assert relerr(gpu[f"y{op}"], cpu[f"y{op}"]) < 1e-12
         assert relerr(gpu[f"y{op}_acc"], cpu[f"y{op}_acc"]) < 1e-12
