@@ -87,6 +87,8 @@ _SIGS = {
                                         C.c_uint32]),
     "h2b_h2matrix_make_single": (C.c_int, [vp]),
     "h2b_h2matrix_set_precision": (C.c_int, [vp, C.c_int]),
+    "h2b_h2matrix_set_matvec_shape": (C.c_int, [vp, _u32p]),
+    "h2b_h2matrix_get_matvec_shape": (C.c_int, [vp, _u32p]),
     "h2b_h2matrix_addeval_single": (C.c_int, [C.c_double, C.c_double, vp, vp, vp]),
     "h2b_residual_norm": (C.c_int, [C.c_uint32, vp, _f64p, vp, vp, C.POINTER(C.c_double)]),
     "h2b_solve_gmres_noalloc": (C.c_int, [C.c_uint32, vp, _f64p, vp, vp, C.c_double,

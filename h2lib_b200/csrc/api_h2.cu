@@ -206,7 +206,7 @@ extern "C" void h2b_h2matrix_del(h2b_h2matrix *h) {
   dfree(h->d_xio, st); dfree(h->d_yio, st); dfree(h->d_mverr, st);
   // the structure, unless it belongs to the matrix this one was made like
   if (!h->shared) {
-    for (int i = 0; i < 3; i++) dfree(h->d_items[i], st);
+    dfree(h->d_items, st);
     devtree_free(h->rt, st);
     devtree_free(h->ct, st);
     dfree(h->d_adm_rc, st); dfree(h->d_adm_cc, st);
@@ -350,10 +350,10 @@ extern "C" h2b_h2matrix *h2b_h2matrix_new(const h2b_bem *bem, const h2b_tree *tr
                cudaMallocAsync(&h->d_N, sizeof(double) * W * std::max<uint64_t>(ntot, 1) + H2B_MV_SLACK, h->st) != cudaSuccess ||
                cudaMallocAsync(&h->d_mverr, sizeof(int), h->st) != cudaSuccess ||
                cudaMemsetAsync(h->d_mverr, 0, sizeof(int), h->st) != cudaSuccess ||
-               cudaMallocAsync(&h->d_xp, sizeof(double) * W * nc, h->st) != cudaSuccess ||
+               cudaMallocAsync(&h->d_xp, sizeof(double) * W * nc + H2B_MV_SLACK, h->st) != cudaSuccess ||
                cudaMallocAsync(&h->d_yp, sizeof(double) * W * nr, h->st) != cudaSuccess ||
-               cudaMallocAsync(&h->d_xt, sizeof(double) * W * h->k * tree->col.n, h->st) != cudaSuccess ||
-               cudaMallocAsync(&h->d_yt, sizeof(double) * W * h->k * tree->row.n, h->st) != cudaSuccess ||
+               cudaMallocAsync(&h->d_xt, sizeof(double) * W * h->k * tree->col.n + H2B_MV_SLACK, h->st) != cudaSuccess ||
+               cudaMallocAsync(&h->d_yt, sizeof(double) * W * h->k * tree->row.n + H2B_MV_SLACK, h->st) != cudaSuccess ||
                cudaMallocAsync(&h->d_xio, sizeof(double) * W * nc, h->st) != cudaSuccess ||
                cudaMallocAsync(&h->d_yio, sizeof(double) * W * nr, h->st) != cudaSuccess) {
       h2b_set_error("h2b_h2matrix_new: device allocation failed: %s",
@@ -443,10 +443,10 @@ extern "C" h2b_h2matrix *h2b_h2matrix_new_like(const h2b_bem *bem, const h2b_h2m
        cudaMallocAsync(&h->d_N, sizeof(double) * W * std::max<uint64_t>(h->near_total, 1) + H2B_MV_SLACK, h->st) ||
        cudaMallocAsync(&h->d_mverr, sizeof(int), h->st) ||
        cudaMemsetAsync(h->d_mverr, 0, sizeof(int), h->st) ||
-       cudaMallocAsync(&h->d_xp, sizeof(double) * W * nc, h->st) ||
+       cudaMallocAsync(&h->d_xp, sizeof(double) * W * nc + H2B_MV_SLACK, h->st) ||
        cudaMallocAsync(&h->d_yp, sizeof(double) * W * nr, h->st) ||
-       cudaMallocAsync(&h->d_xt, sizeof(double) * W * h->k * h->ct.n, h->st) ||
-       cudaMallocAsync(&h->d_yt, sizeof(double) * W * h->k * h->rt.n, h->st) ||
+       cudaMallocAsync(&h->d_xt, sizeof(double) * W * h->k * h->ct.n + H2B_MV_SLACK, h->st) ||
+       cudaMallocAsync(&h->d_yt, sizeof(double) * W * h->k * h->rt.n + H2B_MV_SLACK, h->st) ||
        cudaMallocAsync(&h->d_xio, sizeof(double) * W * nc, h->st) ||
        cudaMallocAsync(&h->d_yio, sizeof(double) * W * nr, h->st)))
     rc = H2B_ERR_NOMEM;
@@ -475,62 +475,66 @@ int h2b_h2_check_mv_error(const h2b_h2matrix *h) {
 int h2b_h2_build_mv_items(h2b_h2matrix *h) {
   const h2b_ctree &R = h->tree->row, &C = h->tree->col;
   const uint32_t k = h->k, W = h->cx ? 2 : 1;
-  std::vector<MvItem> ph[3];
-  // rows per slice of a flattened basis: the knob, at most one panel of H2B_MV_PANEL_BYTES
+  // items ordered by kind: forward, nearfield, coupling, backward (the matvec runs the first two
+  // kinds in one launch, then the coupling, then the backward slices)
+  std::vector<MvItem> it;
+  uint32_t start[4] = {0, 0, 0, 0};
+  const uint32_t pb = h->mv_panel_bytes;
   auto slice_rows = [&](uint32_t want) {
-    const uint32_t cap = std::max<uint32_t>(1, H2B_MV_PANEL_BYTES / (8u * k));
+    const uint32_t cap = std::max<uint32_t>(1, pb / (8u * k));
     return std::max<uint32_t>(1, std::min(want, cap));
   };
   // columns per panel of a block with `rows` rows and complex entries when W = 2
   auto panel_cols = [&](uint32_t rows) {
-    return std::max<uint32_t>(1, H2B_MV_PANEL_BYTES / (8u * W * std::max<uint32_t>(rows, 1)));
+    return std::max<uint32_t>(1, pb / (8u * W * std::max<uint32_t>(rows, 1)));
   };
-  // 1a: forward slices, x_t -> xt_t, over every admissible column cluster
   const uint32_t fr = slice_rows(h->mv_fwd_rows), br = slice_rows(h->mv_back_rows);
+  // forward slices, x_t -> xt_t, over every admissible column cluster
   for (uint32_t t = 0; t < C.n; t++) {
     if (!h->ct.h_adm[t]) continue;
     for (uint32_t r0 = 0; r0 < C.size[t]; r0 += fr)
-      ph[0].push_back(MvItem{h->ct.h_woff[t] + (uint64_t) r0 * k, k,
-                             std::min(fr, C.size[t] - r0), C.off[t] + r0, k * t, h->ct.h_seg[t],
-                             0u});
+      it.push_back(MvItem{h->ct.h_woff[t] + (uint64_t) r0 * k, k, std::min(fr, C.size[t] - r0),
+                          C.off[t] + r0, k * t, h->ct.h_seg[t], H2B_MV_FORWARD});
   }
-  // 1b: nearfield blocks, in column panels
+  // nearfield blocks, in column panels
+  start[H2B_MV_NEAR] = (uint32_t) it.size();
   for (size_t b = 0; b < h->h_nrc.size(); b++) {
     const uint32_t r = h->h_nrc[b], c = h->h_ncc[b], rows = R.size[r], cols = C.size[c];
     const uint32_t pc = panel_cols(rows);
     for (uint32_t c0 = 0; c0 < cols; c0 += pc)
-      ph[0].push_back(MvItem{h->h_noff[b] + (uint64_t) c0 * rows, rows, std::min(pc, cols - c0),
-                             C.off[c] + c0, R.off[r], h->rt.h_seg[r], H2B_MV_SRC1});
+      it.push_back(MvItem{h->h_noff[b] + (uint64_t) c0 * rows, rows, std::min(pc, cols - c0),
+                          C.off[c] + c0, R.off[r], h->rt.h_seg[r], H2B_MV_NEAR});
   }
-  // 2: coupling blocks, in column panels
+  // coupling blocks, in column panels
+  start[H2B_MV_COUPLING] = (uint32_t) it.size();
   for (size_t b = 0; b < h->h_arc.size(); b++) {
     const uint32_t r = h->h_arc[b], c = h->h_acc[b], pc = panel_cols(k);
     for (uint32_t c0 = 0; c0 < k; c0 += pc)
-      ph[1].push_back(MvItem{(uint64_t) b * k * k + (uint64_t) c0 * k, k, std::min(pc, k - c0),
-                             k * c + c0, k * r, h->rt.h_seg[r], H2B_MV_SRC1});
+      it.push_back(MvItem{(uint64_t) b * k * k + (uint64_t) c0 * k, k, std::min(pc, k - c0),
+                          k * c + c0, k * r, h->rt.h_seg[r], H2B_MV_COUPLING});
   }
-  // 3: backward slices, yt_t -> y_t (W_t^T transposed), over every admissible row cluster
+  // backward slices, yt_t -> y_t (W_t^T transposed), over every admissible row cluster
+  start[H2B_MV_BACKWARD] = (uint32_t) it.size();
   for (uint32_t t = 0; t < R.n; t++) {
     if (!h->rt.h_adm[t]) continue;
     for (uint32_t r0 = 0; r0 < R.size[t]; r0 += br)
-      ph[2].push_back(MvItem{h->rt.h_woff[t] + (uint64_t) r0 * k, k,
-                             std::min(br, R.size[t] - r0), k * t, R.off[t] + r0, h->rt.h_seg[t],
-                             H2B_MV_TRANS});
+      it.push_back(MvItem{h->rt.h_woff[t] + (uint64_t) r0 * k, k, std::min(br, R.size[t] - r0),
+                          k * t, R.off[t] + r0, h->rt.h_seg[t], H2B_MV_BACKWARD | H2B_MV_TRANS});
   }
-  for (int i = 0; i < 3; i++) {
-    dfree(h->d_items[i], h->st);
-    int rc = upload(&h->d_items[i], ph[i], h->st);
-    if (rc != H2B_OK) return rc;
-    MvPhase &m = h->mvph[i];
-    m.items = h->d_items[i];
-    m.n = (uint32_t) ph[i].size();
-    m.max_bytes = 0;
-    m.max_rows = 0;
-    for (const MvItem &it : ph[i]) {
-      const uint32_t esz = 8u * ((it.flags & H2B_MV_SRC1) ? W : 1u);
-      m.max_bytes = std::max<uint32_t>(m.max_bytes, it.rows * it.cols * esz);
-      if (!(it.flags & H2B_MV_TRANS)) m.max_rows = std::max(m.max_rows, it.rows);
-    }
+  dfree(h->d_items, h->st);
+  int rc;
+  if ((rc = upload(&h->d_items, it, h->st))) return rc;
+  MvItems &m = h->mvitems;
+  m.items = h->d_items;
+  m.n = (uint32_t) it.size();
+  for (int q = 0; q < 4; q++) m.start[q] = start[q];
+  m.max_bytes = m.max_rows = m.max_x = 0;
+  for (const MvItem &e : it) {
+    const uint32_t kind = e.flags & H2B_MV_KIND;
+    const bool cpx = kind == H2B_MV_NEAR || kind == H2B_MV_COUPLING;
+    m.max_bytes = std::max<uint32_t>(m.max_bytes, e.rows * e.cols * 8u * (cpx ? W : 1u));
+    if (!(e.flags & H2B_MV_TRANS)) m.max_rows = std::max(m.max_rows, e.rows);
+    m.max_x = std::max(m.max_x, (e.flags & H2B_MV_TRANS) ? e.rows : e.cols);
   }
   return H2B_OK;
 }
@@ -551,7 +555,7 @@ void h2b_h2_fill_mvm_plan(h2b_h2matrix *h) {
   p.yp = h->d_yp;
   p.xt = h->d_xt;
   p.yt = h->d_yt;
-  for (int i = 0; i < 3; i++) p.ph[i] = h->mvph[i];
+  p.items = h->mvitems;
   p.Wc = h->ct.d_W;
   p.Wr = h->rt.d_W;
   p.N = h->d_N;
@@ -593,6 +597,7 @@ static int assemble_basis(h2b_h2matrix *h, DevCTree &t, int basis, int dn) {
   la.m = (int) h->m;
   la.k = (int) h->k;
   la.ns = (int) h->ns;
+  la.split = std::max(1, std::min((int) h->k, h->leaf_split));
   int rc = h2b_far_leaf_basis(&la, basis == H2B_BASIS_LINEAR, dn, h->st);
   if (rc != H2B_OK) return rc;
   FarTransferArgs ta{t.d_nonroot, t.d_father, t.d_pts, t.d_E, t.nnonroot, (int) h->m, (int) h->k,
@@ -627,6 +632,49 @@ extern "C" int h2b_h2matrix_set_precision(h2b_h2matrix *h, int precision) {
     return H2B_ERR_ARG;
   }
   h->quad_fp32 = precision == H2B_FP32;
+  return H2B_OK;
+}
+
+extern "C" int h2b_h2matrix_set_matvec_shape(h2b_h2matrix *h, const uint32_t shape[H2B_SHAPE_N]) {
+  if (!h || !shape) return H2B_ERR_ARG;
+  const uint32_t fr = shape[0] ? shape[0] : h->mv_fwd_rows;
+  const uint32_t br = shape[1] ? shape[1] : h->mv_back_rows;
+  const uint32_t pb = shape[4] ? shape[4] * 1024u : h->mv_panel_bytes;
+  if (shape[2] > 8 || shape[3] > 8 || (shape[3] && shape[3] < 2) ||
+      (shape[4] && (shape[4] < 4 || shape[4] > 64)) || shape[5] > h->k) {
+    h2b_set_error("h2b_h2matrix_set_matvec_shape: CTAs per SM <= 8, stages 2..8, panels 4..64 "
+                  "KiB, leaf CTAs <= k");
+    return H2B_ERR_ARG;
+  }
+  if (fr != h->mv_fwd_rows || br != h->mv_back_rows || pb != h->mv_panel_bytes) {
+    if (h->shared) {
+      h2b_set_error("h2b_h2matrix_set_matvec_shape: slice and panel sizes belong to the shared "
+                    "structure");
+      return H2B_ERR_STATE;
+    }
+    H2B_CUDA_TRY(cudaStreamSynchronize(h->st));  // no product reads the old items
+    h->mv_fwd_rows = fr;
+    h->mv_back_rows = br;
+    h->mv_panel_bytes = pb;
+    int rc = h2b_h2_build_mv_items(h);
+    if (rc != H2B_OK) return rc;
+    H2B_CUDA_TRY(cudaStreamSynchronize(h->st));
+  }
+  if (shape[2]) h->mv_ctas = (int) shape[2];
+  if (shape[3]) h->mv_stages = (int) shape[3];
+  if (shape[5]) h->leaf_split = (int) shape[5];
+  h2b_h2_fill_mvm_plan(h);
+  return H2B_OK;
+}
+
+extern "C" int h2b_h2matrix_get_matvec_shape(const h2b_h2matrix *h, uint32_t shape[H2B_SHAPE_N]) {
+  if (!h || !shape) return H2B_ERR_ARG;
+  shape[0] = h->mv_fwd_rows;
+  shape[1] = h->mv_back_rows;
+  shape[2] = (uint32_t) h->mv_ctas;
+  shape[3] = (uint32_t) h->mv_stages;
+  shape[4] = h->mv_panel_bytes / 1024u;
+  shape[5] = (uint32_t) h->leaf_split;
   return H2B_OK;
 }
 

@@ -45,13 +45,15 @@ struct h2b_h2matrix {
   uint32_t m = 0, k = 0, ns = 0;
   int cx = 0, num_sms = 148;
   int quad_fp32 = 0;  // distant-pair quadrature in FP32 (h2b_h2matrix_set_precision)
-  // matvec work items of the three launches (h2mvm.h), owned by the structure's owner, and the
-  // knobs they were built with: rows per forward / backward slice; CTAs per SM and stages of the
-  // item kernel
-  MvItem *d_items[3] = {nullptr, nullptr, nullptr};
-  MvPhase mvph[3] = {};
+  // matvec work items (h2mvm.h), owned by the structure's owner, and the knobs they were built
+  // with: rows per forward / backward slice, largest panel; CTAs per SM and stages of the item
+  // kernel
+  MvItem *d_items = nullptr;
+  MvItems mvitems = {};
   uint32_t mv_fwd_rows = 64, mv_back_rows = 64;
-  int mv_ctas = 2, mv_stages = 3;
+  int mv_ctas = 3, mv_stages = 2;
+  uint32_t mv_panel_bytes = H2B_MV_PANEL_BYTES;
+  int leaf_split = 2;  // CTAs per leaf of the leaf-basis kernel (each a range of the k columns)
   int *d_mverr = nullptr;  // the item kernel's error flag (one per matrix)
   // host copies of the block lists: admissible (row, column cluster), nearfield (row, column
   // cluster, offset of the block in N)

@@ -55,8 +55,8 @@ __device__ __forceinline__ double dlagr_bar(double x, const double *xi, double w
 }
 
 // Leaf bases.  Rows of leaf c: its triangles (constant basis) or vertices (linear basis).  A
-// leaf's nu range is split over LEAF_SPLIT CTAs (CTA (leaf, part) computes the columns
-// [part k / LEAF_SPLIT, ...)), so that the launch has several CTAs per SM.  The CTA's triangle
+// leaf's nu range is split over a.split CTAs (CTA (leaf, part) computes the columns
+// [part k / split, ...)), so that the launch has several CTAs per SM.  The CTA's triangle
 // list (TriRef, local row indices) is processed in batches of BATCH triangles: first the
 // one-dimensional Lagrange values (and derivatives) at every quadrature point of the batch are
 // tabulated in shared memory (3 axes x m), then each (triangle, nu) work item forms the tensor
@@ -65,26 +65,23 @@ __device__ __forceinline__ double dlagr_bar(double x, const double *xi, double w
 // around it) and written once.
 constexpr int BATCH = 32;
 constexpr int NSMAX = 64;   // single-triangle rule points (q^2, q <= 8)
-#ifndef H2B_LEAF_SPLIT
-#define H2B_LEAF_SPLIT 2
-#endif
-constexpr int LEAF_SPLIT = H2B_LEAF_SPLIT;
 
 template <bool LINEAR, bool DN>
 __global__ void __launch_bounds__(256) leaf_basis_kernel(FarLeafArgs a) {
   extern __shared__ double smem[];
   __shared__ double wbar[3][MMAX];
-  const uint32_t leaf = blockIdx.x / LEAF_SPLIT, part = blockIdx.x % LEAF_SPLIT;
+  const uint32_t split = (uint32_t) a.split;
+  const uint32_t leaf = blockIdx.x / split, part = blockIdx.x % split;
   const uint32_t c = a.leaves[leaf];
   const int m = a.m, k = a.k;
-  const int nu0 = (int) ((part * (uint32_t) k) / LEAF_SPLIT);
-  const int nu1 = (int) (((part + 1) * (uint32_t) k) / LEAF_SPLIT);
+  const int nu0 = (int) ((part * (uint32_t) k) / split);
+  const int nu1 = (int) (((part + 1) * (uint32_t) k) / split);
   const int kp = nu1 - nu0;
   const uint32_t rows = a.size[c];
   const uint32_t tr0 = a.tr_off[leaf], ntr = a.tr_len[leaf];
   const double *pts = a.pts + (size_t) c * 3 * m;
   const int ns = a.ns;
-  const int kpmax = (k + LEAF_SPLIT - 1) / LEAF_SPLIT;
+  const int kpmax = (k + (int) split - 1) / (int) split;
   double *V = smem;                                   // rows * kp (the CTA's columns)
   double *tab = V + (size_t) rows * kpmax;            // BATCH * ns * 3 * m
   double *dtab = tab + (size_t) BATCH * ns * 3 * m;   // same size (derivatives, DN only)
@@ -246,7 +243,11 @@ __global__ void __launch_bounds__(256) coupling_kernel(FarCouplingArgs a) {
 
 extern "C" int h2b_far_leaf_basis(const FarLeafArgs *a, int linear, int dn, cudaStream_t st) {
   if (a->nleaves == 0) return H2B_OK;
-  const size_t smem = sizeof(double) * ((size_t) a->max_rows * ((a->k + LEAF_SPLIT - 1) / LEAF_SPLIT) +
+  if (a->split < 1 || a->split > a->k) {
+    h2b_set_error("leaf basis: %d CTAs per leaf outside 1..%d", a->split, a->k);
+    return H2B_ERR_ARG;
+  }
+  const size_t smem = sizeof(double) * ((size_t) a->max_rows * ((a->k + a->split - 1) / a->split) +
                                         2 * (size_t) BATCH * a->ns * 3 * a->m);
   if (smem > 200u * 1024u || a->ns > NSMAX) {
     h2b_set_error("leaf basis block of %u x %d (rule of %d points) exceeds shared memory",
@@ -256,7 +257,7 @@ extern "C" int h2b_far_leaf_basis(const FarLeafArgs *a, int linear, int dn, cuda
 #define LAUNCH(L, D)                                                                        \
   do {                                                                                      \
     H2B_CUDA_TRY((h2b_allow_smem<leaf_basis_kernel<L, D>>()));                             \
-    leaf_basis_kernel<L, D><<<a->nleaves * LEAF_SPLIT, 256, smem, st>>>(*a);                \
+    leaf_basis_kernel<L, D><<<a->nleaves * (uint32_t) a->split, 256, smem, st>>>(*a);     \
     h2b_note_launch();                                                                      \
   } while (0)
   if (linear && dn) LAUNCH(true, true);

@@ -21,6 +21,7 @@ struct FarLeafArgs {
   uint32_t nleaves, max_rows;
   int m, k, ns;
   int transposed;           // store V^T (k x rows) instead of V (rows x k)
+  int split;                // CTAs per leaf (each a contiguous range of the k columns), 1..k
 };
 
 struct FarTransferArgs {

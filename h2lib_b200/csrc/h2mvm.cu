@@ -9,21 +9,23 @@
 // t's own indices, stored transposed (k x |t|).  The forward transform is then xt_t = W_t^T x_t
 // and the backward transform y_t += W_t yt_t for every such cluster independently.
 //
-// Every product is a list of small dense GEMV work items (h2mvm.h: MvItem) in three launches:
-//   1. forward + nearfield: xt_t += (W_t^T slice) x_slice, and y_r += N_b x_c;
-//   2. coupling: yt_r += S_b xt_c;
-//   3. backward: y_slice += (W_t^T slice)^T yt_t;
-// between a gather (xp = x[idx], accumulators cleared) and a scatter (y[idx] += alpha yp).
-// Vectors are kept in cluster order, so every item's x and y are contiguous slices.
+// Every product is a list of small dense GEMV work items (h2mvm.h: MvItem), ordered by kind and
+// run by three launches of one persistent kernel between a gather (xp = x[idx], accumulators
+// cleared) and a scatter (y[idx] += alpha yp):
+//   1. forward     xt_t += (W_t^T slice) x_slice,   and nearfield   y_r += N_b x_c
+//   2. coupling    yt_r += S_b xt_c
+//   3. backward    y_slice += (W_t^T slice)^T yt_t
+// Vectors are kept in cluster order, so every item's x and y are contiguous slices.  (Running
+// all three in one launch, with counters per cluster carrying the dependences, measured slower:
+// the counter and claim atomics cost more than the two launch boundaries.)
 //
-// The item kernel is persistent (a few CTAs per SM, items taken round-robin) and streams each
-// item's panel — a contiguous column-major block of N, S or W^T — into a ring of shared-memory
-// stages with one bulk asynchronous copy (cp.async.bulk global -> shared, completion counted on
-// an mbarrier per stage), so that several panels per SM are in flight while the GEMV of an
-// earlier one runs from shared memory.  The copies are local to this GPU and have no cluster
-// multicast.  Every wait on a stage is bounded: on time-out the kernel sets the plan's error
-// flag, waits (bounded) for its copies in flight and returns.  Partial sums reach their outputs
-// with FP64 atomics (an output row is shared by several items).
+// The kernel streams each item's panel — a contiguous column-major block of N, S or W^T — and its
+// x slice into a ring of shared-memory stages with bulk asynchronous copies (cp.async.bulk
+// global -> shared, completion counted on an mbarrier per stage), issued by a producer warp, so
+// that several panels per SM are in flight while consumer warps multiply earlier ones from
+// shared memory.  The copies are local to this GPU and have no cluster multicast.  Every wait is
+// bounded: on time-out the kernel sets the plan's error flag, waits (bounded) for its copies in
+// flight and returns.  Partial sums reach their outputs with FP64 atomics.
 // CX: complex coefficients (Helmholtz) — S, N, x, y complex (interleaved); W real.
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -104,16 +106,19 @@ __global__ void scatter_multi_kernel(MvmVecs v, const uint32_t *__restrict__ idx
 struct MvLaunch {
   const MvItem *items;
   uint32_t n;
-  const void *A[2];        // panel arrays: A[0] real; A[1] complex pairs when CX
-  const double *X[2];      // x work vectors of the two triples
-  double *Y[2];            // y work vectors
-  size_t sx[2], sy[2];     // column strides (doubles)
+  const void *A[4];        // panel array per kind: W_c^T, N, S, W_r^T (N, S complex when CX)
+  const double *X[4];      // x work vector per kind
+  double *Y[4];            // y work vector per kind
+  size_t sx[4], sy[4];     // column strides (doubles)
+  uint32_t first;          // the launch's items: first .. first + n - 1 of the list
   uint32_t nrhs, nseg;
   const uint32_t *mask;
   int *err;
   uint32_t stage_bytes;    // bytes per stage (multiple of 128)
+  uint32_t panel_bytes;    // panel region of a stage; the x slices of every column follow
+  uint32_t xcol_bytes;     // bytes per x slice of one column (multiple of 16, with slack)
   uint32_t stages;
-  uint32_t red_doubles;    // cross-warp reduction buffer
+  uint32_t red_doubles;    // one of the two cross-warp reduction buffers
 };
 
 __device__ __forceinline__ uint32_t smem_addr(const void *p) {
@@ -137,17 +142,27 @@ __device__ __forceinline__ bool bar_wait(uint32_t bar, uint32_t parity) {
   return false;
 }
 
-// Panel of item m: first byte (16-byte aligned, at or before the panel) and byte count (a
-// multiple of 16 that covers the panel).  The arrays carry 64 bytes of slack at their end.
+// [lo, lo + bytes): the 16-byte aligned span that covers [addr, addr + n); delta = addr - lo.
+// The arrays and work vectors carry at least 16 bytes of slack after their ends.
+__device__ __forceinline__ void span16(const void *addr, size_t n, const char *&lo,
+                                       uint32_t &delta, uint32_t &bytes) {
+  const uintptr_t a = reinterpret_cast<uintptr_t>(addr);
+  lo = reinterpret_cast<const char *>(a & ~(uintptr_t) 15);
+  delta = (uint32_t) (a & 15u);
+  bytes = (uint32_t) ((delta + n + 15) & ~(size_t) 15);
+}
+
+// complex panel entries: nearfield and coupling panels of a complex operator
+__device__ __forceinline__ bool complex_panel(uint32_t kind) {
+  return kind == H2B_MV_NEAR || kind == H2B_MV_COUPLING;
+}
+
 template <bool CX, typename T>
-__device__ __forceinline__ void panel_span(const MvLaunch &L, const MvItem &m, const char *&src,
-                                           uint32_t &delta, uint32_t &bytes) {
-  const int s = m.flags & H2B_MV_SRC1;
-  const size_t esz = sizeof(T) * ((CX && s) ? 2 : 1);
-  const char *addr = reinterpret_cast<const char *>(L.A[s]) + m.p * esz;
-  src = reinterpret_cast<const char *>(reinterpret_cast<uintptr_t>(addr) & ~(uintptr_t) 15);
-  delta = (uint32_t) (addr - src);
-  bytes = (uint32_t) ((delta + (size_t) m.rows * m.cols * esz + 15) & ~(size_t) 15);
+__device__ __forceinline__ const char *panel_addr(const MvLaunch &L, const MvItem &m, size_t &n) {
+  const uint32_t kind = m.flags & H2B_MV_KIND;
+  const size_t esz = sizeof(T) * ((CX && complex_panel(kind)) ? 2 : 1);
+  n = (size_t) m.rows * m.cols * esz;
+  return reinterpret_cast<const char *>(L.A[kind]) + m.p * esz;
 }
 
 template <bool PCX, typename T>
@@ -161,19 +176,25 @@ __device__ __forceinline__ void entry(const T *P, size_t e, double &re, double &
   }
 }
 
-// y[0, R) += P x[0, C) from the panel in shared memory: warps take columns, lanes rows; the
-// warps' partial sums meet in `red` and reach y with one atomic addition per row.
-template <bool CX, bool PCX, typename T>
-__device__ __forceinline__ void gemv_n(const T *P, uint32_t R, uint32_t C, const double *x,
-                                       double *y, double *red) {
+// Named barrier of the consumer warps (barrier 0 stays __syncthreads').
+__device__ __forceinline__ void consumers_sync() {
+  asm volatile("bar.sync 1, %0;" ::"r"(NWARP * 32) : "memory");
+}
+
+// y[0, R) += P x[0, C) from the stage: warps take columns, lanes rows; the warps' partial sums
+// meet in `red` (after a consumer barrier) and reach y with one atomic addition per row.
+// `release` is called when the warp has read the stage for the last time.
+template <bool CX, bool PCX, typename T, typename F>
+__device__ __forceinline__ void gemv_n(const T *P, uint32_t R, uint32_t C, const double *xs,
+                                       double *y, double *red, F release) {
   constexpr int W = CX ? 2 : 1;
   const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
   double sr[MAXROWS / 32], si[MAXROWS / 32];
 #pragma unroll
   for (int j = 0; j < MAXROWS / 32; j++) sr[j] = si[j] = 0.0;
-#pragma unroll 2
+#pragma unroll 4
   for (uint32_t c = warp; c < C; c += NWARP) {
-    const double xr = __ldg(x + W * c), xi = CX ? __ldg(x + W * c + 1) : 0.0;
+    const double xr = xs[W * c], xi = CX ? xs[W * c + 1] : 0.0;
 #pragma unroll
     for (int j = 0; j < MAXROWS / 32; j++) {
       const uint32_t r = lane + 32u * j;
@@ -190,6 +211,7 @@ __device__ __forceinline__ void gemv_n(const T *P, uint32_t R, uint32_t C, const
       }
     }
   }
+  release();
 #pragma unroll
   for (int j = 0; j < MAXROWS / 32; j++) {
     const uint32_t r = lane + 32u * j;
@@ -198,32 +220,33 @@ __device__ __forceinline__ void gemv_n(const T *P, uint32_t R, uint32_t C, const
       if (CX) red[W * (warp * R + r) + 1] = si[j];
     }
   }
-  __syncthreads();
-  for (uint32_t r = threadIdx.x; r < R; r += blockDim.x) {
+  consumers_sync();
+  for (uint32_t r = threadIdx.x; r < R; r += NWARP * 32) {
     double ar = 0.0, ai = 0.0;
 #pragma unroll
     for (int w = 0; w < NWARP; w++) {
       ar += red[W * (w * R + r)];
       if (CX) ai += red[W * (w * R + r) + 1];
     }
-    atomicAdd(y + W * r, ar);
-    if (CX) atomicAdd(y + W * r + 1, ai);
+    if (y) {
+      atomicAdd(y + W * r, ar);
+      if (CX) atomicAdd(y + W * r + 1, ai);
+    }
   }
-  __syncthreads();  // red is reused
 }
 
 // y[0, C) += P^T x[0, R) for a real panel: a warp per column, lanes over the rows, shuffle sums.
-template <bool CX, typename T>
-__device__ __forceinline__ void gemv_t(const T *P, uint32_t R, uint32_t C, const double *x,
-                                       double *y) {
+template <bool CX, typename T, typename F>
+__device__ __forceinline__ void gemv_t(const T *P, uint32_t R, uint32_t C, const double *xs,
+                                       double *y, F release) {
   constexpr int W = CX ? 2 : 1;
   const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
   double xr[MAXROWS / 32], xi[MAXROWS / 32];
 #pragma unroll
   for (int j = 0; j < MAXROWS / 32; j++) {
     const uint32_t r = lane + 32u * j;
-    xr[j] = r < R ? __ldg(x + W * r) : 0.0;
-    xi[j] = (CX && r < R) ? __ldg(x + W * r + 1) : 0.0;
+    xr[j] = r < R ? xs[W * r] : 0.0;
+    xi[j] = (CX && r < R) ? xs[W * r + 1] : 0.0;
   }
   for (uint32_t c = warp; c < C; c += NWARP) {
     double sr = 0.0, si = 0.0;
@@ -243,112 +266,228 @@ __device__ __forceinline__ void gemv_t(const T *P, uint32_t R, uint32_t C, const
       if (CX) atomicAdd(y + W * c + 1, si);
     }
   }
+  release();
 }
 
+// Warp NWARP produces: for each of the CTA's items (first + blockIdx.x + i gridDim.x) it copies
+// the panel and the x slice of every right-hand side into stage i % S (one bulk copy each,
+// completion on full[s]) after the consumers have released the stage's previous contents
+// (empty[s]), and puts the descriptor in the stage's slot (a sentinel after the last item).
+// Warps 0 .. NWARP-1 consume: wait on full[s], agree on the outcome (barrier with an OR vote, so
+// that all of them stop or none), multiply, release the stage, and combine their partial sums
+// (one consumer barrier per product; the reduction buffer alternates between products).
 template <bool CX, typename T>
-__global__ void __launch_bounds__(TPB) mv_items_kernel(MvLaunch L) {
+__global__ void __launch_bounds__(TPB + 32) mv_items_kernel(MvLaunch L) {
   extern __shared__ __align__(128) unsigned char smem[];
+  constexpr int W = CX ? 2 : 1;
   const uint32_t S = L.stages;
   unsigned char *stage0 = smem;
   double *red = reinterpret_cast<double *>(smem + (size_t) S * L.stage_bytes);
-  uint64_t *bars = reinterpret_cast<uint64_t *>(red + L.red_doubles);
-  // items of this CTA: blockIdx.x + i gridDim.x
-  const uint32_t mine = L.n > blockIdx.x ? (L.n - blockIdx.x + gridDim.x - 1) / gridDim.x : 0u;
+  MvItem *slot = reinterpret_cast<MvItem *>(red + 2 * (size_t) L.red_doubles);
+  uint64_t *full = reinterpret_cast<uint64_t *>(slot + S);
+  uint64_t *empty = full + S;
+  const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
   if (threadIdx.x == 0) {
-    for (uint32_t s = 0; s < S; s++)
-      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&bars[s])));
+    for (uint32_t s = 0; s < S; s++) {
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&full[s])));
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(&empty[s])),
+                   "r"(NWARP));
+    }
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   __syncthreads();
-  auto issue = [&](uint32_t i) {  // thread 0: the copy of this CTA's i-th item into stage i % S
-    const MvItem m = L.items[blockIdx.x + i * gridDim.x];
-    const char *src;
-    uint32_t delta, bytes;
-    panel_span<CX, T>(L, m, src, delta, bytes);
-    const uint32_t bar = smem_addr(&bars[i % S]);
-    const uint32_t dst = smem_addr(stage0 + (size_t) (i % S) * L.stage_bytes);
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes)
-                 : "memory");
-    asm volatile(
-        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
-        ::"r"(dst), "l"(src), "r"(bytes), "r"(bar)
-        : "memory");
-  };
-  if (threadIdx.x == 0)
-    for (uint32_t i = 0; i < S && i < mine; i++) issue(i);
 
-  for (uint32_t i = 0; i < mine; i++) {
-    const uint32_t s = i % S;
-    const bool ok = bar_wait(smem_addr(&bars[s]), (i / S) & 1u);
-    if (__syncthreads_or(!ok)) {
-      // a copy did not complete: flag it, wait (bounded) for the copies still in flight, stop
-      if (threadIdx.x == 0) {
-        atomicExch(L.err, 1);
-        for (uint32_t j = i; j < i + S && j < mine; j++)
-          bar_wait(smem_addr(&bars[j % S]), (j / S) & 1u);
+  if (warp == NWARP) {
+    // ---- producer (one lane): this CTA's items first + blockIdx.x + i gridDim.x, the next
+    // descriptor fetched while the current copies run
+    if (lane != 0) return;
+    const uint32_t mine =
+        L.n > blockIdx.x ? (L.n - blockIdx.x + gridDim.x - 1) / gridDim.x : 0u;
+    MvItem m;
+    if (mine) m = L.items[L.first + blockIdx.x];
+    uint32_t i = 0;
+    bool ok = true;
+    for (;; i++) {
+      const uint32_t s = i % S;
+      if (i >= S && !(ok = bar_wait(smem_addr(&empty[s]), ((i / S) - 1) & 1u))) break;
+      const uint32_t bar = smem_addr(&full[s]);
+      if (i >= mine) {
+        slot[s].flags = H2B_MV_NONE;  // sentinel: no more items
+        asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
+        break;
       }
+      slot[s] = m;
+      size_t n;
+      const char *pa = panel_addr<CX, T>(L, m, n), *lo;
+      uint32_t delta, bytes;
+      span16(pa, n, lo, delta, bytes);
+      const int t = m.flags & H2B_MV_KIND;
+      const size_t xn = (size_t) W * sizeof(double) * ((m.flags & H2B_MV_TRANS) ? m.rows : m.cols);
+      uint32_t total = bytes;
+      for (uint32_t q = 0; q < L.nrhs; q++) {
+        const char *xl;
+        uint32_t xd, xb;
+        span16(L.X[t] + q * L.sx[t] + (size_t) W * m.xo, xn, xl, xd, xb);
+        total += xb;
+      }
+      const uint32_t dst = smem_addr(stage0 + (size_t) s * L.stage_bytes);
+      // the generic-proxy reads of the stage's previous contents are ordered before these copies
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(total)
+                   : "memory");
+      asm volatile(
+          "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+          ::"r"(dst), "l"(lo), "r"(bytes), "r"(bar)
+          : "memory");
+      for (uint32_t q = 0; q < L.nrhs; q++) {
+        const char *xl;
+        uint32_t xd, xb;
+        span16(L.X[t] + q * L.sx[t] + (size_t) W * m.xo, xn, xl, xd, xb);
+        asm volatile(
+            "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+            ::"r"(dst + L.panel_bytes + q * L.xcol_bytes), "l"(xl), "r"(xb), "r"(bar)
+            : "memory");
+      }
+      if (i + 1 < mine) m = L.items[L.first + blockIdx.x + (i + 1) * gridDim.x];
+    }
+    if (!ok) {
+      // a wait ran out: flag it and wait (bounded) for the copies this warp issued before it
+      // leaves the CTA's shared memory (the consumers stop at their next stage)
+      atomicExch(L.err, 1);
+      for (uint32_t j = i > S ? i - S : 0; j < i; j++)
+        bar_wait(smem_addr(&full[j % S]), (j / S) & 1u);
+    }
+    return;
+  }
+
+  // ---- consumers
+  uint32_t nred = 0;  // gemv_n calls so far: the reduction buffer alternates between calls
+  for (uint32_t i = 0;; i++) {
+    const uint32_t s = i % S;
+    const bool ok = bar_wait(smem_addr(&full[s]), (i / S) & 1u);
+    // every consumer thread takes part: all of them stop, or none
+    uint32_t any_lost;
+    asm volatile("{\n .reg .pred p, q;\n setp.eq.u32 p, %1, 0;\n"
+                 " bar.red.or.pred q, 1, %2, p;\n selp.u32 %0, 1, 0, q;\n}"
+                 : "=r"(any_lost)
+                 : "r"((uint32_t) ok), "r"(NWARP * 32)
+                 : "memory");
+    if (any_lost) {
+      if (threadIdx.x == 0) atomicExch(L.err, 1);
       return;
     }
-    const MvItem m = L.items[blockIdx.x + i * gridDim.x];
-    const char *src;
+    const MvItem m = slot[s];
+    if (m.flags == H2B_MV_NONE) return;  // the list is exhausted
+    const unsigned char *stage = stage0 + (size_t) s * L.stage_bytes;
+    size_t n;
+    const char *pa = panel_addr<CX, T>(L, m, n), *lo;
     uint32_t delta, bytes;
-    panel_span<CX, T>(L, m, src, delta, bytes);
-    const unsigned char *panel = stage0 + (size_t) s * L.stage_bytes + delta;
-    const int t = m.flags & H2B_MV_SRC1;
-    for (uint32_t q = 0; q < L.nrhs; q++) {
-      if (!col_on(L.mask, L.nseg, m.seg, q)) continue;
-      const double *x = L.X[t] + q * L.sx[t] + (size_t) (CX ? 2 : 1) * m.xo;
-      double *y = L.Y[t] + q * L.sy[t] + (size_t) (CX ? 2 : 1) * m.yo;
-      if (m.flags & H2B_MV_TRANS) {
-        gemv_t<CX>(reinterpret_cast<const T *>(panel), m.rows, m.cols, x, y);
-      } else if (CX && t) {
-        gemv_n<CX, CX>(reinterpret_cast<const T *>(panel), m.rows, m.cols, x, y, red);
-      } else {
-        gemv_n<CX, false>(reinterpret_cast<const T *>(panel), m.rows, m.cols, x, y, red);
+    span16(pa, n, lo, delta, bytes);
+    const T *P = reinterpret_cast<const T *>(stage + delta);
+    const int t = m.flags & H2B_MV_KIND;
+    // columns whose system is done are skipped; the stage is released after the last one used
+    uint32_t last = L.nrhs;
+    for (uint32_t q = L.nrhs; q-- > 0;)
+      if (col_on(L.mask, L.nseg, m.seg, q)) {
+        last = q;
+        break;
       }
+    auto release_now = [&]() {
+      __syncwarp();
+      if (lane == 0)
+        asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(&empty[s]))
+                     : "memory");
+    };
+    auto keep = [] {};
+    if (last == L.nrhs) {
+      release_now();
+      continue;
     }
-    __syncthreads();  // every thread is done with stage s
-    if (threadIdx.x == 0 && i + S < mine) {
-      // the generic-proxy reads of stage s are ordered before the async-proxy copy into it
-      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-      issue(i + S);
+    for (uint32_t q = 0; q <= last; q++) {
+      if (!col_on(L.mask, L.nseg, m.seg, q)) continue;
+      const char *xl;
+      uint32_t xd, xb;
+      span16(L.X[t] + q * L.sx[t] + (size_t) W * m.xo,
+             (size_t) W * sizeof(double) * ((m.flags & H2B_MV_TRANS) ? m.rows : m.cols), xl, xd,
+             xb);
+      const double *xs =
+          reinterpret_cast<const double *>(stage + L.panel_bytes + q * L.xcol_bytes + xd);
+      double *y = L.Y[t] + q * L.sy[t] + (size_t) W * m.yo;
+      if (m.flags & H2B_MV_TRANS) {
+        if (q == last) gemv_t<CX>(P, m.rows, m.cols, xs, y, release_now);
+        else gemv_t<CX>(P, m.rows, m.cols, xs, y, keep);
+      } else {
+        double *rb = red + (size_t) (nred++ & 1u) * L.red_doubles;
+        if (CX && complex_panel(t)) {
+          if (q == last) gemv_n<CX, CX>(P, m.rows, m.cols, xs, y, rb, release_now);
+          else gemv_n<CX, CX>(P, m.rows, m.cols, xs, y, rb, keep);
+        } else {
+          if (q == last) gemv_n<CX, false>(P, m.rows, m.cols, xs, y, rb, release_now);
+          else gemv_n<CX, false>(P, m.rows, m.cols, xs, y, rb, keep);
+        }
+      }
     }
   }
 }
 
+// Stage layout: the panel (FP64 panel bytes scaled to the storage type, plus 32 bytes for the
+// alignment and rounding slack) and the x slices of nrhs columns.
 template <typename T>
-uint32_t stage_bytes_of(const MvPhase &ph) {
-  // the FP64 panel bytes scaled to the storage type, plus the alignment and rounding slack
+uint32_t panel_region(const MvItems &ph) {
   const size_t b = (size_t) ph.max_bytes * sizeof(T) / sizeof(double) + 32;
   return (uint32_t) ((b + 127) & ~(size_t) 127);
 }
 
-template <bool CX, typename T>
-size_t smem_of(const MvPhase &ph, uint32_t stages) {
-  const size_t red = (size_t) NWARP * std::max<uint32_t>(ph.max_rows, 1) * (CX ? 2 : 1);
-  return (size_t) stages * stage_bytes_of<T>(ph) + sizeof(double) * red + 8 * stages;
+template <bool CX>
+uint32_t xcol_region(const MvItems &ph) {
+  return (uint32_t) ((sizeof(double) * (CX ? 2 : 1) * ph.max_x + 32 + 15) & ~(size_t) 15);
 }
 
 template <bool CX, typename T>
-int launch_phase(const MvmPlan *p, int phase, const MvLaunch &base, cudaStream_t st) {
-  const MvPhase &ph = p->ph[phase];
-  if (ph.n == 0) return H2B_OK;
+uint32_t stage_of(const MvItems &ph, uint32_t nrhs) {
+  const size_t b = panel_region<T>(ph) + (size_t) nrhs * xcol_region<CX>(ph);
+  return (uint32_t) ((b + 127) & ~(size_t) 127);
+}
+
+template <bool CX, typename T>
+size_t smem_of(const MvItems &ph, uint32_t stages, uint32_t nrhs) {
+  const size_t red = (size_t) NWARP * std::max<uint32_t>(ph.max_rows, 1) * (CX ? 2 : 1);
+  return (size_t) stages * stage_of<CX, T>(ph, nrhs) + 2 * sizeof(double) * red +
+         (sizeof(MvItem) + 16) * stages;
+}
+
+template <bool CX, typename T>
+int launch_range(const MvmPlan *p, const MvLaunch &base, uint32_t first, uint32_t last,
+                 cudaStream_t st) {
+  const MvItems &ph = p->items;
+  if (last <= first) return H2B_OK;
   MvLaunch L = base;
   L.items = ph.items;
-  L.n = ph.n;
+  L.first = first;
+  L.n = last - first;
   L.stages = (uint32_t) std::max(2, std::min(8, p->stages));
-  L.stage_bytes = stage_bytes_of<T>(ph);
+  L.panel_bytes = panel_region<T>(ph);
+  L.xcol_bytes = xcol_region<CX>(ph);
+  L.stage_bytes = stage_of<CX, T>(ph, L.nrhs);
   L.red_doubles = (uint32_t) ((size_t) NWARP * std::max<uint32_t>(ph.max_rows, 1) * (CX ? 2 : 1));
-  const size_t smem = smem_of<CX, T>(ph, L.stages);
-  if (smem > H2B_MAX_DYN_SMEM || ph.max_rows > MAXROWS) {
-    h2b_set_error("matvec: item panel of %u bytes / %u rows exceeds the kernel's limits",
-                  ph.max_bytes, ph.max_rows);
+  const size_t smem = smem_of<CX, T>(ph, L.stages, L.nrhs);
+  if (smem > H2B_MAX_DYN_SMEM || ph.max_rows > MAXROWS || ph.max_x > 65536) {
+    h2b_set_error("matvec: item panel of %u bytes / %u rows / %u right-hand sides exceeds the "
+                  "kernel's limits", ph.max_bytes, ph.max_rows, L.nrhs);
     return H2B_ERR_ARG;
   }
   H2B_CUDA_TRY((h2b_allow_smem<mv_items_kernel<CX, T>>()));
+  int occ = 0;
+  H2B_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, mv_items_kernel<CX, T>,
+                                                             TPB + 32, smem));
+  if (occ < 1) {
+    h2b_set_error("matvec: the item kernel does not fit an SM (%zu bytes of shared memory)", smem);
+    return H2B_ERR_ARG;
+  }
   const int sms = p->num_sms > 0 ? p->num_sms : 148;
-  const uint32_t grid = std::min<uint32_t>(ph.n, (uint32_t) (std::max(1, p->ctas_per_sm) * sms));
-  mv_items_kernel<CX, T><<<grid, TPB, smem, st>>>(L);
+  const int per_sm = std::min(occ, std::max(1, p->ctas_per_sm));
+  const uint32_t grid = std::min<uint32_t>(L.n, (uint32_t) (per_sm * sms));
+  mv_items_kernel<CX, T><<<grid, TPB + 32, smem, st>>>(L);
   h2b_note_launch();
   return H2B_OK;
 }
@@ -370,22 +509,24 @@ int launch_all(const MvmPlan *p, const double *x, size_t ldx, double *y, size_t 
   L.nseg = v.nseg;
   L.mask = v.mask;
   L.err = p->err;
-  const void *Wc = SINGLE ? (const void *) p->fWc : (const void *) p->Wc;
-  const void *Wr = SINGLE ? (const void *) p->fWr : (const void *) p->Wr;
-  const void *N = SINGLE ? (const void *) p->fN : (const void *) p->N;
-  const void *S = SINGLE ? (const void *) p->fS : (const void *) p->S;
-  // 1: forward slices (W_c^T, xp -> xt) and nearfield blocks (N, xp -> yp)
-  L.A[0] = Wc, L.X[0] = v.xp, L.Y[0] = v.xt, L.sx[0] = v.sxp, L.sy[0] = v.sxt;
-  L.A[1] = N, L.X[1] = v.xp, L.Y[1] = v.yp, L.sx[1] = v.sxp, L.sy[1] = v.syp;
-  int rc = launch_phase<CX, T>(p, 0, L, st);
-  // 2: coupling blocks (S, xt -> yt)
-  L.A[0] = nullptr, L.X[0] = nullptr, L.Y[0] = nullptr;
-  L.A[1] = S, L.X[1] = v.xt, L.Y[1] = v.yt, L.sx[1] = v.sxt, L.sy[1] = v.syt;
-  if (rc == H2B_OK) rc = launch_phase<CX, T>(p, 1, L, st);
-  // 3: backward slices (W_r^T transposed, yt -> yp)
-  L.A[0] = Wr, L.X[0] = v.yt, L.Y[0] = v.yp, L.sx[0] = v.syt, L.sy[0] = v.syp;
-  L.A[1] = nullptr, L.X[1] = nullptr, L.Y[1] = nullptr;
-  if (rc == H2B_OK) rc = launch_phase<CX, T>(p, 2, L, st);
+  L.A[H2B_MV_FORWARD] = SINGLE ? (const void *) p->fWc : (const void *) p->Wc;
+  L.A[H2B_MV_NEAR] = SINGLE ? (const void *) p->fN : (const void *) p->N;
+  L.A[H2B_MV_COUPLING] = SINGLE ? (const void *) p->fS : (const void *) p->S;
+  L.A[H2B_MV_BACKWARD] = SINGLE ? (const void *) p->fWr : (const void *) p->Wr;
+  L.X[H2B_MV_FORWARD] = v.xp, L.Y[H2B_MV_FORWARD] = v.xt;
+  L.sx[H2B_MV_FORWARD] = v.sxp, L.sy[H2B_MV_FORWARD] = v.sxt;
+  L.X[H2B_MV_NEAR] = v.xp, L.Y[H2B_MV_NEAR] = v.yp;
+  L.sx[H2B_MV_NEAR] = v.sxp, L.sy[H2B_MV_NEAR] = v.syp;
+  L.X[H2B_MV_COUPLING] = v.xt, L.Y[H2B_MV_COUPLING] = v.yt;
+  L.sx[H2B_MV_COUPLING] = v.sxt, L.sy[H2B_MV_COUPLING] = v.syt;
+  L.X[H2B_MV_BACKWARD] = v.yt, L.Y[H2B_MV_BACKWARD] = v.yp;
+  L.sx[H2B_MV_BACKWARD] = v.syt, L.sy[H2B_MV_BACKWARD] = v.syp;
+  const MvItems &it = p->items;
+  // forward + nearfield, coupling (reads xt), backward (reads yt)
+  int rc = launch_range<CX, T>(p, L, 0, it.start[H2B_MV_COUPLING], st);
+  if (rc == H2B_OK)
+    rc = launch_range<CX, T>(p, L, it.start[H2B_MV_COUPLING], it.start[H2B_MV_BACKWARD], st);
+  if (rc == H2B_OK) rc = launch_range<CX, T>(p, L, it.start[H2B_MV_BACKWARD], it.n, st);
   if (rc != H2B_OK) return rc;
   scatter_multi_kernel<CX><<<gz, 256, 0, st>>>(v, p->ridx, y, ldy, p->nrow, ar, ai);
   h2b_note_launch();
@@ -419,11 +560,11 @@ extern "C" int h2b_mvm_prepare(void) {
   return H2B_OK;
 }
 
-extern "C" size_t h2b_mvm_smem_bytes(const MvmPlan *p, int phase, int single, int stages) {
-  const MvPhase &ph = p->ph[phase];
+extern "C" size_t h2b_mvm_smem_bytes(const MvmPlan *p, int single, int stages) {
+  const MvItems &ph = p->items;
   if (p->cx)
-    return single ? smem_of<true, float>(ph, stages) : smem_of<true, double>(ph, stages);
-  return single ? smem_of<false, float>(ph, stages) : smem_of<false, double>(ph, stages);
+    return single ? smem_of<true, float>(ph, stages, 1) : smem_of<true, double>(ph, stages, 1);
+  return single ? smem_of<false, float>(ph, stages, 1) : smem_of<false, double>(ph, stages, 1);
 }
 
 extern "C" int h2b_mvm_launch_single(const MvmPlan *p, const double *x, double *y, double ar,
@@ -446,8 +587,10 @@ extern "C" int h2b_mvm_launch(const MvmPlan *p, const double *x, double *y, doub
 
 extern "C" size_t h2b_mvm_work_doubles(const MvmPlan *p, uint32_t nrhs) {
   const size_t W = p->cx ? 2 : 1;
+  // the vectors and 8 doubles of slack after the last one (x slices are copied in 16-byte
+  // aligned spans)
   return nrhs * W * ((size_t) p->ncol + p->nrow +
-                     (size_t) p->k * (p->ncol_clusters + p->nrow_clusters));
+                     (size_t) p->k * (p->ncol_clusters + p->nrow_clusters)) + 8;
 }
 
 extern "C" int h2b_mvm_launch_batch(const MvmPlan *p, int single, uint32_t nrhs, const double *x,

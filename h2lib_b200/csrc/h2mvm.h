@@ -4,11 +4,20 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
-// One GEMV work item of a product: a panel P (rows x cols, column-major, ld = rows, contiguous)
-// of one of a launch's two panel arrays, applied as y[0, rows) += P x[0, cols) or, transposed,
-// y[0, cols) += P^T x[0, rows); x and y are slices of the launch's work vectors.
-#define H2B_MV_SRC1 1u       // panel, x and y from the launch's second triple (else the first)
-#define H2B_MV_TRANS 2u      // y += P^T x
+// One GEMV work item of a product: a panel P (rows x cols, column-major, ld = rows, contiguous),
+// applied as y[0, rows) += P x[0, cols) or, transposed, y[0, cols) += P^T x[0, rows); x and y
+// are slices of the product's work vectors.  The kind selects the panel array and the vectors:
+//   forward    W_c^T slice, x = xp, y = xt
+//   nearfield  N block panel, x = xp, y = yp
+//   coupling   S block panel, x = xt, y = yt
+//   backward   W_r^T slice (transposed), x = yt, y = yp
+#define H2B_MV_FORWARD 0u
+#define H2B_MV_NEAR 1u
+#define H2B_MV_COUPLING 2u
+#define H2B_MV_BACKWARD 3u
+#define H2B_MV_KIND 3u       // flags & H2B_MV_KIND: the kind
+#define H2B_MV_TRANS 4u      // y += P^T x
+#define H2B_MV_NONE 0xFFFFFFFFu
 struct MvItem {
   uint64_t p;                // element offset of the panel in its array
   uint32_t rows, cols;
@@ -18,16 +27,17 @@ struct MvItem {
 };
 static_assert(sizeof(MvItem) == 32, "MvItem is 32 bytes");
 
-// Items of one launch.  Panels of array 0 are real; panels of array 1 are complex when the
-// operator is.  The shared-memory stage of a launch holds its largest panel.
-struct MvPhase {
+// The items of a product, ordered by kind: start[k] is the first item of kind k.
+struct MvItems {
   const MvItem *items;       // device
   uint32_t n;
+  uint32_t start[4];
   uint32_t max_bytes;        // largest panel in bytes at FP64 storage
   uint32_t max_rows;         // largest rows of an untransposed item
+  uint32_t max_x;            // longest x slice (elements: cols, or rows when transposed)
 };
 
-// Panels are split so that none exceeds this many bytes at FP64 storage.
+// Default largest panel of a work item (bytes at FP64 storage); blocks and slices are split to fit.
 #define H2B_MV_PANEL_BYTES (32u * 1024u)
 
 struct MvmPlan {
@@ -36,12 +46,11 @@ struct MvmPlan {
   uint32_t nrow, ncol, nrow_clusters, ncol_clusters;
   const uint32_t *ridx, *cidx;   // device index arrays of the row / column tree
   double *xp, *yp, *xt, *yt;     // work vectors of one column
-  // the three launches: forward transform + nearfield, coupling, backward transform
-  MvPhase ph[3];
+  MvItems items;
   // panel arrays (FP64) and their FP32 copies (NULL until made)
   const double *Wc, *Wr, *N, *S;
   const float *fWc, *fWr, *fN, *fS;
-  int *err;                      // device flag: a panel copy did not complete
+  int *err;                      // device flag: a wait for a panel copy ran out
   // launch shape of the item kernel: resident CTAs per SM and pipeline stages
   int ctas_per_sm, stages;
 };
@@ -65,4 +74,4 @@ extern "C" int h2b_mvm_launch_batch(const MvmPlan *p, int single, uint32_t nrhs,
 // so that no later launch, possibly inside a CUDA graph capture, has to.
 extern "C" int h2b_mvm_prepare(void);
 // Shared-memory bytes of the item kernel for a launch shape (for the autotuner's candidates).
-extern "C" size_t h2b_mvm_smem_bytes(const MvmPlan *p, int phase, int single, int stages);
+extern "C" size_t h2b_mvm_smem_bytes(const MvmPlan *p, int single, int stages);
