@@ -207,6 +207,7 @@ extern "C" void h2b_h2matrix_del(h2b_h2matrix *h) {
   // the structure, unless it belongs to the matrix this one was made like
   if (!h->shared) {
     dfree(h->d_items, st);
+    dfree(h->d_items_single, st);
     devtree_free(h->rt, st);
     devtree_free(h->ct, st);
     dfree(h->d_adm_rc, st); dfree(h->d_adm_cc, st);
@@ -472,14 +473,15 @@ int h2b_h2_check_mv_error(const h2b_h2matrix *h) {
   return H2B_OK;
 }
 
-int h2b_h2_build_mv_items(h2b_h2matrix *h) {
+// The item list of a product for panels of pb bytes at FP64 storage, ordered by kind: forward,
+// nearfield, coupling, backward (the matvec runs the first two kinds in one launch, then the
+// coupling, then the backward slices).
+static void build_items(const h2b_h2matrix *h, uint32_t pb, uint32_t fwd_rows, uint32_t back_rows,
+                        std::vector<MvItem> &it, MvItems &m) {
   const h2b_ctree &R = h->tree->row, &C = h->tree->col;
   const uint32_t k = h->k, W = h->cx ? 2 : 1;
-  // items ordered by kind: forward, nearfield, coupling, backward (the matvec runs the first two
-  // kinds in one launch, then the coupling, then the backward slices)
-  std::vector<MvItem> it;
   uint32_t start[4] = {0, 0, 0, 0};
-  const uint32_t pb = h->mv_panel_bytes;
+  it.clear();
   auto slice_rows = [&](uint32_t want) {
     const uint32_t cap = std::max<uint32_t>(1, pb / (8u * k));
     return std::max<uint32_t>(1, std::min(want, cap));
@@ -488,7 +490,7 @@ int h2b_h2_build_mv_items(h2b_h2matrix *h) {
   auto panel_cols = [&](uint32_t rows) {
     return std::max<uint32_t>(1, pb / (8u * W * std::max<uint32_t>(rows, 1)));
   };
-  const uint32_t fr = slice_rows(h->mv_fwd_rows), br = slice_rows(h->mv_back_rows);
+  const uint32_t fr = slice_rows(fwd_rows), br = slice_rows(back_rows);
   // forward slices, x_t -> xt_t, over every admissible column cluster
   for (uint32_t t = 0; t < C.n; t++) {
     if (!h->ct.h_adm[t]) continue;
@@ -521,21 +523,33 @@ int h2b_h2_build_mv_items(h2b_h2matrix *h) {
       it.push_back(MvItem{h->rt.h_woff[t] + (uint64_t) r0 * k, k, std::min(br, R.size[t] - r0),
                           k * t, R.off[t] + r0, h->rt.h_seg[t], H2B_MV_BACKWARD | H2B_MV_TRANS});
   }
-  dfree(h->d_items, h->st);
-  int rc;
-  if ((rc = upload(&h->d_items, it, h->st))) return rc;
-  MvItems &m = h->mvitems;
-  m.items = h->d_items;
   m.n = (uint32_t) it.size();
   for (int q = 0; q < 4; q++) m.start[q] = start[q];
-  m.max_bytes = m.max_rows = m.max_x = 0;
+  m.max_bytes = m.max_rows = m.max_cols_t = m.max_x = 0;
   for (const MvItem &e : it) {
     const uint32_t kind = e.flags & H2B_MV_KIND;
     const bool cpx = kind == H2B_MV_NEAR || kind == H2B_MV_COUPLING;
     m.max_bytes = std::max<uint32_t>(m.max_bytes, e.rows * e.cols * 8u * (cpx ? W : 1u));
     if (!(e.flags & H2B_MV_TRANS)) m.max_rows = std::max(m.max_rows, e.rows);
+    else m.max_cols_t = std::max(m.max_cols_t, e.cols);
     m.max_x = std::max(m.max_x, (e.flags & H2B_MV_TRANS) ? e.rows : e.cols);
   }
+}
+
+// Two lists: one for the FP64 product, and one for the product from the FP32 copies with twice
+// the entries per panel (the same bytes per copy).
+int h2b_h2_build_mv_items(h2b_h2matrix *h) {
+  std::vector<MvItem> it, its;
+  build_items(h, h->mv_panel_bytes, h->mv_fwd_rows, h->mv_back_rows, it, h->mvitems);
+  build_items(h, 2 * h->mv_panel_bytes, 2 * h->mv_fwd_rows, 2 * h->mv_back_rows, its,
+              h->mvitems_single);
+  dfree(h->d_items, h->st);
+  dfree(h->d_items_single, h->st);
+  int rc;
+  if ((rc = upload(&h->d_items, it, h->st)) || (rc = upload(&h->d_items_single, its, h->st)))
+    return rc;
+  h->mvitems.items = h->d_items;
+  h->mvitems_single.items = h->d_items_single;
   return H2B_OK;
 }
 
@@ -556,6 +570,7 @@ void h2b_h2_fill_mvm_plan(h2b_h2matrix *h) {
   p.xt = h->d_xt;
   p.yt = h->d_yt;
   p.items = h->mvitems;
+  p.items_single = h->mvitems_single;
   p.Wc = h->ct.d_W;
   p.Wr = h->rt.d_W;
   p.N = h->d_N;
@@ -566,6 +581,7 @@ void h2b_h2_fill_mvm_plan(h2b_h2matrix *h) {
   p.fS = h->f_S;
   p.err = h->d_mverr;
   p.ctas_per_sm = h->mv_ctas;
+  p.warps = h->mv_warps;
   p.stages = h->mv_stages;
   h2b_mvm_prepare();
 }
@@ -640,10 +656,10 @@ extern "C" int h2b_h2matrix_set_matvec_shape(h2b_h2matrix *h, const uint32_t sha
   const uint32_t fr = shape[0] ? shape[0] : h->mv_fwd_rows;
   const uint32_t br = shape[1] ? shape[1] : h->mv_back_rows;
   const uint32_t pb = shape[4] ? shape[4] * 1024u : h->mv_panel_bytes;
-  if (shape[2] > 8 || shape[3] > 8 || (shape[3] && shape[3] < 2) ||
-      (shape[4] && (shape[4] < 4 || shape[4] > 64)) || shape[5] > h->k) {
-    h2b_set_error("h2b_h2matrix_set_matvec_shape: CTAs per SM <= 8, stages 2..8, panels 4..64 "
-                  "KiB, leaf CTAs <= k");
+  if (shape[2] > 8 || shape[3] > 4 || (shape[4] && (shape[4] < 4 || shape[4] > 64)) ||
+      shape[5] > h->k || shape[6] > 8) {
+    h2b_set_error("h2b_h2matrix_set_matvec_shape: CTAs per SM <= 8, stages per warp <= 4, panels "
+                  "4..64 KiB, leaf CTAs <= k, consumer warps <= 8");
     return H2B_ERR_ARG;
   }
   if (fr != h->mv_fwd_rows || br != h->mv_back_rows || pb != h->mv_panel_bytes) {
@@ -663,6 +679,7 @@ extern "C" int h2b_h2matrix_set_matvec_shape(h2b_h2matrix *h, const uint32_t sha
   if (shape[2]) h->mv_ctas = (int) shape[2];
   if (shape[3]) h->mv_stages = (int) shape[3];
   if (shape[5]) h->leaf_split = (int) shape[5];
+  if (shape[6]) h->mv_warps = (int) shape[6];
   h2b_h2_fill_mvm_plan(h);
   return H2B_OK;
 }
@@ -675,6 +692,7 @@ extern "C" int h2b_h2matrix_get_matvec_shape(const h2b_h2matrix *h, uint32_t sha
   shape[3] = (uint32_t) h->mv_stages;
   shape[4] = h->mv_panel_bytes / 1024u;
   shape[5] = (uint32_t) h->leaf_split;
+  shape[6] = (uint32_t) h->mv_warps;
   return H2B_OK;
 }
 

@@ -46,12 +46,12 @@ struct h2b_h2matrix {
   int cx = 0, num_sms = 148;
   int quad_fp32 = 0;  // distant-pair quadrature in FP32 (h2b_h2matrix_set_precision)
   // matvec work items (h2mvm.h), owned by the structure's owner, and the knobs they were built
-  // with: rows per forward / backward slice, largest panel; CTAs per SM and stages of the item
-  // kernel
-  MvItem *d_items = nullptr;
-  MvItems mvitems = {};
-  uint32_t mv_fwd_rows = 64, mv_back_rows = 64;
-  int mv_ctas = 3, mv_stages = 2;
+  // with: rows per forward / backward slice, largest panel; CTAs per SM, consumer warps and
+  // stages per consumer warp of the item kernel
+  MvItem *d_items = nullptr, *d_items_single = nullptr;
+  MvItems mvitems = {}, mvitems_single = {};  // the FP64 product's and the FP32 product's
+  uint32_t mv_fwd_rows = 32, mv_back_rows = 32;
+  int mv_ctas = 4, mv_warps = 3, mv_stages = 1;
   uint32_t mv_panel_bytes = H2B_MV_PANEL_BYTES;
   int leaf_split = 2;  // CTAs per leaf of the leaf-basis kernel (each a range of the k columns)
   int *d_mverr = nullptr;  // the item kernel's error flag (one per matrix)

@@ -38,9 +38,9 @@
 
 namespace {
 
-constexpr int TPB = 256;
-constexpr int NWARP = TPB / 32;
-constexpr int MAXROWS = 128;                 // rows of an untransposed item (k <= 125, 64-row tiles)
+constexpr int MAXTHREADS = 288;              // up to 8 consumer warps and the producer warp
+constexpr int MAXROWS = 128;                 // rows of an untransposed item, columns of a transposed
+                                             // one (four 32-lane slots)
 constexpr uint32_t WAIT_LIMIT = 1u << 24;    // try_wait polls before a stage counts as lost
 
 // Vectors of a product with nrhs right-hand sides.  With a mask (batched solves on a forest:
@@ -117,8 +117,8 @@ struct MvLaunch {
   uint32_t stage_bytes;    // bytes per stage (multiple of 128)
   uint32_t panel_bytes;    // panel region of a stage; the x slices of every column follow
   uint32_t xcol_bytes;     // bytes per x slice of one column (multiple of 16, with slack)
-  uint32_t stages;
-  uint32_t red_doubles;    // one of the two cross-warp reduction buffers
+  uint32_t stages;         // ring stages, a multiple of nw: stage s belongs to consumer warp s % nw
+  uint32_t nw;             // consumer warps; warp nw produces
 };
 
 __device__ __forceinline__ uint32_t smem_addr(const void *p) {
@@ -165,42 +165,44 @@ __device__ __forceinline__ const char *panel_addr(const MvLaunch &L, const MvIte
   return reinterpret_cast<const char *>(L.A[kind]) + m.p * esz;
 }
 
+// entry e of a panel (complex entries as one vector load: a complex panel starts on a multiple of
+// its entry size, so the stage copy keeps that alignment)
 template <bool PCX, typename T>
 __device__ __forceinline__ void entry(const T *P, size_t e, double &re, double &im) {
   if constexpr (PCX) {
-    re = (double) P[2 * e];
-    im = (double) P[2 * e + 1];
+    using V2 = typename std::conditional<std::is_same<T, float>::value, float2, double2>::type;
+    const V2 v = reinterpret_cast<const V2 *>(P)[e];
+    re = (double) v.x;
+    im = (double) v.y;
   } else {
     re = (double) P[e];
     im = 0.0;
   }
 }
 
-// Named barrier of the consumer warps (barrier 0 stays __syncthreads').
-__device__ __forceinline__ void consumers_sync() {
-  asm volatile("bar.sync 1, %0;" ::"r"(NWARP * 32) : "memory");
-}
-
-// y[0, R) += P x[0, C) from the stage: warps take columns, lanes rows; the warps' partial sums
-// meet in `red` (after a consumer barrier) and reach y with one atomic addition per row.
-// `release` is called when the warp has read the stage for the last time.
-template <bool CX, bool PCX, typename T, typename F>
-__device__ __forceinline__ void gemv_n(const T *P, uint32_t R, uint32_t C, const double *xs,
-                                       double *y, double *red, F release) {
+// y[0, R) += P x[0, C) by one warp: lanes take rows (SL slots of 32), the warp runs over the
+// columns; one atomic addition per row.
+template <bool CX, bool PCX, typename T, int SL>
+__device__ __forceinline__ void warp_gemv_n(const T *__restrict__ P, uint32_t R, uint32_t C,
+                                            const double *__restrict__ xs, double *y,
+                                            uint32_t lane) {
   constexpr int W = CX ? 2 : 1;
-  const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
-  double sr[MAXROWS / 32], si[MAXROWS / 32];
+  double sr[SL], si[SL];
+  bool on[SL];
 #pragma unroll
-  for (int j = 0; j < MAXROWS / 32; j++) sr[j] = si[j] = 0.0;
+  for (int j = 0; j < SL; j++) {
+    sr[j] = si[j] = 0.0;
+    on[j] = lane + 32u * j < R;
+  }
 #pragma unroll 4
-  for (uint32_t c = warp; c < C; c += NWARP) {
+  for (uint32_t c = 0; c < C; c++) {
     const double xr = xs[W * c], xi = CX ? xs[W * c + 1] : 0.0;
+    const T *col = P + (size_t) (PCX ? 2 : 1) * c * R;
 #pragma unroll
-    for (int j = 0; j < MAXROWS / 32; j++) {
-      const uint32_t r = lane + 32u * j;
-      if (r < R) {
+    for (int j = 0; j < SL; j++) {
+      if (on[j]) {
         double pr, pi;
-        entry<PCX>(P, r + (size_t) c * R, pr, pi);
+        entry<PCX>(col, lane + 32u * j, pr, pi);
         if (PCX) {
           sr[j] = fma(pr, xr, fma(-pi, xi, sr[j]));
           si[j] = fma(pr, xi, fma(pi, xr, si[j]));
@@ -211,111 +213,115 @@ __device__ __forceinline__ void gemv_n(const T *P, uint32_t R, uint32_t C, const
       }
     }
   }
-  release();
 #pragma unroll
-  for (int j = 0; j < MAXROWS / 32; j++) {
-    const uint32_t r = lane + 32u * j;
-    if (r < R) {
-      red[W * (warp * R + r)] = sr[j];
-      if (CX) red[W * (warp * R + r) + 1] = si[j];
-    }
-  }
-  consumers_sync();
-  for (uint32_t r = threadIdx.x; r < R; r += NWARP * 32) {
-    double ar = 0.0, ai = 0.0;
-#pragma unroll
-    for (int w = 0; w < NWARP; w++) {
-      ar += red[W * (w * R + r)];
-      if (CX) ai += red[W * (w * R + r) + 1];
-    }
-    if (y) {
-      atomicAdd(y + W * r, ar);
-      if (CX) atomicAdd(y + W * r + 1, ai);
+  for (int j = 0; j < SL; j++) {
+    if (on[j]) {
+      const uint32_t r = lane + 32u * j;
+      atomicAdd(y + W * r, sr[j]);
+      if (CX) atomicAdd(y + W * r + 1, si[j]);
     }
   }
 }
 
-// y[0, C) += P^T x[0, R) for a real panel: a warp per column, lanes over the rows, shuffle sums.
-template <bool CX, typename T, typename F>
-__device__ __forceinline__ void gemv_t(const T *P, uint32_t R, uint32_t C, const double *xs,
-                                       double *y, F release) {
+// y[0, C) += P^T x[0, R) by one warp for a real panel: lanes take columns (SL slots of 32) and
+// run over the rows from a lane-dependent start, row (it + lane) mod R at step it, so that the
+// warp's reads of the column-major panel fall in distinct banks.
+template <bool CX, typename T, int SL>
+__device__ __forceinline__ void warp_gemv_t(const T *__restrict__ P, uint32_t R, uint32_t C,
+                                            const double *__restrict__ xs, double *y,
+                                            uint32_t lane) {
   constexpr int W = CX ? 2 : 1;
-  const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
-  double xr[MAXROWS / 32], xi[MAXROWS / 32];
+  double sr[SL], si[SL];
+  bool on[SL];
 #pragma unroll
-  for (int j = 0; j < MAXROWS / 32; j++) {
-    const uint32_t r = lane + 32u * j;
-    xr[j] = r < R ? xs[W * r] : 0.0;
-    xi[j] = (CX && r < R) ? xs[W * r + 1] : 0.0;
+  for (int j = 0; j < SL; j++) {
+    sr[j] = si[j] = 0.0;
+    on[j] = lane + 32u * j < C;
   }
-  for (uint32_t c = warp; c < C; c += NWARP) {
-    double sr = 0.0, si = 0.0;
+  uint32_t r = lane % R;
+#pragma unroll 4
+  for (uint32_t it = 0; it < R; it++) {
+    const double xr = xs[W * r], xi = CX ? xs[W * r + 1] : 0.0;
 #pragma unroll
-    for (int j = 0; j < MAXROWS / 32; j++) {
-      const uint32_t r = lane + 32u * j;
-      if (r < R) {
-        const double p = (double) P[r + (size_t) c * R];
-        sr = fma(p, xr[j], sr);
-        if (CX) si = fma(p, xi[j], si);
+    for (int j = 0; j < SL; j++) {
+      if (on[j]) {
+        const double p = (double) P[r + (size_t) (lane + 32u * j) * R];
+        sr[j] = fma(p, xr, sr[j]);
+        if (CX) si[j] = fma(p, xi, si[j]);
       }
     }
-    sr = warp_sum(sr);
-    if (CX) si = warp_sum(si);
-    if (lane == 0) {
-      atomicAdd(y + W * c, sr);
-      if (CX) atomicAdd(y + W * c + 1, si);
+    r = r + 1 == R ? 0u : r + 1;
+  }
+#pragma unroll
+  for (int j = 0; j < SL; j++) {
+    if (on[j]) {
+      const uint32_t c = lane + 32u * j;
+      atomicAdd(y + W * c, sr[j]);
+      if (CX) atomicAdd(y + W * c + 1, si[j]);
     }
   }
-  release();
 }
 
-// Warp NWARP produces: for each of the CTA's items (first + blockIdx.x + i gridDim.x) it copies
-// the panel and the x slice of every right-hand side into stage i % S (one bulk copy each,
-// completion on full[s]) after the consumers have released the stage's previous contents
-// (empty[s]), and puts the descriptor in the stage's slot (a sentinel after the last item).
-// Warps 0 .. NWARP-1 consume: wait on full[s], agree on the outcome (barrier with an OR vote, so
-// that all of them stop or none), multiply, release the stage, and combine their partial sums
-// (one consumer barrier per product; the reduction buffer alternates between products).
+template <bool CX, bool PCX, typename T>
+__device__ __forceinline__ void gemv_n_any(const T *P, uint32_t R, uint32_t C, const double *xs,
+                                           double *y, uint32_t lane) {
+  switch ((R + 31) >> 5) {
+    case 1: warp_gemv_n<CX, PCX, T, 1>(P, R, C, xs, y, lane); break;
+    case 2: warp_gemv_n<CX, PCX, T, 2>(P, R, C, xs, y, lane); break;
+    case 3: warp_gemv_n<CX, PCX, T, 3>(P, R, C, xs, y, lane); break;
+    default: warp_gemv_n<CX, PCX, T, 4>(P, R, C, xs, y, lane); break;
+  }
+}
+
 template <bool CX, typename T>
-__global__ void __launch_bounds__(TPB + 32) mv_items_kernel(MvLaunch L) {
+__device__ __forceinline__ void gemv_t_any(const T *P, uint32_t R, uint32_t C, const double *xs,
+                                           double *y, uint32_t lane) {
+  switch ((C + 31) >> 5) {
+    case 1: warp_gemv_t<CX, T, 1>(P, R, C, xs, y, lane); break;
+    case 2: warp_gemv_t<CX, T, 2>(P, R, C, xs, y, lane); break;
+    case 3: warp_gemv_t<CX, T, 3>(P, R, C, xs, y, lane); break;
+    default: warp_gemv_t<CX, T, 4>(P, R, C, xs, y, lane); break;
+  }
+}
+
+// Warp nw produces: for each of the CTA's items i (list entry first + blockIdx.x + i gridDim.x)
+// it copies the panel and the x slice of every right-hand side into stage i % S (one bulk copy
+// each, completion on full[s]) once the stage's previous item has been released (empty[s]), and
+// puts the descriptor in the stage's slot.
+// Consumer warp w multiplies the items i = w, w + nw, ... alone: S is a multiple of nw, so stage
+// i % S always belongs to the same warp, and no barrier joins the consumer warps.  Every wait is
+// bounded; a warp whose wait runs out sets the error flag and leaves, and the others' bounded
+// waits end the CTA.
+template <bool CX, typename T>
+__global__ void __launch_bounds__(MAXTHREADS) mv_items_kernel(MvLaunch L) {
   extern __shared__ __align__(128) unsigned char smem[];
   constexpr int W = CX ? 2 : 1;
   const uint32_t S = L.stages;
   unsigned char *stage0 = smem;
-  double *red = reinterpret_cast<double *>(smem + (size_t) S * L.stage_bytes);
-  MvItem *slot = reinterpret_cast<MvItem *>(red + 2 * (size_t) L.red_doubles);
+  MvItem *slot = reinterpret_cast<MvItem *>(smem + (size_t) S * L.stage_bytes);
   uint64_t *full = reinterpret_cast<uint64_t *>(slot + S);
   uint64_t *empty = full + S;
   const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
+  const uint32_t mine = L.n > blockIdx.x ? (L.n - blockIdx.x + gridDim.x - 1) / gridDim.x : 0u;
   if (threadIdx.x == 0) {
     for (uint32_t s = 0; s < S; s++) {
       asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&full[s])));
-      asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(&empty[s])),
-                   "r"(NWARP));
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&empty[s])));
     }
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   __syncthreads();
 
-  if (warp == NWARP) {
-    // ---- producer (one lane): this CTA's items first + blockIdx.x + i gridDim.x, the next
-    // descriptor fetched while the current copies run
-    if (lane != 0) return;
-    const uint32_t mine =
-        L.n > blockIdx.x ? (L.n - blockIdx.x + gridDim.x - 1) / gridDim.x : 0u;
-    MvItem m;
-    if (mine) m = L.items[L.first + blockIdx.x];
+  if (warp == L.nw) {
+    // ---- producer (one lane): the next descriptor is fetched while the current copies run
+    if (lane != 0 || mine == 0) return;
+    MvItem m = L.items[L.first + blockIdx.x];
     uint32_t i = 0;
     bool ok = true;
-    for (;; i++) {
+    for (; i < mine; i++) {
       const uint32_t s = i % S;
       if (i >= S && !(ok = bar_wait(smem_addr(&empty[s]), ((i / S) - 1) & 1u))) break;
       const uint32_t bar = smem_addr(&full[s]);
-      if (i >= mine) {
-        slot[s].flags = H2B_MV_NONE;  // sentinel: no more items
-        asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
-        break;
-      }
       slot[s] = m;
       size_t n;
       const char *pa = panel_addr<CX, T>(L, m, n), *lo;
@@ -352,32 +358,23 @@ __global__ void __launch_bounds__(TPB + 32) mv_items_kernel(MvLaunch L) {
     }
     if (!ok) {
       // a wait ran out: flag it and wait (bounded) for the copies this warp issued before it
-      // leaves the CTA's shared memory (the consumers stop at their next stage)
+      // leaves the CTA's shared memory (the consumers give up at their next stage)
       atomicExch(L.err, 1);
       for (uint32_t j = i > S ? i - S : 0; j < i; j++)
         bar_wait(smem_addr(&full[j % S]), (j / S) & 1u);
     }
     return;
   }
+  if (warp > L.nw) return;
 
   // ---- consumers
-  uint32_t nred = 0;  // gemv_n calls so far: the reduction buffer alternates between calls
-  for (uint32_t i = 0;; i++) {
+  for (uint32_t i = warp; i < mine; i += L.nw) {
     const uint32_t s = i % S;
-    const bool ok = bar_wait(smem_addr(&full[s]), (i / S) & 1u);
-    // every consumer thread takes part: all of them stop, or none
-    uint32_t any_lost;
-    asm volatile("{\n .reg .pred p, q;\n setp.eq.u32 p, %1, 0;\n"
-                 " bar.red.or.pred q, 1, %2, p;\n selp.u32 %0, 1, 0, q;\n}"
-                 : "=r"(any_lost)
-                 : "r"((uint32_t) ok), "r"(NWARP * 32)
-                 : "memory");
-    if (any_lost) {
-      if (threadIdx.x == 0) atomicExch(L.err, 1);
+    if (!bar_wait(smem_addr(&full[s]), (i / S) & 1u)) {
+      if (lane == 0) atomicExch(L.err, 1);
       return;
     }
     const MvItem m = slot[s];
-    if (m.flags == H2B_MV_NONE) return;  // the list is exhausted
     const unsigned char *stage = stage0 + (size_t) s * L.stage_bytes;
     size_t n;
     const char *pa = panel_addr<CX, T>(L, m, n), *lo;
@@ -385,48 +382,24 @@ __global__ void __launch_bounds__(TPB + 32) mv_items_kernel(MvLaunch L) {
     span16(pa, n, lo, delta, bytes);
     const T *P = reinterpret_cast<const T *>(stage + delta);
     const int t = m.flags & H2B_MV_KIND;
-    // columns whose system is done are skipped; the stage is released after the last one used
-    uint32_t last = L.nrhs;
-    for (uint32_t q = L.nrhs; q-- > 0;)
-      if (col_on(L.mask, L.nseg, m.seg, q)) {
-        last = q;
-        break;
-      }
-    auto release_now = [&]() {
-      __syncwarp();
-      if (lane == 0)
-        asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(&empty[s]))
-                     : "memory");
-    };
-    auto keep = [] {};
-    if (last == L.nrhs) {
-      release_now();
-      continue;
-    }
-    for (uint32_t q = 0; q <= last; q++) {
-      if (!col_on(L.mask, L.nseg, m.seg, q)) continue;
+    const bool trans = (m.flags & H2B_MV_TRANS) != 0;
+    const size_t xn = (size_t) W * sizeof(double) * (trans ? m.rows : m.cols);
+    for (uint32_t q = 0; q < L.nrhs; q++) {
+      if (!col_on(L.mask, L.nseg, m.seg, q)) continue;  // the column's system is done
       const char *xl;
       uint32_t xd, xb;
-      span16(L.X[t] + q * L.sx[t] + (size_t) W * m.xo,
-             (size_t) W * sizeof(double) * ((m.flags & H2B_MV_TRANS) ? m.rows : m.cols), xl, xd,
-             xb);
+      span16(L.X[t] + q * L.sx[t] + (size_t) W * m.xo, xn, xl, xd, xb);
       const double *xs =
           reinterpret_cast<const double *>(stage + L.panel_bytes + q * L.xcol_bytes + xd);
       double *y = L.Y[t] + q * L.sy[t] + (size_t) W * m.yo;
-      if (m.flags & H2B_MV_TRANS) {
-        if (q == last) gemv_t<CX>(P, m.rows, m.cols, xs, y, release_now);
-        else gemv_t<CX>(P, m.rows, m.cols, xs, y, keep);
-      } else {
-        double *rb = red + (size_t) (nred++ & 1u) * L.red_doubles;
-        if (CX && complex_panel(t)) {
-          if (q == last) gemv_n<CX, CX>(P, m.rows, m.cols, xs, y, rb, release_now);
-          else gemv_n<CX, CX>(P, m.rows, m.cols, xs, y, rb, keep);
-        } else {
-          if (q == last) gemv_n<CX, false>(P, m.rows, m.cols, xs, y, rb, release_now);
-          else gemv_n<CX, false>(P, m.rows, m.cols, xs, y, rb, keep);
-        }
-      }
+      if (trans) gemv_t_any<CX, T>(P, m.rows, m.cols, xs, y, lane);
+      else if (CX && complex_panel(t)) gemv_n_any<CX, CX, T>(P, m.rows, m.cols, xs, y, lane);
+      else gemv_n_any<CX, false, T>(P, m.rows, m.cols, xs, y, lane);
     }
+    __syncwarp();
+    if (lane == 0)
+      asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(&empty[s]))
+                   : "memory");
   }
 }
 
@@ -451,35 +424,40 @@ uint32_t stage_of(const MvItems &ph, uint32_t nrhs) {
 
 template <bool CX, typename T>
 size_t smem_of(const MvItems &ph, uint32_t stages, uint32_t nrhs) {
-  const size_t red = (size_t) NWARP * std::max<uint32_t>(ph.max_rows, 1) * (CX ? 2 : 1);
-  return (size_t) stages * stage_of<CX, T>(ph, nrhs) + 2 * sizeof(double) * red +
-         (sizeof(MvItem) + 16) * stages;
+  return (size_t) stages * (stage_of<CX, T>(ph, nrhs) + sizeof(MvItem) + 16);
+}
+
+// consumer warps and ring stages of a launch shape (stages per consumer warp 1..4)
+void ring_shape(const MvmPlan *p, uint32_t &nw, uint32_t &stages) {
+  nw = (uint32_t) std::max(1, std::min(MAXTHREADS / 32 - 1, p->warps));
+  stages = nw * (uint32_t) std::max(1, std::min(4, p->stages));
 }
 
 template <bool CX, typename T>
-int launch_range(const MvmPlan *p, const MvLaunch &base, uint32_t first, uint32_t last,
-                 cudaStream_t st) {
-  const MvItems &ph = p->items;
+int launch_range(const MvmPlan *p, const MvItems &ph, const MvLaunch &base, uint32_t first,
+                 uint32_t last, cudaStream_t st) {
   if (last <= first) return H2B_OK;
   MvLaunch L = base;
   L.items = ph.items;
   L.first = first;
   L.n = last - first;
-  L.stages = (uint32_t) std::max(2, std::min(8, p->stages));
+  ring_shape(p, L.nw, L.stages);
   L.panel_bytes = panel_region<T>(ph);
   L.xcol_bytes = xcol_region<CX>(ph);
   L.stage_bytes = stage_of<CX, T>(ph, L.nrhs);
-  L.red_doubles = (uint32_t) ((size_t) NWARP * std::max<uint32_t>(ph.max_rows, 1) * (CX ? 2 : 1));
   const size_t smem = smem_of<CX, T>(ph, L.stages, L.nrhs);
-  if (smem > H2B_MAX_DYN_SMEM || ph.max_rows > MAXROWS || ph.max_x > 65536) {
-    h2b_set_error("matvec: item panel of %u bytes / %u rows / %u right-hand sides exceeds the "
-                  "kernel's limits", ph.max_bytes, ph.max_rows, L.nrhs);
+  if (smem > H2B_MAX_DYN_SMEM || ph.max_rows > MAXROWS || ph.max_cols_t > MAXROWS ||
+      ph.max_x > 65536) {
+    h2b_set_error("matvec: item panel of %u bytes / %u rows / %u transposed columns / %u "
+                  "right-hand sides exceeds the kernel's limits (%zu bytes of shared memory)",
+                  ph.max_bytes, ph.max_rows, ph.max_cols_t, L.nrhs, smem);
     return H2B_ERR_ARG;
   }
+  const int threads = (int) (L.nw + 1) * 32;
   H2B_CUDA_TRY((h2b_allow_smem<mv_items_kernel<CX, T>>()));
   int occ = 0;
   H2B_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, mv_items_kernel<CX, T>,
-                                                             TPB + 32, smem));
+                                                             threads, smem));
   if (occ < 1) {
     h2b_set_error("matvec: the item kernel does not fit an SM (%zu bytes of shared memory)", smem);
     return H2B_ERR_ARG;
@@ -487,7 +465,7 @@ int launch_range(const MvmPlan *p, const MvLaunch &base, uint32_t first, uint32_
   const int sms = p->num_sms > 0 ? p->num_sms : 148;
   const int per_sm = std::min(occ, std::max(1, p->ctas_per_sm));
   const uint32_t grid = std::min<uint32_t>(L.n, (uint32_t) (per_sm * sms));
-  mv_items_kernel<CX, T><<<grid, TPB + 32, smem, st>>>(L);
+  mv_items_kernel<CX, T><<<grid, threads, smem, st>>>(L);
   h2b_note_launch();
   return H2B_OK;
 }
@@ -521,12 +499,12 @@ int launch_all(const MvmPlan *p, const double *x, size_t ldx, double *y, size_t 
   L.sx[H2B_MV_COUPLING] = v.sxt, L.sy[H2B_MV_COUPLING] = v.syt;
   L.X[H2B_MV_BACKWARD] = v.yt, L.Y[H2B_MV_BACKWARD] = v.yp;
   L.sx[H2B_MV_BACKWARD] = v.syt, L.sy[H2B_MV_BACKWARD] = v.syp;
-  const MvItems &it = p->items;
+  const MvItems &it = SINGLE ? p->items_single : p->items;
   // forward + nearfield, coupling (reads xt), backward (reads yt)
-  int rc = launch_range<CX, T>(p, L, 0, it.start[H2B_MV_COUPLING], st);
+  int rc = launch_range<CX, T>(p, it, L, 0, it.start[H2B_MV_COUPLING], st);
   if (rc == H2B_OK)
-    rc = launch_range<CX, T>(p, L, it.start[H2B_MV_COUPLING], it.start[H2B_MV_BACKWARD], st);
-  if (rc == H2B_OK) rc = launch_range<CX, T>(p, L, it.start[H2B_MV_BACKWARD], it.n, st);
+    rc = launch_range<CX, T>(p, it, L, it.start[H2B_MV_COUPLING], it.start[H2B_MV_BACKWARD], st);
+  if (rc == H2B_OK) rc = launch_range<CX, T>(p, it, L, it.start[H2B_MV_BACKWARD], it.n, st);
   if (rc != H2B_OK) return rc;
   scatter_multi_kernel<CX><<<gz, 256, 0, st>>>(v, p->ridx, y, ldy, p->nrow, ar, ai);
   h2b_note_launch();
@@ -560,8 +538,10 @@ extern "C" int h2b_mvm_prepare(void) {
   return H2B_OK;
 }
 
-extern "C" size_t h2b_mvm_smem_bytes(const MvmPlan *p, int single, int stages) {
-  const MvItems &ph = p->items;
+extern "C" size_t h2b_mvm_smem_bytes(const MvmPlan *p, int single) {
+  const MvItems &ph = single ? p->items_single : p->items;
+  uint32_t nw, stages;
+  ring_shape(p, nw, stages);
   if (p->cx)
     return single ? smem_of<true, float>(ph, stages, 1) : smem_of<true, double>(ph, stages, 1);
   return single ? smem_of<false, float>(ph, stages, 1) : smem_of<false, double>(ph, stages, 1);

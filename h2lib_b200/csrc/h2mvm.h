@@ -17,7 +17,6 @@
 #define H2B_MV_BACKWARD 3u
 #define H2B_MV_KIND 3u       // flags & H2B_MV_KIND: the kind
 #define H2B_MV_TRANS 4u      // y += P^T x
-#define H2B_MV_NONE 0xFFFFFFFFu
 struct MvItem {
   uint64_t p;                // element offset of the panel in its array
   uint32_t rows, cols;
@@ -34,11 +33,12 @@ struct MvItems {
   uint32_t start[4];
   uint32_t max_bytes;        // largest panel in bytes at FP64 storage
   uint32_t max_rows;         // largest rows of an untransposed item
+  uint32_t max_cols_t;       // largest columns of a transposed item
   uint32_t max_x;            // longest x slice (elements: cols, or rows when transposed)
 };
 
 // Default largest panel of a work item (bytes at FP64 storage); blocks and slices are split to fit.
-#define H2B_MV_PANEL_BYTES (32u * 1024u)
+#define H2B_MV_PANEL_BYTES (16u * 1024u)
 
 struct MvmPlan {
   int cx, num_sms;
@@ -46,13 +46,15 @@ struct MvmPlan {
   uint32_t nrow, ncol, nrow_clusters, ncol_clusters;
   const uint32_t *ridx, *cidx;   // device index arrays of the row / column tree
   double *xp, *yp, *xt, *yt;     // work vectors of one column
-  MvItems items;
+  MvItems items;                 // the FP64 product's items
+  MvItems items_single;          // the items of the product from the FP32 copies (larger panels)
   // panel arrays (FP64) and their FP32 copies (NULL until made)
   const double *Wc, *Wr, *N, *S;
   const float *fWc, *fWr, *fN, *fS;
   int *err;                      // device flag: a wait for a panel copy ran out
-  // launch shape of the item kernel: resident CTAs per SM and pipeline stages
-  int ctas_per_sm, stages;
+  // launch shape of the item kernel: resident CTAs per SM, consumer warps per CTA and ring
+  // stages per consumer warp
+  int ctas_per_sm, warps, stages;
 };
 
 extern "C" int h2b_mvm_launch(const MvmPlan *p, const double *x, double *y, double ar, double ai,
@@ -73,5 +75,5 @@ extern "C" int h2b_mvm_launch_batch(const MvmPlan *p, int single, uint32_t nrhs,
 // Sets the item kernel's shared-memory limit (once per process); called when a matrix is made,
 // so that no later launch, possibly inside a CUDA graph capture, has to.
 extern "C" int h2b_mvm_prepare(void);
-// Shared-memory bytes of the item kernel for a launch shape (for the autotuner's candidates).
-extern "C" size_t h2b_mvm_smem_bytes(const MvmPlan *p, int single, int stages);
+// Shared-memory bytes per CTA of the item kernel at the plan's launch shape.
+extern "C" size_t h2b_mvm_smem_bytes(const MvmPlan *p, int single);

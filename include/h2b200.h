@@ -248,12 +248,14 @@ int h2b_h2matrix_set_precision(h2b_h2matrix *h2, int precision);
 
 /* Launch shape of the matrix-vector product (the knobs h2b_h2matrix_autotune searches):
  * shape[0] rows per forward slice of a flattened column basis, [1] rows per backward slice of the
- * row basis, [2] resident CTAs per SM of the item kernel, [3] shared-memory pipeline stages per
- * CTA, [4] largest panel of a work item in KiB at FP64 storage (4..64; blocks and slices are
- * split to fit), [5] leaf-basis CTAs per leaf.  A value of 0 keeps the current setting.  Slice
- * and panel sizes belong to the matrix's structure: a matrix made with h2b_h2matrix_new_like
- * shares them and can change only [2], [3] and [5].  No reference counterpart. */
-#define H2B_SHAPE_N 6
+ * row basis, [2] resident CTAs per SM of the item kernel, [3] shared-memory ring stages per
+ * consumer warp (1..4), [4] largest panel of a work item in KiB at FP64 storage (4..64; blocks
+ * and slices are split to fit; the FP32 product's items hold twice the entries), [5] leaf-basis
+ * CTAs per leaf, [6] consumer warps per CTA of the item kernel (1..8).  A value of 0 keeps the
+ * current setting.  Slice and panel sizes belong to the matrix's structure: a matrix made with
+ * h2b_h2matrix_new_like shares them and can change only [2], [3], [5] and [6].  No reference
+ * counterpart. */
+#define H2B_SHAPE_N 7
 int h2b_h2matrix_set_matvec_shape(h2b_h2matrix *h2, const uint32_t shape[H2B_SHAPE_N]);
 int h2b_h2matrix_get_matvec_shape(const h2b_h2matrix *h2, uint32_t shape[H2B_SHAPE_N]);
 
