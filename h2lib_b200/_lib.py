@@ -89,6 +89,10 @@ _SIGS = {
     "h2b_h2matrix_set_precision": (C.c_int, [vp, C.c_int]),
     "h2b_h2matrix_set_matvec_shape": (C.c_int, [vp, _u32p]),
     "h2b_h2matrix_get_matvec_shape": (C.c_int, [vp, _u32p]),
+    "h2b_h2matrix_autotune": (C.c_int, [vp, C.c_uint32, _u32p, _f64p]),
+    "h2b_autotune_save": (C.c_int, [C.c_char_p]),
+    "h2b_autotune_load": (C.c_int, [C.c_char_p]),
+    "h2b_autotune_clear": (C.c_int, []),
     "h2b_h2matrix_addeval_single": (C.c_int, [C.c_double, C.c_double, vp, vp, vp]),
     "h2b_residual_norm": (C.c_int, [C.c_uint32, vp, _f64p, vp, vp, C.POINTER(C.c_double)]),
     "h2b_solve_gmres_noalloc": (C.c_int, [C.c_uint32, vp, _f64p, vp, vp, C.c_double,
@@ -106,6 +110,10 @@ _SIGS = {
     "h2b_l2_error_harmonic_multi": (C.c_int, [vp, C.c_uint32, _u32p, C.c_uint32, _f64p, vp,
                                               _f64p, _f64p]),
     "h2b_integrate_plane_wave": (C.c_int, [vp, _f64p, _f64p, C.c_double, C.c_double, vp]),
+    "h2b_integrate_point_source": (C.c_int, [vp, _f64p, C.c_double, C.c_double, C.c_double,
+                                             vp]),
+    "h2b_eval_brakhage_werner": (C.c_int, [vp, C.c_uint32, _f64p, vp, C.c_double, C.c_double,
+                                           vp]),
 }
 
 

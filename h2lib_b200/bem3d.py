@@ -279,6 +279,32 @@ class H2Matrix:
         check(lib.h2b_h2matrix_make_single(self.handle), "h2matrix_make_single")
         return self
 
+    SHAPE_NAMES = ("fwd_rows", "back_rows", "ctas_per_sm", "stages_per_warp", "panel_kib",
+                   "leaf_ctas", "consumer_warps")
+
+    def matvec_shape(self):
+        """The launch shape of the matvec and leaf-basis kernels (h2b_h2matrix_get_matvec_shape)."""
+        sh = np.zeros(7, dtype=np.uint32)
+        check(lib.h2b_h2matrix_get_matvec_shape(self.handle, sh), "get_matvec_shape")
+        return dict(zip(self.SHAPE_NAMES, (int(v) for v in sh)))
+
+    def set_matvec_shape(self, **kw):
+        """Sets entries of the launch shape by name (see matvec_shape); the others are kept."""
+        sh = np.zeros(7, dtype=np.uint32)
+        for k, v in kw.items():
+            sh[self.SHAPE_NAMES.index(k)] = v
+        check(lib.h2b_h2matrix_set_matvec_shape(self.handle, sh), "set_matvec_shape")
+        return self
+
+    def autotune(self, matvec=True, leaf=False):
+        """h2b_h2matrix_autotune: the chosen shape and the costs (device ms) before and after."""
+        flags = (1 if matvec else 0) | (2 if leaf else 0)
+        sh = np.zeros(7, dtype=np.uint32)
+        ms = np.zeros(4)
+        check(lib.h2b_h2matrix_autotune(self.handle, flags, sh, ms), "autotune")
+        return dict(shape=self.matvec_shape(), matvec_ms=(float(ms[0]), float(ms[1])),
+                    bases_ms=(float(ms[2]), float(ms[3])))
+
     def info(self):
         info = np.zeros(8, dtype=np.uint64)
         check(lib.h2b_h2matrix_info(self.handle, info), "h2matrix_info")
@@ -462,6 +488,49 @@ def integrate_plane_wave(bem, kvec, src=(0.0, 0.0, 0.0), coef=1.0, b=None):
                                        np.asarray(src, dtype=np.float64), coef.real, coef.imag,
                                        _ptr(b)), "integrate_plane_wave")
     return b
+
+
+def integrate_point_source(bem, src, k, coef=1.0, b=None):
+    """b_i = coef * int e^{ik|x - src|} / |x - src| phi_i(x) dx with the row basis
+    (integrate_bem3d_c/l_avector with rhs_dirichlet_point_helmholtzbem3d, Library/bem3d.c:8579,
+    :8631, Library/helmholtzbem3d.c:1521)."""
+    if b is None:
+        b = np.zeros(bem.rows, dtype=np.complex128)
+    coef = complex(coef)
+    check(lib.h2b_integrate_point_source(bem.handle, np.asarray(src, dtype=np.float64), float(k),
+                                         coef.real, coef.imag, _ptr(b)), "integrate_point_source")
+    return b
+
+
+def eval_brakhage_werner(bem, w, points, eta):
+    """Brakhage-Werner potential of the density w at the points (n x 3) outside the surface
+    (eval_brakhage_werner_c / _l, Tests/test_helmholtzbem3d.c:68 / :134)."""
+    pts = np.ascontiguousarray(points, dtype=np.float64).reshape(-1, 3)
+    w = np.ascontiguousarray(w, dtype=np.complex128)
+    u = np.zeros(len(pts), dtype=np.complex128)
+    eta = complex(eta)
+    check(lib.h2b_eval_brakhage_werner(bem.handle, len(pts), pts.ravel(), _ptr(w), eta.real,
+                                       eta.imag, _ptr(u)), "eval_brakhage_werner")
+    return u
+
+
+def outer_points(n=20, half=10.0):
+    """The evaluation points of the reference's exterior test (max_rel_outer_error,
+    Tests/test_helmholtzbem3d.c:224): an n x n grid of the plane y = 0 over [-half, half]^2,
+    the points with x^2 + z^2 > 1."""
+    pts = []
+    for j in range(n):
+        for i in range(n):
+            p = (-half + (2 * half / (n - 1)) * i, 0.0, -half + (2 * half / (n - 1)) * j)
+            if p[0] ** 2 + p[2] ** 2 > 1:
+                pts.append(p)
+    return np.array(pts)
+
+
+def point_source_field(points, src, k):
+    """e^{ik|x - src|} / |x - src| (rhs_dirichlet_point_helmholtzbem3d)."""
+    r = np.linalg.norm(np.asarray(points) - np.asarray(src), axis=1)
+    return np.exp(1j * k * r) / r
 
 
 def quad_export(q, q2, row_basis, col_basis, which):

@@ -196,6 +196,7 @@ extern "C" void h2b_h2matrix_del(h2b_h2matrix *h) {
   cudaStream_t st = h->st;
   if (st) cudaStreamSynchronize(st);
   if (h->cst) cudaStreamSynchronize(h->cst);  // pending asynchronous exports read the blocks
+  if (h->shared && h->owner) h->owner->sharers.n--;
   // the operator's own data
   for (DevCTree *t : {&h->rt, &h->ct}) {
     dfree(t->d_V, st); dfree(t->d_E, st); dfree(t->d_W, st);
@@ -372,6 +373,7 @@ extern "C" h2b_h2matrix *h2b_h2matrix_new(const h2b_bem *bem, const h2b_tree *tr
     h->h_nrc = nrc;
     h->h_ncc = ncc;
     h->h_noff = noff;
+    h2b_tune_lookup(h);
     rc = h2b_h2_build_mv_items(h);
   }
   // single-triangle rule (raw and linear-basis weighted)
@@ -413,6 +415,9 @@ extern "C" h2b_h2matrix *h2b_h2matrix_new_like(const h2b_bem *bem, const h2b_h2m
   h2b_h2matrix *h = new h2b_h2matrix(*like);
   h->bem = bem;
   h->shared = 1;
+  // the structure's owner: the model matrix itself, or the matrix it shares with
+  h->owner = like->shared ? like->owner : like;
+  h->owner->sharers.n++;
   h->st = nullptr;
   h->cst = nullptr;
   h->ev_copy = nullptr;
@@ -663,9 +668,9 @@ extern "C" int h2b_h2matrix_set_matvec_shape(h2b_h2matrix *h, const uint32_t sha
     return H2B_ERR_ARG;
   }
   if (fr != h->mv_fwd_rows || br != h->mv_back_rows || pb != h->mv_panel_bytes) {
-    if (h->shared) {
-      h2b_set_error("h2b_h2matrix_set_matvec_shape: slice and panel sizes belong to the shared "
-                    "structure");
+    if (h->shared || h->sharers.n > 0) {
+      h2b_set_error("h2b_h2matrix_set_matvec_shape: slice and panel sizes belong to a structure "
+                    "that other matrices share");
       return H2B_ERR_STATE;
     }
     H2B_CUDA_TRY(cudaStreamSynchronize(h->st));  // no product reads the old items

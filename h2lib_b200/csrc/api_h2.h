@@ -1,6 +1,8 @@
 // H2 matrix handle layout shared by api_h2.cu and api_solve.cu.
 #pragma once
 
+#include <atomic>
+
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -62,6 +64,16 @@ struct h2b_h2matrix {
   // 1: the tree, block and nearfield-plan arrays belong to another matrix (h2b_h2matrix_new_like);
   // only the operator's own data (bases, transfers, W, S, N, work vectors) are freed here
   int shared = 0;
+  // the matrix whose structure this one shares, and (on that matrix) how many matrices share its
+  // structure: while any do, its slice and panel sizes (the shared work items) stay fixed
+  const h2b_h2matrix *owner = nullptr;
+  struct Count {  // a copy (h2b_h2matrix_new_like) starts at zero
+    std::atomic<int> n{0};
+    Count() = default;
+    Count(const Count &) {}
+    Count &operator=(const Count &) { return *this; }
+  };
+  mutable Count sharers;
   cudaStream_t st = nullptr;
   DevCTree rt, ct;
   uint32_t nadm = 0, nnear = 0, ntiles = 0, nsing = 0;
@@ -92,6 +104,8 @@ struct h2b_h2matrix {
 void h2b_h2_fill_mvm_plan(h2b_h2matrix *h);
 // (Re)build the matvec work items from the structure and the matrix's slice knobs (owner only).
 int h2b_h2_build_mv_items(h2b_h2matrix *h);
+// Applies the autotuner's cached shape for h's size class, if any (before the items are built).
+void h2b_tune_lookup(h2b_h2matrix *h);
 // H2B_ERR_TIMEOUT (and the flag cleared) if a matvec of h lost a panel copy; synchronises h->st.
 int h2b_h2_check_mv_error(const h2b_h2matrix *h);
 // Bytes of slack after every panel array: a panel copy may read up to 15 bytes past its panel.

@@ -252,12 +252,38 @@ int h2b_h2matrix_set_precision(h2b_h2matrix *h2, int precision);
  * consumer warp (1..4), [4] largest panel of a work item in KiB at FP64 storage (4..64; blocks
  * and slices are split to fit; the FP32 product's items hold twice the entries), [5] leaf-basis
  * CTAs per leaf, [6] consumer warps per CTA of the item kernel (1..8).  A value of 0 keeps the
- * current setting.  Slice and panel sizes belong to the matrix's structure: a matrix made with
- * h2b_h2matrix_new_like shares them and can change only [2], [3], [5] and [6].  No reference
- * counterpart. */
+ * current setting.  Slice and panel sizes belong to the matrix's structure: while matrices made
+ * with h2b_h2matrix_new_like share it, neither they nor the model matrix can change them (only
+ * [2], [3], [5] and [6]; H2B_ERR_STATE otherwise).  No reference counterpart. */
 #define H2B_SHAPE_N 7
 int h2b_h2matrix_set_matvec_shape(h2b_h2matrix *h2, const uint32_t shape[H2B_SHAPE_N]);
 int h2b_h2matrix_get_matvec_shape(const h2b_h2matrix *h2, uint32_t shape[H2B_SHAPE_N]);
+
+/* Autotuner: times candidate launch shapes on the assembled matrix itself (CUDA events on its
+ * stream) and keeps the fastest.  H2B_TUNE_MATVEC searches the matvec shape (panels of 12, 16
+ * and 24 KiB with slices as wide, 2..8 CTAs per SM, 1..4 consumer warps, 1..2 stages per warp,
+ * every candidate whose CTAs fit an SM together); the cost is the FP64 product's time, plus the
+ * FP32 product's when the matrix has FP32 copies.  A matrix whose structure is shared
+ * (h2b_h2matrix_new_like, either side) keeps its panel size, and matrices made like this one
+ * before the call keep their own launch shape.  H2B_TUNE_LEAF times the assembly of both cluster
+ * bases at 1, 2, 4 and 8 CTAs per leaf and leaves the bases as the chosen split assembles them
+ * (the splits order a leaf's quadrature sums differently, so entries change by rounding only;
+ * FP32 copies are remade afterwards).  The result goes to a process-wide cache keyed by
+ * (complex, rank k, floor(log2(rows * columns))) that h2b_h2matrix_new applies to later matrices
+ * of the same class.  shape (optional) receives the chosen shape, ms (optional) [0] the matvec
+ * cost at the starting shape, [1] at the chosen one, [2] the basis assembly at the starting
+ * split, [3] at the chosen one (0 where not tuned).  Every candidate gives the same product up
+ * to FP64 rounding (only the grouping of the atomic additions changes).  No reference
+ * counterpart (H2Lib's only knob is its OpenMP task depth, Library/basic.c). */
+#define H2B_TUNE_MATVEC 1u
+#define H2B_TUNE_LEAF 2u
+int h2b_h2matrix_autotune(h2b_h2matrix *h2, uint32_t flags, uint32_t shape[H2B_SHAPE_N],
+                          double ms[4]);
+/* The autotuner's cache as text (one line per size class), to carry tuned shapes across
+ * processes; load merges into the cache and rejects a malformed file; clear empties it. */
+int h2b_autotune_save(const char *path);
+int h2b_autotune_load(const char *path);
+int h2b_autotune_clear(void);
 
 /* FP32 copies of the nearfield blocks, coupling matrices and flattened cluster bases, read by the
  * mixed-precision matvec (half the bytes of the FP64 product).  Call after assembly; any later
@@ -414,6 +440,25 @@ int h2b_l2_error_harmonic_multi(const h2b_bem *bem, uint32_t surfaces,
  * datum -u_inc of a sound-soft scatterer.  b: interleaved complex, host or device. */
 int h2b_integrate_plane_wave(const h2b_bem *bem, const double kvec[3], const double src[3],
                              double coef_re, double coef_im, double *b);
+
+/* b = coef * int f(x) phi_i(x) dx for the point source f(x) = e^{ik|x - src|} / |x - src| (real
+ * k >= 0), tested with the operator's row basis: b[t] per triangle for the constant basis, b[v]
+ * per vertex for the linear basis.  Replaces integrate_bem3d_c_avector / _l_avector
+ * (Library/bem3d.c:8579 / :8631) with rhs_dirichlet_point_helmholtzbem3d
+ * (Library/helmholtzbem3d.c:1521), the Dirichlet datum of the reference's exterior test problem
+ * (Tests/test_helmholtzbem3d.c:422) whose exact solution is f itself.  b: interleaved complex,
+ * host or device. */
+int h2b_integrate_point_source(const h2b_bem *bem, const double src[3], double k, double coef_re,
+                               double coef_im, double *b);
+
+/* u[p] = the Brakhage-Werner potential of the density w (the operator's column basis, complex) at
+ * points[3 p] outside the surface: sum over triangles of int (d_n(y) G(x, y) - i eta G(x, y)) w(y)
+ * dy with the operator's wavenumber, by the single-triangle rule.  The evaluation of
+ * eval_brakhage_werner_c / _l (Tests/test_helmholtzbem3d.c:68 / :134), with which the reference
+ * states a solve's error against the exact exterior field.  npoints <= 2^24; points, w, u host or
+ * device (u interleaved complex). */
+int h2b_eval_brakhage_werner(const h2b_bem *bem, uint32_t npoints, const double *points,
+                             const double *w, double eta_re, double eta_im, double *u);
 
 /* ------------------------------------------------------------------------------------------
  * Solve server: continuous admission of Dirichlet solves (no counterpart in the reference,
