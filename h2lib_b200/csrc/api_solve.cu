@@ -427,6 +427,123 @@ __global__ void plane_wave_kernel(HarmArgs a, double k0, double k1, double k2, d
   b[2 * t + 1] = cre * si + cim * sr;
 }
 
+// e^{i k r} / r, the Helmholtz point source of rhs_dirichlet_point_helmholtzbem3d
+// (Library/helmholtzbem3d.c:1521), at distance r
+__device__ __forceinline__ void point_wave(double k, double r, double &re, double &im) {
+  double s, c;
+  sincos(k * r, &s, &c);
+  re = c / r;
+  im = s / r;
+}
+
+// Dirichlet datum of a point source at (z0, z1, z2) tested with the basis: b[t] =
+// coef g_t sum_q w_q f(x_q) for the constant basis (integrate_bem3d_c_avector,
+// Library/bem3d.c:8579), b[v] += coef g_t sum_q w_l(q) f(x_q) over the triangle's vertices v_l
+// for the linear basis (integrate_bem3d_l_avector, :8631); f = e^{ik|x-z|} / |x-z|
+__global__ void point_source_kernel(HarmArgs a, double k, double cre, double cim, int linear,
+                                    double *b) {
+  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= a.nt) return;
+  const TriRec &T = a.tri[t];
+  double sr[3] = {0.0, 0.0, 0.0}, si[3] = {0.0, 0.0, 0.0};
+  for (int q = 0; q < a.ns; q++) {
+    double X[3];
+    tri_point(T, a.xs[q], a.ys[q], X);
+    const double d0 = X[0] - a.z0, d1 = X[1] - a.z1, d2 = X[2] - a.z2;
+    double fr, fi;
+    point_wave(k, sqrt(d0 * d0 + d1 * d1 + d2 * d2), fr, fi);
+    if (linear) {
+      for (int l = 0; l < 3; l++) {
+        sr[l] += a.wsl[l * a.ns + q] * fr;
+        si[l] += a.wsl[l * a.ns + q] * fi;
+      }
+    } else {
+      sr[0] += a.ws[q] * fr;
+      si[0] += a.ws[q] * fi;
+    }
+  }
+  for (int l = 0; l < (linear ? 3 : 1); l++) {
+    const double re = sr[l] * T.g, im = si[l] * T.g;
+    const double br = cre * re - cim * im, bi = cre * im + cim * re;
+    if (linear) {
+      atomicAdd(&b[2 * T.v[l]], br);
+      atomicAdd(&b[2 * T.v[l] + 1], bi);
+    } else {
+      b[2 * t] = br;
+      b[2 * t + 1] = bi;
+    }
+  }
+}
+
+// Brakhage-Werner potential u(x) = sum_t w_t int_t (d_n(y) G(x, y) - i eta G(x, y)) dy of the
+// density w at points x outside the surface, G the Helmholtz fundamental solution with the
+// operator's k (complex), by the single-triangle rule: per quadrature point y_q, with d = x - y_q
+// and r = |d|, kconst g_t w_t(q) e^{ikr} / r^3 ((1 - ikr) d.n - i eta r^2); w_t(q) = w[t] w_q for
+// the constant basis, sum_l w[v_l] w_l(q) for the linear basis.  One CTA per point, threads over
+// triangles, a fixed-order reduction (the same sum on every run).  Evaluation of
+// eval_brakhage_werner_c / _l (Tests/test_helmholtzbem3d.c:68 / :134).
+constexpr int BW_THREADS = 256;
+__global__ void __launch_bounds__(BW_THREADS)
+    bw_eval_kernel(HarmArgs a, const double *pts, const double *w, int linear, double kr,
+                   double ki, double er, double ei, double kconst, double *out) {
+  __shared__ double red[2][BW_THREADS / 32];
+  const double *x = pts + 3 * (size_t) blockIdx.x;
+  const double x0 = x[0], x1 = x[1], x2 = x[2];
+  double ur = 0.0, ui = 0.0;
+  for (uint32_t t = threadIdx.x; t < a.nt; t += BW_THREADS) {
+    const TriRec &T = a.tri[t];
+    double wr[3], wi[3];
+    if (linear) {
+      for (int l = 0; l < 3; l++) wr[l] = w[2 * T.v[l]], wi[l] = w[2 * T.v[l] + 1];
+    } else {
+      wr[0] = w[2 * t], wi[0] = w[2 * t + 1];
+    }
+    double sr = 0.0, si = 0.0;
+    for (int q = 0; q < a.ns; q++) {
+      double Y[3];
+      tri_point(T, a.xs[q], a.ys[q], Y);
+      const double d0 = x0 - Y[0], d1 = x1 - Y[1], d2 = x2 - Y[2];
+      const double r2 = d0 * d0 + d1 * d1 + d2 * d2, r = sqrt(r2);
+      const double dn = d0 * T.n[0] + d1 * T.n[1] + d2 * T.n[2];
+      double s, c;
+      sincos(kr * r, &s, &c);
+      const double e = exp(-ki * r) / (r2 * r);
+      // (1 - ikr) dn - i eta r^2 with k = kr + i ki, eta = er + i ei
+      const double pr = (1.0 + ki * r) * dn + ei * r2, pi = -kr * r * dn - er * r2;
+      const double qr = e * (c * pr - s * pi), qi = e * (c * pi + s * pr);
+      // weight of the point: the density at y_q
+      double vr, vi;
+      if (linear) {
+        vr = vi = 0.0;
+        for (int l = 0; l < 3; l++) {
+          vr += a.wsl[l * a.ns + q] * wr[l];
+          vi += a.wsl[l * a.ns + q] * wi[l];
+        }
+      } else {
+        vr = a.ws[q] * wr[0];
+        vi = a.ws[q] * wi[0];
+      }
+      sr += qr * vr - qi * vi;
+      si += qr * vi + qi * vr;
+    }
+    ur += sr * T.g;
+    ui += si * T.g;
+  }
+  ur = warp_sum(ur);
+  ui = warp_sum(ui);
+  if ((threadIdx.x & 31) == 0) {
+    red[0][threadIdx.x >> 5] = ur;
+    red[1][threadIdx.x >> 5] = ui;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double a0 = 0.0, a1 = 0.0;
+    for (int i = 0; i < BW_THREADS / 32; i++) a0 += red[0][i], a1 += red[1][i];
+    out[2 * blockIdx.x] = kconst * a0;
+    out[2 * blockIdx.x + 1] = kconst * a1;
+  }
+}
+
 // Several surfaces (triangle ranges tri_off[s] .. tri_off[s+1]) and right-hand sides: the source
 // of (surface s, column r) is zs[3 (s + r nseg)].  Columns of the vertex vectors are nv long.
 struct MultiZ {
@@ -740,6 +857,73 @@ extern "C" int h2b_integrate_plane_wave(const h2b_bem *bem, const double kvec[3]
                                                           coef_im, db);
   H2B_CUDA_TRY(cudaGetLastError());
   H2B_CUDA_TRY(cudaMemcpyAsync(b, db, sizeof(double) * 2 * s->nt, cudaMemcpyDefault, st));
+  H2B_CUDA_TRY(cudaStreamSynchronize(st));
+  return H2B_OK;
+}
+
+extern "C" int h2b_integrate_point_source(const h2b_bem *bem, const double src[3], double k,
+                                          double coef_re, double coef_im, double *b) {
+  if (!bem || !src || !b) {
+    h2b_set_error("h2b_integrate_point_source: NULL argument");
+    return H2B_ERR_ARG;
+  }
+  const h2b_surface *s = bem->s;
+  const int linear = bem->row_basis == H2B_BASIS_LINEAR;
+  const size_t n = linear ? s->nv : s->nt;
+  cudaStream_t st = s->stream;
+  DevBuf buf;
+  buf.st = st;
+  H2B_CUDA_TRY(cudaMallocAsync(&buf.p, sizeof(double) * (2 * n + 6 * 64), st));
+  double *db = (double *) buf.p, *rule = db + 2 * n;
+  HarmArgs a;
+  int rc = harm_args(bem, src, rule, &a, st);
+  if (rc != H2B_OK) return rc;
+  if (linear) H2B_CUDA_TRY(cudaMemsetAsync(db, 0, sizeof(double) * 2 * n, st));
+  point_source_kernel<<<(s->nt + 127) / 128, 128, 0, st>>>(a, k, coef_re, coef_im, linear, db);
+  h2b_note_launch();
+  H2B_CUDA_TRY(cudaGetLastError());
+  H2B_CUDA_TRY(cudaMemcpyAsync(b, db, sizeof(double) * 2 * n, cudaMemcpyDefault, st));
+  H2B_CUDA_TRY(cudaStreamSynchronize(st));
+  return H2B_OK;
+}
+
+extern "C" int h2b_eval_brakhage_werner(const h2b_bem *bem, uint32_t npoints, const double *points,
+                                        const double *w, double eta_re, double eta_im,
+                                        double *u) {
+  if (!bem || (npoints && (!points || !w || !u))) {
+    h2b_set_error("h2b_eval_brakhage_werner: NULL argument");
+    return H2B_ERR_ARG;
+  }
+  if (bem->pde != H2B_HELMHOLTZ) {
+    h2b_set_error("h2b_eval_brakhage_werner: needs a Helmholtz operator");
+    return H2B_ERR_ARG;
+  }
+  if (npoints == 0) return H2B_OK;
+  if (npoints > (1u << 24)) {
+    h2b_set_error("h2b_eval_brakhage_werner: at most 2^24 points per call");
+    return H2B_ERR_ARG;
+  }
+  const h2b_surface *s = bem->s;
+  const int linear = bem->col_basis == H2B_BASIS_LINEAR;
+  const size_t n = linear ? s->nv : s->nt;
+  cudaStream_t st = s->stream;
+  DevBuf buf;
+  buf.st = st;
+  H2B_CUDA_TRY(cudaMallocAsync(&buf.p, sizeof(double) * (2 * n + 5 * (size_t) npoints + 6 * 64),
+                               st));
+  double *dw = (double *) buf.p, *dp = dw + 2 * n, *du = dp + 3 * (size_t) npoints,
+         *rule = du + 2 * (size_t) npoints;
+  const double z0[3] = {0.0, 0.0, 0.0};
+  HarmArgs a;
+  int rc = harm_args(bem, z0, rule, &a, st);
+  if (rc != H2B_OK) return rc;
+  H2B_CUDA_TRY(cudaMemcpyAsync(dw, w, sizeof(double) * 2 * n, cudaMemcpyDefault, st));
+  H2B_CUDA_TRY(cudaMemcpyAsync(dp, points, sizeof(double) * 3 * npoints, cudaMemcpyDefault, st));
+  bw_eval_kernel<<<npoints, BW_THREADS, 0, st>>>(a, dp, dw, linear, bem->k_re, bem->k_im, eta_re,
+                                                 eta_im, bem->kconst, du);
+  h2b_note_launch();
+  H2B_CUDA_TRY(cudaGetLastError());
+  H2B_CUDA_TRY(cudaMemcpyAsync(u, du, sizeof(double) * 2 * npoints, cudaMemcpyDefault, st));
   H2B_CUDA_TRY(cudaStreamSynchronize(st));
   return H2B_OK;
 }

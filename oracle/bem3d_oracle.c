@@ -1347,3 +1347,88 @@ orc_l2_error_harmonic(uint32_t nv, const double *x, uint32_t nt, const uint32_t 
   *norm = sqrt(nn);
   return 0;
 }
+
+/* Dirichlet datum of the point source f(x) = e^{ik|x - z|} / |x - z| tested with the constant
+ * (b per triangle) or linear basis (b per vertex), by the single-triangle rule:
+ * integrate_bem3d_c_avector / integrate_bem3d_l_avector (Library/bem3d.c:8579 / :8631) with
+ * rhs_dirichlet_point_helmholtzbem3d (Library/helmholtzbem3d.c:1521).  b interleaved complex. */
+int
+orc_integrate_point_source(uint32_t nv, const double *x, uint32_t nt, const uint32_t *t,
+                           const double *g, uint32_t q, int linear, const double z[3], double k,
+                           double *b)
+{
+  double xs[4096], ys[4096], ws[4096];
+  uint32_t i, l, qq, ns = q * q, n = linear ? nv : nt;
+  if (single_rule(q, xs, ys, ws)) return -1;
+  for (i = 0; i < 2 * n; i++) b[i] = 0.0;
+  for (i = 0; i < nt; i++) {
+    const uint32_t *tv = t + 3 * (size_t) i;
+    const double *A = x + 3 * (size_t) tv[0], *B = x + 3 * (size_t) tv[1], *C = x + 3 * (size_t) tv[2];
+    for (l = 0; l < (linear ? 3u : 1u); l++) {
+      cplx sum = 0.0;
+      for (qq = 0; qq < ns; qq++) {
+        double tx = xs[qq], sx = ys[qq], X[3], r;
+        int d;
+        for (d = 0; d < 3; d++) X[d] = A[d] * (1.0 - tx) + B[d] * (tx - sx) + C[d] * sx;
+        r = sqrt((X[0] - z[0]) * (X[0] - z[0]) + (X[1] - z[1]) * (X[1] - z[1]) +
+                 (X[2] - z[2]) * (X[2] - z[2]));
+        sum += (linear ? ws[qq] * nodal(1, l, tx, sx) : ws[qq]) * cexp(I * k * r) / r;
+      }
+      sum *= g[i];
+      {
+        const uint32_t o = linear ? tv[l] : i;
+        b[2 * o] += creal(sum);
+        b[2 * o + 1] += cimag(sum);
+      }
+    }
+  }
+  return 0;
+}
+
+/* Brakhage-Werner potential of the density w (constant: per triangle, linear: per vertex;
+ * interleaved complex) at npoints points: sum over triangles of
+ * 1/(4 pi) g_t sum_q w(y_q) e^{ikr} / r^3 ((1 - ikr) d.n - i eta r^2), d = x - y_q, r = |d|:
+ * eval_brakhage_werner_c / _l (Tests/test_helmholtzbem3d.c:68 / :134). */
+int
+orc_eval_brakhage_werner(uint32_t nv, const double *x, uint32_t nt, const uint32_t *t,
+                         const double *n, const double *g, uint32_t q, int linear, double k_re,
+                         double k_im, double eta_re, double eta_im, const double *w,
+                         uint32_t npoints, const double *pts, double *u)
+{
+  double xs[4096], ys[4096], ws[4096];
+  const cplx k = k_re + I * k_im, eta = eta_re + I * eta_im;
+  uint32_t p, i, l, qq, ns = q * q;
+  (void) nv;
+  if (single_rule(q, xs, ys, ws)) return -1;
+  for (p = 0; p < npoints; p++) {
+    const double *P = pts + 3 * (size_t) p;
+    cplx res = 0.0;
+    for (i = 0; i < nt; i++) {
+      const uint32_t *tv = t + 3 * (size_t) i;
+      const double *A = x + 3 * (size_t) tv[0], *B = x + 3 * (size_t) tv[1],
+                   *C = x + 3 * (size_t) tv[2], *N = n + 3 * (size_t) i;
+      cplx sum = 0.0;
+      for (qq = 0; qq < ns; qq++) {
+        double tx = xs[qq], sx = ys[qq], d[3], r2, r, dn;
+        cplx wy = 0.0;
+        int e;
+        for (e = 0; e < 3; e++) d[e] = P[e] - (A[e] * (1.0 - tx) + B[e] * (tx - sx) + C[e] * sx);
+        r2 = d[0] * d[0] + d[1] * d[1] + d[2] * d[2];
+        r = sqrt(r2);
+        dn = d[0] * N[0] + d[1] * N[1] + d[2] * N[2];
+        if (linear) {
+          for (l = 0; l < 3; l++)
+            wy += ws[qq] * nodal(1, l, tx, sx) * (w[2 * tv[l]] + I * w[2 * tv[l] + 1]);
+        } else {
+          wy = ws[qq] * (w[2 * i] + I * w[2 * i + 1]);
+        }
+        sum += wy * cexp(I * k * r) / (r2 * r) * ((1.0 - I * k * r) * dn - I * eta * r2);
+      }
+      res += sum * g[i];
+    }
+    res *= 0.0795774715459476679; /* 1 / (4 pi) */
+    u[2 * p] = creal(res);
+    u[2 * p + 1] = cimag(res);
+  }
+  return 0;
+}

@@ -54,6 +54,12 @@ def _load():
         d.orc_l2_error_harmonic.argtypes = [C.c_uint32, _f64p, C.c_uint32, _u32p, _f64p, _f64p,
                                             C.c_uint32, _f64p, _f64p, C.POINTER(C.c_double),
                                             C.POINTER(C.c_double)]
+        d.orc_integrate_point_source.argtypes = [C.c_uint32, _f64p, C.c_uint32, _u32p, _f64p,
+                                                 C.c_uint32, C.c_int, _f64p, C.c_double, vp]
+        d.orc_eval_brakhage_werner.argtypes = [C.c_uint32, _f64p, C.c_uint32, _u32p, _f64p,
+                                               _f64p, C.c_uint32, C.c_int, C.c_double,
+                                               C.c_double, C.c_double, C.c_double, vp,
+                                               C.c_uint32, _f64p, vp]
         _dll = d
     return _dll
 
@@ -177,3 +183,24 @@ def l2_error_harmonic(mesh, z, u, q=2):
                                          np.ascontiguousarray(u, dtype=np.float64),
                                          C.byref(e), C.byref(n)) == 0
     return e.value, n.value
+
+
+def integrate_point_source(mesh, z, k, linear, q=2):
+    """Point-source Dirichlet datum tested with the constant / linear basis (complex)."""
+    b = np.zeros(mesh.nv if linear else mesh.nt, dtype=np.complex128)
+    assert _load().orc_integrate_point_source(mesh.nv, mesh.x, mesh.nt, mesh.t, mesh.g, q,
+                                              1 if linear else 0,
+                                              np.asarray(z, dtype=np.float64), k, _p(b)) == 0
+    return b
+
+
+def eval_brakhage_werner(mesh, w, points, k, eta, linear, q=2):
+    """Brakhage-Werner potential of the density w at the points (complex)."""
+    pts = np.ascontiguousarray(points, dtype=np.float64).reshape(-1, 3)
+    w = np.ascontiguousarray(w, dtype=np.complex128)
+    u = np.zeros(len(pts), dtype=np.complex128)
+    k, eta = complex(k), complex(eta)
+    assert _load().orc_eval_brakhage_werner(mesh.nv, mesh.x, mesh.nt, mesh.t, mesh.n, mesh.g, q,
+                                            1 if linear else 0, k.real, k.imag, eta.real,
+                                            eta.imag, _p(w), len(pts), pts.ravel(), _p(u)) == 0
+    return u

@@ -8,6 +8,9 @@
  * Usage: gen_golden <outdir> <section> [...]
  * Sections (real build):    quad sphere8 sphere4 h2small config2 cube adlp
  * Sections (complex build): helm_sphere4 helm_h2small config3 config3_k8 helm_gmres helm_adlp
+ *                           helm_point
+ * The complex build also links the reference's Tests/test_helmholtzbem3d.c (its main renamed) for
+ * that test's evaluation of the exterior field.
  */
 #include <math.h>
 #include <stdio.h>
@@ -1173,6 +1176,111 @@ section_helm_gmres(void)
   del_macrosurface3d(mg);
 }
 
+/* The reference test's own evaluation of a Brakhage-Werner density at points outside the surface
+ * and its error measure, compiled from Tests/test_helmholtzbem3d.c (main renamed there). */
+field eval_brakhage_werner_c(pcbem3d bem, pcavector w, field eta, real *x);
+field eval_brakhage_werner_l(pcbem3d bem, pcavector w, field eta, real *x);
+real max_rel_outer_error(pcbem3d bem, helmholtz_data *hdata, pcavector x, boundary_func3d rhs,
+                         basisfunctionbem3d basis);
+
+/* The Brakhage-Werner operator on dense matrices */
+typedef struct {
+  pamatrix V, KM;
+  field eta;
+} bw_dense_t;
+
+static void
+addeval_bw_dense(field alpha, void *matrix, pcavector x, pavector y)
+{
+  bw_dense_t *bw = (bw_dense_t *) matrix;
+  addeval_amatrix_avector(alpha, bw->KM, x, y);
+  addeval_amatrix_avector(-I * alpha * bw->eta, bw->V, x, y);
+}
+
+/* The reference's exterior test problem (Tests/test_helmholtzbem3d.c:354-459 with main's
+ * parameters, :694): unit sphere with 512 triangles, k = 2, quadrature orders 2 / 4, a point
+ * source at (0, 0, 0.2) inside, kvec (k, 0, 0).  Per basis (constant "hpc", linear "hpl"): the
+ * tested datum b (integrate_bem3d_c/l_avector with rhs_dirichlet_point_helmholtzbem3d), the
+ * Brakhage-Werner system (K + M/2) - i k V assembled densely and solved by GMRES(50) to 1e-12,
+ * the evaluation points of max_rel_outer_error, the potential of the solution there
+ * (eval_brakhage_werner_c / _l with eta = k) and the maximal relative error against the source's
+ * field. */
+static void
+section_helm_point(void)
+{
+  pmacrosurface3d mg = new_sphere_macrosurface3d();
+  psurface3d gr = build_from_macrosurface3d_surface3d(mg, 8);
+  const field k = 2.0;
+  real kvec[3] = {2.0, 0.0, 0.0}, source[3] = {0.0, 0.0, 0.2};
+  helmholtz_data hdata;
+  int lin;
+
+  hdata.kvec = kvec;
+  hdata.source = source;
+  for (lin = 0; lin < 2; lin++) {
+    basisfunctionbem3d basis = lin ? BASIS_LINEAR_BEM3D : BASIS_CONSTANT_BEM3D;
+    const char *p = lin ? "hpl" : "hpc";
+    uint n = lin ? gr->vertices : gr->triangles;
+    pbem3d slp = new_slp_helmholtz_bem3d(k, gr, 2, 4, basis, basis);
+    pbem3d dlp = new_dlp_helmholtz_bem3d(k, gr, 2, 4, basis, basis, 0.5);
+    pamatrix V = new_amatrix(n, n), KM = new_amatrix(n, n);
+    pavector b = new_avector(n), x = new_avector(n);
+    bw_dense_t bw;
+    uint iter, i, j, np = 0;
+    real (*pts)[3] = (real (*)[3]) allocreal(3 * 400);
+    field *y;
+    char name[64];
+
+    assemble_bem3d_amatrix(slp, V);
+    assemble_bem3d_amatrix(dlp, KM);
+    if (lin)
+      integrate_bem3d_l_avector(dlp, rhs_dirichlet_point_helmholtzbem3d, b, &hdata);
+    else
+      integrate_bem3d_c_avector(dlp, rhs_dirichlet_point_helmholtzbem3d, b, &hdata);
+    bw.V = V;
+    bw.KM = KM;
+    bw.eta = k;
+    clear_avector(x);
+    iter = solve_gmres_avector(&bw, addeval_bw_dense, b, x, 1.0e-12, 1000, 50);
+    /* the points of max_rel_outer_error (Tests/test_helmholtzbem3d.c:224) */
+    for (j = 0; j < 20; j++)
+      for (i = 0; i < 20; i++) {
+        pts[np][0] = -10.0 + (20.0 / 19) * i;
+        pts[np][1] = 0.0;
+        pts[np][2] = -10.0 + (20.0 / 19) * j;
+        if (pts[np][0] * pts[np][0] + pts[np][2] * pts[np][2] > 1)
+          np++;
+      }
+    y = (field *) malloc(sizeof(field) * np);
+    for (j = 0; j < np; j++)
+      y[j] = lin ? eval_brakhage_werner_l(slp, x, k, pts[j])
+                 : eval_brakhage_werner_c(slp, x, k, pts[j]);
+    snprintf(name, sizeof(name), "%s_b", p);
+    dump_avector(name, b);
+    snprintf(name, sizeof(name), "%s_x", p);
+    dump_avector(name, x);
+    snprintf(name, sizeof(name), "%s_iter", p);
+    dump_scalar(name, (double) iter);
+    snprintf(name, sizeof(name), "%s_points", p);
+    dump_real(name, &pts[0][0], 2, np, 3);
+    snprintf(name, sizeof(name), "%s_u", p);
+    dump(name, "c16", sizeof(field), y, 1, np, 0);
+    snprintf(name, sizeof(name), "%s_maxerr", p);
+    dump_scalar(name, max_rel_outer_error(slp, &hdata, x, rhs_dirichlet_point_helmholtzbem3d,
+                                          basis));
+    free(y);
+    freemem(pts);
+    del_avector(b);
+    del_avector(x);
+    del_amatrix(V);
+    del_amatrix(KM);
+    del_helmholtz_bem3d(slp);
+    del_helmholtz_bem3d(dlp);
+  }
+  del_surface3d(gr);
+  del_macrosurface3d(mg);
+}
+
 #endif
 
 int
@@ -1220,6 +1328,8 @@ main(int argc, char **argv)
       section_config3_k8();
     else if (!strcmp(argv[i], "helm_gmres"))
       section_helm_gmres();
+    else if (!strcmp(argv[i], "helm_point"))
+      section_helm_point();
     else if (!strcmp(argv[i], "helm_adlp"))
       section_helm_adlp();
 #endif

@@ -8,7 +8,7 @@ read the committed .npz files.
     python tests/golden/make_golden.py [section ...]
 
 Sections: quad sphere8 sphere4 h2small config2 cube adlp helm_sphere4 helm_h2small config3
-config3_k8 helm_gmres helm_adlp
+config3_k8 helm_gmres helm_adlp helm_point
 """
 import os
 import subprocess
@@ -24,7 +24,7 @@ REFOUT = os.path.join(ROOT, "oracle", "_ref")
 
 REAL_SECTIONS = ["quad", "sphere8", "sphere4", "h2small", "config2", "cube", "adlp"]
 COMPLEX_SECTIONS = ["helm_sphere4", "helm_h2small", "config3", "config3_k8", "helm_gmres",
-                    "helm_adlp"]
+                    "helm_adlp", "helm_point"]
 DTYPES = {"f8": np.float64, "u4": np.uint32, "c16": np.complex128}
 # Arrays stored only in part, to keep the fixtures small: name -> number of leading columns kept
 # (matrices are written column-major, i.e. shape (cols, rows)).
@@ -41,8 +41,17 @@ def build():
     exes = {}
     for variant, flags in (("real", []), ("complex", ["-DUSE_COMPLEX"])):
         exe = os.path.join(REFOUT, f"gen_golden_{variant}")
+        # the complex build links the reference's Helmholtz test for its exterior-field
+        # evaluation (eval_brakhage_werner_c/_l, max_rel_outer_error), its main renamed
+        extra = []
+        if variant == "complex":
+            obj = os.path.join(REFOUT, "test_helmholtzbem3d.o")
+            subprocess.check_call(["gcc", "-O2", "-w", "-c", *flags, f"-I{REF}/Library",
+                                   "-Dmain=h2lib_test_helmholtzbem3d_main",
+                                   f"{REF}/Tests/test_helmholtzbem3d.c", "-o", obj])
+            extra = [obj]
         subprocess.check_call(["gcc", "-O2", "-w", *flags, f"-I{REF}/Library",
-                               os.path.join(HERE, "gen_golden.c"), "-o", exe,
+                               os.path.join(HERE, "gen_golden.c"), *extra, "-o", exe,
                                f"-L{REFOUT}", f"-lh2ref_{variant}",
                                f"-Wl,-rpath,{REFOUT}", "-lm"])
         exes[variant] = exe

@@ -260,3 +260,17 @@ def test_config2_gmres_trace_pins_the_iteration_allowance(gold):
     assert it == 161 and trace.size == it + 1
     assert trace[-1] <= thr < trace[-2] < 1.02 * thr
     assert np.all(trace[:-1] > thr)
+
+
+@pytest.mark.parametrize("p,linear", [("hpc", False), ("hpl", True)])
+def test_point_source_datum_and_exterior_field(gold, p, linear):
+    """The reference's exterior Helmholtz test problem (Tests/test_helmholtzbem3d.c:422, unit
+    sphere with 512 triangles, k = 2, source (0, 0, 0.2)): the tested datum and the potential of
+    the reference's solution at its evaluation points, as the reference computes them."""
+    g, mesh = gold("helm_point"), mesh_from(gold("sphere8"), "sphere8")
+    b = orc.integrate_point_source(mesh, (0.0, 0.0, 0.2), 2.0, linear)
+    assert np.linalg.norm(b - g[f"{p}_b"]) < 1e-12 * np.linalg.norm(g[f"{p}_b"])
+    pts = g[f"{p}_points"][:40]
+    u = orc.eval_brakhage_werner(mesh, g[f"{p}_x"], pts, 2.0, 2.0, linear)
+    ref = g[f"{p}_u"][:40]
+    assert np.linalg.norm(u - ref) < 1e-12 * np.linalg.norm(ref)
