@@ -172,10 +172,13 @@ __global__ void __launch_bounds__(TPB) vth_kernel(GmresDev g) {
   });
 }
 
-// a -= V u over rows (columns 0..k), then partial norm^2 of a[k+1..n)
+// a -= V u over rows (columns 0..k), then the partial sums of the next bookkeeping phase, in
+// slots 0..k+1 of part: [0] ||a[k+1..n)||^2, [1 + j] sum_{i > k+1} conj(V[i,j]) a[i] (j <= k).  The
+// second are the products of the previous reflectors with the next one (a below row k+1, scaled
+// by the Householder factor gamma), taken before the scaling: gamma is a common factor of them,
+// applied once the bookkeeping has computed it.
 template <bool CX>
-__global__ void __launch_bounds__(TPB) apply_v_norm_kernel(GmresDev g) {
-  __shared__ double red[TPB / 32];
+__global__ void __launch_bounds__(TPB) apply_v_dots_kernel(GmresDev g) {
   __shared__ double us[2 * GMRES_KMAX];
   Sys v;
   uint32_t i, lb;
@@ -187,54 +190,42 @@ __global__ void __launch_bounds__(TPB) apply_v_norm_kernel(GmresDev g) {
   }
   __syncthreads();
   double *a = v.qr + (size_t) (CX ? 2 : 1) * (k + 1) * v.n;
-  double nrm = 0.0;
+  cd ai = {0.0, 0.0};
   if (i < v.n) {
-    cd ai = ld<CX>(a, i);
+    ai = ld<CX>(a, i);
     const uint32_t jmax = i < k ? i : k;  // V[i, j] = 0 for j > i
     for (uint32_t j = 0; j <= jmax; j++)
       ai = csub(ai, cmul(vij<CX>(v, i, j), cd{us[2 * j], us[2 * j + 1]}));
     st<CX>(a, i, ai);
-    if (i >= k + 1) nrm = cabs2(ai);
   }
-  const double s = block_sum(nrm, red);
-  if (threadIdx.x == 0) put_part(g, v, lb, 0, s, 0.0);
-}
-
-// scale a[i > k+1] *= gamma, a[k+1] = alpha; partial z_j = sum_{i>k+1} conj(V[i,j]) a[i]
-template <bool CX>
-__global__ void __launch_bounds__(TPB) scale_vth_kernel(GmresDev g) {
-  Sys v;
-  uint32_t i, lb;
-  if (!vec_view<CX>(g, GMRES_SEL_ACTIVE, v, i, lb)) return;
-  const uint32_t k = v.state->k;
-  const cd gamma = {v.state->gamma_re, v.state->gamma_im};
-  double *a = v.qr + (size_t) (CX ? 2 : 1) * (k + 1) * v.n;
-  cd x = {0.0, 0.0};
   const bool below = i < v.n && i > k + 1;
-  if (below) {
-    x = cmul(ld<CX>(a, i), gamma);
-    st<CX>(a, i, x);
-  }
-  if (i == k + 1 && i < v.n) st<CX>(a, i, cd{v.state->alpha_re, v.state->alpha_im});
-  block_dots<CX>(g, v, lb, k, [&](uint32_t j) {
-    return below ? cmul(cconj(vij<CX>(v, i, j)), x) : cd{0.0, 0.0};
+  block_dots<CX>(g, v, lb, k + 1, [&](uint32_t j) {
+    if (j == 0) return cd{(i < v.n && i >= k + 1) ? cabs2(ai) : 0.0, 0.0};
+    return below ? cmul(cconj(vij<CX>(v, i, j - 1)), ai) : cd{0.0, 0.0};
   });
 }
 
-// q = e_{k} - V_{0..k} u  (k = current dimension after the step)
+// After the bookkeeping of a step (k is the new dimension): the new reflector's rows below k are
+// scaled by gamma (column k of qr; its row k holds the stored rotation), then q = e_k - V_{0..k} u.
+// Each thread scales its own row before it reads it.
 template <bool CX>
-__global__ void __launch_bounds__(TPB) make_q_kernel(GmresDev g) {
+__global__ void __launch_bounds__(TPB) scale_make_q_kernel(GmresDev g) {
   __shared__ double us[2 * GMRES_KMAX];
   Sys v;
   uint32_t i, lb;
   if (!vec_view<CX>(g, GMRES_SEL_ACTIVE, v, i, lb)) return;
   const uint32_t k = v.state->k;
+  const cd gamma = {v.state->gamma_re, v.state->gamma_im};
   for (uint32_t j = threadIdx.x; j <= k; j += TPB) {
     us[2 * j] = v.u[2 * j];
     us[2 * j + 1] = v.u[2 * j + 1];
   }
   __syncthreads();
   if (i >= v.n) return;
+  if (i > k) {
+    double *col = v.qr + (size_t) (CX ? 2 : 1) * k * v.n;
+    st<CX>(col, i, cmul(ld<CX>(col, i), gamma));
+  }
   cd q = {i == k ? 1.0 : 0.0, 0.0};
   const uint32_t jmax = i < k ? i : k;
   for (uint32_t j = 0; j <= jmax; j++) q = csub(q, cmul(vij<CX>(v, i, j), cd{us[2 * j], us[2 * j + 1]}));
@@ -246,7 +237,7 @@ __global__ void __launch_bounds__(TPB) make_q_kernel(GmresDev g) {
 // all its loads in flight at once; the warps' sums are combined in shared memory.  The caller
 // synchronises before reading z.
 __device__ void sum_parts_all(const GmresDev &g, const Sys &v, uint32_t k, double *zr,
-                              double *zi) {
+                              double *zi, uint32_t j0 = 0) {
   constexpr int NW = GMRES_KMAX / 32;  // warps of the bookkeeping CTA (GMRES_KMAX threads)
   __shared__ double wsr[NW][GMRES_KMAX], wsi[NW][GMRES_KMAX];
   const uint32_t lane = threadIdx.x & 31, w = threadIdx.x >> 5;
@@ -254,8 +245,8 @@ __device__ void sum_parts_all(const GmresDev &g, const Sys &v, uint32_t k, doubl
     double sr = 0.0, si = 0.0;
 #pragma unroll 8
     for (uint32_t b = w; b < v.nblk; b += NW) {
-      sr += v.part[(size_t) b * g.ldpart * 2 + 2 * j];
-      si += v.part[(size_t) b * g.ldpart * 2 + 2 * j + 1];
+      sr += v.part[(size_t) b * g.ldpart * 2 + 2 * (j0 + j)];
+      si += v.part[(size_t) b * g.ldpart * 2 + 2 * (j0 + j) + 1];
     }
     wsr[w][j] = sr;
     wsi[w][j] = si;
@@ -375,6 +366,7 @@ template <bool CX>
 __global__ void __launch_bounds__(SMALL_THREADS) small_kernel(GmresDev g, int phase, int sel) {
   __shared__ double zr[GMRES_KMAX], zi[GMRES_KMAX], red[SMALL_THREADS / 32];
   __shared__ double wr[GMRES_KMAX], wi[GMRES_KMAX];
+  __shared__ double hs[4];  // phase 1: gamma, alpha
   const Sys v = sys_view<CX>(g, blockIdx.x);
   GmresState *s = v.state;
   if (!selected(s, sel)) return;
@@ -396,21 +388,30 @@ __global__ void __launch_bounds__(SMALL_THREADS) small_kernel(GmresDev g, int ph
       v.u[2 * t + 1] = u.im;
     }
   } else if (phase == 1) {
-    // after apply_v_norm: Householder scalars of column k+1, rows >= k+1
-    double part = 0.0;
-    for (uint32_t b = t; b < v.nblk; b += SMALL_THREADS) part += v.part[(size_t) b * g.ldpart * 2];
-    const double norm2 = block_sum_small(part, red);
-    if (t == 0) {
-      const double *a = v.qr + (size_t) (CX ? 2 : 1) * (k + 1) * v.n;
-      householder(k + 1 < v.n ? ld<CX>(a, k + 1) : cd{0.0, 0.0}, norm2, s, k + 1, v);
+    // after apply_v_dots: the Householder scalars of column k+1 from ||a[k+1..n)||^2 (part slot
+    // 0); the T column k+1 from the reflector products (part slots 1..k+1, times gamma); u for q;
+    // the Givens rotations of the new Hessenberg column (entry k+1 = alpha); k += 1.
+    {
+      double part = 0.0;
+      for (uint32_t b = t; b < v.nblk; b += SMALL_THREADS)
+        part += v.part[(size_t) b * g.ldpart * 2];
+      const double norm2 = block_sum_small(part, red);
+      if (t == 0) {
+        const double *a = v.qr + (size_t) (CX ? 2 : 1) * (k + 1) * v.n;
+        householder(k + 1 < v.n ? ld<CX>(a, k + 1) : cd{0.0, 0.0}, norm2, s, k + 1, v);
+        hs[0] = s->gamma_re;
+        hs[1] = s->gamma_im;
+        hs[2] = s->alpha_re;
+        hs[3] = s->alpha_im;
+      }
+      __syncthreads();
     }
-  } else if (phase == 2) {
-    // after scale_vth: T column k+1; u for q; Givens; k += 1
     const cd tau = {v.tau[2 * (k + 1)], v.tau[2 * (k + 1) + 1]};
-    sum_parts_all(g, v, k, zr, zi);
+    sum_parts_all(g, v, k, zr, zi, 1u);
     __syncthreads();
-    if (t <= k) {  // + conj(v_t[k+1])
-      const cd z = cadd(cd{zr[t], zi[t]}, cconj(vij<CX>(v, k + 1, t)));
+    if (t <= k) {  // gamma z + conj(v_t[k+1])
+      cd z = cmul(cd{zr[t], zi[t]}, cd{hs[0], hs[1]});
+      z = cadd(z, cconj(vij<CX>(v, k + 1, t)));
       zr[t] = z.re;
       zi[t] = z.im;
     }
@@ -437,7 +438,7 @@ __global__ void __launch_bounds__(SMALL_THREADS) small_kernel(GmresDev g, int ph
     // sequential sweep by one thread never waits on global memory.
     double *col = v.qr + (size_t) (CX ? 2 : 1) * (k + 1) * v.n;
     if (t <= k + 1) {
-      const cd c = ld<CX>(col, t);
+      const cd c = t == k + 1 ? cd{hs[2], hs[3]} : ld<CX>(col, t);
       wr[t] = c.re;
       wi[t] = c.im;
     }
@@ -631,13 +632,13 @@ int step_impl(const GmresDev &g, const GmresOp &op, cudaStream_t st) {
   zero_abuf_kernel<CX><<<nb, TPB, 0, st>>>(g);
   int rc = (op.apply_lo ? op.apply_lo : op.apply)(op.ctx, g.q, g.abuf, 1.0, 0.0, st);
   if (rc != H2B_OK) return rc;
+  // w = V^H a; u = T^H w; a -= V u with the next column's norm and dot products; Householder
+  // scalars, T column, Givens (k += 1); scaled reflector and q
   vth_kernel<CX><<<nb, TPB, 0, st>>>(g);
   small_kernel<CX><<<g.nsys, SMALL_THREADS, 0, st>>>(g, 0, GMRES_SEL_ACTIVE);
-  apply_v_norm_kernel<CX><<<nb, TPB, 0, st>>>(g);
+  apply_v_dots_kernel<CX><<<nb, TPB, 0, st>>>(g);
   small_kernel<CX><<<g.nsys, SMALL_THREADS, 0, st>>>(g, 1, GMRES_SEL_ACTIVE);
-  scale_vth_kernel<CX><<<nb, TPB, 0, st>>>(g);
-  small_kernel<CX><<<g.nsys, SMALL_THREADS, 0, st>>>(g, 2, GMRES_SEL_ACTIVE);
-  make_q_kernel<CX><<<nb, TPB, 0, st>>>(g);
+  scale_make_q_kernel<CX><<<nb, TPB, 0, st>>>(g);
   H2B_CUDA_TRY(cudaGetLastError());
   return H2B_OK;
 }
