@@ -367,6 +367,7 @@ __global__ void __launch_bounds__(SMALL_THREADS) small_kernel(GmresDev g, int ph
   __shared__ double zr[GMRES_KMAX], zi[GMRES_KMAX], red[SMALL_THREADS / 32];
   __shared__ double wr[GMRES_KMAX], wi[GMRES_KMAX];
   __shared__ double hs[4];  // phase 1: gamma, alpha
+  __shared__ double yr[GMRES_KMAX], yi[GMRES_KMAX];  // phase 1: conj(V[k+1, j])
   const Sys v = sys_view<CX>(g, blockIdx.x);
   GmresState *s = v.state;
   if (!selected(s, sel)) return;
@@ -392,6 +393,12 @@ __global__ void __launch_bounds__(SMALL_THREADS) small_kernel(GmresDev g, int ph
     // 0); the T column k+1 from the reflector products (part slots 1..k+1, times gamma); u for q;
     // the Givens rotations of the new Hessenberg column (entry k+1 = alpha); k += 1.
     {
+      // y_j = conj(V[k+1, j]) (j <= k), read before anything waits on the Householder scalars
+      if (t <= k) {
+        const cd y = cconj(vij<CX>(v, k + 1, t));
+        yr[t] = y.re;
+        yi[t] = y.im;
+      }
       double part = 0.0;
       for (uint32_t b = t; b < v.nblk; b += SMALL_THREADS)
         part += v.part[(size_t) b * g.ldpart * 2];
@@ -411,32 +418,36 @@ __global__ void __launch_bounds__(SMALL_THREADS) small_kernel(GmresDev g, int ph
     __syncthreads();
     if (t <= k) {  // gamma z + conj(v_t[k+1])
       cd z = cmul(cd{zr[t], zi[t]}, cd{hs[0], hs[1]});
-      z = cadd(z, cconj(vij<CX>(v, k + 1, t)));
+      z = cadd(z, cd{yr[t], yi[t]});
       zr[t] = z.re;
       zi[t] = z.im;
     }
     __syncthreads();
+    // T column k+1: T[t, k+1] = -tau sum_{j=t..k} T[t, j] z_j, T[k+1, k+1] = tau; and
+    // u = T y with y_{k+1} = 1: both sums run over row t of T in one pass
     if (t <= k) {
-      cd acc = {0.0, 0.0};
-      for (uint32_t j = t; j <= k; j++) acc = cadd(acc, cmul(Tij(g, v, t, j), cd{zr[j], zi[j]}));
-      setT(g, v, t, k + 1, cmul(cd{-tau.re, -tau.im}, acc));
-    }
-    if (t == 0) setT(g, v, k + 1, k + 1, tau);
-    __syncthreads();
-    // u = T y, y_j = conj(V[k+1, j]) (j <= k), y_{k+1} = 1
-    if (t <= k + 1) {
-      cd acc = {0.0, 0.0};
-      for (uint32_t j = t; j <= k + 1; j++) {
-        const cd y = j == k + 1 ? cd{1.0, 0.0} : cconj(vij<CX>(v, k + 1, j));
-        acc = cadd(acc, cmul(Tij(g, v, t, j), y));
+      cd acc = {0.0, 0.0}, uy = {0.0, 0.0};
+#pragma unroll 4
+      for (uint32_t j = t; j <= k; j++) {
+        const cd tv = Tij(g, v, t, j);
+        acc = cadd(acc, cmul(tv, cd{zr[j], zi[j]}));
+        uy = cadd(uy, cmul(tv, cd{yr[j], yi[j]}));
       }
-      v.u[2 * t] = acc.re;
-      v.u[2 * t + 1] = acc.im;
+      const cd tn = cmul(cd{-tau.re, -tau.im}, acc);
+      setT(g, v, t, k + 1, tn);
+      uy = cadd(uy, tn);
+      v.u[2 * t] = uy.re;
+      v.u[2 * t + 1] = uy.im;
+    } else if (t == k + 1) {
+      setT(g, v, k + 1, k + 1, tau);
+      v.u[2 * t] = tau.re;
+      v.u[2 * t + 1] = tau.im;
     }
     // Givens rotations on the new Hessenberg column (rows 0..k+1 of column k+1): the column and
     // the stored rotations (diagonal of the previous columns) are staged in shared memory, so the
     // sequential sweep by one thread never waits on global memory.
     double *col = v.qr + (size_t) (CX ? 2 : 1) * (k + 1) * v.n;
+    __syncthreads();  // zr / zi (read by the T loop above) are reused below
     if (t <= k + 1) {
       const cd c = t == k + 1 ? cd{hs[2], hs[3]} : ld<CX>(col, t);
       wr[t] = c.re;
