@@ -43,6 +43,10 @@ EXECUTED_FLOPS_PER_PAIR = 16 * 37 + 4 * 53 + 4 * 17 + 20
 # workload (sphere split 64), from an ncu capture of the full-size run (single-pass metrics
 # dram__bytes_read.sum + dram__bytes_write.sum)
 NEAR_DIST_TRAFFIC = 5998336 + 214822656
+# DRAM bytes (read + write) of one FP64 matvec product per algorithmic byte: 301.7 MB for
+# 284.3 MB on the sphere split 48 (ncu, dram__bytes_read.sum + dram__bytes_write.sum of the three
+# item-kernel launches of a product), applied to the bench's workload by its stored entries
+MATVEC_TRAFFIC_RATIO = 301.7 / 284.3
 
 
 def parse():
@@ -64,6 +68,8 @@ def parse():
     p.add_argument("--no-serving", action="store_true")
     p.add_argument("--no-helmholtz", action="store_true")
     p.add_argument("--no-mixed", action="store_true")
+    p.add_argument("--no-autotune", action="store_true",
+                   help="keep the default launch shapes (profiling runs: no tuning launches)")
     p.add_argument("--serve-requests", type=int, default=48)
     p.add_argument("--cpu-batch-sample", type=int, default=8)
     p.add_argument("--cpu-serve-budget", type=float, default=60.0)
@@ -316,7 +322,7 @@ def run_ours(a, rank, world, local):
     # ---- autotuner (untimed): matvec launch shape and leaf-basis split, timed on V itself; K,
     # made like V afterwards, starts from the same shape
     V.assemble()
-    tune = V.autotune(matvec=True, leaf=True)
+    tune = None if a.no_autotune else V.autotune(matvec=True, leaf=True)
     K = hb.H2Matrix(dlp, tree, a.m, like=V)  # shares V's device structure
     entries = V.info()["near_entries"] + K.info()["near_entries"]
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
@@ -414,10 +420,12 @@ def run_ours(a, rank, world, local):
     hbm = peaks.get("hbm_gbs", 6650.0)
     roof_mv = {"bound": "hbm", "kernel": "H2 matvec (all kernels of one product)",
                "achieved": mv_bytes / (mv_ms * 1e-3) / 1e9, "peak": hbm, "unit": "GB/s",
-               "frac": mv_bytes / (mv_ms * 1e-3) / 1e9 / hbm, "traffic": None,
+               "frac": mv_bytes / (mv_ms * 1e-3) / 1e9 / hbm,
+               "traffic": int(MATVEC_TRAFFIC_RATIO * mv_bytes),
+               "traffic_source": "ncu on the sphere split 48, scaled by the stored entries",
                "peak_source": "MEASURED_PEAKS.json hbm_gbs" if peaks else "fallback 6650 GB/s",
                "bytes_per_launch": mv_bytes, "launch_ms": mv_ms,
-               "l2": "no flush between products (operator 5x larger than L2)",
+               "l2": "no flush between products (operator 4x larger than L2)",
                "launches_per_product": 5}
     roof_mv32 = {"bound": "hbm", "kernel": "H2 matvec from the FP32 copies (FP64 vectors/sums)",
                  "achieved": mv_bytes / 2 / (mv32_ms * 1e-3) / 1e9, "peak": hbm, "unit": "GB/s",
@@ -552,12 +560,12 @@ def run_ours(a, rank, world, local):
         "pairs_per_operator": pc, "singular_points": sing_points,
         "singular_kernel_evaluations": sing_evals,
         "roofline": roofline, "roofline_matvec": roof_mv, "roofline_matvec_fp32": roof_mv32,
-        "autotune": {"shape": tune["shape"], "matvec_ms_start": tune["matvec_ms"][0],
-                     "matvec_ms_tuned": tune["matvec_ms"][1],
-                     "bases_ms_start": tune["bases_ms"][0],
-                     "bases_ms_tuned": tune["bases_ms"][1],
-                     "what": "h2b_h2matrix_autotune on V before the warm-up (matvec launch shape "
-                             "and leaf-basis CTAs per leaf); K is made like V afterwards"},
+        "autotune": None if tune is None else {
+            "shape": tune["shape"], "matvec_ms_start": tune["matvec_ms"][0],
+            "matvec_ms_tuned": tune["matvec_ms"][1], "bases_ms_start": tune["bases_ms"][0],
+            "bases_ms_tuned": tune["bases_ms"][1],
+            "what": "h2b_h2matrix_autotune on V before the warm-up (matvec launch shape and "
+                    "leaf-basis CTAs per leaf); K is made like V afterwards"},
         "solve": solve, "mixed": mixed,
         "e2e": e2e,
         "clocks": clocks.summary(),
