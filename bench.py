@@ -70,7 +70,7 @@ def parse():
     p.add_argument("--no-mixed", action="store_true")
     p.add_argument("--no-autotune", action="store_true",
                    help="keep the default launch shapes (profiling runs: no tuning launches)")
-    p.add_argument("--serve-requests", type=int, default=48)
+    p.add_argument("--serve-requests", type=int, default=500)
     p.add_argument("--cpu-batch-sample", type=int, default=8)
     p.add_argument("--cpu-serve-budget", type=float, default=60.0)
     p.add_argument("--serve-rates", default="50,200,1000,2000")

@@ -42,6 +42,8 @@ _SIGS = {
                                   C.POINTER(C.c_uint32), vp, vp, vp, vp, vp]),
     "h2b_tree_new": (vp, [C.c_uint32, _f64p, C.c_uint32, _u32p, C.c_int, C.c_int, C.c_uint32,
                           C.c_double]),
+    "h2b_tree_new_device": (vp, [C.c_uint32, _f64p, C.c_uint32, _u32p, C.c_int, C.c_int,
+                                 C.c_uint32, C.c_double]),
     "h2b_tree_new_flat": (vp, [C.c_uint32, _u32p, _u32p, _u32p, _f64p, C.c_uint32, _u32p,
                                C.c_uint32, _u32p, _u32p, _u32p, _f64p, C.c_uint32, _u32p,
                                C.c_uint32, _u32p, _u32p, _u8p]),

@@ -233,9 +233,12 @@ class Tree:
             self.handle = None
 
 
-def build_tree(gr, row_basis, col_basis, clf, eta):
-    return Tree(checkp(lib.h2b_tree_new(gr.vertices, gr.x, gr.triangles, gr.t, row_basis,
-                                        col_basis, clf, eta), "h2b_tree_new"))
+def build_tree(gr, row_basis, col_basis, clf, eta, device=False):
+    """Cluster and block trees, built on the host (h2b_tree_new) or on the device
+    (h2b_tree_new_device); both give the same trees."""
+    fn = lib.h2b_tree_new_device if device else lib.h2b_tree_new
+    return Tree(checkp(fn(gr.vertices, gr.x, gr.triangles, gr.t, row_basis, col_basis, clf, eta),
+                       "h2b_tree_new_device" if device else "h2b_tree_new"))
 
 
 def build_forest(gr, vertex_off, triangle_off, row_basis, col_basis, clf, eta):

@@ -44,9 +44,7 @@ struct FarCouplingArgs {
 };
 
 // Flattened bases (flatbasis.cu): items of at most H2B_FLAT_ROWS rows of one son.
-#ifndef H2B_FLAT_ROWS
 #define H2B_FLAT_ROWS 32
-#endif
 struct FlatArgs {
   const uint32_t *items;     // 4 per item: father, son, first row in the son, rows
   const uint32_t *off, *size;

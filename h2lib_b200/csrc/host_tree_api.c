@@ -8,6 +8,9 @@ int h2b_ctree_build(uint32_t vertices, const double *x, uint32_t triangles, cons
                     int basis, uint32_t clf, h2b_ctree *out);
 int h2b_blist_build(const h2b_ctree *rt, const h2b_ctree *ct, double eta, h2b_blist *out);
 
+/* Block counts of a complete tree (also used by the device builder, devtree.cu). */
+int h2b_tree_finish(h2b_tree *tr);
+
 static int
 finish_tree(h2b_tree *tr)
 {
@@ -25,6 +28,20 @@ finish_tree(h2b_tree *tr)
 }
 
 static int ctree_append(h2b_ctree *dst, const h2b_ctree *src, uint32_t ioff);
+
+int
+h2b_tree_finish(h2b_tree *tr)
+{
+  return finish_tree(tr);
+}
+
+/* dst (empty) = a copy of src (also used by the device builder for equal bases). */
+int h2b_ctree_copy(h2b_ctree *dst, const h2b_ctree *src);
+int
+h2b_ctree_copy(h2b_ctree *dst, const h2b_ctree *src)
+{
+  return ctree_append(dst, src, 0);
+}
 
 h2b_tree *
 h2b_tree_new(uint32_t vertices, const double *x, uint32_t triangles, const uint32_t *t,

@@ -60,16 +60,6 @@ __constant__ double c_dist[5][DIST_TOTAL];
 // factors as w = w_x w_y.  Per order q and point p < q^2: rows t, s, w, w (1-t), w (t-s), w s
 // (the raw weight and the three linear nodal functions times the weight).
 constexpr int SIDE_MAXP = 25;
-// 1: distant pairs of the specialised orders use the factored sum (dist_pair_tensor); 0: the
-// point-by-point sum over the q^4 table.
-#ifndef H2B_DIST_TENSOR
-#define H2B_DIST_TENSOR 1
-#endif
-// 1: the lanes of a warp visit row triangles spread over the tile's list (stage position e holds
-// list entry e * 17 mod n), so that fewer lanes add to the same tile entry at once; 0: list order
-#ifndef H2B_DIST_PERMUTE
-#define H2B_DIST_PERMUTE 0
-#endif
 __constant__ double c_side[5][6][SIDE_MAXP];
 
 // Kernel values from r^2 = |x - y|^2 and dot = <x - y, n> with n the unit normal of the column
@@ -135,18 +125,6 @@ __device__ __forceinline__ void pair_geo(const TriRec &T, const TriRec &S, const
     g.p2[d] = tc - tb;
     g.q1[d] = sb - sa;
     g.q2[d] = sc - sb;
-  }
-}
-
-[[maybe_unused]] __device__ __forceinline__ void pair_geo_id(const TriRec &T, const TriRec &S,
-                                                             PairGeo &g) {
-#pragma unroll
-  for (int d = 0; d < 3; d++) {
-    g.d0[d] = T.a[d] - S.a[d];
-    g.p1[d] = T.b[d] - T.a[d];
-    g.p2[d] = T.c[d] - T.b[d];
-    g.q1[d] = S.b[d] - S.a[d];
-    g.q2[d] = S.c[d] - S.b[d];
   }
 }
 
@@ -498,19 +476,15 @@ struct DistArgs {
 };
 
 // Shared-memory accumulator tile: [NOUT*(CPLX?2:1)][64*64] doubles.
-#ifndef H2B_DIST_MINBLOCKS
-#define H2B_DIST_MINBLOCKS 2
-#endif
-// 1: the tile's row and column triangles are staged in shared memory, structure of arrays, in
+// Resident CTAs per SM of the distant-pair kernel (register budget of 128 per thread).
+constexpr int DIST_MINBLOCKS = 2;
+// The tile's row and column triangles are staged in shared memory, structure of arrays, in
 // chunks of DIST_CHUNK triangles per side (the pair loop then reads consecutive words per warp
-// instead of one 128-byte record per lane from L1); 0: records read per pair from global memory.
-#ifndef H2B_DIST_STAGE
-#define H2B_DIST_STAGE 1
-#endif
+// instead of one 128-byte record per lane from L1).
 constexpr int DIST_CHUNK = 128;
 
 // Staged triangles of one chunk pair.  Edge vectors are formed once per triangle here (the same
-// subtractions pair_geo_id makes per pair, so the pair geometry is bitwise the same).
+// subtractions pair_geo makes with the identity permutation).
 struct DistStage {
   double r[13][DIST_CHUNK];  // row triangles: A (3), B - A (3), C - B (3), Gram determinant, n
   double c[13][DIST_CHUNK];  // column triangles: A, B - A, C - B, Gram determinant * kconst, n
@@ -518,7 +492,7 @@ struct DistStage {
   int32_t rl[3][DIST_CHUNK], cl[3][DIST_CHUNK];   // local output row / column per vertex
 };
 template <int Q, int KK, bool RL, bool CL, bool F32 = false>
-__global__ void __launch_bounds__(256, H2B_DIST_MINBLOCKS) near_dist_kernel(DistArgs a) {
+__global__ void __launch_bounds__(256, DIST_MINBLOCKS) near_dist_kernel(DistArgs a) {
   constexpr int NCH = KT<KK>::NCH;
   constexpr int NR = RL ? 3 : 1, NC = CL ? 3 : 1;
   constexpr int PLANES = KT<KK>::CPLX ? 2 : KT<KK>::NOUT;
@@ -546,7 +520,6 @@ __global__ void __launch_bounds__(256, H2B_DIST_MINBLOCKS) near_dist_kernel(Dist
     cw = &c_dist[4][dist_off(q)];
   }
 
-#if H2B_DIST_STAGE
   // Chunk pairs (column chunk outer): rows are restaged per chunk pair only when the tile has
   // more than one row chunk.  Lanes of a warp take consecutive row triangles of one column
   // triangle: the row arrays are read as consecutive words, the column arrays as a broadcast.
@@ -574,16 +547,8 @@ __global__ void __launch_bounds__(256, H2B_DIST_MINBLOCKS) near_dist_kernel(Dist
           }
         }
         if (c0 == 0 || ntr > (uint32_t) DIST_CHUNK) {
-#if H2B_DIST_PERMUTE
-          const uint32_t rmul = (nr % 17u) ? 17u : 19u;  // prime, coprime to nr <= 128
-#endif
           for (uint32_t e = threadIdx.x; e < nr; e += blockDim.x) {
-#if H2B_DIST_PERMUTE
-            const uint32_t src = (e * rmul) % nr;
-#else
-            const uint32_t src = e;
-#endif
-            const TriRef rt = a.refs[tl.tr_off + r0 + src];
+            const TriRef rt = a.refs[tl.tr_off + r0 + e];
             const TriRec &T = a.tri[rt.t];
 #pragma unroll
             for (int d = 0; d < 3; d++) {
@@ -636,17 +601,10 @@ __global__ void __launch_bounds__(256, H2B_DIST_MINBLOCKS) near_dist_kernel(Dist
             for (int j = 0; j < NC; j++) acc[c][i][j] = 0.0;
 
         if constexpr (Q > 0) {
-#if H2B_DIST_TENSOR
           if constexpr (F32)
             dist_pair_tensor_f32<Q, KK, RL, CL>(g, n0, n1, n2, a.k_re, a.k_imn, acc);
           else
             dist_pair_tensor<Q, KK, RL, CL>(g, n0, n1, n2, a.k_re, a.k_imn, acc);
-#else
-#pragma unroll
-          for (int k = 0; k < Q * Q * Q * Q; k++)
-            quad_point<KK, RL, CL>(g, cx0[k], cx1[k], cy0[k], cy1[k], cw[k], n0, n1, n2, a.k_re,
-                                   a.k_imn, acc);
-#endif
         } else {
           for (int k = 0; k < nq; k++)
             quad_point<KK, RL, CL>(g, cx0[k], cx1[k], cy0[k], cy1[k], cw[k], n0, n1, n2, a.k_re,
@@ -675,81 +633,6 @@ __global__ void __launch_bounds__(256, H2B_DIST_MINBLOCKS) near_dist_kernel(Dist
       }
     }
   }
-#else
-  // Lanes of a warp take consecutive row positions q of one column triangle.  The row triangles
-  // are visited as it = q * mult mod ntr (a bijection, mult prime and not dividing ntr): the
-  // triangle lists follow the vertex order, so neighbours share vertices, and spreading a warp
-  // over the list keeps its lanes' shared-memory atomics off common entries.
-#if H2B_DIST_PERMUTE
-  const uint32_t mult = (ntr % 17u) ? 17u : 19u;
-#else
-  const uint32_t mult = 1u;
-#endif
-  const uint32_t npairs = ntr * nsc;
-  for (uint32_t p = threadIdx.x; p < npairs; p += blockDim.x) {
-    const uint32_t is = p / ntr, q = p - is * ntr;
-    const uint32_t it = (uint32_t) (((uint64_t) q * mult) % ntr);
-    const TriRef rt = a.refs[tl.tr_off + it];
-    const TriRef st = a.refs[tl.sc_off + is];
-    const TriRec &T = a.tri[rt.t];
-    const TriRec &S = a.tri[st.t];
-    const uint32_t tv0 = T.v[0], tv1 = T.v[1], tv2 = T.v[2];
-    const uint32_t sv0 = S.v[0], sv1 = S.v[1], sv2 = S.v[2];
-    const bool singular = tv0 == sv0 || tv0 == sv1 || tv0 == sv2 || tv1 == sv0 || tv1 == sv1 ||
-                          tv1 == sv2 || tv2 == sv0 || tv2 == sv1 || tv2 == sv2;
-    if (singular) continue;
-
-    PairGeo g;
-    pair_geo_id(T, S, g);
-    const TriRec &NT = row_normal<KK>() ? T : S;  // triangle whose normal the kernel uses
-    const double n0 = NT.n[0], n1 = NT.n[1], n2 = NT.n[2];
-    double acc[NCH][NR][NC];
-#pragma unroll
-    for (int c = 0; c < NCH; c++)
-#pragma unroll
-      for (int i = 0; i < NR; i++)
-#pragma unroll
-        for (int j = 0; j < NC; j++) acc[c][i][j] = 0.0;
-
-    if constexpr (Q > 0) {
-#if H2B_DIST_TENSOR
-      if constexpr (F32)
-        dist_pair_tensor_f32<Q, KK, RL, CL>(g, n0, n1, n2, a.k_re, a.k_imn, acc);
-      else
-        dist_pair_tensor<Q, KK, RL, CL>(g, n0, n1, n2, a.k_re, a.k_imn, acc);
-#else
-#pragma unroll
-      for (int k = 0; k < Q * Q * Q * Q; k++)
-        quad_point<KK, RL, CL>(g, cx0[k], cx1[k], cy0[k], cy1[k], cw[k], n0, n1, n2, a.k_re,
-                               a.k_imn, acc);
-#endif
-    } else {
-      for (int k = 0; k < nq; k++)
-        quad_point<KK, RL, CL>(g, cx0[k], cx1[k], cy0[k], cy1[k], cw[k], n0, n1, n2, a.k_re,
-                               a.k_imn, acc);
-    }
-
-    const double f2 = (S.g * a.kconst) * T.g;
-#pragma unroll
-    for (int i = 0; i < NR; i++) {
-      const int lr = rt.l[i];
-#pragma unroll
-      for (int j = 0; j < NC; j++) {
-        const int lc = st.l[j];
-        if (lr < 0 || lc < 0) continue;
-        const int e = lr + H2B_TILE_MAX * lc;
-#pragma unroll
-        for (int c = 0; c < NCH; c++) {
-          const double v = acc[c][i][j] * f2;
-          if constexpr (RL || CL)
-            atomicAdd(&sacc[c * TS + e], v);
-          else
-            sacc[c * TS + e] = v;
-        }
-      }
-    }
-  }
-#endif
   __syncthreads();
 
   const bool ntrans = tl.flags & 1u;
@@ -988,7 +871,7 @@ template <int Q, int KK, bool RL, bool CL, bool F32 = false>
 int launch_dist(const h2b_near_launch *L, cudaStream_t st) {
   constexpr int PLANES = KT<KK>::CPLX ? 2 : KT<KK>::NOUT;
   const size_t smem = sizeof(double) * PLANES * H2B_TILE_MAX * H2B_TILE_MAX +
-                      (H2B_DIST_STAGE ? sizeof(DistStage) : 0);
+                      sizeof(DistStage);
   H2B_CUDA_TRY((h2b_allow_smem<near_dist_kernel<Q, KK, RL, CL, F32>>()));
   DistArgs a;
   a.tri = (const TriRec *) L->tri;

@@ -116,7 +116,7 @@ int h2b_quad_export(uint32_t q, uint32_t q2, int row_basis, int col_basis, int w
                     uint32_t *n, double *x0, double *x1, double *y0, double *y1, double *w10);
 
 /* ------------------------------------------------------------------------------------------
- * Cluster tree and block tree (host)
+ * Cluster tree and block tree
  * ------------------------------------------------------------------------------------------ */
 
 /* Build the row and column cluster trees (build_bem3d_cluster, Library/bem3d.c:932 ->
@@ -126,6 +126,16 @@ int h2b_quad_export(uint32_t q, uint32_t q2, int row_basis, int col_basis, int w
 h2b_tree *h2b_tree_new(uint32_t vertices, const double *x, uint32_t triangles,
                        const uint32_t *t, int row_basis, int col_basis, uint32_t clf,
                        double eta);
+
+/* The same trees as h2b_tree_new (index for index), built on the device: characteristic points
+ * and support boxes, the cluster bisection level by level (one CTA per cluster: bounding box,
+ * longest side, and the reference's in-place partition replayed exactly) and the block
+ * admissibility level by level; the host lays out the levels and numbers the result.  Replaces
+ * build_adaptive_cluster (Library/cluster.c:80) and build_strict_block (Library/block.c:258) as
+ * h2b_tree_new does.  The mesh arrays are host arrays. */
+h2b_tree *h2b_tree_new_device(uint32_t vertices, const double *x, uint32_t triangles,
+                              const uint32_t *t, int row_basis, int col_basis, uint32_t clf,
+                              double eta);
 
 /* Build from explicit flattened trees (what an H2Lib integration passes after walking its own
  * pcluster / pblock): per cluster in pre-order off, size, sons (0 or 2) and the bounding box
