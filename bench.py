@@ -508,7 +508,7 @@ def run_ours(a, rank, world, local):
             s2 = hb.new_slp_laplace_bem3d(g2, 2, 4, L, L)
             d2 = hb.new_dlp_laplace_bem3d(g2, 2, 4, L, L, 0.5)
             t1 = time.perf_counter()
-            tr2 = hb.build_tree(g2, L, L, a.clf, a.eta)
+            tr2 = hb.build_tree(g2, L, L, a.clf, a.eta, device=True)
             t2 = time.perf_counter()
             V2 = hb.H2Matrix(s2, tr2, a.m)
             K2 = hb.H2Matrix(d2, tr2, a.m, like=V2)
@@ -541,7 +541,8 @@ def run_ours(a, rank, world, local):
         e2e_s = dist_max(min(e2e_times), world)
         e2e = {"value": world * entries / e2e_s, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
                "d2h_bytes_per_step": int(d2h),
-               "includes": "mesh upload, operators, cluster/block trees (host C), H2 structure "
+               "includes": "mesh upload, operators, cluster/block trees (h2b_tree_new_device), "
+                           "H2 structure "
                            "upload, assembly of V and K, copy of all nearfield and coupling "
                            "blocks to pinned host memory (coupling copies overlap the nearfield "
                            "assembly; 'assembly' then includes that overlap)",

@@ -87,6 +87,8 @@ uint64_t estimate_bytes(const h2b_request &r) {
   return per_tri * r.triangles + (32ull << 20);
 }
 
+constexpr uint32_t kDeviceTreeTriangles = 8192;
+
 // Run one request to the end on the calling (worker) thread.
 int run_request(Req *q) {
   auto tick = [] { return Clock::now(); };
@@ -108,8 +110,10 @@ int run_request(Req *q) {
                              0.0);
   h2b_bem *dlp = h2b_bem_new(s, d.pde, H2B_DLP, basis, basis, 2, 4, helm ? d.k : 0.0, 0.0, 0.5,
                              0.0);
-  h2b_tree *tr = (slp && dlp) ? h2b_tree_new(nv, q->x.data(), nt, q->t.data(), basis, basis, 64,
-                                             1.4)
+  // trees of larger meshes on the device (the same trees; faster from about 8k triangles, where
+  // the host build's cost outgrows the device build's per-level round trips)
+  auto tree_fn = nt >= kDeviceTreeTriangles ? h2b_tree_new_device : h2b_tree_new;
+  h2b_tree *tr = (slp && dlp) ? tree_fn(nv, q->x.data(), nt, q->t.data(), basis, basis, 64, 1.4)
                               : nullptr;
   h2b_h2matrix *V = tr ? h2b_h2matrix_new(slp, tr, m) : nullptr;
   h2b_h2matrix *K = V ? h2b_h2matrix_new_like(dlp, V) : nullptr;  // shares V's structure
