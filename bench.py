@@ -39,6 +39,11 @@ FLOPS_PER_POINT = {"slp": 64, "dlp": 72}
 # column weights per channel 12) + 4 row points x 53 (x_a 12, <x_a, n> 5, 3 x 3 x 2 outer FMAs
 # 36) + 4 column points x 17 (y_b 12, <y_b, n> 5) + 20 for the scaling
 EXECUTED_FLOPS_PER_PAIR = 16 * 37 + 4 * 53 + 4 * 17 + 20
+# the same for the constant-basis single layer (dense cc SLP leg): 16 point pairs x 23
+# (difference 3, r^2 5, rsqrt 13, weighted sum 2) + 4 row points x 14 (x_a 12, outer sum 2) +
+# 4 column points x 9 (y_b) + 5 (pair offset 3, scaling 2); the reference counts 46 per point
+CC_SLP_FLOPS_PER_PAIR = 16 * 23 + 4 * 14 + 4 * 9 + 5
+CC_SLP_REF_FLOPS_PER_POINT = 46
 # DRAM bytes (read 5,998,336 + write 214,822,656) of one near_dist_kernel launch on the default
 # workload (sphere split 64), from an ncu capture of the full-size run (single-pass metrics
 # dram__bytes_read.sum + dram__bytes_write.sum)
@@ -68,6 +73,8 @@ def parse():
     p.add_argument("--no-serving", action="store_true")
     p.add_argument("--no-helmholtz", action="store_true")
     p.add_argument("--no-mixed", action="store_true")
+    p.add_argument("--no-dense", action="store_true")
+    p.add_argument("--dense-split", type=int, default=32)
     p.add_argument("--no-autotune", action="store_true",
                    help="keep the default launch shapes (profiling runs: no tuning launches)")
     p.add_argument("--serve-requests", type=int, default=500)
@@ -377,6 +384,15 @@ def run_ours(a, rank, world, local):
     executed = pc["distant"] * EXECUTED_FLOPS_PER_PAIR
     achieved = executed / (near_dist_ms * 1e-3) / 1e12
     ref_tflops = dist_flops / (near_dist_ms * 1e-3) / 1e12
+    # distinct triangle pairs: a pair that several nearfield blocks touch (linear basis) is
+    # evaluated once per block, as in the reference; counted once here
+    up = V.unique_pairs()
+    uniq = {"pairs": up, "evaluations_per_distant_pair": pc["distant"] / up["distant"],
+            "executed_flops": up["distant"] * EXECUTED_FLOPS_PER_PAIR,
+            "reference_count_flops": up["distant"] * 16 * (FLOPS_PER_POINT["slp"] +
+                                                           FLOPS_PER_POINT["dlp"])}
+    uniq["executed_tflops"] = uniq["executed_flops"] / (near_dist_ms * 1e-3) / 1e12
+    uniq["reference_count_tflops"] = uniq["reference_count_flops"] / (near_dist_ms * 1e-3) / 1e12
     roofline = {"bound": "fp64", "kernel": "near_dist_kernel (fused SLP+DLP, linear basis)",
                 "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
                 "traffic": NEAR_DIST_TRAFFIC if (a.split, a.clf, a.m) == (64, 64, 4) else None,
@@ -387,7 +403,8 @@ def run_ours(a, rank, world, local):
                 "reference_count": {"flops_per_launch": dist_flops,
                                     "flops_per_pair": 16 * (FLOPS_PER_POINT["slp"] +
                                                             FLOPS_PER_POINT["dlp"]),
-                                    "tflops": ref_tflops, "frac": ref_tflops / peak}}
+                                    "tflops": ref_tflops, "frac": ref_tflops / peak},
+                "unique_pairs": uniq}
 
     # ---- matvec roofline (HBM): bytes of S, N, V, E read once per product.  The operator
     # (0.55 GB of algorithmic bytes, 0.63 GB read) is five times L2, so products run back to back
@@ -702,6 +719,55 @@ def run_batched(a):
     }
 
 
+def run_dense(a, peak):
+    """Dense constant-basis single layer on the sphere split 32 (8192 triangles, q = 2 / 4;
+    assemble_bem3d_amatrix, Library/bem3d.c:9988) into device memory: every triangle pair once,
+    no shared-memory scatter.  The distant-pair kernel is timed by the operator's own events."""
+    import scipy.sparse as sps
+    import torch
+    from h2lib_b200 import bem3d as hb
+    gr = hb.new_sphere_surface3d(a.dense_split)
+    slp = hb.new_slp_laplace_bem3d(gr, 2, 4, hb.BASIS_CONSTANT_BEM3D, hb.BASIS_CONSTANT_BEM3D)
+    n = gr.triangles
+    G = torch.empty((n, n), dtype=torch.float64, device="cuda")  # 512 MB: larger than L2
+    # pairs by vertices shared, from the incidence matrix
+    t = gr.t.astype(np.int64)
+    M = sps.csr_matrix((np.ones(3 * n), (np.repeat(np.arange(n), 3), t.ravel())),
+                       shape=(n, gr.vertices))
+    S = (M @ M.T).tocoo()
+    sing = np.bincount(np.minimum(S.data.astype(np.int64), 3), minlength=4)
+    distant = n * n - int(S.nnz)
+    for _ in range(3):
+        hb.assemble_bem3d_amatrix(slp, G)
+    dist_ms, sing_ms, wall = [], [], []
+    for _ in range(5):
+        t0 = time.perf_counter()
+        hb.assemble_bem3d_amatrix(slp, G)
+        wall.append((time.perf_counter() - t0) * 1e3)
+        ms = slp.timings()
+        dist_ms.append(ms["near_distant"])
+        sing_ms.append(ms["near_singular"])
+    d = statistics.mean(dist_ms)
+    executed = distant * CC_SLP_FLOPS_PER_PAIR
+    ref = distant * 16 * CC_SLP_REF_FLOPS_PER_POINT
+    del G
+    torch.cuda.empty_cache()
+    return {"workload": f"dense cc SLP, sphere split {a.dense_split} ({n} triangles), q 2 / 4, "
+                        "FP64, output in device memory",
+            "pairs": {"distant": distant, "vertex": int(sing[1]), "edge": int(sing[2]),
+                      "identical": int(sing[3])},
+            "near_distant_ms": d, "near_singular_ms": statistics.mean(sing_ms),
+            "call_wall_ms": statistics.mean(wall),
+            "roofline": {"bound": "fp64", "kernel": "near_dist_kernel (constant basis SLP)",
+                         "flops_per_pair": CC_SLP_FLOPS_PER_PAIR,
+                         "achieved": executed / (d * 1e-3) / 1e12, "peak": peak,
+                         "unit": "TFLOP/s", "frac": executed / (d * 1e-3) / 1e12 / peak,
+                         "reference_count": {
+                             "flops_per_pair": 16 * CC_SLP_REF_FLOPS_PER_POINT,
+                             "tflops": ref / (d * 1e-3) / 1e12,
+                             "frac": ref / (d * 1e-3) / 1e12 / peak}}}
+
+
 def run_helmholtz(a):
     """Brakhage-Werner solves of config 3: unit cube split 64 (49152 triangles), constant basis,
     q 2/4, leaf 64, eta 1.4, m 5, plane wave along (1,1,1)/sqrt(3), GMRES(80) to 1e-8, k = 2
@@ -932,6 +998,11 @@ def main():
                 res["batched"] = run_batched(a)
             except Exception as e:  # reported, never hides the headline line
                 res["batched"] = {"error": str(e)[:300]}
+        if not a.no_dense:
+            try:
+                res["dense_cc_slp"] = run_dense(a, res["roofline"]["peak"])
+            except Exception as e:  # reported, never hides the headline line
+                res["dense_cc_slp"] = {"error": str(e)[:300]}
         if not a.no_helmholtz:
             try:
                 res["helmholtz"] = run_helmholtz(a)

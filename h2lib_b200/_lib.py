@@ -61,6 +61,7 @@ _SIGS = {
     "h2b_bem_nearfield": (C.c_int, [vp, vp, C.c_uint32, vp, C.c_uint32, C.c_int, vp,
                                     C.c_uint64]),
     "h2b_bem_assemble_amatrix": (C.c_int, [vp, vp, C.c_uint64]),
+    "h2b_bem_timings": (C.c_int, [vp, _f64p]),
     "h2b_h2matrix_new": (vp, [vp, vp, C.c_uint32]),
     "h2b_h2matrix_new_like": (vp, [vp, vp]),
     "h2b_h2matrix_del": (None, [vp]),
@@ -74,6 +75,7 @@ _SIGS = {
     "h2b_h2matrix_info": (C.c_int, [vp, _u64p]),
     "h2b_h2matrix_timings": (C.c_int, [vp, _f64p]),
     "h2b_h2matrix_pair_counts": (C.c_int, [vp, _u64p]),
+    "h2b_h2matrix_unique_pairs": (C.c_int, [vp, _u64p]),
     "h2b_h2matrix_export": (C.c_int, [vp, C.c_int, C.c_uint32, vp, C.POINTER(C.c_uint64)]),
     "h2b_h2matrix_export_async": (C.c_int, [vp, C.c_int, C.c_uint32, vp]),
     "h2b_h2matrix_export_wait": (C.c_int, [vp]),

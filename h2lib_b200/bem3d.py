@@ -130,6 +130,13 @@ class Bem3d:
         self.cols = gr.vertices if col_basis == BASIS_LINEAR else gr.triangles
         self.dtype = np.complex128 if pde == HELMHOLTZ else np.float64
 
+    def timings(self):
+        """Device ms of the distant and singular kernels of the last nearfield or dense
+        assembly call on this operator."""
+        ms = np.zeros(2)
+        check(lib.h2b_bem_timings(self.handle, ms), "timings")
+        return dict(zip(("near_distant", "near_singular"), ms.tolist()))
+
     def __del__(self):
         if getattr(self, "handle", None):
             try:
@@ -327,6 +334,12 @@ class H2Matrix:
     def pair_counts(self):
         c = np.zeros(4, dtype=np.uint64)
         check(lib.h2b_h2matrix_pair_counts(self.handle, c), "pair_counts")
+        return dict(zip(("distant", "vertex", "edge", "identical"), (int(v) for v in c)))
+
+    def unique_pairs(self):
+        """Distinct triangle pairs among pair_counts(), by the same cases (device bitmap)."""
+        c = np.zeros(4, dtype=np.uint64)
+        check(lib.h2b_h2matrix_unique_pairs(self.handle, c), "unique_pairs")
         return dict(zip(("distant", "vertex", "edge", "identical"), (int(v) for v in c)))
 
     def export(self, part, count=0xFFFFFFFF):

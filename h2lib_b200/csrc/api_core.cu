@@ -320,7 +320,8 @@ extern "C" h2b_bem *h2b_bem_new(const h2b_surface *s, int pde, int layer, int ro
                       cudaMemcpyHostToDevice, st) != cudaSuccess ||
       cudaMallocAsync(&b->d_err, sizeof(int), st) != cudaSuccess ||
       cudaMemsetAsync(b->d_err, 0, sizeof(int), st) != cudaSuccess ||
-      cudaStreamSynchronize(st) != cudaSuccess) {
+      cudaEventCreate(&b->ev[0]) != cudaSuccess || cudaEventCreate(&b->ev[1]) != cudaSuccess ||
+      cudaEventCreate(&b->ev[2]) != cudaSuccess || cudaStreamSynchronize(st) != cudaSuccess) {
     h2b_set_error("h2b_bem_new: %s", cudaGetErrorString(cudaGetLastError()));
     h2b_bem_del(b);
     return NULL;
@@ -333,6 +334,8 @@ extern "C" void h2b_bem_del(h2b_bem *b) {
   // the operator must be deleted before its surface (the frees are ordered on its stream)
   if (b->d_rule) cudaFreeAsync(b->d_rule, b->s->stream);
   if (b->d_err) cudaFreeAsync(b->d_err, b->s->stream);
+  for (int i = 0; i < 3; i++)
+    if (b->ev[i]) cudaEventDestroy(b->ev[i]);
   h2b_quad_free(&b->quad);
   delete b;
 }
@@ -515,7 +518,12 @@ extern "C" int h2b_bem_nearfield(const h2b_bem *bem, const uint32_t *ridx, uint3
   L.nsing = dp.nsing;
   L.nvert = dp.nvert;
   L.out0 = out;
-  rc = h2b_near_launch_kernels(&L, st);
+  // the operator's own events time the two kernels (nearfield diagnostics, h2b_bem_timings)
+  h2b_bem *mb = const_cast<h2b_bem *>(bem);
+  L.ev_between = mb->ev[1];
+  if (cudaEventRecord(mb->ev[0], st) != cudaSuccess) rc = H2B_ERR_CUDA;
+  if (rc == H2B_OK) rc = h2b_near_launch_kernels(&L, st);
+  if (rc == H2B_OK && cudaEventRecord(mb->ev[2], st) != cudaSuccess) rc = H2B_ERR_CUDA;
   if (rc == H2B_OK && !dev_out) {
     if (cudaMemcpy2DAsync(N, ld * es, out, ld_dev * es, out_rows * es, out_cols,
                           cudaMemcpyDeviceToHost, st) != cudaSuccess) {
@@ -531,7 +539,25 @@ extern "C" int h2b_bem_nearfield(const h2b_bem *bem, const uint32_t *ridx, uint3
     h2b_set_error("h2b_bem_nearfield: %s", cudaGetErrorString(cudaGetLastError()));
     rc = H2B_ERR_CUDA;
   }
+  if (rc == H2B_OK) {
+    float a = 0.0f, b = 0.0f;
+    // ev[1] is recorded only when the plan has distant tiles; otherwise both phases read 0
+    if (cudaEventElapsedTime(&a, mb->ev[0], mb->ev[1]) != cudaSuccess ||
+        cudaEventElapsedTime(&b, mb->ev[1], mb->ev[2]) != cudaSuccess) {
+      cudaGetLastError();
+      a = b = 0.0f;
+    }
+    mb->near_ms[0] = a;
+    mb->near_ms[1] = b;
+  }
   return rc;
+}
+
+extern "C" int h2b_bem_timings(const h2b_bem *bem, double ms[2]) {
+  if (!bem || !ms) return H2B_ERR_ARG;
+  ms[0] = bem->near_ms[0];
+  ms[1] = bem->near_ms[1];
+  return H2B_OK;
 }
 
 extern "C" int h2b_bem_assemble_amatrix(const h2b_bem *bem, double *G, uint64_t ld) {

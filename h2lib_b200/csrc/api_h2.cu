@@ -870,6 +870,12 @@ extern "C" int h2b_h2matrix_pair_counts(const h2b_h2matrix *h, uint64_t counts[4
   return H2B_OK;
 }
 
+extern "C" int h2b_h2matrix_unique_pairs(const h2b_h2matrix *h, uint64_t counts[4]) {
+  if (!h || !counts) return H2B_ERR_ARG;
+  return h2b_near_unique_pairs(h->bem->s->d_tri, h->d_refs, h->d_tiles, h->ntiles, h->bem->s->nt,
+                               counts, h->st);
+}
+
 // ------------------------------------------------------------------------------------------
 // inspection
 // ------------------------------------------------------------------------------------------

@@ -35,6 +35,10 @@ struct h2b_bem {
   int vert_merged = 0;  // 1: slot 4 holds h2b_quad_vert_merged's rule (q_singular == 4)
   int vert_tensor = 0;  // 1: the common-vertex rule is packed in tensor form (q_singular == 4)
   int *d_err = nullptr;
+  // device time of the last h2b_bem_nearfield call: events around the distant and singular
+  // kernels, and their elapsed ms (written by that call after its stream synchronises)
+  cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
+  double near_ms[2] = {0.0, 0.0};
 };
 
 struct h2b_devplan {

@@ -1079,6 +1079,58 @@ __global__ void __launch_bounds__(256) classify_kernel(const TriRec *tri, const 
   }
 }
 
+// Distinct triangle pairs of a tile list: every pair (t, s) of a tile sets bit t * nt + s of a
+// bitmap, and a pair whose bit was clear before counts once, by the number of vertices it shares
+// (0 distant, 1 common vertex, 2 common edge, 3 identical).  Staged like classify_kernel.
+__global__ void __launch_bounds__(256) unique_pairs_kernel(const TriRec *tri, const TriRef *refs,
+                                                           const h2b_tile *tiles, uint64_t nt,
+                                                           uint32_t *bitmap,
+                                                           unsigned long long *counts) {
+  __shared__ uint32_t rv[4][CL_CHUNK], cv[4][CL_CHUNK];
+  __shared__ unsigned long long cnt[4];
+  if (threadIdx.x < 4) cnt[threadIdx.x] = 0;
+  const h2b_tile tl = tiles[blockIdx.x];
+  const uint32_t ntr = tl.tr_len, nsc = tl.sc_len;
+  for (uint32_t c0 = 0; c0 < nsc; c0 += CL_CHUNK) {
+    const uint32_t nc = min((uint32_t) CL_CHUNK, nsc - c0);
+    for (uint32_t r0 = 0; r0 < ntr; r0 += CL_CHUNK) {
+      const uint32_t nr = min((uint32_t) CL_CHUNK, ntr - r0);
+      __syncthreads();  // the previous chunk pair is done with the stage (and cnt is zeroed)
+      for (uint32_t e = threadIdx.x; e < nr; e += blockDim.x) {
+        const uint32_t t = refs[tl.tr_off + r0 + e].t;
+        const TriRec &T = tri[t];
+        rv[0][e] = T.v[0];
+        rv[1][e] = T.v[1];
+        rv[2][e] = T.v[2];
+        rv[3][e] = t;
+      }
+      for (uint32_t e = threadIdx.x; e < nc; e += blockDim.x) {
+        const uint32_t t = refs[tl.sc_off + c0 + e].t;
+        const TriRec &S = tri[t];
+        cv[0][e] = S.v[0];
+        cv[1][e] = S.v[1];
+        cv[2][e] = S.v[2];
+        cv[3][e] = t;
+      }
+      __syncthreads();
+      const uint32_t np = nr * nc;
+      for (uint32_t p = threadIdx.x; p < np; p += blockDim.x) {
+        const uint32_t is = p / nr, it = p - is * nr;
+        uint32_t shared = 0;
+#pragma unroll
+        for (int i = 0; i < 3; i++)
+#pragma unroll
+          for (int j = 0; j < 3; j++) shared += rv[i][it] == cv[j][is];
+        const uint64_t bit = (uint64_t) rv[3][it] * nt + cv[3][is];
+        const uint32_t m = 1u << (bit & 31);
+        if (!(atomicOr(&bitmap[bit >> 5], m) & m)) atomicAdd(&cnt[min(shared, 3u)], 1ull);
+      }
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x < 4 && cnt[threadIdx.x]) atomicAdd(&counts[threadIdx.x], cnt[threadIdx.x]);
+}
+
 }  // namespace
 
 extern "C" int h2b_near_classify(const void *tri, const void *refs, const h2b_tile *tiles,
@@ -1094,6 +1146,45 @@ extern "C" int h2b_near_classify(const void *tri, const void *refs, const h2b_ti
   h2b_note_launch();
   H2B_CUDA_TRY(cudaGetLastError());
   return H2B_OK;
+}
+
+extern "C" int h2b_near_unique_pairs(const void *tri, const void *refs, const h2b_tile *tiles,
+                                     uint32_t ntiles, uint32_t nt, uint64_t counts[4],
+                                     cudaStream_t st) {
+  for (int c = 0; c < 4; c++) counts[c] = 0;
+  if (ntiles == 0) return H2B_OK;
+  if (nt > H2B_UNIQUE_PAIRS_MAX_TRIANGLES) {
+    h2b_set_error("unique pair count: %u triangles (the bitmap covers at most %u)", nt,
+                  (unsigned) H2B_UNIQUE_PAIRS_MAX_TRIANGLES);
+    return H2B_ERR_ARG;
+  }
+  const size_t words = ((uint64_t) nt * nt + 31) / 32;
+  uint32_t *bitmap = nullptr;
+  unsigned long long *d_cnt = nullptr;
+  if (cudaMallocAsync((void **) &bitmap, 4 * words + 48, st) != cudaSuccess) {
+    cudaGetLastError();
+    h2b_set_error("unique pair count: no device memory for a %llu-byte bitmap",
+                  (unsigned long long) (4 * words));
+    return H2B_ERR_NOMEM;
+  }
+  d_cnt = (unsigned long long *) (bitmap + ((words + 1) & ~(size_t) 1));
+  int rc = H2B_OK;
+  unsigned long long host[4] = {0, 0, 0, 0};
+  if (cudaMemsetAsync(bitmap, 0, 4 * words + 48, st) != cudaSuccess) rc = H2B_ERR_CUDA;
+  if (rc == H2B_OK) {
+    unique_pairs_kernel<<<ntiles, 256, 0, st>>>((const TriRec *) tri, (const TriRef *) refs,
+                                                 tiles, nt, bitmap, d_cnt);
+    h2b_note_launch();
+    if (cudaGetLastError() != cudaSuccess) rc = H2B_ERR_CUDA;
+  }
+  if (rc == H2B_OK &&
+      (cudaMemcpyAsync(host, d_cnt, sizeof(host), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+       cudaStreamSynchronize(st) != cudaSuccess))
+    rc = H2B_ERR_CUDA;
+  if (rc != H2B_OK) h2b_set_error("unique pair count: %s", cudaGetErrorString(cudaGetLastError()));
+  cudaFreeAsync(bitmap, st);
+  for (int c = 0; c < 4; c++) counts[c] = host[c];
+  return rc;
 }
 
 extern "C" int h2b_near_upload_dist_rules(void) {

@@ -53,6 +53,12 @@ int h2b_near_upload_dist_rules(void);
 int h2b_near_classify(const void *tri, const void *refs, const h2b_tile *tiles, uint32_t ntiles,
                       uint32_t *cursor, const uint32_t *base, h2b_sing *sing, cudaStream_t st);
 int h2b_near_launch_kernels(const h2b_near_launch *L, cudaStream_t st);
+/* Distinct triangle pairs of a tile list, by vertices shared (counts[0] distant, [1] common
+ * vertex, [2] common edge, [3] identical), from a bitmap of nt^2 bits in device memory (freed
+ * before the call returns; synchronises st). */
+#define H2B_UNIQUE_PAIRS_MAX_TRIANGLES 131072u
+int h2b_near_unique_pairs(const void *tri, const void *refs, const h2b_tile *tiles,
+                          uint32_t ntiles, uint32_t nt, uint64_t counts[4], cudaStream_t st);
 
 #ifdef __cplusplus
 }

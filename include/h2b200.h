@@ -212,6 +212,11 @@ int h2b_bem_nearfield(const h2b_bem *bem, const uint32_t *ridx, uint32_t rows,
  * G has n rows and n columns (n = triangles or vertices by basis), column-major with ld. */
 int h2b_bem_assemble_amatrix(const h2b_bem *bem, double *G, uint64_t ld);
 
+/* Device time (ms, CUDA events on the surface's stream) of the last h2b_bem_nearfield or
+ * h2b_bem_assemble_amatrix call on this operator: [0] distant pairs, [1] singular pairs.  No
+ * reference counterpart (diagnostics). */
+int h2b_bem_timings(const h2b_bem *bem, double ms[2]);
+
 /* ------------------------------------------------------------------------------------------
  * H2 matrices
  * ------------------------------------------------------------------------------------------ */
@@ -315,6 +320,12 @@ int h2b_h2matrix_timings(const h2b_h2matrix *h2, double ms[6]);
  * of triangles touching its row and column index sets, as assemble_ll_near_bem3d does
  * (Library/bem3d.c:3038).  No reference counterpart (diagnostics). */
 int h2b_h2matrix_pair_counts(const h2b_h2matrix *h2, uint64_t counts[4]);
+
+/* Distinct triangle pairs among those h2b_h2matrix_pair_counts counts, by the same cases: a pair
+ * of triangles that several nearfield blocks touch (the linear basis) counts once.  Counted on the
+ * device in a bitmap of triangles^2 bits (at most 131072 triangles); synchronises the matrix's
+ * stream.  No reference counterpart (diagnostics). */
+int h2b_h2matrix_unique_pairs(const h2b_h2matrix *h2, uint64_t counts[4]);
 
 /* Copy parts back for inspection, in H2Lib's layouts and orders (pre-order, column-major):
  * part 0: leaf bases of the row basis, 1: transfer matrices of the row basis (all non-root
