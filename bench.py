@@ -44,6 +44,9 @@ EXECUTED_FLOPS_PER_PAIR = 16 * 37 + 4 * 53 + 4 * 17 + 20
 # 4 column points x 9 (y_b) + 5 (pair offset 3, scaling 2); the reference counts 46 per point
 CC_SLP_FLOPS_PER_PAIR = 16 * 23 + 4 * 14 + 4 * 9 + 5
 CC_SLP_REF_FLOPS_PER_POINT = 46
+# reference count per point of the Helmholtz kernels, constant basis (sin, cos and exp counted
+# as 1): single layer 54, double layer 66
+HELM_FLOPS_PER_POINT = {"slp": 54, "dlp": 66}
 # DRAM bytes (read 5,998,336 + write 214,822,656) of one near_dist_kernel launch on the default
 # workload (sphere split 64), from an ncu capture of the full-size run (single-pass metrics
 # dram__bytes_read.sum + dram__bytes_write.sum)
@@ -768,7 +771,7 @@ def run_dense(a, peak):
                              "frac": ref / (d * 1e-3) / 1e12 / peak}}}
 
 
-def run_helmholtz(a):
+def run_helmholtz(a, peak):
     """Brakhage-Werner solves of config 3: unit cube split 64 (49152 triangles), constant basis,
     q 2/4, leaf 64, eta 1.4, m 5, plane wave along (1,1,1)/sqrt(3), GMRES(80) to 1e-8, k = 2
     and 8; FP64 with the reference's Givens rotations, FP64 with unitary rotations, and mixed
@@ -827,8 +830,19 @@ def run_helmholtz(a):
                          "reference test's 20 x 20 grid of the plane y = 0, |x| <= 10, outside "
                          "the unit disc"}
         ent = V.info()["near_entries"] + K.info()["near_entries"]
+        # distant-pair kernels of V and K, in the reference's count (sin / cos / exp = 1 flop):
+        # 16 points per pair x 54 (single layer) or 66 (double layer)
+        tv, tk, pcv = V.timings(), K.timings(), V.pair_counts()
+        ref_flops = pcv["distant"] * 16 * (HELM_FLOPS_PER_POINT["slp"] +
+                                           HELM_FLOPS_PER_POINT["dlp"])
+        near = {"pairs": pcv, "slp_distant_ms": tv["near_distant"],
+                "slp_singular_ms": tv["near_singular"], "dlp_distant_ms": tk["near_distant"],
+                "dlp_singular_ms": tk["near_singular"],
+                "reference_count_tflops": ref_flops / ((tv["near_distant"] + tk["near_distant"])
+                                                       * 1e-3) / 1e12}
+        near["reference_count_frac"] = near["reference_count_tflops"] / peak
         out.append({"k": k, "assembly_s": t_asm, "near_entries_per_s": ent / t_asm,
-                    "point_source": point,
+                    "nearfield": near, "point_source": point,
                     "fp64": {"iterations": it64, "seconds": t64,
                              "rel_residual": hb.residual_norm([K, V], [1.0, -1j * k], b, u64)},
                     "fp64_unitary": {"iterations": itu, "seconds": tu,
@@ -1005,7 +1019,7 @@ def main():
                 res["dense_cc_slp"] = {"error": str(e)[:300]}
         if not a.no_helmholtz:
             try:
-                res["helmholtz"] = run_helmholtz(a)
+                res["helmholtz"] = run_helmholtz(a, res["roofline"]["peak"])
             except Exception as e:  # reported, never hides the headline line
                 res["helmholtz"] = {"error": str(e)[:300]}
         if not a.no_serving:

@@ -403,6 +403,56 @@ int h2b_devplan_upload(const h2b_nearplan *p, cudaStream_t st, h2b_devplan *dp) 
   return H2B_OK;
 }
 
+int h2b_classify_device(const void *d_tri, const void *refs, const h2b_tile *tiles,
+                        uint32_t ntiles, cudaStream_t st, h2b_sing **d_sing, uint32_t cnt[4]) {
+  *d_sing = nullptr;
+  for (int c = 0; c < 4; c++) cnt[c] = 0;
+  uint32_t *d_cur = nullptr;
+  H2B_CUDA_TRY(cudaMallocAsync(&d_cur, sizeof(uint32_t) * 8, st));
+  int rc = H2B_OK;
+  uint32_t host[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  if (cudaMemsetAsync(d_cur, 0, sizeof(uint32_t) * 8, st) != cudaSuccess) rc = H2B_ERR_CUDA;
+  if (rc == H2B_OK) rc = h2b_near_classify(d_tri, refs, tiles, ntiles, d_cur, nullptr, nullptr, st);
+  if (rc == H2B_OK &&
+      (cudaMemcpyAsync(host, d_cur, sizeof(uint32_t) * 4, cudaMemcpyDeviceToHost, st) !=
+           cudaSuccess ||
+       cudaStreamSynchronize(st) != cudaSuccess))
+    rc = H2B_ERR_CUDA;
+  const uint64_t nsing = (uint64_t) host[1] + host[2] + host[3];
+  if (rc == H2B_OK && nsing > UINT32_MAX) {
+    h2b_set_error("singular-pair classification: %llu pairs exceed the 32-bit pair list",
+                  (unsigned long long) nsing);
+    cudaFreeAsync(d_cur, st);
+    return H2B_ERR_ARG;
+  }
+  if (rc == H2B_OK) {
+    // base offsets of the cases in host[4..7]
+    host[4] = 0;
+    host[5] = 0;
+    host[6] = host[1];
+    host[7] = host[1] + host[2];
+    if (nsing &&
+        (cudaMallocAsync((void **) d_sing, sizeof(h2b_sing) * nsing, st) != cudaSuccess ||
+         cudaMemsetAsync(d_cur, 0, sizeof(uint32_t) * 4, st) != cudaSuccess ||
+         cudaMemcpyAsync(d_cur + 4, host + 4, sizeof(uint32_t) * 4, cudaMemcpyHostToDevice, st) !=
+             cudaSuccess))
+      rc = H2B_ERR_CUDA;
+  }
+  if (rc == H2B_OK && nsing)
+    rc = h2b_near_classify(d_tri, refs, tiles, ntiles, d_cur, d_cur + 4, *d_sing, st);
+  if (rc == H2B_OK && cudaStreamSynchronize(st) != cudaSuccess) rc = H2B_ERR_CUDA;
+  if (rc == H2B_ERR_CUDA)
+    h2b_set_error("singular-pair classification: %s", cudaGetErrorString(cudaGetLastError()));
+  cudaFreeAsync(d_cur, st);
+  if (rc != H2B_OK && *d_sing) {
+    cudaFreeAsync(*d_sing, st);
+    *d_sing = nullptr;
+  }
+  if (rc == H2B_OK)
+    for (int c = 1; c <= 3; c++) cnt[c] = host[c];
+  return rc;
+}
+
 void h2b_devplan_free(h2b_devplan *dp, cudaStream_t st) {
   if (dp->tiles) cudaFreeAsync(dp->tiles, st);
   if (dp->refs) cudaFreeAsync(dp->refs, st);
@@ -484,8 +534,11 @@ extern "C" int h2b_bem_nearfield(const h2b_bem *bem, const uint32_t *ridx, uint3
   uint64_t t64 = (uint64_t) ((rows + 63) / 64) * ((cols + 63) / 64);
   uint32_t tile = t64 < 2ull * s->num_sms ? 32 : 64;
 
+  // the singular pairs are found on the device (h2b_classify_device): the host plan only lists
+  // the tiles and their triangles
   h2b_nearplan plan;
   h2b_nearplan_init(&plan);
+  plan.skip_sing = 1;
   rc = h2b_nearplan_add_block(&plan, const_cast<h2b_adjacency *>(&s->adj), bem->row_basis,
                               bem->col_basis, ridx, rows, cidx, cols, 0, (uint32_t) ld_dev,
                               ntrans, tile);
@@ -498,7 +551,20 @@ extern "C" int h2b_bem_nearfield(const h2b_bem *bem, const uint32_t *ridx, uint3
   h2b_devplan dp;
   rc = h2b_devplan_upload(&plan, st, &dp);
   h2b_nearplan_free(&plan);
-  if (rc != H2B_OK) return rc;
+  if (rc != H2B_OK) {
+    h2b_devplan_free(&dp, st);
+    return rc;
+  }
+  {
+    uint32_t cnt[4];
+    rc = h2b_classify_device(s->d_tri, dp.refs, dp.tiles, dp.ntiles, st, &dp.sing, cnt);
+    if (rc != H2B_OK) {
+      h2b_devplan_free(&dp, st);
+      return rc;
+    }
+    dp.nsing = cnt[1] + cnt[2] + cnt[3];
+    dp.nvert = cnt[1];
+  }
 
   double *out = N;
   if (!dev_out) {

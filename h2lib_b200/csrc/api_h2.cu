@@ -227,47 +227,17 @@ extern "C" void h2b_h2matrix_del(h2b_h2matrix *h) {
   delete h;
 }
 
-// Singular pairs of the uploaded tiles, found on the device in two passes (count, then write
-// grouped by Sauter-Schwab case: vertex, edge, identical), and the pair counts per case.
+// Singular pairs of the uploaded tiles (found on the device) and the pair counts per case.
 static int classify_singular(h2b_h2matrix *h, uint64_t all_pairs) {
-  uint32_t *d_cur = nullptr;
-  H2B_CUDA_TRY(cudaMallocAsync(&d_cur, sizeof(uint32_t) * 8, h->st));
-  int rc = H2B_OK;
-  uint32_t cnt[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-  if (cudaMemsetAsync(d_cur, 0, sizeof(uint32_t) * 8, h->st) != cudaSuccess) rc = H2B_ERR_CUDA;
-  if (rc == H2B_OK)
-    rc = h2b_near_classify(h->bem->s->d_tri, h->d_refs, h->d_tiles, h->ntiles, d_cur, nullptr,
-                           nullptr, h->st);
-  if (rc == H2B_OK &&
-      (cudaMemcpyAsync(cnt, d_cur, sizeof(uint32_t) * 4, cudaMemcpyDeviceToHost, h->st) !=
-           cudaSuccess ||
-       cudaStreamSynchronize(h->st) != cudaSuccess))
-    rc = H2B_ERR_CUDA;
+  uint32_t cnt[4] = {0, 0, 0, 0};
+  const int rc = h2b_classify_device(h->bem->s->d_tri, h->d_refs, h->d_tiles, h->ntiles, h->st,
+                                     &h->d_sing, cnt);
+  if (rc != H2B_OK) return rc;
   const uint64_t nsing = (uint64_t) cnt[1] + cnt[2] + cnt[3];
-  if (rc == H2B_OK) {
-    // base offsets of the cases in cnt[4..7]
-    cnt[4] = 0;
-    cnt[5] = 0;
-    cnt[6] = cnt[1];
-    cnt[7] = cnt[1] + cnt[2];
-    h->nsing = (uint32_t) nsing;
-    for (int c = 1; c <= 3; c++) h->pairs[c] = cnt[c];
-    h->pairs[0] = all_pairs - nsing;
-    if (cudaMallocAsync(&h->d_sing, sizeof(h2b_sing) * std::max<uint64_t>(nsing, 1), h->st) != cudaSuccess ||
-        cudaMemsetAsync(d_cur, 0, sizeof(uint32_t) * 4, h->st) != cudaSuccess ||
-        cudaMemcpyAsync(d_cur + 4, cnt + 4, sizeof(uint32_t) * 4, cudaMemcpyHostToDevice, h->st) !=
-            cudaSuccess)
-      rc = H2B_ERR_CUDA;
-  }
-  if (rc == H2B_OK && nsing)
-    rc = h2b_near_classify(h->bem->s->d_tri, h->d_refs, h->d_tiles, h->ntiles, d_cur, d_cur + 4,
-                           h->d_sing, h->st);
-  if (rc == H2B_OK && cudaStreamSynchronize(h->st) != cudaSuccess) rc = H2B_ERR_CUDA;
-  if (rc == H2B_ERR_CUDA)
-    h2b_set_error("h2matrix singular-pair classification: %s",
-                  cudaGetErrorString(cudaGetLastError()));
-  cudaFreeAsync(d_cur, h->st);
-  return rc;
+  h->nsing = (uint32_t) nsing;
+  for (int c = 1; c <= 3; c++) h->pairs[c] = cnt[c];
+  h->pairs[0] = all_pairs - nsing;
+  return H2B_OK;
 }
 
 extern "C" h2b_h2matrix *h2b_h2matrix_new(const h2b_bem *bem, const h2b_tree *tree, uint32_t m) {

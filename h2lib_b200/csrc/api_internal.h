@@ -57,4 +57,10 @@ uint32_t h2b_bem_rows(const h2b_bem *b);
 uint32_t h2b_bem_cols(const h2b_bem *b);
 int h2b_devplan_upload(const h2b_nearplan *p, cudaStream_t st, h2b_devplan *dp);
 void h2b_devplan_free(h2b_devplan *dp, cudaStream_t st);
+// Singular pairs of uploaded tiles, found on the device in two passes (count, then write grouped
+// by Sauter-Schwab case: vertex, edge, identical; order inside a case not fixed).  *d_sing: a
+// stream-ordered device array of cnt[1] + cnt[2] + cnt[3] pairs (nullptr when there are none);
+// cnt[c]: pairs of case c = 1..3.  Synchronises st.
+int h2b_classify_device(const void *d_tri, const void *refs, const h2b_tile *tiles,
+                        uint32_t ntiles, cudaStream_t st, h2b_sing **d_sing, uint32_t cnt[4]);
 int h2b_check_err_flag(const h2b_bem *b, cudaStream_t st);
