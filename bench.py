@@ -835,7 +835,7 @@ def run_helmholtz(a, peak):
         tv, tk, pcv = V.timings(), K.timings(), V.pair_counts()
         ref_flops = pcv["distant"] * 16 * (HELM_FLOPS_PER_POINT["slp"] +
                                            HELM_FLOPS_PER_POINT["dlp"])
-        near = {"pairs": pcv, "slp_distant_ms": tv["near_distant"],
+        near = {"pairs": pcv, "phase_ms": {"V": tv, "K": tk}, "slp_distant_ms": tv["near_distant"],
                 "slp_singular_ms": tv["near_singular"], "dlp_distant_ms": tk["near_distant"],
                 "dlp_singular_ms": tk["near_singular"],
                 "reference_count_tflops": ref_flops / ((tv["near_distant"] + tk["near_distant"])

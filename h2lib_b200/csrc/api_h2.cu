@@ -109,13 +109,13 @@ static int devtree_flat_setup(DevCTree &t, const h2b_ctree &c, const std::vector
 
 // W^T from V and E: leaves first, then the father levels from the deepest up.  `transposed`: the
 // basis stores V^T and E^T (column side); otherwise V and E (row side).
-static int devtree_flatten(DevCTree &t, uint32_t k, int transposed, cudaStream_t st) {
+static int devtree_flatten(DevCTree &t, uint32_t m, uint32_t k, int transposed, cudaStream_t st) {
   FlatLeafArgs la{t.d_wleaves, t.d_size, t.d_voff, t.d_woff, t.d_V, t.d_W, t.nwleaves, (int) k,
                   !transposed};
   int rc = h2b_flat_leaves(&la, st);
   for (int l = (int) t.depth - 1; rc == H2B_OK && l >= 0; l--) {
-    FlatArgs fa{t.d_fitems + 4 * (size_t) t.fitem_start[l], t.d_off, t.d_size, t.d_woff, t.d_E,
-                t.d_W, t.fitem_count[l], (int) k, transposed};
+    FlatArgs fa{t.d_fitems + 4 * (size_t) t.fitem_start[l], t.d_off, t.d_size, t.d_woff,
+                t.d_pts, t.d_W, t.fitem_count[l], (int) m, (int) k};
     rc = h2b_flat_level(&fa, st);
   }
   return rc;
@@ -594,7 +594,7 @@ static int assemble_basis(h2b_h2matrix *h, DevCTree &t, int basis, int dn) {
   FarTransferArgs ta{t.d_nonroot, t.d_father, t.d_pts, t.d_E, t.nnonroot, (int) h->m, (int) h->k,
                      transposed};
   rc = h2b_far_transfer(&ta, h->st);
-  if (rc == H2B_OK) rc = devtree_flatten(t, h->k, transposed, h->st);
+  if (rc == H2B_OK) rc = devtree_flatten(t, h->m, h->k, transposed, h->st);
   return rc;
 }
 

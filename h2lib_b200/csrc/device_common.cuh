@@ -64,6 +64,15 @@ __device__ __forceinline__ double rsqrt_nr(double x) {
   return fma(0.5 * y, e, y);
 }
 
+// Lagrange polynomial mu of the nodes xi[0..m) at x, prod_{l != mu} (x - xi_l) / (xi_mu - xi_l)
+// (the one-dimensional factor of the tensor interpolation, Library/bem3d.c:8497).
+__device__ __forceinline__ double lagrange_1d(double x, const double *xi, int mu, int m) {
+  double v = 1.0;
+  for (int l = 0; l < m; l++)
+    if (l != mu) v *= (x - xi[l]) / (xi[mu] - xi[l]);
+  return v;
+}
+
 // Allow kernel K up to H2B_MAX_DYN_SMEM bytes of dynamic shared memory, once per process
 // (thread-safe static initialisation).  Launches pass the size they need; the attribute never
 // changes afterwards, so launches from several host threads (a solve server's workers) cannot

@@ -23,17 +23,10 @@ namespace {
 
 constexpr int MMAX = 8;
 
-__device__ __forceinline__ double lagr1(double x, const double *xi, int mu, int m) {
-  double v = 1.0;
-  for (int l = 0; l < m; l++)
-    if (l != mu) v *= (x - xi[l]) / (xi[mu] - xi[l]);
-  return v;
-}
-
 // Lagrange polynomial mu of nodes xi[0..m) at x as wbar_mu prod_{l != mu} (x - xi_l), with the
 // barycentric weight wbar_mu = 1 / prod_{l != mu} (xi_mu - xi_l) computed once per node set,
 // and its derivative wbar_mu sum_{l != mu} prod_{l2 != mu, l} (x - xi_l2): the same polynomials
-// as lagr1 (and its derivative) without a division per evaluation.
+// as lagrange_1d (and its derivative) without a division per evaluation.
 __device__ __forceinline__ double lagr_bar(double x, const double *xi, double wbar, int mu, int m) {
   double v = wbar;
   for (int l = 0; l < m; l++)
@@ -193,7 +186,7 @@ __global__ void __launch_bounds__(256) transfer_kernel(FarTransferArgs a) {
   __shared__ double L1[3][MMAX][MMAX];  // L1[d][point a][basis mu]
   for (int e = threadIdx.x; e < 3 * m * m; e += blockDim.x) {
     const int d = e / (m * m), p = (e / m) % m, mu = e % m;
-    L1[d][p][mu] = lagr1(sp[d * m + p], fp + d * m, mu, m);
+    L1[d][p][mu] = lagrange_1d(sp[d * m + p], fp + d * m, mu, m);
   }
   __syncthreads();
   double *E = a.E + (size_t) (c - 1) * k * k;  // clusters 1..n-1 in pre-order

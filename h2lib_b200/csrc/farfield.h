@@ -48,12 +48,11 @@ struct FarCouplingArgs {
 struct FlatArgs {
   const uint32_t *items;     // 4 per item: father, son, first row in the son, rows
   const uint32_t *off, *size;
-  const uint64_t *woff;      // per cluster: offset of W_t (doubles)
-  const double *E;           // transfer matrices (E or E^T), cluster c at (c-1)*k*k
+  const uint64_t *woff;      // per cluster: offset of W_t (doubles); W^T is k x |t| (ld k)
+  const double *pts;         // per cluster: the m one-dimensional nodes per axis (3 m doubles)
   double *W;
   uint32_t nitems;
-  int k;
-  int e_transposed;          // E stored transposed (column side: E^T); W^T is k x |t| always
+  int m, k;
 };
 
 struct FlatLeafArgs {

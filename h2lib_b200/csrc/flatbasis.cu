@@ -41,60 +41,93 @@ __device__ __forceinline__ void cta_copy(double *dst, size_t n, F src) {
   }
 }
 
-// CTA (item, part): item = (father f, son s, first row r0 of s, rows nr <= H2B_FLAT_ROWS), part =
-// up to FLAT_COLS consecutive columns nu of the product (one part for k <= 64); the nr rows of
-// W_s times those columns of E_s land in the rows of s inside W_f.  Short row slices give every
-// level's launch enough CTAs and read each son's rows once; E_s is read by every slice of the son
-// (from L2).  W^T is stored k x |t| (ld k) on both sides.
-constexpr int FLAT_COLS = 64;
+// CTA per item = (father f, son s, first row r0 of s, rows nr <= H2B_FLAT_ROWS): the nr rows of
+// W_s times E_s land in the rows of s inside W_f.  E_s is the tensor product of three m x m
+// one-dimensional transfers, E_s[(a, b, c), (jx, jy, jz)] = Lx[a][jx] Ly[b][jy] Lz[c][jz] with
+// L_d[a][mu] = father polynomial mu of axis d at son node a (the factors of transfer_kernel), so
+// each row, an m x m x m tensor w[a][b][c], is multiplied one axis at a time:
+//   t1[a][b][jz] = sum_c w[a][b][c] Lz[c][jz],  t2[a][jy][jz] = sum_b t1[a][b][jz] Ly[b][jy],
+//   W_f[jx][jy][jz] = sum_a t2[a][jy][jz] Lx[a][jx]
+// -- 3 m^4 multiply-adds per row instead of the k^2 = m^6 of the full product (the same sum,
+// bracketed by axis).  The rows are staged in shared memory in chunks of RB; a thread takes one
+// fibre of m inputs and writes its m outputs, so every input is read once per step.
+template <int M>
+struct FlatShape {
+  static constexpr int K = M * M * M;
+  // rows per chunk: two K-double buffers per row within 96 KiB (at most H2B_FLAT_ROWS)
+  static constexpr int RB = (96 * 1024) / (16 * K) < H2B_FLAT_ROWS ? (96 * 1024) / (16 * K)
+                                                                   : H2B_FLAT_ROWS;
+  static_assert(RB >= 1, "rank too large for the staged flatten");
+};
+
+template <int M>
 __global__ void __launch_bounds__(FLAT_TPB) flatten_kernel(FlatArgs a) {
+  constexpr int K = FlatShape<M>::K, RB = FlatShape<M>::RB, MM = M * M;
   extern __shared__ double sm[];
-  const uint32_t k = (uint32_t) a.k;
-  const uint32_t nparts = (k + FLAT_COLS - 1) / FLAT_COLS;
-  const uint32_t item = blockIdx.x / nparts, part = blockIdx.x % nparts;
-  const uint32_t *it = a.items + 4 * (size_t) item;
+  __shared__ double L[3][M][M];  // L[d][son node][father polynomial]
+  const uint32_t *it = a.items + 4 * (size_t) blockIdx.x;
   const uint32_t f = it[0], s = it[1], r0 = it[2], nr = it[3];
-  const uint32_t c0 = part * FLAT_COLS, nc = min((uint32_t) FLAT_COLS, k - c0);
-  double *sE = sm;                  // sE[j + mu nc] = E_s[mu, c0 + j]
-  double *sW = sm + k * FLAT_COLS;  // W_s[r0 + i, mu] at sW[mu + i (k + 1)]
-  const double *E = a.E + (size_t) (s - 1) * k * k;
+  const double *fp = a.pts + (size_t) f * 3 * M, *sp = a.pts + (size_t) s * 3 * M;
+  for (int e = (int) threadIdx.x; e < 3 * MM; e += (int) blockDim.x) {
+    const int d = e / MM, p = (e / M) % M, mu = e % M;
+    L[d][p][mu] = lagrange_1d(sp[d * M + p], fp + d * M, mu, M);
+  }
+  double *A = sm, *B = sm + (size_t) RB * K;
   const uint32_t rf = a.off[s] - a.off[f] + r0;  // first row inside f
-  const double *Ws = a.W + a.woff[s];
-  double *Wf = a.W + a.woff[f];
-  // E_s from E^T (column side: E_s[mu, nu] = E^T[nu + mu k]) or from E itself (row side:
-  // E_s[mu, nu] = E[mu + nu k])
-  for (uint32_t e = threadIdx.x; e < k * nc; e += blockDim.x) {
-    const uint32_t j = e % nc, mu = e / nc;
-    sE[j + mu * nc] = a.e_transposed ? E[c0 + j + (size_t) mu * k] : E[mu + (size_t) (c0 + j) * k];
-  }
-  // W_s^T (k x |s|, ld k) is contiguous over the item's rows: sW[mu + i (k + 1)] (padded stride,
-  // so that a warp's rows fall in different banks)
-  for (uint32_t e = threadIdx.x; e < nr * k; e += blockDim.x) {
-    const uint32_t mu = e % k, i = e / k;
-    sW[mu + i * (k + 1)] = Ws[(size_t) r0 * k + e];
-  }
-  __syncthreads();
-  // thread = column j = t % 64, rows ig + 4 r (ig = t / 64); a warp writes 32 consecutive nu of
-  // one row of W_f^T
-  static_assert(FLAT_TPB / FLAT_COLS == 4 && H2B_FLAT_ROWS % 4 == 0, "thread mapping");
-  constexpr int RC = H2B_FLAT_ROWS / 4;
-  const uint32_t j = threadIdx.x % FLAT_COLS, ig = threadIdx.x / FLAT_COLS;
-  if (j < nc) {
-    double acc[RC];
+  const double *Ws = a.W + a.woff[s] + (size_t) r0 * K;
+  double *Wf = a.W + a.woff[f] + (size_t) rf * K;
+  for (uint32_t c0 = 0; c0 < nr; c0 += RB) {
+    const uint32_t nc = min((uint32_t) RB, nr - c0);
+    __syncthreads();  // L is ready; the previous chunk's last step has read A
+    // W_s^T rows are contiguous (ld K)
+    for (uint32_t e = threadIdx.x; e < nc * K; e += blockDim.x) A[e] = Ws[(size_t) c0 * K + e];
+    __syncthreads();
+    // z: fibre g = (row, a, b) of A -> B[row][a][b][jz]
+    for (uint32_t g = threadIdx.x; g < nc * MM; g += blockDim.x) {
+      double in[M];
 #pragma unroll
-    for (int r = 0; r < RC; r++) acc[r] = 0.0;
-    for (uint32_t mu = 0; mu < k; mu++) {
-      const double y = sE[j + mu * nc];
+      for (int c = 0; c < M; c++) in[c] = A[(size_t) g * M + c];
 #pragma unroll
-      for (int r = 0; r < RC; r++) {
-        const uint32_t i = ig + 4u * r;
-        if (i < nr) acc[r] = fma(sW[mu + i * (k + 1)], y, acc[r]);
+      for (int jz = 0; jz < M; jz++) {
+        double acc = 0.0;
+#pragma unroll
+        for (int c = 0; c < M; c++) acc = fma(in[c], L[2][c][jz], acc);
+        B[(size_t) g * M + jz] = acc;
       }
     }
+    __syncthreads();
+    // y: fibre g = (row, a, jz) of B (stride M) -> A[row][a][jy][jz]
+    for (uint32_t g = threadIdx.x; g < nc * MM; g += blockDim.x) {
+      const uint32_t jz = g % M, ra = g / M;
+      const double *x = B + (size_t) ra * MM + jz;
+      double in[M];
 #pragma unroll
-    for (int r = 0; r < RC; r++) {
-      const uint32_t i = ig + 4u * r;
-      if (i < nr) Wf[(size_t) (rf + i) * k + c0 + j] = acc[r];
+      for (int b = 0; b < M; b++) in[b] = x[b * M];
+#pragma unroll
+      for (int jy = 0; jy < M; jy++) {
+        double acc = 0.0;
+#pragma unroll
+        for (int b = 0; b < M; b++) acc = fma(in[b], L[1][b][jy], acc);
+        A[(size_t) ra * MM + jy * M + jz] = acc;
+      }
+    }
+    __syncthreads();
+    // x: fibre g = (row, jy, jz) of A (stride M^2) -> W_f rows, consecutive threads writing
+    // consecutive (jy, jz)
+    for (uint32_t g = threadIdx.x; g < nc * MM; g += blockDim.x) {
+      const uint32_t yz = g % MM, row = g / MM;
+      const double *x = A + (size_t) row * K + yz;
+      double in[M];
+#pragma unroll
+      for (int p = 0; p < M; p++) in[p] = x[p * MM];
+      double *o = Wf + (size_t) (c0 + row) * K + yz;
+#pragma unroll
+      for (int jx = 0; jx < M; jx++) {
+        double acc = 0.0;
+#pragma unroll
+        for (int p = 0; p < M; p++) acc = fma(in[p], L[0][p][jx], acc);
+        o[jx * MM] = acc;
+      }
     }
   }
 }
@@ -144,17 +177,33 @@ extern "C" int h2b_flat_leaves(const FlatLeafArgs *a, cudaStream_t st) {
   return H2B_OK;
 }
 
-extern "C" int h2b_flat_level(const FlatArgs *a, cudaStream_t st) {
-  if (a->nitems == 0) return H2B_OK;
-  const size_t smem = sizeof(double) * ((size_t) a->k * FLAT_COLS + (size_t) H2B_FLAT_ROWS * (a->k + 1));
-  if (smem > H2B_MAX_DYN_SMEM) {
-    h2b_set_error("flattened bases: rank %d needs %zu bytes of shared memory", a->k, smem);
-    return H2B_ERR_ARG;
-  }
-  H2B_CUDA_TRY(h2b_allow_smem<flatten_kernel>());
-  const uint32_t nparts = ((uint32_t) a->k + FLAT_COLS - 1) / FLAT_COLS;
-  flatten_kernel<<<a->nitems * nparts, FLAT_TPB, smem, st>>>(*a);
+template <int M>
+static int launch_flatten(const FlatArgs *a, cudaStream_t st) {
+  constexpr size_t smem = sizeof(double) * 2 * FlatShape<M>::RB * FlatShape<M>::K;
+  H2B_CUDA_TRY(h2b_allow_smem<flatten_kernel<M>>());
+  flatten_kernel<M><<<a->nitems, FLAT_TPB, smem, st>>>(*a);
   h2b_note_launch();
   H2B_CUDA_TRY(cudaGetLastError());
   return H2B_OK;
+}
+
+extern "C" int h2b_flat_level(const FlatArgs *a, cudaStream_t st) {
+  if (a->nitems == 0) return H2B_OK;
+  if (a->k != a->m * a->m * a->m) {
+    h2b_set_error("flattened bases: rank %d is not m^3 for m = %d", a->k, a->m);
+    return H2B_ERR_ARG;
+  }
+  switch (a->m) {
+    case 1: return launch_flatten<1>(a, st);
+    case 2: return launch_flatten<2>(a, st);
+    case 3: return launch_flatten<3>(a, st);
+    case 4: return launch_flatten<4>(a, st);
+    case 5: return launch_flatten<5>(a, st);
+    case 6: return launch_flatten<6>(a, st);
+    case 7: return launch_flatten<7>(a, st);
+    case 8: return launch_flatten<8>(a, st);
+    default:
+      h2b_set_error("flattened bases: interpolation order %d outside 1..8", a->m);
+      return H2B_ERR_ARG;
+  }
 }
