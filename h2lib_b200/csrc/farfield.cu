@@ -177,57 +177,89 @@ __global__ void __launch_bounds__(256) leaf_basis_kernel(FarLeafArgs a) {
   }
 }
 
-// Transfer matrix of every non-root cluster: E_c[i, nu] = L^father_nu(xi^c_i), k x k.
-__global__ void __launch_bounds__(256) transfer_kernel(FarTransferArgs a) {
+// Transfer matrix of every non-root cluster: E_c[i, nu] = L^father_nu(xi^c_i), k x k, the
+// product Lx[ia][jx] Ly[ib][jy] Lz[ic][jz] of the one-dimensional factors (i = (ia m + ib) m + ic,
+// nu = (jx m + jy) m + jz).  CTA per cluster, thread per index of the stored matrix's fast
+// dimension (i for E, nu for E^T), looping over the other one: consecutive threads write
+// consecutive words.
+__global__ void __launch_bounds__(128) transfer_kernel(FarTransferArgs a) {
   const uint32_t c = a.clusters[blockIdx.x];
   const uint32_t f = a.father[c];
-  const int m = a.m, k = a.k;
+  const int m = a.m, k = a.k, mm = m * m;
   const double *fp = a.pts + (size_t) f * 3 * m, *sp = a.pts + (size_t) c * 3 * m;
-  __shared__ double L1[3][MMAX][MMAX];  // L1[d][point a][basis mu]
-  for (int e = threadIdx.x; e < 3 * m * m; e += blockDim.x) {
-    const int d = e / (m * m), p = (e / m) % m, mu = e % m;
+  __shared__ double L1[3][MMAX][MMAX];  // L1[d][son node][father polynomial]
+  for (int e = threadIdx.x; e < 3 * mm; e += blockDim.x) {
+    const int d = e / mm, p = (e / m) % m, mu = e % m;
     L1[d][p][mu] = lagrange_1d(sp[d * m + p], fp + d * m, mu, m);
   }
   __syncthreads();
-  double *E = a.E + (size_t) (c - 1) * k * k;  // clusters 1..n-1 in pre-order
-  for (int e = threadIdx.x; e < k * k; e += blockDim.x) {
-    const int i = e % k, nu = e / k;
-    const int ia = i / (m * m), ib = (i / m) % m, ic = i % m;
-    const int jx = nu / (m * m), jy = (nu / m) % m, jz = nu % m;
-    const double v = L1[0][ia][jx] * L1[1][ib][jy] * L1[2][ic][jz];
-    if (a.transposed)
-      E[nu + (size_t) i * k] = v;
-    else
-      E[e] = v;
+  const int t = threadIdx.x;
+  if (t >= k) return;
+  const int t0 = t / mm, t1 = (t / m) % m, t2 = t % m;
+  double *E = a.E + (size_t) (c - 1) * k * k + t;  // clusters 1..n-1 in pre-order
+  int o = 0;
+  if (!a.transposed) {
+    // t = son node i: E[i + nu k] over nu
+    for (int jx = 0; jx < m; jx++)
+      for (int jy = 0; jy < m; jy++) {
+        const double xy = L1[0][t0][jx] * L1[1][t1][jy];
+        for (int jz = 0; jz < m; jz++, o += k) E[o] = xy * L1[2][t2][jz];
+      }
+  } else {
+    // t = father polynomial nu: E^T[nu + i k] over i
+    for (int ia = 0; ia < m; ia++)
+      for (int ib = 0; ib < m; ib++) {
+        const double xy = L1[0][ia][t0] * L1[1][ib][t1];
+        for (int ic = 0; ic < m; ic++, o += k) E[o] = xy * L1[2][ic][t2];
+      }
   }
 }
 
-// Coupling matrices: S_b[i, j] = (1/4pi) g(xi^r_i, xi^c_j), i = (ix m + iy) m + iz.  Written as
-// one coalesced store stream per block (HBM bound: 8 or 16 bytes per entry).  M > 0 fixes the
-// interpolation order at compile time (the index arithmetic then uses constant divisors); the
-// reciprocal distance is the FP64 reciprocal square root of the nearfield kernels.
-template <bool CX, int M>
-__global__ void __launch_bounds__(256) coupling_kernel(FarCouplingArgs a) {
+// Coupling matrices: S_b[i, j] = (1/4pi) g(xi^r_i, xi^c_j), i = (ix m + iy) m + iz.  CTA per
+// block, thread per row i (k <= 128 rows, the CTA rounded up to whole warps): the thread keeps
+// its row point in registers and walks the columns j, whose points the CTA tabulates in shared
+// memory first (every thread then reads the same word: a broadcast), so no index arithmetic is
+// left in the loop.  Column j of S_b is written by consecutive threads (column-major, ld k):
+// 8 or 16 bytes per entry, one store each.
+template <bool CX>
+__global__ void __launch_bounds__(128) coupling_kernel(FarCouplingArgs a) {
+  __shared__ double yc[3][128];
   const uint32_t b = blockIdx.x;
   const uint32_t rc = a.rc[b], cc = a.cc[b];
-  const int m = M > 0 ? M : a.m, k = M > 0 ? M * M * M : a.k;
+  const int m = a.m, k = a.k, mm = m * m;
   const double *rp = a.rpts + (size_t) rc * 3 * m, *cp = a.cpts + (size_t) cc * 3 * m;
-  double *S = a.S + (size_t) b * k * k * (CX ? 2 : 1);
-  for (int e = threadIdx.x; e < k * k; e += blockDim.x) {
-    const int i = e % k, j = e / k;
-    const double x0 = rp[i / (m * m)], x1 = rp[m + (i / m) % m], x2 = rp[2 * m + i % m];
-    const double y0 = cp[j / (m * m)], y1 = cp[m + (j / m) % m], y2 = cp[2 * m + j % m];
-    const double d0 = x0 - y0, d1 = x1 - y1, d2 = x2 - y2;
-    const double r2 = d0 * d0 + d1 * d1 + d2 * d2;
-    const double rinv = rsqrt_nr(r2);
-    if (!CX) {
-      S[e] = a.kconst * rinv;
-    } else {
-      double r = r2 * rinv, rn = rinv, s, c;
-      if (a.k_imn != 0.0) rn *= exp(a.k_imn * r);
-      sincos(a.k_re * r, &s, &c);
-      S[2 * e] = a.kconst * (rn * c);
-      S[2 * e + 1] = a.kconst * (rn * s);
+  for (int j = threadIdx.x; j < k; j += blockDim.x) {
+    yc[0][j] = cp[j / mm];
+    yc[1][j] = cp[m + (j / m) % m];
+    yc[2][j] = cp[2 * m + j % m];
+  }
+  const int i = threadIdx.x;
+  double x0 = 0.0, x1 = 0.0, x2 = 0.0;
+  if (i < k) {
+    x0 = rp[i / mm];
+    x1 = rp[m + (i / m) % m];
+    x2 = rp[2 * m + i % m];
+  }
+  __syncthreads();
+  if (i >= k) return;
+  const double kc = a.kconst, kre = a.k_re, kim = a.k_imn;
+  if (!CX) {
+    double *S = a.S + (size_t) b * k * k + i;
+    for (int j = 0; j < k; j++) {
+      const double d0 = x0 - yc[0][j], d1 = x1 - yc[1][j], d2 = x2 - yc[2][j];
+      const double r2 = fma(d0, d0, fma(d1, d1, d2 * d2));
+      S[(size_t) j * k] = kc * rsqrt_nr(r2);
+    }
+  } else {
+    double2 *S = reinterpret_cast<double2 *>(a.S) + (size_t) b * k * k + i;
+    for (int j = 0; j < k; j++) {
+      const double d0 = x0 - yc[0][j], d1 = x1 - yc[1][j], d2 = x2 - yc[2][j];
+      const double r2 = fma(d0, d0, fma(d1, d1, d2 * d2));
+      const double rinv = rsqrt_nr(r2);
+      double r = r2 * rinv, rn = rinv, sn, cs;
+      if (kim != 0.0) rn *= exp(kim * r);
+      sincos(kre * r, &sn, &cs);
+      S[(size_t) j * k] = make_double2(kc * (rn * cs), kc * (rn * sn));
     }
   }
 }
@@ -268,7 +300,11 @@ extern "C" int h2b_far_transfer(const FarTransferArgs *a, cudaStream_t st) {
     h2b_set_error("interpolation order %d > %d", a->m, MMAX);
     return H2B_ERR_ARG;
   }
-  transfer_kernel<<<a->n, 256, 0, st>>>(*a);
+  if (a->k > 128 || a->k != a->m * a->m * a->m) {
+    h2b_set_error("transfer: rank %d is not m^3 <= 128", a->k);
+    return H2B_ERR_ARG;
+  }
+  transfer_kernel<<<a->n, 32u * (((unsigned) a->k + 31u) / 32u), 0, st>>>(*a);
   h2b_note_launch();
   H2B_CUDA_TRY(cudaGetLastError());
   return H2B_OK;
@@ -276,17 +312,15 @@ extern "C" int h2b_far_transfer(const FarTransferArgs *a, cudaStream_t st) {
 
 extern "C" int h2b_far_coupling(const FarCouplingArgs *a, int cx, cudaStream_t st) {
   if (a->n == 0) return H2B_OK;
-#define LAUNCH(CXV, MV) coupling_kernel<CXV, MV><<<a->n, 256, 0, st>>>(*a)
-  if (cx) {
-    if (a->m == 4) LAUNCH(true, 4);
-    else if (a->m == 5) LAUNCH(true, 5);
-    else LAUNCH(true, 0);
-  } else {
-    if (a->m == 4) LAUNCH(false, 4);
-    else if (a->m == 5) LAUNCH(false, 5);
-    else LAUNCH(false, 0);
+  if (a->k > 128 || a->k != a->m * a->m * a->m) {
+    h2b_set_error("coupling: rank %d is not m^3 <= 128", a->k);
+    return H2B_ERR_ARG;
   }
-#undef LAUNCH
+  const unsigned threads = 32u * (((unsigned) a->k + 31u) / 32u);
+  if (cx)
+    coupling_kernel<true><<<a->n, threads, 0, st>>>(*a);
+  else
+    coupling_kernel<false><<<a->n, threads, 0, st>>>(*a);
   h2b_note_launch();
   H2B_CUDA_TRY(cudaGetLastError());
   return H2B_OK;
