@@ -54,14 +54,19 @@ static void devtree_free(DevCTree &t, cudaStream_t st) {
   dfree(t.d_pts, st); dfree(t.d_V, st); dfree(t.d_E, st); dfree(t.d_refs, st);
   dfree(t.d_tr_off, st); dfree(t.d_tr_len, st);
   dfree(t.d_W, st); dfree(t.d_woff, st); dfree(t.d_fitems, st); dfree(t.d_wleaves, st);
+  dfree(t.d_ppairs, st); dfree(t.d_pfirst, st); dfree(t.d_P, st);
   dfree(t.d_seg, st);
 }
 
 // Flattened bases: W_t for the clusters of admissible blocks (`adm`, ids of this tree) and all
-// their descendants (which the products W_f = [W_s E_s] pass through).  Flatten items are
-// grouped by father level, deepest first.  W is allocated with H2B_MV_SLACK bytes at its end.
+// their descendants.  W_t is formed from the leaves below t directly: the rows of leaf l inside
+// W_t are W_l times the product of the transfers on the path from l up to t, and that product is
+// the tensor product of three m x m products of one-dimensional transfers.  One flatten item per
+// (leaf, needed ancestor) pair and slice of at most H2B_FLAT_ROWS of the leaf's rows; the items
+// write disjoint rows, so one launch covers every level.  W is allocated with H2B_MV_SLACK bytes
+// at its end.
 static int devtree_flat_setup(DevCTree &t, const h2b_ctree &c, const std::vector<uint32_t> &adm,
-                              uint32_t k, cudaStream_t st) {
+                              uint32_t m, uint32_t k, cudaStream_t st) {
   std::vector<char> in_adm(c.n, 0), need(c.n, 0);
   for (uint32_t a : adm) in_adm[a] = 1;
   // pre-order: a father precedes its sons
@@ -75,49 +80,48 @@ static int devtree_flat_setup(DevCTree &t, const h2b_ctree &c, const std::vector
       tot += (uint64_t) c.size[i] * k;
     }
   t.wtotal = tot;
-  std::vector<uint32_t> wleaves, fitems;
+  std::vector<uint32_t> wleaves, pairs, pfirst, fitems;
   for (uint32_t i = 0; i < c.n; i++)
     if (need[i] && c.sons[i] == 0) wleaves.push_back(i);
-  t.fitem_start.assign(c.depth + 1, 0);
-  t.fitem_count.assign(c.depth + 1, 0);
-  uint32_t nitems = 0;
-  for (int l = (int) c.depth - 1; l >= 0; l--) {
-    t.fitem_start[l] = nitems;
-    for (uint32_t f = 0; f < c.n; f++) {
-      if (!need[f] || c.level[f] != (uint32_t) l || c.sons[f] == 0) continue;
-      const uint32_t sons[2] = {c.son0[f], c.son1[f]};
-      for (uint32_t q = 0; q < c.sons[f] && q < 2; q++)
-        for (uint32_t r0 = 0; r0 < c.size[sons[q]]; r0 += H2B_FLAT_ROWS) {
-          const uint32_t nr = std::min<uint32_t>(H2B_FLAT_ROWS, c.size[sons[q]] - r0);
-          fitems.insert(fitems.end(), {f, sons[q], r0, nr});
-          nitems++;
-        }
+  for (uint32_t l : wleaves) {
+    pfirst.push_back((uint32_t) (pairs.size() / 2));
+    for (uint32_t f = c.father[l]; f != UINT32_MAX && need[f]; f = c.father[f]) {
+      const uint32_t pid = (uint32_t) (pairs.size() / 2);
+      pairs.insert(pairs.end(), {l, f});
+      for (uint32_t r0 = 0; r0 < c.size[l]; r0 += H2B_FLAT_ROWS)
+        fitems.insert(fitems.end(),
+                      {pid, r0, std::min<uint32_t>(H2B_FLAT_ROWS, c.size[l] - r0), 0u});
     }
-    t.fitem_count[l] = nitems - t.fitem_start[l];
   }
+  pfirst.push_back((uint32_t) (pairs.size() / 2));
   t.nwleaves = (uint32_t) wleaves.size();
+  t.npairs = (uint32_t) (pairs.size() / 2);
+  t.nfitems = (uint32_t) (fitems.size() / 4);
   t.h_woff = woff;
   t.h_adm = in_adm;
   int rc;
   if ((rc = upload(&t.d_woff, woff, st)) || (rc = upload(&t.d_wleaves, wleaves, st)) ||
-      (rc = upload(&t.d_fitems, fitems, st)))
+      (rc = upload(&t.d_fitems, fitems, st)) || (rc = upload(&t.d_ppairs, pairs, st)) ||
+      (rc = upload(&t.d_pfirst, pfirst, st)))
     return rc;
   H2B_CUDA_TRY(cudaMallocAsync(&t.d_W, sizeof(double) * std::max<uint64_t>(tot, 1) + H2B_MV_SLACK,
                                st));
+  H2B_CUDA_TRY(cudaMallocAsync(
+      &t.d_P, sizeof(double) * std::max<uint64_t>((uint64_t) t.npairs * 3 * m * m, 1), st));
   return H2B_OK;
 }
 
-// W^T from V and E: leaves first, then the father levels from the deepest up.  `transposed`: the
-// basis stores V^T and E^T (column side); otherwise V and E (row side).
+// W^T from V: the leaves first, then the paths' transfer products, then the rows of every
+// needed ancestor in one launch.  `transposed`: the basis stores V^T (column side); otherwise V
+// (row side).
 static int devtree_flatten(DevCTree &t, uint32_t m, uint32_t k, int transposed, cudaStream_t st) {
   FlatLeafArgs la{t.d_wleaves, t.d_size, t.d_voff, t.d_woff, t.d_V, t.d_W, t.nwleaves, (int) k,
                   !transposed};
   int rc = h2b_flat_leaves(&la, st);
-  for (int l = (int) t.depth - 1; rc == H2B_OK && l >= 0; l--) {
-    FlatArgs fa{t.d_fitems + 4 * (size_t) t.fitem_start[l], t.d_off, t.d_size, t.d_woff,
-                t.d_pts, t.d_W, t.fitem_count[l], (int) m, (int) k};
-    rc = h2b_flat_level(&fa, st);
-  }
+  FlatArgs fa{t.d_fitems, t.d_ppairs, t.d_pfirst, t.d_wleaves, t.d_off, t.d_size, t.d_woff,
+              t.d_pts, t.d_P, t.d_W, t.nfitems, t.nwleaves, (int) m, (int) k};
+  if (rc == H2B_OK) rc = h2b_flat_paths(&fa, st);
+  if (rc == H2B_OK) rc = h2b_flat_rows(&fa, st);
   return rc;
 }
 
@@ -199,7 +203,7 @@ extern "C" void h2b_h2matrix_del(h2b_h2matrix *h) {
   if (h->shared && h->owner) h->owner->sharers.n--;
   // the operator's own data
   for (DevCTree *t : {&h->rt, &h->ct}) {
-    dfree(t->d_V, st); dfree(t->d_E, st); dfree(t->d_W, st);
+    dfree(t->d_V, st); dfree(t->d_E, st); dfree(t->d_W, st); dfree(t->d_P, st);
     dfree(t->f_W, st);
   }
   dfree(h->f_N, st); dfree(h->f_S, st); dfree(h->d_S, st); dfree(h->d_N, st);
@@ -335,8 +339,8 @@ extern "C" h2b_h2matrix *h2b_h2matrix_new(const h2b_bem *bem, const h2b_tree *tr
   }
   h2b_nearplan_free(&plan);
   // flattened bases over the admissible clusters, and the matvec work items
-  if (rc == H2B_OK) rc = devtree_flat_setup(h->rt, tree->row, arc, h->k, h->st);
-  if (rc == H2B_OK) rc = devtree_flat_setup(h->ct, tree->col, acc, h->k, h->st);
+  if (rc == H2B_OK) rc = devtree_flat_setup(h->rt, tree->row, arc, m, h->k, h->st);
+  if (rc == H2B_OK) rc = devtree_flat_setup(h->ct, tree->col, acc, m, h->k, h->st);
   if (rc == H2B_OK) {
     h->h_arc = arc;
     h->h_acc = acc;
@@ -397,7 +401,7 @@ extern "C" h2b_h2matrix *h2b_h2matrix_new_like(const h2b_bem *bem, const h2b_h2m
   h->f_S = h->f_N = nullptr;
   h->d_S = h->d_N = h->d_xp = h->d_yp = h->d_xt = h->d_yt = h->d_xio = h->d_yio = nullptr;
   h->d_mverr = nullptr;
-  for (DevCTree *t : {&h->rt, &h->ct}) t->d_V = t->d_E = t->d_W = nullptr, t->f_W = nullptr;
+  for (DevCTree *t : {&h->rt, &h->ct}) t->d_V = t->d_E = t->d_W = t->d_P = nullptr, t->f_W = nullptr;
   int rc = H2B_OK;
   if (cudaStreamCreateWithFlags(&h->st, cudaStreamNonBlocking) != cudaSuccess) rc = H2B_ERR_CUDA;
   for (int e = 0; rc == H2B_OK && e < 12; e++)
@@ -411,6 +415,9 @@ extern "C" h2b_h2matrix *h2b_h2matrix_new_like(const h2b_bem *bem, const h2b_h2m
         cudaMallocAsync(&t->d_E, sizeof(double) * std::max<uint64_t>((uint64_t) (t->n - 1) * kk, 1),
                         h->st) ||
         cudaMallocAsync(&t->d_W, sizeof(double) * std::max<uint64_t>(t->wtotal, 1) + H2B_MV_SLACK,
+                        h->st) ||
+        cudaMallocAsync(&t->d_P,
+                        sizeof(double) * std::max<uint64_t>((uint64_t) t->npairs * 3 * h->m * h->m, 1),
                         h->st))
       rc = H2B_ERR_NOMEM;
   }

@@ -27,10 +27,13 @@ struct DevCTree {
   double *d_W = nullptr;
   uint64_t *d_woff = nullptr;
   uint64_t wtotal = 0;
-  uint32_t *d_fitems = nullptr;  // flatten items (4 uint32 each), grouped by father level
+  uint32_t *d_fitems = nullptr;  // flatten items (4 uint32 each: pair, first row, rows, 0)
   uint32_t *d_wleaves = nullptr; // leaves that carry a W (W_leaf = V_leaf)
-  std::vector<uint32_t> fitem_start, fitem_count;  // flatten items of father level l
-  uint32_t nwleaves = 0;
+  // (leaf, ancestor) pairs of the flattened bases: d_ppairs[2 p] = leaf, [2 p + 1] = ancestor;
+  // the pairs of needed leaf i are d_pfirst[i] .. d_pfirst[i + 1] - 1, nearest ancestor first
+  uint32_t *d_ppairs = nullptr, *d_pfirst = nullptr;
+  uint32_t nwleaves = 0, npairs = 0, nfitems = 0;
+  double *d_P = nullptr;  // per pair: the three m x m products of one-dimensional transfers
   std::vector<uint64_t> h_woff;  // host copy of d_woff
   std::vector<char> h_adm;       // 1: the cluster belongs to an admissible block
   std::vector<uint32_t> h_seg;   // host copy of d_seg

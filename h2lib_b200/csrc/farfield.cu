@@ -52,38 +52,40 @@ __device__ __forceinline__ double dlagr_bar(double x, const double *xi, double w
 // [part k / split, ...)), so that the launch has several CTAs per SM.  The CTA's triangle
 // list (TriRef, local row indices) is processed in batches of BATCH triangles: first the
 // one-dimensional Lagrange values (and derivatives) at every quadrature point of the batch are
-// tabulated in shared memory (3 axes x m), then each (triangle, nu) work item forms the tensor
-// products from the table.  The CTA's columns of V (rows x its nu) are accumulated in shared
-// memory (atomics for the linear basis, where a vertex receives the integrals of all triangles
-// around it) and written once.
+// tabulated in shared memory (3 axes x M), then each thread, which owns one nu of the CTA's range
+// for the whole launch (its three one-dimensional indices formed once), takes the batch's
+// triangles in turn and forms the tensor products from the table.  The interpolation order M is
+// a template parameter, so no index arithmetic divides at run time.  The CTA's columns of V
+// (rows x its nu) are accumulated in shared memory (atomics for the linear basis, where a vertex
+// receives the integrals of all triangles around it) and written once.
 constexpr int BATCH = 32;
 constexpr int NSMAX = 64;   // single-triangle rule points (q^2, q <= 8)
 
-template <bool LINEAR, bool DN>
+template <bool LINEAR, bool DN, int M>
 __global__ void __launch_bounds__(256) leaf_basis_kernel(FarLeafArgs a) {
+  constexpr int K = M * M * M;
   extern __shared__ double smem[];
-  __shared__ double wbar[3][MMAX];
+  __shared__ double wbar[3][M];
   const uint32_t split = (uint32_t) a.split;
   const uint32_t leaf = blockIdx.x / split, part = blockIdx.x % split;
   const uint32_t c = a.leaves[leaf];
-  const int m = a.m, k = a.k;
-  const int nu0 = (int) ((part * (uint32_t) k) / split);
-  const int nu1 = (int) (((part + 1) * (uint32_t) k) / split);
+  const int nu0 = (int) ((part * (uint32_t) K) / split);
+  const int nu1 = (int) (((part + 1) * (uint32_t) K) / split);
   const int kp = nu1 - nu0;
   const uint32_t rows = a.size[c];
   const uint32_t tr0 = a.tr_off[leaf], ntr = a.tr_len[leaf];
-  const double *pts = a.pts + (size_t) c * 3 * m;
+  const double *pts = a.pts + (size_t) c * 3 * M;
   const int ns = a.ns;
-  const int kpmax = (k + (int) split - 1) / (int) split;
+  const int kpmax = (K + (int) split - 1) / (int) split;
   double *V = smem;                                   // rows * kp (the CTA's columns)
-  double *tab = V + (size_t) rows * kpmax;            // BATCH * ns * 3 * m
-  double *dtab = tab + (size_t) BATCH * ns * 3 * m;   // same size (derivatives, DN only)
+  double *tab = V + (size_t) rows * kpmax;            // BATCH * ns * 3 * M
+  double *dtab = tab + (size_t) BATCH * ns * 3 * M;   // same size (derivatives, DN only)
   for (uint32_t e = threadIdx.x; e < rows * (uint32_t) kp; e += blockDim.x) V[e] = 0.0;
-  if (threadIdx.x < 3u * (uint32_t) m) {
-    const int d = (int) threadIdx.x / m, mu = (int) threadIdx.x % m;
-    const double *xi = pts + d * m;
+  if (threadIdx.x < 3u * M) {
+    const int d = (int) threadIdx.x / M, mu = (int) threadIdx.x % M;
+    const double *xi = pts + d * M;
     double p = 1.0;
-    for (int l = 0; l < m; l++)
+    for (int l = 0; l < M; l++)
       if (l != mu) p *= xi[mu] - xi[l];
     wbar[d][mu] = 1.0 / p;
   }
@@ -101,6 +103,12 @@ __global__ void __launch_bounds__(256) leaf_basis_kernel(FarLeafArgs a) {
     if (LINEAR)
       for (int l = 0; l < 3; l++) sw[l][q] = a.wsl[l * ns + q];
   }
+  // this thread's column: lnu = threadIdx.x % kp, triangles threadIdx.x / kp + g * tstep
+  const int tstep = (int) blockDim.x / kp;
+  const int lnu = (int) threadIdx.x % kp, tfirst = (int) threadIdx.x / kp;
+  const bool active = tfirst < tstep;  // threads past the last whole group of kp stay idle
+  const int nu = nu0 + lnu;
+  const int jx = nu / (M * M), jy = (nu / M) % M, jz = nu % M;
   for (uint32_t b0 = 0; b0 < ntr; b0 += BATCH) {
     const uint32_t nb = ntr - b0 < (uint32_t) BATCH ? ntr - b0 : (uint32_t) BATCH;
     __syncthreads();
@@ -117,33 +125,30 @@ __global__ void __launch_bounds__(256) leaf_basis_kernel(FarLeafArgs a) {
       tg[e] = T.g;
     }
     __syncthreads();
-    // table: entry ((s * ns + q) * 3 + d) * m + mu
-    for (uint32_t e = threadIdx.x; e < nb * ns * 3 * m; e += blockDim.x) {
-      const int mu = (int) (e % m), d = (int) ((e / m) % 3);
-      const uint32_t sq = e / (3 * m), s = sq / ns, q = sq % ns;
+    // table: entry ((s * ns + q) * 3 + d) * M + mu
+    for (uint32_t e = threadIdx.x; e < nb * ns * 3 * M; e += blockDim.x) {
+      const int mu = (int) (e % M), d = (int) ((e / M) % 3);
+      const uint32_t sq = e / (3 * M), s = sq / ns, q = sq % ns;
       const double tx = sx[q], sy_ = sy[q];
       const double x = tv[s][d] * (1.0 - tx) + tv[s][3 + d] * (tx - sy_) + tv[s][6 + d] * sy_;
-      const double *xi = pts + d * m;
-      tab[e] = lagr_bar(x, xi, wbar[d][mu], mu, m);
-      if (DN) dtab[e] = dlagr_bar(x, xi, wbar[d][mu], mu, m);
+      const double *xi = pts + d * M;
+      tab[e] = lagr_bar(x, xi, wbar[d][mu], mu, M);
+      if (DN) dtab[e] = dlagr_bar(x, xi, wbar[d][mu], mu, M);
     }
     __syncthreads();
-    // work item = (triangle in batch, nu of this CTA)
-    for (uint32_t it = threadIdx.x; it < nb * (uint32_t) kp; it += blockDim.x) {
-      const uint32_t s = it / (uint32_t) kp;
-      const int lnu = (int) (it - s * (uint32_t) kp), nu = nu0 + lnu;
-      const int jx = nu / (m * m), jy = (nu / m) % m, jz = nu % m;
+    if (!active) continue;
+    for (uint32_t s = tfirst; s < nb; s += tstep) {
       double sum[3] = {0.0, 0.0, 0.0};
       for (int q = 0; q < ns; q++) {
-        const double *t3 = tab + ((size_t) s * ns + q) * 3 * m;
-        const double lx = t3[jx], ly = t3[m + jy], lz = t3[2 * m + jz];
+        const double *t3 = tab + ((size_t) s * ns + q) * 3 * M;
+        const double lx = t3[jx], ly = t3[M + jy], lz = t3[2 * M + jz];
         double val;
         if (!DN) {
           val = lx * ly * lz;
         } else {
-          const double *d3 = dtab + ((size_t) s * ns + q) * 3 * m;
-          val = tn[s][0] * (d3[jx] * ly * lz) + tn[s][1] * (lx * d3[m + jy] * lz) +
-                tn[s][2] * (lx * ly * d3[2 * m + jz]);
+          const double *d3 = dtab + ((size_t) s * ns + q) * 3 * M;
+          val = tn[s][0] * (d3[jx] * ly * lz) + tn[s][1] * (lx * d3[M + jy] * lz) +
+                tn[s][2] * (lx * ly * d3[2 * M + jz]);
         }
         if (LINEAR) {
 #pragma unroll
@@ -168,8 +173,8 @@ __global__ void __launch_bounds__(256) leaf_basis_kernel(FarLeafArgs a) {
   if (a.transposed) {
     // V^T, k x rows column-major: consecutive threads write consecutive nu
     for (uint32_t e = threadIdx.x; e < rows * (uint32_t) kp; e += blockDim.x) {
-      const uint32_t lnu = e % (uint32_t) kp, i = e / (uint32_t) kp;
-      out[(size_t) nu0 + lnu + (size_t) i * k] = V[i + lnu * rows];
+      const uint32_t l2 = e % (uint32_t) kp, i = e / (uint32_t) kp;
+      out[(size_t) nu0 + l2 + (size_t) i * K] = V[i + l2 * rows];
     }
   } else {
     double *o = out + (size_t) nu0 * rows;
@@ -266,32 +271,47 @@ __global__ void __launch_bounds__(128) coupling_kernel(FarCouplingArgs a) {
 
 }  // namespace
 
+template <bool L, bool D, int M>
+static int launch_leaf(const FarLeafArgs *a, size_t smem, cudaStream_t st) {
+  H2B_CUDA_TRY((h2b_allow_smem<leaf_basis_kernel<L, D, M>>()));
+  leaf_basis_kernel<L, D, M><<<a->nleaves * (uint32_t) a->split, 256, smem, st>>>(*a);
+  h2b_note_launch();
+  H2B_CUDA_TRY(cudaGetLastError());
+  return H2B_OK;
+}
+
+template <bool L, bool D>
+static int launch_leaf_m(const FarLeafArgs *a, size_t smem, cudaStream_t st) {
+  switch (a->m) {
+    case 1: return launch_leaf<L, D, 1>(a, smem, st);
+    case 2: return launch_leaf<L, D, 2>(a, smem, st);
+    case 3: return launch_leaf<L, D, 3>(a, smem, st);
+    case 4: return launch_leaf<L, D, 4>(a, smem, st);
+    case 5: return launch_leaf<L, D, 5>(a, smem, st);
+    default:
+      h2b_set_error("leaf basis: interpolation order %d outside 1..5", a->m);
+      return H2B_ERR_ARG;
+  }
+}
+
 extern "C" int h2b_far_leaf_basis(const FarLeafArgs *a, int linear, int dn, cudaStream_t st) {
   if (a->nleaves == 0) return H2B_OK;
   if (a->split < 1 || a->split > a->k) {
     h2b_set_error("leaf basis: %d CTAs per leaf outside 1..%d", a->split, a->k);
     return H2B_ERR_ARG;
   }
+  // the derivative table only for the normal-derivative bases
   const size_t smem = sizeof(double) * ((size_t) a->max_rows * ((a->k + a->split - 1) / a->split) +
-                                        2 * (size_t) BATCH * a->ns * 3 * a->m);
-  if (smem > 200u * 1024u || a->ns > NSMAX) {
+                                        (dn ? 2 : 1) * (size_t) BATCH * a->ns * 3 * a->m);
+  if (smem > 200u * 1024u || a->ns > NSMAX || (a->k + a->split - 1) / a->split > 256) {
     h2b_set_error("leaf basis block of %u x %d (rule of %d points) exceeds shared memory",
                   a->max_rows, a->k, a->ns);
     return H2B_ERR_ARG;
   }
-#define LAUNCH(L, D)                                                                        \
-  do {                                                                                      \
-    H2B_CUDA_TRY((h2b_allow_smem<leaf_basis_kernel<L, D>>()));                             \
-    leaf_basis_kernel<L, D><<<a->nleaves * (uint32_t) a->split, 256, smem, st>>>(*a);     \
-    h2b_note_launch();                                                                      \
-  } while (0)
-  if (linear && dn) LAUNCH(true, true);
-  else if (linear) LAUNCH(true, false);
-  else if (dn) LAUNCH(false, true);
-  else LAUNCH(false, false);
-#undef LAUNCH
-  H2B_CUDA_TRY(cudaGetLastError());
-  return H2B_OK;
+  if (linear && dn) return launch_leaf_m<true, true>(a, smem, st);
+  if (linear) return launch_leaf_m<true, false>(a, smem, st);
+  if (dn) return launch_leaf_m<false, true>(a, smem, st);
+  return launch_leaf_m<false, false>(a, smem, st);
 }
 
 extern "C" int h2b_far_transfer(const FarTransferArgs *a, cudaStream_t st) {

@@ -43,15 +43,19 @@ struct FarCouplingArgs {
   double kconst, k_re, k_imn;
 };
 
-// Flattened bases (flatbasis.cu): items of at most H2B_FLAT_ROWS rows of one son.
+// Flattened bases (flatbasis.cu): items of at most H2B_FLAT_ROWS rows of one leaf.
 #define H2B_FLAT_ROWS 32
 struct FlatArgs {
-  const uint32_t *items;     // 4 per item: father, son, first row in the son, rows
+  const uint32_t *items;     // 4 per item: (leaf, ancestor) pair, first row in the leaf, rows, 0
+  const uint32_t *pairs;     // 2 per pair: leaf, ancestor
+  const uint32_t *pfirst;    // per needed leaf: its first pair (nleaves + 1 entries)
+  const uint32_t *leaves;    // needed leaves
   const uint32_t *off, *size;
   const uint64_t *woff;      // per cluster: offset of W_t (doubles); W^T is k x |t| (ld k)
   const double *pts;         // per cluster: the m one-dimensional nodes per axis (3 m doubles)
+  double *P;                 // per pair: 3 m x m transfer products (written by h2b_flat_paths)
   double *W;
-  uint32_t nitems;
+  uint32_t nitems, nleaves;
   int m, k;
 };
 
@@ -68,7 +72,8 @@ struct FlatLeafArgs {
 extern "C" int h2b_flat_leaves(const FlatLeafArgs *a, cudaStream_t st);
 extern "C" int h2b_to_single(const double *in, float *out, size_t n, int num_sms,
                              cudaStream_t st);
-extern "C" int h2b_flat_level(const FlatArgs *a, cudaStream_t st);
+extern "C" int h2b_flat_paths(const FlatArgs *a, cudaStream_t st);
+extern "C" int h2b_flat_rows(const FlatArgs *a, cudaStream_t st);
 
 extern "C" int h2b_far_leaf_basis(const FarLeafArgs *a, int linear, int dn, cudaStream_t st);
 extern "C" int h2b_far_transfer(const FarTransferArgs *a, cudaStream_t st);

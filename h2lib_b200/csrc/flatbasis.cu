@@ -4,7 +4,11 @@
 // on t's indices: W_leaf = V_leaf and, for a father f with sons s,
 //   W_f restricted to the rows of s = W_s E_s
 // (the recursion of the reference's forward/backward transforms, Library/clusterbasis.c:524/749,
-// multiplied out once after assembly).  With W the forward transform is xt_t = W_t^T x_t and the
+// multiplied out once after assembly), i.e. the rows of a leaf l inside W_f are
+// W_l E_l E_{father(l)} ... up to f.  Every E is a tensor product of three one-dimensional
+// transfers, so the path's product is too: it is formed per (leaf, ancestor) pair as three m x m
+// matrices, and all ancestors' rows are then written in one launch, with no level-to-level
+// dependence.  With W the forward transform is xt_t = W_t^T x_t and the
 // backward transform y_t += W_t yt_t for all clusters at once: no level-to-level dependence, so
 // the matvec streams W at HBM bandwidth instead of climbing the tree one level per step.
 // Both sides store W transposed (W^T: k x |t|, column-major, ld = k), so that a slice of rows of
@@ -41,16 +45,51 @@ __device__ __forceinline__ void cta_copy(double *dst, size_t n, F src) {
   }
 }
 
-// CTA per item = (father f, son s, first row r0 of s, rows nr <= H2B_FLAT_ROWS): the nr rows of
-// W_s times E_s land in the rows of s inside W_f.  E_s is the tensor product of three m x m
-// one-dimensional transfers, E_s[(a, b, c), (jx, jy, jz)] = Lx[a][jx] Ly[b][jy] Lz[c][jz] with
-// L_d[a][mu] = father polynomial mu of axis d at son node a (the factors of transfer_kernel), so
-// each row, an m x m x m tensor w[a][b][c], is multiplied one axis at a time:
-//   t1[a][b][jz] = sum_c w[a][b][c] Lz[c][jz],  t2[a][jy][jz] = sum_b t1[a][b][jz] Ly[b][jy],
-//   W_f[jx][jy][jz] = sum_a t2[a][jy][jz] Lx[a][jx]
-// -- 3 m^4 multiply-adds per row instead of the k^2 = m^6 of the full product (the same sum,
-// bracketed by axis).  The rows are staged in shared memory in chunks of RB; a thread takes one
-// fibre of m inputs and writes its m outputs, so every input is read once per step.
+// Transfer products of the (leaf, ancestor) pairs: CTA per needed leaf l, walking up its
+// ancestors f_1 = father(l), f_2, ... (the pairs of l, nearest first).  For every axis d,
+//   P_1 = L_d(l -> f_1),  P_q = P_{q-1} L_d(f_{q-1} -> f_q),
+// with L_d(c -> f)[a][mu] = polynomial mu of f's nodes at c's node a (the one-dimensional factor
+// of the transfer E_c); E_l E_{f_1} ... E_{f_{q-1}} is then the tensor product of the three P_q.
+template <int M>
+__global__ void __launch_bounds__(128) flatten_paths_kernel(FlatArgs a) {
+  constexpr int MM = M * M;
+  __shared__ double P[3][M][M], L[3][M][M];
+  const uint32_t p0 = a.pfirst[blockIdx.x], p1 = a.pfirst[blockIdx.x + 1];
+  uint32_t node = a.leaves[blockIdx.x];
+  const int e = (int) threadIdx.x, d = e / MM, pa = (e / M) % M, mu = e % M;
+  for (uint32_t p = p0; p < p1; p++) {
+    const uint32_t f = a.pairs[2 * (size_t) p + 1];
+    if (e < 3 * MM)
+      L[d][pa][mu] = lagrange_1d(a.pts[(size_t) node * 3 * M + d * M + pa],
+                                 a.pts + (size_t) f * 3 * M + d * M, mu, M);
+    __syncthreads();
+    double v = 0.0;
+    if (e < 3 * MM) {
+      if (p == p0) {
+        v = L[d][pa][mu];
+      } else {
+#pragma unroll
+        for (int b = 0; b < M; b++) v = fma(P[d][pa][b], L[d][b][mu], v);
+      }
+    }
+    __syncthreads();  // P and L are read
+    if (e < 3 * MM) {
+      P[d][pa][mu] = v;
+      a.P[(size_t) p * 3 * MM + e] = v;
+    }
+    node = f;
+  }
+}
+
+// CTA per item = ((leaf l, ancestor f) pair, first row r0 of l, rows nr <= H2B_FLAT_ROWS): the nr
+// rows of W_l times the pair's transfer product land in the rows of l inside W_f.  The product is
+// the tensor product of the three m x m factors P_d, so each row, an m x m x m tensor w[a][b][c],
+// is multiplied one axis at a time:
+//   t1[a][b][jz] = sum_c w[a][b][c] Pz[c][jz],  t2[a][jy][jz] = sum_b t1[a][b][jz] Py[b][jy],
+//   W_f[jx][jy][jz] = sum_a t2[a][jy][jz] Px[a][jx]
+// -- 3 m^4 multiply-adds per row instead of the k^2 = m^6 of the full product.  The rows are
+// staged in shared memory in chunks of RB; a thread takes one fibre of m inputs and writes its m
+// outputs, so every input is read once per step.
 template <int M>
 struct FlatShape {
   static constexpr int K = M * M * M;
@@ -61,25 +100,23 @@ struct FlatShape {
 };
 
 template <int M>
-__global__ void __launch_bounds__(FLAT_TPB) flatten_kernel(FlatArgs a) {
+__global__ void __launch_bounds__(FLAT_TPB) flatten_rows_kernel(FlatArgs a) {
   constexpr int K = FlatShape<M>::K, RB = FlatShape<M>::RB, MM = M * M;
   extern __shared__ double sm[];
-  __shared__ double L[3][M][M];  // L[d][son node][father polynomial]
+  __shared__ double L[3][M][M];  // the pair's three transfer products
   const uint32_t *it = a.items + 4 * (size_t) blockIdx.x;
-  const uint32_t f = it[0], s = it[1], r0 = it[2], nr = it[3];
-  const double *fp = a.pts + (size_t) f * 3 * M, *sp = a.pts + (size_t) s * 3 * M;
-  for (int e = (int) threadIdx.x; e < 3 * MM; e += (int) blockDim.x) {
-    const int d = e / MM, p = (e / M) % M, mu = e % M;
-    L[d][p][mu] = lagrange_1d(sp[d * M + p], fp + d * M, mu, M);
-  }
+  const uint32_t pid = it[0], r0 = it[1], nr = it[2];
+  const uint32_t l = a.pairs[2 * (size_t) pid], f = a.pairs[2 * (size_t) pid + 1];
+  for (int e = (int) threadIdx.x; e < 3 * MM; e += (int) blockDim.x)
+    (&L[0][0][0])[e] = a.P[(size_t) pid * 3 * MM + e];
   double *A = sm, *B = sm + (size_t) RB * K;
-  const uint32_t rf = a.off[s] - a.off[f] + r0;  // first row inside f
-  const double *Ws = a.W + a.woff[s] + (size_t) r0 * K;
+  const uint32_t rf = a.off[l] - a.off[f] + r0;  // first row inside f
+  const double *Ws = a.W + a.woff[l] + (size_t) r0 * K;
   double *Wf = a.W + a.woff[f] + (size_t) rf * K;
   for (uint32_t c0 = 0; c0 < nr; c0 += RB) {
     const uint32_t nc = min((uint32_t) RB, nr - c0);
     __syncthreads();  // L is ready; the previous chunk's last step has read A
-    // W_s^T rows are contiguous (ld K)
+    // W_l^T rows are contiguous (ld K)
     for (uint32_t e = threadIdx.x; e < nc * K; e += blockDim.x) A[e] = Ws[(size_t) c0 * K + e];
     __syncthreads();
     // z: fibre g = (row, a, b) of A -> B[row][a][b][jz]
@@ -178,32 +215,41 @@ extern "C" int h2b_flat_leaves(const FlatLeafArgs *a, cudaStream_t st) {
 }
 
 template <int M>
-static int launch_flatten(const FlatArgs *a, cudaStream_t st) {
-  constexpr size_t smem = sizeof(double) * 2 * FlatShape<M>::RB * FlatShape<M>::K;
-  H2B_CUDA_TRY(h2b_allow_smem<flatten_kernel<M>>());
-  flatten_kernel<M><<<a->nitems, FLAT_TPB, smem, st>>>(*a);
+static int launch_flatten(const FlatArgs *a, int rows, cudaStream_t st) {
+  if (!rows) {
+    flatten_paths_kernel<M><<<a->nleaves, 128, 0, st>>>(*a);
+  } else {
+    constexpr size_t smem = sizeof(double) * 2 * FlatShape<M>::RB * FlatShape<M>::K;
+    H2B_CUDA_TRY(h2b_allow_smem<flatten_rows_kernel<M>>());
+    flatten_rows_kernel<M><<<a->nitems, FLAT_TPB, smem, st>>>(*a);
+  }
   h2b_note_launch();
   H2B_CUDA_TRY(cudaGetLastError());
   return H2B_OK;
 }
 
-extern "C" int h2b_flat_level(const FlatArgs *a, cudaStream_t st) {
-  if (a->nitems == 0) return H2B_OK;
+static int flatten_dispatch(const FlatArgs *a, int rows, cudaStream_t st) {
+  if ((rows ? a->nitems : a->nleaves) == 0) return H2B_OK;
   if (a->k != a->m * a->m * a->m) {
     h2b_set_error("flattened bases: rank %d is not m^3 for m = %d", a->k, a->m);
     return H2B_ERR_ARG;
   }
   switch (a->m) {
-    case 1: return launch_flatten<1>(a, st);
-    case 2: return launch_flatten<2>(a, st);
-    case 3: return launch_flatten<3>(a, st);
-    case 4: return launch_flatten<4>(a, st);
-    case 5: return launch_flatten<5>(a, st);
-    case 6: return launch_flatten<6>(a, st);
-    case 7: return launch_flatten<7>(a, st);
-    case 8: return launch_flatten<8>(a, st);
+    case 1: return launch_flatten<1>(a, rows, st);
+    case 2: return launch_flatten<2>(a, rows, st);
+    case 3: return launch_flatten<3>(a, rows, st);
+    case 4: return launch_flatten<4>(a, rows, st);
+    case 5: return launch_flatten<5>(a, rows, st);
     default:
-      h2b_set_error("flattened bases: interpolation order %d outside 1..8", a->m);
+      h2b_set_error("flattened bases: interpolation order %d outside 1..5", a->m);
       return H2B_ERR_ARG;
   }
+}
+
+extern "C" int h2b_flat_paths(const FlatArgs *a, cudaStream_t st) {
+  return flatten_dispatch(a, 0, st);
+}
+
+extern "C" int h2b_flat_rows(const FlatArgs *a, cudaStream_t st) {
+  return flatten_dispatch(a, 1, st);
 }
