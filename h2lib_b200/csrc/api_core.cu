@@ -175,6 +175,12 @@ extern "C" h2b_surface *h2b_surface_new(uint32_t vertices, const double *x, uint
                       s->stream) != cudaSuccess ||
       cudaMemcpyAsync(s->d_x, x, sizeof(double) * 3ull * vertices, cudaMemcpyHostToDevice,
                       s->stream) != cudaSuccess ||
+      cudaMallocAsync(&s->d_vt_off, sizeof(uint32_t) * (vertices + 1ull), s->stream) != cudaSuccess ||
+      cudaMallocAsync(&s->d_vt_tri, sizeof(uint32_t) * 3ull * triangles, s->stream) != cudaSuccess ||
+      cudaMemcpyAsync(s->d_vt_off, s->adj.off, sizeof(uint32_t) * (vertices + 1ull),
+                      cudaMemcpyHostToDevice, s->stream) != cudaSuccess ||
+      cudaMemcpyAsync(s->d_vt_tri, s->adj.tri, sizeof(uint32_t) * 3ull * triangles,
+                      cudaMemcpyHostToDevice, s->stream) != cudaSuccess ||
       cudaStreamSynchronize(s->stream) != cudaSuccess) {
     h2b_set_error("h2b_surface_new: %s", cudaGetErrorString(cudaGetLastError()));
     h2b_surface_del(s);
@@ -191,6 +197,8 @@ extern "C" void h2b_surface_del(h2b_surface *s) {
   // frees do not synchronise the device (other handles keep running)
   if (s->d_tri) cudaFreeAsync(s->d_tri, s->stream);
   if (s->d_x) cudaFreeAsync(s->d_x, s->stream);
+  if (s->d_vt_off) cudaFreeAsync(s->d_vt_off, s->stream);
+  if (s->d_vt_tri) cudaFreeAsync(s->d_vt_tri, s->stream);
   if (s->stream) cudaStreamDestroy(s->stream);
   h2b_adjacency_free(&s->adj);
   delete s;
@@ -403,7 +411,7 @@ int h2b_devplan_upload(const h2b_nearplan *p, cudaStream_t st, h2b_devplan *dp) 
   return H2B_OK;
 }
 
-int h2b_classify_device(const void *d_tri, const void *refs, const h2b_tile *tiles,
+int h2b_classify_device(const h2b_surface *s, const void *refs, const h2b_tile *tiles,
                         uint32_t ntiles, cudaStream_t st, h2b_sing **d_sing, uint32_t cnt[4]) {
   *d_sing = nullptr;
   for (int c = 0; c < 4; c++) cnt[c] = 0;
@@ -412,7 +420,9 @@ int h2b_classify_device(const void *d_tri, const void *refs, const h2b_tile *til
   int rc = H2B_OK;
   uint32_t host[8] = {0, 0, 0, 0, 0, 0, 0, 0};
   if (cudaMemsetAsync(d_cur, 0, sizeof(uint32_t) * 8, st) != cudaSuccess) rc = H2B_ERR_CUDA;
-  if (rc == H2B_OK) rc = h2b_near_classify(d_tri, refs, tiles, ntiles, d_cur, nullptr, nullptr, st);
+  if (rc == H2B_OK)
+    rc = h2b_near_classify(s->d_tri, refs, tiles, ntiles, s->d_vt_off, s->d_vt_tri, d_cur, nullptr,
+                           nullptr, st);
   if (rc == H2B_OK &&
       (cudaMemcpyAsync(host, d_cur, sizeof(uint32_t) * 4, cudaMemcpyDeviceToHost, st) !=
            cudaSuccess ||
@@ -439,7 +449,8 @@ int h2b_classify_device(const void *d_tri, const void *refs, const h2b_tile *til
       rc = H2B_ERR_CUDA;
   }
   if (rc == H2B_OK && nsing)
-    rc = h2b_near_classify(d_tri, refs, tiles, ntiles, d_cur, d_cur + 4, *d_sing, st);
+    rc = h2b_near_classify(s->d_tri, refs, tiles, ntiles, s->d_vt_off, s->d_vt_tri, d_cur,
+                           d_cur + 4, *d_sing, st);
   if (rc == H2B_OK && cudaStreamSynchronize(st) != cudaSuccess) rc = H2B_ERR_CUDA;
   if (rc == H2B_ERR_CUDA)
     h2b_set_error("singular-pair classification: %s", cudaGetErrorString(cudaGetLastError()));
@@ -557,7 +568,7 @@ extern "C" int h2b_bem_nearfield(const h2b_bem *bem, const uint32_t *ridx, uint3
   }
   {
     uint32_t cnt[4];
-    rc = h2b_classify_device(s->d_tri, dp.refs, dp.tiles, dp.ntiles, st, &dp.sing, cnt);
+    rc = h2b_classify_device(s, dp.refs, dp.tiles, dp.ntiles, st, &dp.sing, cnt);
     if (rc != H2B_OK) {
       h2b_devplan_free(&dp, st);
       return rc;

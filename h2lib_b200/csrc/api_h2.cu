@@ -234,7 +234,7 @@ extern "C" void h2b_h2matrix_del(h2b_h2matrix *h) {
 // Singular pairs of the uploaded tiles (found on the device) and the pair counts per case.
 static int classify_singular(h2b_h2matrix *h, uint64_t all_pairs) {
   uint32_t cnt[4] = {0, 0, 0, 0};
-  const int rc = h2b_classify_device(h->bem->s->d_tri, h->d_refs, h->d_tiles, h->ntiles, h->st,
+  const int rc = h2b_classify_device(h->bem->s, h->d_refs, h->d_tiles, h->ntiles, h->st,
                                      &h->d_sing, cnt);
   if (rc != H2B_OK) return rc;
   const uint64_t nsing = (uint64_t) cnt[1] + cnt[2] + cnt[3];

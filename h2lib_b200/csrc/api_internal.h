@@ -21,6 +21,7 @@ struct h2b_surface {
   h2b_adjacency adj{};
   TriRec *d_tri = nullptr;      // nt records
   double *d_x = nullptr;        // 3*nv
+  uint32_t *d_vt_off = nullptr, *d_vt_tri = nullptr;  // vertex -> triangles (CSR, from adj)
 };
 
 struct h2b_bem {
@@ -61,6 +62,6 @@ void h2b_devplan_free(h2b_devplan *dp, cudaStream_t st);
 // by Sauter-Schwab case: vertex, edge, identical; order inside a case not fixed).  *d_sing: a
 // stream-ordered device array of cnt[1] + cnt[2] + cnt[3] pairs (nullptr when there are none);
 // cnt[c]: pairs of case c = 1..3.  Synchronises st.
-int h2b_classify_device(const void *d_tri, const void *refs, const h2b_tile *tiles,
+int h2b_classify_device(const h2b_surface *s, const void *refs, const h2b_tile *tiles,
                         uint32_t ntiles, cudaStream_t st, h2b_sing **d_sing, uint32_t cnt[4]);
 int h2b_check_err_flag(const h2b_bem *b, cudaStream_t st);

@@ -125,15 +125,30 @@ __global__ void __launch_bounds__(256) leaf_basis_kernel(FarLeafArgs a) {
       tg[e] = T.g;
     }
     __syncthreads();
-    // table: entry ((s * ns + q) * 3 + d) * M + mu
-    for (uint32_t e = threadIdx.x; e < nb * ns * 3 * M; e += blockDim.x) {
-      const int mu = (int) (e % M), d = (int) ((e / M) % 3);
-      const uint32_t sq = e / (3 * M), s = sq / ns, q = sq % ns;
-      const double tx = sx[q], sy_ = sy[q];
-      const double x = tv[s][d] * (1.0 - tx) + tv[s][3 + d] * (tx - sy_) + tv[s][6 + d] * sy_;
+    // table: entry ((s * ns + q) * 3 + d) * M + mu; a thread keeps one (d, mu) and steps through
+    // the (s, q) points with the rule's point count as a running remainder (no division by ns)
+    if (threadIdx.x < (blockDim.x / (3 * M)) * (3 * M)) {
+      const int dm = (int) threadIdx.x % (3 * M), d = dm / M, mu = dm % M;
+      const uint32_t step = blockDim.x / (3 * M);
       const double *xi = pts + d * M;
-      tab[e] = lagr_bar(x, xi, wbar[d][mu], mu, M);
-      if (DN) dtab[e] = dlagr_bar(x, xi, wbar[d][mu], mu, M);
+      const double wb = wbar[d][mu];
+      uint32_t sq = threadIdx.x / (3 * M), s = 0, q = sq;
+      while (q >= (uint32_t) ns) {
+        q -= ns;
+        s++;
+      }
+      for (; sq < nb * ns; sq += step) {
+        const double tx = sx[q], sy_ = sy[q];
+        const double x = tv[s][d] * (1.0 - tx) + tv[s][3 + d] * (tx - sy_) + tv[s][6 + d] * sy_;
+        const size_t e = (size_t) sq * 3 * M + dm;
+        tab[e] = lagr_bar(x, xi, wb, mu, M);
+        if (DN) dtab[e] = dlagr_bar(x, xi, wb, mu, M);
+        q += step;
+        while (q >= (uint32_t) ns) {
+          q -= ns;
+          s++;
+        }
+      }
     }
     __syncthreads();
     if (!active) continue;

@@ -1006,17 +1006,15 @@ __device__ uint32_t pair_code_dev(const uint32_t tv[3], const uint32_t sv[3]) {
          (sp[2] << 12);
 }
 
-// One CTA per tile, a thread per triangle pair; warp-aggregated atomics per case.
-// The tile's vertex ids are staged in shared memory in chunks of CL_CHUNK triangles per side (a
-// warp then reads consecutive words, or one broadcast word, instead of one triangle record per
-// lane).
+// Every pair of one tile tested for a shared vertex (the fallback of classify_kernel for long
+// column lists); warp-aggregated atomics per case.  The tile's vertex ids are staged in shared
+// memory in chunks of CL_CHUNK triangles per side (a warp then reads consecutive words, or one
+// broadcast word, instead of one triangle record per lane).
 constexpr int CL_CHUNK = 256;
 template <bool WRITE>
-__global__ void __launch_bounds__(256) classify_kernel(const TriRec *tri, const TriRef *refs,
-                                                       const h2b_tile *tiles, uint32_t *cursor,
-                                                       const uint32_t *base, h2b_sing *out) {
+__device__ void classify_all_pairs(const TriRec *tri, const TriRef *refs, const h2b_tile &tl,
+                                   uint32_t *cursor, const uint32_t *base, h2b_sing *out) {
   __shared__ uint32_t rv[3][CL_CHUNK], cv[3][CL_CHUNK];
-  const h2b_tile tl = tiles[blockIdx.x];
   const uint32_t ntr = tl.tr_len, nsc = tl.sc_len;
   const uint32_t lane = threadIdx.x & 31;
   for (uint32_t c0 = 0; c0 < nsc; c0 += CL_CHUNK) {
@@ -1131,18 +1129,97 @@ __global__ void __launch_bounds__(256) unique_pairs_kernel(const TriRec *tri, co
   if (threadIdx.x < 4 && cnt[threadIdx.x]) atomicAdd(&counts[threadIdx.x], cnt[threadIdx.x]);
 }
 
+
+// One CTA per tile.  The tile's column triangles go into a shared-memory hash table (triangle id
+// -> position in the column list); a thread per row triangle t visits the triangles around t's
+// vertices (the surface's vertex -> triangle lists) and looks each one up, so the pairs found are
+// exactly the tile's pairs that share a vertex, without testing the others.  A triangle around
+// several vertices of t is taken at the first of them.  Counts per case are gathered in shared
+// memory: the count pass adds them to cursor[c]; the write pass reserves the tile's range of
+// case c with one atomic and writes its pairs there.  Column lists longer than half the table
+// take classify_all_pairs.
+constexpr int CL_HASH = 1024;  // slots, a power of two
+__device__ __forceinline__ uint32_t cl_slot(uint32_t t) { return (t * 2654435761u) >> 22; }
+
+template <bool WRITE>
+__global__ void __launch_bounds__(256) classify_kernel(const TriRec *tri, const TriRef *refs,
+                                                       const h2b_tile *tiles,
+                                                       const uint32_t *vt_off,
+                                                       const uint32_t *vt_tri, uint32_t *cursor,
+                                                       const uint32_t *base, h2b_sing *out) {
+  __shared__ uint32_t hkey[CL_HASH];
+  __shared__ uint32_t hval[CL_HASH];
+  __shared__ uint32_t cnt[4], cur[4], rsv[4];
+  const h2b_tile tl = tiles[blockIdx.x];
+  const uint32_t ntr = tl.tr_len, nsc = tl.sc_len;
+  if (nsc > (uint32_t) CL_HASH / 2) {
+    classify_all_pairs<WRITE>(tri, refs, tl, cursor, base, out);
+    return;
+  }
+  for (uint32_t e = threadIdx.x; e < (uint32_t) CL_HASH; e += blockDim.x) hkey[e] = UINT32_MAX;
+  if (threadIdx.x < 4) cnt[threadIdx.x] = cur[threadIdx.x] = 0;
+  __syncthreads();
+  for (uint32_t e = threadIdx.x; e < nsc; e += blockDim.x) {
+    const uint32_t t = refs[tl.sc_off + e].t;
+    uint32_t h = cl_slot(t);
+    while (atomicCAS(&hkey[h], UINT32_MAX, t) != UINT32_MAX) h = (h + 1) & (CL_HASH - 1);
+    hval[h] = e;
+  }
+  __syncthreads();
+  // pass 0 counts the tile's pairs per case; pass 1 (write pass only) writes them
+  for (int pass = 0; pass < (WRITE ? 2 : 1); pass++) {
+    for (uint32_t i = threadIdx.x; i < ntr; i += blockDim.x) {
+      const uint32_t t = refs[tl.tr_off + i].t;
+      const uint32_t tv[3] = {tri[t].v[0], tri[t].v[1], tri[t].v[2]};
+#pragma unroll
+      for (int k = 0; k < 3; k++) {
+        for (uint32_t a = vt_off[tv[k]]; a < vt_off[tv[k] + 1]; a++) {
+          const uint32_t s = vt_tri[a];
+          const uint32_t sv[3] = {tri[s].v[0], tri[s].v[1], tri[s].v[2]};
+          bool seen = false;
+#pragma unroll
+          for (int k2 = 0; k2 < k; k2++) seen |= sv[0] == tv[k2] || sv[1] == tv[k2] || sv[2] == tv[k2];
+          if (seen) continue;
+          uint32_t h = cl_slot(s);
+          while (hkey[h] != s && hkey[h] != UINT32_MAX) h = (h + 1) & (CL_HASH - 1);
+          if (hkey[h] != s) continue;
+          const uint32_t code = pair_code_dev(tv, sv), c = code & 3u;
+          if (pass == 0) {
+            atomicAdd(&cnt[c], 1u);
+          } else {
+            h2b_sing sg;
+            sg.tile = blockIdx.x;
+            sg.tr = tl.tr_off + i;
+            sg.sc = tl.sc_off + hval[h];
+            sg.code = code;
+            out[base[c] + rsv[c] + atomicAdd(&cur[c], 1u)] = sg;
+          }
+        }
+      }
+    }
+    __syncthreads();
+    if (pass == 0 && threadIdx.x >= 1 && threadIdx.x <= 3 && cnt[threadIdx.x]) {
+      const uint32_t b = atomicAdd(&cursor[threadIdx.x], cnt[threadIdx.x]);
+      if (WRITE) rsv[threadIdx.x] = b;
+    }
+    __syncthreads();
+  }
+}
+
 }  // namespace
 
 extern "C" int h2b_near_classify(const void *tri, const void *refs, const h2b_tile *tiles,
-                                 uint32_t ntiles, uint32_t *cursor, const uint32_t *base,
-                                 h2b_sing *sing, cudaStream_t st) {
+                                 uint32_t ntiles, const uint32_t *vt_off, const uint32_t *vt_tri,
+                                 uint32_t *cursor, const uint32_t *base, h2b_sing *sing,
+                                 cudaStream_t st) {
   if (ntiles == 0) return H2B_OK;
   if (sing)
     classify_kernel<true><<<ntiles, 256, 0, st>>>((const TriRec *) tri, (const TriRef *) refs,
-                                                  tiles, cursor, base, sing);
+                                                  tiles, vt_off, vt_tri, cursor, base, sing);
   else
     classify_kernel<false><<<ntiles, 256, 0, st>>>((const TriRec *) tri, (const TriRef *) refs,
-                                                   tiles, cursor, nullptr, nullptr);
+                                                   tiles, vt_off, vt_tri, cursor, nullptr,
+                                                   nullptr);
   h2b_note_launch();
   H2B_CUDA_TRY(cudaGetLastError());
   return H2B_OK;

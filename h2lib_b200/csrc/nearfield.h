@@ -47,11 +47,13 @@ typedef struct {
 
 int h2b_near_upload_dist_rules(void);
 /* Singular pairs of a tile list on the device (the pairs that share a vertex, with the vertex
- * permutation code of h2b_pair_code).  sing == NULL: add the number of pairs of each case c to
- * cursor[c] (c = 1 vertex, 2 edge, 3 identical).  Otherwise write the pairs of case c to
- * sing[base[c] + cursor[c]++] (cursor zeroed by the caller); the order inside a case is not fixed. */
+ * permutation code of h2b_pair_code).  vt_off / vt_tri: the surface's vertex -> triangle lists
+ * (CSR).  sing == NULL: add the number of pairs of each case c to cursor[c] (c = 1 vertex,
+ * 2 edge, 3 identical).  Otherwise write the pairs of case c to sing[base[c] + cursor[c]++]
+ * (cursor zeroed by the caller); the order inside a case is not fixed. */
 int h2b_near_classify(const void *tri, const void *refs, const h2b_tile *tiles, uint32_t ntiles,
-                      uint32_t *cursor, const uint32_t *base, h2b_sing *sing, cudaStream_t st);
+                      const uint32_t *vt_off, const uint32_t *vt_tri, uint32_t *cursor,
+                      const uint32_t *base, h2b_sing *sing, cudaStream_t st);
 int h2b_near_launch_kernels(const h2b_near_launch *L, cudaStream_t st);
 /* Distinct triangle pairs of a tile list, by vertices shared (counts[0] distant, [1] common
  * vertex, [2] common edge, [3] identical), from a bitmap of nt^2 bits in device memory (freed
