@@ -35,14 +35,15 @@ Z = (1.2, 1.2, 1.2)
 # linear-basis single layer 64, double layer 72
 FLOPS_PER_POINT = {"slp": 64, "dlp": 72}
 # flops the tensor-factored distant-pair sum executes per triangle pair for SLP+DLP, linear basis,
-# q = 2 (FMA = 2): 16 point pairs x 37 (difference 3, r^2 5, rsqrt 13, normal part 4, three
-# column weights per channel 12) + 4 row points x 53 (x_a 12, <x_a, n> 5, 3 x 3 x 2 outer FMAs
-# 36) + 4 column points x 17 (y_b 12, <y_b, n> 5) + 20 for the scaling
-EXECUTED_FLOPS_PER_PAIR = 16 * 37 + 4 * 53 + 4 * 17 + 20
+# q = 2 (FMA = 2), from the staged quadrature points: 16 point pairs x 37 (difference 3, r^2 5,
+# rsqrt 13, normal part 4, three column weights per channel 12) + 4 row points x 41 (<x_a, n> 5,
+# 3 x 3 x 2 outer FMAs 36) + 20 for the scaling.  The points themselves and their normal
+# components are formed once per staged triangle (about 1 flop per pair, not counted).
+EXECUTED_FLOPS_PER_PAIR = 16 * 37 + 4 * 41 + 20
 # the same for the constant-basis single layer (dense cc SLP leg): 16 point pairs x 23
-# (difference 3, r^2 5, rsqrt 13, weighted sum 2) + 4 row points x 14 (x_a 12, outer sum 2) +
-# 4 column points x 9 (y_b) + 5 (pair offset 3, scaling 2); the reference counts 46 per point
-CC_SLP_FLOPS_PER_PAIR = 16 * 23 + 4 * 14 + 4 * 9 + 5
+# (difference 3, r^2 5, rsqrt 13, weighted sum 2) + 4 row points x 2 (outer sum) + 2 (scaling);
+# the reference counts 46 per point
+CC_SLP_FLOPS_PER_PAIR = 16 * 23 + 4 * 2 + 2
 CC_SLP_REF_FLOPS_PER_POINT = 46
 # reference count per point of the Helmholtz kernels, constant basis (sin, cos and exp counted
 # as 1): single layer 54, double layer 66

@@ -25,6 +25,8 @@
 #include <stdint.h>
 #include <string.h>
 
+#include <type_traits>
+
 #include "device_common.cuh"
 #include "h2b200_plan.h"
 #include "nearfield.h"
@@ -491,6 +493,102 @@ struct DistStage {
   uint32_t rv[3][DIST_CHUNK], cv[3][DIST_CHUNK];  // vertex ids
   int32_t rl[3][DIST_CHUNK], cl[3][DIST_CHUNK];   // local output row / column per vertex
 };
+
+// Staged triangles of the q = 2 FP64 kernels: the four points of the one-triangle rule are formed
+// once per triangle here (the tensor rule's points are their pairs), with each point's component
+// along the triangle's own normal, so a pair only forms the differences.
+constexpr int PT_X = 0, PT_G = 12, PT_N = 13, PT_DN = 16, PT_ROWS = 20;
+struct DistStagePts {
+  double r[PT_ROWS][DIST_CHUNK];  // row triangles: x_a (3 a + d), Gram determinant, n, <x_a, n>
+  double c[PT_ROWS][DIST_CHUNK];  // column triangles: y_b, Gram determinant * kconst, n, <y_b, n>
+  uint32_t rv[3][DIST_CHUNK], cv[3][DIST_CHUNK];  // vertex ids
+  int32_t rl[3][DIST_CHUNK], cl[3][DIST_CHUNK];   // local output row / column per vertex
+};
+
+// Point e < 4 of the q = 2 one-triangle rule on (A, B, C): A + s0 (B - A) + s1 (C - B), and its
+// component along n, into rows PT_X.., PT_DN.. of a stage array; the triangle's Gram determinant
+// (times gscale) and normal into PT_G, PT_N..
+__device__ __forceinline__ void stage_points(double (&st)[PT_ROWS][DIST_CHUNK], uint32_t e,
+                                             const TriRec &T, double gscale) {
+  const double(&sd)[6][SIDE_MAXP] = c_side[1];
+#pragma unroll
+  for (int a = 0; a < 4; a++) {
+    double x[3];
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+      x[d] = fma(sd[1][a], T.c[d] - T.b[d], fma(sd[0][a], T.b[d] - T.a[d], T.a[d]));
+      st[PT_X + 3 * a + d][e] = x[d];
+    }
+    st[PT_DN + a][e] = fma(x[0], T.n[0], fma(x[1], T.n[1], x[2] * T.n[2]));
+  }
+#pragma unroll
+  for (int d = 0; d < 3; d++) st[PT_N + d][e] = T.n[d];
+  st[PT_G][e] = T.g * gscale;
+}
+
+// One distant pair with the q = 2 tensor rule from staged points, summed column side first:
+//   acc[c][i][j] = sum_a w_a phi_i(x_a) sum_b w_b phi_j(y_b) k_c(x_a, y_b).
+// The normal component of x_a - y_b takes the staged component on the normal's own triangle
+// and forms the other one here.  Same sum as dist_pair_tensor, from absolute points.
+template <int KK, bool RL, bool CL>
+__device__ __forceinline__ void dist_pair_points(const DistStagePts &sg, uint32_t ri, uint32_t ci,
+                                                 double k_re, double k_imn,
+                                                 double (&acc)[KT<KK>::NCH][RL ? 3 : 1][CL ? 3 : 1]) {
+  constexpr int NCH = KT<KK>::NCH, NC = CL ? 3 : 1, NR = RL ? 3 : 1, P = 4;
+  constexpr bool DOT = uses_normal<KK>(), RN = row_normal<KK>();
+  const double(&sd)[6][SIDE_MAXP] = c_side[1];
+  double n[3] = {0.0, 0.0, 0.0};
+  if (DOT) {
+#pragma unroll
+    for (int d = 0; d < 3; d++) n[d] = RN ? sg.r[PT_N + d][ri] : sg.c[PT_N + d][ci];
+  }
+  double yb[P][3], nyb[P];
+#pragma unroll
+  for (int b = 0; b < P; b++) {
+#pragma unroll
+    for (int d = 0; d < 3; d++) yb[b][d] = sg.c[PT_X + 3 * b + d][ci];
+    nyb[b] = !DOT ? 0.0
+                  : RN ? fma(yb[b][0], n[0], fma(yb[b][1], n[1], yb[b][2] * n[2]))
+                       : sg.c[PT_DN + b][ci];
+  }
+#pragma unroll
+  for (int a = 0; a < P; a++) {
+    double xa[3];
+#pragma unroll
+    for (int d = 0; d < 3; d++) xa[d] = sg.r[PT_X + 3 * a + d][ri];
+    const double nxa = !DOT ? 0.0
+                            : RN ? sg.r[PT_DN + a][ri]
+                                 : fma(xa[0], n[0], fma(xa[1], n[1], xa[2] * n[2]));
+    double in[NCH][NC];
+#pragma unroll
+    for (int c = 0; c < NCH; c++)
+#pragma unroll
+      for (int j = 0; j < NC; j++) in[c][j] = 0.0;
+#pragma unroll
+    for (int b = 0; b < P; b++) {
+      const double dx = xa[0] - yb[b][0], dy = xa[1] - yb[b][1], dz = xa[2] - yb[b][2];
+      const double r2 = fma(dx, dx, fma(dy, dy, dz * dz));
+      double kv[2];
+      eval_kernel<KK>(r2, nxa - nyb[b], k_re, k_imn, kv);
+#pragma unroll
+      for (int c = 0; c < NCH; c++)
+#pragma unroll
+        for (int j = 0; j < NC; j++) in[c][j] = fma(sd[CL ? 3 + j : 2][b], kv[c], in[c][j]);
+    }
+#pragma unroll
+    for (int c = 0; c < NCH; c++)
+#pragma unroll
+      for (int i = 0; i < NR; i++)
+#pragma unroll
+        for (int j = 0; j < NC; j++)
+          acc[c][i][j] = fma(sd[RL ? 3 + i : 2][a], in[c][j], acc[c][i][j]);
+  }
+}
+
+// the stage of a kernel variant: staged points for the q = 2 FP64 kernels
+template <int Q, bool F32>
+using DistStageOf = std::conditional_t<Q == 2 && !F32, DistStagePts, DistStage>;
+
 template <int Q, int KK, bool RL, bool CL, bool F32 = false>
 __global__ void __launch_bounds__(256, DIST_MINBLOCKS) near_dist_kernel(DistArgs a) {
   constexpr int NCH = KT<KK>::NCH;
@@ -523,7 +621,8 @@ __global__ void __launch_bounds__(256, DIST_MINBLOCKS) near_dist_kernel(DistArgs
   // Chunk pairs (column chunk outer): rows are restaged per chunk pair only when the tile has
   // more than one row chunk.  Lanes of a warp take consecutive row triangles of one column
   // triangle: the row arrays are read as consecutive words, the column arrays as a broadcast.
-  DistStage &sg = *reinterpret_cast<DistStage *>(sacc + PLANES * TS);
+  constexpr bool PTS = Q == 2 && !F32;
+  DistStageOf<Q, F32> &sg = *reinterpret_cast<DistStageOf<Q, F32> *>(sacc + PLANES * TS);
   for (uint32_t c0 = 0; c0 < nsc; c0 += DIST_CHUNK) {
     const uint32_t nc = min((uint32_t) DIST_CHUNK, nsc - c0);
     for (uint32_t r0 = 0; r0 < ntr; r0 += DIST_CHUNK) {
@@ -534,32 +633,46 @@ __global__ void __launch_bounds__(256, DIST_MINBLOCKS) near_dist_kernel(DistArgs
           for (uint32_t e = threadIdx.x; e < nc; e += blockDim.x) {
             const TriRef st = a.refs[tl.sc_off + c0 + e];
             const TriRec &S = a.tri[st.t];
+            if constexpr (PTS) {
+              stage_points(sg.c, e, S, a.kconst);
+            } else {
+#pragma unroll
+              for (int d = 0; d < 3; d++) {
+                sg.c[d][e] = S.a[d];
+                sg.c[3 + d][e] = S.b[d] - S.a[d];
+                sg.c[6 + d][e] = S.c[d] - S.b[d];
+                sg.c[10 + d][e] = S.n[d];
+              }
+              sg.c[9][e] = S.g * a.kconst;
+            }
 #pragma unroll
             for (int d = 0; d < 3; d++) {
-              sg.c[d][e] = S.a[d];
-              sg.c[3 + d][e] = S.b[d] - S.a[d];
-              sg.c[6 + d][e] = S.c[d] - S.b[d];
-              sg.c[10 + d][e] = S.n[d];
               sg.cv[d][e] = S.v[d];
               sg.cl[d][e] = st.l[d];
             }
-            sg.c[9][e] = S.g * a.kconst;
           }
         }
         if (c0 == 0 || ntr > (uint32_t) DIST_CHUNK) {
           for (uint32_t e = threadIdx.x; e < nr; e += blockDim.x) {
             const TriRef rt = a.refs[tl.tr_off + r0 + e];
             const TriRec &T = a.tri[rt.t];
+            if constexpr (PTS) {
+              stage_points(sg.r, e, T, 1.0);
+            } else {
+#pragma unroll
+              for (int d = 0; d < 3; d++) {
+                sg.r[d][e] = T.a[d];
+                sg.r[3 + d][e] = T.b[d] - T.a[d];
+                sg.r[6 + d][e] = T.c[d] - T.b[d];
+                sg.r[10 + d][e] = T.n[d];
+              }
+              sg.r[9][e] = T.g;
+            }
 #pragma unroll
             for (int d = 0; d < 3; d++) {
-              sg.r[d][e] = T.a[d];
-              sg.r[3 + d][e] = T.b[d] - T.a[d];
-              sg.r[6 + d][e] = T.c[d] - T.b[d];
-              sg.r[10 + d][e] = T.n[d];
               sg.rv[d][e] = T.v[d];
               sg.rl[d][e] = rt.l[d];
             }
-            sg.r[9][e] = T.g;
           }
         }
         __syncthreads();
@@ -580,18 +693,6 @@ __global__ void __launch_bounds__(256, DIST_MINBLOCKS) near_dist_kernel(DistArgs
         const bool singular = tv0 == sv0 || tv0 == sv1 || tv0 == sv2 || tv1 == sv0 ||
                               tv1 == sv1 || tv1 == sv2 || tv2 == sv0 || tv2 == sv1 || tv2 == sv2;
         if (singular) continue;
-        PairGeo g;
-#pragma unroll
-        for (int d = 0; d < 3; d++) {
-          g.d0[d] = sg.r[d][ri] - sg.c[d][ci];
-          g.p1[d] = sg.r[3 + d][ri];
-          g.p2[d] = sg.r[6 + d][ri];
-          g.q1[d] = sg.c[3 + d][ci];
-          g.q2[d] = sg.c[6 + d][ci];
-        }
-        const double(&nn)[13][DIST_CHUNK] = row_normal<KK>() ? sg.r : sg.c;
-        const uint32_t ni = row_normal<KK>() ? ri : ci;
-        const double n0 = nn[10][ni], n1 = nn[11][ni], n2 = nn[12][ni];
         double acc[NCH][NR][NC];
 #pragma unroll
         for (int c = 0; c < NCH; c++)
@@ -599,19 +700,35 @@ __global__ void __launch_bounds__(256, DIST_MINBLOCKS) near_dist_kernel(DistArgs
           for (int i = 0; i < NR; i++)
 #pragma unroll
             for (int j = 0; j < NC; j++) acc[c][i][j] = 0.0;
-
-        if constexpr (Q > 0) {
-          if constexpr (F32)
-            dist_pair_tensor_f32<Q, KK, RL, CL>(g, n0, n1, n2, a.k_re, a.k_imn, acc);
-          else
-            dist_pair_tensor<Q, KK, RL, CL>(g, n0, n1, n2, a.k_re, a.k_imn, acc);
+        double f2;
+        if constexpr (PTS) {
+          dist_pair_points<KK, RL, CL>(sg, ri, ci, a.k_re, a.k_imn, acc);
+          f2 = sg.c[PT_G][ci] * sg.r[PT_G][ri];
         } else {
-          for (int k = 0; k < nq; k++)
-            quad_point<KK, RL, CL>(g, cx0[k], cx1[k], cy0[k], cy1[k], cw[k], n0, n1, n2, a.k_re,
-                                   a.k_imn, acc);
+          PairGeo g;
+#pragma unroll
+          for (int d = 0; d < 3; d++) {
+            g.d0[d] = sg.r[d][ri] - sg.c[d][ci];
+            g.p1[d] = sg.r[3 + d][ri];
+            g.p2[d] = sg.r[6 + d][ri];
+            g.q1[d] = sg.c[3 + d][ci];
+            g.q2[d] = sg.c[6 + d][ci];
+          }
+          const double(&nn)[13][DIST_CHUNK] = row_normal<KK>() ? sg.r : sg.c;
+          const uint32_t ni = row_normal<KK>() ? ri : ci;
+          const double n0 = nn[10][ni], n1 = nn[11][ni], n2 = nn[12][ni];
+          if constexpr (Q > 0) {
+            if constexpr (F32)
+              dist_pair_tensor_f32<Q, KK, RL, CL>(g, n0, n1, n2, a.k_re, a.k_imn, acc);
+            else
+              dist_pair_tensor<Q, KK, RL, CL>(g, n0, n1, n2, a.k_re, a.k_imn, acc);
+          } else {
+            for (int k = 0; k < nq; k++)
+              quad_point<KK, RL, CL>(g, cx0[k], cx1[k], cy0[k], cy1[k], cw[k], n0, n1, n2,
+                                     a.k_re, a.k_imn, acc);
+          }
+          f2 = sg.c[9][ci] * sg.r[9][ri];
         }
-
-        const double f2 = sg.c[9][ci] * sg.r[9][ri];
 #pragma unroll
         for (int i = 0; i < NR; i++) {
           const int lr = sg.rl[i][ri];
@@ -871,7 +988,7 @@ template <int Q, int KK, bool RL, bool CL, bool F32 = false>
 int launch_dist(const h2b_near_launch *L, cudaStream_t st) {
   constexpr int PLANES = KT<KK>::CPLX ? 2 : KT<KK>::NOUT;
   const size_t smem = sizeof(double) * PLANES * H2B_TILE_MAX * H2B_TILE_MAX +
-                      sizeof(DistStage);
+                      sizeof(DistStageOf<Q, F32>);
   H2B_CUDA_TRY((h2b_allow_smem<near_dist_kernel<Q, KK, RL, CL, F32>>()));
   DistArgs a;
   a.tri = (const TriRec *) L->tri;
