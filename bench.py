@@ -787,7 +787,8 @@ def run_helmholtz(a, peak):
     for k in (2.0, 8.0):
         slp = hb.new_slp_helmholtz_bem3d(k, gr, 2, 4, C, C)
         dlp = hb.new_dlp_helmholtz_bem3d(k, gr, 2, 4, C, C, 0.5)
-        V, K = hb.H2Matrix(slp, tree, 5), hb.H2Matrix(dlp, tree, 5)
+        V = hb.H2Matrix(slp, tree, 5)
+        K = hb.H2Matrix(dlp, tree, 5, like=V)  # shares V's device structure
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         V.assemble()

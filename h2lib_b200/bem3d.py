@@ -5,6 +5,7 @@ function); every compute call goes through the C ABI of libh2b200.so (include/h2
 Arrays may be numpy arrays (host) or CUDA tensors exposing data_ptr() (device).
 """
 import ctypes as C
+import sys
 
 import numpy as np
 
@@ -61,7 +62,9 @@ class Surface3d:
         return self._dev
 
     def __del__(self):
-        if getattr(self, "_dev", None):
+        # at interpreter exit the handles are left to the process teardown: the garbage
+        # collector may finalise an object after the surface or structure it depends on
+        if getattr(self, "_dev", None) and not sys.is_finalizing():
             try:
                 lib.h2b_surface_del(self._dev)
             except Exception:  # interpreter shutdown
@@ -138,7 +141,9 @@ class Bem3d:
         return dict(zip(("near_distant", "near_singular"), ms.tolist()))
 
     def __del__(self):
-        if getattr(self, "handle", None):
+        # at interpreter exit the handles are left to the process teardown: the garbage
+        # collector may finalise an object after the surface or structure it depends on
+        if getattr(self, "handle", None) and not sys.is_finalizing():
             try:
                 lib.h2b_bem_del(self.handle)
             except Exception:  # interpreter shutdown
@@ -232,7 +237,9 @@ class Tree:
         return rec
 
     def __del__(self):
-        if getattr(self, "handle", None):
+        # at interpreter exit the handles are left to the process teardown: the garbage
+        # collector may finalise an object after the surface or structure it depends on
+        if getattr(self, "handle", None) and not sys.is_finalizing():
             try:
                 lib.h2b_tree_del(self.handle)
             except Exception:  # interpreter shutdown
@@ -354,7 +361,9 @@ class H2Matrix:
         return out
 
     def __del__(self):
-        if getattr(self, "handle", None):
+        # at interpreter exit the handles are left to the process teardown: the garbage
+        # collector may finalise an object after the surface or structure it depends on
+        if getattr(self, "handle", None) and not sys.is_finalizing():
             try:
                 lib.h2b_h2matrix_del(self.handle)
             except Exception:  # interpreter shutdown

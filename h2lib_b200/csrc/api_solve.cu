@@ -22,12 +22,38 @@ struct Combo {
   double *work = nullptr;
   const uint32_t *mask = nullptr;
   uint32_t nseg = 1;
+  // two operators on one structure with equal coupling matrices and row bases (a double layer
+  // beside its single layer): applied as one product that reads those once
+  bool pair = false;
 };
+
+// Two matrices built on one structure (h2b_h2matrix_new_like) for the same surface, PDE,
+// wavenumber, interpolation order and row basis, neither an adjoint double layer: their coupling
+// matrices (the kernel at the interpolation points) and their row bases (Lagrange polynomials)
+// are computed from the same data by the same kernels, so they are equal.
+static bool same_farfield(const h2b_h2matrix *a, const h2b_h2matrix *b) {
+  const h2b_h2matrix *oa = a->shared ? a->owner : a, *ob = b->shared ? b->owner : b;
+  const h2b_bem *ea = a->bem, *eb = b->bem;
+  return oa == ob && a->cx == b->cx && a->m == b->m && ea->s == eb->s && ea->pde == eb->pde &&
+         ea->k_re == eb->k_re && ea->k_im == eb->k_im && ea->kconst == eb->kconst &&
+         ea->q == eb->q && ea->row_basis == eb->row_basis && ea->layer != H2B_ADLP &&
+         eb->layer != H2B_ADLP;
+}
 
 template <bool SINGLE>
 int combo_apply_t(void *ctx, const double *x, double *y, double ar, double ai, cudaStream_t st) {
   const Combo *c = (const Combo *) ctx;
   const size_t col = (size_t) (c->ops[0]->cx ? 2 : 1) * c->ops[0]->rt.nidx;
+  if (c->pair && !c->mask && (c->nrhs == 1 || !c->work)) {
+    const double a0r = ar * c->cre[0] - ai * c->cim[0], a0i = ar * c->cim[0] + ai * c->cre[0];
+    const double a1r = ar * c->cre[1] - ai * c->cim[1], a1i = ar * c->cim[1] + ai * c->cre[1];
+    for (uint32_t r = 0; r < c->nrhs; r++) {
+      int rc = h2b_mvm_launch_pair(&c->ops[0]->mvm, &c->ops[1]->mvm, SINGLE ? 1 : 0, x + r * col,
+                                   y + r * col, a0r, a0i, a1r, a1i, c->work, st);
+      if (rc != H2B_OK) return rc;
+    }
+    return H2B_OK;
+  }
   if (c->work) {
     for (uint32_t i = 0; i < c->nterms; i++) {
       const double br = ar * c->cre[i] - ai * c->cim[i], bi = ar * c->cim[i] + ai * c->cre[i];
@@ -75,6 +101,7 @@ int check_ops(uint32_t nterms, const h2b_h2matrix *const *ops, const double *coe
     c->cre[i] = coef[2 * i];
     c->cim[i] = coef[2 * i + 1];
   }
+  c->pair = nterms == 2 && same_farfield(ops[0], ops[1]);
   return H2B_OK;
 }
 
@@ -176,6 +203,7 @@ static int solve_segments(Combo &combo, uint32_t nseg, const uint32_t *seg_off, 
     forest = forest && forest_matches(h->rt, nseg, seg_off) && forest_matches(h->ct, nseg, seg_off);
     nwork = std::max(nwork, h2b_mvm_work_doubles(&h->mvm, nrhs));
   }
+  if (combo.pair) nwork = std::max(nwork, h2b_mvm_pair_work_doubles(&combo.ops[0]->mvm));
   H2B_CUDA_TRY(cudaMallocAsync(&work.p, sizeof(double) * nwork, st));
   combo.work = (double *) work.p;
   combo.mask = forest ? g.mask : nullptr;

@@ -528,6 +528,76 @@ MvmVecs plan_vecs(const MvmPlan *p) {
 
 bool has_single(const MvmPlan *p) { return p->fWc && p->fWr && p->fN && p->fS; }
 
+// xs = b xp and xp = a xp, n entries (complex: interleaved pairs).
+template <bool CX>
+__global__ void scale_copy_kernel(double *__restrict__ xp, double *__restrict__ xs, uint32_t n,
+                                  double ar, double ai, double br, double bi) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    if (CX) {
+      const double re = xp[2 * i], im = xp[2 * i + 1];
+      xs[2 * i] = br * re - bi * im;
+      xs[2 * i + 1] = br * im + bi * re;
+      xp[2 * i] = ar * re - ai * im;
+      xp[2 * i + 1] = ar * im + ai * re;
+    } else {
+      const double v = xp[i];
+      xs[i] = br * v;
+      xp[i] = ar * v;
+    }
+  }
+}
+
+// y += a A x + b B x for two matrices on one structure whose coupling matrices and row bases
+// are equal (the caller checks): the forward transforms and nearfield blocks of both run on
+// their own scaled copies of x into p's accumulators, then p's coupling matrices and row basis
+// are applied once.
+template <bool CX, bool SINGLE>
+int launch_pair(const MvmPlan *p, const MvmPlan *q, const double *x, double *y, double ar,
+                double ai, double br, double bi, const MvmVecs &v, double *xq, cudaStream_t st) {
+  using T = typename std::conditional<SINGLE, float, double>::type;
+  const size_t W = CX ? 2 : 1;
+  const int sms = p->num_sms > 0 ? p->num_sms : 148;
+  const uint32_t zn = p->nrow > p->ncol ? p->nrow : p->ncol;
+  const uint32_t gz = std::min<uint32_t>((zn + 255) / 256 + 1, (uint32_t) (4 * sms));
+  const size_t nyp = W * p->nrow, nxt = W * (size_t) p->k * p->ncol_clusters,
+               nyt = W * (size_t) p->k * p->nrow_clusters;
+  gather_zero_kernel<CX><<<gz, 256, 0, st>>>(x, 0, p->cidx, p->ncol, v, nyp, nxt, nyt);
+  h2b_note_launch();
+  scale_copy_kernel<CX><<<gz, 256, 0, st>>>(v.xp, xq, p->ncol, ar, ai, br, bi);
+  h2b_note_launch();
+  MvLaunch L{};
+  L.nrhs = 1;
+  L.nseg = 1;
+  L.mask = nullptr;
+  L.err = p->err;
+  L.A[H2B_MV_FORWARD] = SINGLE ? (const void *) p->fWc : (const void *) p->Wc;
+  L.A[H2B_MV_NEAR] = SINGLE ? (const void *) p->fN : (const void *) p->N;
+  L.A[H2B_MV_COUPLING] = SINGLE ? (const void *) p->fS : (const void *) p->S;
+  L.A[H2B_MV_BACKWARD] = SINGLE ? (const void *) p->fWr : (const void *) p->Wr;
+  L.X[H2B_MV_FORWARD] = v.xp, L.Y[H2B_MV_FORWARD] = v.xt;
+  L.X[H2B_MV_NEAR] = v.xp, L.Y[H2B_MV_NEAR] = v.yp;
+  L.X[H2B_MV_COUPLING] = v.xt, L.Y[H2B_MV_COUPLING] = v.yt;
+  L.X[H2B_MV_BACKWARD] = v.yt, L.Y[H2B_MV_BACKWARD] = v.yp;
+  MvLaunch Lq = L;
+  Lq.A[H2B_MV_FORWARD] = SINGLE ? (const void *) q->fWc : (const void *) q->Wc;
+  Lq.A[H2B_MV_NEAR] = SINGLE ? (const void *) q->fN : (const void *) q->N;
+  Lq.X[H2B_MV_FORWARD] = xq;
+  Lq.X[H2B_MV_NEAR] = xq;
+  const MvItems &it = SINGLE ? p->items_single : p->items;
+  const MvItems &iq = SINGLE ? q->items_single : q->items;
+  int rc = launch_range<CX, T>(p, it, L, 0, it.start[H2B_MV_COUPLING], st);
+  if (rc == H2B_OK) rc = launch_range<CX, T>(p, iq, Lq, 0, iq.start[H2B_MV_COUPLING], st);
+  if (rc == H2B_OK)
+    rc = launch_range<CX, T>(p, it, L, it.start[H2B_MV_COUPLING], it.start[H2B_MV_BACKWARD], st);
+  if (rc == H2B_OK) rc = launch_range<CX, T>(p, it, L, it.start[H2B_MV_BACKWARD], it.n, st);
+  if (rc != H2B_OK) return rc;
+  scatter_multi_kernel<CX><<<gz, 256, 0, st>>>(v, p->ridx, y, 0, p->nrow, 1.0, 0.0);
+  h2b_note_launch();
+  H2B_CUDA_TRY(cudaGetLastError());
+  return H2B_OK;
+}
+
+
 }  // namespace
 
 extern "C" int h2b_mvm_prepare(void) {
@@ -563,6 +633,35 @@ extern "C" int h2b_mvm_launch(const MvmPlan *p, const double *x, double *y, doub
   const MvmVecs v = plan_vecs(p);
   return p->cx ? launch_all<true, false>(p, x, 0, y, 0, ar, ai, v, st)
                : launch_all<false, false>(p, x, 0, y, 0, ar, ai, v, st);
+}
+
+extern "C" size_t h2b_mvm_pair_work_doubles(const MvmPlan *p) {
+  // one column of p's vectors, then the second scaled copy of x with its own slack
+  return h2b_mvm_work_doubles(p, 1) + (size_t) (p->cx ? 2 : 1) * p->ncol + 8;
+}
+
+extern "C" int h2b_mvm_launch_pair(const MvmPlan *p, const MvmPlan *q, int single,
+                                   const double *x, double *y, double ar, double ai, double br,
+                                   double bi, double *work, cudaStream_t st) {
+  if (single && (!has_single(p) || !has_single(q))) {
+    h2b_set_error("matvec: no FP32 copy of the H2 matrix (h2b_h2matrix_make_single)");
+    return H2B_ERR_ARG;
+  }
+  MvmVecs v = plan_vecs(p);
+  double *xq = q->xp;
+  if (work) {
+    const size_t W = p->cx ? 2 : 1;
+    v.xp = work;
+    v.yp = v.xp + W * p->ncol;
+    v.xt = v.yp + W * p->nrow;
+    v.yt = v.xt + W * (size_t) p->k * p->ncol_clusters;
+    xq = work + h2b_mvm_work_doubles(p, 1);
+  }
+  if (p->cx)
+    return single ? launch_pair<true, true>(p, q, x, y, ar, ai, br, bi, v, xq, st)
+                  : launch_pair<true, false>(p, q, x, y, ar, ai, br, bi, v, xq, st);
+  return single ? launch_pair<false, true>(p, q, x, y, ar, ai, br, bi, v, xq, st)
+                : launch_pair<false, false>(p, q, x, y, ar, ai, br, bi, v, xq, st);
 }
 
 extern "C" size_t h2b_mvm_work_doubles(const MvmPlan *p, uint32_t nrhs) {

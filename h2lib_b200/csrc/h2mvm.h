@@ -67,6 +67,14 @@ extern "C" int h2b_mvm_launch_single(const MvmPlan *p, const double *x, double *
 // launch sequence that reads the matrix once; `work` holds h2b_mvm_work_doubles(p, nrhs)
 // doubles.  mask (optional, forest matrices): column r of surface s is computed only when
 // mask[s + r * nseg] != 0 (the others receive nothing).  single: the FP32 copies.
+// y += (ar + i ai) A x + (br + i bi) B x for the plans p (A) and q (B) of two matrices on one
+// structure whose coupling matrices and row bases are equal: the coupling matrices and the row
+// basis (p's) are read once.  single: the FP32 copies of both.  work: NULL (the plans' own work
+// vectors) or h2b_mvm_pair_work_doubles(p) doubles.
+extern "C" size_t h2b_mvm_pair_work_doubles(const MvmPlan *p);
+extern "C" int h2b_mvm_launch_pair(const MvmPlan *p, const MvmPlan *q, int single,
+                                   const double *x, double *y, double ar, double ai, double br,
+                                   double bi, double *work, cudaStream_t st);
 extern "C" size_t h2b_mvm_work_doubles(const MvmPlan *p, uint32_t nrhs);
 extern "C" int h2b_mvm_launch_batch(const MvmPlan *p, int single, uint32_t nrhs, const double *x,
                                     size_t ldx, double *y, size_t ldy, double ar, double ai,
