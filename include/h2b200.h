@@ -365,7 +365,10 @@ int h2b_h2matrix_addeval_multi(double alpha_re, double alpha_im, const h2b_h2mat
  * algorithm as init_gmres / step_gmres / finish_gmres (Library/krylov.c:612/659/725): stops when
  * the estimated residual |rhat_k| <= eps * ||b||, restarts every kmax-1 steps, at most
  * maxiter-1 steps.  x holds the start vector and receives the solution.  Returns the number of
- * iterations (>= 0) or a negative H2B_ERR_* code.  coef is interleaved complex (2*nterms). */
+ * iterations (>= 0) or a negative H2B_ERR_* code.  coef is interleaved complex (2*nterms).
+ * Two terms on one structure (h2b_h2matrix_new_like) for the same PDE, wavenumber and row basis,
+ * neither an adjoint double layer (a double layer beside its single layer), are applied as one
+ * product that reads their common coupling matrices and row basis once. */
 int h2b_solve_gmres(uint32_t nterms, const h2b_h2matrix *const *ops, const double *coef,
                     const double *b, double *x, double eps, uint32_t maxiter, uint32_t kmax);
 
