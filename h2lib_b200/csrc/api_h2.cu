@@ -767,7 +767,7 @@ static int launch_near(h2b_h2matrix *h, h2b_h2matrix *h2) {
   L.ev_between = h->ev[7];
   L.fp32 = h->quad_fp32;
   if (h2) {
-    L.kk = H2B_KK_LBOTH;
+    L.kk = h->bem->pde == H2B_LAPLACE ? H2B_KK_LBOTH : H2B_KK_HBOTH;
     L.out1 = h2->d_N;
     L.alpha_re = h2->bem->alpha_re;
     L.alpha_im = h2->bem->alpha_im;
@@ -802,11 +802,13 @@ extern "C" int h2b_h2matrix_assemble_nearfield(h2b_h2matrix *h) {
 extern "C" int h2b_h2matrix_assemble_nearfield_pair(h2b_h2matrix *a, h2b_h2matrix *b) {
   if (!a || !b) return H2B_ERR_ARG;
   const h2b_bem *A = a->bem, *B = b->bem;
-  if (a->tree != b->tree || A->s != B->s || A->pde != H2B_LAPLACE || B->pde != H2B_LAPLACE ||
-      A->layer != H2B_SLP || B->layer != H2B_DLP || A->row_basis != B->row_basis ||
-      A->col_basis != B->col_basis || A->q != B->q || A->q2 != B->q2) {
-    h2b_set_error("h2b_h2matrix_assemble_nearfield_pair: needs a Laplace SLP and DLP pair on the "
-                  "same tree, surface, bases and quadrature orders");
+  if (a->tree != b->tree || A->s != B->s || A->pde != B->pde || A->k_re != B->k_re ||
+      A->k_im != B->k_im || A->layer != H2B_SLP || B->layer != H2B_DLP ||
+      A->row_basis != B->row_basis || A->col_basis != B->col_basis || A->q != B->q ||
+      A->q2 != B->q2) {
+    h2b_set_error("h2b_h2matrix_assemble_nearfield_pair: needs a single and a double layer of "
+                  "the same PDE and wavenumber on the same tree, surface, bases and quadrature "
+                  "orders");
     return H2B_ERR_ARG;
   }
   // b's storage must be idle before a's stream writes it

@@ -40,6 +40,7 @@ constexpr int KK_HSLP = H2B_KK_HSLP;
 constexpr int KK_HDLP = H2B_KK_HDLP;
 constexpr int KK_LADLP = H2B_KK_LADLP;
 constexpr int KK_HADLP = H2B_KK_HADLP;
+constexpr int KK_HBOTH = H2B_KK_HBOTH;
 
 template <int KK> struct KT;
 template <> struct KT<KK_LSLP> { static constexpr int NCH = 1, NOUT = 1; static constexpr bool CPLX = false; };
@@ -49,6 +50,7 @@ template <> struct KT<KK_HSLP> { static constexpr int NCH = 2, NOUT = 1; static 
 template <> struct KT<KK_HDLP> { static constexpr int NCH = 2, NOUT = 1; static constexpr bool CPLX = true; };
 template <> struct KT<KK_LADLP> { static constexpr int NCH = 1, NOUT = 1; static constexpr bool CPLX = false; };
 template <> struct KT<KK_HADLP> { static constexpr int NCH = 2, NOUT = 1; static constexpr bool CPLX = true; };
+template <> struct KT<KK_HBOTH> { static constexpr int NCH = 4, NOUT = 2; static constexpr bool CPLX = true; };
 
 // Distant tensor rules for q = 1..5 (q^4 points each): x0, x1, y0, y1, w.
 constexpr int DIST_TOTAL = 1 + 16 + 81 + 256 + 625;
@@ -69,7 +71,7 @@ __constant__ double c_side[5][6][SIDE_MAXP];
 // <y - x, n_x> = -dot: Library/laplacebem3d.c:136, Library/helmholtzbem3d.c:209).
 template <int KK>
 __device__ __forceinline__ void eval_kernel(double r2, double dot, double k_re, double k_imn,
-                                            double kv[2]) {
+                                            double kv[4]) {
   double rinv = rsqrt_nr(r2);
   if constexpr (KK == KK_LSLP) {
     kv[0] = rinv;
@@ -86,6 +88,20 @@ __device__ __forceinline__ void eval_kernel(double r2, double dot, double k_re, 
     sincos(k_re * r, &s, &c);
     kv[0] = rn * c;
     kv[1] = rn * s;
+  } else if constexpr (KK == KK_HBOTH) {
+    // single layer in kv[0..1], double layer in kv[2..3]: one sine and cosine for both
+    double r = r2 * rinv, rn = rinv, re = (rinv * rinv * rinv) * dot, s, c;
+    if (k_imn != 0.0) {
+      const double e = exp(k_imn * r);
+      rn *= e;
+      re *= e;
+    }
+    const double kr = k_re * r;
+    sincos(kr, &s, &c);
+    kv[0] = rn * c;
+    kv[1] = rn * s;
+    kv[2] = fma(kr, s, c) * re;
+    kv[3] = fma(-c, kr, s) * re;
   } else {  // KK_HDLP, KK_HADLP
     double re = (rinv * rinv * rinv) * (KK == KK_HADLP ? -dot : dot), r = r2 * rinv, s, c;
     if (k_imn != 0.0) re *= exp(k_imn * r);
@@ -98,7 +114,8 @@ __device__ __forceinline__ void eval_kernel(double r2, double dot, double k_re, 
 
 template <int KK>
 constexpr bool uses_normal() {
-  return KK == KK_LDLP || KK == KK_LBOTH || KK == KK_HDLP || KK == KK_LADLP || KK == KK_HADLP;
+  return KK == KK_LDLP || KK == KK_LBOTH || KK == KK_HDLP || KK == KK_LADLP || KK == KK_HADLP ||
+         KK == KK_HBOTH;
 }
 
 // the adjoint double layer differentiates in the row triangle's normal direction
@@ -140,7 +157,7 @@ __device__ __forceinline__ void quad_point(const PairGeo &g, double tx, double s
   double dx = fma(-sy, g.q2[0], fma(-ty, g.q1[0], fma(sx, g.p2[0], fma(tx, g.p1[0], g.d0[0]))));
   double dy = fma(-sy, g.q2[1], fma(-ty, g.q1[1], fma(sx, g.p2[1], fma(tx, g.p1[1], g.d0[1]))));
   double dz = fma(-sy, g.q2[2], fma(-ty, g.q1[2], fma(sx, g.p2[2], fma(tx, g.p1[2], g.d0[2]))));
-  double kv[2];
+  double kv[4];
   const double r2 = fma(dx, dx, fma(dy, dy, dz * dz));
   const double dot = uses_normal<KK>() ? fma(dx, n0, fma(dy, n1, dz * n2)) : 0.0;
   eval_kernel<KK>(r2, dot, k_re, k_imn, kv);
@@ -176,7 +193,7 @@ __device__ __forceinline__ void quad_point_red(const PairGeo &g, double ra, doub
   const double dx = fma(-rc, g.q2[0], fma(rb, g.p2[0], fma(ra, g.p1[0], g.d0[0])));
   const double dy = fma(-rc, g.q2[1], fma(rb, g.p2[1], fma(ra, g.p1[1], g.d0[1])));
   const double dz = fma(-rc, g.q2[2], fma(rb, g.p2[2], fma(ra, g.p1[2], g.d0[2])));
-  double kv[2];
+  double kv[4];
   const double r2 = fma(dx, dx, fma(dy, dy, dz * dz));
   const double dot = uses_normal<KK>() ? fma(dx, n0, fma(dy, n1, dz * n2)) : 0.0;
   eval_kernel<KK>(r2, dot, k_re, k_imn, kv);
@@ -226,7 +243,7 @@ __device__ __forceinline__ void vert_group_tensor(const PairGeo &g, const double
       const double dz = xa[2] - fma(y0, g.q1[2], y1 * g.q2[2]);
       const double r2 = fma(dx, dx, fma(dy, dy, dz * dz));
       const double dot = DOT ? fma(dx, n0, fma(dy, n1, dz * n2)) : 0.0;
-      double kv[2];
+      double kv[4];
       eval_kernel<KK>(r2, dot, k_re, k_imn, kv);
 #pragma unroll
       for (int j = 0; j < NC; j++) {
@@ -289,7 +306,7 @@ __device__ __forceinline__ void vert_item_merged(const PairGeo &g, const double 
     const double dz = xa[2] - fma(y0, g.q1[2], y1 * g.q2[2]);
     const double r2 = fma(dx, dx, fma(dy, dy, dz * dz));
     const double dot = DOT ? fma(dx, n0, fma(dy, n1, dz * n2)) : 0.0;
-    double kv[2];
+    double kv[4];
     eval_kernel<KK>(r2, dot, 0.0, 0.0, kv);
 #pragma unroll
     for (int c = 0; c < NCH; c++) {
@@ -346,7 +363,7 @@ __device__ __forceinline__ void dist_pair_tensor(const PairGeo &g, double n0, do
     for (int b = 0; b < P; b++) {
       const double dx = xa[0] - yb[b][0], dy = xa[1] - yb[b][1], dz = xa[2] - yb[b][2];
       const double r2 = fma(dx, dx, fma(dy, dy, dz * dz));
-      double kv[2];
+      double kv[4];
       eval_kernel<KK>(r2, nxa - nyb[b], k_re, k_imn, kv);
 #pragma unroll
       for (int c = 0; c < NCH; c++)
@@ -371,7 +388,7 @@ __constant__ float c_side_f[5][6][SIDE_MAXP];
 
 template <int KK>
 __device__ __forceinline__ void eval_kernel_f(float r2, float dot, float k_re, float k_imn,
-                                              float kv[2]) {
+                                              float kv[4]) {
   const float rinv = rsqrtf(r2);
   if constexpr (KK == KK_LSLP) {
     kv[0] = rinv;
@@ -388,6 +405,19 @@ __device__ __forceinline__ void eval_kernel_f(float r2, float dot, float k_re, f
     sincosf(k_re * r, &s, &c);
     kv[0] = rn * c;
     kv[1] = rn * s;
+  } else if constexpr (KK == KK_HBOTH) {
+    float r = r2 * rinv, rn = rinv, re = (rinv * rinv * rinv) * dot, s, c;
+    if (k_imn != 0.0f) {
+      const float e = expf(k_imn * r);
+      rn *= e;
+      re *= e;
+    }
+    const float kr = k_re * r;
+    sincosf(kr, &s, &c);
+    kv[0] = rn * c;
+    kv[1] = rn * s;
+    kv[2] = fmaf(kr, s, c) * re;
+    kv[3] = fmaf(-c, kr, s) * re;
   } else {  // KK_HDLP, KK_HADLP
     float re = (rinv * rinv * rinv) * (KK == KK_HADLP ? -dot : dot), r = r2 * rinv, s, c;
     if (k_imn != 0.0f) re *= expf(k_imn * r);
@@ -445,7 +475,7 @@ __device__ __forceinline__ void dist_pair_tensor_f32(const PairGeo &g, double n0
     for (int b = 0; b < P; b++) {
       const float dx = xa[0] - yb[b][0], dy = xa[1] - yb[b][1], dz = xa[2] - yb[b][2];
       const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-      float kv[2];
+      float kv[4];
       eval_kernel_f<KK>(r2, nxa - nyb[b], kr, ki, kv);
 #pragma unroll
       for (int c = 0; c < NCH; c++)
@@ -568,7 +598,7 @@ __device__ __forceinline__ void dist_pair_points(const DistStagePts &sg, uint32_
     for (int b = 0; b < P; b++) {
       const double dx = xa[0] - yb[b][0], dy = xa[1] - yb[b][1], dz = xa[2] - yb[b][2];
       const double r2 = fma(dx, dx, fma(dy, dy, dz * dz));
-      double kv[2];
+      double kv[4];
       eval_kernel<KK>(r2, nxa - nyb[b], k_re, k_imn, kv);
 #pragma unroll
       for (int c = 0; c < NCH; c++)
@@ -589,11 +619,20 @@ __device__ __forceinline__ void dist_pair_points(const DistStagePts &sg, uint32_
 template <int Q, bool F32>
 using DistStageOf = std::conditional_t<Q == 2 && !F32, DistStagePts, DistStage>;
 
+// Threads and resident CTAs of the distant-pair kernel: the four accumulator planes of the fused
+// Helmholtz single and double layer fill most of the shared memory of an SM, so that kind runs
+// one CTA of twice the threads.
+template <int KK>
+constexpr int dist_threads() { return KT<KK>::NCH == 4 ? 512 : 256; }
+template <int KK>
+constexpr int dist_minblocks() { return KT<KK>::NCH == 4 ? 1 : DIST_MINBLOCKS; }
+
 template <int Q, int KK, bool RL, bool CL, bool F32 = false>
-__global__ void __launch_bounds__(256, DIST_MINBLOCKS) near_dist_kernel(DistArgs a) {
+__global__ void __launch_bounds__(dist_threads<KK>(), dist_minblocks<KK>())
+    near_dist_kernel(DistArgs a) {
   constexpr int NCH = KT<KK>::NCH;
   constexpr int NR = RL ? 3 : 1, NC = CL ? 3 : 1;
-  constexpr int PLANES = KT<KK>::CPLX ? 2 : KT<KK>::NOUT;
+  constexpr int PLANES = NCH;  // accumulator planes: one per real channel
   constexpr int TS = H2B_TILE_MAX * H2B_TILE_MAX;
   extern __shared__ double sacc[];
 
@@ -761,6 +800,10 @@ __global__ void __launch_bounds__(256, DIST_MINBLOCKS) near_dist_kernel(DistArgs
     if constexpr (KT<KK>::CPLX) {
       a.out0[2 * o] = sacc[se];
       a.out0[2 * o + 1] = ntrans ? -sacc[TS + se] : sacc[TS + se];
+      if constexpr (KT<KK>::NOUT == 2) {
+        a.out1[2 * o] = sacc[2 * TS + se];
+        a.out1[2 * o + 1] = ntrans ? -sacc[3 * TS + se] : sacc[3 * TS + se];
+      }
     } else {
       a.out0[o] = sacc[se];
       if constexpr (KT<KK>::NOUT == 2) a.out1[o] = sacc[TS + se];
@@ -934,7 +977,19 @@ __global__ void __launch_bounds__(SING_THREADS, 1) near_sing_kernel(SingArgs a) 
                                     : tl.out_off + lr + (uint64_t) lc * tl.ld;
           if constexpr (!RL && !CL) {
             // constant basis: this pair is the whole entry
-            if constexpr (KT<KK>::CPLX) {
+            if constexpr (KT<KK>::CPLX && KT<KK>::NOUT == 2) {
+              // single layer to out0, double layer with the identity term to out1
+              double re = acc[2][0][0] * f2, im = acc[3][0][0] * f2;
+              if (ident) {
+                re += 0.5 * a.alpha_re * T.g;
+                im += 0.5 * a.alpha_im * T.g;
+              }
+              const double sre = acc[0][0][0] * f2, sim = acc[1][0][0] * f2;
+              a.out0[2 * o] = sre;
+              a.out0[2 * o + 1] = ntrans ? -sim : sim;
+              a.out1[2 * o] = re;
+              a.out1[2 * o + 1] = ntrans ? -im : im;
+            } else if constexpr (KT<KK>::CPLX) {
               double re = acc[0][0][0] * f2, im = acc[1][0][0] * f2;
               if (ident) {
                 re += 0.5 * a.alpha_re * T.g;
@@ -952,6 +1007,10 @@ __global__ void __launch_bounds__(SING_THREADS, 1) near_sing_kernel(SingArgs a) 
             if constexpr (KT<KK>::CPLX) {
               atomicAdd(&a.out0[2 * o], acc[0][i][j] * f2);
               atomicAdd(&a.out0[2 * o + 1], (ntrans ? -1.0 : 1.0) * acc[1][i][j] * f2);
+              if constexpr (KT<KK>::NOUT == 2) {
+                atomicAdd(&a.out1[2 * o], acc[2][i][j] * f2);
+                atomicAdd(&a.out1[2 * o + 1], (ntrans ? -1.0 : 1.0) * acc[3][i][j] * f2);
+              }
             } else {
               atomicAdd(&a.out0[o], acc[0][i][j] * f2);
               if constexpr (KT<KK>::NOUT == 2) atomicAdd(&a.out1[o], acc[1][i][j] * f2);
@@ -986,7 +1045,7 @@ __global__ void __launch_bounds__(SING_THREADS, 1) near_sing_kernel(SingArgs a) 
 
 template <int Q, int KK, bool RL, bool CL, bool F32 = false>
 int launch_dist(const h2b_near_launch *L, cudaStream_t st) {
-  constexpr int PLANES = KT<KK>::CPLX ? 2 : KT<KK>::NOUT;
+  constexpr int PLANES = KT<KK>::NCH;
   const size_t smem = sizeof(double) * PLANES * H2B_TILE_MAX * H2B_TILE_MAX +
                       sizeof(DistStageOf<Q, F32>);
   H2B_CUDA_TRY((h2b_allow_smem<near_dist_kernel<Q, KK, RL, CL, F32>>()));
@@ -1001,7 +1060,7 @@ int launch_dist(const h2b_near_launch *L, cudaStream_t st) {
   a.k_imn = L->k_imn;
   a.q = (int) L->q;
   if (L->ntiles > 0) {
-    near_dist_kernel<Q, KK, RL, CL, F32><<<L->ntiles, 256, smem, st>>>(a);
+    near_dist_kernel<Q, KK, RL, CL, F32><<<L->ntiles, dist_threads<KK>(), smem, st>>>(a);
     h2b_note_launch();
   }
   H2B_CUDA_TRY(cudaGetLastError());
@@ -1438,6 +1497,7 @@ extern "C" int h2b_near_launch_kernels(const h2b_near_launch *L, cudaStream_t st
     case KK_HDLP: return launch_kk<KK_HDLP>(L, st);
     case KK_LADLP: return launch_kk<KK_LADLP>(L, st);
     case KK_HADLP: return launch_kk<KK_HADLP>(L, st);
+    case KK_HBOTH: return launch_kk<KK_HBOTH>(L, st);
     default: h2b_set_error("unknown kernel kind %d", L->kk); return H2B_ERR_ARG;
   }
 }

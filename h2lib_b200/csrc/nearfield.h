@@ -19,6 +19,7 @@ extern "C" {
 #define H2B_KK_HDLP 4   /* Helmholtz double layer, complex */
 #define H2B_KK_LADLP 5  /* Laplace adjoint double layer (row normal), real */
 #define H2B_KK_HADLP 6  /* Helmholtz adjoint double layer (row normal), complex */
+#define H2B_KK_HBOTH 7  /* Helmholtz single and double layer together (two complex outputs) */
 
 typedef struct {
   int kk;
@@ -31,7 +32,7 @@ typedef struct {
   const h2b_sing *sing;          /* sorted by case */
   uint32_t nsing;
   uint32_t nvert;                /* vertex pairs at the start of sing (UINT32_MAX: not known) */
-  double *out0, *out1;           /* out1: double-layer output of H2B_KK_LBOTH */
+  double *out0, *out1;           /* out1: double-layer output of H2B_KK_LBOTH / H2B_KK_HBOTH */
   double kconst, k_re, k_imn;    /* 1/(4 pi); Re k; -Im k */
   double alpha_re, alpha_im;     /* identity coefficient of the double layer output */
   double mass[9];                /* linear-basis mass matrix on the reference triangle */

@@ -128,16 +128,13 @@ int run_request(Req *q) {
   std::vector<double> b(W * nd, 0.0), u(W * nd, 0.0), gD;
   rc = (V && K) ? H2B_OK : H2B_ERR_CUDA;
   if (rc == H2B_OK) {
-    if (helm) {
-      if ((rc = h2b_h2matrix_assemble_all(V)) == H2B_OK) rc = h2b_h2matrix_assemble_all(K);
-    } else {
-      for (h2b_h2matrix *h : {V, K}) {
-        if (rc == H2B_OK) rc = h2b_h2matrix_assemble_row_clusterbasis(h);
-        if (rc == H2B_OK) rc = h2b_h2matrix_assemble_col_clusterbasis(h);
-        if (rc == H2B_OK) rc = h2b_h2matrix_assemble_farfield(h);
-      }
-      if (rc == H2B_OK) rc = h2b_h2matrix_assemble_nearfield_pair(V, K);
+    // bases and coupling per operator, the nearfield of both in one pass (Laplace and Helmholtz)
+    for (h2b_h2matrix *h : {V, K}) {
+      if (rc == H2B_OK) rc = h2b_h2matrix_assemble_row_clusterbasis(h);
+      if (rc == H2B_OK) rc = h2b_h2matrix_assemble_col_clusterbasis(h);
+      if (rc == H2B_OK) rc = h2b_h2matrix_assemble_farfield(h);
     }
+    if (rc == H2B_OK) rc = h2b_h2matrix_assemble_nearfield_pair(V, K);
   }
   const auto c2 = tick();
   const h2b_h2matrix *ops[2];

@@ -245,8 +245,10 @@ int h2b_h2matrix_assemble_farfield(h2b_h2matrix *h2);
 int h2b_h2matrix_assemble(h2b_h2matrix *h2);
 int h2b_h2matrix_assemble_all(h2b_h2matrix *h2);
 
-/* Assemble the nearfield blocks of two operators on the same tree in one pass (e.g. V and K
- * of a Laplace Dirichlet problem share every triangle pair and quadrature point). */
+/* Assemble the nearfield blocks of two operators on the same tree in one pass: a single layer
+ * (a) and a double layer (b) of the same PDE (Laplace, or Helmholtz with the same wavenumber)
+ * share every triangle pair and quadrature point, and for Helmholtz the sine and cosine of each
+ * point's k r.  No reference counterpart (the reference fills each operator's blocks). */
 int h2b_h2matrix_assemble_nearfield_pair(h2b_h2matrix *a, h2b_h2matrix *b);
 
 /* Storage and counts: info[0] nearfield entries, [1] coupling entries, [2] leaf-basis entries,

@@ -81,3 +81,26 @@ def test_pair_mixed_solve_meets_fp64_tolerance():
     assert hb.residual_norm([K, V], coefs, b, u32) <= 1.01e-8
     assert abs(it32 - it64) <= 6
     assert np.linalg.norm(u32 - u64) / np.linalg.norm(u64) < 1e-6
+
+
+@pytest.mark.parametrize("basis", [C, L])
+def test_helmholtz_nearfield_pair_equals_separate(basis):
+    """The fused single + double layer nearfield pass of Helmholtz (one sine and cosine per
+    quadrature point for both kernels) against the two operators assembled apart, for a complex
+    wavenumber too (relative to the largest entry, 1e-13)."""
+    from h2lib_b200._lib import check, lib
+    gr = hb.new_sphere_surface3d(8)
+    tree = hb.build_tree(gr, basis, basis, 16, 1.4)
+    for k in (3.0, 3.0 + 0.5j):
+        slp = hb.new_slp_helmholtz_bem3d(k, gr, 2, 4, basis, basis)
+        dlp = hb.new_dlp_helmholtz_bem3d(k, gr, 2, 4, basis, basis, 0.5)
+        V = hb.H2Matrix(slp, tree, 3)
+        K = hb.H2Matrix(dlp, tree, 3, like=V)
+        check(lib.h2b_h2matrix_assemble_nearfield_pair(V.handle, K.handle), "nearfield pair")
+        V2 = hb.H2Matrix(slp, tree, 3)
+        K2 = hb.H2Matrix(dlp, tree, 3, like=V2)
+        check(lib.h2b_h2matrix_assemble_nearfield(V2.handle), "nearfield V")
+        check(lib.h2b_h2matrix_assemble_nearfield(K2.handle), "nearfield K")
+        for a, b in ((V, V2), (K, K2)):
+            na, nb = a.export(5), b.export(5)
+            assert np.max(np.abs(na - nb)) <= 1e-13 * np.max(np.abs(nb))
