@@ -328,59 +328,8 @@ __device__ __forceinline__ void vert_item_merged(const PairGeo &g, const double 
   }
 }
 
-// One distant pair with the q^4 tensor rule, summed column side first:
-//   acc[c][i][j] = sum_a w_a phi_i(x_a) sum_b w_b phi_j(y_b) k_c(x_a, y_b).
-// With X_a = x_a - A_s and Y_b = y_b - A_s the difference is x_a - y_b = X_a - Y_b and the double
-// layer's <x - y, n_y> = <X_a, n_y> - <Y_b, n_y>; X_a, Y_b and their normal components are formed
-// once per point instead of once per point pair.  Same sum as quad_point over the q^4 points, in
-// another order (differences at rounding level).
-template <int Q, int KK, bool RL, bool CL>
-__device__ __forceinline__ void dist_pair_tensor(const PairGeo &g, double n0, double n1, double n2,
-                                                 double k_re, double k_imn,
-                                                 double (&acc)[KT<KK>::NCH][RL ? 3 : 1][CL ? 3 : 1]) {
-  constexpr int NCH = KT<KK>::NCH, NC = CL ? 3 : 1, NR = RL ? 3 : 1, P = Q * Q;
-  constexpr bool DOT = uses_normal<KK>();
-  const double(&sd)[6][SIDE_MAXP] = c_side[Q - 1];
-  double yb[P][3], nyb[P];
-#pragma unroll
-  for (int b = 0; b < P; b++) {
-#pragma unroll
-    for (int d = 0; d < 3; d++) yb[b][d] = fma(sd[1][b], g.q2[d], sd[0][b] * g.q1[d]);
-    nyb[b] = DOT ? fma(yb[b][0], n0, fma(yb[b][1], n1, yb[b][2] * n2)) : 0.0;
-  }
-#pragma unroll
-  for (int a = 0; a < P; a++) {
-    double xa[3];
-#pragma unroll
-    for (int d = 0; d < 3; d++) xa[d] = fma(sd[1][a], g.p2[d], fma(sd[0][a], g.p1[d], g.d0[d]));
-    const double nxa = DOT ? fma(xa[0], n0, fma(xa[1], n1, xa[2] * n2)) : 0.0;
-    double in[NCH][NC];
-#pragma unroll
-    for (int c = 0; c < NCH; c++)
-#pragma unroll
-      for (int j = 0; j < NC; j++) in[c][j] = 0.0;
-#pragma unroll
-    for (int b = 0; b < P; b++) {
-      const double dx = xa[0] - yb[b][0], dy = xa[1] - yb[b][1], dz = xa[2] - yb[b][2];
-      const double r2 = fma(dx, dx, fma(dy, dy, dz * dz));
-      double kv[4];
-      eval_kernel<KK>(r2, nxa - nyb[b], k_re, k_imn, kv);
-#pragma unroll
-      for (int c = 0; c < NCH; c++)
-#pragma unroll
-        for (int j = 0; j < NC; j++) in[c][j] = fma(sd[CL ? 3 + j : 2][b], kv[c], in[c][j]);
-    }
-#pragma unroll
-    for (int c = 0; c < NCH; c++)
-#pragma unroll
-      for (int i = 0; i < NR; i++)
-#pragma unroll
-        for (int j = 0; j < NC; j++)
-          acc[c][i][j] = fma(sd[RL ? 3 + i : 2][a], in[c][j], acc[c][i][j]);
-  }
-}
-
-// FP32 variant of dist_pair_tensor (mixed-precision assembly): the pair geometry is formed in
+// One distant pair with the q^4 tensor rule in FP32 (mixed-precision assembly), summed column
+// side first (w = w_x w_y, as dist_pair_points): the pair geometry is formed in
 // FP64 relative to the column triangle's first vertex and rounded once; points, kernel values
 // (rsqrtf, sincosf, expf) and the q^4 sums run in FP32; the pair's sums are widened to FP64
 // before they are added to the tile.  Entries carry FP32 accuracy (~1e-7 relative).
@@ -559,7 +508,8 @@ __device__ __forceinline__ void stage_points(double (&st)[PT_ROWS][DIST_CHUNK], 
 // One distant pair with the q = 2 tensor rule from staged points, summed column side first:
 //   acc[c][i][j] = sum_a w_a phi_i(x_a) sum_b w_b phi_j(y_b) k_c(x_a, y_b).
 // The normal component of x_a - y_b takes the staged component on the normal's own triangle
-// and forms the other one here.  Same sum as dist_pair_tensor, from absolute points.
+// and forms the other one here.  Same sum as quad_point over the q^4 points, in another order
+// (differences at rounding level).
 template <int KK, bool RL, bool CL>
 __device__ __forceinline__ void dist_pair_points(const DistStagePts &sg, uint32_t ri, uint32_t ci,
                                                  double k_re, double k_imn,
@@ -756,11 +706,8 @@ __global__ void __launch_bounds__(dist_threads<KK>(), dist_minblocks<KK>())
           const double(&nn)[13][DIST_CHUNK] = row_normal<KK>() ? sg.r : sg.c;
           const uint32_t ni = row_normal<KK>() ? ri : ci;
           const double n0 = nn[10][ni], n1 = nn[11][ni], n2 = nn[12][ni];
-          if constexpr (Q > 0) {
-            if constexpr (F32)
-              dist_pair_tensor_f32<Q, KK, RL, CL>(g, n0, n1, n2, a.k_re, a.k_imn, acc);
-            else
-              dist_pair_tensor<Q, KK, RL, CL>(g, n0, n1, n2, a.k_re, a.k_imn, acc);
+          if constexpr (Q > 0) {  // q = 2 in FP32 (the FP64 kernels stage points)
+            dist_pair_tensor_f32<Q, KK, RL, CL>(g, n0, n1, n2, a.k_re, a.k_imn, acc);
           } else {
             for (int k = 0; k < nq; k++)
               quad_point<KK, RL, CL>(g, cx0[k], cx1[k], cy0[k], cy1[k], cw[k], n0, n1, n2,
