@@ -77,7 +77,7 @@ def build(force=False, verbose=False, defines=(), lib=LIB, build_dir=BUILD):
     if jobs or force or not os.path.exists(lib) or \
             any(os.path.getmtime(o) > os.path.getmtime(lib) for o in objs):
         tmp = lib + ".tmp"
-        _compile([nvcc, *ARCH, "-shared", "-o", tmp, *objs, "-lcuda", "-lm"])
+        _compile([nvcc, *ARCH, "-shared", "-o", tmp, *objs, "-lcuda", "-lpthread", "-lm"])
         os.replace(tmp, lib)
     return lib
 

@@ -1,6 +1,8 @@
 /* C-ABI wrappers of the host-side trees (no GPU involved). */
+#include <pthread.h>
 #include <stdlib.h>
 #include <string.h>
+#include <unistd.h>
 
 #include "h2b200_tree.h"
 
@@ -116,15 +118,120 @@ ctree_append(h2b_ctree *dst, const h2b_ctree *src, uint32_t ioff)
   return H2B_OK;
 }
 
+/* One surface of a forest: its trees, built with local vertex ids, are filled in by a worker
+ * thread; the surfaces are independent, so any number of threads gives the same forest. */
+typedef struct {
+  uint32_t surfaces;
+  const uint32_t *vertex_off, *triangle_off, *t;
+  const double *x;
+  int row_basis, col_basis;
+  uint32_t clf;
+  double eta;
+  h2b_tree *ones;
+  int *rc;
+  uint32_t next;
+} forest_job;
+
+static int
+forest_one(forest_job *j, uint32_t m, uint32_t **tl, size_t *tcap)
+{
+  const uint32_t v0 = j->vertex_off[m], nv = j->vertex_off[m + 1] - v0;
+  const uint32_t t0 = j->triangle_off[m], nt = j->triangle_off[m + 1] - t0;
+  h2b_tree *one = &j->ones[m];
+  size_t i;
+  int rc;
+  if (3 * (size_t) nt > *tcap) {
+    uint32_t *p = (uint32_t *) realloc(*tl, sizeof(uint32_t) * 3 * (size_t) nt);
+    if (!p)
+      return H2B_ERR_NOMEM;
+    *tl = p;
+    *tcap = 3 * (size_t) nt;
+  }
+  for (i = 0; i < 3 * (size_t) nt; i++)
+    (*tl)[i] = j->t[3 * (size_t) t0 + i] - v0;
+  rc = h2b_ctree_build(nv, j->x + 3 * (size_t) v0, nt, *tl, j->row_basis, j->clf, &one->row);
+  /* equal bases give equal trees, as in h2b_tree_new */
+  if (rc == H2B_OK)
+    rc = j->col_basis == j->row_basis
+             ? ctree_append(&one->col, &one->row, 0)
+             : h2b_ctree_build(nv, j->x + 3 * (size_t) v0, nt, *tl, j->col_basis, j->clf,
+                               &one->col);
+  if (rc == H2B_OK)
+    rc = h2b_blist_build(&one->row, &one->col, j->eta, &one->blocks);
+  return rc;
+}
+
+static void *
+forest_worker(void *arg)
+{
+  forest_job *j = (forest_job *) arg;
+  uint32_t *tl = NULL;
+  size_t tcap = 0;
+  for (;;) {
+    const uint32_t m = __atomic_fetch_add(&j->next, 1u, __ATOMIC_RELAXED);
+    if (m >= j->surfaces)
+      break;
+    j->rc[m] = forest_one(j, m, &tl, &tcap);
+  }
+  free(tl);
+  return NULL;
+}
+
+/* Host threads for the per-surface builds: the online cores, at most 32 and one per surface. */
+static uint32_t
+forest_threads(uint32_t surfaces)
+{
+  long c = sysconf(_SC_NPROCESSORS_ONLN);
+  uint32_t n = c > 0 ? (uint32_t) c : 1u;
+  if (n > 32u)
+    n = 32u;
+  return n < surfaces ? n : surfaces;
+}
+
+/* Append surface m's trees (already built) to the forest. */
+static int
+forest_append(h2b_tree *tr, const h2b_tree *one, uint32_t v0, uint32_t t0)
+{
+  const uint32_t rc0 = tr->row.n, cc0 = tr->col.n, b0 = tr->blocks.n;
+  const uint32_t nb = b0 + one->blocks.n;
+  uint32_t i;
+  uint32_t *prc, *pcc;
+  uint8_t *padm;
+  int rc = ctree_append(&tr->row, &one->row, tr->row_basis == H2B_BASIS_LINEAR ? v0 : t0);
+  if (rc == H2B_OK)
+    rc = ctree_append(&tr->col, &one->col, tr->col_basis == H2B_BASIS_LINEAR ? v0 : t0);
+  if (rc != H2B_OK)
+    return rc;
+  prc = (uint32_t *) realloc(tr->blocks.rc, sizeof(uint32_t) * nb);
+  if (prc)
+    tr->blocks.rc = prc;
+  pcc = prc ? (uint32_t *) realloc(tr->blocks.cc, sizeof(uint32_t) * nb) : NULL;
+  if (pcc)
+    tr->blocks.cc = pcc;
+  padm = pcc ? (uint8_t *) realloc(tr->blocks.adm, nb) : NULL;
+  if (padm)
+    tr->blocks.adm = padm;
+  if (!prc || !pcc || !padm)
+    return H2B_ERR_NOMEM;
+  for (i = 0; i < one->blocks.n; i++) {
+    tr->blocks.rc[b0 + i] = one->blocks.rc[i] + rc0;
+    tr->blocks.cc[b0 + i] = one->blocks.cc[i] + cc0;
+    tr->blocks.adm[b0 + i] = one->blocks.adm[i];
+  }
+  tr->blocks.n = nb;
+  return H2B_OK;
+}
+
 h2b_tree *
 h2b_tree_new_forest(uint32_t surfaces, const uint32_t *vertex_off, const uint32_t *triangle_off,
                     const double *x, const uint32_t *t, int row_basis, int col_basis, uint32_t clf,
                     double eta)
 {
   h2b_tree *tr;
-  uint32_t m, i;
-  uint32_t *tl = NULL;
-  size_t tcap = 0;
+  forest_job job;
+  pthread_t *th = NULL;
+  uint32_t m, i, nth, started = 0, bad = 0;
+  int rc = H2B_OK;
   if (!vertex_off || !triangle_off || !x || !t || surfaces == 0) {
     h2b_set_error("h2b_tree_new_forest: empty input");
     return NULL;
@@ -134,90 +241,84 @@ h2b_tree_new_forest(uint32_t surfaces, const uint32_t *vertex_off, const uint32_
     h2b_set_error("h2b_tree_new_forest: invalid basis or eta");
     return NULL;
   }
+  if (clf == 0) {
+    h2b_set_error("h2b_tree_new_forest: leaf size must be >= 1");
+    return NULL;
+  }
+  /* every surface is checked here, before any thread starts, so each error names its surface */
+  for (m = 0; m < surfaces; m++) {
+    const uint32_t v0 = vertex_off[m], nv = vertex_off[m + 1] - vertex_off[m];
+    const uint32_t t0 = triangle_off[m], nt = triangle_off[m + 1] - triangle_off[m];
+    if (vertex_off[m + 1] < vertex_off[m] || triangle_off[m + 1] < triangle_off[m] || nv == 0
+        || nt == 0) {
+      h2b_set_error("h2b_tree_new_forest: surface %u is empty or its offsets decrease", m);
+      return NULL;
+    }
+    for (i = 0; i < 3 * nt; i++) {
+      const uint32_t v = t[3 * (size_t) t0 + i];
+      if (v < v0 || v >= v0 + nv) {
+        h2b_set_error("h2b_tree_new_forest: triangle %u of surface %u has a vertex outside it",
+                      t0 + i / 3, m);
+        return NULL;
+      }
+    }
+  }
   tr = (h2b_tree *) calloc(1, sizeof(h2b_tree));
-  if (!tr) {
+  memset(&job, 0, sizeof(job));
+  job.ones = (h2b_tree *) calloc(surfaces, sizeof(h2b_tree));
+  job.rc = (int *) calloc(surfaces, sizeof(int));
+  nth = forest_threads(surfaces);
+  if (nth > 1)
+    th = (pthread_t *) malloc(sizeof(pthread_t) * (nth - 1));
+  if (!tr || !job.ones || !job.rc) {
+    free(th);
+    free(job.rc);
+    free(job.ones);
+    free(tr);
     h2b_set_error("h2b_tree_new_forest: out of host memory");
     return NULL;
   }
   tr->row_basis = row_basis;
   tr->col_basis = col_basis;
+  job.surfaces = surfaces;
+  job.vertex_off = vertex_off;
+  job.triangle_off = triangle_off;
+  job.t = t;
+  job.x = x;
+  job.row_basis = row_basis;
+  job.col_basis = col_basis;
+  job.clf = clf;
+  job.eta = eta;
+  /* the calling thread works too; a thread that cannot start leaves its share to the others */
+  for (i = 0; th && i + 1 < nth; i++)
+    if (pthread_create(&th[started], NULL, forest_worker, &job) == 0)
+      started++;
+  forest_worker(&job);
+  for (i = 0; i < started; i++)
+    pthread_join(th[i], NULL);
+  free(th);
   for (m = 0; m < surfaces; m++) {
-    const uint32_t v0 = vertex_off[m], nv = vertex_off[m + 1] - vertex_off[m];
-    const uint32_t t0 = triangle_off[m], nt = triangle_off[m + 1] - triangle_off[m];
-    h2b_tree one;
-    const uint32_t rc0 = tr->row.n, cc0 = tr->col.n, b0 = tr->blocks.n;
-    int rc;
-    if (vertex_off[m + 1] < vertex_off[m] || triangle_off[m + 1] < triangle_off[m] || nv == 0
-        || nt == 0) {
-      h2b_set_error("h2b_tree_new_forest: surface %u is empty or its offsets decrease", m);
-      free(tl);
-      h2b_tree_del(tr);
-      return NULL;
-    }
-    /* the surface's triangles with local vertex ids */
-    if (3 * (size_t) nt > tcap) {
-      uint32_t *p = (uint32_t *) realloc(tl, sizeof(uint32_t) * 3 * (size_t) nt);
-      if (!p) {
-        free(tl);
-        h2b_tree_del(tr);
-        h2b_set_error("h2b_tree_new_forest: out of host memory");
-        return NULL;
-      }
-      tl = p;
-      tcap = 3 * (size_t) nt;
-    }
-    for (i = 0; i < 3 * nt; i++) {
-      const uint32_t v = t[3 * (size_t) t0 + i];
-      if (v < v0 || v >= v0 + nv) {
-        free(tl);
-        h2b_tree_del(tr);
-        h2b_set_error("h2b_tree_new_forest: triangle %u of surface %u has a vertex outside it",
-                      t0 + i / 3, m);
-        return NULL;
-      }
-      tl[i] = v - v0;
-    }
-    memset(&one, 0, sizeof(one));
-    rc = h2b_ctree_build(nv, x + 3 * (size_t) v0, nt, tl, row_basis, clf, &one.row);
-    if (rc == H2B_OK)
-      rc = h2b_ctree_build(nv, x + 3 * (size_t) v0, nt, tl, col_basis, clf, &one.col);
-    if (rc == H2B_OK)
-      rc = h2b_blist_build(&one.row, &one.col, eta, &one.blocks);
-    if (rc == H2B_OK)
-      rc = ctree_append(&tr->row, &one.row, row_basis == H2B_BASIS_LINEAR ? v0 : t0);
-    if (rc == H2B_OK)
-      rc = ctree_append(&tr->col, &one.col, col_basis == H2B_BASIS_LINEAR ? v0 : t0);
     if (rc == H2B_OK) {
-      const uint32_t nb = b0 + one.blocks.n;
-      uint32_t *prc = (uint32_t *) realloc(tr->blocks.rc, sizeof(uint32_t) * nb);
-      uint32_t *pcc = prc ? (uint32_t *) realloc(tr->blocks.cc, sizeof(uint32_t) * nb) : NULL;
-      uint8_t *padm = pcc ? (uint8_t *) realloc(tr->blocks.adm, nb) : NULL;
-      if (prc) tr->blocks.rc = prc;
-      if (pcc) tr->blocks.cc = pcc;
-      if (padm) tr->blocks.adm = padm;
-      if (!prc || !pcc || !padm)
-        rc = H2B_ERR_NOMEM;
-      else {
-        for (i = 0; i < one.blocks.n; i++) {
-          tr->blocks.rc[b0 + i] = one.blocks.rc[i] + rc0;
-          tr->blocks.cc[b0 + i] = one.blocks.cc[i] + cc0;
-          tr->blocks.adm[b0 + i] = one.blocks.adm[i];
-        }
-        tr->blocks.n = nb;
-      }
+      rc = job.rc[m];
+      if (rc == H2B_OK)
+        rc = forest_append(tr, &job.ones[m], vertex_off[m], triangle_off[m]);
+      if (rc != H2B_OK)
+        bad = m;
     }
-    h2b_ctree_free(&one.row);
-    h2b_ctree_free(&one.col);
-    h2b_blist_free(&one.blocks);
-    if (rc != H2B_OK) {
-      free(tl);
-      h2b_tree_del(tr);
-      if (rc == H2B_ERR_NOMEM)
-        h2b_set_error("h2b_tree_new_forest: out of host memory");
-      return NULL;
-    }
+    h2b_ctree_free(&job.ones[m].row);
+    h2b_ctree_free(&job.ones[m].col);
+    h2b_blist_free(&job.ones[m].blocks);
   }
-  free(tl);
+  free(job.rc);
+  free(job.ones);
+  if (rc != H2B_OK) {
+    h2b_tree_del(tr);
+    if (rc == H2B_ERR_NOMEM)
+      h2b_set_error("h2b_tree_new_forest: out of host memory at surface %u", bad);
+    else
+      h2b_set_error("h2b_tree_new_forest: the trees of surface %u failed (code %d)", bad, rc);
+    return NULL;
+  }
   finish_tree(tr);
   return tr;
 }

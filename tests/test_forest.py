@@ -50,3 +50,44 @@ def test_forest_rejects_crossing_triangles():
     bad[1] -= 1   # the first surface's last vertex now belongs to the second
     with pytest.raises(hb.H2BError):
         hb.build_forest(gu, bad, toff, L, L, 16, 1.4)
+
+
+def test_forest_many_surfaces_mixed_bases():
+    """More surfaces than host threads, unequal sizes and constant rows beside linear columns:
+    the surfaces are built on several threads and appended in order, so each part of the forest
+    (both cluster trees and the blocks) is the tree of its surface alone, shifted."""
+    rng = np.random.default_rng(3)
+    surfs = [hb.new_ellipsoid_surface3d(int(s), rng.uniform(0.5, 2.0, 3))
+             for s in rng.integers(2, 9, 70)]
+    gu, voff, toff = hb.union_surface3d(surfs)
+    forest = hb.build_forest(gu, voff, toff, Cb, L, 8, 1.2)
+    blocks_f = forest.block_records().astype(np.int64)
+    for which, offs in ((0, toff), (1, voff)):
+        rec_f, box_f, idx_f = forest.clusters(which)
+        c0 = 0
+        for m, gr in enumerate(surfs):
+            rec, box, idx = hb.build_tree(gr, Cb, L, 8, 1.2).clusters(which)
+            ioff, n = int(offs[m]), rec.shape[0]
+            part = rec_f[c0:c0 + n].astype(np.int64)
+            np.testing.assert_array_equal(part[:, 0] - ioff, rec[:, 0])
+            np.testing.assert_array_equal(part[:, 1:], rec[:, 1:])
+            np.testing.assert_array_equal(box_f[c0:c0 + n], box)
+            np.testing.assert_array_equal(idx_f[ioff:ioff + idx.size].astype(np.int64) - ioff,
+                                          idx)
+            c0 += n
+        assert c0 == (forest.row_clusters if which == 0 else forest.col_clusters)
+    b0 = 0
+    for m, gr in enumerate(surfs):
+        one = hb.build_tree(gr, Cb, L, 8, 1.2)
+        bf = blocks_f[b0:b0 + one.blocks].copy()
+        bf[:, 0] -= int(toff[m])
+        bf[:, 2] -= int(voff[m])
+        np.testing.assert_array_equal(bf, one.block_records())
+        b0 += one.blocks
+    assert b0 == forest.blocks
+
+
+def test_forest_rejects_zero_leaf_size():
+    gu, voff, toff = hb.union_surface3d(_surfaces()[:2])
+    with pytest.raises(hb.H2BError, match="leaf size"):
+        hb.build_forest(gu, voff, toff, L, L, 0, 1.4)
