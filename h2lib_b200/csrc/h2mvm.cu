@@ -329,30 +329,43 @@ __global__ void __launch_bounds__(MAXTHREADS) mv_items_kernel(MvLaunch L) {
       span16(pa, n, lo, delta, bytes);
       const int t = m.flags & H2B_MV_KIND;
       const size_t xn = (size_t) W * sizeof(double) * ((m.flags & H2B_MV_TRANS) ? m.rows : m.cols);
-      uint32_t total = bytes;
+      // only the columns whose system is still running are copied; an item with none (its
+      // surface's systems have all stopped) loads nothing and its stage completes at once
+      uint32_t total = 0;
+      bool any = false;
       for (uint32_t q = 0; q < L.nrhs; q++) {
+        if (!col_on(L.mask, L.nseg, m.seg, q)) continue;
         const char *xl;
         uint32_t xd, xb;
         span16(L.X[t] + q * L.sx[t] + (size_t) W * m.xo, xn, xl, xd, xb);
         total += xb;
+        any = true;
       }
-      const uint32_t dst = smem_addr(stage0 + (size_t) s * L.stage_bytes);
-      // the generic-proxy reads of the stage's previous contents are ordered before these copies
-      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-      asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(total)
-                   : "memory");
-      asm volatile(
-          "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
-          ::"r"(dst), "l"(lo), "r"(bytes), "r"(bar)
-          : "memory");
-      for (uint32_t q = 0; q < L.nrhs; q++) {
-        const char *xl;
-        uint32_t xd, xb;
-        span16(L.X[t] + q * L.sx[t] + (size_t) W * m.xo, xn, xl, xd, xb);
+      if (!any) {
+        asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
+      } else {
+        total += bytes;
+        const uint32_t dst = smem_addr(stage0 + (size_t) s * L.stage_bytes);
+        // the generic-proxy reads of the stage's previous contents are ordered before these
+        // copies
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar),
+                     "r"(total)
+                     : "memory");
         asm volatile(
-            "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
-            ::"r"(dst + L.panel_bytes + q * L.xcol_bytes), "l"(xl), "r"(xb), "r"(bar)
+            "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, "
+            "[%3];" ::"r"(dst), "l"(lo), "r"(bytes), "r"(bar)
             : "memory");
+        for (uint32_t q = 0; q < L.nrhs; q++) {
+          if (!col_on(L.mask, L.nseg, m.seg, q)) continue;
+          const char *xl;
+          uint32_t xd, xb;
+          span16(L.X[t] + q * L.sx[t] + (size_t) W * m.xo, xn, xl, xd, xb);
+          asm volatile(
+              "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, "
+              "[%3];" ::"r"(dst + L.panel_bytes + q * L.xcol_bytes), "l"(xl), "r"(xb), "r"(bar)
+              : "memory");
+        }
       }
       if (i + 1 < mine) m = L.items[L.first + blockIdx.x + (i + 1) * gridDim.x];
     }
