@@ -269,13 +269,22 @@ class H2Matrix:
     """Device H2 matrix with Chebyshev interpolation (setup_h2matrix_aprx_inter_bem3d,
     Library/bem3d.c:9658)."""
 
-    def __init__(self, bem, tree, m, like=None):
+    def __init__(self, bem, tree, m, like=None, green=None):
         """like: an H2Matrix on the same surface, trees, bases and quadrature whose device
-        structure this one shares (h2b_h2matrix_new_like); it is kept alive by this object."""
+        structure this one shares (h2b_h2matrix_new_like); it is kept alive by this object.
+        green: (l, delta, accur) for the greenhybrid farfield with m Gauss points on each of l
+        parts per box-face axis (setup_h2matrix_aprx_greenhybrid_bem3d, Library/bem3d.c:9689);
+        a matrix made like a greenhybrid one is greenhybrid too."""
         self.bem, self.tree, self.m, self._like = bem, tree, m, like
+        self.green = green if like is None else like.green
         if like is not None:
             self.handle = checkp(lib.h2b_h2matrix_new_like(bem.handle, like.handle),
                                  "h2matrix_new_like")
+        elif green is not None:
+            l, delta, accur = green
+            self.handle = checkp(lib.h2b_h2matrix_new_greenhybrid(bem.handle, tree.handle, m, l,
+                                                                  delta, accur),
+                                 "h2matrix_new_greenhybrid")
         else:
             self.handle = checkp(lib.h2b_h2matrix_new(bem.handle, tree.handle, m),
                                  "h2matrix_new")
@@ -342,6 +351,13 @@ class H2Matrix:
         c = np.zeros(4, dtype=np.uint64)
         check(lib.h2b_h2matrix_pair_counts(self.handle, c), "pair_counts")
         return dict(zip(("distant", "vertex", "edge", "identical"), (int(v) for v in c)))
+
+    def green_ranks(self, side=0):
+        """Ranks of the greenhybrid cluster bases (0 row, 1 column), tree pre-order."""
+        n = self.tree.row_clusters if side == 0 else self.tree.col_clusters
+        out = np.zeros(n, dtype=np.uint32)
+        check(lib.h2b_h2matrix_green_ranks(self.handle, side, _ptr(out)), "green_ranks")
+        return out
 
     def unique_pairs(self):
         """Distinct triangle pairs among pair_counts(), by the same cases (device bitmap)."""

@@ -8,6 +8,7 @@
 #include <vector>
 
 #include "api_h2.h"
+#include "green.h"
 
 // ------------------------------------------------------------------------------------------
 // helpers
@@ -56,6 +57,7 @@ static void devtree_free(DevCTree &t, cudaStream_t st) {
   dfree(t.d_W, st); dfree(t.d_woff, st); dfree(t.d_fitems, st); dfree(t.d_wleaves, st);
   dfree(t.d_ppairs, st); dfree(t.d_pfirst, st); dfree(t.d_P, st);
   dfree(t.d_seg, st);
+  dfree(t.d_gbox, st); dfree(t.d_glev, st); dfree(t.d_gflat, st);
 }
 
 // Flattened bases: W_t for the clusters of admissible blocks (`adm`, ids of this tree) and all
@@ -204,7 +206,7 @@ extern "C" void h2b_h2matrix_del(h2b_h2matrix *h) {
   // the operator's own data
   for (DevCTree *t : {&h->rt, &h->ct}) {
     dfree(t->d_V, st); dfree(t->d_E, st); dfree(t->d_W, st); dfree(t->d_P, st);
-    dfree(t->f_W, st);
+    dfree(t->f_W, st); dfree(t->d_grank, st); dfree(t->d_gpiv, st); dfree(t->d_gE, st);
   }
   dfree(h->f_N, st); dfree(h->f_S, st); dfree(h->d_S, st); dfree(h->d_N, st);
   dfree(h->d_xp, st); dfree(h->d_yp, st); dfree(h->d_xt, st); dfree(h->d_yt, st);
@@ -244,15 +246,10 @@ static int classify_singular(h2b_h2matrix *h, uint64_t all_pairs) {
   return H2B_OK;
 }
 
-extern "C" h2b_h2matrix *h2b_h2matrix_new(const h2b_bem *bem, const h2b_tree *tree, uint32_t m) {
-  if (!bem || !tree) {
-    h2b_set_error("h2b_h2matrix_new: NULL operator or tree");
-    return NULL;
-  }
-  if (m < 1 || m > 5) {
-    h2b_set_error("h2b_h2matrix_new: interpolation order %u outside 1..5", m);
-    return NULL;
-  }
+// The structure of an H2 matrix of rank k (every cluster basis padded to k columns); m is the
+// interpolation order of the Chebyshev path (1 for the greenhybrid bases, which use no nodes).
+static h2b_h2matrix *h2matrix_create(const h2b_bem *bem, const h2b_tree *tree, uint32_t m,
+                                     uint32_t k) {
   const uint32_t nr = h2b_bem_rows(bem), nc = h2b_bem_cols(bem);
   if (tree->row.nidx != nr || tree->col.nidx != nc) {
     h2b_set_error("h2b_h2matrix_new: tree index sets (%u, %u) do not match the operator (%u, %u)",
@@ -264,7 +261,7 @@ extern "C" h2b_h2matrix *h2b_h2matrix_new(const h2b_bem *bem, const h2b_tree *tr
   h->bem = bem;
   h->tree = tree;
   h->m = m;
-  h->k = m * m * m;
+  h->k = k;
   h->cx = bem->pde == H2B_HELMHOLTZ;
   h->num_sms = bem->s->num_sms;
   int rc = H2B_OK;
@@ -372,6 +369,121 @@ extern "C" h2b_h2matrix *h2b_h2matrix_new(const h2b_bem *bem, const h2b_tree *tr
   return h;
 }
 
+extern "C" h2b_h2matrix *h2b_h2matrix_new(const h2b_bem *bem, const h2b_tree *tree, uint32_t m) {
+  if (!bem || !tree) {
+    h2b_set_error("h2b_h2matrix_new: NULL operator or tree");
+    return NULL;
+  }
+  if (m < 1 || m > 5) {
+    h2b_set_error("h2b_h2matrix_new: interpolation order %u outside 1..5", m);
+    return NULL;
+  }
+  return h2matrix_create(bem, tree, m, m * m * m);
+}
+
+// Per operator: ranks, pivots and transfers of the greenhybrid bases of one tree.
+static int green_alloc(DevCTree &t, uint32_t k, cudaStream_t st) {
+  H2B_CUDA_TRY(cudaMallocAsync(&t.d_grank, sizeof(uint32_t) * t.n, st));
+  H2B_CUDA_TRY(cudaMallocAsync(&t.d_gpiv, sizeof(uint32_t) * (size_t) t.n * k, st));
+  H2B_CUDA_TRY(cudaMallocAsync(&t.d_gE, sizeof(double) * (size_t) t.n * k * k, st));
+  return H2B_OK;
+}
+
+// Structure of the greenhybrid bases of one tree: boxes, clusters by level (deepest first) with
+// the rows bound of A_t (a leaf's size; a father's size, at most the 2k pivot rows of its two
+// sons), and the needed non-leaf clusters (flattened bases) by level.
+static int green_setup(DevCTree &t, const h2b_ctree &c, uint32_t k, cudaStream_t st) {
+  uint32_t maxlev = 0;
+  for (uint32_t i = 0; i < c.n; i++) maxlev = std::max(maxlev, c.level[i]);
+  std::vector<char> need(c.n, 0);
+  for (uint32_t i = 0; i < c.n; i++)
+    need[i] = t.h_adm[i] || (c.father[i] != UINT32_MAX && need[c.father[i]]);
+  std::vector<uint32_t> lev, flat;
+  std::vector<double> box((size_t) c.n * 6);
+  t.h_glev_off.assign(1, 0);
+  t.h_gflat_off.assign(1, 0);
+  t.h_glev_rows.clear();
+  for (uint32_t L = maxlev + 1; L-- > 0;) {
+    uint32_t rows = 1;
+    for (uint32_t i = 0; i < c.n; i++) {
+      if (c.level[i] != L) continue;
+      lev.push_back(i);
+      rows = std::max(rows, c.sons[i] == 0 ? c.size[i] : std::min(c.size[i], 2 * k));
+      if (c.sons[i] != 0 && need[i]) flat.push_back(i);
+    }
+    t.h_glev_off.push_back((uint32_t) lev.size());
+    t.h_gflat_off.push_back((uint32_t) flat.size());
+    t.h_glev_rows.push_back(rows);
+  }
+  for (uint32_t i = 0; i < c.n; i++)
+    for (int d = 0; d < 3; d++) {
+      box[6 * (size_t) i + d] = c.bmin[3 * (size_t) i + d];
+      box[6 * (size_t) i + 3 + d] = c.bmax[3 * (size_t) i + d];
+    }
+  int rc;
+  if ((rc = upload(&t.d_gbox, box, st)) || (rc = upload(&t.d_glev, lev, st)) ||
+      (rc = upload(&t.d_gflat, flat, st)))
+    return rc;
+  return green_alloc(t, k, st);
+}
+
+extern "C" h2b_h2matrix *h2b_h2matrix_new_greenhybrid(const h2b_bem *bem, const h2b_tree *tree,
+                                                      uint32_t m, uint32_t l, double delta,
+                                                      double accur) {
+  if (!bem || !tree) {
+    h2b_set_error("h2b_h2matrix_new_greenhybrid: NULL operator or tree");
+    return NULL;
+  }
+  if (bem->pde != H2B_LAPLACE || (bem->layer != H2B_SLP && bem->layer != H2B_DLP)) {
+    h2b_set_error("h2b_h2matrix_new_greenhybrid: built for the Laplace single and double layer");
+    return NULL;
+  }
+  if (m < 1 || l < 1 || m * l > H2B_GREEN_MLMAX || !(accur > 0.0) || !(delta >= 0.0)) {
+    h2b_set_error("h2b_h2matrix_new_greenhybrid: m %u, l %u (m l at most %d), delta %g, "
+                  "accuracy %g", m, l, H2B_GREEN_MLMAX, delta, accur);
+    return NULL;
+  }
+  // the one-dimensional rule: m Gauss points on each of l equal parts of [-1, 1]
+  // (setup_green_bem3d, Library/bem3d.c:4999)
+  double g01[H2B_GREEN_MLMAX], w01[H2B_GREEN_MLMAX], ht[H2B_GREEN_MLMAX], hw[H2B_GREEN_MLMAX];
+  if (m == 1) {
+    ht[0] = 0.0;
+    hw[0] = 2.0;
+  } else {
+    if (h2b_gauss_legendre01(m, g01, w01) != H2B_OK) return NULL;
+    for (uint32_t i = 0; i < m; i++) {
+      ht[i] = 2.0 * g01[i] - 1.0;
+      hw[i] = 2.0 * w01[i];
+    }
+  }
+  const uint32_t ml = m * l, k = 12 * ml * ml;
+  h2b_h2matrix *h = h2matrix_create(bem, tree, 1, k);
+  if (!h) return NULL;
+  h->green = 1;
+  h->g_ml = (int) ml;
+  h->g_delta = delta;
+  h->g_accur = accur;
+  const double cw = 2.0 / (double) l;
+  for (uint32_t j = 1; j <= l; j++) {
+    const double s0 = -1.0 + cw * (j - 1), s1 = -1.0 + cw * j, hh = 0.5 * (s1 - s0);
+    for (uint32_t i = 0; i < m; i++) {
+      h->g_tg[i + (j - 1) * m] = hh * ht[i] + 0.5 * (s1 + s0);
+      h->g_wg[i + (j - 1) * m] = hh * hw[i];
+    }
+  }
+  int rc = green_setup(h->rt, tree->row, k, h->st);
+  if (rc == H2B_OK) rc = green_setup(h->ct, tree->col, k, h->st);
+  if (rc == H2B_OK && cudaStreamSynchronize(h->st) != cudaSuccess) {
+    h2b_set_error("h2b_h2matrix_new_greenhybrid: %s", cudaGetErrorString(cudaGetLastError()));
+    rc = H2B_ERR_CUDA;
+  }
+  if (rc != H2B_OK) {
+    h2b_h2matrix_del(h);
+    return NULL;
+  }
+  return h;
+}
+
 extern "C" h2b_h2matrix *h2b_h2matrix_new_like(const h2b_bem *bem, const h2b_h2matrix *like) {
   if (!bem || !like) {
     h2b_set_error("h2b_h2matrix_new_like: NULL operator or matrix");
@@ -401,7 +513,11 @@ extern "C" h2b_h2matrix *h2b_h2matrix_new_like(const h2b_bem *bem, const h2b_h2m
   h->f_S = h->f_N = nullptr;
   h->d_S = h->d_N = h->d_xp = h->d_yp = h->d_xt = h->d_yt = h->d_xio = h->d_yio = nullptr;
   h->d_mverr = nullptr;
-  for (DevCTree *t : {&h->rt, &h->ct}) t->d_V = t->d_E = t->d_W = t->d_P = nullptr, t->f_W = nullptr;
+  for (DevCTree *t : {&h->rt, &h->ct}) {
+    t->d_V = t->d_E = t->d_W = t->d_P = t->d_gE = nullptr;
+    t->f_W = nullptr;
+    t->d_grank = t->d_gpiv = nullptr;
+  }
   int rc = H2B_OK;
   if (cudaStreamCreateWithFlags(&h->st, cudaStreamNonBlocking) != cudaSuccess) rc = H2B_ERR_CUDA;
   for (int e = 0; rc == H2B_OK && e < 12; e++)
@@ -421,6 +537,8 @@ extern "C" h2b_h2matrix *h2b_h2matrix_new_like(const h2b_bem *bem, const h2b_h2m
                         h->st))
       rc = H2B_ERR_NOMEM;
   }
+  for (DevCTree *t : {&h->rt, &h->ct})
+    if (rc == H2B_OK && h->green) rc = green_alloc(*t, h->k, h->st);
   if (rc == H2B_OK &&
       (cudaMallocAsync(&h->d_S, sizeof(double) * W * std::max<uint64_t>(h->nadm * kk, 1) + H2B_MV_SLACK, h->st) ||
        cudaMallocAsync(&h->d_N, sizeof(double) * W * std::max<uint64_t>(h->near_total, 1) + H2B_MV_SLACK, h->st) ||
@@ -605,6 +723,64 @@ static int assemble_basis(h2b_h2matrix *h, DevCTree &t, int basis, int dn) {
   return rc;
 }
 
+// Greenhybrid bases of one tree: ranks, pivots and transfers level by level (deepest first),
+// then the flattened bases (the leaves' copies, then the fathers' rows level by level).
+static int green_basis(h2b_h2matrix *h, DevCTree &t, int basis, int dcol) {
+  const int transposed = (&t == &h->ct);
+  const uint32_t K = h->k;
+  H2B_CUDA_TRY(cudaMemsetAsync(t.d_gE, 0, sizeof(double) * (size_t) t.n * K * K, h->st));
+  GreenArgs g;
+  memset(&g, 0, sizeof(g));
+  g.tri = h->bem->s->d_tri;
+  g.vt_off = h->bem->s->d_vt_off;
+  g.vt_tri = h->bem->s->d_vt_tri;
+  g.xs = h->d_xs;
+  g.ys = h->d_ys;
+  g.ws = h->d_ws;
+  g.wsl = h->d_wsl;
+  g.ns = (int) h->ns;
+  g.linear = basis == H2B_BASIS_LINEAR;
+  g.dcol = dcol;
+  g.transposed = transposed;
+  g.kconst = h->bem->kconst;
+  g.off = t.d_off;
+  g.size = t.d_size;
+  g.son0 = t.d_son0;
+  g.son1 = t.d_son1;
+  g.idx = t.d_idx;
+  g.box = t.d_gbox;
+  g.voff = t.d_voff;
+  memcpy(g.tg, h->g_tg, sizeof(g.tg));
+  memcpy(g.wg, h->g_wg, sizeof(g.wg));
+  g.ml = h->g_ml;
+  g.K = (int) K;
+  g.delta = h->g_delta;
+  g.accur = h->g_accur;
+  g.rank = t.d_grank;
+  g.piv = t.d_gpiv;
+  g.V = t.d_V;
+  g.E = t.d_gE;
+  int rc = H2B_OK;
+  for (size_t L = 0; rc == H2B_OK && L + 1 < t.h_glev_off.size(); L++) {
+    g.clusters = t.d_glev + t.h_glev_off[L];
+    g.n = t.h_glev_off[L + 1] - t.h_glev_off[L];
+    g.max_rows = t.h_glev_rows[L];
+    rc = h2b_green_basis(&g, h->st);
+  }
+  if (rc != H2B_OK) return rc;
+  FlatLeafArgs la{t.d_wleaves, t.d_size, t.d_voff, t.d_woff, t.d_V, t.d_W, t.nwleaves, (int) K,
+                  !transposed};
+  rc = h2b_flat_leaves(&la, h->st);
+  GreenFlatArgs fa{nullptr, 0, t.d_off, t.d_size, t.d_son0, t.d_son1, t.d_grank, t.d_woff,
+                   t.d_gE, t.d_W, (int) K};
+  for (size_t L = 0; rc == H2B_OK && L + 1 < t.h_gflat_off.size(); L++) {
+    fa.clusters = t.d_gflat + t.h_gflat_off[L];
+    fa.n = t.h_gflat_off[L + 1] - t.h_gflat_off[L];
+    rc = h2b_green_flatten(&fa, h->st);
+  }
+  return rc;
+}
+
 // Phase timings: events 2i / 2i+1 bracket phase i (0 row basis, 1 column basis, 2 coupling,
 // 3 nearfield; event 7 separates the distant and singular nearfield kernels; 9/10 the matvec).
 static void mark(h2b_h2matrix *h, int e) { cudaEventRecord(h->ev[e], h->st); }
@@ -732,7 +908,8 @@ static int row_basis(h2b_h2matrix *h) {
   mark(h, 0);
   // row side: Lagrange polynomials (assemble_bem3d_lagrange_{c,l}_amatrix); normal derivatives
   // for the adjoint double layer (assemble_bem3d_dn_lagrange_*, Library/laplacebem3d.c:1180)
-  int rc = assemble_basis(h, h->rt, h->bem->row_basis, h->bem->layer == H2B_ADLP);
+  int rc = h->green ? green_basis(h, h->rt, h->bem->row_basis, 0)
+                    : assemble_basis(h, h->rt, h->bem->row_basis, h->bem->layer == H2B_ADLP);
   mark(h, 1);
   return rc;
 }
@@ -740,13 +917,25 @@ static int row_basis(h2b_h2matrix *h) {
 static int col_basis(h2b_h2matrix *h) {
   mark(h, 2);
   // column side of the double layer: normal derivatives (assemble_bem3d_dn_lagrange_*)
-  int rc = assemble_basis(h, h->ct, h->bem->col_basis, h->bem->layer == H2B_DLP);
+  int rc = h->green ? green_basis(h, h->ct, h->bem->col_basis, h->bem->layer == H2B_DLP)
+                    : assemble_basis(h, h->ct, h->bem->col_basis, h->bem->layer == H2B_DLP);
   mark(h, 3);
   return rc;
 }
 
 static int coupling(h2b_h2matrix *h) {
   mark(h, 4);
+  if (h->green) {
+    GreenCouplingArgs ga{h->bem->s->d_tri, h->bem->s->d_vt_off, h->bem->s->d_vt_tri,
+                         h->d_adm_rc, h->d_adm_cc, h->rt.d_grank, h->rt.d_gpiv, h->ct.d_grank,
+                         h->ct.d_gpiv, h->d_S, h->nadm, (int) h->k, (int) h->bem->q,
+                         h->bem->row_basis == H2B_BASIS_LINEAR,
+                         h->bem->col_basis == H2B_BASIS_LINEAR, h->bem->layer == H2B_DLP,
+                         h->bem->kconst};
+    const int rc = h2b_green_coupling(&ga, h->st);
+    mark(h, 5);
+    return rc;
+  }
   FarCouplingArgs ca{h->d_adm_rc, h->d_adm_cc, h->rt.d_pts, h->ct.d_pts, h->d_S, h->nadm,
                      (int) h->m, (int) h->k, h->bem->kconst, h->bem->k_re, -h->bem->k_im};
   int rc = h2b_far_coupling(&ca, h->cx, h->st);
@@ -835,6 +1024,22 @@ extern "C" int h2b_h2matrix_assemble_all(h2b_h2matrix *h) {
   if (rc == H2B_OK) rc = coupling(h);
   if (rc == H2B_OK) rc = launch_near(h, nullptr);
   return finish(h, rc, 1 | 2 | 4 | 8);
+}
+
+extern "C" int h2b_h2matrix_green_ranks(const h2b_h2matrix *h, int side, uint32_t *ranks) {
+  if (!h || !ranks || (side != 0 && side != 1)) {
+    h2b_set_error("h2b_h2matrix_green_ranks: NULL matrix or output, or side not 0 / 1");
+    return H2B_ERR_ARG;
+  }
+  if (!h->green) {
+    h2b_set_error("h2b_h2matrix_green_ranks: not a greenhybrid H2 matrix");
+    return H2B_ERR_ARG;
+  }
+  const DevCTree &t = side ? h->ct : h->rt;
+  H2B_CUDA_TRY(cudaMemcpyAsync(ranks, t.d_grank, sizeof(uint32_t) * t.n, cudaMemcpyDeviceToHost,
+                               h->st));
+  H2B_CUDA_TRY(cudaStreamSynchronize(h->st));
+  return H2B_OK;
 }
 
 extern "C" int h2b_h2matrix_timings(const h2b_h2matrix *h, double ms[6]) {

@@ -42,12 +42,25 @@ struct DevCTree {
   uint32_t *d_seg = nullptr;
   std::vector<uint32_t> roots;
   const uint32_t *h_idx = nullptr, *h_off = nullptr, *h_size = nullptr;  // the host tree
+  // greenhybrid bases (green.cu).  Structure: per cluster box (bmin, bmax), the clusters by
+  // level (deepest first, with a bound on the rows of A_t per level) and the needed non-leaf
+  // clusters by level.  Per operator: ranks, pivots (K per cluster), transfers (K x K).
+  double *d_gbox = nullptr;
+  uint32_t *d_glev = nullptr, *d_gflat = nullptr;
+  std::vector<uint32_t> h_glev_off, h_glev_rows, h_gflat_off;
+  uint32_t *d_grank = nullptr, *d_gpiv = nullptr;
+  double *d_gE = nullptr;
 };
 
 struct h2b_h2matrix {
   const h2b_bem *bem = nullptr;
   const h2b_tree *tree = nullptr;
   uint32_t m = 0, k = 0, ns = 0;
+  // greenhybrid farfield (h2b_h2matrix_new_greenhybrid): points per axis and face ml = m l, the
+  // one-dimensional rule on [-1, 1], the box widening delta and the ACA accuracy; k = 12 ml^2
+  int green = 0;
+  int g_ml = 0;
+  double g_tg[9] = {}, g_wg[9] = {}, g_delta = 0.0, g_accur = 0.0;
   int cx = 0, num_sms = 148;
   int quad_fp32 = 0;  // distant-pair quadrature in FP32 (h2b_h2matrix_set_precision)
   // matvec work items (h2mvm.h), owned by the structure's owner, and the knobs they were built

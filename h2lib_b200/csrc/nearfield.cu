@@ -28,6 +28,7 @@
 #include <type_traits>
 
 #include "device_common.cuh"
+#include "green.h"
 #include "h2b200_plan.h"
 #include "nearfield.h"
 
@@ -1385,6 +1386,86 @@ extern "C" int h2b_near_unique_pairs(const void *tri, const void *refs, const h2
   cudaFreeAsync(bitmap, st);
   for (int c = 0; c < 4; c++) counts[c] = host[c];
   return rc;
+}
+
+// Greenhybrid coupling matrices S_b(i, j) = A(xihat_r[i], xihat_c[j]): the operator's entries
+// between the pivot rows of the row cluster and the pivot columns of the column cluster
+// (assemble_bem3d_greenhybrid_uniform, Library/bem3d.c:6493, through nearfield_far =
+// assemble_{cc,ll}_far_bem3d, :1439 / :3264), the distant rule on every pair of triangles of the
+// two basis functions.  K x K column-major per block, zero past the ranks.
+template <bool RL, bool CL, bool DLP>
+__global__ void __launch_bounds__(256) green_coupling_kernel(GreenCouplingArgs a) {
+  const uint32_t b = blockIdx.x;
+  const uint32_t rc = a.adm_rc[b], cc = a.adm_cc[b];
+  const uint32_t K = (uint32_t) a.K, kr = a.rrank[rc], kc = a.crank[cc];
+  const uint32_t *pr = a.rpiv + (size_t) rc * K, *pc = a.cpiv + (size_t) cc * K;
+  double *S = a.S + (size_t) b * K * K;
+  const int q = a.q, np = q * q * q * q, o = dist_off(q);
+  for (uint32_t e = threadIdx.x; e < K * K; e += blockDim.x) {
+    const uint32_t i = e % K, j = e / K;
+    double acc = 0.0;
+    if (i < kr && j < kc) {
+      const uint32_t bi = pr[i], bj = pc[j];
+      const uint32_t t0 = RL ? a.vt_off[bi] : 0u, t1 = RL ? a.vt_off[bi + 1] : 1u;
+      const uint32_t u0 = CL ? a.vt_off[bj] : 0u, u1 = CL ? a.vt_off[bj + 1] : 1u;
+      for (uint32_t ti = t0; ti < t1; ti++) {
+        const TriRec &T = a.tri[RL ? a.vt_tri[ti] : bi];
+        const int ct = RL ? (T.v[0] == bi ? 0 : (T.v[1] == bi ? 1 : 2)) : 0;
+        for (uint32_t si = u0; si < u1; si++) {
+          const TriRec &Sx = a.tri[CL ? a.vt_tri[si] : bj];
+          const int cs = CL ? (Sx.v[0] == bj ? 0 : (Sx.v[1] == bj ? 1 : 2)) : 0;
+          double sum = 0.0;
+          for (int p = 0; p < np; p++) {
+            const double tx = c_dist[0][o + p], sx = c_dist[1][o + p];
+            const double ty = c_dist[2][o + p], sy = c_dist[3][o + p], w = c_dist[4][o + p];
+            const double ax = 1.0 - tx, bx = tx - sx, cx = sx;
+            const double ay = 1.0 - ty, by = ty - sy, cy = sy;
+            const double d0 = (T.a[0] * ax + T.b[0] * bx + T.c[0] * cx) -
+                              (Sx.a[0] * ay + Sx.b[0] * by + Sx.c[0] * cy);
+            const double d1 = (T.a[1] * ax + T.b[1] * bx + T.c[1] * cx) -
+                              (Sx.a[1] * ay + Sx.b[1] * by + Sx.c[1] * cy);
+            const double d2 = (T.a[2] * ax + T.b[2] * bx + T.c[2] * cx) -
+                              (Sx.a[2] * ay + Sx.b[2] * by + Sx.c[2] * cy);
+            const double ri = rsqrt_nr(d0 * d0 + d1 * d1 + d2 * d2);
+            const double f =
+                DLP ? (d0 * Sx.n[0] + d1 * Sx.n[1] + d2 * Sx.n[2]) * (ri * ri * ri) : ri;
+            const double pr_ = RL ? (ct == 0 ? ax : (ct == 1 ? bx : cx)) : 1.0;
+            const double pc_ = CL ? (cs == 0 ? ay : (cs == 1 ? by : cy)) : 1.0;
+            sum += w * pr_ * pc_ * f;
+          }
+          acc += sum * (T.g * Sx.g * a.kconst);
+        }
+      }
+    }
+    S[i + (size_t) j * K] = acc;
+  }
+}
+
+template <bool RL, bool CL, bool DLP>
+static int launch_green_coupling(const GreenCouplingArgs *a, cudaStream_t st) {
+  green_coupling_kernel<RL, CL, DLP><<<a->n, 256, 0, st>>>(*a);
+  h2b_note_launch();
+  H2B_CUDA_TRY(cudaGetLastError());
+  return H2B_OK;
+}
+
+template <bool RL, bool CL>
+static int launch_green_coupling_l(const GreenCouplingArgs *a, cudaStream_t st) {
+  return a->dlp ? launch_green_coupling<RL, CL, true>(a, st)
+                : launch_green_coupling<RL, CL, false>(a, st);
+}
+
+extern "C" int h2b_green_coupling(const GreenCouplingArgs *a, cudaStream_t st) {
+  if (a->n == 0) return H2B_OK;
+  if (a->q < 1 || a->q > 5) {
+    h2b_set_error("greenhybrid coupling: quadrature order %d outside 1..5", a->q);
+    return H2B_ERR_ARG;
+  }
+  if (a->rlinear)
+    return a->clinear ? launch_green_coupling_l<true, true>(a, st)
+                      : launch_green_coupling_l<true, false>(a, st);
+  return a->clinear ? launch_green_coupling_l<false, true>(a, st)
+                    : launch_green_coupling_l<false, false>(a, st);
 }
 
 extern "C" int h2b_near_upload_dist_rules(void) {

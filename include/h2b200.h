@@ -232,6 +232,21 @@ h2b_h2matrix *h2b_h2matrix_new(const h2b_bem *bem, const h2b_tree *tree, uint32_
  * coupling and nearfield storage are allocated.  `like` must outlive the new matrix.  No
  * reference counterpart (H2Lib builds the cluster bases of each operator separately). */
 h2b_h2matrix *h2b_h2matrix_new_like(const h2b_bem *bem, const h2b_h2matrix *like);
+/* H2 matrix with the greenhybrid farfield (setup_h2matrix_aprx_greenhybrid_bem3d,
+ * Library/bem3d.c:9689, with the cube quadrature points build_bem3d_cube_quadpoints, :5063):
+ * m Gauss points on each of l parts per axis of every face of the cluster box widened by
+ * delta * (largest box side), cluster bases from full-pivoting ACA to the accuracy `accur` of the
+ * kernel matrix on those points, coupling matrices = the operator's entries between the pivot
+ * rows and columns.  Ranks vary per cluster; the bases and couplings are padded to
+ * k = 12 (m l)^2 columns.  Laplace single and double layer; 1 <= m l <= 3.  The assembly calls
+ * are those of h2b_h2matrix_new (h2b_h2matrix_assemble, or the three basis / farfield calls and
+ * the nearfield); h2b_h2matrix_new_like on it gives a second operator with its own greenhybrid
+ * bases on the same structure. */
+h2b_h2matrix *h2b_h2matrix_new_greenhybrid(const h2b_bem *bem, const h2b_tree *tree, uint32_t m,
+                                           uint32_t l, double delta, double accur);
+/* Ranks of the greenhybrid cluster bases (side 0 row, 1 column), one per cluster in the tree's
+ * pre-order: ranks[clusters]. */
+int h2b_h2matrix_green_ranks(const h2b_h2matrix *h, int side, uint32_t *ranks);
 void h2b_h2matrix_del(h2b_h2matrix *h2);
 
 /* Assembly.  Replace assemble_bem3d_h2matrix_row_clusterbasis (Library/bem3d.c:10407),

@@ -6,7 +6,7 @@
  * Built twice: without USE_COMPLEX (Laplace, real field) and with it (Helmholtz, complex field).
  *
  * Usage: gen_golden <outdir> <section> [...]
- * Sections (real build):    quad sphere8 sphere4 h2small config2 cube adlp
+ * Sections (real build):    quad sphere8 sphere4 h2small config2 cube adlp green
  * Sections (complex build): helm_sphere4 helm_h2small config3 config3_k8 helm_gmres helm_adlp
  *                           helm_point
  * The complex build also links the reference's Tests/test_helmholtzbem3d.c (its main renamed) for
@@ -508,6 +508,81 @@ h2_op(const char *prefix, psurface3d gr, pbem3d op, basisfunctionbem3d basis, ui
   del_cluster(root);
 }
 
+/* Ranks of a cluster basis, pre-order. */
+static void
+collect_ranks(pcclusterbasis cb, uint **r, uint *n, uint *cap)
+{
+  uint i;
+  if (*n == *cap) {
+    *cap = *cap ? 2 * *cap : 256;
+    *r = realloc(*r, sizeof(uint) * *cap);
+  }
+  (*r)[(*n)++] = cb->k;
+  for (i = 0; i < cb->sons; i++)
+    collect_ranks(cb->son[i], r, n, cap);
+}
+
+static void
+dump_ranks(const char *prefix, pcclusterbasis cb)
+{
+  uint *r = NULL, n = 0, cap = 0;
+  collect_ranks(cb, &r, &n, &cap);
+  dump_uint(prefix, r, 1, n, 0);
+  free(r);
+}
+
+/* H2 matrix with the greenhybrid farfield (setup_h2matrix_aprx_greenhybrid_bem3d, cube quadrature
+ * points): ranks, bases, the first coupling matrices and a matvec with a seeded vector. */
+static void
+green_op(const char *prefix, psurface3d gr, pbem3d op, basisfunctionbem3d basis, uint clf,
+         real eta, uint m, uint l, real delta, real accur, uint parts_limit)
+{
+  pcluster root;
+  pblock broot;
+  pclusterbasis rb, cb;
+  ph2matrix G;
+  pavector x, y;
+  char name[256];
+
+  root = build_bem3d_cluster(op, clf, basis);
+  broot = build_strict_block(root, root, &eta, admissible_max_cluster);
+  dump_cluster(prefix, root);
+  dump_block(prefix, broot, root, root);
+  rb = build_from_cluster_clusterbasis(root);
+  cb = build_from_cluster_clusterbasis(root);
+  G = build_from_block_h2matrix(broot, rb, cb);
+  setup_h2matrix_aprx_greenhybrid_bem3d(op, rb, cb, broot, m, l, delta, accur,
+                                        build_bem3d_cube_quadpoints);
+  assemble_bem3d_h2matrix_row_clusterbasis(op, rb);
+  assemble_bem3d_h2matrix_col_clusterbasis(op, cb);
+  assemble_bem3d_h2matrix(op, G);
+  snprintf(name, sizeof(name), "%s_row_k", prefix);
+  dump_ranks(name, rb);
+  snprintf(name, sizeof(name), "%s_col_k", prefix);
+  dump_ranks(name, cb);
+  snprintf(name, sizeof(name), "%s_row", prefix);
+  dump_basis(name, rb);
+  snprintf(name, sizeof(name), "%s_col", prefix);
+  dump_basis(name, cb);
+  snprintf(name, sizeof(name), "%s_parts", prefix);
+  dump_h2parts(name, G, parts_limit);
+  x = new_avector(G->cb->t->size);
+  y = new_avector(G->rb->t->size);
+  seeded_avector(x, 5);
+  snprintf(name, sizeof(name), "%s_x", prefix);
+  dump_avector(name, x);
+  clear_avector(y);
+  addeval_h2matrix_avector(1.0, G, x, y);
+  snprintf(name, sizeof(name), "%s_y", prefix);
+  dump_avector(name, y);
+  del_avector(x);
+  del_avector(y);
+  del_h2matrix(G);
+  del_block(broot);
+  freemem(root->idx);
+  del_cluster(root);
+}
+
 /* ---------- sections ---------- */
 
 #ifndef USE_COMPLEX
@@ -791,6 +866,47 @@ section_h2small(void)
   psurface3d gr = build_from_macrosurface3d_surface3d(mg, 8);
   h2_case("h2ll", gr, BASIS_LINEAR_BEM3D, 16, 1.4, 3, 24, 1);
   h2_case("h2cc", gr, BASIS_CONSTANT_BEM3D, 16, 1.4, 3, 24, 0);
+  del_surface3d(gr);
+  del_macrosurface3d(mg);
+}
+
+/* Greenhybrid H2 matrices (the reference's Laplace test parameters m 2, l 1, delta 1, accuracy
+ * 5e-3) on the sphere refined 8 times, scaled to an ellipsoid and turned: single layer with
+ * linear and constant bases, double layer with linear bases. */
+static void
+section_green(void)
+{
+  pmacrosurface3d mg = new_sphere_macrosurface3d();
+  psurface3d gr = build_from_macrosurface3d_surface3d(mg, 8);
+  pbem3d slp_l, slp_c, dlp_l;
+  uint v;
+  /* scaled and turned out of the axes: the cluster boxes and their quadrature points are then
+   * aligned with no symmetry of the mesh, so no two candidates of a pivot search tie */
+  const real ax[3] = { 1.0, 0.8, 0.65 }, ca = cos(0.37), sa = sin(0.37), cb = cos(0.61),
+             sb = sin(0.61), cc = cos(0.23), sc = sin(0.23);
+  for (v = 0; v < gr->vertices; v++) {
+    real p0 = gr->x[v][0] * ax[0], p1 = gr->x[v][1] * ax[1], p2 = gr->x[v][2] * ax[2], q0, q1, q2;
+    q1 = cc * p1 - sc * p2;            /* about x */
+    q2 = sc * p1 + cc * p2;
+    q0 = cb * p0 + sb * q2;            /* about y */
+    q2 = -sb * p0 + cb * q2;
+    p0 = ca * q0 - sa * q1;            /* about z */
+    p1 = sa * q0 + ca * q1;
+    gr->x[v][0] = p0;
+    gr->x[v][1] = p1;
+    gr->x[v][2] = q2;
+  }
+  prepare_surface3d(gr);
+  dump_mesh("green", gr);
+  slp_l = new_slp_laplace_bem3d(gr, 2, 4, BASIS_LINEAR_BEM3D, BASIS_LINEAR_BEM3D);
+  green_op("gsll", gr, slp_l, BASIS_LINEAR_BEM3D, 16, 1.4, 2, 1, 1.0, 5e-3, 24);
+  del_bem3d(slp_l);
+  slp_c = new_slp_laplace_bem3d(gr, 2, 4, BASIS_CONSTANT_BEM3D, BASIS_CONSTANT_BEM3D);
+  green_op("gscc", gr, slp_c, BASIS_CONSTANT_BEM3D, 16, 1.4, 2, 1, 1.0, 5e-3, 24);
+  del_bem3d(slp_c);
+  dlp_l = new_dlp_laplace_bem3d(gr, 2, 4, BASIS_LINEAR_BEM3D, BASIS_LINEAR_BEM3D, 0.5);
+  green_op("gdll", gr, dlp_l, BASIS_LINEAR_BEM3D, 16, 1.4, 2, 1, 1.0, 5e-3, 24);
+  del_bem3d(dlp_l);
   del_surface3d(gr);
   del_macrosurface3d(mg);
 }
@@ -1317,6 +1433,8 @@ main(int argc, char **argv)
       section_cube();
     else if (!strcmp(argv[i], "adlp"))
       section_adlp();
+    else if (!strcmp(argv[i], "green"))
+      section_green();
 #else
     if (!strcmp(argv[i], "helm_sphere4"))
       section_helm_sphere4();

@@ -7,7 +7,7 @@ read the committed .npz files.
 
     python tests/golden/make_golden.py [section ...]
 
-Sections: quad sphere8 sphere4 h2small config2 cube adlp helm_sphere4 helm_h2small config3
+Sections: quad sphere8 sphere4 h2small config2 cube adlp green helm_sphere4 helm_h2small config3
 config3_k8 helm_gmres helm_adlp helm_point
 """
 import os
@@ -22,7 +22,7 @@ ROOT = os.path.dirname(os.path.dirname(HERE))
 REF = os.environ.get("REF", "/root/reference")
 REFOUT = os.path.join(ROOT, "oracle", "_ref")
 
-REAL_SECTIONS = ["quad", "sphere8", "sphere4", "h2small", "config2", "cube", "adlp"]
+REAL_SECTIONS = ["quad", "sphere8", "sphere4", "h2small", "config2", "cube", "adlp", "green"]
 COMPLEX_SECTIONS = ["helm_sphere4", "helm_h2small", "config3", "config3_k8", "helm_gmres",
                     "helm_adlp", "helm_point"]
 DTYPES = {"f8": np.float64, "u4": np.uint32, "c16": np.complex128}

@@ -1,0 +1,63 @@
+"""Greenhybrid H2 matrices on the B200 against the reference's (tests/golden/green.npz, made by
+setup_h2matrix_aprx_greenhybrid_bem3d, Library/bem3d.c:9689, with the reference test's m 2, l 1,
+delta 1, accuracy 5e-3): the same rank in every row and column cluster basis (the same pivots of
+the cross approximations), and the matvec with the fixture's vector to 1e-10 relative.  The
+fixture's mesh is a sphere scaled and turned out of the axes: on a mesh with the symmetries of the
+axis-aligned boxes, entries that are equal in exact arithmetic tie in the pivot searches, and which
+of them wins depends on the last bit of each quadrature sum."""
+import os
+
+import numpy as np
+import pytest
+
+from h2lib_b200 import bem3d as hb
+
+pytestmark = pytest.mark.gpu
+GOLD = os.path.join(os.path.dirname(__file__), "golden", "green.npz")
+L, C = hb.BASIS_LINEAR_BEM3D, hb.BASIS_CONSTANT_BEM3D
+
+
+def _op(prefix, gr):
+    if prefix == "gsll":
+        return hb.new_slp_laplace_bem3d(gr, 2, 4, L, L), L
+    if prefix == "gscc":
+        return hb.new_slp_laplace_bem3d(gr, 2, 4, C, C), C
+    return hb.new_dlp_laplace_bem3d(gr, 2, 4, L, L, 0.5), L
+
+
+@pytest.mark.parametrize("prefix", ["gsll", "gscc", "gdll"])
+def test_greenhybrid_matches_reference(prefix):
+    d = np.load(GOLD)
+    gr = hb.Surface3d(d["green_x"], d["green_t"])
+    bem, basis = _op(prefix, gr)
+    tree = hb.build_tree(gr, basis, basis, 16, 1.4)
+    H = hb.H2Matrix(bem, tree, 2, green=(1, 1.0, 5e-3)).assemble()
+    bad = [int(np.sum(H.green_ranks(s) != d[f"{prefix}_{side}_k"]))
+           for s, side in ((0, "row"), (1, "col"))]
+    x = d[f"{prefix}_x"].copy()
+    y = hb.addeval_h2matrix_avector(1.0, H, x, np.zeros(H.rows))
+    ref = d[f"{prefix}_y"]
+    err = np.linalg.norm(y - ref) / np.linalg.norm(ref)
+    assert bad == [0, 0] and err <= 1e-10, (bad, err)
+
+
+def test_greenhybrid_like_and_accuracy():
+    """The double layer made like the single layer's greenhybrid matrix has its own bases (the
+    column side differentiates), and both products stay within the ACA accuracy of the
+    interpolation H2 matrices of order 4 on a finer sphere."""
+    gr = hb.new_sphere_surface3d(16)
+    tree = hb.build_tree(gr, L, L, 16, 1.4)
+    slp = hb.new_slp_laplace_bem3d(gr, 2, 4, L, L)
+    dlp = hb.new_dlp_laplace_bem3d(gr, 2, 4, L, L, 0.5)
+    V = hb.H2Matrix(slp, tree, 2, green=(1, 1.0, 1e-4)).assemble()
+    K = hb.H2Matrix(dlp, tree, 2, like=V).assemble()
+    Vi = hb.H2Matrix(slp, tree, 4).assemble()
+    Ki = hb.H2Matrix(dlp, tree, 4, like=Vi).assemble()
+    rng = np.random.default_rng(2)
+    x = rng.standard_normal(V.cols)
+    for A, B in ((V, Vi), (K, Ki)):
+        ya = hb.addeval_h2matrix_avector(1.0, A, x.copy(), np.zeros(A.rows))
+        yb = hb.addeval_h2matrix_avector(1.0, B, x.copy(), np.zeros(B.rows))
+        assert np.linalg.norm(ya - yb) <= 1e-3 * np.linalg.norm(yb)
+    assert not np.array_equal(K.green_ranks(1), V.green_ranks(1))
+    np.testing.assert_array_equal(K.green_ranks(0), V.green_ranks(0))
