@@ -78,6 +78,7 @@ def parse():
     p.add_argument("--no-helmholtz", action="store_true")
     p.add_argument("--no-mixed", action="store_true")
     p.add_argument("--no-dense", action="store_true")
+    p.add_argument("--no-green", action="store_true")
     p.add_argument("--dense-split", type=int, default=32)
     p.add_argument("--no-autotune", action="store_true",
                    help="keep the default launch shapes (profiling runs: no tuning launches)")
@@ -772,6 +773,52 @@ def run_dense(a, peak):
                              "frac": ref / (d * 1e-3) / 1e12 / peak}}}
 
 
+def run_green(a):
+    """Laplace single layer with the greenhybrid farfield (setup_h2matrix_aprx_greenhybrid_bem3d,
+    Library/bem3d.c:9689; the reference test's m 2, l 1, delta 1, accuracy 5e-3) on the config-2
+    sphere and tree: per-phase device times of the assembly, the matvec, the ranks, the product's
+    distance from the interpolation H2 matrix (m 4), and the reference's CPU assembly of the same
+    matrix (oracle/_ref/ref_bench green)."""
+    from h2lib_b200 import bem3d as hb
+    L = hb.BASIS_LINEAR_BEM3D
+    gr = hb.new_sphere_surface3d(a.split)
+    tree = hb.build_tree(gr, L, L, a.clf, a.eta)
+    slp = hb.new_slp_laplace_bem3d(gr, 2, 4, L, L)
+    H = hb.H2Matrix(slp, tree, 2, green=(1, 1.0, 5e-3))
+    H.assemble()
+    walls, phases = [], []
+    for _ in range(3):
+        t0 = time.perf_counter()
+        H.assemble()
+        walls.append(time.perf_counter() - t0)
+        phases.append(H.timings())
+    ph = {k: statistics.mean(p[k] for p in phases) for k in phases[0]}
+    rng = np.random.default_rng(4)
+    x = rng.standard_normal(H.cols)
+    y = hb.addeval_h2matrix_avector(1.0, H, x.copy(), np.zeros(H.rows))
+    mv = []
+    for _ in range(5):
+        hb.addeval_h2matrix_avector(1.0, H, x.copy(), np.zeros(H.rows))
+        mv.append(H.timings()["matvec"])
+    Vi = hb.H2Matrix(slp, tree, 4).assemble()
+    yi = hb.addeval_h2matrix_avector(1.0, Vi, x.copy(), np.zeros(H.rows))
+    rk = H.green_ranks(0)
+    out = {"workload": f"Laplace SLP, sphere split {a.split} ({gr.triangles} triangles), linear "
+                       f"basis, q 2/4, leaf {a.clf}, eta {a.eta}, greenhybrid m 2 l 1 delta 1 "
+                       "accuracy 5e-3 (k = 48)",
+           "assembly_wall_s": statistics.mean(walls),
+           "phase_ms": {"bases": ph["row_basis"] + ph["col_basis"], "coupling": ph["coupling"],
+                        "near_distant": ph["near_distant"], "near_singular": ph["near_singular"]},
+           "matvec_ms": statistics.mean(mv),
+           "ranks": {"root": int(rk[0]), "mean": float(rk.mean()), "max": int(rk.max())},
+           "rel_diff_vs_interpolation_m4": float(np.linalg.norm(y - yi) / np.linalg.norm(yi))}
+    ref = run_ref(REF_BENCH, ["green", a.split, a.clf, a.eta, 2, 1, 1.0, 5e-3])
+    if ref is not None:
+        out["cpu_reference"] = ref
+        out["assembly_speedup_vs_cpu_reference"] = ref["seconds"] / out["assembly_wall_s"]
+    return out
+
+
 def run_helmholtz(a, peak):
     """Brakhage-Werner solves of config 3: unit cube split 64 (49152 triangles), constant basis,
     q 2/4, leaf 64, eta 1.4, m 5, plane wave along (1,1,1)/sqrt(3), GMRES(80) to 1e-8, k = 2
@@ -1030,6 +1077,11 @@ def main():
                 res["helmholtz"] = run_helmholtz(a, res["roofline"]["peak"])
             except Exception as e:  # reported, never hides the headline line
                 res["helmholtz"] = {"error": str(e)[:300]}
+        if not a.no_green:
+            try:
+                res["greenhybrid"] = run_green(a)
+            except Exception as e:  # reported, never hides the headline line
+                res["greenhybrid"] = {"error": str(e)[:300]}
         if not a.no_serving:
             try:
                 res["serving"] = run_serving(a)

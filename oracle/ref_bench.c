@@ -10,6 +10,11 @@
  *       Laplace single + double layer H2 matrices on the sphere refined x split (linear basis,
  *       q 2/4): per step both operators' bases, nearfield and farfield; --solve then times the
  *       interior Dirichlet GMRES(50) solve to 1e-8 and one matrix-vector product.
+ *   ref_bench green split clf eta m l delta accur                      (real build)
+ *       Laplace single layer with the greenhybrid farfield (setup_h2matrix_aprx_greenhybrid_bem3d,
+ *       Library/bem3d.c:9689, cube quadrature points) on the sphere refined x split (linear
+ *       basis, q 2/4): one assembly timed by phase (bases, nearfield, farfield) and one
+ *       matrix-vector product.
  *   ref_bench helmholtz split k clf eta m applications [--solve]       (complex build)
  *       Brakhage-Werner operator (K + M/2) - i k V on the cube refined x split (constant basis):
  *       one assembly of both operators, `applications` timed operator applications, and with
@@ -366,6 +371,51 @@ static int mode_requests(int argc, char **argv) {
   return 0;
 }
 
+#ifndef USE_COMPLEX
+static int mode_green(int argc, char **argv) {
+  if (argc < 9) return 2;
+  const uint split = atoi(argv[2]), clf = atoi(argv[3]), m = atoi(argv[5]), l = atoi(argv[6]);
+  real eta = atof(argv[4]);
+  const real delta = atof(argv[7]), accur = atof(argv[8]);
+  pmacrosurface3d mg = new_sphere_macrosurface3d();
+  psurface3d gr = build_from_macrosurface3d_surface3d(mg, split);
+  prepare_surface3d(gr);
+  pbem3d slp = new_slp_laplace_bem3d(gr, 2, 4, BASIS_LINEAR_BEM3D, BASIS_LINEAR_BEM3D);
+  pcluster root = build_bem3d_cluster(slp, clf, BASIS_LINEAR_BEM3D);
+  pblock broot = build_strict_block(root, root, &eta, admissible_max_cluster);
+  pclusterbasis rb = build_from_cluster_clusterbasis(root);
+  pclusterbasis cb = build_from_cluster_clusterbasis(root);
+  ph2matrix G = build_from_block_h2matrix(broot, rb, cb);
+  double t[3] = {0.0, 0.0, 0.0}, tm;
+  pavector x, y;
+  setup_h2matrix_aprx_greenhybrid_bem3d(slp, rb, cb, broot, m, l, delta, accur,
+                                        build_bem3d_cube_quadpoints);
+  assemble(slp, G, t);
+  x = new_avector(gr->vertices);
+  y = new_avector(gr->vertices);
+  random_avector(x);
+  clear_avector(y);
+  tic();
+  addeval_h2matrix_avector(1.0, G, x, y);
+  tm = toc();
+  printf("{\"threads\": %d, \"triangles\": %u, \"vertices\": %u, \"seconds\": %.6f, "
+         "\"bases\": %.6f, \"nearfield\": %.6f, \"farfield\": %.6f, \"matvec_seconds\": %.6f, "
+         "\"root_rank\": %u}\n",
+         threads(), gr->triangles, gr->vertices, t[0] + t[1] + t[2], t[0], t[1], t[2], tm,
+         rb->k);
+  del_avector(x);
+  del_avector(y);
+  del_h2matrix(G);
+  del_block(broot);
+  freemem(root->idx);
+  del_cluster(root);
+  del_bem3d(slp);
+  del_surface3d(gr);
+  del_macrosurface3d(mg);
+  return 0;
+}
+#endif
+
 int main(int argc, char **argv) {
   int rc = 2;
   init_h2lib(&argc, &argv);
@@ -373,14 +423,16 @@ int main(int argc, char **argv) {
   if (argc >= 2 && !strcmp(argv[1], "requests")) rc = mode_requests(argc, argv);
 #ifndef USE_COMPLEX
   else if (argc >= 2 && !strcmp(argv[1], "assembly")) rc = mode_assembly(argc, argv);
+  else if (argc >= 2 && !strcmp(argv[1], "green")) rc = mode_green(argc, argv);
 #else
   else if (argc >= 2 && !strcmp(argv[1], "helmholtz")) rc = mode_helmholtz(argc, argv);
 #endif
   if (rc == 2)
     fprintf(stderr,
             "usage: %s assembly split clf eta m steps warmup [--solve]   (real build)\n"
+            "       %s green split clf eta m l delta accur               (real build)\n"
             "       %s helmholtz split k clf eta m applications [--solve] (complex build)\n"
-            "       %s requests file\n", argv[0], argv[0], argv[0]);
+            "       %s requests file\n", argv[0], argv[0], argv[0], argv[0]);
   del_stopwatch(sw);
   uninit_h2lib();
   return rc;
