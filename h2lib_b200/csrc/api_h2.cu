@@ -473,6 +473,16 @@ extern "C" h2b_h2matrix *h2b_h2matrix_new_greenhybrid(const h2b_bem *bem, const 
   }
   int rc = green_setup(h->rt, tree->row, k, h->st);
   if (rc == H2B_OK) rc = green_setup(h->ct, tree->col, k, h->st);
+  {
+    const h2b_ctree &r = tree->row, &c = tree->col;
+    h->g_same = bem->row_basis == bem->col_basis && r.n == c.n && r.nidx == c.nidx &&
+                !memcmp(r.off, c.off, sizeof(uint32_t) * r.n) &&
+                !memcmp(r.size, c.size, sizeof(uint32_t) * r.n) &&
+                !memcmp(r.sons, c.sons, sizeof(uint32_t) * r.n) &&
+                !memcmp(r.idx, c.idx, sizeof(uint32_t) * r.nidx) &&
+                !memcmp(r.bmin, c.bmin, sizeof(double) * 3 * r.n) &&
+                !memcmp(r.bmax, c.bmax, sizeof(double) * 3 * r.n);
+  }
   if (rc == H2B_OK && cudaStreamSynchronize(h->st) != cudaSuccess) {
     h2b_set_error("h2b_h2matrix_new_greenhybrid: %s", cudaGetErrorString(cudaGetLastError()));
     rc = H2B_ERR_CUDA;
@@ -510,6 +520,7 @@ extern "C" h2b_h2matrix *h2b_h2matrix_new_like(const h2b_bem *bem, const h2b_h2m
   for (int e = 0; e < 12; e++) h->ev[e] = nullptr;
   for (int i = 0; i < 6; i++) h->ms[i] = 0.0f;
   h->quad_fp32 = 0;
+  h->g_row_ready = 0;
   h->f_S = h->f_N = nullptr;
   h->d_S = h->d_N = h->d_xp = h->d_yp = h->d_xt = h->d_yt = h->d_xio = h->d_yio = nullptr;
   h->d_mverr = nullptr;
@@ -904,12 +915,30 @@ static int finish(h2b_h2matrix *h, int rc, unsigned phases) {
   return H2B_OK;
 }
 
+// The single layer's column kernels are its row kernels (kernel_col = fundamental_row,
+// dnz_kernel_col = dnz_fundamental_row, Library/laplacebem3d.c:870/897): on equal trees the
+// column basis is the row basis, and its ranks, pivots, transfers and flattened bases are copied.
+static int green_copy_col(h2b_h2matrix *h) {
+  const uint32_t K = h->k;
+  DevCTree &r = h->rt, &c = h->ct;
+  H2B_CUDA_TRY(cudaMemcpyAsync(c.d_grank, r.d_grank, sizeof(uint32_t) * r.n,
+                               cudaMemcpyDeviceToDevice, h->st));
+  H2B_CUDA_TRY(cudaMemcpyAsync(c.d_gpiv, r.d_gpiv, sizeof(uint32_t) * (size_t) r.n * K,
+                               cudaMemcpyDeviceToDevice, h->st));
+  H2B_CUDA_TRY(cudaMemcpyAsync(c.d_gE, r.d_gE, sizeof(double) * (size_t) r.n * K * K,
+                               cudaMemcpyDeviceToDevice, h->st));
+  H2B_CUDA_TRY(cudaMemcpyAsync(c.d_W, r.d_W, sizeof(double) * r.wtotal, cudaMemcpyDeviceToDevice,
+                               h->st));
+  return H2B_OK;
+}
+
 static int row_basis(h2b_h2matrix *h) {
   mark(h, 0);
   // row side: Lagrange polynomials (assemble_bem3d_lagrange_{c,l}_amatrix); normal derivatives
   // for the adjoint double layer (assemble_bem3d_dn_lagrange_*, Library/laplacebem3d.c:1180)
   int rc = h->green ? green_basis(h, h->rt, h->bem->row_basis, 0)
                     : assemble_basis(h, h->rt, h->bem->row_basis, h->bem->layer == H2B_ADLP);
+  h->g_row_ready = h->green && rc == H2B_OK;
   mark(h, 1);
   return rc;
 }
@@ -917,8 +946,13 @@ static int row_basis(h2b_h2matrix *h) {
 static int col_basis(h2b_h2matrix *h) {
   mark(h, 2);
   // column side of the double layer: normal derivatives (assemble_bem3d_dn_lagrange_*)
-  int rc = h->green ? green_basis(h, h->ct, h->bem->col_basis, h->bem->layer == H2B_DLP)
-                    : assemble_basis(h, h->ct, h->bem->col_basis, h->bem->layer == H2B_DLP);
+  int rc;
+  if (h->green && h->g_same && h->g_row_ready && h->bem->layer == H2B_SLP &&
+      h->rt.h_woff == h->ct.h_woff)
+    rc = green_copy_col(h);
+  else
+    rc = h->green ? green_basis(h, h->ct, h->bem->col_basis, h->bem->layer == H2B_DLP)
+                  : assemble_basis(h, h->ct, h->bem->col_basis, h->bem->layer == H2B_DLP);
   mark(h, 3);
   return rc;
 }
@@ -1081,6 +1115,11 @@ extern "C" int h2b_h2matrix_info(const h2b_h2matrix *h, uint64_t info[8]) {
 extern "C" int h2b_h2matrix_export(const h2b_h2matrix *h, int part, uint32_t count, double *out,
                                    uint64_t *ndoubles) {
   if (!h || !ndoubles) return H2B_ERR_ARG;
+  if (h->green && part >= 0 && part <= 3) {
+    h2b_set_error("h2b_h2matrix_export: the bases of a greenhybrid H2 matrix have per-cluster "
+                  "ranks; only parts 4 and 5 are exported");
+    return H2B_ERR_ARG;
+  }
   const uint64_t W = h->cx ? 2 : 1, kk = (uint64_t) h->k * h->k;
   const double *src = nullptr;
   uint64_t n = 0;

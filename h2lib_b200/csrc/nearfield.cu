@@ -1393,7 +1393,7 @@ extern "C" int h2b_near_unique_pairs(const void *tri, const void *refs, const h2
 // (assemble_bem3d_greenhybrid_uniform, Library/bem3d.c:6493, through nearfield_far =
 // assemble_{cc,ll}_far_bem3d, :1439 / :3264), the distant rule on every pair of triangles of the
 // two basis functions.  K x K column-major per block, zero past the ranks.
-template <bool RL, bool CL, bool DLP>
+template <int Q, bool RL, bool CL, bool DLP>
 __global__ void __launch_bounds__(256) green_coupling_kernel(GreenCouplingArgs a) {
   const uint32_t b = blockIdx.x;
   const uint32_t rc = a.adm_rc[b], cc = a.adm_cc[b];
@@ -1411,29 +1411,70 @@ __global__ void __launch_bounds__(256) green_coupling_kernel(GreenCouplingArgs a
       for (uint32_t ti = t0; ti < t1; ti++) {
         const TriRec &T = a.tri[RL ? a.vt_tri[ti] : bi];
         const int ct = RL ? (T.v[0] == bi ? 0 : (T.v[1] == bi ? 1 : 2)) : 0;
-        for (uint32_t si = u0; si < u1; si++) {
-          const TriRec &Sx = a.tri[CL ? a.vt_tri[si] : bj];
-          const int cs = CL ? (Sx.v[0] == bj ? 0 : (Sx.v[1] == bj ? 1 : 2)) : 0;
-          double sum = 0.0;
-          for (int p = 0; p < np; p++) {
-            const double tx = c_dist[0][o + p], sx = c_dist[1][o + p];
-            const double ty = c_dist[2][o + p], sy = c_dist[3][o + p], w = c_dist[4][o + p];
+        if constexpr (Q > 0) {
+          // the distant rule is one q^2-point rule per triangle (w = w_x w_y): the row
+          // triangle's points and basis-weighted weights once per triangle, the column
+          // triangle's once per pair
+          constexpr int P = Q * Q;
+          const double(&sd)[6][SIDE_MAXP] = c_side[Q - 1];
+          double xa[P][3], wa[P];
+#pragma unroll
+          for (int p = 0; p < P; p++) {
+            const double tx = sd[0][p], sx = sd[1][p];
             const double ax = 1.0 - tx, bx = tx - sx, cx = sx;
-            const double ay = 1.0 - ty, by = ty - sy, cy = sy;
-            const double d0 = (T.a[0] * ax + T.b[0] * bx + T.c[0] * cx) -
-                              (Sx.a[0] * ay + Sx.b[0] * by + Sx.c[0] * cy);
-            const double d1 = (T.a[1] * ax + T.b[1] * bx + T.c[1] * cx) -
-                              (Sx.a[1] * ay + Sx.b[1] * by + Sx.c[1] * cy);
-            const double d2 = (T.a[2] * ax + T.b[2] * bx + T.c[2] * cx) -
-                              (Sx.a[2] * ay + Sx.b[2] * by + Sx.c[2] * cy);
-            const double ri = rsqrt_nr(d0 * d0 + d1 * d1 + d2 * d2);
-            const double f =
-                DLP ? (d0 * Sx.n[0] + d1 * Sx.n[1] + d2 * Sx.n[2]) * (ri * ri * ri) : ri;
-            const double pr_ = RL ? (ct == 0 ? ax : (ct == 1 ? bx : cx)) : 1.0;
-            const double pc_ = CL ? (cs == 0 ? ay : (cs == 1 ? by : cy)) : 1.0;
-            sum += w * pr_ * pc_ * f;
+#pragma unroll
+            for (int d = 0; d < 3; d++) xa[p][d] = T.a[d] * ax + T.b[d] * bx + T.c[d] * cx;
+            wa[p] = RL ? sd[3 + ct][p] : sd[2][p];
           }
-          acc += sum * (T.g * Sx.g * a.kconst);
+          for (uint32_t si = u0; si < u1; si++) {
+            const TriRec &Sx = a.tri[CL ? a.vt_tri[si] : bj];
+            const int cs = CL ? (Sx.v[0] == bj ? 0 : (Sx.v[1] == bj ? 1 : 2)) : 0;
+            double part = 0.0;
+#pragma unroll
+            for (int p = 0; p < P; p++) {
+              const double ty = sd[0][p], sy = sd[1][p];
+              const double ay = 1.0 - ty, by = ty - sy, cy = sy;
+              const double y0 = Sx.a[0] * ay + Sx.b[0] * by + Sx.c[0] * cy;
+              const double y1 = Sx.a[1] * ay + Sx.b[1] * by + Sx.c[1] * cy;
+              const double y2 = Sx.a[2] * ay + Sx.b[2] * by + Sx.c[2] * cy;
+              double pb = 0.0;
+#pragma unroll
+              for (int r = 0; r < P; r++) {
+                const double d0 = xa[r][0] - y0, d1 = xa[r][1] - y1, d2 = xa[r][2] - y2;
+                const double ri = rsqrt_nr(fma(d0, d0, fma(d1, d1, d2 * d2)));
+                const double f =
+                    DLP ? fma(d0, Sx.n[0], fma(d1, Sx.n[1], d2 * Sx.n[2])) * (ri * ri * ri) : ri;
+                pb = fma(wa[r], f, pb);
+              }
+              part = fma(CL ? sd[3 + cs][p] : sd[2][p], pb, part);
+            }
+            acc += part * (T.g * Sx.g * a.kconst);
+          }
+        } else {
+          for (uint32_t si = u0; si < u1; si++) {
+            const TriRec &Sx = a.tri[CL ? a.vt_tri[si] : bj];
+            const int cs = CL ? (Sx.v[0] == bj ? 0 : (Sx.v[1] == bj ? 1 : 2)) : 0;
+            double sum = 0.0;
+            for (int p = 0; p < np; p++) {
+              const double tx = c_dist[0][o + p], sx = c_dist[1][o + p];
+              const double ty = c_dist[2][o + p], sy = c_dist[3][o + p], w = c_dist[4][o + p];
+              const double ax = 1.0 - tx, bx = tx - sx, cx = sx;
+              const double ay = 1.0 - ty, by = ty - sy, cy = sy;
+              const double d0 = (T.a[0] * ax + T.b[0] * bx + T.c[0] * cx) -
+                                (Sx.a[0] * ay + Sx.b[0] * by + Sx.c[0] * cy);
+              const double d1 = (T.a[1] * ax + T.b[1] * bx + T.c[1] * cx) -
+                                (Sx.a[1] * ay + Sx.b[1] * by + Sx.c[1] * cy);
+              const double d2 = (T.a[2] * ax + T.b[2] * bx + T.c[2] * cx) -
+                                (Sx.a[2] * ay + Sx.b[2] * by + Sx.c[2] * cy);
+              const double ri = rsqrt_nr(d0 * d0 + d1 * d1 + d2 * d2);
+              const double f =
+                  DLP ? (d0 * Sx.n[0] + d1 * Sx.n[1] + d2 * Sx.n[2]) * (ri * ri * ri) : ri;
+              const double pr_ = RL ? (ct == 0 ? ax : (ct == 1 ? bx : cx)) : 1.0;
+              const double pc_ = CL ? (cs == 0 ? ay : (cs == 1 ? by : cy)) : 1.0;
+              sum += w * pr_ * pc_ * f;
+            }
+            acc += sum * (T.g * Sx.g * a.kconst);
+          }
         }
       }
     }
@@ -1443,7 +1484,10 @@ __global__ void __launch_bounds__(256) green_coupling_kernel(GreenCouplingArgs a
 
 template <bool RL, bool CL, bool DLP>
 static int launch_green_coupling(const GreenCouplingArgs *a, cudaStream_t st) {
-  green_coupling_kernel<RL, CL, DLP><<<a->n, 256, 0, st>>>(*a);
+  if (a->q == 2)
+    green_coupling_kernel<2, RL, CL, DLP><<<a->n, 256, 0, st>>>(*a);
+  else
+    green_coupling_kernel<0, RL, CL, DLP><<<a->n, 256, 0, st>>>(*a);
   h2b_note_launch();
   H2B_CUDA_TRY(cudaGetLastError());
   return H2B_OK;

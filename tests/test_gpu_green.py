@@ -4,7 +4,8 @@ delta 1, accuracy 5e-3): the same rank in every row and column cluster basis (th
 the cross approximations), and the matvec with the fixture's vector to 1e-10 relative.  The
 fixture's mesh is a sphere scaled and turned out of the axes: on a mesh with the symmetries of the
 axis-aligned boxes, entries that are equal in exact arithmetic tie in the pivot searches, and which
-of them wins depends on the last bit of each quadrature sum."""
+of them wins depends on the last bit of each quadrature sum.  The single layers take their column
+bases from their row bases (equal trees and kernels), the double layer forms its own."""
 import os
 
 import numpy as np
@@ -61,3 +62,4 @@ def test_greenhybrid_like_and_accuracy():
         assert np.linalg.norm(ya - yb) <= 1e-3 * np.linalg.norm(yb)
     assert not np.array_equal(K.green_ranks(1), V.green_ranks(1))
     np.testing.assert_array_equal(K.green_ranks(0), V.green_ranks(0))
+
