@@ -391,7 +391,8 @@ static int green_alloc(DevCTree &t, uint32_t k, cudaStream_t st) {
 
 // Structure of the greenhybrid bases of one tree: boxes, clusters by level (deepest first) with
 // the rows bound of A_t (a leaf's size; a father's size, at most the 2k pivot rows of its two
-// sons), and the needed non-leaf clusters (flattened bases) by level.
+// sons), and by level the flatten items of the needed non-leaf clusters (father, son, first
+// row, rows: slices of at most H2B_GREEN_FLAT_ROWS rows of each son).
 static int green_setup(DevCTree &t, const h2b_ctree &c, uint32_t k, cudaStream_t st) {
   uint32_t maxlev = 0;
   for (uint32_t i = 0; i < c.n; i++) maxlev = std::max(maxlev, c.level[i]);
@@ -409,10 +410,16 @@ static int green_setup(DevCTree &t, const h2b_ctree &c, uint32_t k, cudaStream_t
       if (c.level[i] != L) continue;
       lev.push_back(i);
       rows = std::max(rows, c.sons[i] == 0 ? c.size[i] : std::min(c.size[i], 2 * k));
-      if (c.sons[i] != 0 && need[i]) flat.push_back(i);
+      if (c.sons[i] != 0 && need[i])
+        for (uint32_t so : {c.son0[i], c.son1[i]}) {
+          if (so == UINT32_MAX) continue;
+          for (uint32_t r0 = 0; r0 < c.size[so]; r0 += H2B_GREEN_FLAT_ROWS)
+            flat.insert(flat.end(),
+                        {i, so, r0, std::min<uint32_t>(H2B_GREEN_FLAT_ROWS, c.size[so] - r0)});
+        }
     }
     t.h_glev_off.push_back((uint32_t) lev.size());
-    t.h_gflat_off.push_back((uint32_t) flat.size());
+    t.h_gflat_off.push_back((uint32_t) (flat.size() / 4));
     t.h_glev_rows.push_back(rows);
   }
   for (uint32_t i = 0; i < c.n; i++)
@@ -785,7 +792,7 @@ static int green_basis(h2b_h2matrix *h, DevCTree &t, int basis, int dcol) {
   GreenFlatArgs fa{nullptr, 0, t.d_off, t.d_size, t.d_son0, t.d_son1, t.d_grank, t.d_woff,
                    t.d_gE, t.d_W, (int) K};
   for (size_t L = 0; rc == H2B_OK && L + 1 < t.h_gflat_off.size(); L++) {
-    fa.clusters = t.d_gflat + t.h_gflat_off[L];
+    fa.items = t.d_gflat + 4 * (size_t) t.h_gflat_off[L];
     fa.n = t.h_gflat_off[L + 1] - t.h_gflat_off[L];
     rc = h2b_green_flatten(&fa, h->st);
   }

@@ -43,8 +43,8 @@ struct DevCTree {
   std::vector<uint32_t> roots;
   const uint32_t *h_idx = nullptr, *h_off = nullptr, *h_size = nullptr;  // the host tree
   // greenhybrid bases (green.cu).  Structure: per cluster box (bmin, bmax), the clusters by
-  // level (deepest first, with a bound on the rows of A_t per level) and the needed non-leaf
-  // clusters by level.  Per operator: ranks, pivots (K per cluster), transfers (K x K).
+  // level (deepest first, with a bound on the rows of A_t per level) and the flatten items of the
+  // needed non-leaf clusters by level (4 uint32 each).  Per operator: ranks, pivots (K per cluster), transfers (K x K).
   double *d_gbox = nullptr;
   uint32_t *d_glev = nullptr, *d_gflat = nullptr;
   std::vector<uint32_t> h_glev_off, h_glev_rows, h_gflat_off;

@@ -268,28 +268,25 @@ __global__ void __launch_bounds__(GT) green_basis_kernel(GreenArgs g) {
   }
 }
 
-// W_t rows of son s = W_s E_s (the son's rank columns of W_s), one CTA per cluster.
+// W_t rows of son s = W_s E_s (the son's rank columns of W_s): one CTA per item of at most
+// H2B_GREEN_FLAT_ROWS rows of one son, E_s in shared memory.
 __global__ void __launch_bounds__(GT) green_flatten_kernel(GreenFlatArgs a) {
   extern __shared__ double sE[];
-  const uint32_t t = a.clusters[blockIdx.x];
+  const uint4 it = reinterpret_cast<const uint4 *>(a.items)[blockIdx.x];
+  const uint32_t t = it.x, s = it.y, r0 = it.z, nr = it.w;
   const int K = a.K;
+  const uint32_t ks = a.rank[s], o = a.off[s] - a.off[t];
+  const double *E = a.E + (size_t) s * K * K;
+  const double *Ws = a.W + a.woff[s];
   double *Wt = a.W + a.woff[t];
-  for (int si = 0; si < 2; si++) {
-    const uint32_t s = si ? a.son1[t] : a.son0[t];
-    if (s == UINT32_MAX) continue;
-    const uint32_t ks = a.rank[s], rows = a.size[s], o = a.off[s] - a.off[t];
-    const double *E = a.E + (size_t) s * K * K;
-    const double *Ws = a.W + a.woff[s];
-    __syncthreads();
-    for (int e = (int) threadIdx.x; e < K * K; e += (int) blockDim.x) sE[e] = E[e];
-    __syncthreads();
-    for (uint32_t e = threadIdx.x; e < rows * (uint32_t) K; e += blockDim.x) {
-      const uint32_t r = e / (uint32_t) K, nu = e % (uint32_t) K;
-      const double *w = Ws + (size_t) r * K;
-      double v = 0.0;
-      for (uint32_t mu = 0; mu < ks; mu++) v = fma(w[mu], sE[mu + (size_t) nu * K], v);
-      Wt[(size_t) (o + r) * K + nu] = v;
-    }
+  for (int e = (int) threadIdx.x; e < K * K; e += (int) blockDim.x) sE[e] = E[e];
+  __syncthreads();
+  for (uint32_t e = threadIdx.x; e < nr * (uint32_t) K; e += blockDim.x) {
+    const uint32_t r = r0 + e / (uint32_t) K, nu = e % (uint32_t) K;
+    const double *w = Ws + (size_t) r * K;
+    double v = 0.0;
+    for (uint32_t mu = 0; mu < ks; mu++) v = fma(w[mu], sE[mu + (size_t) nu * K], v);
+    Wt[(size_t) (o + r) * K + nu] = v;
   }
 }
 

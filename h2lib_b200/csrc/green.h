@@ -43,8 +43,10 @@ struct GreenArgs {
   double *E;                 // per cluster: K x K transfer to the father (column-major)
 };
 
+#define H2B_GREEN_FLAT_ROWS 64  // rows of a son per flatten item
+
 struct GreenFlatArgs {
-  const uint32_t *clusters;  // needed non-leaf clusters of one level
+  const uint32_t *items;  // per item (father, son, first row, rows) of one level
   uint32_t n;
   const uint32_t *off, *size, *son0, *son1, *rank;
   const uint64_t *woff;
