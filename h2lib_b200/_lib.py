@@ -66,6 +66,7 @@ _SIGS = {
     "h2b_h2matrix_new_like": (vp, [vp, vp]),
     "h2b_h2matrix_new_greenhybrid": (vp, [vp, vp, C.c_uint32, C.c_uint32, C.c_double, C.c_double]),
     "h2b_h2matrix_green_ranks": (C.c_int, [vp, C.c_int, vp]),
+    "h2b_h2matrix_export_green": (C.c_int, [vp, C.c_int, vp, vp]),
     "h2b_h2matrix_del": (None, [vp]),
     "h2b_h2matrix_assemble_row_clusterbasis": (C.c_int, [vp]),
     "h2b_h2matrix_assemble_col_clusterbasis": (C.c_int, [vp]),

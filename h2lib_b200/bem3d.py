@@ -359,6 +359,16 @@ class H2Matrix:
         check(lib.h2b_h2matrix_green_ranks(self.handle, side, _ptr(out)), "green_ranks")
         return out
 
+    def export_green(self, part):
+        """Greenhybrid parts with their per-cluster ranks (h2b_h2matrix_export_green): 0 / 2 row /
+        column leaf bases, 1 / 3 transfers, 4 couplings, concatenated in H2Lib's layouts."""
+        n = np.zeros(1, dtype=np.uint64)
+        check(lib.h2b_h2matrix_export_green(self.handle, part, None, _ptr(n)), "export_green")
+        out = np.zeros(int(n[0]))
+        check(lib.h2b_h2matrix_export_green(self.handle, part, _ptr(out), _ptr(n)),
+              "export_green")
+        return out
+
     def unique_pairs(self):
         """Distinct triangle pairs among pair_counts(), by the same cases (device bitmap)."""
         c = np.zeros(4, dtype=np.uint64)

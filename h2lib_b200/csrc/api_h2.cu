@@ -528,6 +528,7 @@ extern "C" h2b_h2matrix *h2b_h2matrix_new_like(const h2b_bem *bem, const h2b_h2m
   for (int i = 0; i < 6; i++) h->ms[i] = 0.0f;
   h->quad_fp32 = 0;
   h->g_row_ready = 0;
+  h->g_col_copied = 0;
   h->f_S = h->f_N = nullptr;
   h->d_S = h->d_N = h->d_xp = h->d_yp = h->d_xt = h->d_yt = h->d_xio = h->d_yio = nullptr;
   h->d_mverr = nullptr;
@@ -955,11 +956,14 @@ static int col_basis(h2b_h2matrix *h) {
   // column side of the double layer: normal derivatives (assemble_bem3d_dn_lagrange_*)
   int rc;
   if (h->green && h->g_same && h->g_row_ready && h->bem->layer == H2B_SLP &&
-      h->rt.h_woff == h->ct.h_woff)
+      h->rt.h_woff == h->ct.h_woff) {
     rc = green_copy_col(h);
-  else
+    h->g_col_copied = 1;
+  } else {
     rc = h->green ? green_basis(h, h->ct, h->bem->col_basis, h->bem->layer == H2B_DLP)
                   : assemble_basis(h, h->ct, h->bem->col_basis, h->bem->layer == H2B_DLP);
+    h->g_col_copied = 0;
+  }
   mark(h, 3);
   return rc;
 }
@@ -1080,6 +1084,82 @@ extern "C" int h2b_h2matrix_green_ranks(const h2b_h2matrix *h, int side, uint32_
   H2B_CUDA_TRY(cudaMemcpyAsync(ranks, t.d_grank, sizeof(uint32_t) * t.n, cudaMemcpyDeviceToHost,
                                h->st));
   H2B_CUDA_TRY(cudaStreamSynchronize(h->st));
+  return H2B_OK;
+}
+
+extern "C" int h2b_h2matrix_export_green(const h2b_h2matrix *h, int part, double *out,
+                                         uint64_t *ndoubles) {
+  if (!h || !ndoubles || part < 0 || part > 4) {
+    h2b_set_error("h2b_h2matrix_export_green: NULL matrix or count, or part outside 0..4");
+    return H2B_ERR_ARG;
+  }
+  if (!h->green) {
+    h2b_set_error("h2b_h2matrix_export_green: not a greenhybrid H2 matrix");
+    return H2B_ERR_ARG;
+  }
+  const uint32_t K = h->k;
+  std::vector<uint32_t> rr(h->rt.n), rcr(h->ct.n);
+  H2B_CUDA_TRY(cudaMemcpyAsync(rr.data(), h->rt.d_grank, sizeof(uint32_t) * h->rt.n,
+                               cudaMemcpyDeviceToHost, h->st));
+  H2B_CUDA_TRY(cudaMemcpyAsync(rcr.data(), h->ct.d_grank, sizeof(uint32_t) * h->ct.n,
+                               cudaMemcpyDeviceToHost, h->st));
+  H2B_CUDA_TRY(cudaStreamSynchronize(h->st));
+  uint64_t n = 0;
+  if (part == 4) {
+    for (uint32_t b = 0; b < h->nadm; b++) n += (uint64_t) rr[h->h_arc[b]] * rcr[h->h_acc[b]];
+  } else {
+    const int col = part >= 2;
+    const h2b_ctree &c = col ? h->tree->col : h->tree->row;
+    const std::vector<uint32_t> &rk = col ? rcr : rr;
+    for (uint32_t i = 0; i < c.n; i++) {
+      if (part % 2 == 0 && c.sons[i] == 0) n += (uint64_t) c.size[i] * rk[i];
+      if (part % 2 == 1 && c.father[i] != UINT32_MAX) n += (uint64_t) rk[i] * rk[c.father[i]];
+    }
+  }
+  *ndoubles = n;
+  if (!out) return H2B_OK;
+  uint64_t o = 0;
+  if (part == 4) {
+    std::vector<double> S((size_t) h->nadm * K * K);
+    H2B_CUDA_TRY(cudaMemcpy(S.data(), h->d_S, sizeof(double) * S.size(), cudaMemcpyDeviceToHost));
+    for (uint32_t b = 0; b < h->nadm; b++) {
+      const uint32_t kr = rr[h->h_arc[b]], kc = rcr[h->h_acc[b]];
+      for (uint32_t j = 0; j < kc; j++)
+        for (uint32_t i = 0; i < kr; i++) out[o++] = S[(size_t) b * K * K + i + (size_t) j * K];
+    }
+    return H2B_OK;
+  }
+  const int col = part >= 2;
+  const h2b_ctree &c = col ? h->tree->col : h->tree->row;
+  const std::vector<uint32_t> &rk = col ? rcr : rr;
+  const DevCTree &t = col ? h->ct : h->rt;
+  if (part % 2 == 1) {
+    std::vector<double> E((size_t) c.n * K * K);
+    H2B_CUDA_TRY(cudaMemcpy(E.data(), t.d_gE, sizeof(double) * E.size(), cudaMemcpyDeviceToHost));
+    for (uint32_t i = 0; i < c.n; i++) {
+      if (c.father[i] == UINT32_MAX) continue;
+      const uint32_t ks = rk[i], kf = rk[c.father[i]];
+      for (uint32_t j = 0; j < kf; j++)
+        for (uint32_t r = 0; r < ks; r++) out[o++] = E[(size_t) i * K * K + r + (size_t) j * K];
+    }
+    return H2B_OK;
+  }
+  // leaf bases: the row side stores V (size x K, column-major), the column side V^T; a copied
+  // column basis has only the row side's
+  const int from_row = col && h->g_col_copied;
+  const DevCTree &tv = from_row ? h->rt : t;
+  std::vector<double> V(tv.vtotal);
+  H2B_CUDA_TRY(cudaMemcpy(V.data(), tv.d_V, sizeof(double) * V.size(), cudaMemcpyDeviceToHost));
+  uint64_t voff = 0;
+  for (uint32_t i = 0; i < c.n; i++) {
+    if (c.sons[i] != 0) continue;
+    const uint32_t sz = c.size[i], k = rk[i];
+    const double *v = V.data() + voff;
+    for (uint32_t j = 0; j < k; j++)
+      for (uint32_t r = 0; r < sz; r++)
+        out[o++] = (col && !from_row) ? v[j + (size_t) r * K] : v[r + (size_t) j * sz];
+    voff += (uint64_t) sz * K;
+  }
   return H2B_OK;
 }
 

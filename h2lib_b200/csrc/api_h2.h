@@ -63,6 +63,7 @@ struct h2b_h2matrix {
   // 1: equal row and column trees and bases (the column basis of the single layer is then the
   // row basis); g_row_ready: the row basis of the current assembly is in place
   int g_same = 0, g_row_ready = 0;
+  int g_col_copied = 0;  // the column basis was copied (its leaf bases are the row side's)
   double g_tg[9] = {}, g_wg[9] = {}, g_delta = 0.0, g_accur = 0.0;
   int cx = 0, num_sms = 148;
   int quad_fp32 = 0;  // distant-pair quadrature in FP32 (h2b_h2matrix_set_precision)

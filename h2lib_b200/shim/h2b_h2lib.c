@@ -109,6 +109,12 @@ typedef struct {
   h2b_bem *g;
   pcsurface3d gr;
   uint m;  /* interpolation order (setup_h2matrix_aprx_inter_bem3d), 0 until set */
+  /* greenhybrid farfield (setup_h2matrix_aprx_greenhybrid_bem3d with the cube points): m is then
+   * its Gauss order, and l, delta and the ACA accuracy are kept here */
+  int layer;  /* H2B_SLP / H2B_DLP / H2B_ADLP */
+  int green;
+  uint gl;
+  double gdelta, gaccur;
 } bem_rec;
 
 typedef struct {
@@ -203,6 +209,8 @@ static void attach(pbem3d bem, pcsurface3d gr, int layer, uint q, uint q2, field
   r->g = g;
   r->gr = gr;
   r->m = 0;
+  r->layer = layer;
+  r->green = 0;
   pthread_mutex_unlock(&g_lock);
   bem->nearfield = shim_nearfield;
 }
@@ -306,7 +314,37 @@ void setup_h2matrix_aprx_inter_bem3d(pbem3d bem, pcclusterbasis rb, pcclusterbas
   o_(bem, rb, cb, tree, m);
   pthread_mutex_lock(&g_lock);
   bem_rec *r = find_bem(bem);
-  if (r) r->m = m;
+  if (r) {
+    r->m = m;
+    r->green = 0;
+  }
+  pthread_mutex_unlock(&g_lock);
+}
+
+void setup_h2matrix_aprx_greenhybrid_bem3d(pbem3d bem, pcclusterbasis rb, pcclusterbasis cb,
+                                           pcblock tree, uint m, uint l, real delta, real accur,
+                                           quadpoints3d quadpoints) {
+  ORIGINAL(setup_h2matrix_aprx_greenhybrid_bem3d);
+  o_(bem, rb, cb, tree, m, l, delta, accur, quadpoints);
+  pthread_mutex_lock(&g_lock);
+  bem_rec *r = find_bem(bem);
+  if (r) {
+    /* the device builds the Laplace single and double layer with the cube points */
+#ifdef USE_COMPLEX
+    const int device = 0;
+#else
+    const int device = quadpoints == build_bem3d_cube_quadpoints && r->layer != H2B_ADLP;
+#endif
+    if (device) {
+      r->m = m;
+      r->green = 1;
+      r->gl = l;
+      r->gdelta = delta;
+      r->gaccur = accur;
+    } else {
+      r->green = -1;  /* other point sets: the H2 matrices stay on H2Lib's CPU path */
+    }
+  }
   pthread_mutex_unlock(&g_lock);
 }
 
@@ -523,7 +561,53 @@ static void fill_basis(pclusterbasis cb, uint k, basis_cursor *c, int is_root) {
   for (uint s = 0; s < cb->sons; s++) fill_basis(cb->son[s], k, c, 0);
 }
 
-static void fill_bases(const h2b_h2matrix *h, pclusterbasis rb, pclusterbasis cb, uint k) {
+/* Greenhybrid bases: per-cluster ranks (pre-order ids), V_t (|t| x k_t) and E_s (k_s x k_father),
+ * as assemble_bem3d_greenhybrid_leaf_row_clusterbasis / _transfer_row_ leave them
+ * (Library/bem3d.c:6194/6262). */
+static void fill_green_basis(pclusterbasis cb, const uint32_t *rank, uint *id, basis_cursor *c,
+                             uint kf, int is_root) {
+  const uint k = rank[(*id)++];
+  cb->k = k;
+  if (!is_root) {
+    resize_amatrix(&cb->E, k, kf);
+    c->E = copy_into(&cb->E, c->E, 0);
+  }
+  if (cb->sons == 0) {
+    resize_amatrix(&cb->V, cb->t->size, k);
+    c->V = copy_into(&cb->V, c->V, 0);
+  } else {
+    resize_amatrix(&cb->V, 0, k);
+  }
+  for (uint s = 0; s < cb->sons; s++) fill_green_basis(cb->son[s], rank, id, c, k, 0);
+}
+
+static double *export_green(const h2b_h2matrix *h, int part) {
+  uint64_t n = 0;
+  check(h2b_h2matrix_export_green(h, part, NULL, &n), "h2b_h2matrix_export_green");
+  double *buf = (double *) malloc(sizeof(double) * (n ? n : 1));
+  if (!buf) die("out of host memory");
+  check(h2b_h2matrix_export_green(h, part, buf, &n), "h2b_h2matrix_export_green");
+  return buf;
+}
+
+static void fill_bases(const h2b_h2matrix *h, pclusterbasis rb, pclusterbasis cb, uint k,
+                       int green) {
+  for (int side = 0; side < 2 && green; side++) {
+    pclusterbasis b = side ? cb : rb;
+    if (!b) continue;
+    uint32_t *rank = (uint32_t *) malloc(sizeof(uint32_t) * b->t->desc);
+    if (!rank) die("out of host memory");
+    check(h2b_h2matrix_green_ranks(h, side, rank), "h2b_h2matrix_green_ranks");
+    double *V = export_green(h, side ? 2 : 0), *E = export_green(h, side ? 3 : 1);
+    basis_cursor c = {V, E};
+    uint id = 0;
+    fill_green_basis(b, rank, &id, &c, 0, 1);
+    update_tree_clusterbasis(b);
+    free(V);
+    free(E);
+    free(rank);
+  }
+  if (green) return;
   for (int side = 0; side < 2; side++) {
     pclusterbasis b = side ? cb : rb;
     if (!b) continue;
@@ -537,15 +621,19 @@ static void fill_bases(const h2b_h2matrix *h, pclusterbasis rb, pclusterbasis cb
   }
 }
 
-static void fill_blocks(const h2b_h2matrix *h, const leaf_list *l, int near, int far, uint k) {
+static void fill_blocks(const h2b_h2matrix *h, const leaf_list *l, int near, int far, uint k,
+                        int green) {
   uint64_t n;
   if (far) {
-    double *S = export_part(h, 4, &n);
+    /* greenhybrid couplings are k_row x k_col with the ranks of the host bases, which the
+     * basis assembly has filled (assemble_bem3d_greenhybrid_uniform, Library/bem3d.c:6493) */
+    double *S = green ? export_green(h, 4) : export_part(h, 4, &n);
     const double *p = S;
     for (uint i = 0; i < l->n; i++)
       if (l->adm[i]) {
         puniform U = l->leaf[i]->u;
-        resize_amatrix(&U->S, k, k);
+        if (green) resize_amatrix(&U->S, U->rb->k, U->cb->k);
+        else resize_amatrix(&U->S, k, k);
         p = copy_into(&U->S, p, 1);
       }
     free(S);
@@ -565,11 +653,20 @@ static void fill_blocks(const h2b_h2matrix *h, const leaf_list *l, int near, int
 
 static bem_rec *h2_bem(pcbem3d bem, const char *who) {
   bem_rec *r = g_bypass ? NULL : find_bem(bem);
+  if (r && r->green < 0) return NULL;
   if (r && r->m == 0) {
     fprintf(stderr, "h2b_h2lib: %s before setup_h2matrix_aprx_inter_bem3d\n", who);
     abort();
   }
   return r;
+}
+
+static h2b_h2matrix *new_matrix(const bem_rec *r, h2b_tree *tree) {
+  h2b_h2matrix *h = r->green > 0 ? h2b_h2matrix_new_greenhybrid(r->g, tree, r->m, r->gl,
+                                                                r->gdelta, r->gaccur)
+                                 : h2b_h2matrix_new(r->g, tree, r->m);
+  if (!h) die(r->green > 0 ? "h2b_h2matrix_new_greenhybrid" : "h2b_h2matrix_new");
+  return h;
 }
 
 static void basis_assembly(pcbem3d bem, pclusterbasis b, int column) {
@@ -587,13 +684,12 @@ static void basis_assembly(pcbem3d bem, pclusterbasis b, int column) {
     return;
   }
   h2b_tree *tree = device_tree(NULL, b, NULL);
-  h2b_h2matrix *h = h2b_h2matrix_new(r->g, tree, r->m);
-  if (!h) die("h2b_h2matrix_new");
+  h2b_h2matrix *h = new_matrix(r, tree);
   check(column ? h2b_h2matrix_assemble_col_clusterbasis(h)
                : h2b_h2matrix_assemble_row_clusterbasis(h), "cluster basis assembly");
   uint64_t info[8];
   check(h2b_h2matrix_info(h, info), "h2b_h2matrix_info");
-  fill_bases(h, column ? NULL : b, column ? b : NULL, (uint) info[7]);
+  fill_bases(h, column ? NULL : b, column ? b : NULL, (uint) info[7], r->green > 0);
   h2b_h2matrix_del(h);
   h2b_tree_del(tree);
   pthread_mutex_unlock(&g_lock);
@@ -623,8 +719,7 @@ static int h2_assembly(pbem3d bem, ph2matrix G, int what) {
     }
   leaf_list l;
   h2b_tree *tree = device_tree(G, NULL, &l);
-  h2b_h2matrix *h = h2b_h2matrix_new(r->g, tree, r->m);
-  if (!h) die("h2b_h2matrix_new");
+  h2b_h2matrix *h = new_matrix(r, tree);
   uint64_t info[8];
   check(h2b_h2matrix_info(h, info), "h2b_h2matrix_info");
   const uint k = (uint) info[7];
@@ -632,14 +727,14 @@ static int h2_assembly(pbem3d bem, ph2matrix G, int what) {
     // the bases as well: the device matrix serves later products and solves; H2Lib's host bases
     // receive the same values its own basis assembly would give
     check(h2b_h2matrix_assemble_all(h), "h2b_h2matrix_assemble_all");
-    fill_bases(h, G->rb, G->cb, k);
-    fill_blocks(h, &l, 1, 1, k);
+    fill_bases(h, G->rb, G->cb, k, r->green > 0);
+    fill_blocks(h, &l, 1, 1, k, r->green > 0);
   } else if (what == 1) {
     check(h2b_h2matrix_assemble_nearfield(h), "h2b_h2matrix_assemble_nearfield");
-    fill_blocks(h, &l, 1, 0, k);
+    fill_blocks(h, &l, 1, 0, k, r->green > 0);
   } else {
     check(h2b_h2matrix_assemble_farfield(h), "h2b_h2matrix_assemble_farfield");
-    fill_blocks(h, &l, 0, 1, k);
+    fill_blocks(h, &l, 0, 1, k, r->green > 0);
   }
   leaves_free(&l);
   if (what == 0) {

@@ -247,6 +247,14 @@ h2b_h2matrix *h2b_h2matrix_new_greenhybrid(const h2b_bem *bem, const h2b_tree *t
 /* Ranks of the greenhybrid cluster bases (side 0 row, 1 column), one per cluster in the tree's
  * pre-order: ranks[clusters]. */
 int h2b_h2matrix_green_ranks(const h2b_h2matrix *h, int side, uint32_t *ranks);
+/* The greenhybrid bases and couplings in H2Lib's layouts with their per-cluster ranks (what the
+ * reference's assemble_bem3d_greenhybrid_* callbacks leave in the clusterbasis and uniform
+ * structs): part 0 / 2 the row / column leaf bases V_t (|t| x k_t, column-major, leaves in
+ * pre-order), 1 / 3 the transfers E_s (k_s x k_father, column-major, non-root clusters in
+ * pre-order), 4 the coupling matrices S (k_row x k_col, column-major, admissible blocks in the
+ * tree's block order).  The nearfield is h2b_h2matrix_export part 5.  out NULL: only the count
+ * in *ndoubles. */
+int h2b_h2matrix_export_green(const h2b_h2matrix *h, int part, double *out, uint64_t *ndoubles);
 void h2b_h2matrix_del(h2b_h2matrix *h2);
 
 /* Assembly.  Replace assemble_bem3d_h2matrix_row_clusterbasis (Library/bem3d.c:10407),

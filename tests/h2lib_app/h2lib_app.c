@@ -8,7 +8,8 @@
  * the shim bypassed, i.e. H2Lib's own CPU code on the host structures the shim filled.
  *
  * Real build (Laplace): sphere refined x8, dense cc single layer; linear-basis single and double
- * layer H2 matrices (leaf 16, eta 1.4, m 3), products, and the interior Dirichlet GMRES(50) solve.
+ * layer H2 matrices (leaf 16, eta 1.4, m 3), products, and the interior Dirichlet GMRES(50) solve;
+ * greenhybrid single and double layer H2 matrices on the sphere scaled and turned, products.
  * Complex build (Helmholtz, k = 2): the same sphere, constant basis: a single-layer block through
  * the nearfield callback, the dense double layer, single and double layer H2 matrices (leaf 16,
  * eta 1.4, m 3), products and a GMRES solve of V.
@@ -82,6 +83,40 @@ static void seeded(pavector x) {
 #endif
   }
 }
+
+/* Greenhybrid H2 matrix of `op` (m 2, l 1, delta 1, accuracy 5e-3, cube points: the reference
+ * test's parameters), assembled the way Tests/test_laplacebem3d.c does it. */
+#ifndef USE_COMPLEX
+static ph2matrix green_of(pbem3d op, pcluster root, pblock broot) {
+  pclusterbasis rb = build_from_cluster_clusterbasis(root);
+  pclusterbasis cb = build_from_cluster_clusterbasis(root);
+  ph2matrix G = build_from_block_h2matrix(broot, rb, cb);
+  setup_h2matrix_aprx_greenhybrid_bem3d(op, rb, cb, broot, 2, 1, 1.0, 5e-3,
+                                        build_bem3d_cube_quadpoints);
+  assemble_bem3d_h2matrix_row_clusterbasis(op, rb);
+  assemble_bem3d_h2matrix_col_clusterbasis(op, cb);
+  assemble_bem3d_h2matrix(op, G);
+  return G;
+}
+
+/* the sphere scaled to an ellipsoid and turned out of the axes (no pivot ties in the cross
+ * approximations, whose winners would otherwise depend on the last bit of a quadrature sum) */
+static void turn(psurface3d gr) {
+  const real ax[3] = { 1.0, 0.8, 0.65 }, ca = cos(0.37), sa = sin(0.37), cb = cos(0.61),
+             sb = sin(0.61), cc = cos(0.23), sc = sin(0.23);
+  for (uint v = 0; v < gr->vertices; v++) {
+    real p0 = gr->x[v][0] * ax[0], p1 = gr->x[v][1] * ax[1], p2 = gr->x[v][2] * ax[2], q0, q1, q2;
+    q1 = cc * p1 - sc * p2;
+    q2 = sc * p1 + cc * p2;
+    q0 = cb * p0 + sb * q2;
+    q2 = -sb * p0 + cb * q2;
+    gr->x[v][0] = ca * q0 - sa * q1;
+    gr->x[v][1] = sa * q0 + ca * q1;
+    gr->x[v][2] = q2;
+  }
+  prepare_surface3d(gr);
+}
+#endif
 
 /* H2 matrix of `op` on the tree of `root`, assembled the way H2Lib's tests do it. */
 static ph2matrix h2_of(pbem3d op, pcluster root, pblock broot, uint m) {
@@ -192,6 +227,33 @@ int main(int argc, char **argv) {
     del_cluster(root);
     del_laplace_bem3d(slp);
     del_laplace_bem3d(dlp);
+  }
+  {
+    /* greenhybrid single and double layer on the turned ellipsoid */
+    psurface3d ge = build_from_macrosurface3d_surface3d(mg, 8);
+    pbem3d slp, dlp;
+    ph2matrix V, K;
+    pavector x;
+    turn(ge);
+    slp = new_slp_laplace_bem3d(ge, 2, 4, BASIS_LINEAR_BEM3D, BASIS_LINEAR_BEM3D);
+    dlp = new_dlp_laplace_bem3d(ge, 2, 4, BASIS_LINEAR_BEM3D, BASIS_LINEAR_BEM3D, 0.5);
+    root = build_bem3d_cluster(slp, 16, BASIS_LINEAR_BEM3D);
+    broot = build_strict_block(root, root, &eta, admissible_max_cluster);
+    V = green_of(slp, root, broot);
+    K = green_of(dlp, root, broot);
+    x = new_avector(ge->vertices);
+    seeded(x);
+    products("Vg", V, x);
+    products("Kg", K, x);
+    del_avector(x);
+    del_h2matrix(V);
+    del_h2matrix(K);
+    del_block(broot);
+    freemem(root->idx);
+    del_cluster(root);
+    del_laplace_bem3d(slp);
+    del_laplace_bem3d(dlp);
+    del_surface3d(ge);
   }
 #else
   {

@@ -18,6 +18,20 @@ GOLD = os.path.join(os.path.dirname(__file__), "golden", "green.npz")
 L, C = hb.BASIS_LINEAR_BEM3D, hb.BASIS_CONSTANT_BEM3D
 
 
+def _fathers(sons):
+    """Father of every cluster of a pre-order tree given the son counts (-1 for the root)."""
+    father = np.full(len(sons), -1)
+    stack = []
+    for i in range(len(sons)):
+        while stack and stack[-1][1] == 0:
+            stack.pop()
+        if stack:
+            father[i] = stack[-1][0]
+            stack[-1][1] -= 1
+        stack.append([i, int(sons[i])])
+    return father
+
+
 def _op(prefix, gr):
     if prefix == "gsll":
         return hb.new_slp_laplace_bem3d(gr, 2, 4, L, L), L
@@ -40,6 +54,37 @@ def test_greenhybrid_matches_reference(prefix):
     ref = d[f"{prefix}_y"]
     err = np.linalg.norm(y - ref) / np.linalg.norm(ref)
     assert bad == [0, 0] and err <= 1e-10, (bad, err)
+    # the bases and the first coupling matrices themselves, in H2Lib's layouts: every leaf
+    # basis, and the transfers into every father whose basis the matrix uses (a cluster of an
+    # admissible block or below one).  The fathers above them are never used; their cross
+    # approximations run to ranks near min(rows, columns), where the last pivots are chosen
+    # among residuals that cancellation has left with few correct digits, so either code's
+    # rounding picks its own (equally accurate) pivots there.
+    rec, blocks = d[f"{prefix}_ctree"].astype(np.int64), d[f"{prefix}_blocks"].astype(np.int64)
+    father = _fathers(rec[:, 2])
+    for side, (po, ps) in ((0, (0, 1)), (1, (2, 3))):
+        k = d[f"{prefix}_{'row' if side == 0 else 'col'}_k"].astype(np.int64)
+        used = np.zeros(len(rec), dtype=bool)
+        key = {(int(o), int(z)): i for i, (o, z) in enumerate(rec[:, :2])}
+        for b in blocks[blocks[:, 4] == 1]:
+            used[key[(int(b[po]), int(b[ps]))]] = True
+        for i in range(len(rec)):
+            used[i] |= father[i] >= 0 and used[father[i]]
+        name = "row" if side == 0 else "col"
+        gV, wV = H.export_green(2 * side), d[f"{prefix}_{name}_V"]
+        assert gV.shape == wV.shape and np.max(np.abs(gV - wV)) <= 1e-9 * np.max(np.abs(wV))
+        gE, wE = H.export_green(2 * side + 1), d[f"{prefix}_{name}_E"]
+        assert gE.shape == wE.shape
+        o = 0
+        for i in range(len(rec)):
+            if father[i] < 0:
+                continue
+            n = int(k[i] * k[father[i]])
+            if used[father[i]]:
+                assert np.max(np.abs(gE[o:o + n] - wE[o:o + n])) <= 1e-9 * np.max(np.abs(wE)), i
+            o += n
+    S, want = H.export_green(4), d[f"{prefix}_parts_S"]
+    assert np.max(np.abs(S[:want.size] - want)) <= 1e-10 * np.max(np.abs(want))
 
 
 def test_greenhybrid_like_and_accuracy():

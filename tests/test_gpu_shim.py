@@ -12,6 +12,9 @@ Compared (the tolerances of the other GPU parity tests):
   * solve_gmres_h2matrix_avector and solve_gmres_avector with addeval_h2matrix_avector: iteration
     count within one (the device GMRES applies the Householder reflectors in another order) and
     solution to 1e-6;
+  * greenhybrid single and double layer products on a turned ellipsoid (1e-10), from the device
+    and from H2Lib's CPU code on the bases, transfers and couplings with per-cluster ranks that
+    the shim wrote back;
   * the Helmholtz build: a single-layer block through the bem->nearfield plugin point, the dense
     double layer matrix, the products and a GMRES solve of the single layer operator;
 and the shim's counters show that the device did the work.
@@ -65,6 +68,12 @@ def test_h2lib_program_through_the_shim(field):
         assert relerr(gpu["b"], cpu["b"]) < 1e-12
         assert abs(gpu["gmres_iter2"][0] - cpu["gmres_iter2"][0]) <= 1
         assert relerr(gpu["u2"], cpu["u2"]) < 1e-6
+        # greenhybrid (setup_h2matrix_aprx_greenhybrid_bem3d): the device's products, and H2Lib's
+        # own product on the per-cluster-rank bases and couplings the shim wrote back
+        for op in ("Vg", "Kg"):
+            assert relerr(gpu[f"y{op}"], cpu[f"y{op}"]) < 1e-10
+            assert relerr(gpu[f"y{op}_acc"], cpu[f"y{op}_acc"]) < 1e-10
+            assert relerr(gpu[f"y{op}_host"], cpu[f"y{op}"]) < 1e-10
     else:
         b = cpu["block_slp"].reshape(5, 7).T
         assert rel_entry_err(gpu["block_slp"].reshape(5, 7).T, b) < 1e-12
