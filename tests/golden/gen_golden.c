@@ -872,7 +872,7 @@ section_h2small(void)
 
 /* Greenhybrid H2 matrices (the reference's Laplace test parameters m 2, l 1, delta 1, accuracy
  * 5e-3) on the sphere refined 8 times, scaled to an ellipsoid and turned: single layer with
- * linear and constant bases, double layer with linear bases. */
+ * linear and constant bases, double layer with linear and constant bases. */
 static void
 section_green(void)
 {
@@ -906,6 +906,9 @@ section_green(void)
   del_bem3d(slp_c);
   dlp_l = new_dlp_laplace_bem3d(gr, 2, 4, BASIS_LINEAR_BEM3D, BASIS_LINEAR_BEM3D, 0.5);
   green_op("gdll", gr, dlp_l, BASIS_LINEAR_BEM3D, 16, 1.4, 2, 1, 1.0, 5e-3, 24);
+  del_bem3d(dlp_l);
+  dlp_l = new_dlp_laplace_bem3d(gr, 2, 4, BASIS_CONSTANT_BEM3D, BASIS_CONSTANT_BEM3D, 0.5);
+  green_op("gdcc", gr, dlp_l, BASIS_CONSTANT_BEM3D, 16, 1.4, 2, 1, 1.0, 5e-3, 24);
   del_bem3d(dlp_l);
   del_surface3d(gr);
   del_macrosurface3d(mg);

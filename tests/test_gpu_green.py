@@ -37,10 +37,12 @@ def _op(prefix, gr):
         return hb.new_slp_laplace_bem3d(gr, 2, 4, L, L), L
     if prefix == "gscc":
         return hb.new_slp_laplace_bem3d(gr, 2, 4, C, C), C
+    if prefix == "gdcc":
+        return hb.new_dlp_laplace_bem3d(gr, 2, 4, C, C, 0.5), C
     return hb.new_dlp_laplace_bem3d(gr, 2, 4, L, L, 0.5), L
 
 
-@pytest.mark.parametrize("prefix", ["gsll", "gscc", "gdll"])
+@pytest.mark.parametrize("prefix", ["gsll", "gscc", "gdll", "gdcc"])
 def test_greenhybrid_matches_reference(prefix):
     d = np.load(GOLD)
     gr = hb.Surface3d(d["green_x"], d["green_t"])

@@ -13,7 +13,7 @@ from h2lib_b200 import bem3d as hb
 
 GOLD = os.path.join(os.path.dirname(__file__), "golden", "green.npz")
 CASES = [("gsll", hb.BASIS_LINEAR_BEM3D), ("gscc", hb.BASIS_CONSTANT_BEM3D),
-         ("gdll", hb.BASIS_LINEAR_BEM3D)]
+         ("gdll", hb.BASIS_LINEAR_BEM3D), ("gdcc", hb.BASIS_CONSTANT_BEM3D)]
 
 
 @pytest.mark.parametrize("prefix,basis", CASES)
