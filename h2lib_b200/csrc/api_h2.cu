@@ -976,7 +976,13 @@ static int coupling(h2b_h2matrix *h) {
                          h->ct.d_gpiv, h->d_S, h->nadm, (int) h->k, (int) h->bem->q,
                          h->bem->row_basis == H2B_BASIS_LINEAR,
                          h->bem->col_basis == H2B_BASIS_LINEAR, h->bem->layer == H2B_DLP,
-                         h->bem->kconst};
+                         h->bem->kconst, 0};
+    uint32_t deg = 1;
+    if (h->bem->col_basis == H2B_BASIS_LINEAR) {
+      const h2b_adjacency &adj = h->bem->s->adj;
+      for (uint32_t v = 0; v < adj.nv; v++) deg = std::max(deg, adj.off[v + 1] - adj.off[v]);
+    }
+    ga.max_elems = h->k * deg;
     const int rc = h2b_green_coupling(&ga, h->st);
     mark(h, 5);
     return rc;

@@ -64,6 +64,8 @@ struct GreenCouplingArgs {
   uint32_t n;
   int K, q, rlinear, clinear, dlp;
   double kconst;
+  uint32_t max_elems;  // bound on a block's column triangles over its pivots (K x the largest
+                       // vertex degree, or K for constant bases)
 };
 
 extern "C" {

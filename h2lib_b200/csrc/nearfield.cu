@@ -1482,12 +1482,113 @@ __global__ void __launch_bounds__(256) green_coupling_kernel(GreenCouplingArgs a
   }
 }
 
+// The same entries with the column triangles staged once per block: for every pivot column its
+// triangles' four rule points, their weights times the basis function, Gram determinant and
+// 1/(4 pi), and the normal (q = 2).  A thread then reads its column's triangles from shared
+// memory instead of forming their points once per row triangle.
+template <bool RL, bool CL, bool DLP>
+__global__ void __launch_bounds__(256) green_coupling_staged_kernel(GreenCouplingArgs a) {
+  extern __shared__ __align__(16) unsigned char gsm[];
+  constexpr int P = 4;
+  const uint32_t b = blockIdx.x;
+  const uint32_t rc = a.adm_rc[b], cc = a.adm_cc[b];
+  const uint32_t K = (uint32_t) a.K, kr = a.rrank[rc], kc = a.crank[cc];
+  const uint32_t *pr = a.rpiv + (size_t) rc * K, *pc = a.cpiv + (size_t) cc * K;
+  double *S = a.S + (size_t) b * K * K;
+  const double(&sd)[6][SIDE_MAXP] = c_side[1];
+  uint32_t *coff = reinterpret_cast<uint32_t *>(gsm);           // K + 1 (padded to 16 bytes)
+  double *cy = reinterpret_cast<double *>(gsm + 16 * ((4 * (K + 1) + 15) / 16));
+  const uint32_t emax = (uint32_t) a.max_elems;
+  double *cw = cy + (size_t) emax * 3 * P;                        // emax x P weights
+  double *cn = cw + (size_t) emax * P;                            // emax x 3 normals
+  if (threadIdx.x == 0) {
+    uint32_t o = 0;
+    for (uint32_t j = 0; j < kc; j++) {
+      coff[j] = o;
+      o += CL ? a.vt_off[pc[j] + 1] - a.vt_off[pc[j]] : 1u;
+    }
+    coff[kc] = o;
+  }
+  __syncthreads();
+  for (uint32_t j = threadIdx.x; j < kc; j += blockDim.x) {
+    const uint32_t bj = pc[j];
+    const uint32_t u0 = CL ? a.vt_off[bj] : 0u, u1 = CL ? a.vt_off[bj + 1] : 1u;
+    for (uint32_t u = u0; u < u1; u++) {
+      const uint32_t f = coff[j] + (u - u0);
+      const TriRec &Sx = a.tri[CL ? a.vt_tri[u] : bj];
+      const int cs = CL ? (Sx.v[0] == bj ? 0 : (Sx.v[1] == bj ? 1 : 2)) : 0;
+      const double gk = Sx.g * a.kconst;
+      for (int p = 0; p < P; p++) {
+        const double ty = sd[0][p], sy = sd[1][p];
+        const double ay = 1.0 - ty, by = ty - sy, cy_ = sy;
+        for (int d = 0; d < 3; d++)
+          cy[((size_t) f * P + p) * 3 + d] = Sx.a[d] * ay + Sx.b[d] * by + Sx.c[d] * cy_;
+        cw[(size_t) f * P + p] = (CL ? sd[3 + cs][p] : sd[2][p]) * gk;
+      }
+      for (int d = 0; d < 3; d++) cn[(size_t) f * 3 + d] = Sx.n[d];
+    }
+  }
+  __syncthreads();
+  for (uint32_t e = threadIdx.x; e < K * K; e += blockDim.x) {
+    const uint32_t i = e % K, j = e / K;
+    double acc = 0.0;
+    if (i < kr && j < kc) {
+      const uint32_t bi = pr[i];
+      const uint32_t t0 = RL ? a.vt_off[bi] : 0u, t1 = RL ? a.vt_off[bi + 1] : 1u;
+      const uint32_t f0 = coff[j], f1 = coff[j + 1];
+      for (uint32_t ti = t0; ti < t1; ti++) {
+        const TriRec &T = a.tri[RL ? a.vt_tri[ti] : bi];
+        const int ct = RL ? (T.v[0] == bi ? 0 : (T.v[1] == bi ? 1 : 2)) : 0;
+        double xa[P][3], wa[P];
+#pragma unroll
+        for (int p = 0; p < P; p++) {
+          const double tx = sd[0][p], sx = sd[1][p];
+          const double ax = 1.0 - tx, bx = tx - sx, cx = sx;
+#pragma unroll
+          for (int d = 0; d < 3; d++) xa[p][d] = T.a[d] * ax + T.b[d] * bx + T.c[d] * cx;
+          wa[p] = RL ? sd[3 + ct][p] : sd[2][p];
+        }
+        double part = 0.0;
+        for (uint32_t f = f0; f < f1; f++) {
+          const double *y = cy + (size_t) f * P * 3, *w = cw + (size_t) f * P;
+          const double n0 = cn[3 * (size_t) f], n1 = cn[3 * (size_t) f + 1],
+                       n2 = cn[3 * (size_t) f + 2];
+#pragma unroll
+          for (int p = 0; p < P; p++) {
+            const double y0 = y[3 * p], y1 = y[3 * p + 1], y2 = y[3 * p + 2];
+            double pb = 0.0;
+#pragma unroll
+            for (int r = 0; r < P; r++) {
+              const double d0 = xa[r][0] - y0, d1 = xa[r][1] - y1, d2 = xa[r][2] - y2;
+              const double ri = rsqrt_nr(fma(d0, d0, fma(d1, d1, d2 * d2)));
+              const double fv = DLP ? fma(d0, n0, fma(d1, n1, d2 * n2)) * (ri * ri * ri) : ri;
+              pb = fma(wa[r], fv, pb);
+            }
+            part = fma(w[p], pb, part);
+          }
+        }
+        acc += part * T.g;
+      }
+    }
+    S[i + (size_t) j * K] = acc;
+  }
+}
+
+size_t green_coupling_smem(int K, uint32_t max_elems) {
+  return 16 * ((4 * ((size_t) K + 1) + 15) / 16) + sizeof(double) * (size_t) max_elems * (12 + 4 + 3);
+}
+
 template <bool RL, bool CL, bool DLP>
 static int launch_green_coupling(const GreenCouplingArgs *a, cudaStream_t st) {
-  if (a->q == 2)
+  const size_t smem = green_coupling_smem(a->K, a->max_elems);
+  if (a->q == 2 && smem <= H2B_MAX_DYN_SMEM) {
+    H2B_CUDA_TRY((h2b_allow_smem<green_coupling_staged_kernel<RL, CL, DLP>>()));
+    green_coupling_staged_kernel<RL, CL, DLP><<<a->n, 256, smem, st>>>(*a);
+  } else if (a->q == 2) {
     green_coupling_kernel<2, RL, CL, DLP><<<a->n, 256, 0, st>>>(*a);
-  else
+  } else {
     green_coupling_kernel<0, RL, CL, DLP><<<a->n, 256, 0, st>>>(*a);
+  }
   h2b_note_launch();
   H2B_CUDA_TRY(cudaGetLastError());
   return H2B_OK;
