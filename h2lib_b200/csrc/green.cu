@@ -24,16 +24,8 @@ __device__ __forceinline__ Best better(Best a, Best b) {
   return (b.v > a.v || (b.v == a.v && b.l < a.l)) ? b : a;
 }
 
-// Largest |A(i, j)|^2 over i, j >= k (A column-major, ld = rows), the same in every thread.
-__device__ Best block_argmax(const double *A, uint32_t rows, uint32_t cols, uint32_t k,
-                             Best *red) {
-  Best b{0.0, 0xFFFFFFFFu};
-  const uint32_t nr = rows - k, tot = nr * (cols - k);
-  for (uint32_t e = threadIdx.x; e < tot; e += blockDim.x) {
-    const uint32_t i = k + e % nr, j = k + e / nr;
-    const double a = A[i + (size_t) j * rows];
-    b = better(b, Best{a * a, j * rows + i});
-  }
+// The CTA's best of every thread's candidate b, the same in every thread.
+__device__ Best block_best(Best b, Best *red) {
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) {
     Best c;
@@ -51,6 +43,19 @@ __device__ Best block_argmax(const double *A, uint32_t rows, uint32_t cols, uint
   }
   __syncthreads();
   return red[GT / 32];
+}
+
+// Largest |A(i, j)|^2 over i, j >= k (A column-major, ld = rows), the same in every thread.
+__device__ Best block_argmax(const double *A, uint32_t rows, uint32_t cols, uint32_t k,
+                             Best *red) {
+  Best b{0.0, 0xFFFFFFFFu};
+  const uint32_t nr = rows - k, tot = nr * (cols - k);
+  for (uint32_t e = threadIdx.x; e < tot; e += blockDim.x) {
+    const uint32_t i = k + e % nr, j = k + e / nr;
+    const double a = A[i + (size_t) j * rows];
+    b = better(b, Best{a * a, j * rows + i});
+  }
+  return block_best(b, red);
 }
 
 // Quadrature points and weighted normals of the widened box surface (build_bem3d_cube_quadpoints,
@@ -226,17 +231,21 @@ __global__ void __launch_bounds__(GT) green_basis_kernel(GreenArgs g) {
     const double aij = 1.0 / A[k + (size_t) k * rows];
     for (uint32_t i = k + 1 + threadIdx.x; i < rows; i += blockDim.x) A[i + (size_t) k * rows] *= aij;
     __syncthreads();
+    // the rank-one update, and the next pivot search over the entries it writes (the remaining
+    // submatrix is exactly those)
     const uint32_t nr = rows - k - 1, nc = cols - k - 1;
+    Best cand{0.0, 0xFFFFFFFFu};
     for (uint32_t e = threadIdx.x; e < nr * nc; e += blockDim.x) {
       const uint32_t i = k + 1 + e % nr, j = k + 1 + e / nr;
       // no contraction: a - (l u) rounded as the reference's scalar loop rounds it
-      A[i + (size_t) j * rows] =
-          __dsub_rn(A[i + (size_t) j * rows], __dmul_rn(A[i + (size_t) k * rows], A[k + (size_t) j * rows]));
+      const double v = __dsub_rn(A[i + (size_t) j * rows],
+                                 __dmul_rn(A[i + (size_t) k * rows], A[k + (size_t) j * rows]));
+      A[i + (size_t) j * rows] = v;
+      cand = better(cand, Best{v * v, j * rows + i});
     }
-    __syncthreads();
     k++;
+    bst = block_best(cand, red);  // its barriers also order the update before the next swaps
     if (k >= maxrank) break;
-    bst = block_argmax(A, rows, cols, k, red);
   }
 
   // V = C (C on the pivot rows)^-1 (copy_lower_aca_amatrix + triangularsolve_amatrix,
