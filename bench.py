@@ -775,8 +775,9 @@ def run_dense(a, peak):
 
 def run_green(a):
     """Laplace single layer with the greenhybrid farfield (setup_h2matrix_aprx_greenhybrid_bem3d,
-    Library/bem3d.c:9689; the reference test's m 2, l 1, delta 1, accuracy 5e-3) on the config-2
-    sphere and tree: per-phase device times of the assembly, the matvec, the ranks, the product's
+    Library/bem3d.c:9689; the reference test's m 2, l 1, delta 1, accuracy 5e-3) on the sphere
+    and tree of the headline workload (split 64, 32768 triangles, leaf 64, eta 1.4 by default):
+    per-phase device times of the assembly, the matvec, the ranks, the product's
     distance from the interpolation H2 matrix (m 4), and the reference's CPU assembly of the same
     matrix (oracle/_ref/ref_bench green)."""
     from h2lib_b200 import bem3d as hb
