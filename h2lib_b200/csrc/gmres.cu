@@ -134,13 +134,22 @@ __device__ __forceinline__ void block_dots(const GmresDev &g, const Sys &v, uint
                                            uint32_t k, F pj) {
   __shared__ double ws[2][TPB / 32][GMRES_KMAX + 1];
   const uint32_t lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  for (uint32_t j = 0; j <= k; j++) {
-    const cd p = pj(j);
-    const double sr = warp_sum(p.re);
-    const double si = CX ? warp_sum(p.im) : 0.0;
-    if (lane == 0) {
-      ws[0][w][j] = sr;
-      ws[1][w][j] = si;
+  // eight columns at a time: their loads are issued together and their eight shuffle trees
+  // interleave, instead of one load and one dependent tree per column (each column's sum is
+  // the same tree either way)
+  constexpr uint32_t CH = 8;
+  for (uint32_t j0 = 0; j0 <= k; j0 += CH) {
+    cd p[CH];
+#pragma unroll
+    for (uint32_t u = 0; u < CH; u++) p[u] = j0 + u <= k ? pj(j0 + u) : cd{0.0, 0.0};
+#pragma unroll
+    for (uint32_t u = 0; u < CH; u++) {
+      const double sr = warp_sum(p[u].re);
+      const double si = CX ? warp_sum(p[u].im) : 0.0;
+      if (lane == 0 && j0 + u <= k) {
+        ws[0][w][j0 + u] = sr;
+        ws[1][w][j0 + u] = si;
+      }
     }
   }
   __syncthreads();
